@@ -1,0 +1,244 @@
+"""Dense assembly and potential evaluation on the device.
+
+``assemble_dense_device`` is the fused replacement of
+``bempp_cl.core.dense_assembler.assemble_dense`` (core/dense_assembler.py:49-98):
+the regular pass and the singular correction both run on the GPU and the
+matrix stays in HBM as a torch tensor.  The functions below take the
+reference's own descriptor / space / parameter objects (duck-typed: a
+``bempp_cl`` object and the matching ``bempp_cuda`` object both work).
+
+Precision: ``device_interface`` "cuda" is FP64 end to end; "cuda_mixed"
+evaluates regular DP0 pairs in FP32 (see csrc/regular.cu) and keeps the
+singular pairs in FP64.  Everything else in "cuda_mixed" stays FP64.
+"""
+
+import numpy as _np
+import torch as _torch
+
+from . import _lib
+from .device import (
+    current_stream,
+    device_grid,
+    device_singular_rule,
+    device_space,
+    ptr,
+    require_cuda,
+)
+from .quadrature import triangle_rule
+
+_REG_CACHE = {}
+
+
+def precision_of(device_interface):
+    parts = str(device_interface).split("_")
+    if parts[0] != "cuda":
+        raise ValueError("device interface %r is not a cuda interface" % (device_interface,))
+    if len(parts) > 1 and parts[1] == "mixed":
+        return _lib.MIXED
+    return _lib.FP64
+
+
+def kernel_ids(descriptor):
+    try:
+        kernel = _lib.KERNEL_IDS[descriptor.kernel_type]
+        assembly = _lib.ASSEMBLY_IDS[descriptor.assembly_type]
+    except KeyError as exc:
+        raise ValueError("operator %r is not supported by the cuda interface" % (descriptor.identifier,)) from exc
+    return kernel, assembly
+
+
+def kernel_params(options):
+    p = _np.zeros(4, dtype=_np.float64)
+    opts = _np.asarray(options, dtype=_np.float64).ravel()
+    if len(opts) > 4:
+        raise ValueError("at most four kernel options are supported")
+    p[: len(opts)] = opts
+    return p
+
+
+def _set_params(args, options):
+    p = kernel_params(options)
+    for i in range(4):
+        args.params[i] = float(p[i])
+
+
+def regular_rule(order):
+    key = int(order)
+    if key not in _REG_CACHE:
+        points, weights = triangle_rule(key)
+        _REG_CACHE[key] = (_np.ascontiguousarray(points.T), _np.ascontiguousarray(weights))
+    return _REG_CACHE[key]
+
+
+def _grids_identical(domain, dual_to_range):
+    return domain.grid == dual_to_range.grid
+
+
+def regular_into(
+    result, descriptor, domain, dual_to_range, parameters, precision=_lib.FP64, overwrite=False, stream=None
+):
+    """Add (or with ``overwrite`` store) the regular part into the device tensor ``result``."""
+    require_cuda()
+    kernel, assembly = kernel_ids(descriptor)
+    tgrid = device_grid(dual_to_range.grid)
+    sgrid = device_grid(domain.grid)
+    tspace = device_space(dual_to_range)
+    sspace = device_space(domain)
+    points, weights = regular_rule(parameters.quadrature.regular)
+    args = _lib.RegularArgs()
+    args.kernel = kernel
+    args.assembly = assembly
+    args.precision = precision
+    args.is_complex = 1 if result.is_complex() else 0
+    _set_params(args, descriptor.options)
+    args.test_grid = tgrid.record()
+    args.trial_grid = sgrid.record()
+    args.test = tspace.record()
+    args.trial = sspace.record()
+    args.grids_identical = 1 if _grids_identical(domain, dual_to_range) else 0
+    args.nq = len(weights)
+    args.quad_points = points.ctypes.data
+    args.quad_weights = weights.ctypes.data
+    args.result = ptr(result)
+    args.ld = result.stride(0)
+    args.overwrite = 1 if overwrite else 0
+    _lib.check(_lib.load().bemppcuda_assemble_regular(args, stream or current_stream()))
+    return result
+
+
+def dp0_fast_path(descriptor, domain, dual_to_range, parameters):
+    """True when the regular pass can overwrite every entry (no pre-zeroing needed)."""
+    if descriptor.assembly_type != "default_scalar":
+        return False
+    if int(parameters.quadrature.regular) != 4:
+        return False
+    return bool(device_space(domain).dof_is_position and device_space(dual_to_range).dof_is_position)
+
+
+def singular_into_dense(result, descriptor, domain, dual_to_range, parameters, diag_shift=0.0, stream=None):
+    """Scatter the Sauter-Schwab pairs into the dense device tensor ``result``."""
+    kernel, assembly = kernel_ids(descriptor)
+    grid = domain.grid
+    rule = device_singular_rule(grid, parameters.quadrature.singular, dual_to_range.support, domain.support)
+    args = _lib.SingularArgs()
+    args.kernel = kernel
+    args.assembly = assembly
+    args.is_complex = 1 if result.is_complex() else 0
+    _set_params(args, descriptor.options)
+    args.grid = device_grid(grid).record()
+    args.test = device_space(dual_to_range).record()
+    args.trial = device_space(domain).record()
+    rule.fill(args)
+    args.values = None
+    args.dense = ptr(result)
+    args.ld = result.stride(0)
+    args.diag_shift = float(diag_shift)
+    _lib.check(_lib.load().bemppcuda_assemble_singular(args, stream or current_stream()))
+    return result
+
+
+def result_dtype(descriptor):
+    return _torch.complex128 if descriptor.is_complex else _torch.float64
+
+
+def assemble_dense_device(domain, dual_to_range, parameters, descriptor, device_interface="cuda", out=None):
+    """Full dense weak form (regular + singular) as a device tensor (rows, cols)."""
+    require_cuda()
+    precision = precision_of(device_interface)
+    if getattr(domain, "requires_dof_transformation", False) or getattr(
+        dual_to_range, "requires_dof_transformation", False
+    ):
+        raise ValueError("Spaces that require dof transformations not supported for dense assembly.")
+    rows = int(dual_to_range.global_dof_count)
+    cols = int(domain.global_dof_count)
+    dtype = result_dtype(descriptor)
+    fast = dp0_fast_path(descriptor, domain, dual_to_range, parameters)
+    if out is None:
+        out = _torch.empty((rows, cols), dtype=dtype, device="cuda") if fast else _torch.zeros(
+            (rows, cols), dtype=dtype, device="cuda"
+        )
+    elif not fast:
+        out.zero_()
+    if precision == _lib.MIXED and not fast:
+        precision = _lib.FP64
+    regular_into(out, descriptor, domain, dual_to_range, parameters, precision=precision, overwrite=fast)
+    if _grids_identical(domain, dual_to_range):
+        singular_into_dense(out, descriptor, domain, dual_to_range, parameters)
+    return out
+
+
+def assemble_combined_field_device(domain, dual_to_range, parameters, options, eta, identity_coefficient=0.0,
+                                   device_interface="cuda", out=None):
+    """DP0 Helmholtz DLP + eta * SLP + identity_coefficient * I in one fused pass.
+
+    ``options`` are the Helmholtz kernel options [Re k, Im k].  The identity
+    term is the DP0 mass matrix (element areas on the diagonal).
+    """
+    from .operators import OperatorDescriptor
+
+    opts = list(kernel_params(options)[:2]) + [complex(eta).real, complex(eta).imag]
+    desc = OperatorDescriptor("helmholtz_combined_field_boundary", opts, "helmholtz_combined_field", "default_scalar",
+                              "double", True, None, 1)
+    require_cuda()
+    precision = precision_of(device_interface)
+    rows = int(dual_to_range.global_dof_count)
+    cols = int(domain.global_dof_count)
+    fast = dp0_fast_path(desc, domain, dual_to_range, parameters)
+    if out is None:
+        out = (_torch.empty if fast else _torch.zeros)((rows, cols), dtype=_torch.complex128, device="cuda")
+    elif not fast:
+        out.zero_()
+    regular_into(out, desc, domain, dual_to_range, parameters, precision=precision if fast else _lib.FP64,
+                 overwrite=fast)
+    if _grids_identical(domain, dual_to_range):
+        singular_into_dense(out, desc, domain, dual_to_range, parameters, diag_shift=identity_coefficient)
+    elif identity_coefficient != 0.0:
+        raise ValueError("an identity term needs identical domain and dual grids")
+    return out
+
+
+def potential_workspace_bytes(args):
+    return int(_lib.load().bemppcuda_potential_workspace_bytes(args))
+
+
+def evaluate_potential_device(space, descriptor, points, local_coefficients, parameters, stream=None):
+    """Potential (kdim, npoints) complex128 device tensor.
+
+    ``local_coefficients`` are the element-local coefficients (nshape * ne,)
+    complex128, i.e. ``space.map_to_full_grid @ x`` of the reference
+    (dense_potential_assembler.py:30-34); ``points`` is a (3, npoints) array.
+    """
+    require_cuda()
+    kernel, assembly = kernel_ids(descriptor)
+    kdim = 3 if assembly in (_lib.ASM_EFIE, _lib.ASM_MFIE) else 1
+    dgrid = device_grid(space.grid)
+    dspace = device_space(space)
+    pts = points if isinstance(points, _torch.Tensor) else _torch.as_tensor(_np.ascontiguousarray(_np.asarray(points, dtype=_np.float64).T))
+    pts = pts.to(device="cuda", dtype=_torch.float64).contiguous()
+    coeff = local_coefficients
+    if not isinstance(coeff, _torch.Tensor):
+        coeff = _torch.as_tensor(_np.ascontiguousarray(_np.asarray(coeff, dtype=_np.complex128)))
+    coeff = coeff.to(device="cuda", dtype=_torch.complex128).contiguous()
+    qp, qw = regular_rule(parameters.quadrature.regular)
+    npoints = pts.shape[0]
+    result = _torch.empty((kdim, npoints), dtype=_torch.complex128, device="cuda")
+    args = _lib.PotentialArgs()
+    args.kernel = kernel
+    args.assembly = assembly
+    args.precision = _lib.FP64
+    _set_params(args, descriptor.options)
+    args.grid = dgrid.record()
+    args.space = dspace.record()
+    args.nq = len(qw)
+    args.quad_points = qp.ctypes.data
+    args.quad_weights = qw.ctypes.data
+    args.npoints = npoints
+    args.points = ptr(pts)
+    args.coefficients = ptr(coeff)
+    args.result = ptr(result)
+    need = potential_workspace_bytes(args)
+    workspace = _torch.empty(max(need // 8, 1), dtype=_torch.float64, device="cuda")
+    args.workspace = ptr(workspace)
+    args.workspace_bytes = need
+    _lib.check(_lib.load().bemppcuda_evaluate_potential(args, stream or current_stream()))
+    return result

@@ -1,0 +1,191 @@
+"""Device-resident copies of grids, spaces and singular rules.
+
+Host objects (``bempp_cuda`` or ``bempp_cl`` grids and spaces, duck-typed)
+are uploaded once per CUDA device and cached on the object itself, so a
+second assembly on the same grid moves no geometry.  torch is used only for
+the allocation and host-to-device copies; every kernel is in libbemppcuda.so.
+
+HBM layout:
+* grid: vertices (nv, 3) f64, elements (ne, 3) i32, geometry record
+  (25, ne) f64 written by ``bemppcuda_grid_geometry``
+* space: support (nsupport,) i32, local2global (ne, nshape) i32, local
+  multipliers (ne, nshape) f64, normal multipliers (ne,) i32
+* singular rule: point tables (P, 2) f64, weights (W,) f64, six (npairs,)
+  i32 pair arrays (test / trial element, three offsets, point count)
+"""
+
+import ctypes as _ct
+
+import numpy as _np
+import torch as _torch
+
+from . import _lib
+from .quadrature import SingularPairs
+
+_CACHE_ATTR = "_bempp_cuda_device_cache"
+
+
+def require_cuda():
+    if not _torch.cuda.is_available():
+        raise RuntimeError("bempp_cuda needs a CUDA device (B200, sm_100a); none is visible")
+    _lib.load()
+
+
+def current_stream():
+    return _ct.c_void_p(_torch.cuda.current_stream().cuda_stream)
+
+
+def ptr(t):
+    return _ct.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _cache(obj):
+    cache = getattr(obj, "_bempp_cuda_device_cache_dict", None)
+    if cache is None:
+        cache = {}
+        try:
+            setattr(obj, "_bempp_cuda_device_cache_dict", cache)
+        except AttributeError:
+            pass
+    return cache
+
+
+def to_device(array, dtype):
+    return _torch.as_tensor(_np.ascontiguousarray(array)).to(device="cuda", dtype=dtype, non_blocking=False)
+
+
+class DeviceGrid(object):
+    """Vertices, elements and the per-element geometry record on the device."""
+
+    def __init__(self, grid):
+        vertices = _np.ascontiguousarray(_np.asarray(grid.vertices, dtype=_np.float64).T)
+        elements = _np.ascontiguousarray(_np.asarray(grid.elements).T.astype(_np.int32))
+        self.nvertices = vertices.shape[0]
+        self.nelements = elements.shape[0]
+        self.vertices = to_device(vertices, _torch.float64)
+        self.elements = to_device(elements, _torch.int32)
+        self.geom = _torch.empty((_lib.GEOM_FIELDS, max(self.nelements, 1)), dtype=_torch.float64, device="cuda")
+        _lib.check(
+            _lib.load().bemppcuda_grid_geometry(
+                ptr(self.vertices),
+                self.nvertices,
+                ptr(self.elements),
+                self.nelements,
+                ptr(self.geom),
+                current_stream(),
+            )
+        )
+        self.h2d_bytes = vertices.nbytes + elements.nbytes
+
+    def record(self):
+        return _lib.GridRec(self.nvertices, self.nelements, ptr(self.geom), ptr(self.elements))
+
+
+class DeviceSpace(object):
+    """Support list and dof maps of one space on the device."""
+
+    def __init__(self, space):
+        nshape = int(space.number_of_shape_functions)
+        self.nshape = nshape
+        self.shapeset = _lib.SHAPESET_IDS[space.shapeset.identifier]
+        support = _np.asarray(space.support_elements, dtype=_np.int64)
+        l2g = _np.asarray(space.local2global).reshape(-1, nshape)
+        mult = _np.asarray(space.local_multipliers, dtype=_np.float64).reshape(-1, nshape)
+        self.nsupport = len(support)
+        self.ndofs = int(space.global_dof_count)
+        pos = (
+            nshape == 1
+            and self.nsupport == self.ndofs
+            and _np.array_equal(l2g[support, 0], _np.arange(self.nsupport))
+            and _np.all(mult[support, 0] == 1.0)
+        )
+        self.dof_is_position = 1 if pos else 0
+        self.support = to_device(support.astype(_np.int32), _torch.int32)
+        self.l2g = to_device(l2g.astype(_np.int32), _torch.int32)
+        self.mult = to_device(mult, _torch.float64)
+        nm = _np.asarray(space.normal_multipliers, dtype=_np.int32)
+        self.normal_mult = to_device(nm, _torch.int32)
+        self.h2d_bytes = support.size * 4 + l2g.size * 4 + mult.nbytes + nm.nbytes
+
+    def record(self):
+        return _lib.Space(
+            self.shapeset,
+            self.nshape,
+            self.nsupport,
+            ptr(self.support),
+            ptr(self.l2g),
+            ptr(self.mult),
+            ptr(self.normal_mult),
+            self.ndofs,
+            self.dof_is_position,
+            0,
+        )
+
+
+class DeviceSingularRule(object):
+    """Flattened Sauter-Schwab pair list and point tables on the device."""
+
+    def __init__(self, arrays):
+        tp, sp, w, te, se, toff, soff, woff, npts = arrays
+        tp = _np.ascontiguousarray(_np.asarray(tp, dtype=_np.float64).T)  # (P, 2)
+        sp = _np.ascontiguousarray(_np.asarray(sp, dtype=_np.float64).T)
+        self.npoints_table = tp.shape[0]
+        self.nweights = len(w)
+        self.npairs = len(te)
+        self.test_points = to_device(tp, _torch.float64)
+        self.trial_points = to_device(sp, _torch.float64)
+        self.weights = to_device(_np.asarray(w, dtype=_np.float64), _torch.float64)
+        ints = [_np.asarray(a).astype(_np.int32) for a in (te, se, toff, soff, woff, npts)]
+        (self.test_elements, self.trial_elements, self.test_offsets, self.trial_offsets, self.weights_offsets,
+         self.npoints) = [to_device(a, _torch.int32) for a in ints]
+        self.h2d_bytes = tp.nbytes + sp.nbytes + 8 * len(w) + sum(a.nbytes for a in ints)
+
+    def fill(self, args):
+        args.npairs = self.npairs
+        args.npoints_table = self.npoints_table
+        args.test_points = ptr(self.test_points)
+        args.trial_points = ptr(self.trial_points)
+        args.weights = ptr(self.weights)
+        args.nweights = self.nweights
+        args.test_elements = ptr(self.test_elements)
+        args.trial_elements = ptr(self.trial_elements)
+        args.test_offsets = ptr(self.test_offsets)
+        args.trial_offsets = ptr(self.trial_offsets)
+        args.weights_offsets = ptr(self.weights_offsets)
+        args.npoints = ptr(self.npoints)
+
+
+def device_grid(grid):
+    dev = _torch.cuda.current_device()
+    cache = _cache(grid)
+    key = ("grid", dev)
+    if key not in cache:
+        cache[key] = DeviceGrid(grid)
+    return cache[key]
+
+
+def device_space(space):
+    dev = _torch.cuda.current_device()
+    cache = _cache(space)
+    key = ("space", dev)
+    if key not in cache:
+        cache[key] = DeviceSpace(space)
+    return cache[key]
+
+
+def device_singular_rule(grid, order, test_support, trial_support):
+    """Singular pairs of ``grid`` at ``order`` for the given supports (cached on the grid)."""
+    dev = _torch.cuda.current_device()
+    cache = _cache(grid)
+    key = ("singular", dev, int(order), _np.asarray(test_support).tobytes(), _np.asarray(trial_support).tobytes())
+    if key not in cache:
+        pairs = SingularPairs(grid, order, test_support, trial_support)
+        cache[key] = DeviceSingularRule(pairs.arrays())
+    return cache[key]
+
+
+def clear_cache(obj):
+    """Drop the device copies held for a grid or space."""
+    cache = getattr(obj, "_bempp_cuda_device_cache_dict", None)
+    if cache:
+        cache.clear()

@@ -1,0 +1,463 @@
+"""Operator factories mirroring ``bempp_cl.api.operators`` for the cuda interface.
+
+The factories build the same ``OperatorDescriptor`` the reference builds
+(bempp_cl/api/operators/__init__.py:11-14; identifiers, option arrays,
+kernel and assembly types as in boundary/{laplace,helmholtz,
+modified_helmholtz,maxwell}.py, potential/*.py and far_field/*.py), so a
+script written against the reference reads the same here:
+
+    space = function_space(grid, "DP", 0)
+    op = boundary.helmholtz.single_layer(space, space, space, 10.0)
+    mat = op.weak_form()          # DenseDeviceOperator, matrix in HBM
+    y = mat @ x                    # device matvec
+
+This module exists so the path can run where bempp_cl is not installed; when
+it is, ``bempp_cuda.plugin.install()`` makes the reference's own factories
+accept ``device_interface="cuda"`` instead.
+"""
+
+import collections as _collections
+import types as _types
+
+import numpy as _np
+import torch as _torch
+
+OperatorDescriptor = _collections.namedtuple(
+    "OperatorDescriptor",
+    "identifier options kernel_type assembly_type precision is_complex singular_part kernel_dimension",
+)
+
+
+class _Quadrature(object):
+    def __init__(self):
+        self.regular = 4
+        self.singular = 4
+
+
+class Parameters(object):
+    """Quadrature orders read by the assembly (api/utils/parameters.py:27-28)."""
+
+    def __init__(self):
+        self.quadrature = _Quadrature()
+
+
+def _params(parameters):
+    return parameters if parameters is not None else Parameters()
+
+
+class DenseDeviceOperator(object):
+    """Dense discrete operator whose matrix stays on the GPU.
+
+    Mirrors DenseDiscreteBoundaryOperator (discrete_boundary_operator.py:177-252):
+    ``shape``, ``dtype``, ``A`` (host copy), ``@`` / ``dot`` (device matvec /
+    matmat for device tensors, host in -> host out for ndarrays) and linear
+    combinations.
+    """
+
+    def __init__(self, tensor):
+        self.tensor = tensor
+
+    @property
+    def shape(self):
+        return tuple(self.tensor.shape)
+
+    @property
+    def dtype(self):
+        return _np.complex128 if self.tensor.is_complex() else _np.float64
+
+    @property
+    def A(self):
+        return self.tensor.cpu().numpy()
+
+    def to_dense(self):
+        return self.A
+
+    def dot(self, x):
+        if isinstance(x, _torch.Tensor):
+            xt = x.to(self.tensor.dtype) if not self.tensor.is_complex() or x.is_complex() else x.to(self.tensor.dtype)
+            return self.tensor @ xt
+        x = _np.asarray(x)
+        cdtype = _torch.complex128 if (self.tensor.is_complex() or _np.iscomplexobj(x)) else _torch.float64
+        mat = self.tensor if self.tensor.dtype == cdtype else self.tensor.to(cdtype)
+        return (mat @ _torch.as_tensor(x).to(device=self.tensor.device, dtype=cdtype)).cpu().numpy()
+
+    def __matmul__(self, x):
+        return self.dot(x)
+
+    def __call__(self, x):
+        return self.dot(x)
+
+    def _combine(self, other, a, b):
+        if isinstance(other, DenseDeviceOperator):
+            t1, t2 = self.tensor, other.tensor
+            if t1.is_complex() != t2.is_complex():
+                t1, t2 = t1.to(_torch.complex128), t2.to(_torch.complex128)
+            return DenseDeviceOperator(a * t1 + b * t2)
+        if isinstance(other, DiagonalOperator):
+            out = self.tensor * a if a != 1 else self.tensor.clone()
+            vals = other.values.to(out.device)
+            if not out.is_complex() and (vals.is_complex() or isinstance(b, complex)):
+                out = out.to(_torch.complex128)
+            out.diagonal().add_(b * vals.to(out.dtype))
+            return DenseDeviceOperator(out)
+        return NotImplemented
+
+    def __add__(self, other):
+        return self._combine(other, 1, 1)
+
+    def __radd__(self, other):
+        return self.__add__(other)
+
+    def __sub__(self, other):
+        return self._combine(other, 1, -1)
+
+    def __mul__(self, alpha):
+        if _np.isscalar(alpha):
+            t = self.tensor
+            if isinstance(alpha, complex) and not t.is_complex():
+                t = t.to(_torch.complex128)
+            return DenseDeviceOperator(t * alpha)
+        return self.dot(alpha)
+
+    def __rmul__(self, alpha):
+        return self.__mul__(alpha)
+
+    def __neg__(self):
+        return DenseDeviceOperator(-self.tensor)
+
+
+class DiagonalOperator(object):
+    """Diagonal discrete operator (the DP0 mass matrix) with device values."""
+
+    def __init__(self, values):
+        self.values = values
+
+    @property
+    def shape(self):
+        n = self.values.shape[0]
+        return (n, n)
+
+    def __mul__(self, alpha):
+        return DiagonalOperator(self.values * alpha)
+
+    __rmul__ = __mul__
+
+    def __neg__(self):
+        return DiagonalOperator(-self.values)
+
+
+class BoundaryOperator(object):
+    """Boundary operator with a lazily assembled, cached weak form (boundary_operator.py:36-41)."""
+
+    def __init__(self, domain, range_, dual_to_range, descriptor, device_interface="cuda", parameters=None):
+        self.domain = domain
+        self.range = range_
+        self.dual_to_range = dual_to_range
+        self.descriptor = descriptor
+        self.device_interface = device_interface or "cuda"
+        self.parameters = _params(parameters)
+        self._weak_form = None
+
+    def weak_form(self):
+        if self._weak_form is None:
+            self._weak_form = self._assemble()
+        return self._weak_form
+
+    def _assemble(self):
+        from .assembly import assemble_dense_device
+
+        return DenseDeviceOperator(
+            assemble_dense_device(self.domain, self.dual_to_range, self.parameters, self.descriptor, self.device_interface)
+        )
+
+    def __add__(self, other):
+        return _SumOperator(self, other, 1.0, 1.0)
+
+    def __sub__(self, other):
+        return _SumOperator(self, other, 1.0, -1.0)
+
+    def __mul__(self, alpha):
+        return _ScaledOperator(self, alpha)
+
+    __rmul__ = __mul__
+
+    def __neg__(self):
+        return _ScaledOperator(self, -1.0)
+
+
+def linear_terms(op, coef=1.0):
+    """Flatten sums and scalings into [(coefficient, leaf operator)]."""
+    if isinstance(op, _SumOperator):
+        return linear_terms(op._a, coef * op._ca) + linear_terms(op._b, coef * op._cb)
+    if isinstance(op, _ScaledOperator):
+        return linear_terms(op._op, coef * op._alpha)
+    return [(coef, op)]
+
+
+def _fused_combined_field(op):
+    """Assemble a DP0 Helmholtz a*DLP + b*SLP + c*I in one pass, or return None.
+
+    The reference assembles each term and adds the dense weak forms
+    (boundary_operator.py:134-169); here the shared kernel work (distance,
+    exp(ikr)) is done once per quadrature pair (csrc/regular.cu).
+    """
+    terms = linear_terms(op)
+    dlp = [(c, t) for c, t in terms if t.descriptor is not None and t.descriptor.kernel_type == "helmholtz_double_layer"]
+    slp = [(c, t) for c, t in terms if t.descriptor is not None and t.descriptor.kernel_type == "helmholtz_single_layer"
+           and t.descriptor.assembly_type == "default_scalar"]
+    ident = [(c, t) for c, t in terms if isinstance(t, IdentityOperator)]
+    if len(dlp) != 1 or len(slp) != 1 or len(ident) > 1 or len(dlp) + len(slp) + len(ident) != len(terms):
+        return None
+    (a, d), (b, s) = dlp[0], slp[0]
+    if list(d.descriptor.options) != list(s.descriptor.options) or a == 0:
+        return None
+    if not (d.domain == s.domain and d.dual_to_range == s.dual_to_range):
+        return None
+    if d.device_interface != s.device_interface:
+        return None
+    if d.domain.number_of_shape_functions != 1 or d.dual_to_range.number_of_shape_functions != 1:
+        return None
+    c = ident[0][0] if ident else 0.0
+    if ident and not (ident[0][1].domain == d.domain and ident[0][1].dual_to_range == d.dual_to_range):
+        return None
+    from .assembly import assemble_combined_field_device
+
+    eta = complex(b) / complex(a)
+    shift = complex(c) / complex(a)
+    if shift.imag != 0.0:
+        return None
+    mat = assemble_combined_field_device(d.domain, d.dual_to_range, d.parameters, d.descriptor.options, eta,
+                                         shift.real, d.device_interface)
+    if complex(a) != 1.0:
+        mat.mul_(complex(a))
+    return DenseDeviceOperator(mat)
+
+
+class _SumOperator(BoundaryOperator):
+    def __init__(self, a, b, ca, cb):
+        super().__init__(a.domain, a.range, a.dual_to_range, None, a.device_interface, a.parameters)
+        self._a, self._b, self._ca, self._cb = a, b, ca, cb
+
+    def _assemble(self):
+        fused = _fused_combined_field(self)
+        if fused is not None:
+            return fused
+        wa = self._a.weak_form()
+        wb = self._b.weak_form()
+        if isinstance(wa, DiagonalOperator):
+            wa, wb, ca, cb = wb, wa, self._cb, self._ca
+        else:
+            ca, cb = self._ca, self._cb
+        if isinstance(wb, DiagonalOperator):
+            return (wa * ca) + (wb * cb) if ca != 1 else wa + (wb * cb)
+        return wa._combine(wb, ca, cb)
+
+
+class _ScaledOperator(BoundaryOperator):
+    def __init__(self, op, alpha):
+        super().__init__(op.domain, op.range, op.dual_to_range, None, op.device_interface, op.parameters)
+        self._op, self._alpha = op, alpha
+
+    def _assemble(self):
+        return self._op.weak_form() * self._alpha
+
+
+class IdentityOperator(BoundaryOperator):
+    """L2 identity for DP0 spaces: diagonal of element areas (sparse.py:6-60)."""
+
+    def _assemble(self):
+        if self.domain.number_of_shape_functions != 1 or self.dual_to_range.number_of_shape_functions != 1:
+            raise ValueError("the device identity is implemented for DP0 spaces")
+        if not (self.domain == self.dual_to_range):
+            raise ValueError("the device identity needs identical DP0 domain and dual spaces")
+        areas = _np.asarray(self.domain.grid.volumes)[self.domain.support_elements]
+        return DiagonalOperator(_torch.as_tensor(areas, dtype=_torch.float64, device="cuda"))
+
+
+def _create(identifier, domain, range_, dual_to_range, options, kernel_type, assembly_type, is_complex,
+            parameters, device_interface, precision):
+    descriptor = OperatorDescriptor(
+        identifier, list(options), kernel_type, assembly_type, precision or "double", is_complex, None, 1
+    )
+    return BoundaryOperator(domain, range_, dual_to_range, descriptor, device_interface, parameters)
+
+
+def _helmholtz_options(k):
+    return [float(_np.real(k)), float(_np.imag(k))]
+
+
+def _boundary(kind, name, kernel_type, assembly_type, is_complex, options_fn):
+    def factory(domain, range_, dual_to_range, *args, parameters=None, assembler="dense", device_interface="cuda",
+                precision=None):
+        options = options_fn(*args)
+        return _create(kind + "_" + name + "_boundary", domain, range_, dual_to_range, options, kernel_type,
+                       assembly_type, is_complex, parameters, device_interface, precision)
+
+    factory.__name__ = name
+    return factory
+
+
+def _helmholtz_factory(name, kernel, assembly, modified_kernel, modified_assembly):
+    def factory(domain, range_, dual_to_range, wavenumber, parameters=None, assembler="dense",
+                device_interface="cuda", precision=None):
+        if _np.real(wavenumber) == 0:
+            # helmholtz.py:22: purely imaginary k -> modified Helmholtz with omega = Im k
+            return _create("modified_helmholtz_" + name + "_boundary", domain, range_, dual_to_range,
+                           [float(_np.imag(wavenumber))], modified_kernel, modified_assembly, False, parameters,
+                           device_interface, precision)
+        if name == "hypersingular" and domain.shapeset.identifier != "p1_discontinuous":
+            raise ValueError("Domain shapeset must be of type 'p1_discontinuous'.")
+        return _create("helmholtz_" + name + "_boundary", domain, range_, dual_to_range,
+                       _helmholtz_options(wavenumber), kernel, assembly, True, parameters, device_interface,
+                       precision)
+
+    factory.__name__ = name
+    return factory
+
+
+def _maxwell_factory(name, assembly):
+    def factory(domain, range_, dual_to_range, wavenumber, parameters=None, assembler="dense",
+                device_interface="cuda", precision=None):
+        if domain.identifier != "rwg0" or dual_to_range.identifier != "snc0":
+            raise ValueError("Operator only defined for domain = 'rwg' and 'dual_to_range = 'snc")
+        return _create("maxwell_" + name + "_boundary", domain, range_, dual_to_range, _helmholtz_options(wavenumber),
+                       "helmholtz_single_layer", assembly, True, parameters, device_interface, precision)
+
+    factory.__name__ = name
+    return factory
+
+
+def _laplace_hyp(domain, range_, dual_to_range, parameters=None, assembler="dense", device_interface="cuda",
+                 precision=None):
+    if domain.shapeset.identifier != "p1_discontinuous":
+        raise ValueError("Domain shapeset must be of type 'p1_discontinuous'.")
+    return _create("laplace_hypersingular_boundary", domain, range_, dual_to_range, [], "laplace_single_layer",
+                   "laplace_hypersingular", False, parameters, device_interface, precision)
+
+
+def _identity(domain, range_, dual_to_range, parameters=None, device_interface="cuda", precision=None):
+    descriptor = OperatorDescriptor("l2_identity", [], "l2_identity", "default_sparse", precision or "double",
+                                    False, None, 1)
+    return IdentityOperator(domain, range_, dual_to_range, descriptor, device_interface, parameters)
+
+
+boundary = _types.SimpleNamespace(
+    laplace=_types.SimpleNamespace(
+        single_layer=_boundary("laplace", "single_layer", "laplace_single_layer", "default_scalar", False, lambda: []),
+        double_layer=_boundary("laplace", "double_layer", "laplace_double_layer", "default_scalar", False, lambda: []),
+        adjoint_double_layer=_boundary("laplace", "adjoint_double_layer", "laplace_adjoint_double_layer",
+                                       "default_scalar", False, lambda: []),
+        hypersingular=_laplace_hyp,
+    ),
+    helmholtz=_types.SimpleNamespace(
+        single_layer=_helmholtz_factory("single_layer", "helmholtz_single_layer", "default_scalar",
+                                        "modified_helmholtz_single_layer", "default_scalar"),
+        double_layer=_helmholtz_factory("double_layer", "helmholtz_double_layer", "default_scalar",
+                                        "modified_helmholtz_double_layer", "default_scalar"),
+        adjoint_double_layer=_helmholtz_factory("adjoint_double_layer", "helmholtz_adjoint_double_layer",
+                                                "default_scalar", "modified_helmholtz_adjoint_double_layer",
+                                                "default_scalar"),
+        hypersingular=_helmholtz_factory("hypersingular", "helmholtz_single_layer", "helmholtz_hypersingular",
+                                         "modified_helmholtz_single_layer", "modified_helmholtz_hypersingular"),
+    ),
+    modified_helmholtz=_types.SimpleNamespace(
+        single_layer=_boundary("modified_helmholtz", "single_layer", "modified_helmholtz_single_layer",
+                               "default_scalar", False, lambda omega: [float(omega)]),
+        double_layer=_boundary("modified_helmholtz", "double_layer", "modified_helmholtz_double_layer",
+                               "default_scalar", False, lambda omega: [float(omega)]),
+        adjoint_double_layer=_boundary("modified_helmholtz", "adjoint_double_layer",
+                                       "modified_helmholtz_adjoint_double_layer", "default_scalar", False,
+                                       lambda omega: [float(omega)]),
+        hypersingular=_boundary("modified_helmholtz", "hypersingular", "modified_helmholtz_single_layer",
+                                "modified_helmholtz_hypersingular", False, lambda omega: [float(omega)]),
+    ),
+    maxwell=_types.SimpleNamespace(
+        electric_field=_maxwell_factory("electric_field", "maxwell_electric_field"),
+        magnetic_field=_maxwell_factory("magnetic_field", "maxwell_magnetic_field"),
+    ),
+    sparse=_types.SimpleNamespace(identity=_identity),
+)
+
+
+class PotentialOperator(object):
+    """Potential evaluation operator (potential_operator.py:14; dense_potential_assembler.py:8-40)."""
+
+    def __init__(self, space, points, descriptor, device_interface="cuda", parameters=None):
+        self.space = space
+        self.points = _np.asarray(points, dtype=_np.float64)
+        self.descriptor = descriptor
+        self.device_interface = device_interface or "cuda"
+        self.parameters = _params(parameters)
+
+    def evaluate_device(self, coefficients):
+        """(kernel_dimension, npoints) complex device tensor for dof ``coefficients``."""
+        from .assembly import evaluate_potential_device
+
+        local = self.space.map_to_full_grid @ _np.asarray(coefficients)
+        return evaluate_potential_device(self.space, self.descriptor, self.points, local, self.parameters)
+
+    def evaluate(self, grid_fun):
+        coeffs = getattr(grid_fun, "coefficients", grid_fun)
+        out = self.evaluate_device(_np.asarray(coeffs, dtype=_np.complex128)).cpu().numpy()
+        if not self.descriptor.is_complex and not _np.iscomplexobj(coeffs):
+            return out.real.copy()
+        return out
+
+
+def _potential(identifier, kernel_type, assembly_type, is_complex, kdim, options_fn, check=None):
+    def factory(space, points, *args, parameters=None, assembler="dense", device_interface="cuda", precision=None):
+        if check:
+            check(space)
+        descriptor = OperatorDescriptor(identifier, list(options_fn(*args)), kernel_type, assembly_type,
+                                        precision or "double", is_complex, None, kdim)
+        return PotentialOperator(space, points, descriptor, device_interface, parameters)
+
+    return factory
+
+
+def _require_rwg(space):
+    if space.identifier != "rwg0":
+        raise ValueError("Space must be an RWG type function space.")
+
+
+potential = _types.SimpleNamespace(
+    laplace=_types.SimpleNamespace(
+        single_layer=_potential("laplace_single_layer_potential", "laplace_single_layer", "default_scalar", False, 1,
+                                lambda: []),
+        double_layer=_potential("laplace_double_layer_potential", "laplace_double_layer", "default_scalar", False, 1,
+                                lambda: []),
+    ),
+    helmholtz=_types.SimpleNamespace(
+        single_layer=_potential("helmholtz_single_layer_potential", "helmholtz_single_layer", "default_scalar", True,
+                                1, _helmholtz_options),
+        double_layer=_potential("helmholtz_double_layer_potential", "helmholtz_double_layer", "default_scalar", True,
+                                1, _helmholtz_options),
+    ),
+    modified_helmholtz=_types.SimpleNamespace(
+        single_layer=_potential("modified_helmholtz_single_layer_potential", "modified_helmholtz_single_layer",
+                                "default_scalar", False, 1, lambda omega: [float(omega)]),
+        double_layer=_potential("modified_helmholtz_double_layer_potential", "modified_helmholtz_double_layer",
+                                "default_scalar", False, 1, lambda omega: [float(omega)]),
+    ),
+    maxwell=_types.SimpleNamespace(
+        electric_field=_potential("maxwell_electric_field_potential", "helmholtz_single_layer",
+                                  "maxwell_electric_field", True, 3, _helmholtz_options, _require_rwg),
+        magnetic_field=_potential("maxwell_magnetic_field_potential", "helmholtz_single_layer",
+                                  "maxwell_magnetic_field", True, 3, _helmholtz_options, _require_rwg),
+    ),
+)
+
+far_field = _types.SimpleNamespace(
+    helmholtz=_types.SimpleNamespace(
+        single_layer=_potential("helmholtz_far_field_single_layer_potential", "helmholtz_far_field_single_layer",
+                                "default_scalar", True, 1, _helmholtz_options),
+        double_layer=_potential("helmholtz_far_field_double_layer_potential", "helmholtz_far_field_double_layer",
+                                "default_scalar", True, 1, _helmholtz_options),
+    ),
+    maxwell=_types.SimpleNamespace(
+        electric_field=_potential("maxwell_far_field_electric_field_potential", "helmholtz_far_field_single_layer",
+                                  "maxwell_electric_far_field", True, 3, _helmholtz_options, _require_rwg),
+        magnetic_field=_potential("maxwell_far_field_magnetic_field_potential", "helmholtz_far_field_single_layer",
+                                  "maxwell_magnetic_far_field", True, 3, _helmholtz_options, _require_rwg),
+    ),
+)

@@ -1,0 +1,279 @@
+// Singular (Sauter-Schwab) quadrature for coincident, edge-adjacent and
+// vertex-adjacent element pairs.
+//
+// Replaces default_scalar_singular_kernel (numba_kernels.py:1471-1526),
+// laplace/helmholtz/modified hypersingular_singular (:1530-1784) and
+// maxwell_efield_singular / maxwell_mfield_singular (:1973-2147).
+//
+// One warp per pair: the lanes stride over the pair's 512-1536 quadrature
+// points (coalesced reads of the point and weight tables), accumulate the
+// nshape x nshape local block in registers and combine it with xor-shuffle
+// reductions.  Always FP64.  Output either to the flat per-pair value array
+// of the reference interface or scattered straight into a dense matrix.
+#include "common.cuh"
+
+namespace bc {
+
+struct SingParams {
+    const double *g;
+    int64_t ne;
+    const uint32_t *te, *se, *toff, *soff, *woff, *npts;
+    const double *tp, *sp, *w;
+    int64_t npairs;
+    const int32_t *tnm, *snm;
+    int nt, ns;
+    int is_complex;
+    int pad;
+    double p[4];
+    void *values;
+    void *dense;
+    int64_t ld;
+    const uint32_t *tl2g, *sl2g;
+    const double *tmult, *smult;
+    double diag_shift;
+};
+
+constexpr int SING_WARPS = 8;
+
+template <int ASM, int K>
+__global__ void __launch_bounds__(32 * SING_WARPS) singular_pairs(SingParams prm) {
+    const int lane = threadIdx.x & 31;
+    const int64_t k = (int64_t)blockIdx.x * SING_WARPS + (threadIdx.x >> 5);
+    if (k >= prm.npairs) return;
+    const int64_t t = prm.te[k], s = prm.se[k];
+    Geom gt, gs;
+    load_geom(prm.g, prm.ne, t, prm.tnm ? (double)prm.tnm[t] : 1.0, gt);
+    load_geom(prm.g, prm.ne, s, prm.snm ? (double)prm.snm[s] : 1.0, gs);
+    const int nt = prm.nt, ns = prm.ns;
+    constexpr bool HYP = (ASM == BEMPPCUDA_ASM_LAPLACE_HYP || ASM == BEMPPCUDA_ASM_HELM_HYP ||
+                          ASM == BEMPPCUDA_ASM_MODHELM_HYP);
+    constexpr bool MAXWELL = (ASM == BEMPPCUDA_ASM_EFIE || ASM == BEMPPCUDA_ASM_MFIE);
+    double cp[3][3];
+    if (HYP) {
+        double ct[3][3], cs[3][3];
+        surface_curls(prm.g, prm.ne, t, gt.n, ct);
+        surface_curls(prm.g, prm.ne, s, gs.n, cs);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) cp[i][j] = ct[i][0] * cs[j][0] + ct[i][1] * cs[j][1] + ct[i][2] * cs[j][2];
+    }
+    const double normal_prod = gt.n[0] * gs.n[0] + gt.n[1] * gs.n[1] + gt.n[2] * gs.n[2];
+    const double kr = prm.p[0], ki = prm.p[1];
+
+    double are[3][3], aim[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) are[i][j] = aim[i][j] = 0.0;
+
+    const int64_t toff = prm.toff[k], soff = prm.soff[k], woff = prm.woff[k];
+    const int n = (int)prm.npts[k];
+    for (int m = lane; m < n; m += 32) {
+        const double2 tpm = reinterpret_cast<const double2 *>(prm.tp)[toff + m];
+        const double2 spm = reinterpret_cast<const double2 *>(prm.sp)[soff + m];
+        const double w = __ldg(prm.w + woff + m);
+        double x[3], y[3];
+        to_global(gt, tpm.x, tpm.y, x);
+        to_global(gs, spm.x, spm.y, y);
+        const cplx kv = greens<K>(x, y, gt.n, gs.n, prm.p);
+        double pt[3], ps[3];
+        scalar_shape(nt, tpm.x, tpm.y, pt);
+        scalar_shape(ns, spm.x, spm.y, ps);
+        if (ASM == BEMPPCUDA_ASM_SCALAR) {
+            const cplx kw = cscale(kv, w);
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+                    if (i < nt && j < ns) {
+                        const double f = pt[i] * ps[j];
+                        are[i][j] = fma(kw.re, f, are[i][j]);
+                        aim[i][j] = fma(kw.im, f, aim[i][j]);
+                    }
+        } else if (ASM == BEMPPCUDA_ASM_LAPLACE_HYP) {
+            are[0][0] = fma(kv.re, w, are[0][0]);
+        } else if (HYP) {
+            double k2r = 0.0, k2i = 0.0;
+            if (ASM == BEMPPCUDA_ASM_HELM_HYP) {
+                k2r = -(kr * kr - ki * ki);
+                k2i = -(2.0 * kr * ki);
+            } else {
+                k2r = kr * kr;
+            }
+            const cplx kw = cscale(kv, w);
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const double mm = pt[i] * ps[j] * normal_prod;
+                    const cplx v = cmul(kw, cplx{cp[i][j] + k2r * mm, k2i * mm});
+                    are[i][j] += v.re;
+                    aim[i][j] += v.im;
+                }
+        } else {
+            double bt[3][3], bs[3][3];
+            rwg_values(gt, tpm.x, tpm.y, bt);
+            rwg_values(gs, spm.x, spm.y, bs);
+            const cplx kw = cscale(kv, w);
+            if (ASM == BEMPPCUDA_ASM_EFIE) {
+                const double kk = kr * kr + ki * ki;
+                const double div = 4.0 / (gt.ie * gs.ie);
+                const cplx inv_ik = {-ki / kk, -kr / kk};
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        const double dot = bt[i][0] * bs[j][0] + bt[i][1] * bs[j][1] + bt[i][2] * bs[j][2];
+                        const cplx fac = {ki * dot - div * inv_ik.re, -kr * dot - div * inv_ik.im};
+                        const cplx v = cmul(kw, fac);
+                        are[i][j] += v.re;
+                        aim[i][j] += v.im;
+                    }
+            } else {
+                const double df[3] = {x[0] - y[0], x[1] - y[1], x[2] - y[2]};
+                const double d2 = df[0] * df[0] + df[1] * df[1] + df[2] * df[2];
+                const double d = sqrt(d2);
+                const cplx f = cmul(kw, cplx{(-ki * d - 1.0) / d2, kr * d / d2});
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        const double c0 = bt[i][1] * bs[j][2] - bt[i][2] * bs[j][1];
+                        const double c1 = bt[i][2] * bs[j][0] - bt[i][0] * bs[j][2];
+                        const double c2 = bt[i][0] * bs[j][1] - bt[i][1] * bs[j][0];
+                        const double tr = df[0] * c0 + df[1] * c1 + df[2] * c2;
+                        are[i][j] += f.re * tr;
+                        aim[i][j] += f.im * tr;
+                    }
+            }
+        }
+    }
+
+    // reduce across the warp
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const bool live = (ASM == BEMPPCUDA_ASM_LAPLACE_HYP) ? (i == 0 && j == 0) : (i < nt && j < ns);
+            if (live) {
+                are[i][j] = warp_sum(are[i][j]);
+                aim[i][j] = warp_sum(aim[i][j]);
+            }
+        }
+    if (lane != 0) return;
+    const double scale = gt.ie * gs.ie;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        if (i >= nt) continue;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            if (j >= ns) continue;
+            double vr, vi;
+            if (ASM == BEMPPCUDA_ASM_LAPLACE_HYP) {
+                vr = are[0][0] * scale * cp[i][j];
+                vi = 0.0;
+            } else {
+                double f = scale;
+                if (MAXWELL) f *= edge_length(prm.g, prm.ne, t, i) * edge_length(prm.g, prm.ne, s, j);
+                vr = are[i][j] * f;
+                vi = aim[i][j] * f;
+            }
+            if (prm.values) {
+                const int64_t idx = (k * nt + i) * ns + j;
+                if (prm.is_complex) {
+                    double *o = reinterpret_cast<double *>(prm.values) + 2 * idx;
+                    o[0] += vr;
+                    o[1] += vi;
+                } else {
+                    reinterpret_cast<double *>(prm.values)[idx] += vr;
+                }
+            } else {
+                const double mt = prm.tmult[t * nt + i], ms = prm.smult[s * ns + j];
+                if (mt == 0.0 || ms == 0.0) continue;
+                const int64_t row = prm.tl2g[t * nt + i], col = prm.sl2g[s * ns + j];
+                if (t == s && nt == 1 && ns == 1) vr += prm.diag_shift * 0.5 * gt.ie;
+                const double m = mt * ms;
+                if (prm.is_complex) {
+                    double *o = reinterpret_cast<double *>(prm.dense) + 2 * (row * prm.ld + col);
+                    atomicAdd(o, vr * m);
+                    atomicAdd(o + 1, vi * m);
+                } else {
+                    atomicAdd(reinterpret_cast<double *>(prm.dense) + row * prm.ld + col, vr * m);
+                }
+            }
+        }
+    }
+}
+
+template <int ASM, int K>
+static cudaError_t launch_sing(const SingParams &prm, cudaStream_t st) {
+    const unsigned blocks = (unsigned)((prm.npairs + SING_WARPS - 1) / SING_WARPS);
+    singular_pairs<ASM, K><<<blocks, 32 * SING_WARPS, 0, st>>>(prm);
+    return cudaGetLastError();
+}
+
+}  // namespace bc
+
+using namespace bc;
+
+int bc_singular_launch(const bemppcuda_singular_args *a, cudaStream_t st) {
+    SingParams prm;
+    prm.g = a->grid.geom;
+    prm.ne = a->grid.nelements;
+    prm.te = a->test_elements;
+    prm.se = a->trial_elements;
+    prm.toff = a->test_offsets;
+    prm.soff = a->trial_offsets;
+    prm.woff = a->weights_offsets;
+    prm.npts = a->npoints;
+    prm.tp = a->test_points;
+    prm.sp = a->trial_points;
+    prm.w = a->weights;
+    prm.npairs = a->npairs;
+    prm.tnm = a->test.normal_mult;
+    prm.snm = a->trial.normal_mult;
+    prm.nt = a->test.nshape;
+    prm.ns = a->trial.nshape;
+    prm.is_complex = a->is_complex;
+    prm.pad = 0;
+    for (int i = 0; i < 4; ++i) prm.p[i] = a->params[i];
+    prm.values = a->values;
+    prm.dense = a->dense;
+    prm.ld = a->ld;
+    prm.tl2g = a->test.l2g;
+    prm.sl2g = a->trial.l2g;
+    prm.tmult = a->test.mult;
+    prm.smult = a->trial.mult;
+    prm.diag_shift = a->diag_shift;
+    if (prm.npairs == 0) return BEMPPCUDA_OK;
+    cudaError_t err = cudaSuccess;
+    switch (a->assembly) {
+    case BEMPPCUDA_ASM_SCALAR:
+        switch (a->kernel) {
+        case BEMPPCUDA_LAPLACE_SLP: err = launch_sing<0, BEMPPCUDA_LAPLACE_SLP>(prm, st); break;
+        case BEMPPCUDA_LAPLACE_DLP: err = launch_sing<0, BEMPPCUDA_LAPLACE_DLP>(prm, st); break;
+        case BEMPPCUDA_LAPLACE_ADLP: err = launch_sing<0, BEMPPCUDA_LAPLACE_ADLP>(prm, st); break;
+        case BEMPPCUDA_HELMHOLTZ_SLP: err = launch_sing<0, BEMPPCUDA_HELMHOLTZ_SLP>(prm, st); break;
+        case BEMPPCUDA_HELMHOLTZ_DLP: err = launch_sing<0, BEMPPCUDA_HELMHOLTZ_DLP>(prm, st); break;
+        case BEMPPCUDA_HELMHOLTZ_ADLP: err = launch_sing<0, BEMPPCUDA_HELMHOLTZ_ADLP>(prm, st); break;
+        case BEMPPCUDA_MODHELM_SLP: err = launch_sing<0, BEMPPCUDA_MODHELM_SLP>(prm, st); break;
+        case BEMPPCUDA_MODHELM_DLP: err = launch_sing<0, BEMPPCUDA_MODHELM_DLP>(prm, st); break;
+        case BEMPPCUDA_MODHELM_ADLP: err = launch_sing<0, BEMPPCUDA_MODHELM_ADLP>(prm, st); break;
+        case BEMPPCUDA_HELMHOLTZ_COMBINED: err = launch_sing<0, BEMPPCUDA_HELMHOLTZ_COMBINED>(prm, st); break;
+        default: bc_set_error("kernel %d not valid for singular assembly", a->kernel); return BEMPPCUDA_ERR_INVALID;
+        }
+        break;
+    case BEMPPCUDA_ASM_LAPLACE_HYP: err = launch_sing<1, BEMPPCUDA_LAPLACE_SLP>(prm, st); break;
+    case BEMPPCUDA_ASM_HELM_HYP: err = launch_sing<2, BEMPPCUDA_HELMHOLTZ_SLP>(prm, st); break;
+    case BEMPPCUDA_ASM_MODHELM_HYP: err = launch_sing<3, BEMPPCUDA_MODHELM_SLP>(prm, st); break;
+    case BEMPPCUDA_ASM_EFIE: err = launch_sing<4, BEMPPCUDA_HELMHOLTZ_SLP>(prm, st); break;
+    case BEMPPCUDA_ASM_MFIE: err = launch_sing<5, BEMPPCUDA_HELMHOLTZ_SLP>(prm, st); break;
+    default: bc_set_error("assembly type %d unknown", a->assembly); return BEMPPCUDA_ERR_INVALID;
+    }
+    if (err != cudaSuccess) {
+        bc_set_error("singular assembly launch failed: %s", cudaGetErrorString(err));
+        return BEMPPCUDA_ERR_CUDA;
+    }
+    return BEMPPCUDA_OK;
+}

@@ -1,0 +1,195 @@
+/*
+ * bemppcuda: B200 (sm_100a) dense Galerkin assembly and potential evaluation.
+ *
+ * Flat C ABI.  Every data pointer is a DEVICE pointer unless the field says
+ * HOST; the library never allocates, frees or retains caller memory.  Every
+ * entry point returns 0 on success or a negative status and never aborts;
+ * bemppcuda_last_error() gives the message of the last failure on the
+ * calling thread.  Work is enqueued on the given CUDA stream (NULL = legacy
+ * default stream) and is asynchronous with respect to the host.
+ *
+ * The entry points replace the device back ends that bempp-cl selects
+ * through bempp_cl/core/dispatcher.py:
+ *   bemppcuda_assemble_regular   <- numba_assemblers.dense_assembler
+ *                                   (bempp_cl/core/numba_assemblers.py:58-112)
+ *   bemppcuda_assemble_singular  <- numba_assemblers.singular_assembler
+ *                                   (bempp_cl/core/numba_assemblers.py:6-55)
+ *   bemppcuda_evaluate_potential <- numba_assemblers.potential_assembler
+ *                                   evaluator (bempp_cl/core/numba_assemblers.py:115-164)
+ *   bemppcuda_grid_geometry      <- Grid._compute_geometric_quantities
+ *                                   (bempp_cl/api/grid/grid.py:552-590)
+ */
+#ifndef BEMPPCUDA_H
+#define BEMPPCUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define BEMPPCUDA_OK 0
+#define BEMPPCUDA_ERR_INVALID (-1)     /* bad argument: size, pointer, id */
+#define BEMPPCUDA_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define BEMPPCUDA_ERR_UNSUPPORTED (-3) /* valid request this build does not implement */
+#define BEMPPCUDA_ERR_WORKSPACE (-4)   /* workspace smaller than required */
+
+/* Green's functions (kernel_type strings of bempp_cl/core/numba_kernels.py:39-64) */
+#define BEMPPCUDA_LAPLACE_SLP 0
+#define BEMPPCUDA_LAPLACE_DLP 1
+#define BEMPPCUDA_LAPLACE_ADLP 2
+#define BEMPPCUDA_HELMHOLTZ_SLP 3
+#define BEMPPCUDA_HELMHOLTZ_DLP 4
+#define BEMPPCUDA_HELMHOLTZ_ADLP 5
+#define BEMPPCUDA_MODHELM_SLP 6
+#define BEMPPCUDA_MODHELM_DLP 7
+#define BEMPPCUDA_MODHELM_ADLP 8
+#define BEMPPCUDA_FARFIELD_SLP 9
+#define BEMPPCUDA_FARFIELD_DLP 10
+/* Fused Helmholtz combined field: DLP + eta * SLP with params = (Re k, Im k,
+   Re eta, Im eta).  No reference counterpart as one kernel: the reference
+   assembles the two operators separately and adds the weak forms
+   (boundary_operator.py:134-169); this computes the same sum in one pass. */
+#define BEMPPCUDA_HELMHOLTZ_COMBINED 11
+
+/* assembly types (assembly_type strings of numba_kernels.py:11-34) */
+#define BEMPPCUDA_ASM_SCALAR 0      /* default_scalar */
+#define BEMPPCUDA_ASM_LAPLACE_HYP 1 /* laplace_hypersingular */
+#define BEMPPCUDA_ASM_HELM_HYP 2    /* helmholtz_hypersingular */
+#define BEMPPCUDA_ASM_MODHELM_HYP 3 /* modified_helmholtz_hypersingular */
+#define BEMPPCUDA_ASM_EFIE 4        /* maxwell_electric_field (+ _far_field for potentials) */
+#define BEMPPCUDA_ASM_MFIE 5        /* maxwell_magnetic_field (+ _far_field for potentials) */
+
+/* shape sets */
+#define BEMPPCUDA_SHAPE_P0 0  /* p0_discontinuous, 1 function */
+#define BEMPPCUDA_SHAPE_P1 1  /* p1_discontinuous, 3 functions */
+#define BEMPPCUDA_SHAPE_RWG 2 /* rwg0 / snc0 reference functions, Piola-mapped */
+
+/* precision of the regular (non-adjacent) element pairs */
+#define BEMPPCUDA_FP64 0
+#define BEMPPCUDA_MIXED 1 /* FP32 kernel evaluation, FP64 per-entry accumulation */
+
+/* geometry record: BEMPPCUDA_GEOM_FIELDS doubles per element, stored field-major
+   (field f of element e at geom[f * nelements + e]):
+   0-2 vertex 0, 3-5 v1 - v0, 6-8 v2 - v0, 9-11 unit normal, 12 integration
+   element, 13-15 edge lengths |v0-v1|, |v2-v0|, |v1-v2|, 16-21 J (J^T J)^-1
+   row-major (3 x 2), 22-24 centroid. */
+#define BEMPPCUDA_GEOM_FIELDS 25
+
+#define BEMPPCUDA_MAX_REGULAR_POINTS 16
+
+/* One function space restricted to its support elements. */
+typedef struct {
+    int32_t shapeset;           /* BEMPPCUDA_SHAPE_* */
+    int32_t nshape;             /* 1 or 3 */
+    int64_t nsupport;           /* number of support elements */
+    const uint32_t *support;    /* (nsupport,) element ids, increasing */
+    const uint32_t *l2g;        /* (nelements, nshape) global dof of each local function */
+    const double *mult;         /* (nelements, nshape) local multipliers */
+    const int32_t *normal_mult; /* (nelements,) +1/-1; NULL means all +1 */
+    int64_t ndofs;              /* global dof count (matrix extent) */
+    int32_t dof_is_position;    /* 1: nshape == 1, dof of support[i] is i, mult 1 */
+    int32_t pad;
+} bemppcuda_space;
+
+typedef struct {
+    int64_t nvertices;
+    int64_t nelements;
+    const double *geom;      /* BEMPPCUDA_GEOM_FIELDS * nelements, from bemppcuda_grid_geometry */
+    const int32_t *elements; /* (nelements, 3) vertex ids, element-major */
+} bemppcuda_grid;
+
+/* Regular-pair assembly: result[l2g_test, l2g_trial] (+)= sum over element pairs
+   that share no vertex when the grids are identical (numba_kernels.py:980-2278). */
+typedef struct {
+    int32_t kernel;     /* BEMPPCUDA_* Green's function */
+    int32_t assembly;   /* BEMPPCUDA_ASM_* */
+    int32_t precision;  /* BEMPPCUDA_FP64 or BEMPPCUDA_MIXED */
+    int32_t is_complex; /* result is complex128 (1) or float64 (0) */
+    double params[4];   /* kernel parameters: (Re k, Im k) or (omega) */
+    bemppcuda_grid test_grid;
+    bemppcuda_grid trial_grid;
+    bemppcuda_space test;  /* dual_to_range */
+    bemppcuda_space trial; /* domain */
+    int32_t grids_identical;
+    int32_t nq;                 /* regular rule size <= BEMPPCUDA_MAX_REGULAR_POINTS */
+    const double *quad_points;  /* HOST (nq, 2) reference points */
+    const double *quad_weights; /* HOST (nq,) */
+    void *result;               /* (rows, ld) row-major float64 or complex128 */
+    int64_t ld;                 /* row stride in entries */
+    int32_t overwrite;          /* DP0 fast path only: store instead of add, zero for adjacent pairs */
+    int32_t pad;
+} bemppcuda_regular_args;
+
+/* Singular pairs (Sauter-Schwab), the arrays of
+   _SingularQuadratureRuleInterfaceGalerkin.get_arrays (core/singular_assembler.py:251-278). */
+typedef struct {
+    int32_t kernel;
+    int32_t assembly;
+    int32_t is_complex;
+    int32_t pad0;
+    double params[4];
+    bemppcuda_grid grid;
+    bemppcuda_space test;
+    bemppcuda_space trial;
+    int64_t npairs;
+    int64_t npoints_table;        /* columns of the point tables */
+    const double *test_points;    /* (npoints_table, 2) point-major */
+    const double *trial_points;   /* (npoints_table, 2) */
+    const double *weights;        /* weight table */
+    int64_t nweights;
+    const uint32_t *test_elements;
+    const uint32_t *trial_elements;
+    const uint32_t *test_offsets;
+    const uint32_t *trial_offsets;
+    const uint32_t *weights_offsets;
+    const uint32_t *npoints;
+    /* output: exactly one of the two */
+    void *values;      /* flat (npairs, nshape_test, nshape_trial), accumulated into */
+    void *dense;       /* or: scatter value * multipliers into result[l2g_test, l2g_trial] */
+    int64_t ld;        /* row stride of dense */
+    double diag_shift; /* added to the coincident entries of a DP0 dense output, times the
+                          integration element / 2 (the -1/2 I term of a combined-field form) */
+} bemppcuda_singular_args;
+
+/* Potential / far-field evaluation (numba_kernels.py:1788-1849, 2281-2570). */
+typedef struct {
+    int32_t kernel;   /* Green's function; far-field kernels treat points as directions */
+    int32_t assembly; /* BEMPPCUDA_ASM_SCALAR, _EFIE or _MFIE */
+    int32_t precision;
+    int32_t pad0;
+    double params[4];
+    bemppcuda_grid grid;
+    bemppcuda_space space;      /* nshape and shapeset; l2g / mult unused */
+    int32_t nq;
+    int32_t pad1;
+    const double *quad_points;  /* HOST (nq, 2) */
+    const double *quad_weights; /* HOST (nq,) */
+    int64_t npoints;
+    const double *points;       /* (npoints, 3) point-major */
+    const double *coefficients; /* complex128 (nelements * nshape): element-local coefficients */
+    void *result;               /* complex128 (kdim, npoints) */
+    void *workspace;            /* bemppcuda_potential_workspace_bytes() bytes */
+    int64_t workspace_bytes;
+} bemppcuda_potential_args;
+
+int bemppcuda_version(void);
+int bemppcuda_last_error(char *buffer, int64_t length);
+
+/* Per-element geometry from vertices (3, nv) vertex-major xyz and elements
+   (nelements, 3).  Writes BEMPPCUDA_GEOM_FIELDS * nelements doubles. */
+int bemppcuda_grid_geometry(const double *vertices, int64_t nvertices, const int32_t *elements, int64_t nelements,
+                            double *geom, void *stream);
+
+int bemppcuda_assemble_regular(const bemppcuda_regular_args *args, void *stream);
+int bemppcuda_assemble_singular(const bemppcuda_singular_args *args, void *stream);
+
+int64_t bemppcuda_potential_workspace_bytes(const bemppcuda_potential_args *args);
+int bemppcuda_evaluate_potential(const bemppcuda_potential_args *args, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BEMPPCUDA_H */
