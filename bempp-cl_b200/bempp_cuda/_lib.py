@@ -162,6 +162,7 @@ SIGNATURES = {
     "bemppcuda_assemble_singular": (_ct.c_int, [_ct.POINTER(SingularArgs), _vp]),
     "bemppcuda_potential_workspace_bytes": (_i64, [_ct.POINTER(PotentialArgs)]),
     "bemppcuda_evaluate_potential": (_ct.c_int, [_ct.POINTER(PotentialArgs), _vp]),
+    "bemppcuda_fma_probe": (_ct.c_int, [_i32, _i64, _i64, _vp, _ct.POINTER(_ct.c_double), _vp]),
 }
 
 _lib = None

@@ -173,19 +173,32 @@ def device_space(space):
     return cache[key]
 
 
+def singular_rule_arrays(grid, order, test_support, trial_support):
+    """Host pair arrays of ``grid`` at ``order`` (cached on the grid, like its adjacency)."""
+    cache = _cache(grid)
+    key = ("singular_host", int(order), _np.asarray(test_support).tobytes(), _np.asarray(trial_support).tobytes())
+    if key not in cache:
+        cache[key] = SingularPairs(grid, order, test_support, trial_support).arrays()
+    return cache[key]
+
+
 def device_singular_rule(grid, order, test_support, trial_support):
-    """Singular pairs of ``grid`` at ``order`` for the given supports (cached on the grid)."""
+    """Singular pairs of ``grid`` at ``order`` for the given supports, on the device."""
     dev = _torch.cuda.current_device()
     cache = _cache(grid)
     key = ("singular", dev, int(order), _np.asarray(test_support).tobytes(), _np.asarray(trial_support).tobytes())
     if key not in cache:
-        pairs = SingularPairs(grid, order, test_support, trial_support)
-        cache[key] = DeviceSingularRule(pairs.arrays())
+        cache[key] = DeviceSingularRule(singular_rule_arrays(grid, order, test_support, trial_support))
     return cache[key]
 
 
-def clear_cache(obj):
-    """Drop the device copies held for a grid or space."""
+def clear_cache(obj, device_only=False):
+    """Drop the device copies (and with ``device_only=False`` the host tables) held for a grid or space."""
     cache = getattr(obj, "_bempp_cuda_device_cache_dict", None)
-    if cache:
+    if not cache:
+        return
+    if not device_only:
         cache.clear()
+        return
+    for key in [k for k in cache if k[0] != "singular_host"]:
+        del cache[key]

@@ -1,0 +1,492 @@
+#!/usr/bin/env python
+"""Benchmark: Helmholtz combined-field dense assembly on B200.
+
+Workload (default): regular_sphere(6) (32768 triangles), DP0 spaces, k = 10,
+the indirect combined-field operator  A = DLP - 1/2 I - i k SLP  as a dense
+32768 x 32768 complex128 matrix.  One step = one full assembly of A (regular
+pairs + Sauter-Schwab singular pairs + identity), matrix resident in HBM.
+
+* ``value``: entries/s of the mixed-precision assembly (FP32 regular pairs,
+  FP64 singular pairs, FP64 per-entry sums), inputs already on the device.
+* ``fp64``: the same for the FP64 path, plus the mixed/FP64 ratio and the
+  relative Frobenius error of the mixed matrix against the FP64 matrix.
+* ``e2e``: entries/s through the public operator API (``dlp - 0.5*ident -
+  1j*k*slp`` then ``weak_form()``), with every step re-uploading the grid
+  from pinned host memory and copying the whole matrix back into pinned host
+  memory.
+* ``roofline``: the regular-pair kernel (the dominant launch), algorithmic
+  flops / CUDA-event time against the FP32 (or FP64) FMA peak measured in the
+  same run by ``bemppcuda_fma_probe``.
+* ``cpu_baseline``: the oracle (a C/OpenMP restatement of the reference Numba
+  kernels) on a bounded row sample of the same operator, all host cores.
+
+Multi-GPU (torchrun): the rows (test elements) are split into one contiguous
+block per rank; each rank assembles its block with no collective (strong
+scaling, total work fixed).  ``--impl reference`` times the oracle port of the
+reference CPU path on rank 0 only.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "bempp-cl_b200"))
+sys.path.insert(0, ROOT)
+os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+
+import numpy as np  # noqa: E402
+
+# algorithmic flops per quadrature-point pair (add/sub/mul = 1, FMA = 2, sqrt,
+# div, sin, cos, exp = 1 each; software expansions not counted)
+FLOPS_PER_QPE = {
+    "helmholtz_combined_field": 35,  # shared r, exp(ikr) of DLP and SLP
+    "helmholtz_single_layer": 20,
+    "helmholtz_double_layer": 30,
+    "laplace_single_layer": 13,
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--level", type=int, default=6)
+    ap.add_argument("--k", type=float, default=10.0)
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time per baseline sample")
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def row_block(n, world, rank):
+    lo = (n * rank) // world
+    hi = (n * (rank + 1)) // world
+    return lo, hi
+
+
+def build_problem(level, world, rank):
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+
+    grid = regular_sphere(level)
+    domain = function_space(grid, "DP", 0)
+    lo, hi = row_block(grid.number_of_elements, world, rank)
+    dual = domain if (lo, hi) == (0, grid.number_of_elements) else function_space(
+        grid, "DP", 0, support_elements=np.arange(lo, hi)
+    )
+    return grid, domain, dual
+
+
+def combined_descriptor(k):
+    from bempp_cuda.operators import OperatorDescriptor
+
+    eta = -1j * k
+    return OperatorDescriptor("helmholtz_combined_field_boundary", [k, 0.0, eta.real, eta.imag],
+                              "helmholtz_combined_field", "default_scalar", "double", True, None, 1)
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler(object):
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.device_index = device_index
+        self.proc = None
+        self.path = os.path.join("/tmp", "bempp_cuda_clocks_%d.csv" % os.getpid())
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device_index), "--query-gpu=" + self.QUERY, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() in ("active", "1"):
+                    reasons.add(name)
+        os.unlink(self.path)
+        return {
+            "sm_mhz": float(np.median(sm)) if sm else None,
+            "sm_max_mhz": float(max(smax)) if smax else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+# ----------------------------------------------------------------------------- GPU arm
+def measure_fma_peaks(torch):
+    """FP32 and FP64 FMA throughput (TFLOP/s) from the library's probe kernel."""
+    import ctypes
+
+    from bempp_cuda import _lib
+    from bempp_cuda.device import current_stream
+
+    lib = _lib.load()
+    props = torch.cuda.get_device_properties(torch.cuda.current_device())
+    blocks = props.multi_processor_count * 8
+    out = {}
+    for name, prec, dtype, iters in (("fp32", _lib.MIXED, torch.float32, 20000), ("fp64", _lib.FP64, torch.float64, 10000)):
+        sink = torch.zeros(blocks, dtype=dtype, device="cuda")
+        flops = ctypes.c_double(0.0)
+        best = 0.0
+        for rep in range(4):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            _lib.check(lib.bemppcuda_fma_probe(prec, iters, blocks, ctypes.c_void_p(sink.data_ptr()),
+                                               ctypes.byref(flops), current_stream()))
+            e1.record()
+            torch.cuda.synchronize()
+            if rep:
+                best = max(best, flops.value / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+        out[name] = best
+    return out
+
+
+def gpu_arm(args, world, rank, local):
+    import torch
+
+    from bempp_cuda import _lib
+    from bempp_cuda.assembly import regular_into, singular_into_dense
+    from bempp_cuda.device import clear_cache, device_grid, device_singular_rule, device_space
+    from bempp_cuda.operators import Parameters
+
+    torch.cuda.set_device(local)
+    grid, domain, dual = build_problem(args.level, world, rank)
+    params = Parameters()
+    desc = combined_descriptor(args.k)
+    rows, cols = dual.global_dof_count, domain.global_dof_count
+    entries = rows * cols
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+    # device-resident inputs (uploaded once, outside the timed region)
+    device_grid(grid)
+    device_space(domain)
+    device_space(dual)
+    rule = device_singular_rule(grid, params.quadrature.singular, dual.support, domain.support)
+    npairs_singular = rule.npairs
+    out = torch.empty((rows, cols), dtype=torch.complex128, device="cuda")
+
+    def one_step(precision, events=None):
+        if events is not None:
+            events[0].record()
+        regular_into(out, desc, domain, dual, params, precision=precision, overwrite=True)
+        if events is not None:
+            events[1].record()
+        singular_into_dense(out, desc, domain, dual, params, diag_shift=-0.5)
+        if events is not None:
+            events[2].record()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def timed(precision, steps, warmup, sample_clocks):
+        for _ in range(warmup):
+            one_step(precision)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)]
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        sampler = ClockSampler(local) if sample_clocks else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.3)
+        start.record()
+        for s in range(steps):
+            one_step(precision, ev[s])
+        stop.record()
+        torch.cuda.synchronize()
+        clocks = sampler.stop() if sampler else None
+        barrier()
+        total_ms = start.elapsed_time(stop)
+        reg_ms = [ev[s][0].elapsed_time(ev[s][1]) for s in range(steps)]
+        sing_ms = [ev[s][1].elapsed_time(ev[s][2]) for s in range(steps)]
+        if dist is not None:
+            t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total_ms = float(t.item())
+        return total_ms, float(np.mean(reg_ms)), float(np.mean(sing_ms)), clocks
+
+    peaks = measure_fma_peaks(torch)
+
+    result = {}
+    # FP64 path first, keep its matrix for the operator error of the mixed path
+    fp64 = None
+    ref64 = None
+    total_entries = int(grid.number_of_elements) ** 2
+    if not args.skip_fp64:
+        t64, reg64, sing64, _ = timed(_lib.FP64, args.steps, args.warmup, False)
+        fp64 = {"value": total_entries * args.steps / (t64 * 1e-3), "unit": "entries/s",
+                "ms_per_step": t64 / args.steps, "regular_ms": reg64, "singular_ms": sing64}
+        ref64 = out.clone() if rows * cols * 16 * 3 < torch.cuda.get_device_properties(local).total_memory * 0.85 else None
+    tmx, regmx, singmx, clocks = timed(_lib.MIXED, args.steps, args.warmup, True)
+    value = total_entries * args.steps / (tmx * 1e-3)
+    if fp64 is not None:
+        fp64["mixed_over_fp64"] = value / fp64["value"]
+        if ref64 is not None:
+            err = torch.linalg.norm(out - ref64) / torch.linalg.norm(ref64)
+            fp64["mixed_rel_fro_err"] = float(err.item())
+            del ref64
+        torch.cuda.empty_cache()
+
+    # roofline of the regular-pair kernel (mixed precision)
+    regular_pairs = rows * cols - npairs_singular
+    qpe = 36 * regular_pairs
+    flops = qpe * FLOPS_PER_QPE["helmholtz_combined_field"]
+    achieved = flops / (regmx * 1e-3) / 1e12
+    roof = {"bound": "fp32", "achieved": achieved, "peak": peaks["fp32"], "unit": "TFLOP/s",
+            "frac": achieved / peaks["fp32"], "traffic": None,
+            "kernel": "regular_dp0<HELMHOLTZ_COMBINED, MIXED>", "kernel_ms": regmx,
+            "flops_per_qpe": FLOPS_PER_QPE["helmholtz_combined_field"], "qpe_per_launch": qpe,
+            "peak_source": "bemppcuda_fma_probe, measured in this run"}
+    if fp64 is not None:
+        a64 = flops / (fp64["regular_ms"] * 1e-3) / 1e12
+        fp64["roofline"] = {"bound": "fp64", "achieved": a64, "peak": peaks["fp64"], "unit": "TFLOP/s",
+                            "frac": a64 / peaks["fp64"], "kernel_ms": fp64["regular_ms"]}
+
+    # end to end through the public API (host in, host out)
+    e2e = None
+    if not args.skip_e2e:
+        e2e = e2e_measure(args, torch, grid, domain, dual, world, dist, clear_cache, total_entries)
+
+    line = {
+        "metric": "entries/s Helmholtz assembly, mixed vs FP64 GPU at rel err <=1e-6; shape-grads/s",
+        "value": value,
+        "unit": "entries/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": tmx / args.steps,
+        "higher_is_better": True,
+        "scaling": "strong",
+        "vs_baseline": None,
+        "dtype": "f32+f64",
+        "data": "synthetic: regular_sphere(%d) unit sphere, generated by octahedron subdivision" % args.level,
+        "config": {
+            "workload": "Helmholtz combined-field DLP - 1/2 I - i k SLP, DP0, regular_sphere(%d), %d x %d complex128, "
+                        "k=%g, regular order 4, singular order 4" % (args.level, grid.number_of_elements,
+                                                                      grid.number_of_elements, args.k),
+            "elements": int(grid.number_of_elements),
+            "precision": "mixed: FP32 regular pairs, FP64 singular pairs and per-entry sums",
+            "parallelism": "row blocks x%d" % world,
+            "l2": "output %.1f GB per step > 126 MB L2; compute-bound kernel" % (total_entries * 16 / 1e9),
+        },
+        "gpu_launches": 2 * args.steps,
+        "clocks": clocks,
+        "roofline": roof,
+        "fp64": fp64,
+        "fma_peaks_tflops": peaks,
+        "regular_ms": regmx,
+        "singular_ms": singmx,
+    }
+    if e2e is not None:
+        line["e2e"] = e2e
+    return line
+
+
+def e2e_measure(args, torch, grid, domain, dual, world, dist, clear_cache, total_entries):
+    """Public-API steps: pinned host grid in, pinned host matrix out."""
+    from bempp_cuda import operators
+    from bempp_cuda.grid import Grid
+    from bempp_cuda.space import function_space
+
+    rows, cols = dual.global_dof_count, domain.global_dof_count
+    host_out = torch.empty((rows, cols), dtype=torch.complex128, pin_memory=True)
+    # the user's host objects: grid and spaces are built once, as in a bempp script
+    g = Grid(np.asarray(grid.vertices), np.asarray(grid.elements))
+    d = function_space(g, "DP", 0)
+    lo = int(dual.support_elements[0])
+    t = d if rows == cols else function_space(g, "DP", 0, support_elements=np.arange(lo, lo + rows))
+
+    def step():
+        # device copies are dropped, so every step uploads vertices, elements, dof maps and singular tables
+        for obj in (g, d, t):
+            clear_cache(obj, device_only=True)
+        slp = operators.boundary.helmholtz.single_layer(d, d, t, args.k, device_interface="cuda_mixed")
+        dlp = operators.boundary.helmholtz.double_layer(d, d, t, args.k, device_interface="cuda_mixed")
+        ident = operators.boundary.sparse.identity(d, d, t, device_interface="cuda_mixed")
+        lhs = dlp - 0.5 * ident - 1j * args.k * slp
+        mat = lhs.weak_form()
+        host_out.copy_(mat.tensor, non_blocking=True)
+
+    for _ in range(max(1, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(args.steps):
+        step()
+    stop.record()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    ms = max(start.elapsed_time(stop), wall * 1e3)
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    from bempp_cuda.device import device_grid, device_singular_rule, device_space
+
+    h2d = (device_grid(g).h2d_bytes + device_space(d).h2d_bytes + (device_space(t).h2d_bytes if t is not d else 0)
+           + device_singular_rule(g, 4, t.support, d.support).h2d_bytes)
+    return {"value": total_entries * args.steps / (ms * 1e-3), "unit": "entries/s", "ms_per_step": ms / args.steps,
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(rows * cols * 16),
+            "note": "each step builds a new Grid from pinned host arrays (host geometry, adjacency and singular "
+                    "tables included), uploads it, assembles with the fused kernels and copies the matrix to "
+                    "pinned host memory"}
+
+
+# ----------------------------------------------------------------------------- CPU arm
+def cpu_sample(args, target_seconds):
+    """Oracle (C/OpenMP port of the reference kernels) on the first R rows of the operator.
+
+    Returns (entries/s, description).  R is calibrated so one sample takes
+    about ``target_seconds`` on this host.
+    """
+    from oracle import oracle as orc
+
+    from bempp_cuda.quadrature import SingularPairs, triangle_rule
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+
+    grid = regular_sphere(args.level)
+    n = grid.number_of_elements
+    domain = function_space(grid, "DP", 0)
+    qp, qw = triangle_rule(4)
+    eta = -1j * args.k
+    options = [args.k, 0.0, eta.real, eta.imag]
+
+    def run(r):
+        dual = function_space(grid, "DP", 0, support_elements=np.arange(r))
+        rule = SingularPairs(grid, 4, dual.support, domain.support).arrays()
+        t0 = time.perf_counter()
+        mat = orc.assemble_dense("helmholtz_combined_field", "default_scalar", options, True, domain, dual, qp, qw, rule)
+        mat[np.arange(r), np.arange(r)] += -0.5 * grid.volumes[:r]
+        return time.perf_counter() - t0
+
+    orc.lib()
+    t = run(8)
+    r = int(min(n, max(8, 8 * target_seconds / max(t, 1e-3))))
+    return r, run
+
+
+def reference_arm(args, world, rank):
+    if rank != 0:
+        return None
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    r, run = cpu_sample(args, args.cpu_seconds)
+    n = 8 * 4**args.level
+    for _ in range(min(args.warmup, 1)):
+        run(max(8, r // 8))
+    times = [run(r) for _ in range(args.steps)]
+    total = sum(times)
+    value = r * n * args.steps / total
+    sample = "%d rows x %d columns of the %d x %d operator per step (regular + singular + identity)" % (r, n, n, n)
+    return {
+        "metric": "entries/s Helmholtz assembly, mixed vs FP64 GPU at rel err <=1e-6; shape-grads/s",
+        "value": value,
+        "unit": "entries/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True,
+        "scaling": "strong",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic: regular_sphere(%d) unit sphere" % args.level,
+        "config": {"workload": "Helmholtz combined-field DLP - 1/2 I - i k SLP, DP0, regular_sphere(%d), k=%g"
+                               % (args.level, args.k), "elements": n},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "entries/s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "entries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        line = reference_arm(args, world, rank)
+        if line is not None:
+            print(json.dumps(line))
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
+    line = gpu_arm(args, world, rank, local)
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+        r, run = cpu_sample(args, args.cpu_seconds)
+        t = run(r)
+        n = 8 * 4**args.level
+        line["cpu_baseline"] = {"value": r * n / t, "unit": "entries/s", "cores": cores, "kind": "port",
+                                "sample": "%d rows x %d columns of the same operator, oracle (C/OpenMP restatement "
+                                          "of the reference Numba kernels)" % (r, n)}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -188,6 +188,14 @@ int bemppcuda_assemble_singular(const bemppcuda_singular_args *args, void *strea
 int64_t bemppcuda_potential_workspace_bytes(const bemppcuda_potential_args *args);
 int bemppcuda_evaluate_potential(const bemppcuda_potential_args *args, void *stream);
 
+/* Measurement utility, no reference counterpart: launches `blocks` x 256
+   threads that each run 32 independent FMAs per iteration in FP64
+   (precision = BEMPPCUDA_FP64) or FP32 (otherwise); *flops receives the
+   floating-point operation count (FMA = 2) so that flops / elapsed time is the
+   pipe throughput.  `sink` needs `blocks` elements of the chosen type. */
+int bemppcuda_fma_probe(int32_t precision, int64_t iterations, int64_t blocks, void *sink, double *flops,
+                        void *stream);
+
 #ifdef __cplusplus
 }
 #endif
