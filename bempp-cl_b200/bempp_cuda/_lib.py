@@ -163,7 +163,11 @@ SIGNATURES = {
     "bemppcuda_potential_workspace_bytes": (_i64, [_ct.POINTER(PotentialArgs)]),
     "bemppcuda_evaluate_potential": (_ct.c_int, [_ct.POINTER(PotentialArgs), _vp]),
     "bemppcuda_fma_probe": (_ct.c_int, [_i32, _i64, _i64, _vp, _ct.POINTER(_ct.c_double), _vp]),
+    "bemppcuda_evaluate_potential_noalloc": (_ct.c_int, [_ct.POINTER(PotentialArgs), _vp]),
 }
+
+# fixed workspace of bemppcuda_evaluate_potential_noalloc, in doubles
+NOALLOC_SCRATCH_DOUBLES = 3 * 1024 * 1024
 
 _lib = None
 

@@ -188,6 +188,24 @@ int bemppcuda_assemble_singular(const bemppcuda_singular_args *args, void *strea
 int64_t bemppcuda_potential_workspace_bytes(const bemppcuda_potential_args *args);
 int bemppcuda_evaluate_potential(const bemppcuda_potential_args *args, void *stream);
 
+/* Potential evaluation for callers that cannot allocate device memory.  No
+   counterpart in the reference (its evaluator allocates host arrays freely).
+   Same arguments and results as bemppcuda_evaluate_potential, but
+   args->workspace / workspace_bytes are ignored: the source table goes into a
+   fixed array of BEMPPCUDA_NOALLOC_SCRATCH_DOUBLES doubles (24 MiB) that the
+   library keeps on every GPU that loads it, so the call allocates nothing.
+   It is meant for code that only receives input and output device buffers
+   from a host application owning all device memory (a plugin inside a
+   solver's memory pool, an embedding runtime without a CUDA allocation
+   binding), where cudaMalloc may fail or would synchronize the device.
+   Problems whose table exceeds the array (space.nsupport * nq * 14 doubles)
+   are rejected with BEMPPCUDA_ERR_WORKSPACE.  All calls on a device share
+   the array: calls that can overlap on the GPU race, so order them on one
+   stream.  The first call on a device looks up the array's address; make it
+   before any stream capture starts on that device. */
+#define BEMPPCUDA_NOALLOC_SCRATCH_DOUBLES (3 * 1024 * 1024)
+int bemppcuda_evaluate_potential_noalloc(const bemppcuda_potential_args *args, void *stream);
+
 /* Measurement utility, no reference counterpart: launches `blocks` x 256
    threads that each run 32 independent FMAs per iteration in FP64
    (precision = BEMPPCUDA_FP64) or FP32 (otherwise); *flops receives the
