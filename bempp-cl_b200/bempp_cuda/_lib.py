@@ -99,6 +99,7 @@ class RegularArgs(_ct.Structure):
         ("ld", _i64),
         ("overwrite", _i32),
         ("pad", _i32),
+        ("phase_radius", _ct.c_double),
     ]
 
 

@@ -102,6 +102,8 @@ def regular_into(
     args.result = ptr(result)
     args.ld = result.stride(0)
     args.overwrite = 1 if overwrite else 0
+    # a little slack over the exact bound keeps rounding of the radii on the safe side
+    args.phase_radius = 1.0001 * (tgrid.radius + sgrid.radius)
     _lib.check(_lib.load().bemppcuda_assemble_regular(args, stream or current_stream()))
     return result
 

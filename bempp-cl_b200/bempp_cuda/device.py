@@ -76,6 +76,10 @@ class DeviceGrid(object):
             )
         )
         self.h2d_bytes = vertices.nbytes + elements.nbytes
+        # largest centroid-to-vertex distance: bounds every quadrature point's offset from its centroid
+        corners = vertices[elements]  # (ne, 3, 3)
+        centroids = corners.mean(axis=1, keepdims=True)
+        self.radius = float(_np.sqrt(((corners - centroids) ** 2).sum(axis=2)).max()) if self.nelements else 0.0
 
     def record(self):
         return _lib.GridRec(self.nvertices, self.nelements, ptr(self.geom), ptr(self.elements))

@@ -25,6 +25,7 @@ struct QuadRule {
     double x[BEMPPCUDA_MAX_REGULAR_POINTS];
     double y[BEMPPCUDA_MAX_REGULAR_POINTS];
     double w[BEMPPCUDA_MAX_REGULAR_POINTS];
+    float wf[BEMPPCUDA_MAX_REGULAR_POINTS];  // w rounded to FP32 for the mixed path
 };
 
 // Geometry of one element read from the field-major record.

@@ -258,6 +258,7 @@ int bc_potential_launch(const bemppcuda_potential_args *a, double *workspace, cu
         rule.x[i] = i < a->nq ? a->quad_points[2 * i] : 0.0;
         rule.y[i] = i < a->nq ? a->quad_points[2 * i + 1] : 0.0;
         rule.w[i] = i < a->nq ? a->quad_weights[i] : 0.0;
+        rule.wf[i] = (float)rule.w[i];
     }
     if (prm.npoints == 0) return BEMPPCUDA_OK;
     const bool maxwell = a->assembly != BEMPPCUDA_ASM_SCALAR;

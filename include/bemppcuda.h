@@ -120,6 +120,9 @@ typedef struct {
     int64_t ld;                 /* row stride in entries */
     int32_t overwrite;          /* DP0 fast path only: store instead of add, zero for adjacent pairs */
     int32_t pad;
+    double phase_radius;        /* R_test + R_trial, R = largest centroid-to-vertex distance of a grid;
+                                   lets the mixed path skip the phase range reduction when
+                                   |k| * phase_radius <= 1; 0 = unknown (always reduce) */
 } bemppcuda_regular_args;
 
 /* Singular pairs (Sauter-Schwab), the arrays of
