@@ -1,0 +1,251 @@
+"""Dense solves on the device: GMRES, multi-right-hand-side GMRES and FP64 refinement.
+
+``gmres`` mirrors ``bempp_cl.api.linalg.gmres`` (api/linalg/iterative_solvers.py:47-93):
+it takes a boundary operator and a grid function, solves the weak form
+against the projections onto the dual space and returns a grid function in
+the domain (plus the info code, and optionally residuals / iteration count).
+The reference hands the weak form to scipy's GMRES with ``ndarray.dot``
+matvecs on the host; here the matrix stays in HBM and every matvec is a
+device GEMV (matmat for several right-hand sides, cuBLAS through torch).
+
+``gmres_tensor`` is restarted GMRES on torch tensors: Arnoldi with classical
+Gram-Schmidt and one re-orthogonalisation (two GEMVs against the basis per
+step instead of j dot products), Givens rotations on the small Hessenberg
+system on the host.  Convergence test: ||b - A x|| <= tol ||b|| (the
+relative-residual test of scipy's gmres).
+
+``solve_refined`` is mixed-precision iterative refinement: an inner GMRES on
+a complex64 copy of the matrix, corrections accumulated in complex128, and
+the residual b - A x recomputed in complex128 with the complex128 matrix
+after every inner solve, until ||b - A x|| <= tol ||b||.
+"""
+
+import time as _time
+
+import numpy as _np
+import torch as _torch
+
+
+def _norm(v):
+    return float(_torch.linalg.vector_norm(v).item())
+
+
+def gmres_tensor(matvec, b, x0=None, tol=1e-5, restart=None, maxiter=None, callback=None):
+    """Solve A x = b for one right-hand side; return (x, info, residuals, iterations).
+
+    ``matvec(v)`` returns A v for a device vector of b's dtype.  ``info`` is 0
+    on convergence, else the number of iterations done (scipy convention).
+    """
+    n = b.shape[0]
+    restart = min(restart or 100, n)
+    maxiter = maxiter or 10 * n
+    dtype = b.dtype
+    x = _torch.zeros_like(b) if x0 is None else x0.clone()
+    bnorm = _norm(b)
+    residuals = []
+    if bnorm == 0.0:
+        return x, 0, [0.0], 0
+    r = b - matvec(x) if x0 is not None else b.clone()
+    beta = _norm(r)
+    residuals.append(beta / bnorm)
+    iterations = 0
+    while True:
+        if beta <= tol * bnorm:
+            return x, 0, residuals, iterations
+        V = _torch.empty((restart + 1, n), dtype=dtype, device=b.device)
+        V[0] = r / beta
+        H = _np.zeros((restart + 1, restart), dtype=_np.complex128)
+        cs = _np.zeros(restart, dtype=_np.complex128)
+        sn = _np.zeros(restart, dtype=_np.complex128)
+        g = _np.zeros(restart + 1, dtype=_np.complex128)
+        g[0] = beta
+        j_done = 0
+        converged = False
+        for j in range(restart):
+            w = matvec(V[j])
+            basis = V[: j + 1]
+            h = _torch.mv(basis.conj(), w)
+            w = w - _torch.mv(basis.transpose(0, 1), h)
+            h2 = _torch.mv(basis.conj(), w)
+            w = w - _torch.mv(basis.transpose(0, 1), h2)
+            h = (h + h2).to(_torch.complex128).cpu().numpy()
+            hn = _norm(w)
+            if hn > 0.0:
+                V[j + 1] = w / hn
+            col = _np.zeros(restart + 1, dtype=_np.complex128)
+            col[: j + 1] = h
+            col[j + 1] = hn
+            for i in range(j):
+                t = cs[i] * col[i] + sn[i] * col[i + 1]
+                col[i + 1] = -_np.conj(sn[i]) * col[i] + _np.conj(cs[i]) * col[i + 1]
+                col[i] = t
+            # rotation G = [[c, s], [-conj(s), conj(c)]] with G (a, b)^T = (rho, 0)^T
+            a, bb = col[j], col[j + 1]
+            denom = _np.sqrt(abs(a) ** 2 + abs(bb) ** 2)
+            if denom == 0.0:
+                cs[j], sn[j] = 1.0, 0.0
+            else:
+                cs[j] = _np.conj(a) / denom
+                sn[j] = _np.conj(bb) / denom
+            col[j] = denom
+            col[j + 1] = 0.0
+            H[:, j] = col
+            g[j + 1] = -_np.conj(sn[j]) * g[j]
+            g[j] = cs[j] * g[j]
+            iterations += 1
+            j_done = j + 1
+            res = abs(g[j + 1])
+            residuals.append(res / bnorm)
+            if callback is not None:
+                callback(res / bnorm)
+            if res <= tol * bnorm or hn == 0.0 or iterations >= maxiter:
+                converged = res <= tol * bnorm or hn == 0.0
+                break
+        # solve the triangular system and update x
+        y = _np.zeros(j_done, dtype=_np.complex128)
+        for i in range(j_done - 1, -1, -1):
+            y[i] = (g[i] - H[i, i + 1 : j_done] @ y[i + 1 :]) / H[i, i]
+        yt = _torch.as_tensor(y, device=b.device).to(dtype if dtype.is_complex else _torch.complex128)
+        if not dtype.is_complex:
+            yt = yt.real.to(dtype)
+        x = x + _torch.mv(V[:j_done].transpose(0, 1), yt)
+        if converged:
+            return x, 0, residuals, iterations
+        if iterations >= maxiter:
+            return x, iterations, residuals, iterations
+        r = b - matvec(x)
+        beta = _norm(r)
+
+
+def gmres_block(matmat, B, tol=1e-5, restart=None, maxiter=None):
+    """Several right-hand sides with shared matmats: columns of B (n, m).
+
+    One GMRES per column, but every Arnoldi step multiplies the matrix with
+    the basis vectors of all unconverged columns at once (one pass over the
+    matrix for m vectors: a GEMM instead of m GEMVs).  Givens rotations per
+    column on the host.  Returns (X, infos, iterations per column).
+    """
+    n, m = B.shape
+    restart = min(restart or 100, n)
+    maxiter = maxiter or 10 * n
+    X = _torch.zeros_like(B)
+    bnorms = _torch.linalg.vector_norm(B, dim=0).cpu().numpy()
+    iters = _np.zeros(m, dtype=int)
+    R = B.clone()
+    while True:
+        rn = _torch.linalg.vector_norm(R, dim=0).cpu().numpy()
+        active = [c for c in range(m) if rn[c] > tol * bnorms[c] and iters[c] < maxiter]
+        if not active:
+            break
+        na = len(active)
+        idx = _torch.tensor(active, device=B.device)
+        beta = rn[active]
+        V = _torch.empty((restart + 1, n, na), dtype=B.dtype, device=B.device)
+        V[0] = R[:, idx] / _torch.as_tensor(beta, device=B.device).to(B.dtype)
+        H = _np.zeros((na, restart + 1, restart), dtype=_np.complex128)
+        cs = _np.zeros((na, restart), dtype=_np.complex128)
+        sn = _np.zeros((na, restart), dtype=_np.complex128)
+        g = _np.zeros((na, restart + 1), dtype=_np.complex128)
+        g[:, 0] = beta
+        steps = 0
+        for j in range(restart):
+            W = matmat(V[j])
+            basis = V[: j + 1]
+            h = _torch.einsum("kna,na->ka", basis.conj(), W)
+            W = W - _torch.einsum("kna,ka->na", basis, h)
+            h2 = _torch.einsum("kna,na->ka", basis.conj(), W)
+            W = W - _torch.einsum("kna,ka->na", basis, h2)
+            hn = _torch.linalg.vector_norm(W, dim=0)
+            V[j + 1] = W / _torch.where(hn > 0, hn, _torch.ones_like(hn)).to(B.dtype)
+            hcol = (h + h2).to(_torch.complex128).cpu().numpy()  # (j+1, na)
+            hnn = hn.to(_torch.float64).cpu().numpy()
+            steps = j + 1
+            for a in range(na):
+                col = _np.zeros(restart + 1, dtype=_np.complex128)
+                col[: j + 1] = hcol[:, a]
+                col[j + 1] = hnn[a]
+                for i in range(j):
+                    t = cs[a, i] * col[i] + sn[a, i] * col[i + 1]
+                    col[i + 1] = -_np.conj(sn[a, i]) * col[i] + _np.conj(cs[a, i]) * col[i + 1]
+                    col[i] = t
+                x0, x1 = col[j], col[j + 1]
+                den = _np.sqrt(abs(x0) ** 2 + abs(x1) ** 2)
+                cs[a, j], sn[a, j] = (1.0, 0.0) if den == 0.0 else (_np.conj(x0) / den, _np.conj(x1) / den)
+                col[j], col[j + 1] = den, 0.0
+                H[a, :, j] = col
+                g[a, j + 1] = -_np.conj(sn[a, j]) * g[a, j]
+                g[a, j] = cs[a, j] * g[a, j]
+            if all(abs(g[a, j + 1]) <= tol * bnorms[c] for a, c in enumerate(active)) or bool((hnn == 0).all()):
+                break
+        Y = _np.zeros((steps, na), dtype=_np.complex128)
+        for a in range(na):
+            for i in range(steps - 1, -1, -1):
+                Y[i, a] = (g[a, i] - H[a, i, i + 1 : steps] @ Y[i + 1 :, a]) / H[a, i, i]
+        Yt = _torch.as_tensor(Y, device=B.device).to(B.dtype)
+        X[:, idx] += _torch.einsum("kna,ka->na", V[:steps], Yt)
+        iters[active] += steps
+        R = B - matmat(X)
+    rn = _torch.linalg.vector_norm(R, dim=0).cpu().numpy()
+    infos = [0 if rn[c] <= tol * bnorms[c] else int(iters[c]) for c in range(m)]
+    return X, infos, [int(v) for v in iters]
+
+
+def solve_refined(matrix, b, tol=1e-8, inner_tol=1e-4, restart=100, maxiter=2000, max_refinements=20,
+                  inner_dtype=_torch.complex64):
+    """Mixed-precision iterative refinement; returns (x, info dict).
+
+    ``matrix`` is the (complex128) device matrix; the inner solves use a
+    copy in ``inner_dtype``; residuals are formed in complex128.
+    """
+    t0 = _time.perf_counter()
+    low = matrix.to(inner_dtype)
+    b = b.to(matrix.dtype)
+    bnorm = _norm(b)
+    x = _torch.zeros_like(b)
+    r = b.clone()
+    history = []
+    inner_iterations = []
+    for _ in range(max_refinements):
+        res = _norm(r) / bnorm
+        history.append(res)
+        if res <= tol:
+            break
+        rl = r.to(inner_dtype)
+        d, info, _, its = gmres_tensor(lambda v: _torch.mv(low, v), rl, tol=inner_tol, restart=restart,
+                                       maxiter=maxiter)
+        inner_iterations.append(its)
+        x = x + d.to(matrix.dtype)
+        r = b - _torch.mv(matrix, x)
+    _torch.cuda.synchronize() if matrix.is_cuda else None
+    info = {
+        "refinements": len(inner_iterations),
+        "inner_iterations": inner_iterations,
+        "relative_residuals": history,
+        "converged": history[-1] <= tol,
+        "seconds": _time.perf_counter() - t0,
+    }
+    del low
+    return x, info
+
+
+def gmres(A, b, tol=1e-5, restart=None, maxiter=None, use_strong_form=False, return_residuals=False,
+          return_iteration_count=False):
+    """GMRES on the device for a bempp_cuda boundary operator and grid function."""
+    from .grid_function import GridFunction
+
+    if use_strong_form:
+        raise ValueError("the strong form is not implemented for the cuda interface")
+    mat = A.weak_form()
+    rhs = b.projections(A.dual_to_range)
+    dtype = mat.tensor.dtype if mat.tensor.is_complex() or not _np.iscomplexobj(rhs) else _torch.complex128
+    M = mat.tensor.to(dtype)
+    bt = _torch.as_tensor(_np.asarray(rhs)).to(device=M.device, dtype=dtype)
+    x, info, residuals, its = gmres_tensor(lambda v: _torch.mv(M, v), bt, tol=tol, restart=restart,
+                                           maxiter=maxiter)
+    sol = GridFunction(A.domain, coefficients=x.cpu().numpy())
+    out = [sol, info]
+    if return_residuals:
+        out.append(residuals)
+    if return_iteration_count:
+        out.append(its)
+    return tuple(out)

@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-solve", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time per baseline sample")
     return ap.parse_args()
 
@@ -274,11 +275,14 @@ def gpu_arm(args, world, rank, local):
         ref64 = out.clone() if rows * cols * 16 * 3 < torch.cuda.get_device_properties(local).total_memory * 0.85 else None
     tmx, regmx, singmx, clocks = timed(_lib.MIXED, args.steps, args.warmup, True)
     value = total_entries * args.steps / (tmx * 1e-3)
+    solve = None
     if fp64 is not None:
         fp64["mixed_over_fp64"] = value / fp64["value"]
         if ref64 is not None:
             err = torch.linalg.norm(out - ref64) / torch.linalg.norm(ref64)
             fp64["mixed_rel_fro_err"] = float(err.item())
+            if world == 1 and not args.skip_solve:
+                solve = solve_measure(args, torch, grid, domain, ref64, out)
             del ref64
         torch.cuda.empty_cache()
 
@@ -334,7 +338,36 @@ def gpu_arm(args, world, rank, local):
     }
     if e2e is not None:
         line["e2e"] = e2e
+    if solve is not None:
+        line["solve"] = solve
     return line
+
+
+def solve_measure(args, torch, grid, domain, a64, amx):
+    """C3 solve: plane wave exp(i k z), FP64 GMRES vs mixed assembly + FP64-residual refinement."""
+    from bempp_cuda.grid_function import GridFunction
+    from bempp_cuda.linalg import gmres_tensor, solve_refined
+
+    k = args.k
+
+    def minus_incident(x, n, domain_index, result):
+        result[0] = -np.exp(1j * k * x[2])
+
+    b = torch.as_tensor(GridFunction(domain, fun=minus_incident).projections(domain), device="cuda")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    x64, info, res, its = gmres_tensor(lambda v: torch.mv(a64, v), b, tol=1e-8, restart=200, maxiter=2000)
+    torch.cuda.synchronize()
+    t64 = time.perf_counter() - t0
+    xmx, rinfo = solve_refined(amx, b, tol=1e-8, inner_tol=1e-4, restart=200)
+    diff = float((torch.linalg.norm(xmx - x64) / torch.linalg.norm(x64)).item())
+    res_true = float((torch.linalg.norm(b - torch.mv(a64, xmx)) / torch.linalg.norm(b)).item())
+    return {"rhs": "projection of -exp(i k z) onto DP0", "tol": 1e-8,
+            "fp64": {"iterations": its, "info": info, "seconds": t64, "final_residual": res[-1]},
+            "mixed_refined": {"refinements": rinfo["refinements"], "inner_iterations": rinfo["inner_iterations"],
+                              "residuals": rinfo["relative_residuals"], "seconds": rinfo["seconds"],
+                              "inner_dtype": "complex64"},
+            "solution_rel_diff_vs_fp64": diff, "mixed_solution_residual_in_fp64_operator": res_true}
 
 
 def e2e_measure(args, torch, grid, domain, dual, world, dist, clear_cache, total_entries):
