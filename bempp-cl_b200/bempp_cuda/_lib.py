@@ -154,6 +154,48 @@ class PotentialArgs(_ct.Structure):
     ]
 
 
+class BatchProblem(_ct.Structure):
+    _fields_ = [
+        ("grid", GridRec),
+        ("support", _vp),
+        ("result", _vp),
+        ("ld", _i64),
+        ("params", _ct.c_double * 4),
+        ("phase_radius", _ct.c_double),
+        ("precision", _i32),
+        ("pad", _i32),
+        ("pair_begin", _i64),
+        ("pair_count", _i64),
+    ]
+
+
+class BatchArgs(_ct.Structure):
+    _fields_ = [
+        ("kernel", _i32),
+        ("nproblems", _i32),
+        ("problems", _ct.POINTER(BatchProblem)),
+        ("nq", _i32),
+        ("blocks_per_sm", _i32),
+        ("quad_points", _vp),
+        ("quad_weights", _vp),
+        ("npairs", _i64),
+        ("test_points", _vp),
+        ("trial_points", _vp),
+        ("weights", _vp),
+        ("test_elements", _vp),
+        ("trial_elements", _vp),
+        ("test_offsets", _vp),
+        ("trial_offsets", _vp),
+        ("weights_offsets", _vp),
+        ("npoints", _vp),
+        ("diag_shift", _ct.c_double),
+        ("rows_per_item", _i32),
+        ("pad", _i32),
+        ("workspace", _vp),
+        ("workspace_bytes", _i64),
+    ]
+
+
 # every exported symbol of include/bemppcuda.h with (restype, argtypes)
 SIGNATURES = {
     "bemppcuda_version": (_ct.c_int, []),
@@ -165,6 +207,9 @@ SIGNATURES = {
     "bemppcuda_evaluate_potential": (_ct.c_int, [_ct.POINTER(PotentialArgs), _vp]),
     "bemppcuda_fma_probe": (_ct.c_int, [_i32, _i64, _i64, _vp, _ct.POINTER(_ct.c_double), _vp]),
     "bemppcuda_evaluate_potential_noalloc": (_ct.c_int, [_ct.POINTER(PotentialArgs), _vp]),
+    "bemppcuda_batch_workspace_bytes": (_i64, [_i32]),
+    "bemppcuda_batch_prepare": (_ct.c_int, [_ct.POINTER(BatchArgs), _vp]),
+    "bemppcuda_batch_launch": (_ct.c_int, [_ct.POINTER(BatchArgs), _vp]),
 }
 
 # fixed workspace of bemppcuda_evaluate_potential_noalloc, in doubles

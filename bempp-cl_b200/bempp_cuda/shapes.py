@@ -8,6 +8,8 @@ gives 8 * 4**level outward-oriented triangles and 4 * 4**level + 2 vertices
 (L4: 2048 / 1026, L5: 8192 / 4098, L6: 32768 / 16386).
 """
 
+import functools as _functools
+
 import numpy as _np
 
 from .grid import Grid
@@ -23,34 +25,48 @@ def _octahedron():
     return vertices, faces
 
 
+@_functools.lru_cache(maxsize=16)
+def _sphere_arrays_cached(level):
+    vertices, faces = _octahedron()
+    verts = vertices.copy()
+    for _ in range(level):
+        nv = verts.shape[0]
+        # the three edges of every face, as sorted vertex pairs
+        e = _np.concatenate([faces[:, [0, 1]], faces[:, [1, 2]], faces[:, [2, 0]]])
+        key = _np.minimum(e[:, 0], e[:, 1]) * nv + _np.maximum(e[:, 0], e[:, 1])
+        uniq, inverse = _np.unique(key, return_inverse=True)
+        # number new vertices by first appearance (face-major, edge ab, bc, ca)
+        nf = faces.shape[0]
+        idx = _np.arange(3 * nf)
+        order_key = _np.full(len(uniq), 3 * nf, dtype=_np.int64)
+        _np.minimum.at(order_key, inverse, (idx % nf) * 3 + idx // nf)
+        rank = _np.empty(len(uniq), dtype=_np.int64)
+        rank[_np.argsort(order_key, kind="stable")] = _np.arange(len(uniq))
+        lo = uniq // nv
+        hi = uniq % nv
+        mids = verts[lo] + verts[hi]
+        mids /= _np.linalg.norm(mids, axis=1, keepdims=True)
+        new_verts = _np.empty((nv + len(uniq), 3))
+        new_verts[:nv] = verts
+        new_verts[nv + rank] = mids
+        m = nv + rank[inverse]
+        ab, bc, ca = m[:nf], m[nf : 2 * nf], m[2 * nf :]
+        a_, b_, c_ = faces[:, 0], faces[:, 1], faces[:, 2]
+        new_faces = _np.empty((4 * nf, 3), dtype=_np.int64)
+        new_faces[0::4] = _np.stack([a_, ab, ca], axis=1)
+        new_faces[1::4] = _np.stack([ab, b_, bc], axis=1)
+        new_faces[2::4] = _np.stack([ca, bc, c_], axis=1)
+        new_faces[3::4] = _np.stack([ab, bc, ca], axis=1)
+        verts, faces = new_verts, new_faces
+    return verts.T.copy(), faces.T.copy()
+
+
 def sphere_arrays(level):
     """Return (vertices (3, nv), elements (3, ne)) of the subdivided octahedron."""
     if level < 0:
         raise ValueError("level must be non-negative")
-    vertices, faces = _octahedron()
-    verts = [v for v in vertices]
-    for _ in range(level):
-        midpoint = {}
-        new_faces = _np.empty((4 * len(faces), 3), dtype=_np.int64)
-
-        def mid(a, b):
-            key = (a, b) if a < b else (b, a)
-            idx = midpoint.get(key)
-            if idx is None:
-                p = verts[a] + verts[b]
-                verts.append(p / _np.linalg.norm(p))
-                idx = len(verts) - 1
-                midpoint[key] = idx
-            return idx
-
-        for k, (a, b, c) in enumerate(faces):
-            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
-            new_faces[4 * k + 0] = (a, ab, ca)
-            new_faces[4 * k + 1] = (ab, b, bc)
-            new_faces[4 * k + 2] = (ca, bc, c)
-            new_faces[4 * k + 3] = (ab, bc, ca)
-        faces = new_faces
-    return _np.array(verts).T.copy(), faces.T.copy()
+    v, e = _sphere_arrays_cached(int(level))
+    return v.copy(), e.copy()
 
 
 def regular_sphere(level):

@@ -177,6 +177,49 @@ typedef struct {
     int64_t workspace_bytes;
 } bemppcuda_potential_args;
 
+/* Batched DP0 assembly (many grids / wavenumbers in one persistent launch).
+   No single reference counterpart: the reference assembles one operator per
+   weak_form() call (core/dense_assembler.py:49-98); this assembles a list of
+   them.  Each problem has identical full-support DP0 test and trial spaces on
+   its own grid (rows = columns = elements). */
+typedef struct {
+    bemppcuda_grid grid;
+    const uint32_t *support; /* (nelements,) 0, 1, ..., nelements - 1 */
+    void *result;            /* complex128 (nelements, ld), every entry written */
+    int64_t ld;
+    double params[4];        /* (Re k, Im k, Re eta, Im eta) */
+    double phase_radius;     /* 2 x largest centroid-to-vertex distance of the grid (0 = unknown) */
+    int32_t precision;       /* BEMPPCUDA_FP64 or BEMPPCUDA_MIXED */
+    int32_t pad;
+    int64_t pair_begin;      /* first singular pair of this problem in the concatenated arrays */
+    int64_t pair_count;
+} bemppcuda_batch_problem;
+
+typedef struct {
+    int32_t kernel;                           /* BEMPPCUDA_HELMHOLTZ_SLP or _COMBINED, for all problems */
+    int32_t nproblems;
+    const bemppcuda_batch_problem *problems;  /* HOST array of nproblems entries */
+    int32_t nq;                               /* must be 6 */
+    int32_t blocks_per_sm;                    /* persistent grid = blocks_per_sm x SMs (0: 4) */
+    const double *quad_points;                /* HOST (nq, 2) */
+    const double *quad_weights;               /* HOST (nq,) */
+    int64_t npairs;                           /* singular pairs of all problems, concatenated */
+    const double *test_points;                /* shared Sauter-Schwab tables (P, 2) */
+    const double *trial_points;
+    const double *weights;
+    const uint32_t *test_elements;            /* element ids local to each problem's grid */
+    const uint32_t *trial_elements;
+    const uint32_t *test_offsets;
+    const uint32_t *trial_offsets;
+    const uint32_t *weights_offsets;
+    const uint32_t *npoints;
+    double diag_shift;                        /* + diag_shift * area on coincident entries */
+    int32_t rows_per_item;                    /* test elements per work item, 1..32 (0: 32) */
+    int32_t pad;
+    void *workspace;                          /* bemppcuda_batch_workspace_bytes(nproblems) bytes */
+    int64_t workspace_bytes;
+} bemppcuda_batch_args;
+
 int bemppcuda_version(void);
 int bemppcuda_last_error(char *buffer, int64_t length);
 
@@ -208,6 +251,16 @@ int bemppcuda_evaluate_potential(const bemppcuda_potential_args *args, void *str
    before any stream capture starts on that device. */
 #define BEMPPCUDA_NOALLOC_SCRATCH_DOUBLES (3 * 1024 * 1024)
 int bemppcuda_evaluate_potential_noalloc(const bemppcuda_potential_args *args, void *stream);
+
+int64_t bemppcuda_batch_workspace_bytes(int32_t nproblems);
+/* Upload the problem table into the workspace (host-to-device copy on the
+   stream, then a stream synchronize); call again whenever the list changes. */
+int bemppcuda_batch_prepare(const bemppcuda_batch_args *args, void *stream);
+/* Reset the work counter, run the persistent regular-pair kernel over every
+   (problem, tile) item and the batched singular kernel.  Device work only
+   (a memset and two launches), so it can be captured in a CUDA graph once
+   bemppcuda_batch_prepare has run. */
+int bemppcuda_batch_launch(const bemppcuda_batch_args *args, void *stream);
 
 /* Measurement utility, no reference counterpart: launches `blocks` x 256
    threads that each run 32 independent FMAs per iteration in FP64
