@@ -19,6 +19,11 @@ pairs + Sauter-Schwab singular pairs + identity), matrix resident in HBM.
   same run by ``bemppcuda_fma_probe``.
 * ``cpu_baseline``: the oracle (a C/OpenMP restatement of the reference Numba
   kernels) on a bounded row sample of the same operator, all host cores.
+* ``batch``: 64 DP0 Helmholtz single-layer problems on seeded ellipsoids
+  (regular_sphere(3..5) scaled per axis, k ~ U[1, 16]) assembled in one
+  persistent launch per precision after autotuning, then replayed as a CUDA
+  graph together with the 8-right-hand-side product of every problem; the
+  same problems assembled one launch pair at a time give the unbatched time.
 
 Multi-GPU (torchrun): the rows (test elements) are split into one contiguous
 block per rank; each rank assembles its block with no collective (strong
@@ -62,6 +67,7 @@ def parse():
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-solve", action="store_true")
+    ap.add_argument("--skip-batch", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time per baseline sample")
     return ap.parse_args()
 
@@ -306,6 +312,12 @@ def gpu_arm(args, world, rank, local):
     if not args.skip_e2e:
         e2e = e2e_measure(args, torch, grid, domain, dual, world, dist, clear_cache, total_entries)
 
+    batch = None
+    if not args.skip_batch:
+        del out
+        torch.cuda.empty_cache()
+        batch = batch_measure(args, torch, world, rank, dist)
+
     line = {
         "metric": "entries/s Helmholtz assembly, mixed vs FP64 GPU at rel err <=1e-6; shape-grads/s",
         "value": value,
@@ -340,6 +352,8 @@ def gpu_arm(args, world, rank, local):
         line["e2e"] = e2e
     if solve is not None:
         line["solve"] = solve
+    if batch is not None:
+        line["batch"] = batch
     return line
 
 
@@ -368,6 +382,120 @@ def solve_measure(args, torch, grid, domain, a64, amx):
                               "residuals": rinfo["relative_residuals"], "seconds": rinfo["seconds"],
                               "inner_dtype": "complex64"},
             "solution_rel_diff_vs_fp64": diff, "mixed_solution_residual_in_fp64_operator": res_true}
+
+
+def batch_shard(sizes, world, rank):
+    """Problems of this rank: largest first onto the least-loaded rank (load = entries = n^2)."""
+    load = [0] * world
+    mine = []
+    for i in sorted(range(len(sizes)), key=lambda j: (-sizes[j], j)):
+        r = min(range(world), key=lambda j: (load[j], j))
+        load[r] += sizes[i] ** 2
+        if r == rank:
+            mine.append(i)
+    return sorted(mine)
+
+
+def batch_measure(args, torch, world, rank, dist):
+    """64 DP0 Helmholtz SLP problems (ellipsoids L in {3,4,5}, k ~ U[1,16]) in one persistent launch.
+
+    Each precision is autotuned, then one CUDA graph holding the batched
+    assembly and the 8-right-hand-side products of every problem is replayed.
+    The same problems assembled one after another through the single-problem
+    kernels give the unbatched time.
+    """
+    from bempp_cuda import _lib, operators
+    from bempp_cuda.assembly import regular_into, singular_into_dense
+    from bempp_cuda.batch import BatchAssembler, c4_problems
+    from bempp_cuda.operators import Parameters
+
+    probs = c4_problems(64, seed=0)
+    mine = batch_shard([g.number_of_elements for g, _ in probs], world, rank)
+    grids = [probs[i][0] for i in mine]
+    ks = [probs[i][1] for i in mine]
+    rhs = []
+    for i in mine:
+        rng = np.random.default_rng(1000 + i)
+        n = probs[i][0].number_of_elements
+        rhs.append(torch.as_tensor(rng.standard_normal((n, 8)) + 1j * rng.standard_normal((n, 8)), device="cuda"))
+    entries_all = sum(g.number_of_elements ** 2 for g, _ in probs)
+
+    def max_ms(ms):
+        if dist is None:
+            return ms
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def events_ms(fn, steps):
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return max_ms(e0.elapsed_time(e1) / steps)
+
+    res = {"problems": len(probs), "elements": sorted(g.number_of_elements for g, _ in probs),
+           "entries": entries_all, "rhs_per_problem": 8, "shards": "largest-first onto least-loaded rank"}
+    outputs64 = None
+    for prec in ("fp64", "mixed"):
+        ba = BatchAssembler(grids, ks, precision=prec)
+        t0 = time.perf_counter()
+        shape, timings = ba.autotune()
+        tune_s = time.perf_counter() - t0
+        prods = [torch.empty_like(x) for x in rhs]
+        ba.capture(rhs, prods)
+        for _ in range(args.warmup):
+            ba.replay()
+        launch_ms = events_ms(ba.launch, args.steps)
+        graph_ms = events_ms(ba.replay, args.steps)
+        entry = {"rows_per_item": shape[0], "ctas_per_sm": shape[1], "autotune_s": tune_s,
+                 "shapes_timed": len(timings), "launch_ms": launch_ms, "graph_ms": graph_ms,
+                 "entries_per_s": entries_all / (launch_ms * 1e-3),
+                 "graph_entries_per_s": entries_all / (graph_ms * 1e-3)}
+        if prec == "fp64":
+            outputs64 = [o.clone() for o in ba.outputs]
+        else:
+            errs = [(torch.linalg.norm(a - b) / torch.linalg.norm(b)).item() for a, b in zip(ba.outputs, outputs64)]
+            entry["max_rel_fro_err_vs_fp64"] = max(errs) if errs else 0.0
+        res[prec] = entry
+        del ba, prods
+        torch.cuda.empty_cache()
+    del outputs64
+
+    # unbatched: the same problems one by one (two launches each), device inputs resident
+    params = Parameters()
+    singles = []
+    for g, k in zip(grids, ks):
+        from bempp_cuda.space import function_space
+
+        sp = function_space(g, "DP", 0)
+        desc = operators.boundary.helmholtz.single_layer(sp, sp, sp, k).descriptor
+        singles.append((sp, desc, torch.empty((g.number_of_elements,) * 2, dtype=torch.complex128, device="cuda")))
+
+    def sequential(precision):
+        def run():
+            for sp, desc, out in singles:
+                regular_into(out, desc, sp, sp, params, precision=precision, overwrite=True)
+                singular_into_dense(out, desc, sp, sp, params)
+        return run
+
+    for prec, code in (("fp64", _lib.FP64), ("mixed", _lib.MIXED)):
+        run = sequential(code)
+        for _ in range(args.warmup):
+            run()
+        ms = events_ms(run, args.steps)
+        res[prec]["unbatched_ms"] = ms
+        res[prec]["batched_speedup"] = ms / res[prec]["launch_ms"]
+    res["mixed_over_fp64"] = res["mixed"]["entries_per_s"] / res["fp64"]["entries_per_s"]
+    del singles
+    torch.cuda.empty_cache()
+    return res
 
 
 def e2e_measure(args, torch, grid, domain, dual, world, dist, clear_cache, total_entries):
