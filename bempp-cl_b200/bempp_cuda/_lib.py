@@ -196,6 +196,49 @@ class BatchArgs(_ct.Structure):
     ]
 
 
+class ShapeArgs(_ct.Structure):
+    _fields_ = [
+        ("grid", GridRec),
+        ("normal_mult", _vp),
+        ("k", _ct.c_double),
+        ("dlp_coeff", _ct.c_double),
+        ("eta", _ct.c_double * 2),
+        ("deta_dk", _ct.c_double * 2),
+        ("identity", _ct.c_double),
+        ("nq", _i32),
+        ("ndirections", _i32),
+        ("quad_points", _vp),
+        ("quad_weights", _vp),
+        ("npairs", _i64),
+        ("test_points", _vp),
+        ("trial_points", _vp),
+        ("weights", _vp),
+        ("test_elements", _vp),
+        ("trial_elements", _vp),
+        ("test_offsets", _vp),
+        ("trial_offsets", _vp),
+        ("weights_offsets", _vp),
+        ("npoints", _vp),
+        ("directions", _vp),
+        ("ff_dlp_coeff", _ct.c_double),
+        ("ff_eta", _ct.c_double * 2),
+        ("ff_deta_dk", _ct.c_double * 2),
+        ("incident", _ct.c_double * 3),
+        ("rhs_coeff", _ct.c_double * 2),
+        ("phi", _vp),
+        ("lam", _vp),
+        ("u", _vp),
+        ("scale_operator", _ct.c_double),
+        ("scale_farfield", _ct.c_double),
+        ("scale_rhs", _ct.c_double),
+        ("vertex_grad", _vp),
+        ("k_grad", _vp),
+        ("out", _vp),
+        ("workspace", _vp),
+        ("workspace_bytes", _i64),
+    ]
+
+
 # every exported symbol of include/bemppcuda.h with (restype, argtypes)
 SIGNATURES = {
     "bemppcuda_version": (_ct.c_int, []),
@@ -210,6 +253,10 @@ SIGNATURES = {
     "bemppcuda_batch_workspace_bytes": (_i64, [_i32]),
     "bemppcuda_batch_prepare": (_ct.c_int, [_ct.POINTER(BatchArgs), _vp]),
     "bemppcuda_batch_launch": (_ct.c_int, [_ct.POINTER(BatchArgs), _vp]),
+    "bemppcuda_shape_workspace_bytes": (_i64, [_i64]),
+    "bemppcuda_farfield_matrix_dp0": (_ct.c_int, [_ct.POINTER(ShapeArgs), _vp]),
+    "bemppcuda_plane_wave_dp0": (_ct.c_int, [_ct.POINTER(ShapeArgs), _vp]),
+    "bemppcuda_shape_adjoint_dp0": (_ct.c_int, [_ct.POINTER(ShapeArgs), _vp]),
 }
 
 # fixed workspace of bemppcuda_evaluate_potential_noalloc, in doubles

@@ -75,13 +75,19 @@ def _grids_identical(domain, dual_to_range):
 
 
 def regular_into(
-    result, descriptor, domain, dual_to_range, parameters, precision=_lib.FP64, overwrite=False, stream=None
+    result, descriptor, domain, dual_to_range, parameters, precision=_lib.FP64, overwrite=False, stream=None,
+    geometry=None,
 ):
-    """Add (or with ``overwrite`` store) the regular part into the device tensor ``result``."""
+    """Add (or with ``overwrite`` store) the regular part into the device tensor ``result``.
+
+    ``geometry`` (a DeviceGrid-like object with ``record()`` and ``radius``)
+    replaces the device geometry of both grids, e.g. a grid whose vertices
+    moved while its elements stayed the same.
+    """
     require_cuda()
     kernel, assembly = kernel_ids(descriptor)
-    tgrid = device_grid(dual_to_range.grid)
-    sgrid = device_grid(domain.grid)
+    tgrid = geometry or device_grid(dual_to_range.grid)
+    sgrid = geometry or device_grid(domain.grid)
     tspace = device_space(dual_to_range)
     sspace = device_space(domain)
     points, weights = regular_rule(parameters.quadrature.regular)
@@ -117,8 +123,9 @@ def dp0_fast_path(descriptor, domain, dual_to_range, parameters):
     return bool(device_space(domain).dof_is_position and device_space(dual_to_range).dof_is_position)
 
 
-def singular_into_dense(result, descriptor, domain, dual_to_range, parameters, diag_shift=0.0, stream=None):
-    """Scatter the Sauter-Schwab pairs into the dense device tensor ``result``."""
+def singular_into_dense(result, descriptor, domain, dual_to_range, parameters, diag_shift=0.0, stream=None,
+                        geometry=None):
+    """Scatter the Sauter-Schwab pairs into the dense device tensor ``result`` (``geometry`` as in regular_into)."""
     kernel, assembly = kernel_ids(descriptor)
     grid = domain.grid
     rule = device_singular_rule(grid, parameters.quadrature.singular, dual_to_range.support, domain.support)
@@ -127,7 +134,7 @@ def singular_into_dense(result, descriptor, domain, dual_to_range, parameters, d
     args.assembly = assembly
     args.is_complex = 1 if result.is_complex() else 0
     _set_params(args, descriptor.options)
-    args.grid = device_grid(grid).record()
+    args.grid = (geometry or device_grid(grid)).record()
     args.test = device_space(dual_to_range).record()
     args.trial = device_space(domain).record()
     rule.fill(args)

@@ -1,0 +1,670 @@
+// Shape derivatives of a DP0 Helmholtz scattering functional (adjoint method).
+//
+// For A phi = b, u = F phi and a real functional of u, the adjoint vector
+// lambda reduces the vertex gradient to three contractions
+//   Re(lambda^H dA phi), Re(u^H dF phi), Re(lambda^H db),
+// each a sum over element pairs (or elements) of derivatives of quadrature
+// sums.  Nothing here forms dA/dx: every pass recomputes the quadrature.
+//
+// Notation for one element pair (test t, trial s), DP0, one quadrature-point
+// pair (x in t, y in s), d = y - x, r = |d|, G = exp(ikr) / (4 pi r),
+// z = ikr - 1, c_s = (v1 - v0) x (v2 - v0) of s (so c_s = ie_s n_s),
+// u = (d . c_s) / r^2:
+//   A_ts = ie_t sum w [ beta G z u + eta ie_s G ]         (DLP + eta SLP)
+// with beta = dlp_coeff * normal multiplier of s.  Contracted with
+// c' = conj(lambda_t) phi_s ie_t and Gc = c' w G:
+//   d/dd    : gd = a1 d + a2 c_s,
+//             a1 = [beta u Re(Gc (3 - k^2 r^2 - 3ikr)) + ie_s Re(Gc z eta)] / r^2,
+//             a2 = beta Re(Gc z) / r^2
+//   d/dc_s  : a2 d
+//   d/die_s : Re(Gc eta)
+//   d/die_t : Re(Gc (beta z u + eta ie_s)) / ie_t
+//   d/dk    : Re(Gc (-beta k r^2 u + (i eta r + eta') ie_s))
+// (from dG/dr = G z / r, d(G z / r^2)/dr = G (3 - 3ikr - k^2 r^2) / r^3,
+// dG/dk = i r G, d(G z / r^2)/dk = -k G).  x = v0 + xi e1 + eta e2 with
+// e1 = v1 - v0, e2 = v2 - v0, so vertex a of t receives -sum N_a(x) gd and
+// vertex b of s receives +sum N_b(y) gd; c and ie go through the cross
+// product:  d(C . c)/dv1 = e2 x C, d(C . c)/dv2 = C x e1,
+// d ie/dv1 = e2 x n, d ie/dv2 = n x e1, and dv0 = -(dv1 + dv2) for both.
+//
+// The quadrature points are fixed in reference coordinates (regular rule and
+// Sauter-Schwab tables alike), so these are exact derivatives of the
+// discrete operator; near the singular set every derivative of d is O(r)
+// (shared vertices move with both elements), so the singular rules integrate
+// the differentiated kernel as they integrate the kernel itself.
+#include "common.cuh"
+#include "fastmath.cuh"
+
+namespace bc {
+
+// Per-element partial sums, SH_ACC doubles per element (element-major):
+//  0-2  sum gd            (element as test)     10-12 sum gd           (element as trial)
+//  3-5  sum xi(x) gd                            13-15 sum xi(y) gd
+//  6-8  sum eta(x) gd                           16-18 sum eta(y) gd
+//  9    sum ie_t d/die_t                        19-21 sum a2 d
+//                                               22    sum Re(Gc eta)
+//                                               23    d/dk
+constexpr int SH_ACC = 24;
+constexpr int SH_THREADS = 128;
+constexpr int SH_TCHUNK = 32;
+constexpr int SH_TILES = 8;  // test chunks per block
+constexpr int SH_WARPS = SH_THREADS / 32;
+constexpr int SHS_WARPS = 8;  // singular kernel: pairs per block
+constexpr int SH_NQ = 6;
+
+struct ShapeParams {
+    const double *g;
+    int64_t ne, nv;
+    const int32_t *el;
+    const int32_t *nm;
+    double k, beta, eta_re, eta_im, deta_re, deta_im, ident;
+    const double2 *phi, *lam, *u;
+    double *acc, *vgrad, *kgrad;
+    int64_t npairs;
+    const double2 *tp, *sp;
+    const double *w;
+    const int32_t *te, *se, *toff, *soff, *woff, *npts;
+    int ndir;
+    int pad;
+    const double *dirs;
+    double ff_beta, ff_eta_re, ff_eta_im, ff_deta_re, ff_deta_im;
+    double inc[3];
+    double rhs_re, rhs_im;
+    double scale_op, scale_ff, scale_rhs;
+    void *out;
+};
+
+struct QpeTerms {
+    double gd[3];
+    double a2, ival, ere, kval;
+};
+
+__device__ __forceinline__ void cross3(const double a[3], const double b[3], double o[3]) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// One quadrature-point pair of the combined kernel, contracted with c' = (cre, cim).
+__device__ __forceinline__ void qpe_terms(const double d[3], double w, double cre, double cim, const double cs[3],
+                                          double ies, double bet, const ShapeParams &P, QpeTerms &o) {
+    const double r2 = fma(d[2], d[2], fma(d[1], d[1], d[0] * d[0]));
+    const double rinv = rsqrt(r2);
+    const double r = r2 * rinv;
+    const double rinv2 = rinv * rinv;
+    const double kr = P.k * r;
+    double sn, cn;
+    sincos_cw64(kr, &sn, &cn);
+    const double f = w * rinv * BC_INV_4PI;
+    const double gr = cn * f, gi = sn * f;
+    const double Gr = cre * gr - cim * gi, Gi = fma(cre, gi, cim * gr);  // Gc = c' w G
+    const double u = fma(d[2], cs[2], fma(d[1], cs[1], d[0] * cs[0])) * rinv2;
+    const double Zr = fma(-Gi, kr, -Gr), Zi = fma(Gr, kr, -Gi);  // Gc z
+    const double reGcEta = Gr * P.eta_re - Gi * P.eta_im;
+    const double reGzEta = Zr * P.eta_re - Zi * P.eta_im;
+    const double t1 = fma(Gr, 3.0 - kr * kr, 3.0 * kr * Gi);  // Re(Gc (3 - k^2 r^2 - 3ikr))
+    const double bu = bet * u;
+    const double a1 = fma(bu, t1, ies * reGzEta) * rinv2;
+    const double a2 = bet * Zr * rinv2;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o.gd[c] = fma(a1, d[c], a2 * cs[c]);
+    o.a2 = a2;
+    o.ival = fma(bu, Zr, ies * reGcEta);
+    o.ere = reGcEta;
+    const double er = P.deta_re - P.eta_im * r, ei = fma(P.eta_re, r, P.deta_im);
+    o.kval = fma(-bu * P.k * r2, Gr, ies * (Gr * er - Gi * ei));
+}
+
+__device__ __forceinline__ bool touches(const int *a, int b0, int b1, int b2) {
+    return (a[0] == b0) | (a[0] == b1) | (a[0] == b2) | (a[1] == b0) | (a[1] == b1) | (a[1] == b2) | (a[2] == b0) |
+           (a[2] == b1) | (a[2] == b2);
+}
+
+struct ShapeTile {
+    double x[SH_TCHUNK][SH_NQ][3];
+    double2 lc[SH_TCHUNK];  // conj(lambda_t) ie_t
+    int v[SH_TCHUNK][3];
+    double red[SH_WARPS][SH_TCHUNK][10];
+};
+
+// Regular pairs: one thread per trial element, SH_TILES chunks of SH_TCHUNK
+// test elements staged in shared memory.  Trial-side sums stay in registers
+// for the whole block; test-side sums are reduced over the warp (shuffles),
+// then over the block's warps (shared memory), then added to the workspace.
+__global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadRule rule) {
+    __shared__ ShapeTile sb;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t s = (int64_t)blockIdx.x * SH_THREADS + threadIdx.x;
+    const bool active = s < P.ne;
+    double y[SH_NQ][3], cs[3] = {0.0, 0.0, 0.0};
+    double ies = 0.0, bet = 0.0, pr = 0.0, pim = 0.0;
+    int sv0 = -1, sv1 = -1, sv2 = -1;
+    if (active) {
+        Geom gs;
+        load_geom(P.g, P.ne, s, 1.0, gs);
+#pragma unroll
+        for (int q = 0; q < SH_NQ; ++q) to_global(gs, rule.x[q], rule.y[q], y[q]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) cs[c] = gs.n[c] * gs.ie;
+        ies = gs.ie;
+        bet = P.beta * (P.nm ? (double)P.nm[s] : 1.0);
+        const double2 ph = P.phi[s];
+        pr = ph.x;
+        pim = ph.y;
+        sv0 = P.el[3 * s];
+        sv1 = P.el[3 * s + 1];
+        sv2 = P.el[3 * s + 2];
+    } else {
+#pragma unroll
+        for (int q = 0; q < SH_NQ; ++q) y[q][0] = y[q][1] = y[q][2] = 0.0;
+    }
+    double ty[3] = {0.0, 0.0, 0.0}, xy[3] = {0.0, 0.0, 0.0}, yy[3] = {0.0, 0.0, 0.0}, cy[3] = {0.0, 0.0, 0.0};
+    double ey = 0.0, kacc = 0.0;
+
+    for (int tile = 0; tile < SH_TILES; ++tile) {
+        const int64_t t0 = ((int64_t)blockIdx.y * SH_TILES + tile) * SH_TCHUNK;
+        if (t0 >= P.ne) break;  // uniform over the block
+        const int tcount = (int)min((int64_t)SH_TCHUNK, P.ne - t0);
+        __syncthreads();  // previous tile's shared data fully consumed
+        for (int idx = threadIdx.x; idx < tcount; idx += SH_THREADS) {
+            const int64_t t = t0 + idx;
+            Geom g;
+            load_geom(P.g, P.ne, t, 1.0, g);
+#pragma unroll
+            for (int p = 0; p < SH_NQ; ++p) to_global(g, rule.x[p], rule.y[p], sb.x[idx][p]);
+            const double2 l = P.lam[t];
+            sb.lc[idx] = make_double2(l.x * g.ie, -l.y * g.ie);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) sb.v[idx][c] = P.el[3 * t + c];
+        }
+        __syncthreads();
+        for (int tt = 0; tt < tcount; ++tt) {
+            double px[10];
+#pragma unroll
+            for (int f = 0; f < 10; ++f) px[f] = 0.0;
+            const bool skip = !active || touches(sb.v[tt], sv0, sv1, sv2);
+            if (!skip) {
+                const double2 lc = sb.lc[tt];
+                const double cre = lc.x * pr - lc.y * pim, cim = fma(lc.x, pim, lc.y * pr);
+                for (int p = 0; p < SH_NQ; ++p) {
+                    const double x0 = sb.x[tt][p][0], x1 = sb.x[tt][p][1], x2 = sb.x[tt][p][2];
+                    const double wp = rule.w[p];
+                    double pp[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+                    for (int q = 0; q < SH_NQ; ++q) {
+                        const double d[3] = {y[q][0] - x0, y[q][1] - x1, y[q][2] - x2};
+                        QpeTerms o;
+                        qpe_terms(d, wp * rule.w[q], cre, cim, cs, ies, bet, P, o);
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            pp[c] += o.gd[c];
+                            xy[c] = fma(rule.x[q], o.gd[c], xy[c]);
+                            yy[c] = fma(rule.y[q], o.gd[c], yy[c]);
+                            cy[c] = fma(o.a2, d[c], cy[c]);
+                        }
+                        px[9] += o.ival;
+                        ey += o.ere;
+                        kacc += o.kval;
+                    }
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        px[c] += pp[c];
+                        px[3 + c] = fma(rule.x[p], pp[c], px[3 + c]);
+                        px[6 + c] = fma(rule.y[p], pp[c], px[6 + c]);
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < 3; ++c) ty[c] += px[c];
+            }
+#pragma unroll
+            for (int f = 0; f < 10; ++f) px[f] = warp_sum(px[f]);
+            if (lane == 0)
+#pragma unroll
+                for (int f = 0; f < 10; ++f) sb.red[warp][tt][f] = px[f];
+        }
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < tcount * 10; idx += SH_THREADS) {
+            const int tt = idx / 10, f = idx - 10 * (idx / 10);
+            double v = 0.0;
+#pragma unroll
+            for (int wi = 0; wi < SH_WARPS; ++wi) v += sb.red[wi][tt][f];
+            if (v != 0.0) atomicAdd(P.acc + (t0 + tt) * SH_ACC + f, v);
+        }
+    }
+    if (active) {
+        double *a = P.acc + s * SH_ACC;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            atomicAdd(a + 10 + c, ty[c]);
+            atomicAdd(a + 13 + c, xy[c]);
+            atomicAdd(a + 16 + c, yy[c]);
+            atomicAdd(a + 19 + c, cy[c]);
+        }
+        atomicAdd(a + 22, ey);
+        atomicAdd(a + 23, kacc);
+    }
+}
+
+// Singular pairs: one warp per pair, lanes over its Sauter-Schwab points.
+__global__ void __launch_bounds__(32 * SHS_WARPS) shape_singular(ShapeParams P) {
+    const int lane = threadIdx.x & 31;
+    const int64_t k = (int64_t)blockIdx.x * SHS_WARPS + (threadIdx.x >> 5);
+    if (k >= P.npairs) return;
+    const int64_t t = P.te[k], s = P.se[k];
+    Geom gt, gs;
+    load_geom(P.g, P.ne, t, 1.0, gt);
+    load_geom(P.g, P.ne, s, 1.0, gs);
+    const double2 l = P.lam[t], ph = P.phi[s];
+    const double cre = (l.x * ph.x + l.y * ph.y) * gt.ie, cim = (l.x * ph.y - l.y * ph.x) * gt.ie;
+    const double cs[3] = {gs.n[0] * gs.ie, gs.n[1] * gs.ie, gs.n[2] * gs.ie};
+    const double bet = P.beta * (P.nm ? (double)P.nm[s] : 1.0);
+    const double ies = gs.ie;
+    // 0-2 sum gd, 3-5 xi(x) gd, 6-8 eta(x) gd, 9-11 xi(y) gd, 12-14 eta(y) gd, 15-17 a2 d, 18 ival, 19 ere, 20 k
+    double a[21];
+#pragma unroll
+    for (int f = 0; f < 21; ++f) a[f] = 0.0;
+    const int64_t toff = P.toff[k], soff = P.soff[k], woff = P.woff[k];
+    const int n = P.npts[k];
+    for (int m = lane; m < n; m += 32) {
+        const double2 tpm = P.tp[toff + m], spm = P.sp[soff + m];
+        const double w = P.w[woff + m];
+        double x[3], y[3];
+        to_global(gt, tpm.x, tpm.y, x);
+        to_global(gs, spm.x, spm.y, y);
+        const double d[3] = {y[0] - x[0], y[1] - x[1], y[2] - x[2]};
+        QpeTerms o;
+        qpe_terms(d, w, cre, cim, cs, ies, bet, P, o);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            a[c] += o.gd[c];
+            a[3 + c] = fma(tpm.x, o.gd[c], a[3 + c]);
+            a[6 + c] = fma(tpm.y, o.gd[c], a[6 + c]);
+            a[9 + c] = fma(spm.x, o.gd[c], a[9 + c]);
+            a[12 + c] = fma(spm.y, o.gd[c], a[12 + c]);
+            a[15 + c] = fma(o.a2, d[c], a[15 + c]);
+        }
+        a[18] += o.ival;
+        a[19] += o.ere;
+        a[20] += o.kval;
+    }
+#pragma unroll
+    for (int f = 0; f < 21; ++f) a[f] = warp_sum(a[f]);
+    if (lane != 0) return;
+    double *at = P.acc + t * SH_ACC, *as = P.acc + s * SH_ACC;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        atomicAdd(at + c, a[c]);
+        atomicAdd(at + 3 + c, a[3 + c]);
+        atomicAdd(at + 6 + c, a[6 + c]);
+        atomicAdd(as + 10 + c, a[c]);
+        atomicAdd(as + 13 + c, a[9 + c]);
+        atomicAdd(as + 16 + c, a[12 + c]);
+        atomicAdd(as + 19 + c, a[15 + c]);
+    }
+    atomicAdd(at + 9, a[18]);
+    atomicAdd(as + 22, a[19]);
+    atomicAdd(as + 23, a[20]);
+}
+
+// Vertex gradient of one element from "trial-type" sums: sum of a gradient
+// with respect to points y (T, sum xi(y) ., sum eta(y) .), a vector C
+// contracted with c = e1 x e2, and a coefficient of ie.
+__device__ __forceinline__ void trial_chain(const Geom &g, const double di[3][3], const double T[3],
+                                            const double X[3], const double Y[3], const double C[3], double cie,
+                                            double gv[3][3]) {
+    double w1[3], w2[3];
+    cross3(g.j1, C, w1);
+    cross3(C, g.j0, w2);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        gv[0][c] += T[c] - X[c] - Y[c] - w1[c] - w2[c] + cie * di[0][c];
+        gv[1][c] += X[c] + w1[c] + cie * di[1][c];
+        gv[2][c] += Y[c] + w2[c] + cie * di[2][c];
+    }
+}
+
+// One thread per element: chain rule of the operator sums, the far-field and
+// right-hand-side terms, scatter to the vertices, and the wavenumber sum.
+__global__ void __launch_bounds__(128) shape_finish(ShapeParams P, QuadRule rule) {
+    __shared__ double s_k[4];
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double kloc = 0.0;
+    if (e < P.ne) {
+        Geom g;
+        load_geom(P.g, P.ne, e, 1.0, g);
+        const double nmv = P.nm ? (double)P.nm[e] : 1.0;
+        double di[3][3];
+        cross3(g.j1, g.n, di[1]);
+        cross3(g.n, g.j0, di[2]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) di[0][c] = -(di[1][c] + di[2][c]);
+        double gv[3][3];
+#pragma unroll
+        for (int v = 0; v < 3; ++v) gv[v][0] = gv[v][1] = gv[v][2] = 0.0;
+
+        if (P.scale_op != 0.0) {
+            const double *a = P.acc + e * SH_ACC;
+            const double2 l = P.lam[e], ph = P.phi[e];
+            double go[3][3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                go[0][c] = -(a[c] - a[3 + c] - a[6 + c]);
+                go[1][c] = -a[3 + c];
+                go[2][c] = -a[6 + c];
+            }
+            const double idc = (l.x * ph.x + l.y * ph.y) * P.ident * 0.5;  // identity: A_ee += ident ie_e / 2
+            const double cie = a[9] / g.ie + a[22] + idc;
+            trial_chain(g, di, a + 10, a + 13, a + 16, a + 19, cie, go);
+#pragma unroll
+            for (int v = 0; v < 3; ++v)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) gv[v][c] = P.scale_op * go[v][c];
+            kloc = P.scale_op * a[23];
+        }
+
+        if (P.scale_ff != 0.0 && P.ndir > 0) {
+            // F_je = sum_q w_q / (4 pi) B_j exp(-i k d_j . y_q), B_j = -i k beta (d_j . c) + eta ie
+            const double2 ph = P.phi[e];
+            const double bet = P.ff_beta * nmv;
+            double c_e[3];
+            cross3(g.j0, g.j1, c_e);
+            double yq[SH_NQ][3];
+#pragma unroll
+            for (int q = 0; q < SH_NQ; ++q) to_global(g, rule.x[q], rule.y[q], yq[q]);
+            double T[3] = {0.0, 0.0, 0.0}, X[3] = {0.0, 0.0, 0.0}, Y[3] = {0.0, 0.0, 0.0}, C[3] = {0.0, 0.0, 0.0};
+            double cie = 0.0, kf = 0.0;
+            for (int j = 0; j < P.ndir; ++j) {
+                const double dj[3] = {P.dirs[3 * j], P.dirs[3 * j + 1], P.dirs[3 * j + 2]};
+                const double2 uj = P.u[j];
+                // cj = conj(u_j) phi_e
+                const double cjr = uj.x * ph.x + uj.y * ph.y, cji = uj.x * ph.y - uj.y * ph.x;
+                const double dc = dj[0] * c_e[0] + dj[1] * c_e[1] + dj[2] * c_e[2];
+                const double Br = P.ff_eta_re * g.ie, Bi = fma(-P.k * bet, dc, P.ff_eta_im * g.ie);
+                for (int q = 0; q < rule.nq; ++q) {
+                    const double dy = dj[0] * yq[q][0] + dj[1] * yq[q][1] + dj[2] * yq[q][2];
+                    double sn, cn;
+                    sincos_cw64(P.k * dy, &sn, &cn);  // exp(-i k d.y) = (cn, -sn)
+                    const double f = rule.w[q] * BC_INV_4PI;
+                    const double Vr = (cjr * cn + cji * sn) * f, Vi = (cji * cn - cjr * sn) * f;
+                    const double VBr = Vr * Br - Vi * Bi, VBi = fma(Vr, Bi, Vi * Br);
+                    const double gy = P.k * VBi;
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const double gyc = gy * dj[c];
+                        T[c] += gyc;
+                        X[c] = fma(rule.x[q], gyc, X[c]);
+                        Y[c] = fma(rule.y[q], gyc, Y[c]);
+                        C[c] = fma(P.k * bet * Vi, dj[c], C[c]);
+                    }
+                    cie += Vr * P.ff_eta_re - Vi * P.ff_eta_im;
+                    kf += Vr * P.ff_deta_re * g.ie - Vi * fma(-bet, dc, P.ff_deta_im * g.ie) + dy * VBi;
+                }
+            }
+            double gf[3][3];
+#pragma unroll
+            for (int v = 0; v < 3; ++v) gf[v][0] = gf[v][1] = gf[v][2] = 0.0;
+            trial_chain(g, di, T, X, Y, C, cie, gf);
+#pragma unroll
+            for (int v = 0; v < 3; ++v)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) gv[v][c] = fma(P.scale_ff, gf[v][c], gv[v][c]);
+            kloc = fma(P.scale_ff, kf, kloc);
+        }
+
+        if (P.scale_rhs != 0.0) {
+            // b_e = rho ie sum_p w_p exp(i k d_inc . x_p), contracted with conj(lambda_e)
+            const double2 l = P.lam[e];
+            const double cbr = l.x * P.rhs_re + l.y * P.rhs_im, cbi = l.x * P.rhs_im - l.y * P.rhs_re;
+            double gb[3][3];
+#pragma unroll
+            for (int v = 0; v < 3; ++v) gb[v][0] = gb[v][1] = gb[v][2] = 0.0;
+            double cie = 0.0, kb = 0.0;
+            for (int p = 0; p < rule.nq; ++p) {
+                double x[3];
+                to_global(g, rule.x[p], rule.y[p], x);
+                const double dx = P.inc[0] * x[0] + P.inc[1] * x[1] + P.inc[2] * x[2];
+                double sn, cn;
+                sincos_cw64(P.k * dx, &sn, &cn);
+                const double Er = (cbr * cn - cbi * sn) * rule.w[p], Ei = fma(cbr, sn, cbi * cn) * rule.w[p];
+                cie += Er;
+                const double gx = -P.k * Ei * g.ie;
+                const double nb[3] = {1.0 - rule.x[p] - rule.y[p], rule.x[p], rule.y[p]};
+#pragma unroll
+                for (int v = 0; v < 3; ++v)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) gb[v][c] = fma(nb[v] * gx, P.inc[c], gb[v][c]);
+                kb -= dx * Ei * g.ie;
+            }
+#pragma unroll
+            for (int v = 0; v < 3; ++v)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) gv[v][c] = fma(P.scale_rhs, fma(cie, di[v][c], gb[v][c]), gv[v][c]);
+            kloc = fma(P.scale_rhs, kb, kloc);
+        }
+
+#pragma unroll
+        for (int v = 0; v < 3; ++v) {
+            const int64_t vid = P.el[3 * e + v];
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                if (gv[v][c] != 0.0) atomicAdd(P.vgrad + 3 * vid + c, gv[v][c]);
+        }
+    }
+    kloc = warp_sum(kloc);
+    if ((threadIdx.x & 31) == 0) s_k[threadIdx.x >> 5] = kloc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double v = s_k[0] + s_k[1] + s_k[2] + s_k[3];
+        if (v != 0.0) atomicAdd(P.kgrad, v);
+    }
+}
+
+// F[j, e]: thread per entry, elements fastest (coalesced stores).
+__global__ void __launch_bounds__(128) shape_farfield(ShapeParams P, QuadRule rule) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= P.ne * (int64_t)P.ndir) return;
+    const int64_t j = idx / P.ne, e = idx - j * P.ne;
+    Geom g;
+    load_geom(P.g, P.ne, e, 1.0, g);
+    const double bet = P.ff_beta * (P.nm ? (double)P.nm[e] : 1.0);
+    double c_e[3];
+    cross3(g.j0, g.j1, c_e);
+    const double dj[3] = {P.dirs[3 * j], P.dirs[3 * j + 1], P.dirs[3 * j + 2]};
+    const double dc = dj[0] * c_e[0] + dj[1] * c_e[1] + dj[2] * c_e[2];
+    const double Br = P.ff_eta_re * g.ie, Bi = fma(-P.k * bet, dc, P.ff_eta_im * g.ie);
+    double sr = 0.0, si = 0.0;
+    for (int q = 0; q < rule.nq; ++q) {
+        double y[3];
+        to_global(g, rule.x[q], rule.y[q], y);
+        double sn, cn;
+        sincos_cw64(P.k * (dj[0] * y[0] + dj[1] * y[1] + dj[2] * y[2]), &sn, &cn);
+        sr = fma(rule.w[q], cn, sr);
+        si = fma(-rule.w[q], sn, si);
+    }
+    sr *= BC_INV_4PI;
+    si *= BC_INV_4PI;
+    reinterpret_cast<double2 *>(P.out)[idx] = make_double2(sr * Br - si * Bi, fma(sr, Bi, si * Br));
+}
+
+__global__ void __launch_bounds__(128) shape_plane_wave(ShapeParams P, QuadRule rule) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= P.ne) return;
+    Geom g;
+    load_geom(P.g, P.ne, e, 1.0, g);
+    double sr = 0.0, si = 0.0;
+    for (int p = 0; p < rule.nq; ++p) {
+        double x[3];
+        to_global(g, rule.x[p], rule.y[p], x);
+        double sn, cn;
+        sincos_cw64(P.k * (P.inc[0] * x[0] + P.inc[1] * x[1] + P.inc[2] * x[2]), &sn, &cn);
+        sr = fma(rule.w[p], cn, sr);
+        si = fma(rule.w[p], sn, si);
+    }
+    sr *= g.ie;
+    si *= g.ie;
+    reinterpret_cast<double2 *>(P.out)[e] = make_double2(P.rhs_re * sr - P.rhs_im * si, fma(P.rhs_re, si, P.rhs_im * sr));
+}
+
+}  // namespace bc
+
+using namespace bc;
+
+static bool finite_value(double v) { return v == v && v < 1e300 && v > -1e300; }
+
+static int shape_setup(const bemppcuda_shape_args *a, ShapeParams &P, QuadRule &rule, const char *what) {
+    if (!a) {
+        bc_set_error("%s: null argument struct", what);
+        return BEMPPCUDA_ERR_INVALID;
+    }
+    if (a->grid.nelements <= 0 || a->grid.nvertices <= 0 || !a->grid.geom || !a->grid.elements) {
+        bc_set_error("%s: grid geometry, elements and sizes are required", what);
+        return BEMPPCUDA_ERR_INVALID;
+    }
+    if (a->nq != SH_NQ || !a->quad_points || !a->quad_weights) {
+        bc_set_error("%s: the 6-point regular rule (order 4) is required (got nq = %d)", what, a->nq);
+        return BEMPPCUDA_ERR_INVALID;
+    }
+    const double vals[] = {a->k, a->dlp_coeff, a->eta[0], a->eta[1], a->deta_dk[0], a->deta_dk[1], a->identity,
+                           a->ff_dlp_coeff, a->ff_eta[0], a->ff_eta[1], a->ff_deta_dk[0], a->ff_deta_dk[1],
+                           a->incident[0], a->incident[1], a->incident[2], a->rhs_coeff[0], a->rhs_coeff[1],
+                           a->scale_operator, a->scale_farfield, a->scale_rhs};
+    for (double v : vals)
+        if (!finite_value(v)) {
+            bc_set_error("%s: wavenumber, coefficients and scales must be finite", what);
+            return BEMPPCUDA_ERR_INVALID;
+        }
+    P.g = a->grid.geom;
+    P.ne = a->grid.nelements;
+    P.nv = a->grid.nvertices;
+    P.el = a->grid.elements;
+    P.nm = a->normal_mult;
+    P.k = a->k;
+    P.beta = a->dlp_coeff;
+    P.eta_re = a->eta[0];
+    P.eta_im = a->eta[1];
+    P.deta_re = a->deta_dk[0];
+    P.deta_im = a->deta_dk[1];
+    P.ident = a->identity;
+    P.phi = reinterpret_cast<const double2 *>(a->phi);
+    P.lam = reinterpret_cast<const double2 *>(a->lambda);
+    P.u = reinterpret_cast<const double2 *>(a->u);
+    P.acc = reinterpret_cast<double *>(a->workspace);
+    P.vgrad = a->vertex_grad;
+    P.kgrad = a->k_grad;
+    P.npairs = a->npairs;
+    P.tp = reinterpret_cast<const double2 *>(a->test_points);
+    P.sp = reinterpret_cast<const double2 *>(a->trial_points);
+    P.w = a->weights;
+    P.te = a->test_elements;
+    P.se = a->trial_elements;
+    P.toff = a->test_offsets;
+    P.soff = a->trial_offsets;
+    P.woff = a->weights_offsets;
+    P.npts = a->npoints;
+    P.ndir = a->ndirections;
+    P.pad = 0;
+    P.dirs = a->directions;
+    P.ff_beta = a->ff_dlp_coeff;
+    P.ff_eta_re = a->ff_eta[0];
+    P.ff_eta_im = a->ff_eta[1];
+    P.ff_deta_re = a->ff_deta_dk[0];
+    P.ff_deta_im = a->ff_deta_dk[1];
+    for (int c = 0; c < 3; ++c) P.inc[c] = a->incident[c];
+    P.rhs_re = a->rhs_coeff[0];
+    P.rhs_im = a->rhs_coeff[1];
+    P.scale_op = a->scale_operator;
+    P.scale_ff = a->scale_farfield;
+    P.scale_rhs = a->scale_rhs;
+    P.out = a->out;
+    rule.nq = a->nq;
+    rule.pad = 0;
+    for (int i = 0; i < BEMPPCUDA_MAX_REGULAR_POINTS; ++i) {
+        rule.x[i] = i < a->nq ? a->quad_points[2 * i] : 0.0;
+        rule.y[i] = i < a->nq ? a->quad_points[2 * i + 1] : 0.0;
+        rule.w[i] = i < a->nq ? a->quad_weights[i] : 0.0;
+        rule.wf[i] = (float)rule.w[i];
+    }
+    return BEMPPCUDA_OK;
+}
+
+extern "C" {
+
+int64_t bemppcuda_shape_workspace_bytes(int64_t nelements) {
+    return nelements > 0 ? nelements * SH_ACC * (int64_t)sizeof(double) : 0;
+}
+
+int bemppcuda_farfield_matrix_dp0(const bemppcuda_shape_args *a, void *stream) {
+    ShapeParams P;
+    QuadRule rule;
+    int rc = shape_setup(a, P, rule, "farfield_matrix_dp0");
+    if (rc) return rc;
+    if (P.ndir <= 0 || !P.dirs || !P.out) {
+        bc_set_error("farfield_matrix_dp0: directions and an output of ndirections x nelements are required");
+        return BEMPPCUDA_ERR_INVALID;
+    }
+    const int64_t n = P.ne * (int64_t)P.ndir;
+    shape_farfield<<<(unsigned)((n + 127) / 128), 128, 0, (cudaStream_t)stream>>>(P, rule);
+    return bc_check_launch("farfield_matrix_dp0");
+}
+
+int bemppcuda_plane_wave_dp0(const bemppcuda_shape_args *a, void *stream) {
+    ShapeParams P;
+    QuadRule rule;
+    int rc = shape_setup(a, P, rule, "plane_wave_dp0");
+    if (rc) return rc;
+    if (!P.out) {
+        bc_set_error("plane_wave_dp0: output vector required");
+        return BEMPPCUDA_ERR_INVALID;
+    }
+    shape_plane_wave<<<(unsigned)((P.ne + 127) / 128), 128, 0, (cudaStream_t)stream>>>(P, rule);
+    return bc_check_launch("plane_wave_dp0");
+}
+
+int bemppcuda_shape_adjoint_dp0(const bemppcuda_shape_args *a, void *stream) {
+    ShapeParams P;
+    QuadRule rule;
+    int rc = shape_setup(a, P, rule, "shape_adjoint_dp0");
+    if (rc) return rc;
+    if (!P.vgrad || !P.kgrad) {
+        bc_set_error("shape_adjoint_dp0: vertex_grad and k_grad outputs are required");
+        return BEMPPCUDA_ERR_INVALID;
+    }
+    const bool op = P.scale_op != 0.0, ff = P.scale_ff != 0.0, rhs = P.scale_rhs != 0.0;
+    if ((op && (!P.phi || !P.lam)) || (ff && (!P.phi || !P.u || !P.dirs || P.ndir <= 0)) || (rhs && !P.lam)) {
+        bc_set_error("shape_adjoint_dp0: phi / lambda / u / directions missing for a term with a nonzero scale");
+        return BEMPPCUDA_ERR_INVALID;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    if (op) {
+        const int64_t need = bemppcuda_shape_workspace_bytes(P.ne);
+        if (!P.acc || a->workspace_bytes < need) {
+            bc_set_error("shape_adjoint_dp0: workspace of %lld bytes required (got %lld)", (long long)need,
+                         (long long)a->workspace_bytes);
+            return BEMPPCUDA_ERR_WORKSPACE;
+        }
+        if (P.npairs < 0 || (P.npairs > 0 && (!P.tp || !P.sp || !P.w || !P.te || !P.se || !P.toff || !P.soff ||
+                                              !P.woff || !P.npts))) {
+            bc_set_error("shape_adjoint_dp0: singular pair tables missing");
+            return BEMPPCUDA_ERR_INVALID;
+        }
+        if (cudaMemsetAsync(P.acc, 0, need, st) != cudaSuccess) return bc_check_launch("shape_adjoint_dp0 memset");
+        const int64_t by = (P.ne + SH_TCHUNK * SH_TILES - 1) / (SH_TCHUNK * SH_TILES);
+        if (by > 65535) {
+            bc_set_error("shape_adjoint_dp0: %lld elements exceed the launch grid", (long long)P.ne);
+            return BEMPPCUDA_ERR_UNSUPPORTED;
+        }
+        dim3 grid((unsigned)((P.ne + SH_THREADS - 1) / SH_THREADS), (unsigned)by);
+        shape_regular<<<grid, SH_THREADS, 0, st>>>(P, rule);
+        rc = bc_check_launch("shape_adjoint_dp0 regular pairs");
+        if (rc) return rc;
+        if (P.npairs > 0) {
+            shape_singular<<<(unsigned)((P.npairs + SHS_WARPS - 1) / SHS_WARPS), 32 * SHS_WARPS, 0, st>>>(P);
+            rc = bc_check_launch("shape_adjoint_dp0 singular pairs");
+            if (rc) return rc;
+        }
+    }
+    shape_finish<<<(unsigned)((P.ne + 127) / 128), 128, 0, st>>>(P, rule);
+    return bc_check_launch("shape_adjoint_dp0 element pass");
+}
+
+}  // extern "C"

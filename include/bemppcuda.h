@@ -270,6 +270,82 @@ int bemppcuda_batch_launch(const bemppcuda_batch_args *args, void *stream);
 int bemppcuda_fma_probe(int32_t precision, int64_t iterations, int64_t blocks, void *sink, double *flops,
                         void *stream);
 
+/* Shape derivatives of a DP0 Helmholtz scattering functional.  No single
+   reference counterpart: the reference has no derivatives.  The operator is
+       A = dlp_coeff * DLP + eta * SLP + identity * I        (DP0 x DP0, one grid)
+   assembled by bemppcuda_assemble_regular (kernel BEMPPCUDA_HELMHOLTZ_COMBINED,
+   params (k, 0, eta)) and bemppcuda_assemble_singular (diag_shift = identity);
+   the far-field matrix is
+       F[j, e] = ff_dlp_coeff * DLP_ff(d_j) + ff_eta * SLP_ff(d_j)
+   with the kernels of helmholtz_far_field_{double,single}_layer
+   (bempp_cl/core/numba_kernels.py:402-449); the right-hand side is
+       b[e] = rhs_coeff * int_e exp(i k d_inc . x) dx
+   with the regular rule (GridFunction projection onto DP0).  The wavenumber is
+   real.  Quadrature points are fixed in reference coordinates, so the
+   derivatives are exact derivatives of the discrete quantities. */
+typedef struct {
+    bemppcuda_grid grid;               /* geometry record of the (deformed) grid + elements */
+    const int32_t *normal_mult;        /* (nelements,) DP0 normal multipliers; NULL means all +1 */
+    double k;                          /* real wavenumber */
+    double dlp_coeff;                  /* operator coefficients */
+    double eta[2];
+    double deta_dk[2];                 /* d eta / d k, e.g. -i for eta = -i k */
+    double identity;
+    int32_t nq;                        /* regular rule (6 points, order 4) */
+    int32_t ndirections;               /* far-field directions */
+    const double *quad_points;         /* HOST (nq, 2) */
+    const double *quad_weights;        /* HOST (nq,) */
+    /* Sauter-Schwab pairs of the DP0 space: every pair of elements sharing a vertex */
+    int64_t npairs;
+    const double *test_points;         /* (P, 2) */
+    const double *trial_points;        /* (P, 2) */
+    const double *weights;             /* (W,) */
+    const int32_t *test_elements;      /* (npairs,) */
+    const int32_t *trial_elements;
+    const int32_t *test_offsets;
+    const int32_t *trial_offsets;
+    const int32_t *weights_offsets;
+    const int32_t *npoints;
+    /* far field */
+    const double *directions;          /* (ndirections, 3) unit vectors */
+    double ff_dlp_coeff;
+    double ff_eta[2];
+    double ff_deta_dk[2];
+    /* right-hand side */
+    double incident[3];                /* d_inc */
+    double rhs_coeff[2];
+    /* complex128 vectors */
+    const void *phi;                   /* (nelements,) solution of A phi = b */
+    const void *lambda;                /* (nelements,) adjoint solution of A^H lambda = F^H u */
+    const void *u;                     /* (ndirections,) far field u = F phi */
+    /* gradient contributions, each added with its scale:
+         scale_operator * Re(lambda^H dA phi) + scale_farfield * Re(u^H dF phi)
+       + scale_rhs * Re(lambda^H db) */
+    double scale_operator;
+    double scale_farfield;
+    double scale_rhs;
+    double *vertex_grad;               /* (nvertices, 3) accumulated (+=) */
+    double *k_grad;                    /* (1,) accumulated (+=) */
+    void *out;                         /* forward outputs: F (ndirections, nelements) row-major or b (nelements,) */
+    void *workspace;                   /* >= bemppcuda_shape_workspace_bytes(nelements) */
+    int64_t workspace_bytes;
+} bemppcuda_shape_args;
+
+int64_t bemppcuda_shape_workspace_bytes(int64_t nelements);
+
+/* F[j, e] into args->out (complex128, ndirections x nelements). */
+int bemppcuda_farfield_matrix_dp0(const bemppcuda_shape_args *args, void *stream);
+
+/* b[e] into args->out (complex128, nelements). */
+int bemppcuda_plane_wave_dp0(const bemppcuda_shape_args *args, void *stream);
+
+/* Adds the vertex and wavenumber gradients of the three contractions above.
+   The operator part never forms dA/dx: one pass over every regular element
+   pair (quadrature recomputed, per-element partial sums in the workspace)
+   and one over the singular pairs, then one per-element pass that applies
+   the geometry chain rule and adds the far-field and right-hand-side terms. */
+int bemppcuda_shape_adjoint_dp0(const bemppcuda_shape_args *args, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
