@@ -19,6 +19,10 @@ pairs + Sauter-Schwab singular pairs + identity), matrix resident in HBM.
   same run by ``bemppcuda_fma_probe``.
 * ``cpu_baseline``: the oracle (a C/OpenMP restatement of the reference Numba
   kernels) on a bounded row sample of the same operator, all host cores.
+* ``shape_gradient``: gradients/s of the far-field objective of a perturbed
+  L5 sphere (k = 6) with respect to all vertex coordinates and k, with the
+  adjoint-kernel cost relative to one forward assembly and a central
+  difference check on 20 coordinates.
 * ``batch``: 64 DP0 Helmholtz single-layer problems on seeded ellipsoids
   (regular_sphere(3..5) scaled per axis, k ~ U[1, 16]) assembled in one
   persistent launch per precision after autotuning, then replayed as a CUDA
@@ -68,6 +72,9 @@ def parse():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-solve", action="store_true")
     ap.add_argument("--skip-batch", action="store_true")
+    ap.add_argument("--skip-shape", action="store_true")
+    ap.add_argument("--skip-fd", action="store_true")
+    ap.add_argument("--shape-level", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time per baseline sample")
     return ap.parse_args()
 
@@ -317,6 +324,10 @@ def gpu_arm(args, world, rank, local):
         del out
         torch.cuda.empty_cache()
         batch = batch_measure(args, torch, world, rank, dist)
+    shape = None
+    if not args.skip_shape and world == 1:
+        torch.cuda.empty_cache()
+        shape = shape_measure(args, torch)
 
     line = {
         "metric": "entries/s Helmholtz assembly, mixed vs FP64 GPU at rel err <=1e-6; shape-grads/s",
@@ -354,6 +365,8 @@ def gpu_arm(args, world, rank, local):
         line["solve"] = solve
     if batch is not None:
         line["batch"] = batch
+    if shape is not None:
+        line["shape_gradient"] = shape
     return line
 
 
@@ -495,6 +508,95 @@ def batch_measure(args, torch, world, rank, dist):
     res["mixed_over_fp64"] = res["mixed"]["entries_per_s"] / res["fp64"]["entries_per_s"]
     del singles
     torch.cuda.empty_cache()
+    return res
+
+
+def shape_measure(args, torch):
+    """Shape gradient of J = sum_j |u_inf(d_j)|^2 (32 Fibonacci directions) on a perturbed L5 sphere, k = 6.
+
+    One step = forward (device geometry, combined-field assembly, LU, solve,
+    far field, J) + backward (adjoint solve, adjoint kernels).  The adjoint
+    kernels are compared with one forward assembly (regular + singular pass).
+    Central differences (h = 1e-6) on 20 seeded coordinates and on k check
+    the gradient at this size.
+    """
+    from bempp_cuda.shape_gradient import FarFieldObjective
+    from bempp_cuda.shapes import perturbed_sphere
+
+    grid, _ = perturbed_sphere(args.shape_level, seed=0)
+    obj = FarFieldObjective(grid)
+    k = 6.0
+    x0 = obj.vertices.clone()
+    names = ("geometry", "assembly", "lu", "solve_farfield", "adjoint_solve", "adjoint_kernels")
+
+    def step(ev=None):
+        def mark(i):
+            if ev is not None:
+                ev[i].record()
+        mark(0)
+        geo = obj.geometry(x0)
+        mark(1)
+        a = obj.assemble(geo, k)
+        mark(2)
+        lu, piv = torch.linalg.lu_factor(a)
+        mark(3)
+        del a
+        b = obj.rhs(geo, k)
+        phi = torch.linalg.lu_solve(lu, piv, b.unsqueeze(1)).squeeze(1)
+        ff = obj.farfield_matrix(geo, k)
+        u = ff @ phi
+        value = (u.real ** 2 + u.imag ** 2).sum()
+        mark(4)
+        from bempp_cuda.shape_gradient import ScatteringState
+
+        state = ScatteringState(geo, lu, piv, phi, u, ff)
+        lam = obj.adjoint(state)
+        mark(5)
+        vgrad, kgrad = obj.gradient(state, k, lam=lam)
+        mark(6)
+        return value, vgrad, kgrad
+
+    for _ in range(max(args.warmup, 1)):
+        step()
+    torch.cuda.synchronize()
+    steps = max(args.steps, 1)
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(7)] for _ in range(steps)]
+    t0 = time.perf_counter()
+    for s in range(steps):
+        value, vgrad, kgrad = step(evs[s])
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - t0) / steps
+    parts = {n: float(np.mean([evs[s][i].elapsed_time(evs[s][i + 1]) for s in range(steps)]))
+             for i, n in enumerate(names)}
+    device_ms = evs[0][0].elapsed_time(evs[-1][6]) / steps
+    res = {"workload": "perturbed regular_sphere(%d) (%d elements, %d vertices), k=6, DP0 combined field, "
+                       "32 Fibonacci far-field directions, incident exp(i k z)"
+                       % (args.shape_level, grid.number_of_elements, obj.base.nvertices),
+           "shape_grads_per_s": 1e3 / max(device_ms, wall * 1e3),
+           "ms_per_gradient": max(device_ms, wall * 1e3), "parts_ms": parts,
+           "adjoint_kernels_over_forward_assembly": parts["adjoint_kernels"] / parts["assembly"],
+           "backward_over_forward": (parts["adjoint_solve"] + parts["adjoint_kernels"])
+           / (parts["geometry"] + parts["assembly"] + parts["lu"] + parts["solve_farfield"]),
+           "J": float(value.item())}
+    if not args.skip_fd:
+        h = 1e-6
+        rng = np.random.default_rng(7)
+        flat = rng.choice(obj.base.nvertices * 3, size=20, replace=False)
+        fd, ad = [], []
+        for f in flat:
+            v, c = int(f) // 3, int(f) % 3
+            xp = x0.clone()
+            xm = x0.clone()
+            xp[v, c] += h
+            xm[v, c] -= h
+            fd.append((obj.evaluate(xp, k).item() - obj.evaluate(xm, k).item()) / (2 * h))
+            ad.append(vgrad[v, c].item())
+        fd = np.array(fd)
+        ad = np.array(ad)
+        fdk = (obj.evaluate(x0, k + h).item() - obj.evaluate(x0, k - h).item()) / (2 * h)
+        res["fd_check"] = {"h": h, "coordinates": 20, "rel_err_norm": float(np.linalg.norm(ad - fd) / np.linalg.norm(fd)),
+                           "max_rel_err": float(np.max(np.abs(ad - fd) / np.abs(fd))),
+                           "k_rel_err": float(abs(kgrad.item() - fdk) / abs(fdk))}
     return res
 
 
