@@ -32,6 +32,7 @@ constexpr size_t kCounterBytes = 256;
 union TileShared {
     TestBlock64 b64;
     TestBlock32 b32;
+    TestBlock32p b32p;
 };
 
 template <int K>
@@ -51,12 +52,14 @@ __device__ __forceinline__ void run_tile(const BatchDev &P, const QuadRule &rule
     } else {
         if (P.ck)
             regular_dp0_mixed_tile<K, true, 0>(P.prm, rule, tx, t0, rows, sh.b32);
+        else if (!(P.prm.p[0] > 0.0))  // the packed path needs k > 0
+            regular_dp0_mixed_tile<K, false, 0>(P.prm, rule, tx, t0, rows, sh.b32);
         else if (P.phase_class == 2)
-            regular_dp0_mixed2_tile<K, 2>(P.prm, rule, tx, t0, rows, sh.b32);
+            regular_dp0_mixed2_tile<K, 2>(P.prm, rule, tx, t0, rows, sh.b32p);
         else if (P.phase_class == 1)
-            regular_dp0_mixed2_tile<K, 1>(P.prm, rule, tx, t0, rows, sh.b32);
+            regular_dp0_mixed2_tile<K, 1>(P.prm, rule, tx, t0, rows, sh.b32p);
         else
-            regular_dp0_mixed2_tile<K, 0>(P.prm, rule, tx, t0, rows, sh.b32);
+            regular_dp0_mixed2_tile<K, 0>(P.prm, rule, tx, t0, rows, sh.b32p);
     }
 }
 

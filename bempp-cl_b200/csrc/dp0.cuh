@@ -482,11 +482,35 @@ __device__ __forceinline__ void sincos2(float2 x, float2 *s, float2 *c) {
     }
 }
 
+// Test block of the packed path: per test point m = -2 kappa (x_p - c_t) and
+// |kappa (x_p - c_t)|^2, with kappa = k (Helmholtz) or 1 (Laplace).
+struct TestBlock32p {
+    float4 m[DP0_TCHUNK][NQ6];
+    double c[DP0_TCHUNK][3];  // centroid
+    float n[DP0_TCHUNK][3];
+    double ie[DP0_TCHUNK];
+    int v[DP0_TCHUNK][3];
+};
+
+// Lengths are measured in units of 1/k (kappa = k > 0, Laplace kappa = 1):
+// with primes for scaled quantities r' = k r, the phase offset is
+// theta = r' - r_c' with no multiplication by k, and
+//   e^{ikr}/r          = k e^{i theta'} / r',
+//   (ikr - 1)(d.n)/r^3 = k^2 (i r' - 1)(d'.n) / r'^3,
+// so per quadrature-point pair (f = w_q / r', g1 = f (d'.n) / r', g0 = g1 / r')
+//   SLP part: sum f (cos, sin)
+//   DLP part: (i r' - 1) g0 (cos + i sin) = -(g0 cos + g1 sin) + i (g1 cos - g0 sin),
+// accumulated as four packed sums.  The FP32 sums run over the test points of
+// one quadrature weight (the order-4 rule has two orbits of three points) and
+// are then added in FP64 with that weight; kappa, eta and the centroid phase
+// exp(i k r_c) are applied per entry in FP64.
 template <int K, int PHC>
 __device__ __forceinline__ void regular_dp0_mixed2_tile(const RegParams &prm, const QuadRule &rule,
-                                                    int64_t tile_x, int64_t t0, int rows, TestBlock32 &sb) {
+                                                    int64_t tile_x, int64_t t0, int rows, TestBlock32p &sb) {
     using T = KernelTraits<K>;
     constexpr int NP = NQ6 / 2;
+    constexpr bool DL = T::normal;  // double-layer type (DLP, ADLP, combined)
+    const double kap = T::helm ? prm.p[0] : 1.0;  // callers guarantee k > 0 for the Helmholtz family
     // rows <= DP0_TCHUNK test elements starting at t0
     const int tcount = (int)min((int64_t)rows, prm.ntest - t0);
     for (int idx = threadIdx.x; idx < tcount; idx += blockDim.x) {
@@ -499,8 +523,9 @@ __device__ __forceinline__ void regular_dp0_mixed2_tile(const RegParams &prm, co
         for (int p = 0; p < NQ6; ++p) {
             double x[3];
             to_global(g, rule.x[p], rule.y[p], x);
-            const float o0 = (float)(x[0] - c[0]), o1 = (float)(x[1] - c[1]), o2 = (float)(x[2] - c[2]);
-            sb.o[idx][p] = make_float4(o0, o1, o2, fmaf(o2, o2, fmaf(o1, o1, o0 * o0)));
+            const float o0 = (float)(kap * (x[0] - c[0])), o1 = (float)(kap * (x[1] - c[1])),
+                        o2 = (float)(kap * (x[2] - c[2]));
+            sb.m[idx][p] = make_float4(-2.f * o0, -2.f * o1, -2.f * o2, fmaf(o2, o2, fmaf(o1, o1, o0 * o0)));
         }
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
@@ -521,7 +546,7 @@ __device__ __forceinline__ void regular_dp0_mixed2_tile(const RegParams &prm, co
     double sc[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) sc[d] = __ldg(prm.sg + (22 + d) * prm.sne + s);
-    // trial point offsets, packed by pairs of quadrature points
+    // scaled trial point offsets, packed by pairs of quadrature points
     float2 yx[NP], yyy[NP], yz[NP], yy2[NP], yn2[NP], wq2[NP];
     const float sn0 = (float)gs.n[0], sn1 = (float)gs.n[1], sn2 = (float)gs.n[2];
 #pragma unroll
@@ -532,7 +557,7 @@ __device__ __forceinline__ void regular_dp0_mixed2_tile(const RegParams &prm, co
             double v[3];
             to_global(gs, rule.x[2 * j + h], rule.y[2 * j + h], v);
 #pragma unroll
-            for (int d = 0; d < 3; ++d) o[h][d] = (float)(v[d] - sc[d]);
+            for (int d = 0; d < 3; ++d) o[h][d] = (float)(kap * (v[d] - sc[d]));
         }
         yx[j] = f2(o[0][0], o[1][0]);
         yyy[j] = f2(o[0][1], o[1][1]);
@@ -541,104 +566,122 @@ __device__ __forceinline__ void regular_dp0_mixed2_tile(const RegParams &prm, co
         yn2[j] = fma2(yz[j], b2(sn2), fma2(yyy[j], b2(sn1), mul2(yx[j], b2(sn0))));
         wq2[j] = f2(rule.wf[2 * j], rule.wf[2 * j + 1]);
     }
-    const double kr = prm.p[0];
-    const float2 k2 = b2((float)kr);
-    const float etar_s = (float)prm.p[2], etai_s = (float)prm.p[3];
+    // per-entry factors: kappa eta (SLP part; eta = 1 for a single layer), kappa^2 (DLP part)
+    const double ek_r = (K == BEMPPCUDA_HELMHOLTZ_COMBINED) ? kap * prm.p[2] : kap;
+    const double ek_i = (K == BEMPPCUDA_HELMHOLTZ_COMBINED) ? kap * prm.p[3] : 0.0;
+    const double k2d = kap * kap;
 
     for (int tt = 0; tt < tcount; ++tt) {
         const int64_t row = t0 + tt;
         const bool adj = prm.grids_identical && shares_vertex(sb.v[tt], sv0, sv1, sv2);
         double acc_re = 0.0, acc_im = 0.0;
         if (!adj) {
-            const double D0 = sc[0] - sb.c[tt][0], D1 = sc[1] - sb.c[tt][1], D2 = sc[2] - sb.c[tt][2];
+            const double D0 = kap * (sc[0] - sb.c[tt][0]), D1 = kap * (sc[1] - sb.c[tt][1]),
+                         D2 = kap * (sc[2] - sb.c[tt][2]);
             const double rc2 = fma(D2, D2, fma(D1, D1, D0 * D0));
             const double rc = sqrt(rc2);
             double ph_s = 0.0, ph_c = 1.0;
-            if (T::helm) sincos_cw64(kr * rc, &ph_s, &ph_c);
+            if (T::helm) sincos_cw64(rc, &ph_s, &ph_c);
             const float D0f = (float)D0, D1f = (float)D1, D2f = (float)D2;
             const float2 rcf2 = b2((float)rc), rc2f2 = b2((float)rc2);
-            float nx0 = sn0, nx1 = sn1, nx2 = sn2;
+            // dotv' = k (y - x).n_s (DLP) or -k (y - x).n_t (ADLP) = cp_p + ynq_q
+            float nh0 = 0.f, nh1 = 0.f, nh2 = 0.f, Dn = 0.f;
             float2 ynq[NP];
-            if (T::adjoint) {
-                nx0 = sb.n[tt][0];
-                nx1 = sb.n[tt][1];
-                nx2 = sb.n[tt][2];
+            if (DL) {
+                if (T::adjoint) {
+                    const float nx0 = sb.n[tt][0], nx1 = sb.n[tt][1], nx2 = sb.n[tt][2];
 #pragma unroll
-                for (int j = 0; j < NP; ++j)
-                    ynq[j] = mul2(b2(-1.f), fma2(yz[j], b2(nx2), fma2(yyy[j], b2(nx1), mul2(yx[j], b2(nx0)))));
-            } else {
+                    for (int j = 0; j < NP; ++j)
+                        ynq[j] = fma2(yz[j], b2(-nx2), fma2(yyy[j], b2(-nx1), mul2(yx[j], b2(-nx0))));
+                    Dn = -fmaf(D2f, nx2, fmaf(D1f, nx1, D0f * nx0));
+                    nh0 = -0.5f * nx0;
+                    nh1 = -0.5f * nx1;
+                    nh2 = -0.5f * nx2;
+                } else {
 #pragma unroll
-                for (int j = 0; j < NP; ++j) ynq[j] = yn2[j];
+                    for (int j = 0; j < NP; ++j) ynq[j] = yn2[j];
+                    Dn = fmaf(D2f, sn2, fmaf(D1f, sn1, D0f * sn0));
+                    nh0 = 0.5f * sn0;
+                    nh1 = 0.5f * sn1;
+                    nh2 = 0.5f * sn2;
+                }
             }
-            const float Dn = fmaf(D2f, nx2, fmaf(D1f, nx1, D0f * nx0));
             const float2 D0d = b2(2.f * D0f), D1d = b2(2.f * D1f), D2d = b2(2.f * D2f);
             float2 A[NP];
 #pragma unroll
             for (int j = 0; j < NP; ++j) A[j] = fma2(D2d, yz[j], fma2(D1d, yyy[j], fma2(D0d, yx[j], yy2[j])));
-            double a64r = 0.0, a64i = 0.0;
+            double er = 0.0, ei = 0.0;
+            float2 s0r = b2(0.f), s0i = b2(0.f), P = b2(0.f), Q = b2(0.f), R = b2(0.f), S = b2(0.f);
             for (int p = 0; p < NQ6; ++p) {
-                const float4 o = sb.o[tt][p];
-                const float Bp = fmaf(-2.f, fmaf(D2f, o.z, fmaf(D1f, o.y, D0f * o.x)), o.w);
-                const float cp = Dn - fmaf(o.z, nx2, fmaf(o.y, nx1, o.x * nx0));
-                const float2 ox = b2(-2.f * o.x), oy = b2(-2.f * o.y), oz = b2(-2.f * o.z), Bp2 = b2(Bp);
-                const float2 cp2 = b2(T::adjoint ? -cp : cp);
-                // s0 = sum f e^{i theta} (single-layer part), s1 = sum f v (i k - 1/r) e^{i theta}
-                float2 s0r = b2(0.f), s0i = b2(0.f), s1r = b2(0.f), s1i = b2(0.f);
+                const float4 m = sb.m[tt][p];
+                // r'^2 - r_c'^2 = A_q + B_p - 2 yo'_q . o'_p,  B_p = |o'_p|^2 - 2 D'.o'_p
+                const float Bp = fmaf(D2f, m.z, fmaf(D1f, m.y, fmaf(D0f, m.x, m.w)));
+                const float2 mx = b2(m.x), my = b2(m.y), mz = b2(m.z), Bp2 = b2(Bp);
+                float2 cp2 = b2(0.f);
+                if (DL) cp2 = b2(fmaf(m.z, nh2, fmaf(m.y, nh1, fmaf(m.x, nh0, Dn))));
 #pragma unroll
                 for (int j = 0; j < NP; ++j) {
-                    // r^2 - r_c^2 = A_q + B_p - 2 yo_q . o_p
-                    const float2 sdot = fma2(yz[j], oz, fma2(yyy[j], oy, fma2(yx[j], ox, add2(A[j], Bp2))));
+                    const float2 sdot = fma2(yz[j], mz, fma2(yyy[j], my, fma2(yx[j], mx, add2(A[j], Bp2))));
                     const float2 r2 = add2(rc2f2, sdot);
                     const float2 rinv = f2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
-                    const float2 den = fma2(r2, rinv, rcf2);
-                    const float2 delta = mul2(sdot, f2(rcp_approx(den.x), rcp_approx(den.y)));
                     const float2 f = mul2(wq2[j], rinv);
-                    float2 dotv = b2(0.f);
-                    if (T::normal) dotv = add2(cp2, ynq[j]);  // adjoint sign folded into cp2 / ynq
                     if (K == BEMPPCUDA_LAPLACE_SLP) {
                         s0r = add2(f, s0r);
                     } else if (K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_LAPLACE_ADLP) {
-                        s1r = fma2(mul2(f, dotv), mul2(rinv, rinv), s1r);
+                        const float2 g1 = mul2(mul2(f, add2(cp2, ynq[j])), rinv);
+                        P = fma2(g1, rinv, P);
                     } else {
+                        const float2 den = fma2(r2, rinv, rcf2);
+                        const float2 th = mul2(sdot, f2(rcp_approx(den.x), rcp_approx(den.y)));
                         float2 sn, cs;
-                        sincos2<PHC>(mul2(k2, delta), &sn, &cs);
+                        sincos2<PHC>(th, &sn, &cs);
                         if (K == BEMPPCUDA_HELMHOLTZ_SLP || K == BEMPPCUDA_HELMHOLTZ_COMBINED) {
                             s0r = fma2(f, cs, s0r);
                             s0i = fma2(f, sn, s0i);
                         }
-                        if (K != BEMPPCUDA_HELMHOLTZ_SLP) {
-                            const float2 g = mul2(f, mul2(dotv, rinv));
-                            const float2 h1 = fma2(rinv, cs, mul2(k2, sn));
-                            const float2 h2 = fma2(k2, cs, mul2(rinv, mul2(sn, b2(-1.f))));
-                            s1r = fma2(g, h1, s1r);  // sign of -g h1 applied per test point
-                            s1i = fma2(g, h2, s1i);
+                        if (DL) {
+                            const float2 g1 = mul2(mul2(f, add2(cp2, ynq[j])), rinv);
+                            const float2 g0 = mul2(g1, rinv);
+                            P = fma2(g0, cs, P);
+                            Q = fma2(g1, sn, Q);
+                            R = fma2(g1, cs, R);
+                            S = fma2(g0, sn, S);
                         }
                     }
                 }
-                // combine: eta * s0 - s1r + i s1i  (Laplace DLP: -s1r; SLP: s0)
-                float sr, sim;
-                {
-                    const float a0 = s0r.x + s0r.y, b0 = s0i.x + s0i.y, a1 = s1r.x + s1r.y, b1 = s1i.x + s1i.y;
-                    if (K == BEMPPCUDA_LAPLACE_SLP || K == BEMPPCUDA_HELMHOLTZ_SLP) {
-                        sr = a0;
-                        sim = b0;
+                // flush the FP32 sums where the test-point weight changes:
+                // entry += w_p [kappa eta S0 + kappa^2 (-(P + Q) + i (R - S))]
+                if (p == NQ6 - 1 || rule.w[p + 1] != rule.w[p]) {
+                    const double wp = rule.w[p];
+                    if (K == BEMPPCUDA_LAPLACE_SLP) {
+                        er = fma(wp, (double)(s0r.x + s0r.y), er);
+                        s0r = b2(0.f);
                     } else if (K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_LAPLACE_ADLP) {
-                        sr = -a1;
-                        sim = 0.f;
-                    } else if (K == BEMPPCUDA_HELMHOLTZ_COMBINED) {
-                        sr = fmaf(etar_s, a0, fmaf(-etai_s, b0, -a1));
-                        sim = fmaf(etar_s, b0, fmaf(etai_s, a0, b1));
+                        er = fma(-wp, (double)(P.x + P.y), er);
+                        P = b2(0.f);
                     } else {
-                        sr = -a1;
-                        sim = b1;
+                        double vr = 0.0, vi = 0.0;
+                        if (K == BEMPPCUDA_HELMHOLTZ_SLP || K == BEMPPCUDA_HELMHOLTZ_COMBINED) {
+                            const double sr = (double)(s0r.x + s0r.y), sim = (double)(s0i.x + s0i.y);
+                            vr = fma(ek_r, sr, -ek_i * sim);
+                            vi = fma(ek_r, sim, ek_i * sr);
+                            s0r = s0i = b2(0.f);
+                        }
+                        if (DL) {
+                            const float2 pq = add2(P, Q);
+                            const float2 rs = fma2(S, b2(-1.f), R);
+                            vr = fma(-k2d, (double)(pq.x + pq.y), vr);
+                            vi = fma(k2d, (double)(rs.x + rs.y), vi);
+                            P = Q = R = S = b2(0.f);
+                        }
+                        er = fma(wp, vr, er);
+                        ei = fma(wp, vi, ei);
                     }
                 }
-                a64r = fma(rule.w[p], (double)sr, a64r);
-                a64i = fma(rule.w[p], (double)sim, a64i);
             }
             const double scale = BC_INV_4PI * sb.ie[tt] * gs.ie;
-            acc_re = (a64r * ph_c - a64i * ph_s) * scale;
-            acc_im = (a64r * ph_s + a64i * ph_c) * scale;
+            acc_re = (er * ph_c - ei * ph_s) * scale;
+            acc_im = (er * ph_s + ei * ph_c) * scale;
         }
         store_entry(prm, row, si, adj, acc_re, acc_im);
     }
@@ -646,9 +689,13 @@ __device__ __forceinline__ void regular_dp0_mixed2_tile(const RegParams &prm, co
     __syncthreads();  // the shared block is reused by the next tile of a persistent loop
 }
 
+#ifndef BC_MIXED2_MIN_BLOCKS
+#define BC_MIXED2_MIN_BLOCKS 4
+#endif
+
 template <int K, int PHC>
-__global__ void __launch_bounds__(DP0_THREADS, 5) regular_dp0_mixed2(RegParams prm, QuadRule rule) {
-    __shared__ TestBlock32 sb;
+__global__ void __launch_bounds__(DP0_THREADS, BC_MIXED2_MIN_BLOCKS) regular_dp0_mixed2(RegParams prm, QuadRule rule) {
+    __shared__ TestBlock32p sb;
     regular_dp0_mixed2_tile<K, PHC>(prm, rule, blockIdx.x, (int64_t)blockIdx.y * DP0_TCHUNK, DP0_TCHUNK, sb);
 }
 

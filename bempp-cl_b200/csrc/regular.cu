@@ -231,8 +231,10 @@ static cudaError_t launch_dp0(const RegParams &prm, const QuadRule &rule, int mi
                               cudaStream_t st) {
     dim3 grid((unsigned)((prm.ntrial + DP0_THREADS - 1) / DP0_THREADS), (unsigned)((prm.ntest + DP0_TCHUNK - 1) / DP0_TCHUNK));
     const bool ck = prm.p[1] != 0.0 && KernelTraits<K>::helm;
+    // the packed path measures lengths in units of 1/k: Helmholtz needs k > 0
+    const bool packed = !KernelTraits<K>::helm || prm.p[0] > 0.0;
     if constexpr (!KernelTraits<K>::modhelm) {
-        if (mixed && !ck) {
+        if (mixed && !ck && packed) {
             if (phase_class == 2)
                 regular_dp0_mixed2<K, 2><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
             else if (phase_class == 1)

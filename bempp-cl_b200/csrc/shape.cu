@@ -386,7 +386,7 @@ __global__ void __launch_bounds__(128) shape_finish(ShapeParams P, QuadRule rule
                     sincos_cw64(P.k * dy, &sn, &cn);  // exp(-i k d.y) = (cn, -sn)
                     const double f = rule.w[q] * BC_INV_4PI;
                     const double Vr = (cjr * cn + cji * sn) * f, Vi = (cji * cn - cjr * sn) * f;
-                    const double VBr = Vr * Br - Vi * Bi, VBi = fma(Vr, Bi, Vi * Br);
+                    const double VBi = fma(Vr, Bi, Vi * Br);  // Im(V B)
                     const double gy = P.k * VBi;
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
