@@ -98,7 +98,7 @@ class RegularArgs(_ct.Structure):
         ("result", _vp),
         ("ld", _i64),
         ("overwrite", _i32),
-        ("pad", _i32),
+        ("no_symmetry", _i32),
         ("phase_radius", _ct.c_double),
     ]
 

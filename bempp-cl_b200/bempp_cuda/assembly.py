@@ -76,13 +76,16 @@ def _grids_identical(domain, dual_to_range):
 
 def regular_into(
     result, descriptor, domain, dual_to_range, parameters, precision=_lib.FP64, overwrite=False, stream=None,
-    geometry=None,
+    geometry=None, symmetric=True,
 ):
     """Add (or with ``overwrite`` store) the regular part into the device tensor ``result``.
 
     ``geometry`` (a DeviceGrid-like object with ``record()`` and ``radius``)
     replaces the device geometry of both grids, e.g. a grid whose vertices
-    moved while its elements stayed the same.
+    moved while its elements stayed the same.  With ``symmetric`` (default)
+    the library computes A_ij and A_ji from one sweep when both spaces are the
+    same DP0 space of one grid; ``symmetric=False`` evaluates every entry on
+    its own.
     """
     require_cuda()
     kernel, assembly = kernel_ids(descriptor)
@@ -108,6 +111,7 @@ def regular_into(
     args.result = ptr(result)
     args.ld = result.stride(0)
     args.overwrite = 1 if overwrite else 0
+    args.no_symmetry = 0 if symmetric else 1
     # a little slack over the exact bound keeps rounding of the radii on the safe side
     args.phase_radius = 1.0001 * (tgrid.radius + sgrid.radius)
     _lib.check(_lib.load().bemppcuda_assemble_regular(args, stream or current_stream()))

@@ -1,0 +1,418 @@
+// Symmetric DP0 tiles: test and trial are the same DP0 space on one grid, so
+// the element pair (i, j) and its transpose (j, i) use the same quadrature
+// points with the roles of x and y exchanged.  One sweep over the 36 point
+// pairs of (i, j), i < j, gives both entries:
+//   single layer      A_ij = A_ji            (the kernel is symmetric in x, y)
+//   double layer      A_ij with (y - x).n_j, A_ji with (x - y).n_i
+//   adjoint double    the double-layer pair with the two entries exchanged
+//   combined field    double layer + eta * the shared single layer
+// so r, 1/r and exp(ikr) are evaluated once per point pair for two entries.
+// A launch covers the tiles on or above the diagonal (row chunk <= column
+// block); inside a diagonal tile only i <= j is processed, and i == j (the
+// coincident pair, always adjacent) is zeroed for the singular pass.
+// Entry (i, j) is stored by the thread of column j (coalesced); entry (j, i)
+// lands in row j (one 8- or 16-byte store per row, merged in L2 with the
+// stores of neighbouring rows of the same warp).
+#pragma once
+
+#include "dp0.cuh"
+
+namespace bc {
+
+template <int K>
+struct SymTraits {
+    static constexpr bool slp_part = (K == BEMPPCUDA_LAPLACE_SLP || K == BEMPPCUDA_HELMHOLTZ_SLP ||
+                                      K == BEMPPCUDA_HELMHOLTZ_COMBINED);
+    static constexpr bool dlp_part = (K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_LAPLACE_ADLP ||
+                                      K == BEMPPCUDA_HELMHOLTZ_DLP || K == BEMPPCUDA_HELMHOLTZ_ADLP ||
+                                      K == BEMPPCUDA_HELMHOLTZ_COMBINED);
+    static constexpr bool swap = (K == BEMPPCUDA_LAPLACE_ADLP || K == BEMPPCUDA_HELMHOLTZ_ADLP);
+    static constexpr bool helm = KernelTraits<K>::helm;
+    static constexpr bool supported = slp_part || dlp_part;
+};
+
+struct TestBlock64s {
+    double x[DP0_TCHUNK][NQ6][3];
+    double xn[DP0_TCHUNK][NQ6];  // (x_p - c_i).n_i: zero up to rounding, kept as the plain path keeps it
+    double c[DP0_TCHUNK][3];
+    double n[DP0_TCHUNK][3];
+    double ie[DP0_TCHUNK];
+    int v[DP0_TCHUNK][3];
+};
+
+// FP64, real wavenumber.  PHC as in regular_dp0_fp64_tile.
+template <int K, int PHC>
+__device__ __forceinline__ void regular_dp0_fp64_sym_tile(const RegParams &prm, const QuadRule &rule,
+                                                        int64_t tile_x, int64_t t0, int rows, TestBlock64s &sb) {
+    using ST = SymTraits<K>;
+    constexpr bool PH = PHC > 0 && ST::helm;
+    const int tcount = (int)min((int64_t)rows, prm.ntest - t0);
+    for (int idx = threadIdx.x; idx < tcount; idx += blockDim.x) {
+        const int64_t t = prm.tsup[t0 + idx];
+        Geom g;
+        load_geom(prm.tg, prm.tne, t, prm.tnm ? (double)prm.tnm[t] : 1.0, g);
+        double c[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) c[d] = __ldg(prm.tg + (22 + d) * prm.tne + t);
+        for (int p = 0; p < NQ6; ++p) {
+            double x[3];
+            to_global(g, rule.x[p], rule.y[p], x);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) sb.x[idx][p][d] = x[d];
+            sb.xn[idx][p] = fma(x[2] - c[2], g.n[2], fma(x[1] - c[1], g.n[1], (x[0] - c[0]) * g.n[0]));
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            sb.n[idx][d] = g.n[d];
+            sb.c[idx][d] = c[d];
+            sb.v[idx][d] = __ldg(prm.tel + 3 * t + d);
+        }
+        sb.ie[idx] = g.ie;
+    }
+    __syncthreads();
+
+    const int64_t si = tile_x * DP0_THREADS + threadIdx.x;
+    if (si < prm.ntrial && t0 <= si) {
+    const int64_t s = prm.ssup[si];
+    Geom gs;
+    load_geom(prm.sg, prm.sne, s, prm.snm ? (double)prm.snm[s] : 1.0, gs);
+    const int sv0 = __ldg(prm.sel + 3 * s), sv1 = __ldg(prm.sel + 3 * s + 1), sv2 = __ldg(prm.sel + 3 * s + 2);
+    double sc[3] = {0.0, 0.0, 0.0};
+    if (PH)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) sc[d] = __ldg(prm.sg + (22 + d) * prm.sne + s);
+    double y[NQ6][3];
+#pragma unroll
+    for (int q = 0; q < NQ6; ++q) to_global(gs, rule.x[q], rule.y[q], y[q]);
+    const double kr = prm.p[0], etar = prm.p[2], etai = prm.p[3];
+    // (y_q - v0_j).n_j, the plain path's split of the normal term of A_ij
+    double ynv[NQ6];
+    if (ST::dlp_part)
+#pragma unroll
+        for (int q = 0; q < NQ6; ++q)
+            ynv[q] = fma(y[q][2] - gs.v0[2], gs.n[2], fma(y[q][1] - gs.v0[1], gs.n[1], (y[q][0] - gs.v0[0]) * gs.n[0]));
+
+    for (int tt = 0; tt < tcount; ++tt) {
+        const int64_t row = t0 + tt;
+        if (row > si) break;  // rows increase with tt: the rest of this column lies below the diagonal
+        const bool adj = row == si || (prm.grids_identical && shares_vertex(sb.v[tt], sv0, sv1, sv2));
+        double a_re = 0.0, a_im = 0.0, b_re = 0.0, b_im = 0.0;  // A_ij, A_ji
+        if (!adj) {
+            double rc = 0.0, ph_s = 0.0, ph_c = 1.0;
+            if (PH) {
+                const double D0 = sc[0] - sb.c[tt][0], D1 = sc[1] - sb.c[tt][1], D2 = sc[2] - sb.c[tt][2];
+                rc = sqrt(fma(D2, D2, fma(D1, D1, D0 * D0)));
+                sincos_cw64(kr * rc, &ph_s, &ph_c);
+            }
+            // (c_i - y_q).n_i: the transposed entry's normal term split about the test centroid
+            double ynt[NQ6];
+            if (ST::dlp_part)
+#pragma unroll
+                for (int q = 0; q < NQ6; ++q)
+                    ynt[q] = fma(sb.c[tt][2] - y[q][2], sb.n[tt][2],
+                                 fma(sb.c[tt][1] - y[q][1], sb.n[tt][1], (sb.c[tt][0] - y[q][0]) * sb.n[tt][0]));
+            double s0r = 0.0, s0i = 0.0, u_re = 0.0, u_im = 0.0, v_re = 0.0, v_im = 0.0;
+            for (int p = 0; p < NQ6; ++p) {
+                const double x0 = sb.x[tt][p][0], x1 = sb.x[tt][p][1], x2 = sb.x[tt][p][2];
+                double xn = 0.0, xnt = 0.0;
+                if (ST::dlp_part) {
+                    xn = fma(gs.v0[2] - x2, gs.n[2], fma(gs.v0[1] - x1, gs.n[1], (gs.v0[0] - x0) * gs.n[0]));
+                    xnt = sb.xn[tt][p];
+                }
+                double pr = 0.0, pi = 0.0, ur = 0.0, ui = 0.0, vr = 0.0, vi = 0.0;
+#pragma unroll
+                for (int q = 0; q < NQ6; ++q) {
+                    const double d0 = y[q][0] - x0, d1 = y[q][1] - x1, d2 = y[q][2] - x2;
+                    const double r2 = fma(d2, d2, fma(d1, d1, d0 * d0));
+                    const double rinv = rsqrt(r2);
+                    const double f = rule.w[q] * rinv;
+                    if (!ST::helm) {
+                        if (ST::slp_part) pr += f;
+                        if (ST::dlp_part) {
+                            const double g3 = f * rinv * rinv;
+                            ur = fma(g3, ynv[q] + xn, ur);
+                            vr = fma(g3, ynt[q] + xnt, vr);
+                        }
+                    } else {
+                        const double r = r2 * rinv;
+                        double sn, cs;
+                        if (PH && PHC == 2)
+                            sincos_half64(kr * (r - rc), &sn, &cs);
+                        else if (PH)
+                            sincos_small64(kr * (r - rc), &sn, &cs);
+                        else
+                            sincos_cw64(kr * r, &sn, &cs);
+                        if (ST::slp_part) {
+                            pr = fma(f, cs, pr);
+                            pi = fma(f, sn, pi);
+                        }
+                        if (ST::dlp_part) {
+                            // (ikr - 1) e^{ikr} / r^3: -h1 + i h2 per unit f (dot) / r
+                            const double fr = f * rinv;
+                            const double h1 = fma(rinv, cs, kr * sn), h2 = fma(kr, cs, -rinv * sn);
+                            const double g = fr * (ynv[q] + xn), gt = fr * (ynt[q] + xnt);
+                            ur = fma(g, h1, ur);
+                            ui = fma(g, h2, ui);
+                            vr = fma(gt, h1, vr);
+                            vi = fma(gt, h2, vi);
+                        }
+                    }
+                }
+                const double wp = rule.w[p];
+                s0r = fma(wp, pr, s0r);
+                s0i = fma(wp, pi, s0i);
+                u_re = fma(wp, ur, u_re);
+                u_im = fma(wp, ui, u_im);
+                v_re = fma(wp, vr, v_re);
+                v_im = fma(wp, vi, v_im);
+            }
+            // kernel values: Laplace DLP -sum f dot / r^2; Helmholtz DLP -u_re + i u_im
+            double dr = 0.0, di = 0.0, er = 0.0, ei = 0.0;  // double-layer parts of A_ij, A_ji
+            if (ST::dlp_part) {
+                dr = -u_re;
+                di = ST::helm ? u_im : 0.0;
+                er = -v_re;
+                ei = ST::helm ? v_im : 0.0;
+            }
+            if (K == BEMPPCUDA_HELMHOLTZ_COMBINED) {
+                const double sr = fma(etar, s0r, -etai * s0i), sim = fma(etar, s0i, etai * s0r);
+                a_re = dr + sr;
+                a_im = di + sim;
+                b_re = er + sr;
+                b_im = ei + sim;
+            } else if (ST::slp_part) {
+                a_re = b_re = s0r;
+                a_im = b_im = s0i;
+            } else if (ST::swap) {
+                a_re = er;
+                a_im = ei;
+                b_re = dr;
+                b_im = di;
+            } else {
+                a_re = dr;
+                a_im = di;
+                b_re = er;
+                b_im = ei;
+            }
+            const double scale = BC_INV_4PI * sb.ie[tt] * gs.ie;
+            if (PH) {
+                double tr = a_re * ph_c - a_im * ph_s;
+                a_im = (a_re * ph_s + a_im * ph_c) * scale;
+                a_re = tr * scale;
+                tr = b_re * ph_c - b_im * ph_s;
+                b_im = (b_re * ph_s + b_im * ph_c) * scale;
+                b_re = tr * scale;
+            } else {
+                a_re *= scale;
+                a_im *= scale;
+                b_re *= scale;
+                b_im *= scale;
+            }
+        }
+        store_entry(prm, row, si, adj, a_re, a_im);
+        if (row != si) store_entry(prm, si, row, adj, b_re, b_im);
+    }
+    }
+    __syncthreads();  // the shared block is reused by the next tile of a persistent loop
+}
+
+}  // namespace bc
+
+namespace bc {
+
+// Packed mixed precision in wavenumber-scaled units (as regular_dp0_mixed2_tile).
+// Per point pair, with g = w (d'.n) / r'^2 and the shared factors
+// h1 = cos / r' + sin, h2 = cos - sin / r', the double-layer part of an entry
+// is -g h1 + i g h2 (times kappa^2); the two entries differ only in (d'.n).
+template <int K, int PHC>
+__device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm, const QuadRule &rule,
+                                                         int64_t tile_x, int64_t t0, int rows, TestBlock32p &sb) {
+    using ST = SymTraits<K>;
+    constexpr int NP = NQ6 / 2;
+    const double kap = ST::helm ? prm.p[0] : 1.0;  // callers guarantee k > 0 for the Helmholtz family
+    const int tcount = (int)min((int64_t)rows, prm.ntest - t0);
+    for (int idx = threadIdx.x; idx < tcount; idx += blockDim.x) {
+        const int64_t t = prm.tsup[t0 + idx];
+        Geom g;
+        load_geom(prm.tg, prm.tne, t, prm.tnm ? (double)prm.tnm[t] : 1.0, g);
+        double c[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) c[d] = __ldg(prm.tg + (22 + d) * prm.tne + t);
+        for (int p = 0; p < NQ6; ++p) {
+            double x[3];
+            to_global(g, rule.x[p], rule.y[p], x);
+            const float o0 = (float)(kap * (x[0] - c[0])), o1 = (float)(kap * (x[1] - c[1])),
+                        o2 = (float)(kap * (x[2] - c[2]));
+            sb.m[idx][p] = make_float4(-2.f * o0, -2.f * o1, -2.f * o2, fmaf(o2, o2, fmaf(o1, o1, o0 * o0)));
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            sb.c[idx][d] = c[d];
+            sb.n[idx][d] = (float)g.n[d];
+            sb.v[idx][d] = __ldg(prm.tel + 3 * t + d);
+        }
+        sb.ie[idx] = g.ie;
+    }
+    __syncthreads();
+
+    const int64_t si = tile_x * DP0_THREADS + threadIdx.x;
+    if (si < prm.ntrial && t0 <= si) {
+    const int64_t s = prm.ssup[si];
+    Geom gs;
+    load_geom(prm.sg, prm.sne, s, prm.snm ? (double)prm.snm[s] : 1.0, gs);
+    const int sv0 = __ldg(prm.sel + 3 * s), sv1 = __ldg(prm.sel + 3 * s + 1), sv2 = __ldg(prm.sel + 3 * s + 2);
+    double sc[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) sc[d] = __ldg(prm.sg + (22 + d) * prm.sne + s);
+    float2 yx[NP], yyy[NP], yz[NP], yy2[NP], yn2[NP], wq2[NP];
+    const float sn0 = (float)gs.n[0], sn1 = (float)gs.n[1], sn2 = (float)gs.n[2];
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+        float o[2][3];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            double v[3];
+            to_global(gs, rule.x[2 * j + h], rule.y[2 * j + h], v);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) o[h][d] = (float)(kap * (v[d] - sc[d]));
+        }
+        yx[j] = f2(o[0][0], o[1][0]);
+        yyy[j] = f2(o[0][1], o[1][1]);
+        yz[j] = f2(o[0][2], o[1][2]);
+        yy2[j] = fma2(yz[j], yz[j], fma2(yyy[j], yyy[j], mul2(yx[j], yx[j])));
+        yn2[j] = fma2(yz[j], b2(sn2), fma2(yyy[j], b2(sn1), mul2(yx[j], b2(sn0))));
+        wq2[j] = f2(rule.wf[2 * j], rule.wf[2 * j + 1]);
+    }
+    const double ek_r = (K == BEMPPCUDA_HELMHOLTZ_COMBINED) ? kap * prm.p[2] : kap;
+    const double ek_i = (K == BEMPPCUDA_HELMHOLTZ_COMBINED) ? kap * prm.p[3] : 0.0;
+    const double k2d = kap * kap;
+
+    for (int tt = 0; tt < tcount; ++tt) {
+        const int64_t row = t0 + tt;
+        if (row > si) break;
+        const bool adj = row == si || (prm.grids_identical && shares_vertex(sb.v[tt], sv0, sv1, sv2));
+        double a_re = 0.0, a_im = 0.0, b_re = 0.0, b_im = 0.0;  // A_ij, A_ji
+        if (!adj) {
+            const double D0 = kap * (sc[0] - sb.c[tt][0]), D1 = kap * (sc[1] - sb.c[tt][1]),
+                         D2 = kap * (sc[2] - sb.c[tt][2]);
+            const double rc2 = fma(D2, D2, fma(D1, D1, D0 * D0));
+            const double rc = sqrt(rc2);
+            double ph_s = 0.0, ph_c = 1.0;
+            if (ST::helm) sincos_cw64(rc, &ph_s, &ph_c);
+            const float D0f = (float)D0, D1f = (float)D1, D2f = (float)D2;
+            const float2 rcf2 = b2((float)rc), rc2f2 = b2((float)rc2);
+            // k (y - x).n_j = cp_p + yn2_q and k (x - y).n_i = ct_p + ynt_q
+            float nh0 = 0.f, nh1 = 0.f, nh2 = 0.f, Dn = 0.f, th0 = 0.f, th1 = 0.f, th2 = 0.f, Dt = 0.f;
+            float2 ynt[NP];
+            if (ST::dlp_part) {
+                const float tn0 = sb.n[tt][0], tn1 = sb.n[tt][1], tn2 = sb.n[tt][2];
+#pragma unroll
+                for (int j = 0; j < NP; ++j)
+                    ynt[j] = fma2(yz[j], b2(-tn2), fma2(yyy[j], b2(-tn1), mul2(yx[j], b2(-tn0))));
+                Dn = fmaf(D2f, sn2, fmaf(D1f, sn1, D0f * sn0));
+                nh0 = 0.5f * sn0;
+                nh1 = 0.5f * sn1;
+                nh2 = 0.5f * sn2;
+                Dt = -fmaf(D2f, tn2, fmaf(D1f, tn1, D0f * tn0));
+                th0 = -0.5f * tn0;
+                th1 = -0.5f * tn1;
+                th2 = -0.5f * tn2;
+            }
+            const float2 D0d = b2(2.f * D0f), D1d = b2(2.f * D1f), D2d = b2(2.f * D2f);
+            float2 A[NP];
+#pragma unroll
+            for (int j = 0; j < NP; ++j) A[j] = fma2(D2d, yz[j], fma2(D1d, yyy[j], fma2(D0d, yx[j], yy2[j])));
+            float2 s0r = b2(0.f), s0i = b2(0.f), ur = b2(0.f), ui = b2(0.f), vr = b2(0.f), vi = b2(0.f);
+            for (int p = 0; p < NQ6; ++p) {
+                const float4 m = sb.m[tt][p];
+                const float Bp = fmaf(D2f, m.z, fmaf(D1f, m.y, fmaf(D0f, m.x, m.w)));
+                const float2 mx = b2(m.x), my = b2(m.y), mz = b2(m.z), Bp2 = b2(Bp);
+                float2 cp2 = b2(0.f), ct2 = b2(0.f);
+                if (ST::dlp_part) {
+                    cp2 = b2(fmaf(m.z, nh2, fmaf(m.y, nh1, fmaf(m.x, nh0, Dn))));
+                    ct2 = b2(fmaf(m.z, th2, fmaf(m.y, th1, fmaf(m.x, th0, Dt))));
+                }
+#pragma unroll
+                for (int j = 0; j < NP; ++j) {
+                    const float2 sdot = fma2(yz[j], mz, fma2(yyy[j], my, fma2(yx[j], mx, add2(A[j], Bp2))));
+                    const float2 r2 = add2(rc2f2, sdot);
+                    const float2 rinv = f2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+                    const float2 f = mul2(wq2[j], rinv);
+                    if (!ST::helm) {
+                        if (ST::slp_part) s0r = add2(f, s0r);
+                        if (ST::dlp_part) {
+                            const float2 fr = mul2(mul2(f, rinv), rinv);
+                            ur = fma2(fr, add2(cp2, yn2[j]), ur);
+                            vr = fma2(fr, add2(ct2, ynt[j]), vr);
+                        }
+                    } else {
+                        const float2 den = fma2(r2, rinv, rcf2);
+                        const float2 th = mul2(sdot, f2(rcp_approx(den.x), rcp_approx(den.y)));
+                        float2 sn, cs;
+                        sincos2<PHC>(th, &sn, &cs);
+                        if (ST::slp_part) {
+                            s0r = fma2(f, cs, s0r);
+                            s0i = fma2(f, sn, s0i);
+                        }
+                        if (ST::dlp_part) {
+                            const float2 fr = mul2(f, rinv);
+                            const float2 h1 = fma2(rinv, cs, sn);
+                            const float2 h2 = fma2(mul2(rinv, b2(-1.f)), sn, cs);
+                            const float2 g = mul2(fr, add2(cp2, yn2[j])), gt = mul2(fr, add2(ct2, ynt[j]));
+                            ur = fma2(g, h1, ur);
+                            ui = fma2(g, h2, ui);
+                            vr = fma2(gt, h1, vr);
+                            vi = fma2(gt, h2, vi);
+                        }
+                    }
+                }
+                // flush where the test-point weight changes:
+                // entry += w_p [kappa eta S0 + kappa^2 (-h1 sum + i h2 sum)]
+                if (p == NQ6 - 1 || rule.w[p + 1] != rule.w[p]) {
+                    const double wp = rule.w[p];
+                    double sr = 0.0, sim = 0.0;
+                    if (ST::slp_part) {
+                        const double xr = (double)(s0r.x + s0r.y), xi = (double)(s0i.x + s0i.y);
+                        sr = fma(ek_r, xr, -ek_i * xi);
+                        sim = fma(ek_r, xi, ek_i * xr);
+                        s0r = s0i = b2(0.f);
+                    }
+                    double dr = 0.0, di = 0.0, er = 0.0, ei = 0.0;
+                    if (ST::dlp_part) {
+                        dr = -k2d * (double)(ur.x + ur.y);
+                        er = -k2d * (double)(vr.x + vr.y);
+                        if (ST::helm) {
+                            di = k2d * (double)(ui.x + ui.y);
+                            ei = k2d * (double)(vi.x + vi.y);
+                        }
+                        ur = ui = vr = vi = b2(0.f);
+                    }
+                    if (ST::swap) {
+                        a_re = fma(wp, er, a_re);
+                        a_im = fma(wp, ei, a_im);
+                        b_re = fma(wp, dr, b_re);
+                        b_im = fma(wp, di, b_im);
+                    } else {
+                        a_re = fma(wp, sr + dr, a_re);
+                        a_im = fma(wp, sim + di, a_im);
+                        b_re = fma(wp, sr + er, b_re);
+                        b_im = fma(wp, sim + ei, b_im);
+                    }
+                }
+            }
+            const double scale = BC_INV_4PI * sb.ie[tt] * gs.ie;
+            double tr = a_re * ph_c - a_im * ph_s;
+            a_im = (a_re * ph_s + a_im * ph_c) * scale;
+            a_re = tr * scale;
+            tr = b_re * ph_c - b_im * ph_s;
+            b_im = (b_re * ph_s + b_im * ph_c) * scale;
+            b_re = tr * scale;
+        }
+        store_entry(prm, row, si, adj, a_re, a_im);
+        if (row != si) store_entry(prm, si, row, adj, b_re, b_im);
+    }
+    }
+    __syncthreads();
+}
+
+}  // namespace bc

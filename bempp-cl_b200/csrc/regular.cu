@@ -22,7 +22,7 @@
 //    with atomicAdd into the (pre-zeroed or accumulating) result.
 #include <cstdio>
 
-#include "dp0.cuh"
+#include "dp0_sym.cuh"
 
 namespace bc {
 
@@ -226,10 +226,51 @@ __global__ void __launch_bounds__(GEN_THREADS) regular_generic(RegParams prm, Qu
     }
 }
 
+// Symmetric sweeps: blockIdx.x = column block, blockIdx.y = row chunk; chunks
+// that start below the block's last column have no pair i <= j and exit
+// before touching shared memory.
+template <int K, int PHC>
+__global__ void __launch_bounds__(DP0_THREADS) regular_dp0_fp64_sym(RegParams prm, QuadRule rule) {
+    const int64_t t0 = (int64_t)blockIdx.y * DP0_TCHUNK;
+    if (t0 >= ((int64_t)blockIdx.x + 1) * DP0_THREADS) return;
+    __shared__ TestBlock64s sb;
+    regular_dp0_fp64_sym_tile<K, PHC>(prm, rule, blockIdx.x, t0, DP0_TCHUNK, sb);
+}
+
+template <int K, int PHC>
+__global__ void __launch_bounds__(DP0_THREADS, 3) regular_dp0_mixed_sym(RegParams prm, QuadRule rule) {
+    const int64_t t0 = (int64_t)blockIdx.y * DP0_TCHUNK;
+    if (t0 >= ((int64_t)blockIdx.x + 1) * DP0_THREADS) return;
+    __shared__ TestBlock32p sb;
+    regular_dp0_mixed_sym_tile<K, PHC>(prm, rule, blockIdx.x, t0, DP0_TCHUNK, sb);
+}
+
 template <int K>
-static cudaError_t launch_dp0(const RegParams &prm, const QuadRule &rule, int mixed, int phase_class,
+static cudaError_t launch_dp0(const RegParams &prm, const QuadRule &rule, int mixed, int phase_class, bool sym,
                               cudaStream_t st) {
     dim3 grid((unsigned)((prm.ntrial + DP0_THREADS - 1) / DP0_THREADS), (unsigned)((prm.ntest + DP0_TCHUNK - 1) / DP0_TCHUNK));
+    if constexpr (SymTraits<K>::supported) {
+        // same DP0 space on both sides, real wavenumber (k > 0 for the scaled mixed path)
+        const bool real_k = !KernelTraits<K>::helm || (prm.p[1] == 0.0 && (!mixed || prm.p[0] > 0.0));
+        if (sym && real_k) {
+            if (mixed) {
+                if (phase_class == 2)
+                    regular_dp0_mixed_sym<K, 2><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+                else if (phase_class == 1)
+                    regular_dp0_mixed_sym<K, 1><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+                else
+                    regular_dp0_mixed_sym<K, 0><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+            } else {
+                if (phase_class == 2)
+                    regular_dp0_fp64_sym<K, 2><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+                else if (phase_class == 1)
+                    regular_dp0_fp64_sym<K, 1><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+                else
+                    regular_dp0_fp64_sym<K, 0><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+            }
+            return cudaGetLastError();
+        }
+    }
     const bool ck = prm.p[1] != 0.0 && KernelTraits<K>::helm;
     // the packed path measures lengths in units of 1/k: Helmholtz needs k > 0
     const bool packed = !KernelTraits<K>::helm || prm.p[0] > 0.0;
@@ -334,18 +375,22 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
     // 1/2 lets the sine / cosine skip the range reduction (classes 1, 2)
     const double theta = fabs(a->params[0]) * a->phase_radius;
     const int phase_class = a->phase_radius > 0.0 ? (theta <= 0.5 ? 2 : (theta <= 1.0 ? 1 : 0)) : 0;
+    // one DP0 space on both sides of one grid: each element pair gives A_ij and A_ji
+    const bool sym = dp0 && !a->no_symmetry && a->grids_identical && a->test.support == a->trial.support &&
+                     a->test.nsupport == a->trial.nsupport && a->test_grid.geom == a->trial_grid.geom &&
+                     a->test.normal_mult == a->trial.normal_mult && prm.ntest == prm.ntrial;
     if (dp0) {
         switch (a->kernel) {
-        case BEMPPCUDA_LAPLACE_SLP: err = launch_dp0<BEMPPCUDA_LAPLACE_SLP>(prm, rule, mixed, phase_class, st); break;
-        case BEMPPCUDA_LAPLACE_DLP: err = launch_dp0<BEMPPCUDA_LAPLACE_DLP>(prm, rule, mixed, phase_class, st); break;
-        case BEMPPCUDA_LAPLACE_ADLP: err = launch_dp0<BEMPPCUDA_LAPLACE_ADLP>(prm, rule, mixed, phase_class, st); break;
-        case BEMPPCUDA_HELMHOLTZ_SLP: err = launch_dp0<BEMPPCUDA_HELMHOLTZ_SLP>(prm, rule, mixed, phase_class, st); break;
-        case BEMPPCUDA_HELMHOLTZ_DLP: err = launch_dp0<BEMPPCUDA_HELMHOLTZ_DLP>(prm, rule, mixed, phase_class, st); break;
-        case BEMPPCUDA_HELMHOLTZ_ADLP: err = launch_dp0<BEMPPCUDA_HELMHOLTZ_ADLP>(prm, rule, mixed, phase_class, st); break;
-        case BEMPPCUDA_MODHELM_SLP: err = launch_dp0<BEMPPCUDA_MODHELM_SLP>(prm, rule, mixed, phase_class, st); break;
-        case BEMPPCUDA_MODHELM_DLP: err = launch_dp0<BEMPPCUDA_MODHELM_DLP>(prm, rule, mixed, phase_class, st); break;
-        case BEMPPCUDA_MODHELM_ADLP: err = launch_dp0<BEMPPCUDA_MODHELM_ADLP>(prm, rule, mixed, phase_class, st); break;
-        case BEMPPCUDA_HELMHOLTZ_COMBINED: err = launch_dp0<BEMPPCUDA_HELMHOLTZ_COMBINED>(prm, rule, mixed, phase_class, st); break;
+        case BEMPPCUDA_LAPLACE_SLP: err = launch_dp0<BEMPPCUDA_LAPLACE_SLP>(prm, rule, mixed, phase_class, sym, st); break;
+        case BEMPPCUDA_LAPLACE_DLP: err = launch_dp0<BEMPPCUDA_LAPLACE_DLP>(prm, rule, mixed, phase_class, sym, st); break;
+        case BEMPPCUDA_LAPLACE_ADLP: err = launch_dp0<BEMPPCUDA_LAPLACE_ADLP>(prm, rule, mixed, phase_class, sym, st); break;
+        case BEMPPCUDA_HELMHOLTZ_SLP: err = launch_dp0<BEMPPCUDA_HELMHOLTZ_SLP>(prm, rule, mixed, phase_class, sym, st); break;
+        case BEMPPCUDA_HELMHOLTZ_DLP: err = launch_dp0<BEMPPCUDA_HELMHOLTZ_DLP>(prm, rule, mixed, phase_class, sym, st); break;
+        case BEMPPCUDA_HELMHOLTZ_ADLP: err = launch_dp0<BEMPPCUDA_HELMHOLTZ_ADLP>(prm, rule, mixed, phase_class, sym, st); break;
+        case BEMPPCUDA_MODHELM_SLP: err = launch_dp0<BEMPPCUDA_MODHELM_SLP>(prm, rule, mixed, phase_class, sym, st); break;
+        case BEMPPCUDA_MODHELM_DLP: err = launch_dp0<BEMPPCUDA_MODHELM_DLP>(prm, rule, mixed, phase_class, sym, st); break;
+        case BEMPPCUDA_MODHELM_ADLP: err = launch_dp0<BEMPPCUDA_MODHELM_ADLP>(prm, rule, mixed, phase_class, sym, st); break;
+        case BEMPPCUDA_HELMHOLTZ_COMBINED: err = launch_dp0<BEMPPCUDA_HELMHOLTZ_COMBINED>(prm, rule, mixed, phase_class, sym, st); break;
         default: bc_set_error("kernel %d not valid for boundary assembly", a->kernel); return BEMPPCUDA_ERR_INVALID;
         }
     } else {
