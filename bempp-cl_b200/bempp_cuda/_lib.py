@@ -236,6 +236,7 @@ class ShapeArgs(_ct.Structure):
         ("out", _vp),
         ("workspace", _vp),
         ("workspace_bytes", _i64),
+        ("phase_radius", _ct.c_double),
     ]
 
 

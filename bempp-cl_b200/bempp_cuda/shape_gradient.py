@@ -136,6 +136,7 @@ class FarFieldObjective(object):
         for c in range(3):
             a.incident[c] = self.incident[c]
         a.rhs_coeff[0], a.rhs_coeff[1] = -1.0, 0.0
+        a.phase_radius = 1.0001 * 2.0 * geometry.radius
         return a
 
     def descriptor(self, k):

@@ -9,7 +9,7 @@
 // launch over the concatenated pair list (FP64).
 #include <cstring>
 
-#include "dp0.cuh"
+#include "dp0_sym.cuh"
 
 namespace bc {
 
@@ -18,7 +18,7 @@ struct BatchDev {
     int64_t tile_begin;
     int64_t tiles_x;
     int32_t rows;  // test elements per work item (<= DP0_TCHUNK)
-    int32_t pad0;
+    int32_t sym;   // symmetric sweep: items cover the tiles on or above the diagonal
     int64_t pair_begin;
     int32_t precision;
     int32_t phase_class;
@@ -31,6 +31,7 @@ constexpr size_t kCounterBytes = 256;
 
 union TileShared {
     TestBlock64 b64;
+    TestBlock64s b64s;
     TestBlock32 b32;
     TestBlock32p b32p;
 };
@@ -63,6 +64,43 @@ __device__ __forceinline__ void run_tile(const BatchDev &P, const QuadRule &rule
     }
 }
 
+// Symmetric sweep of one problem (real k; k > 0 on the mixed path): tile
+// (tx, ty) = columns [128 tx, 128 tx + 128) x rows [rows ty, rows ty + rows).
+template <int K>
+__device__ __forceinline__ void run_tile_sym(const BatchDev &P, const QuadRule &rule, int64_t tx, int64_t ty,
+                                             TileShared &sh) {
+    const int64_t t0 = ty * P.rows;
+    const int rows = P.rows;
+    if (P.precision == BEMPPCUDA_FP64) {
+        if (P.phase_class == 2)
+            regular_dp0_fp64_sym_tile<K, 2>(P.prm, rule, tx, t0, rows, sh.b64s);
+        else if (P.phase_class == 1)
+            regular_dp0_fp64_sym_tile<K, 1>(P.prm, rule, tx, t0, rows, sh.b64s);
+        else
+            regular_dp0_fp64_sym_tile<K, 0>(P.prm, rule, tx, t0, rows, sh.b64s);
+    } else {
+        if (P.phase_class == 2)
+            regular_dp0_mixed_sym_tile<K, 2>(P.prm, rule, tx, t0, rows, sh.b32p);
+        else if (P.phase_class == 1)
+            regular_dp0_mixed_sym_tile<K, 1>(P.prm, rule, tx, t0, rows, sh.b32p);
+        else
+            regular_dp0_mixed_sym_tile<K, 0>(P.prm, rule, tx, t0, rows, sh.b32p);
+    }
+}
+
+// Tiles before column tx of a symmetric problem: column u holds g (u + 1)
+// row tiles (g = 128 / rows), clipped to the row-tile count only in the last column.
+__host__ __device__ __forceinline__ int64_t sym_tiles_before(int64_t tx, int64_t g) { return g * tx * (tx + 1) / 2; }
+
+__device__ __forceinline__ void sym_coords(const BatchDev &P, int64_t local, int64_t *tx, int64_t *ty) {
+    const int64_t g = DP0_THREADS / P.rows;
+    int64_t c = (int64_t)((sqrt(1.0 + 8.0 * (double)local / (double)g) - 1.0) * 0.5);
+    while (c > 0 && sym_tiles_before(c, g) > local) --c;
+    while (c + 1 < P.tiles_x && sym_tiles_before(c + 1, g) <= local) ++c;
+    *tx = c;
+    *ty = local - sym_tiles_before(c, g);
+}
+
 // Index of the last problem whose range starts at or before `item`.
 __device__ __forceinline__ int find_problem(const BatchDev *__restrict__ probs, int nprob, int64_t item,
                                             bool by_pairs) {
@@ -93,7 +131,13 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_batch(const BatchDev *__r
         if (tile >= total_tiles) break;
         const BatchDev &P = probs[find_problem(probs, nprob, tile, false)];
         const int64_t local = tile - P.tile_begin;
-        run_tile<K>(P, rule, local % P.tiles_x, local / P.tiles_x, sh);
+        if (P.sym) {
+            int64_t tx, ty;
+            sym_coords(P, local, &tx, &ty);
+            run_tile_sym<K>(P, rule, tx, ty, sh);
+        } else {
+            run_tile<K>(P, rule, local % P.tiles_x, local / P.tiles_x, sh);
+        }
     }
 }
 
@@ -150,12 +194,22 @@ __global__ void __launch_bounds__(32 * SB_WARPS) singular_batch(const BatchDev *
 
 using namespace bc;
 
-static int64_t tiles_of(int64_t n, int rows) {
-    return ((n + DP0_THREADS - 1) / DP0_THREADS) * ((n + rows - 1) / rows);
+static int64_t tiles_of(int64_t n, int rows, bool sym) {
+    const int64_t tx = (n + DP0_THREADS - 1) / DP0_THREADS, ty = (n + rows - 1) / rows;
+    if (!sym || tx == 0) return tx * ty;
+    const int64_t g = DP0_THREADS / rows;
+    return sym_tiles_before(tx - 1, g) + (ty < g * tx ? ty : g * tx);
 }
 
 static int rows_of(const bemppcuda_batch_args *a) {
     return (a->rows_per_item >= 1 && a->rows_per_item <= DP0_TCHUNK) ? a->rows_per_item : DP0_TCHUNK;
+}
+
+// The symmetric sweep needs a real wavenumber (k > 0 for the scaled mixed
+// path) and a row height that divides the 128-column block.
+static bool sym_of(const bemppcuda_batch_problem &p, int rows) {
+    if (DP0_THREADS % rows != 0 || p.params[1] != 0.0) return false;
+    return p.precision == BEMPPCUDA_FP64 || p.params[0] > 0.0;
 }
 
 extern "C" int64_t bemppcuda_batch_workspace_bytes(int32_t nproblems) {
@@ -236,8 +290,9 @@ extern "C" int bemppcuda_batch_prepare(const bemppcuda_batch_args *a, void *stre
         r.ld = p.ld;
         d.tile_begin = tiles;
         d.tiles_x = (p.grid.nelements + DP0_THREADS - 1) / DP0_THREADS;
-        tiles += tiles_of(p.grid.nelements, rows_of(a));
         d.rows = rows_of(a);
+        d.sym = sym_of(p, d.rows) ? 1 : 0;
+        tiles += tiles_of(p.grid.nelements, d.rows, d.sym != 0);
         d.pair_begin = p.pair_begin;
         d.precision = p.precision;
         const double theta = fabs(p.params[0]) * p.phase_radius;
@@ -289,7 +344,8 @@ extern "C" int bemppcuda_batch_launch(const bemppcuda_batch_args *a, void *strea
         return BEMPPCUDA_ERR_CUDA;
     }
     int64_t total_tiles = 0;
-    for (int i = 0; i < a->nproblems; ++i) total_tiles += tiles_of(a->problems[i].grid.nelements, rows_of(a));
+    for (int i = 0; i < a->nproblems; ++i)
+        total_tiles += tiles_of(a->problems[i].grid.nelements, rows_of(a), sym_of(a->problems[i], rows_of(a)));
     QuadRule rule;
     rule.nq = a->nq;
     rule.pad = 0;

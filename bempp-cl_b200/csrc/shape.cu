@@ -37,20 +37,23 @@
 
 namespace bc {
 
-// Per-element partial sums, SH_ACC doubles per element (element-major):
-//  0-2  sum gd            (element as test)     10-12 sum gd           (element as trial)
-//  3-5  sum xi(x) gd                            13-15 sum xi(y) gd
-//  6-8  sum eta(x) gd                           16-18 sum eta(y) gd
-//  9    sum ie_t d/die_t                        19-21 sum a2 d
-//                                               22    sum Re(Gc eta)
-//                                               23    d/dk
-constexpr int SH_ACC = 24;
+// Per-element partial sums, SH_ACC doubles per element (element-major).  For
+// the points z of element e (test points when e is the row element, trial
+// points when it is the column element) with local coordinates (xi, eta):
+//  0-2   sum dF/dz                 (test side -gd, trial side +gd)
+//  3-5   sum xi(z) dF/dz
+//  6-8   sum eta(z) dF/dz
+//  9-11  sum a2 d                  (e as trial: derivative through c_e)
+//  12    coefficient of d ie_e     (test: ival / ie_e, trial: ere)
+//  13    d/dk
+constexpr int SH_ACC = 16;
 constexpr int SH_THREADS = 128;
 constexpr int SH_TCHUNK = 32;
-constexpr int SH_TILES = 8;  // test chunks per block
+constexpr int SH_TILES = 8;  // row chunks per block
 constexpr int SH_WARPS = SH_THREADS / 32;
 constexpr int SHS_WARPS = 8;  // singular kernel: pairs per block
 constexpr int SH_NQ = 6;
+constexpr int SH_RED = 13;  // row-element sums reduced across a block
 
 struct ShapeParams {
     const double *g;
@@ -65,7 +68,7 @@ struct ShapeParams {
     const double *w;
     const int32_t *te, *se, *toff, *soff, *woff, *npts;
     int ndir;
-    int pad;
+    int phase_class;
     const double *dirs;
     double ff_beta, ff_eta_re, ff_eta_im, ff_deta_re, ff_deta_im;
     double inc[3];
@@ -85,20 +88,15 @@ __device__ __forceinline__ void cross3(const double a[3], const double b[3], dou
     o[2] = a[0] * b[1] - a[1] * b[0];
 }
 
-// One quadrature-point pair of the combined kernel, contracted with c' = (cre, cim).
-__device__ __forceinline__ void qpe_terms(const double d[3], double w, double cre, double cim, const double cs[3],
-                                          double ies, double bet, const ShapeParams &P, QpeTerms &o) {
-    const double r2 = fma(d[2], d[2], fma(d[1], d[1], d[0] * d[0]));
-    const double rinv = rsqrt(r2);
-    const double r = r2 * rinv;
-    const double rinv2 = rinv * rinv;
-    const double kr = P.k * r;
-    double sn, cn;
-    sincos_cw64(kr, &sn, &cn);
-    const double f = w * rinv * BC_INV_4PI;
-    const double gr = cn * f, gi = sn * f;
-    const double Gr = cre * gr - cim * gi, Gi = fma(cre, gi, cim * gr);  // Gc = c' w G
+// One ordered quadrature-point pair of the combined kernel.  (gr, gi) = w
+// exp(ik(r - r_c)) / (4 pi r) and (cre, cim) = conj(lambda_t) phi_s ie_t
+// exp(ik r_c), so Gc = c' w G; d = y - x runs from the test point to the trial point.
+__device__ __forceinline__ void qpe_ordered(const double d[3], double r, double rinv2, double gr, double gi,
+                                            double cre, double cim, const double cs[3], double ies, double bet,
+                                            const ShapeParams &P, QpeTerms &o) {
+    const double Gr = cre * gr - cim * gi, Gi = fma(cre, gi, cim * gr);
     const double u = fma(d[2], cs[2], fma(d[1], cs[1], d[0] * cs[0])) * rinv2;
+    const double kr = P.k * r;
     const double Zr = fma(-Gi, kr, -Gr), Zi = fma(Gr, kr, -Gi);  // Gc z
     const double reGcEta = Gr * P.eta_re - Gi * P.eta_im;
     const double reGzEta = Zr * P.eta_re - Zi * P.eta_im;
@@ -112,7 +110,19 @@ __device__ __forceinline__ void qpe_terms(const double d[3], double w, double cr
     o.ival = fma(bu, Zr, ies * reGcEta);
     o.ere = reGcEta;
     const double er = P.deta_re - P.eta_im * r, ei = fma(P.eta_re, r, P.deta_im);
-    o.kval = fma(-bu * P.k * r2, Gr, ies * (Gr * er - Gi * ei));
+    o.kval = fma(-bu * P.k * r * r, Gr, ies * (Gr * er - Gi * ei));
+}
+
+// exp(i theta) for the phase offset theta = k (r - r_c) of class PHC (0: any
+// argument, 1: |theta| <= 1, 2: |theta| <= 1/2).
+template <int PHC>
+__device__ __forceinline__ void phase64(double th, double *s, double *c) {
+    if (PHC == 2)
+        sincos_half64(th, s, c);
+    else if (PHC == 1)
+        sincos_small64(th, s, c);
+    else
+        sincos_cw64(th, s, c);
 }
 
 __device__ __forceinline__ bool touches(const int *a, int b0, int b1, int b2) {
@@ -122,22 +132,34 @@ __device__ __forceinline__ bool touches(const int *a, int b0, int b1, int b2) {
 
 struct ShapeTile {
     double x[SH_TCHUNK][SH_NQ][3];
-    double2 lc[SH_TCHUNK];  // conj(lambda_t) ie_t
+    double cr[SH_TCHUNK][3];  // ie_i n_i
+    double ce[SH_TCHUNK][3];  // centroid
+    double2 lc[SH_TCHUNK];    // conj(lambda_i) ie_i
+    double2 ph[SH_TCHUNK];    // phi_i
+    double ie[SH_TCHUNK];
+    double bet[SH_TCHUNK];
     int v[SH_TCHUNK][3];
-    double red[SH_WARPS][SH_TCHUNK][10];
+    double red[SH_WARPS][SH_TCHUNK][SH_RED];
 };
 
-// Regular pairs: one thread per trial element, SH_TILES chunks of SH_TCHUNK
-// test elements staged in shared memory.  Trial-side sums stay in registers
-// for the whole block; test-side sums are reduced over the warp (shuffles),
-// then over the block's warps (shared memory), then added to the workspace.
+// Regular pairs, symmetric sweep: one thread per column element j, rows i < j
+// staged SH_TCHUNK at a time, SH_TILES chunks per block.  Each unordered pair
+// gives the ordered pairs (i, j) (test i, trial j) and (j, i) (test j, trial
+// i) from one evaluation of r and the phase.  Column sums stay in registers
+// for the whole block; row sums are reduced over the warp (shuffles), then
+// over the block's warps (shared memory), then added to the workspace.
+template <int PHC>
 __global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadRule rule) {
+    const int64_t row0 = (int64_t)blockIdx.y * SH_TILES * SH_TCHUNK;
+    const int64_t col0 = (int64_t)blockIdx.x * SH_THREADS;
+    if (row0 >= col0 + SH_THREADS) return;  // the whole block lies below the diagonal
     __shared__ ShapeTile sb;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t s = (int64_t)blockIdx.x * SH_THREADS + threadIdx.x;
+    const int64_t s = col0 + threadIdx.x;
     const bool active = s < P.ne;
-    double y[SH_NQ][3], cs[3] = {0.0, 0.0, 0.0};
-    double ies = 0.0, bet = 0.0, pr = 0.0, pim = 0.0;
+    double y[SH_NQ][3], cs[3] = {0.0, 0.0, 0.0}, sc[3] = {0.0, 0.0, 0.0};
+    double ies = 0.0, ies_inv = 0.0, bet = 0.0;
+    double2 phs = make_double2(0.0, 0.0), ls = make_double2(0.0, 0.0);
     int sv0 = -1, sv1 = -1, sv2 = -1;
     if (active) {
         Geom gs;
@@ -145,12 +167,16 @@ __global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadR
 #pragma unroll
         for (int q = 0; q < SH_NQ; ++q) to_global(gs, rule.x[q], rule.y[q], y[q]);
 #pragma unroll
-        for (int c = 0; c < 3; ++c) cs[c] = gs.n[c] * gs.ie;
+        for (int c = 0; c < 3; ++c) {
+            cs[c] = gs.n[c] * gs.ie;
+            sc[c] = __ldg(P.g + (22 + c) * P.ne + s);
+        }
         ies = gs.ie;
+        ies_inv = 1.0 / gs.ie;
         bet = P.beta * (P.nm ? (double)P.nm[s] : 1.0);
-        const double2 ph = P.phi[s];
-        pr = ph.x;
-        pim = ph.y;
+        phs = P.phi[s];
+        const double2 l = P.lam[s];
+        ls = make_double2(l.x * gs.ie, -l.y * gs.ie);  // conj(lambda_j) ie_j
         sv0 = P.el[3 * s];
         sv1 = P.el[3 * s + 1];
         sv2 = P.el[3 * s + 2];
@@ -158,73 +184,116 @@ __global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadR
 #pragma unroll
         for (int q = 0; q < SH_NQ; ++q) y[q][0] = y[q][1] = y[q][2] = 0.0;
     }
-    double ty[3] = {0.0, 0.0, 0.0}, xy[3] = {0.0, 0.0, 0.0}, yy[3] = {0.0, 0.0, 0.0}, cy[3] = {0.0, 0.0, 0.0};
-    double ey = 0.0, kacc = 0.0;
+    // column sums (layout of the workspace, fields 0-13)
+    double cT[3] = {0.0, 0.0, 0.0}, cX[3] = {0.0, 0.0, 0.0}, cY[3] = {0.0, 0.0, 0.0}, cC[3] = {0.0, 0.0, 0.0};
+    double cI = 0.0, cK = 0.0;
 
     for (int tile = 0; tile < SH_TILES; ++tile) {
-        const int64_t t0 = ((int64_t)blockIdx.y * SH_TILES + tile) * SH_TCHUNK;
-        if (t0 >= P.ne) break;  // uniform over the block
+        const int64_t t0 = row0 + (int64_t)tile * SH_TCHUNK;
+        if (t0 >= P.ne || t0 >= col0 + SH_THREADS) break;  // uniform over the block
         const int tcount = (int)min((int64_t)SH_TCHUNK, P.ne - t0);
-        __syncthreads();  // previous tile's shared data fully consumed
+        __syncthreads();  // previous chunk's shared data fully consumed
         for (int idx = threadIdx.x; idx < tcount; idx += SH_THREADS) {
             const int64_t t = t0 + idx;
             Geom g;
             load_geom(P.g, P.ne, t, 1.0, g);
 #pragma unroll
             for (int p = 0; p < SH_NQ; ++p) to_global(g, rule.x[p], rule.y[p], sb.x[idx][p]);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                sb.cr[idx][c] = g.n[c] * g.ie;
+                sb.ce[idx][c] = __ldg(P.g + (22 + c) * P.ne + t);
+                sb.v[idx][c] = P.el[3 * t + c];
+            }
             const double2 l = P.lam[t];
             sb.lc[idx] = make_double2(l.x * g.ie, -l.y * g.ie);
-#pragma unroll
-            for (int c = 0; c < 3; ++c) sb.v[idx][c] = P.el[3 * t + c];
+            sb.ph[idx] = P.phi[t];
+            sb.ie[idx] = g.ie;
+            sb.bet[idx] = P.beta * (P.nm ? (double)P.nm[t] : 1.0);
         }
         __syncthreads();
         for (int tt = 0; tt < tcount; ++tt) {
-            double px[10];
+            const int64_t row = t0 + tt;
+            double rs[SH_RED];  // row sums of this pair
 #pragma unroll
-            for (int f = 0; f < 10; ++f) px[f] = 0.0;
-            const bool skip = !active || touches(sb.v[tt], sv0, sv1, sv2);
+            for (int f = 0; f < SH_RED; ++f) rs[f] = 0.0;
+            const bool skip = !active || row >= s || touches(sb.v[tt], sv0, sv1, sv2);
             if (!skip) {
-                const double2 lc = sb.lc[tt];
-                const double cre = lc.x * pr - lc.y * pim, cim = fma(lc.x, pim, lc.y * pr);
+                // pair phase exp(i k r_c) folded into both contraction coefficients
+                const double D0 = sc[0] - sb.ce[tt][0], D1 = sc[1] - sb.ce[tt][1], D2 = sc[2] - sb.ce[tt][2];
+                const double rc = sqrt(fma(D2, D2, fma(D1, D1, D0 * D0)));
+                double pcs = 1.0, psn = 0.0;
+                if (PHC > 0) sincos_cw64(P.k * rc, &psn, &pcs);
+                const double2 lt = sb.lc[tt], pt = sb.ph[tt];
+                // ordered (i, j): conj(lambda_i) ie_i phi_j;  (j, i): conj(lambda_j) ie_j phi_i
+                double c1r = lt.x * phs.x - lt.y * phs.y, c1i = fma(lt.x, phs.y, lt.y * phs.x);
+                double c2r = ls.x * pt.x - ls.y * pt.y, c2i = fma(ls.x, pt.y, ls.y * pt.x);
+                if (PHC > 0) {
+                    const double a = c1r * pcs - c1i * psn, b = fma(c1r, psn, c1i * pcs);
+                    c1r = a;
+                    c1i = b;
+                    const double e = c2r * pcs - c2i * psn, f = fma(c2r, psn, c2i * pcs);
+                    c2r = e;
+                    c2i = f;
+                }
+                const double iet = sb.ie[tt], iet_inv = 1.0 / iet, bett = sb.bet[tt];
+                const double ct[3] = {sb.cr[tt][0], sb.cr[tt][1], sb.cr[tt][2]};
                 for (int p = 0; p < SH_NQ; ++p) {
                     const double x0 = sb.x[tt][p][0], x1 = sb.x[tt][p][1], x2 = sb.x[tt][p][2];
                     const double wp = rule.w[p];
-                    double pp[3] = {0.0, 0.0, 0.0};
+                    double pp[3] = {0.0, 0.0, 0.0};  // row-element point derivative at x_p
 #pragma unroll
                     for (int q = 0; q < SH_NQ; ++q) {
                         const double d[3] = {y[q][0] - x0, y[q][1] - x1, y[q][2] - x2};
-                        QpeTerms o;
-                        qpe_terms(d, wp * rule.w[q], cre, cim, cs, ies, bet, P, o);
+                        const double r2 = fma(d[2], d[2], fma(d[1], d[1], d[0] * d[0]));
+                        const double rinv = rsqrt(r2);
+                        const double r = r2 * rinv;
+                        const double rinv2 = rinv * rinv;
+                        double sn, cn;
+                        if (PHC > 0)
+                            phase64<PHC>(P.k * (r - rc), &sn, &cn);
+                        else
+                            sincos_cw64(P.k * r, &sn, &cn);
+                        const double f = wp * rule.w[q] * rinv * BC_INV_4PI;
+                        const double gr = cn * f, gi = sn * f;
+                        QpeTerms o1, o2;
+                        // (i, j): x in i (test), y in j (trial), d = y - x
+                        qpe_ordered(d, r, rinv2, gr, gi, c1r, c1i, cs, ies, bet, P, o1);
+                        // (j, i): test point y, trial point x, d' = -d
+                        const double dn[3] = {-d[0], -d[1], -d[2]};
+                        qpe_ordered(dn, r, rinv2, gr, gi, c2r, c2i, ct, iet, bett, P, o2);
+                        // column element j: trial of (i, j) (+gd1), test of (j, i) (-gd2)
 #pragma unroll
                         for (int c = 0; c < 3; ++c) {
-                            pp[c] += o.gd[c];
-                            xy[c] = fma(rule.x[q], o.gd[c], xy[c]);
-                            yy[c] = fma(rule.y[q], o.gd[c], yy[c]);
-                            cy[c] = fma(o.a2, d[c], cy[c]);
+                            const double gj = o1.gd[c] - o2.gd[c];
+                            cT[c] += gj;
+                            cX[c] = fma(rule.x[q], gj, cX[c]);
+                            cY[c] = fma(rule.y[q], gj, cY[c]);
+                            cC[c] = fma(o1.a2, d[c], cC[c]);
+                            pp[c] -= gj;  // row element i: test of (i, j) (-gd1), trial of (j, i) (+gd2)
+                            rs[9 + c] = fma(o2.a2, dn[c], rs[9 + c]);
                         }
-                        px[9] += o.ival;
-                        ey += o.ere;
-                        kacc += o.kval;
+                        cI = fma(o2.ival, ies_inv, cI + o1.ere);
+                        rs[12] = fma(o1.ival, iet_inv, rs[12] + o2.ere);
+                        cK += o1.kval + o2.kval;
                     }
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
-                        px[c] += pp[c];
-                        px[3 + c] = fma(rule.x[p], pp[c], px[3 + c]);
-                        px[6 + c] = fma(rule.y[p], pp[c], px[6 + c]);
+                        rs[c] += pp[c];
+                        rs[3 + c] = fma(rule.x[p], pp[c], rs[3 + c]);
+                        rs[6 + c] = fma(rule.y[p], pp[c], rs[6 + c]);
                     }
                 }
-#pragma unroll
-                for (int c = 0; c < 3; ++c) ty[c] += px[c];
             }
 #pragma unroll
-            for (int f = 0; f < 10; ++f) px[f] = warp_sum(px[f]);
+            for (int f = 0; f < SH_RED; ++f) rs[f] = warp_sum(rs[f]);
             if (lane == 0)
 #pragma unroll
-                for (int f = 0; f < 10; ++f) sb.red[warp][tt][f] = px[f];
+                for (int f = 0; f < SH_RED; ++f) sb.red[warp][tt][f] = rs[f];
         }
         __syncthreads();
-        for (int idx = threadIdx.x; idx < tcount * 10; idx += SH_THREADS) {
-            const int tt = idx / 10, f = idx - 10 * (idx / 10);
+        for (int idx = threadIdx.x; idx < tcount * SH_RED; idx += SH_THREADS) {
+            const int tt = idx / SH_RED, f = idx - SH_RED * (idx / SH_RED);
             double v = 0.0;
 #pragma unroll
             for (int wi = 0; wi < SH_WARPS; ++wi) v += sb.red[wi][tt][f];
@@ -235,17 +304,17 @@ __global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadR
         double *a = P.acc + s * SH_ACC;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            atomicAdd(a + 10 + c, ty[c]);
-            atomicAdd(a + 13 + c, xy[c]);
-            atomicAdd(a + 16 + c, yy[c]);
-            atomicAdd(a + 19 + c, cy[c]);
+            atomicAdd(a + c, cT[c]);
+            atomicAdd(a + 3 + c, cX[c]);
+            atomicAdd(a + 6 + c, cY[c]);
+            atomicAdd(a + 9 + c, cC[c]);
         }
-        atomicAdd(a + 22, ey);
-        atomicAdd(a + 23, kacc);
+        atomicAdd(a + 12, cI);
+        atomicAdd(a + 13, cK);
     }
 }
 
-// Singular pairs: one warp per pair, lanes over its Sauter-Schwab points.
+// Singular pairs: one warp per ordered pair, lanes over its Sauter-Schwab points.
 __global__ void __launch_bounds__(32 * SHS_WARPS) shape_singular(ShapeParams P) {
     const int lane = threadIdx.x & 31;
     const int64_t k = (int64_t)blockIdx.x * SHS_WARPS + (threadIdx.x >> 5);
@@ -272,8 +341,14 @@ __global__ void __launch_bounds__(32 * SHS_WARPS) shape_singular(ShapeParams P) 
         to_global(gt, tpm.x, tpm.y, x);
         to_global(gs, spm.x, spm.y, y);
         const double d[3] = {y[0] - x[0], y[1] - x[1], y[2] - x[2]};
+        const double r2 = fma(d[2], d[2], fma(d[1], d[1], d[0] * d[0]));
+        const double rinv = rsqrt(r2);
+        const double r = r2 * rinv;
+        double sn, cn;
+        sincos_cw64(P.k * r, &sn, &cn);
+        const double f = w * rinv * BC_INV_4PI;
         QpeTerms o;
-        qpe_terms(d, w, cre, cim, cs, ies, bet, P, o);
+        qpe_ordered(d, r, rinv * rinv, cn * f, sn * f, cre, cim, cs, ies, bet, P, o);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             a[c] += o.gd[c];
@@ -293,17 +368,17 @@ __global__ void __launch_bounds__(32 * SHS_WARPS) shape_singular(ShapeParams P) 
     double *at = P.acc + t * SH_ACC, *as = P.acc + s * SH_ACC;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        atomicAdd(at + c, a[c]);
-        atomicAdd(at + 3 + c, a[3 + c]);
-        atomicAdd(at + 6 + c, a[6 + c]);
-        atomicAdd(as + 10 + c, a[c]);
-        atomicAdd(as + 13 + c, a[9 + c]);
-        atomicAdd(as + 16 + c, a[12 + c]);
-        atomicAdd(as + 19 + c, a[15 + c]);
+        atomicAdd(at + c, -a[c]);
+        atomicAdd(at + 3 + c, -a[3 + c]);
+        atomicAdd(at + 6 + c, -a[6 + c]);
+        atomicAdd(as + c, a[c]);
+        atomicAdd(as + 3 + c, a[9 + c]);
+        atomicAdd(as + 6 + c, a[12 + c]);
+        atomicAdd(as + 9 + c, a[15 + c]);
     }
-    atomicAdd(at + 9, a[18]);
-    atomicAdd(as + 22, a[19]);
-    atomicAdd(as + 23, a[20]);
+    atomicAdd(at + 12, a[18] / gt.ie);
+    atomicAdd(as + 12, a[19]);
+    atomicAdd(as + 13, a[20]);
 }
 
 // Vertex gradient of one element from "trial-type" sums: sum of a gradient
@@ -347,19 +422,14 @@ __global__ void __launch_bounds__(128) shape_finish(ShapeParams P, QuadRule rule
             const double2 l = P.lam[e], ph = P.phi[e];
             double go[3][3];
 #pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                go[0][c] = -(a[c] - a[3 + c] - a[6 + c]);
-                go[1][c] = -a[3 + c];
-                go[2][c] = -a[6 + c];
-            }
+            for (int v = 0; v < 3; ++v) go[v][0] = go[v][1] = go[v][2] = 0.0;
             const double idc = (l.x * ph.x + l.y * ph.y) * P.ident * 0.5;  // identity: A_ee += ident ie_e / 2
-            const double cie = a[9] / g.ie + a[22] + idc;
-            trial_chain(g, di, a + 10, a + 13, a + 16, a + 19, cie, go);
+            trial_chain(g, di, a, a + 3, a + 6, a + 9, a[12] + idc, go);
 #pragma unroll
             for (int v = 0; v < 3; ++v)
 #pragma unroll
                 for (int c = 0; c < 3; ++c) gv[v][c] = P.scale_op * go[v][c];
-            kloc = P.scale_op * a[23];
+            kloc = P.scale_op * a[13];
         }
 
         if (P.scale_ff != 0.0 && P.ndir > 0) {
@@ -562,7 +632,11 @@ static int shape_setup(const bemppcuda_shape_args *a, ShapeParams &P, QuadRule &
     P.woff = a->weights_offsets;
     P.npts = a->npoints;
     P.ndir = a->ndirections;
-    P.pad = 0;
+    {
+        // |k| (R_i + R_j) bounds the phase offset k (r - r_c) of every regular pair
+        const double theta = fabs(a->k) * a->phase_radius;
+        P.phase_class = a->phase_radius > 0.0 ? (theta <= 0.5 ? 2 : (theta <= 1.0 ? 1 : 0)) : 0;
+    }
     P.dirs = a->directions;
     P.ff_beta = a->ff_dlp_coeff;
     P.ff_eta_re = a->ff_eta[0];
@@ -654,7 +728,12 @@ int bemppcuda_shape_adjoint_dp0(const bemppcuda_shape_args *a, void *stream) {
             return BEMPPCUDA_ERR_UNSUPPORTED;
         }
         dim3 grid((unsigned)((P.ne + SH_THREADS - 1) / SH_THREADS), (unsigned)by);
-        shape_regular<<<grid, SH_THREADS, 0, st>>>(P, rule);
+        if (P.phase_class == 2)
+            shape_regular<2><<<grid, SH_THREADS, 0, st>>>(P, rule);
+        else if (P.phase_class == 1)
+            shape_regular<1><<<grid, SH_THREADS, 0, st>>>(P, rule);
+        else
+            shape_regular<0><<<grid, SH_THREADS, 0, st>>>(P, rule);
         rc = bc_check_launch("shape_adjoint_dp0 regular pairs");
         if (rc) return rc;
         if (P.npairs > 0) {

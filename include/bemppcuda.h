@@ -331,6 +331,9 @@ typedef struct {
     void *out;                         /* forward outputs: F (ndirections, nelements) row-major or b (nelements,) */
     void *workspace;                   /* >= bemppcuda_shape_workspace_bytes(nelements) */
     int64_t workspace_bytes;
+    double phase_radius;               /* 2 x largest centroid-to-vertex distance, or 0 (unknown): when
+                                          |k| * phase_radius <= 1 the phase offset k (r - r_c) of the
+                                          regular pairs needs no range reduction */
 } bemppcuda_shape_args;
 
 int64_t bemppcuda_shape_workspace_bytes(int64_t nelements);
