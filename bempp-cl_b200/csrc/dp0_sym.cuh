@@ -323,6 +323,7 @@ __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm,
 #pragma unroll
             for (int j = 0; j < NP; ++j) A[j] = fma2(D2d, yz[j], fma2(D1d, yyy[j], fma2(D0d, yx[j], yy2[j])));
             float2 s0r = b2(0.f), s0i = b2(0.f), ur = b2(0.f), ui = b2(0.f), vr = b2(0.f), vi = b2(0.f);
+#pragma unroll 2
             for (int p = 0; p < NQ6; ++p) {
                 const float4 m = sb.m[tt][p];
                 const float Bp = fmaf(D2f, m.z, fmaf(D1f, m.y, fmaf(D0f, m.x, m.w)));

@@ -237,8 +237,12 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_dp0_fp64_sym(RegParams pr
     regular_dp0_fp64_sym_tile<K, PHC>(prm, rule, blockIdx.x, t0, DP0_TCHUNK, sb);
 }
 
+#ifndef BC_MSYM_MIN_BLOCKS
+#define BC_MSYM_MIN_BLOCKS 3
+#endif
+
 template <int K, int PHC>
-__global__ void __launch_bounds__(DP0_THREADS, 3) regular_dp0_mixed_sym(RegParams prm, QuadRule rule) {
+__global__ void __launch_bounds__(DP0_THREADS, BC_MSYM_MIN_BLOCKS) regular_dp0_mixed_sym(RegParams prm, QuadRule rule) {
     const int64_t t0 = (int64_t)blockIdx.y * DP0_TCHUNK;
     if (t0 >= ((int64_t)blockIdx.x + 1) * DP0_THREADS) return;
     __shared__ TestBlock32p sb;
