@@ -26,33 +26,45 @@ import numpy as _np
 import torch as _torch
 
 
-def _norm(v):
-    return float(_torch.linalg.vector_norm(v).item())
+def _norm(v, allreduce=None):
+    if allreduce is None:
+        return float(_torch.linalg.vector_norm(v).item())
+    sq = (v.real.square().sum() + v.imag.square().sum()) if v.is_complex() else v.square().sum()
+    return float(_torch.sqrt(allreduce(sq.reshape(1).to(_torch.float64)))[0].item())
 
 
-def gmres_tensor(matvec, b, x0=None, tol=1e-5, restart=None, maxiter=None, callback=None):
+def gmres_tensor(matvec, b, x0=None, tol=1e-5, restart=None, maxiter=None, callback=None, allreduce=None,
+                 global_size=None):
     """Solve A x = b for one right-hand side; return (x, info, residuals, iterations).
 
     ``matvec(v)`` returns A v for a device vector of b's dtype.  ``info`` is 0
     on convergence, else the number of iterations done (scipy convention).
+
+    Distributed vectors: when every rank holds a block of rows of b and of the
+    iterate, ``allreduce(t)`` must return the sum of ``t`` over the ranks (one
+    all-reduce per orthogonalisation step and per norm) and ``matvec`` maps
+    the local block of v to the local block of A v (gathering what it needs);
+    ``global_size`` caps the restart length.  The small Hessenberg system is
+    replicated, so every rank takes the same steps.
     """
-    n = b.shape[0]
+    n = b.shape[0] if global_size is None else int(global_size)
     restart = min(restart or 100, n)
     maxiter = maxiter or 10 * n
     dtype = b.dtype
+    red = allreduce if allreduce is not None else (lambda t: t)
     x = _torch.zeros_like(b) if x0 is None else x0.clone()
-    bnorm = _norm(b)
+    bnorm = _norm(b, allreduce)
     residuals = []
     if bnorm == 0.0:
         return x, 0, [0.0], 0
     r = b - matvec(x) if x0 is not None else b.clone()
-    beta = _norm(r)
+    beta = _norm(r, allreduce)
     residuals.append(beta / bnorm)
     iterations = 0
     while True:
         if beta <= tol * bnorm:
             return x, 0, residuals, iterations
-        V = _torch.empty((restart + 1, n), dtype=dtype, device=b.device)
+        V = _torch.empty((restart + 1, b.shape[0]), dtype=dtype, device=b.device)
         V[0] = r / beta
         H = _np.zeros((restart + 1, restart), dtype=_np.complex128)
         cs = _np.zeros(restart, dtype=_np.complex128)
@@ -64,12 +76,12 @@ def gmres_tensor(matvec, b, x0=None, tol=1e-5, restart=None, maxiter=None, callb
         for j in range(restart):
             w = matvec(V[j])
             basis = V[: j + 1]
-            h = _torch.mv(basis.conj(), w)
+            h = red(_torch.mv(basis.conj(), w))
             w = w - _torch.mv(basis.transpose(0, 1), h)
-            h2 = _torch.mv(basis.conj(), w)
+            h2 = red(_torch.mv(basis.conj(), w))
             w = w - _torch.mv(basis.transpose(0, 1), h2)
             h = (h + h2).to(_torch.complex128).cpu().numpy()
-            hn = _norm(w)
+            hn = _norm(w, allreduce)
             if hn > 0.0:
                 V[j + 1] = w / hn
             col = _np.zeros(restart + 1, dtype=_np.complex128)
@@ -114,7 +126,7 @@ def gmres_tensor(matvec, b, x0=None, tol=1e-5, restart=None, maxiter=None, callb
         if iterations >= maxiter:
             return x, iterations, residuals, iterations
         r = b - matvec(x)
-        beta = _norm(r)
+        beta = _norm(r, allreduce)
 
 
 def gmres_block(matmat, B, tol=1e-5, restart=None, maxiter=None):
