@@ -23,6 +23,10 @@ pairs + Sauter-Schwab singular pairs + identity), matrix resident in HBM.
   L5 sphere (k = 6) with respect to all vertex coordinates and k, with the
   adjoint-kernel cost relative to one forward assembly and a central
   difference check on 20 coordinates.
+* ``breadth``: FP64 throughput of the other operator families on their
+  configurations (Laplace DP0 L4 with its matvec; Helmholtz P1 SLP / DLP /
+  ADLP / hypersingular L5, k = 5; Maxwell EFIE / MFIE RWG-SNC L4, k = 2;
+  Helmholtz potential at 10 000 points), each beside the oracle on the host.
 * ``batch``: 64 DP0 Helmholtz single-layer problems on seeded ellipsoids
   (regular_sphere(3..5) scaled per axis, k ~ U[1, 16]) assembled in one
   persistent launch per precision after autotuning, then replayed as a CUDA
@@ -74,6 +78,7 @@ def parse():
     ap.add_argument("--skip-batch", action="store_true")
     ap.add_argument("--skip-shape", action="store_true")
     ap.add_argument("--skip-fd", action="store_true")
+    ap.add_argument("--skip-breadth", action="store_true")
     ap.add_argument("--shape-level", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time per baseline sample")
     return ap.parse_args()
@@ -327,6 +332,10 @@ def gpu_arm(args, world, rank, local):
         del out
         torch.cuda.empty_cache()
         batch = batch_measure(args, torch, world, rank, dist)
+    breadth = None
+    if not args.skip_breadth and world == 1:
+        torch.cuda.empty_cache()
+        breadth = breadth_measure(args, torch)
     shape = None
     if not args.skip_shape and world == 1:
         torch.cuda.empty_cache()
@@ -370,6 +379,8 @@ def gpu_arm(args, world, rank, local):
         line["batch"] = batch
     if shape is not None:
         line["shape_gradient"] = shape
+    if breadth is not None:
+        line["breadth"] = breadth
     return line
 
 
@@ -591,6 +602,140 @@ def shape_measure(args, torch):
                            "max_rel_err": float(np.max(np.abs(ad - fd) / np.abs(fd))),
                            "k_rel_err": float(abs(kgrad.item() - fdk) / abs(fdk))}
     return res
+
+
+BREADTH = [
+    # (name, factory path, domain space, dual space, level, wavenumber)
+    ("laplace.single_layer dp0", "laplace.single_layer", ("DP", 0), ("DP", 0), 4, None),
+    ("helmholtz.single_layer p1", "helmholtz.single_layer", ("P", 1), ("P", 1), 5, 5.0),
+    ("helmholtz.double_layer p1", "helmholtz.double_layer", ("P", 1), ("P", 1), 5, 5.0),
+    ("helmholtz.adjoint_double_layer p1", "helmholtz.adjoint_double_layer", ("P", 1), ("P", 1), 5, 5.0),
+    ("helmholtz.hypersingular p1", "helmholtz.hypersingular", ("P", 1), ("P", 1), 5, 5.0),
+    ("maxwell.electric_field rwg/snc", "maxwell.electric_field", ("RWG", 0), ("SNC", 0), 4, 2.0),
+    ("maxwell.magnetic_field rwg/snc", "maxwell.magnetic_field", ("RWG", 0), ("SNC", 0), 4, 2.0),
+]
+
+
+def breadth_measure(args, torch):
+    """FP64 throughput of the other operator families (dense weak form through the operator API).
+
+    GPU: CUDA events around the full assembly (regular + singular passes) of
+    each operator on its configuration, inputs resident.  CPU: the oracle on
+    the same operator one level coarser (4x fewer elements), with all host
+    cores, scaled to the measured level by the number of element pairs (x16);
+    the singular pairs grow only 4x, so the scaled CPU time is an upper bound.
+    Potential: 10 000 points in the shell 1.5 < r < 3 from complex N(0,1) P1
+    coefficients on the level-5 sphere.
+    """
+    from bempp_cuda import operators
+    from bempp_cuda.quadrature import SingularPairs, triangle_rule
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+
+    from oracle import oracle as orc
+
+    grids = {}
+
+    def grid_of(level):
+        if level not in grids:
+            grids[level] = regular_sphere(level)
+        return grids[level]
+
+    def factory(path):
+        obj = operators.boundary
+        for part in path.split("."):
+            obj = getattr(obj, part)
+        return obj
+
+    def build(path, dsp, tsp, level, k):
+        g = grid_of(level)
+        dom = function_space(g, *dsp)
+        dual = function_space(g, *tsp)
+        f = factory(path)
+        return (f(dom, dom, dual) if k is None else f(dom, dom, dual, k)), dom, dual
+
+    out = []
+    for name, path, dsp, tsp, level, k in BREADTH:
+        op, dom, dual = build(path, dsp, tsp, level, k)
+        op._assemble()  # uploads and warms
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(max(args.steps, 1)):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            mat = op._assemble()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            del mat
+        rows, cols = dual.global_dof_count, dom.global_dof_count
+        entry = {"operator": name, "level": level, "k": k, "shape": [rows, cols],
+                 "gpu_ms": float(np.median(ms)), "gpu_entries_per_s": rows * cols / (np.median(ms) * 1e-3)}
+        if not args.skip_cpu:
+            op_c, dom_c, dual_c = build(path, dsp, tsp, level - 1, k)
+            d = op_c.descriptor
+            qp, qw = triangle_rule(4)
+            rule = SingularPairs(dom_c.grid, 4, dual_c.support, dom_c.support).arrays()
+            t0 = time.perf_counter()
+            orc.assemble_dense(d.kernel_type, d.assembly_type, d.options, d.is_complex, dom_c, dual_c, qp, qw, rule)
+            tc = (time.perf_counter() - t0) * 16.0
+            entry["cpu_s_scaled"] = tc
+            entry["cpu_entries_per_s"] = rows * cols / tc
+            entry["gpu_over_cpu"] = entry["gpu_entries_per_s"] / entry["cpu_entries_per_s"]
+        if name.startswith("laplace"):
+            # C1 matvec: HBM-bound GEMV on the resident matrix
+            mat = op._assemble()
+            x = torch.as_tensor(np.random.default_rng(0).standard_normal(cols), device="cuda")
+            for _ in range(3):
+                mat @ x
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(20):
+                mat @ x
+            e1.record()
+            torch.cuda.synchronize()
+            entry["matvec_us"] = e0.elapsed_time(e1) * 1e3 / 20
+            entry["matvec_note"] = "2048^2 f64 = 33.5 MB, resident in the 126 MB L2 between calls"
+            del mat
+        out.append(entry)
+        torch.cuda.empty_cache()
+
+    # potential: 10 000 shell points, P1 coefficients, k = 5
+    g = grid_of(5)
+    sp = function_space(g, "P", 1)
+    rng = np.random.default_rng(1)
+    dirs = rng.standard_normal((3, 10000))
+    dirs /= np.linalg.norm(dirs, axis=0)
+    pts = dirs * (1.5**3 + rng.random(10000) * (3.0**3 - 1.5**3)) ** (1.0 / 3.0)
+    coeffs = rng.standard_normal(sp.global_dof_count) + 1j * rng.standard_normal(sp.global_dof_count)
+    pot = operators.potential.helmholtz.single_layer(sp, pts, 5.0)
+    pot.evaluate_device(coeffs)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(max(args.steps, 1)):
+        pot.evaluate_device(coeffs)
+    e1.record()
+    torch.cuda.synchronize()
+    pms = e0.elapsed_time(e1) / max(args.steps, 1)
+    qpe = 10000 * g.number_of_elements * 6
+    pentry = {"operator": "potential.helmholtz.single_layer p1", "level": 5, "k": 5.0, "points": 10000,
+              "gpu_ms": pms, "gpu_qpe_per_s": qpe / (pms * 1e-3),
+              "note": "includes the host map_to_full_grid product and the coefficient upload"}
+    if not args.skip_cpu:
+        qp, qw = triangle_rule(4)
+        d = pot.descriptor
+        t0 = time.perf_counter()
+        orc.evaluate_potential(d.kernel_type, d.assembly_type, d.options, sp, pts[:, :1000], coeffs, qp, qw)
+        tc = (time.perf_counter() - t0) * 10.0
+        pentry["cpu_s_scaled"] = tc
+        pentry["gpu_over_cpu"] = tc / (pms * 1e-3)
+    out.append(pentry)
+    return out
 
 
 def solve_measure_distributed(args, torch, grid, domain, a_local, world, rank, dist):
