@@ -210,6 +210,11 @@ def measure_fma_peaks(torch):
     return out
 
 
+def traffic_estimate(rows, cols):
+    """DRAM bytes per regular launch: 1.054e9 B measured at 8192^2 (ncu), scaled by the entries."""
+    return 1.054e9 * (rows * cols) / 8192.0**2
+
+
 def gpu_arm(args, world, rank, local):
     import torch
 
@@ -313,9 +318,16 @@ def gpu_arm(args, world, rank, local):
     flops = qpe * FLOPS_PER_QPE["helmholtz_combined_field"]
     achieved = flops / (regmx * 1e-3) / 1e12
     roof = {"bound": "fp32", "achieved": achieved, "peak": peaks["fp32"], "unit": "TFLOP/s",
-            "frac": achieved / peaks["fp32"], "traffic": None,
-            "kernel": "regular_dp0<HELMHOLTZ_COMBINED, MIXED>", "kernel_ms": regmx,
+            "frac": achieved / peaks["fp32"], "traffic": traffic_estimate(rows, cols),
+            "kernel": "regular_dp0_mixed_sym<HELMHOLTZ_COMBINED>" if rows == cols else
+                      "regular_dp0_mixed2<HELMHOLTZ_COMBINED>", "kernel_ms": regmx,
             "flops_per_qpe": FLOPS_PER_QPE["helmholtz_combined_field"], "qpe_per_launch": qpe,
+            "flops_convention": "algorithmic flops of evaluating every entry on its own (the reference's "
+                                "work); the symmetric sweep evaluates each point pair once for A_ij and A_ji, "
+                                "so the hardware evaluates qpe_per_launch / 2 point pairs",
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the same kernel at "
+                              "regular_sphere(5) (profiles/regular_dp0_symmetric_combined_l5.md), scaled by "
+                              "the entry count; the output write is the whole traffic",
             "peak_source": "bemppcuda_fma_probe, measured in this run"}
     if fp64 is not None:
         a64 = flops / (fp64["regular_ms"] * 1e-3) / 1e12
