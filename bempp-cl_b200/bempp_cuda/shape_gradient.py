@@ -66,22 +66,36 @@ class DeviceGeometry(object):
 
 
 class ScatteringState(object):
-    """What the backward pass needs from one forward evaluation."""
+    """What the backward pass needs from one forward evaluation.
 
-    def __init__(self, geometry, lu, pivots, phi, u, farfield):
+    Holds either the LU factors (``lu``, ``pivots``) or, for the iterative
+    solver, the matrix itself (``matrix``)."""
+
+    def __init__(self, geometry, lu, pivots, phi, u, farfield, matrix=None, iterations=None):
         self.geometry = geometry
         self.lu = lu
         self.pivots = pivots
         self.phi = phi
         self.u = u
         self.farfield = farfield
+        self.matrix = matrix
+        self.iterations = iterations
 
 
 class FarFieldObjective(object):
     """J(vertices, k) = sum_j |u_inf(d_j)|^2 for a grid's topology (elements fixed)."""
 
-    def __init__(self, grid, directions=None, incident=(0.0, 0.0, 1.0), parameters=None):
+    def __init__(self, grid, directions=None, incident=(0.0, 0.0, 1.0), parameters=None, solver="lu", tol=1e-12):
+        """``solver``: "lu" (dense complex128 LU on the device, factors reused for
+        the adjoint solve), "lu32" (complex64 LU, refined with complex128
+        residuals b - A x of the FP64 matrix until ||b - A x|| <= tol ||b||; the
+        same factors and refinement for the adjoint) or "gmres" (device GMRES on
+        the resident matrix to relative residual ``tol`` for both solves)."""
         require_cuda()
+        if solver not in ("lu", "lu32", "gmres"):
+            raise ValueError("solver must be 'lu', 'lu32' or 'gmres'")
+        self.solver = solver
+        self.tol = float(tol)
         self.grid = grid
         self.parameters = parameters or Parameters()
         if int(self.parameters.quadrature.regular) != 4:
@@ -169,25 +183,64 @@ class FarFieldObjective(object):
         return f
 
     # ------------------------------------------------------------------ objective and gradient
-    def evaluate(self, vertices, k, keep=False):
+    def _gmres(self, matvec, rhs):
+        from .linalg import gmres_tensor
+
+        x, info, res, its = gmres_tensor(matvec, rhs, tol=self.tol, restart=300, maxiter=3000)
+        if info != 0:
+            raise RuntimeError("GMRES did not reach %g in %d iterations (last residual %g)" % (self.tol, its, res[-1]))
+        return x, its
+
+    def _refine(self, lu, pivots, matvec, rhs, adjoint=False, max_steps=20):
+        """Solve with complex64 factors and complex128 residuals; returns (x, steps)."""
+        bnorm = float(_torch.linalg.vector_norm(rhs).item())
+        x = _torch.zeros_like(rhs)
+        r = rhs
+        for step in range(1, max_steps + 1):
+            d = _torch.linalg.lu_solve(lu, pivots, r.to(_torch.complex64).unsqueeze(1), adjoint=adjoint).squeeze(1)
+            x = x + d.to(_torch.complex128)
+            r = rhs - matvec(x)
+            if float(_torch.linalg.vector_norm(r).item()) <= self.tol * bnorm:
+                return x, step
+        raise RuntimeError("refinement did not reach %g in %d steps" % (self.tol, max_steps))
+
+    def evaluate(self, vertices, k, keep=False, solver=None):
         """J as a 0-d device tensor (and the state for ``gradient`` when ``keep``)."""
+        solver = solver or self.solver
         geometry = self.geometry(vertices)
         a = self.assemble(geometry, k)
-        lu, pivots = _torch.linalg.lu_factor(a)
-        del a
         b = self.rhs(geometry, k)
-        phi = _torch.linalg.lu_solve(lu, pivots, b.unsqueeze(1)).squeeze(1)
+        lu = pivots = matrix = its = None
+        if solver == "lu":
+            lu, pivots = _torch.linalg.lu_factor(a)
+            del a
+            phi = _torch.linalg.lu_solve(lu, pivots, b.unsqueeze(1)).squeeze(1)
+        elif solver == "lu32":
+            matrix = a
+            lu, pivots = _torch.linalg.lu_factor(a.to(_torch.complex64))
+            phi, its = self._refine(lu, pivots, lambda v: _torch.mv(matrix, v), b)
+        else:
+            matrix = a
+            phi, its = self._gmres(lambda v: _torch.mv(matrix, v), b)
         farfield = self.farfield_matrix(geometry, k)
         u = farfield @ phi
         value = (u.real ** 2 + u.imag ** 2).sum()
         if keep:
-            return value, ScatteringState(geometry, lu, pivots, phi, u, farfield)
+            return value, ScatteringState(geometry, lu, pivots, phi, u, farfield, matrix, its)
         return value
 
     def adjoint(self, state):
-        """lambda with A^H lambda = F^H u."""
+        """lambda with A^H lambda = F^H u (same solver as the forward solve)."""
         rhs = state.farfield.conj().transpose(0, 1) @ state.u
-        return _torch.linalg.lu_solve(state.lu, state.pivots, rhs.unsqueeze(1), adjoint=True).squeeze(1)
+        if state.lu is not None and state.matrix is not None:  # complex64 factors, refined
+            ah = state.matrix.mH
+            lam, steps = self._refine(state.lu, state.pivots, lambda v: _torch.mv(ah, v), rhs, adjoint=True)
+            return lam
+        if state.lu is not None:
+            return _torch.linalg.lu_solve(state.lu, state.pivots, rhs.unsqueeze(1), adjoint=True).squeeze(1)
+        ah = state.matrix.mH
+        lam, its = self._gmres(lambda v: _torch.mv(ah, v), rhs)
+        return lam
 
     def gradient(self, state, k, lam=None, scales=(-2.0, 2.0, 2.0)):
         """(dJ/dvertices (nv, 3), dJ/dk) from a kept forward state."""

@@ -168,3 +168,36 @@ def test_adjoint_rejects_missing_vectors():
     assert rc == _lib.ERR_INVALID and "6-point" in _lib.last_error()
     torch.cuda.synchronize()
     assert not vg.any()
+
+
+def test_gmres_solver_gives_the_lu_gradient():
+    from bempp_cuda.shape_gradient import FarFieldObjective, fibonacci_directions
+    from bempp_cuda.shapes import perturbed_sphere
+
+    grid, _ = perturbed_sphere(3, seed=5)
+    lu = FarFieldObjective(grid, directions=fibonacci_directions(32))
+    it = FarFieldObjective(grid, directions=fibonacci_directions(32), solver="gmres", tol=1e-13)
+    v1, s1 = lu.evaluate(lu.vertices, 6.0, keep=True)
+    v2, s2 = it.evaluate(it.vertices, 6.0, keep=True)
+    g1, k1 = lu.gradient(s1, 6.0)
+    g2, k2 = it.gradient(s2, 6.0)
+    assert abs(v1.item() - v2.item()) <= 1e-11 * v1.item()
+    assert (torch.linalg.norm(g1 - g2) / torch.linalg.norm(g1)).item() <= 1e-9
+    assert abs(k1.item() - k2.item()) <= 1e-9 * abs(k1.item())
+    assert s2.iterations is not None and s2.iterations > 0
+
+
+def test_lu32_refined_solver_gives_the_lu_gradient():
+    from bempp_cuda.shape_gradient import FarFieldObjective, fibonacci_directions
+    from bempp_cuda.shapes import perturbed_sphere
+
+    grid, _ = perturbed_sphere(3, seed=6)
+    lu = FarFieldObjective(grid, directions=fibonacci_directions(32))
+    lo = FarFieldObjective(grid, directions=fibonacci_directions(32), solver="lu32", tol=1e-13)
+    v1, s1 = lu.evaluate(lu.vertices, 6.0, keep=True)
+    v2, s2 = lo.evaluate(lo.vertices, 6.0, keep=True)
+    g1, k1 = lu.gradient(s1, 6.0)
+    g2, k2 = lo.gradient(s2, 6.0)
+    assert abs(v1.item() - v2.item()) <= 1e-11 * v1.item()
+    assert (torch.linalg.norm(g1 - g2) / torch.linalg.norm(g1)).item() <= 1e-9
+    assert abs(k1.item() - k2.item()) <= 1e-9 * abs(k1.item())
