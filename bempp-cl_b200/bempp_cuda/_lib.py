@@ -129,6 +129,7 @@ class SingularArgs(_ct.Structure):
         ("dense", _vp),
         ("ld", _i64),
         ("diag_shift", _ct.c_double),
+        ("phase_radius", _ct.c_double),
     ]
 
 

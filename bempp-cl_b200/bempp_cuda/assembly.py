@@ -146,6 +146,7 @@ def singular_into_dense(result, descriptor, domain, dual_to_range, parameters, d
     args.dense = ptr(result)
     args.ld = result.stride(0)
     args.diag_shift = float(diag_shift)
+    args.phase_radius = 1.0001 * 2.0 * (geometry or device_grid(grid)).radius
     _lib.check(_lib.load().bemppcuda_assemble_singular(args, stream or current_stream()))
     return result
 

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include "../../include/bemppcuda.h"
+#include "fastmath.cuh"
 
 #define BC_INV_4PI (0.079577471545947667884441881686257181017229822870228)
 
@@ -102,7 +103,8 @@ __device__ __forceinline__ void scalar_shape(int nshape, double x, double y, dou
 }
 
 // Green's functions in FP64 (numba_kernels.py:176-551).  x: test point,
-// y: trial point, nx / ny: test / trial normals, p: parameters.
+// y: trial point, nx / ny: test / trial normals, p: parameters.  Sine and
+// cosine pairs come from sincos_cw64 (fastmath.cuh).
 template <int K>
 __device__ __forceinline__ cplx greens(const double x[3], const double y[3], const double nx[3], const double ny[3],
                                        const double p[4]) {
@@ -120,7 +122,7 @@ __device__ __forceinline__ cplx greens(const double x[3], const double y[3], con
         return {dot * BC_INV_4PI * rinv * rinv * rinv, 0.0};
     } else if (K == BEMPPCUDA_HELMHOLTZ_SLP) {
         double s, c;
-        sincos(p[0] * r, &s, &c);
+        sincos_cw64(p[0] * r, &s, &c);
         double f = BC_INV_4PI * rinv;
         if (p[1] != 0.0) f *= exp(-p[1] * r);
         return {c * f, s * f};
@@ -129,7 +131,7 @@ __device__ __forceinline__ cplx greens(const double x[3], const double y[3], con
                                                     : -fma(d2, nx[2], fma(d1, nx[1], d0 * nx[0]));
         double lg = dot * BC_INV_4PI * rinv * rinv * rinv;
         double s, c;
-        sincos(p[0] * r, &s, &c);
+        sincos_cw64(p[0] * r, &s, &c);
         if (p[1] != 0.0) lg *= exp(-p[1] * r);
         double fr = c * lg, fi = s * lg;
         double a = -1.0 - p[1] * r, b = p[0] * r;
@@ -138,7 +140,7 @@ __device__ __forceinline__ cplx greens(const double x[3], const double y[3], con
         // DLP + eta SLP: e^{ikr}/(4 pi r) [ (ikr - 1)(y-x).n_y / r^2 + eta ]
         double dot = fma(d2, ny[2], fma(d1, ny[1], d0 * ny[0]));
         double s, c;
-        sincos(p[0] * r, &s, &c);
+        sincos_cw64(p[0] * r, &s, &c);
         double f = BC_INV_4PI * rinv;
         if (p[1] != 0.0) f *= exp(-p[1] * r);
         const double g = dot * rinv * rinv;
@@ -156,13 +158,13 @@ __device__ __forceinline__ cplx greens(const double x[3], const double y[3], con
     } else if (K == BEMPPCUDA_FARFIELD_SLP) {
         double dot = fma(x[2], y[2], fma(x[1], y[1], x[0] * y[0]));
         double s, c;
-        sincos(-p[0] * dot, &s, &c);
+        sincos_cw64(-p[0] * dot, &s, &c);
         return {BC_INV_4PI * c, BC_INV_4PI * s};
     } else {  // BEMPPCUDA_FARFIELD_DLP
         double dot = fma(x[2], y[2], fma(x[1], y[1], x[0] * y[0]));
         double factor = -p[0] * fma(x[2], ny[2], fma(x[1], ny[1], x[0] * ny[0]));
         double s, c;
-        sincos(-p[0] * dot, &s, &c);
+        sincos_cw64(-p[0] * dot, &s, &c);
         return {-factor * BC_INV_4PI * s, factor * BC_INV_4PI * c};
     }
 }

@@ -156,6 +156,9 @@ typedef struct {
     int64_t ld;        /* row stride of dense */
     double diag_shift; /* added to the coincident entries of a DP0 dense output, times the
                           integration element / 2 (the -1/2 I term of a combined-field form) */
+    double phase_radius; /* 2 x largest centroid-to-vertex distance of the grid, or 0 (unknown):
+                            when |k| * phase_radius <= 1 the DP0 path factors exp(ikr) about the
+                            centroid distance (|r - r_c| <= R_i + R_j holds for adjacent pairs too) */
 } bemppcuda_singular_args;
 
 /* Potential / far-field evaluation (numba_kernels.py:1788-1849, 2281-2570). */
