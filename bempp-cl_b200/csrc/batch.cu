@@ -10,6 +10,7 @@
 #include <cstring>
 
 #include "dp0_sym.cuh"
+#include "singular_dp0.cuh"
 
 namespace bc {
 
@@ -163,26 +164,39 @@ __global__ void __launch_bounds__(32 * SB_WARPS) singular_batch(const BatchDev *
     Geom gt, gs;
     load_geom(prm.tg, prm.tne, t, 1.0, gt);
     load_geom(prm.tg, prm.tne, s, 1.0, gs);
-    double are = 0.0, aim = 0.0;
+    double vr = 0.0, vi = 0.0;
+    const double2 *tp = reinterpret_cast<const double2 *>(tab.tp), *sp = reinterpret_cast<const double2 *>(tab.sp);
     const int64_t toff = tab.toff[k], soff = tab.soff[k], woff = tab.woff[k];
     const int n = (int)tab.npts[k];
-    for (int m = lane; m < n; m += 32) {
-        const double2 tpm = reinterpret_cast<const double2 *>(tab.tp)[toff + m];
-        const double2 spm = reinterpret_cast<const double2 *>(tab.sp)[soff + m];
-        const double w = __ldg(tab.w + woff + m);
-        double x[3], y[3];
-        to_global(gt, tpm.x, tpm.y, x);
-        to_global(gs, spm.x, spm.y, y);
-        const cplx kv = greens<K>(x, y, gt.n, gs.n, prm.p);
-        are = fma(kv.re, w, are);
-        aim = fma(kv.im, w, aim);
+    if (P.ck) {
+        // complex wavenumber: Green's function at every point
+        double are = 0.0, aim = 0.0;
+        for (int m = lane; m < n; m += 32) {
+            const double2 tpm = tp[toff + m], spm = sp[soff + m];
+            const double w = __ldg(tab.w + woff + m);
+            double x[3], y[3];
+            to_global(gt, tpm.x, tpm.y, x);
+            to_global(gs, spm.x, spm.y, y);
+            const cplx kv = greens<K>(x, y, gt.n, gs.n, prm.p);
+            are = fma(kv.re, w, are);
+            aim = fma(kv.im, w, aim);
+        }
+        vr = warp_sum(are);
+        vi = warp_sum(aim);
+    } else {
+        if (P.phase_class == 2)
+            sing_dp0_value<K, 2>(prm.tg, prm.tne, t, s, gt, gs, prm.p, tp, sp, tab.w, toff, soff, woff, n, &vr, &vi);
+        else if (P.phase_class == 1)
+            sing_dp0_value<K, 1>(prm.tg, prm.tne, t, s, gt, gs, prm.p, tp, sp, tab.w, toff, soff, woff, n, &vr, &vi);
+        else
+            sing_dp0_value<K, 0>(prm.tg, prm.tne, t, s, gt, gs, prm.p, tp, sp, tab.w, toff, soff, woff, n, &vr, &vi);
+        vr *= BC_INV_4PI;
+        vi *= BC_INV_4PI;
     }
-    are = warp_sum(are);
-    aim = warp_sum(aim);
     if (lane == 0) {
         const double scale = gt.ie * gs.ie;
-        double vr = are * scale;
-        const double vi = aim * scale;
+        vr *= scale;
+        vi *= scale;
         if (t == s) vr += P.diag_shift * 0.5 * gt.ie;
         double2 *o = reinterpret_cast<double2 *>(prm.result) + t * prm.ld + s;
         const double2 old = *o;

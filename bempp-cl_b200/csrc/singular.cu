@@ -11,6 +11,7 @@
 // reductions.  Always FP64.  Output either to the flat per-pair value array
 // of the reference interface or scattered straight into a dense matrix.
 #include "common.cuh"
+#include "singular_dp0.cuh"
 
 namespace bc {
 
@@ -206,22 +207,9 @@ __global__ void __launch_bounds__(32 * SING_WARPS) singular_pairs(SingParams prm
     }
 }
 
-// DP0 scalar kernels (one shape function each side) with a real wavenumber:
-// the 3 x 3 local block reduces to one value, and exp(ikr) is factored about
-// the centroid distance r_c as in the regular DP0 kernels: for any x in
-// element i and y in element j, |r - r_c| <= R_i + R_j, so phase class PHC
-// (|k|(R_i + R_j) <= 1 or 1/2) bounds the per-point phase offset for adjacent
-// pairs as well.  One warp per pair, lanes over the points, two shuffle sums.
+// DP0 scalar kernels with a real wavenumber (singular_dp0.cuh).
 template <int K, int PHC>
 __global__ void __launch_bounds__(32 * SING_WARPS) singular_dp0(SingParams prm) {
-    constexpr bool HELM = (K == BEMPPCUDA_HELMHOLTZ_SLP || K == BEMPPCUDA_HELMHOLTZ_DLP ||
-                           K == BEMPPCUDA_HELMHOLTZ_ADLP || K == BEMPPCUDA_HELMHOLTZ_COMBINED);
-    constexpr bool SL = (K == BEMPPCUDA_LAPLACE_SLP || K == BEMPPCUDA_HELMHOLTZ_SLP ||
-                         K == BEMPPCUDA_HELMHOLTZ_COMBINED);
-    constexpr bool DL = (K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_HELMHOLTZ_DLP ||
-                         K == BEMPPCUDA_HELMHOLTZ_COMBINED);
-    constexpr bool AD = (K == BEMPPCUDA_LAPLACE_ADLP || K == BEMPPCUDA_HELMHOLTZ_ADLP);
-    constexpr bool PH = HELM && PHC > 0;
     const int lane = threadIdx.x & 31;
     const int64_t k = (int64_t)blockIdx.x * SING_WARPS + (threadIdx.x >> 5);
     if (k >= prm.npairs) return;
@@ -229,81 +217,11 @@ __global__ void __launch_bounds__(32 * SING_WARPS) singular_dp0(SingParams prm) 
     Geom gt, gs;
     load_geom(prm.g, prm.ne, t, prm.tnm ? (double)prm.tnm[t] : 1.0, gt);
     load_geom(prm.g, prm.ne, s, prm.snm ? (double)prm.snm[s] : 1.0, gs);
-    const double kr = prm.p[0];
-    double rc = 0.0;
-    if (PH) {
-        const double D0 = __ldg(prm.g + 22 * prm.ne + s) - __ldg(prm.g + 22 * prm.ne + t);
-        const double D1 = __ldg(prm.g + 23 * prm.ne + s) - __ldg(prm.g + 23 * prm.ne + t);
-        const double D2 = __ldg(prm.g + 24 * prm.ne + s) - __ldg(prm.g + 24 * prm.ne + t);
-        rc = sqrt(fma(D2, D2, fma(D1, D1, D0 * D0)));
-    }
-    const double *nv = AD ? gt.n : gs.n;
-    double s0r = 0.0, s0i = 0.0, s1r = 0.0, s1i = 0.0;
-    const int64_t toff = prm.toff[k], soff = prm.soff[k], woff = prm.woff[k];
-    const int n = (int)prm.npts[k];
-    for (int m = lane; m < n; m += 32) {
-        const double2 tpm = reinterpret_cast<const double2 *>(prm.tp)[toff + m];
-        const double2 spm = reinterpret_cast<const double2 *>(prm.sp)[soff + m];
-        const double w = __ldg(prm.w + woff + m);
-        double x[3], y[3];
-        to_global(gt, tpm.x, tpm.y, x);
-        to_global(gs, spm.x, spm.y, y);
-        const double d0 = y[0] - x[0], d1 = y[1] - x[1], d2 = y[2] - x[2];
-        const double r2 = fma(d2, d2, fma(d1, d1, d0 * d0));
-        const double rinv = rsqrt(r2);
-        const double f = w * rinv;
-        double dot = 0.0;
-        if (DL || AD) dot = (AD ? -1.0 : 1.0) * fma(d2, nv[2], fma(d1, nv[1], d0 * nv[0]));
-        if (!HELM) {
-            if (SL) s0r += f;
-            if (DL || AD) s1r = fma(f * dot, rinv * rinv, s1r);
-        } else {
-            const double r = r2 * rinv;
-            double sn, cs;
-            if (PH && PHC == 2)
-                sincos_half64(kr * (r - rc), &sn, &cs);
-            else if (PH)
-                sincos_small64(kr * (r - rc), &sn, &cs);
-            else
-                sincos_cw64(kr * r, &sn, &cs);
-            if (SL) {
-                s0r = fma(f, cs, s0r);
-                s0i = fma(f, sn, s0i);
-            }
-            if (DL || AD) {
-                // (ikr - 1) e^{ikr} (dot) / r^3 = g (-h1 + i h2), g = f dot / r
-                const double g = f * dot * rinv;
-                s1r = fma(g, fma(rinv, cs, kr * sn), s1r);
-                s1i = fma(g, fma(kr, cs, -rinv * sn), s1i);
-            }
-        }
-    }
-    s0r = warp_sum(s0r);
-    if (HELM) s0i = warp_sum(s0i);
-    if (DL || AD) {
-        s1r = warp_sum(s1r);
-        if (HELM) s1i = warp_sum(s1i);
-    }
+    double vr, vi;
+    sing_dp0_value<K, PHC>(prm.g, prm.ne, t, s, gt, gs, prm.p, reinterpret_cast<const double2 *>(prm.tp),
+                           reinterpret_cast<const double2 *>(prm.sp), prm.w, prm.toff[k], prm.soff[k],
+                           prm.woff[k], (int)prm.npts[k], &vr, &vi);
     if (lane != 0) return;
-    // kernel sum: SLP s0; Laplace DLP -s1r; Helmholtz DLP -s1r + i s1i; combined eta s0 + DLP
-    double vr = 0.0, vi = 0.0;
-    if (K == BEMPPCUDA_LAPLACE_SLP || K == BEMPPCUDA_HELMHOLTZ_SLP) {
-        vr = s0r;
-        vi = s0i;
-    } else if (K == BEMPPCUDA_HELMHOLTZ_COMBINED) {
-        vr = fma(prm.p[2], s0r, fma(-prm.p[3], s0i, -s1r));
-        vi = fma(prm.p[2], s0i, fma(prm.p[3], s0r, s1i));
-    } else {
-        vr = -s1r;
-        vi = HELM ? s1i : 0.0;
-    }
-    if (PH) {
-        double ps, pc;
-        sincos_cw64(kr * rc, &ps, &pc);
-        const double tr = vr * pc - vi * ps;
-        vi = fma(vr, ps, vi * pc);
-        vr = tr;
-    }
     const double scale = BC_INV_4PI * gt.ie * gs.ie;
     vr *= scale;
     vi *= scale;

@@ -1,0 +1,113 @@
+// Singular (adjacent) DP0 pairs of the scalar kernels with a real
+// wavenumber: the 3 x 3 local block reduces to one value, and exp(ikr) is
+// factored about the centroid distance r_c as in the regular DP0 kernels: for
+// any x in element i and y in element j, |r - r_c| <= R_i + R_j, so phase
+// class PHC (|k|(R_i + R_j) <= 1 or 1/2) bounds the per-point phase offset
+// for adjacent pairs as well.  One warp per pair, lanes over the points.
+// Used by the single-problem singular kernel and the batched one.
+#pragma once
+
+#include "common.cuh"
+
+namespace bc {
+
+template <int K>
+struct SingDp0Traits {
+    static constexpr bool helm = (K == BEMPPCUDA_HELMHOLTZ_SLP || K == BEMPPCUDA_HELMHOLTZ_DLP ||
+                                  K == BEMPPCUDA_HELMHOLTZ_ADLP || K == BEMPPCUDA_HELMHOLTZ_COMBINED);
+    static constexpr bool sl = (K == BEMPPCUDA_LAPLACE_SLP || K == BEMPPCUDA_HELMHOLTZ_SLP ||
+                                K == BEMPPCUDA_HELMHOLTZ_COMBINED);
+    static constexpr bool dl = (K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_HELMHOLTZ_DLP ||
+                                K == BEMPPCUDA_HELMHOLTZ_COMBINED);
+    static constexpr bool ad = (K == BEMPPCUDA_LAPLACE_ADLP || K == BEMPPCUDA_HELMHOLTZ_ADLP);
+};
+
+// Kernel sum of one adjacent pair over its Sauter-Schwab points, without the
+// integration elements and 1/(4 pi); every lane returns the warp total.
+// g: geometry record (for the centroids), t / s: the pair, p: kernel parameters.
+template <int K, int PHC>
+__device__ __forceinline__ void sing_dp0_value(const double *__restrict__ g, int64_t ne, int64_t t, int64_t s,
+                                               const Geom &gt, const Geom &gs, const double *p,
+                                               const double2 *__restrict__ tp, const double2 *__restrict__ sp,
+                                               const double *__restrict__ w, int64_t toff, int64_t soff,
+                                               int64_t woff, int n, double *vr_out, double *vi_out) {
+    using T = SingDp0Traits<K>;
+    constexpr bool PH = T::helm && PHC > 0;
+    const int lane = threadIdx.x & 31;
+    const double kr = p[0];
+    double rc = 0.0;
+    if (PH) {
+        const double D0 = __ldg(g + 22 * ne + s) - __ldg(g + 22 * ne + t);
+        const double D1 = __ldg(g + 23 * ne + s) - __ldg(g + 23 * ne + t);
+        const double D2 = __ldg(g + 24 * ne + s) - __ldg(g + 24 * ne + t);
+        rc = sqrt(fma(D2, D2, fma(D1, D1, D0 * D0)));
+    }
+    const double *nv = T::ad ? gt.n : gs.n;
+    double s0r = 0.0, s0i = 0.0, s1r = 0.0, s1i = 0.0;
+    for (int m = lane; m < n; m += 32) {
+        const double2 tpm = tp[toff + m];
+        const double2 spm = sp[soff + m];
+        const double wm = __ldg(w + woff + m);
+        double x[3], y[3];
+        to_global(gt, tpm.x, tpm.y, x);
+        to_global(gs, spm.x, spm.y, y);
+        const double d0 = y[0] - x[0], d1 = y[1] - x[1], d2 = y[2] - x[2];
+        const double r2 = fma(d2, d2, fma(d1, d1, d0 * d0));
+        const double rinv = rsqrt(r2);
+        const double f = wm * rinv;
+        double dot = 0.0;
+        if (T::dl || T::ad) dot = (T::ad ? -1.0 : 1.0) * fma(d2, nv[2], fma(d1, nv[1], d0 * nv[0]));
+        if (!T::helm) {
+            if (T::sl) s0r += f;
+            if (T::dl || T::ad) s1r = fma(f * dot, rinv * rinv, s1r);
+        } else {
+            const double r = r2 * rinv;
+            double sn, cs;
+            if (PH && PHC == 2)
+                sincos_half64(kr * (r - rc), &sn, &cs);
+            else if (PH)
+                sincos_small64(kr * (r - rc), &sn, &cs);
+            else
+                sincos_cw64(kr * r, &sn, &cs);
+            if (T::sl) {
+                s0r = fma(f, cs, s0r);
+                s0i = fma(f, sn, s0i);
+            }
+            if (T::dl || T::ad) {
+                // (ikr - 1) e^{ikr} (dot) / r^3 = g (-h1 + i h2), g = f dot / r
+                const double gg = f * dot * rinv;
+                s1r = fma(gg, fma(rinv, cs, kr * sn), s1r);
+                s1i = fma(gg, fma(kr, cs, -rinv * sn), s1i);
+            }
+        }
+    }
+    s0r = warp_sum(s0r);
+    if (T::helm) s0i = warp_sum(s0i);
+    if (T::dl || T::ad) {
+        s1r = warp_sum(s1r);
+        if (T::helm) s1i = warp_sum(s1i);
+    }
+    // SLP s0; Laplace DLP -s1r; Helmholtz DLP -s1r + i s1i; combined eta s0 + DLP
+    double vr = 0.0, vi = 0.0;
+    if (K == BEMPPCUDA_LAPLACE_SLP || K == BEMPPCUDA_HELMHOLTZ_SLP) {
+        vr = s0r;
+        vi = s0i;
+    } else if (K == BEMPPCUDA_HELMHOLTZ_COMBINED) {
+        vr = fma(p[2], s0r, fma(-p[3], s0i, -s1r));
+        vi = fma(p[2], s0i, fma(p[3], s0r, s1i));
+    } else {
+        vr = -s1r;
+        vi = T::helm ? s1i : 0.0;
+    }
+    if (PH) {
+        double ps, pc;
+        sincos_cw64(kr * rc, &ps, &pc);
+        const double tr = vr * pc - vi * ps;
+        vi = fma(vr, ps, vi * pc);
+        vr = tr;
+    }
+    *vr_out = vr;
+    *vi_out = vi;
+}
+
+}  // namespace bc

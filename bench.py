@@ -32,6 +32,8 @@ pairs + Sauter-Schwab singular pairs + identity), matrix resident in HBM.
   persistent launch per precision after autotuning, then replayed as a CUDA
   graph together with the 8-right-hand-side product of every problem; the
   same problems assembled one launch pair at a time give the unbatched time.
+  ``batch.many_small`` repeats this for 256 problems of 128 / 512 elements,
+  where separate launches cannot fill the GPU.
 
 Multi-GPU (torchrun): the rows (test elements) are split into one contiguous
 block per rank; each rank assembles its block with no collective (strong
@@ -344,6 +346,9 @@ def gpu_arm(args, world, rank, local):
         del out
         torch.cuda.empty_cache()
         batch = batch_measure(args, torch, world, rank, dist)
+        torch.cuda.empty_cache()
+        batch["many_small"] = batch_measure(args, torch, world, rank, dist, count=256, levels=(2, 3))
+        del batch["many_small"]["elements"]
     breadth = None
     if not args.skip_breadth and world == 1:
         torch.cuda.empty_cache()
@@ -423,8 +428,8 @@ def solve_measure(args, torch, grid, domain, a64, amx):
             "solution_rel_diff_vs_fp64": diff, "mixed_solution_residual_in_fp64_operator": res_true}
 
 
-def batch_measure(args, torch, world, rank, dist):
-    """64 DP0 Helmholtz SLP problems (ellipsoids L in {3,4,5}, k ~ U[1,16]) in one persistent launch.
+def batch_measure(args, torch, world, rank, dist, count=64, levels=(3, 4, 5)):
+    """``count`` DP0 Helmholtz SLP problems (ellipsoids L in ``levels``, k ~ U[1,16]) in one persistent launch.
 
     Each precision is autotuned, then one CUDA graph holding the batched
     assembly and the 8-right-hand-side products of every problem is replayed.
@@ -436,7 +441,7 @@ def batch_measure(args, torch, world, rank, dist):
     from bempp_cuda.batch import BatchAssembler, c4_problems
     from bempp_cuda.operators import Parameters
 
-    probs = c4_problems(64, seed=0)
+    probs = c4_problems(count, seed=0, levels=levels)
     from bempp_cuda.distributed import shard_problems
 
     mine = shard_problems([g.number_of_elements for g, _ in probs], world, rank)
