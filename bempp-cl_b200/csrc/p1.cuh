@@ -1,0 +1,228 @@
+// Regular pairs of scalar operators on linear (P1 / DP1) and mixed P0 / P1
+// spaces, 6-point rule, real wavenumber: the kernels of numba_kernels.py:980-1074
+// (default_scalar_regular_kernel) and the hypersingular ones of :1078-1467.
+//
+// One thread per trial element, 32 test elements staged in shared memory (as
+// the DP0 tiles).  Per test point p the trial sums
+//   T_j(p) = sum_q w_q K(x_p, y_q) psi_j(q)          (j < NS)
+// are formed first, then L_ij += w_p phi_i(p) T_j(p), so a point pair costs NS
+// complex FMAs instead of NT x NS.  Hypersingular operators reuse the single-
+// layer sums: with constant surface curls per element,
+//   L_ij = (curl_i . curl_j) S - c (n_t . n_s) M_ij,  S = sum_j T_j summed over p
+// (the P1 shape functions add up to 1), c = k^2 (Helmholtz), 0 (Laplace).
+// exp(ikr) is factored about the centroid distance as in the DP0 kernels.
+// The NT x NS block is added to the matrix with FP64 atomics (l2g, multipliers).
+#pragma once
+
+#include "dp0.cuh"
+
+namespace bc {
+
+constexpr int P1_TCHUNK = 32;
+
+struct TestBlockP1 {
+    double x[P1_TCHUNK][NQ6][3];
+    double n[P1_TCHUNK][3];
+    double c[P1_TCHUNK][3];
+    double curl[P1_TCHUNK][3][3];
+    double ie[P1_TCHUNK];
+    int v[P1_TCHUNK][3];
+};
+
+template <int ASM, int K, int NT, int NS, int PHC>
+__global__ void __launch_bounds__(DP0_THREADS) regular_p1(RegParams prm, QuadRule rule) {
+    constexpr bool HYP = (ASM == BEMPPCUDA_ASM_LAPLACE_HYP || ASM == BEMPPCUDA_ASM_HELM_HYP);
+    constexpr bool HELM = (K == BEMPPCUDA_HELMHOLTZ_SLP || K == BEMPPCUDA_HELMHOLTZ_DLP ||
+                           K == BEMPPCUDA_HELMHOLTZ_ADLP);
+    constexpr bool DL = (K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_HELMHOLTZ_DLP);
+    constexpr bool AD = (K == BEMPPCUDA_LAPLACE_ADLP || K == BEMPPCUDA_HELMHOLTZ_ADLP);
+    constexpr bool PH = HELM && PHC > 0;
+    __shared__ TestBlockP1 sb;
+
+    const int64_t t0 = (int64_t)blockIdx.y * P1_TCHUNK;
+    const int tcount = (int)min((int64_t)P1_TCHUNK, prm.ntest - t0);
+    for (int idx = threadIdx.x; idx < tcount; idx += blockDim.x) {
+        const int64_t t = prm.tsup[t0 + idx];
+        Geom g;
+        load_geom(prm.tg, prm.tne, t, prm.tnm ? (double)prm.tnm[t] : 1.0, g);
+        for (int p = 0; p < NQ6; ++p) to_global(g, rule.x[p], rule.y[p], sb.x[idx][p]);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            sb.n[idx][d] = g.n[d];
+            sb.c[idx][d] = __ldg(prm.tg + (22 + d) * prm.tne + t);
+            sb.v[idx][d] = __ldg(prm.tel + 3 * t + d);
+        }
+        if (HYP) {
+            double cu[3][3];
+            surface_curls(prm.tg, prm.tne, t, g.n, cu);
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) sb.curl[idx][i][d] = cu[i][d];
+        }
+        sb.ie[idx] = g.ie;
+    }
+    __syncthreads();
+
+    const int64_t si = (int64_t)blockIdx.x * DP0_THREADS + threadIdx.x;
+    if (si >= prm.ntrial) return;
+    const int64_t s = prm.ssup[si];
+    Geom gs;
+    load_geom(prm.sg, prm.sne, s, prm.snm ? (double)prm.snm[s] : 1.0, gs);
+    const int sv0 = __ldg(prm.sel + 3 * s), sv1 = __ldg(prm.sel + 3 * s + 1), sv2 = __ldg(prm.sel + 3 * s + 2);
+    double y[NQ6][3];
+#pragma unroll
+    for (int q = 0; q < NQ6; ++q) to_global(gs, rule.x[q], rule.y[q], y[q]);
+    double sc[3] = {0.0, 0.0, 0.0};
+    if (PH)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) sc[d] = __ldg(prm.sg + (22 + d) * prm.sne + s);
+    double curl_s[3][3];
+    if (HYP) surface_curls(prm.sg, prm.sne, s, gs.n, curl_s);
+    // trial shape values times the trial weights
+    double psw[NQ6][NS];
+#pragma unroll
+    for (int q = 0; q < NQ6; ++q) {
+        if (NS == 1) {
+            psw[q][0] = rule.w[q];
+        } else {
+            psw[q][0] = rule.w[q] * (1.0 - rule.x[q] - rule.y[q]);
+            psw[q][1 % NS] = rule.w[q] * rule.x[q];
+            psw[q][2 % NS] = rule.w[q] * rule.y[q];
+        }
+    }
+    const double kr = prm.p[0];
+    // (y_q - v0_s).n_s, the split of the double-layer normal term about the trial vertex 0
+    double ynv[NQ6];
+    if (DL)
+#pragma unroll
+        for (int q = 0; q < NQ6; ++q)
+            ynv[q] = fma(y[q][2] - gs.v0[2], gs.n[2], fma(y[q][1] - gs.v0[1], gs.n[1], (y[q][0] - gs.v0[0]) * gs.n[0]));
+
+    for (int tt = 0; tt < tcount; ++tt) {
+        if (prm.grids_identical && shares_vertex(sb.v[tt], sv0, sv1, sv2)) continue;
+        const int64_t t = prm.tsup[t0 + tt];
+        double rc = 0.0, ph_s = 0.0, ph_c = 1.0;
+        if (PH) {
+            const double D0 = sc[0] - sb.c[tt][0], D1 = sc[1] - sb.c[tt][1], D2 = sc[2] - sb.c[tt][2];
+            rc = sqrt(fma(D2, D2, fma(D1, D1, D0 * D0)));
+            sincos_cw64(kr * rc, &ph_s, &ph_c);
+        }
+        double lre[NT][NS], lim[NT][NS];
+#pragma unroll
+        for (int i = 0; i < NT; ++i)
+#pragma unroll
+            for (int j = 0; j < NS; ++j) lre[i][j] = lim[i][j] = 0.0;
+        double sre = 0.0, sim = 0.0;  // HYP: sum_pq w G
+        for (int p = 0; p < NQ6; ++p) {
+            const double x0 = sb.x[tt][p][0], x1 = sb.x[tt][p][1], x2 = sb.x[tt][p][2];
+            double xn = 0.0;
+            if (DL) xn = fma(gs.v0[2] - x2, gs.n[2], fma(gs.v0[1] - x1, gs.n[1], (gs.v0[0] - x0) * gs.n[0]));
+            double tre[NS], tim[NS];
+#pragma unroll
+            for (int j = 0; j < NS; ++j) tre[j] = tim[j] = 0.0;
+#pragma unroll
+            for (int q = 0; q < NQ6; ++q) {
+                const double d0 = y[q][0] - x0, d1 = y[q][1] - x1, d2 = y[q][2] - x2;
+                const double r2 = fma(d2, d2, fma(d1, d1, d0 * d0));
+                const double rinv = rsqrt(r2);
+                double kre, kim = 0.0;  // kernel value without 1/(4 pi)
+                if (!HELM) {
+                    if (K == BEMPPCUDA_LAPLACE_SLP) {
+                        kre = rinv;
+                    } else {
+                        const double dot = DL ? ynv[q] + xn
+                                              : fma(d2, sb.n[tt][2], fma(d1, sb.n[tt][1], d0 * sb.n[tt][0]));
+                        kre = (DL ? -dot : dot) * rinv * rinv * rinv;
+                    }
+                } else {
+                    const double r = r2 * rinv;
+                    double sn, cs;
+                    if (PH && PHC == 2)
+                        sincos_half64(kr * (r - rc), &sn, &cs);
+                    else if (PH)
+                        sincos_small64(kr * (r - rc), &sn, &cs);
+                    else
+                        sincos_cw64(kr * r, &sn, &cs);
+                    if (K == BEMPPCUDA_HELMHOLTZ_SLP) {
+                        kre = cs * rinv;
+                        kim = sn * rinv;
+                    } else {
+                        // (ikr - 1) e^{ikr} dot / r^3 = g (-h1 + i h2), g = dot / r^2
+                        const double dot = DL ? ynv[q] + xn
+                                              : -fma(d2, sb.n[tt][2], fma(d1, sb.n[tt][1], d0 * sb.n[tt][0]));
+                        const double g = dot * rinv * rinv;
+                        kre = -g * fma(rinv, cs, kr * sn);
+                        kim = g * fma(kr, cs, -rinv * sn);
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < NS; ++j) {
+                    tre[j] = fma(kre, psw[q][j], tre[j]);
+                    tim[j] = fma(kim, psw[q][j], tim[j]);
+                }
+            }
+            const double wp = rule.w[p];
+            double phw[NT];
+            if (NT == 1) {
+                phw[0] = wp;
+            } else {
+                phw[0] = wp * (1.0 - rule.x[p] - rule.y[p]);
+                phw[1 % NT] = wp * rule.x[p];
+                phw[2 % NT] = wp * rule.y[p];
+            }
+#pragma unroll
+            for (int i = 0; i < NT; ++i)
+#pragma unroll
+                for (int j = 0; j < NS; ++j) {
+                    lre[i][j] = fma(phw[i], tre[j], lre[i][j]);
+                    lim[i][j] = fma(phw[i], tim[j], lim[i][j]);
+                }
+            if (HYP)
+#pragma unroll
+                for (int j = 0; j < NS; ++j) {
+                    sre = fma(wp, tre[j], sre);
+                    sim = fma(wp, tim[j], sim);
+                }
+        }
+        const double scale = BC_INV_4PI * sb.ie[tt] * gs.ie;
+        double cpf = 0.0;
+        if (HYP) cpf = ASM == BEMPPCUDA_ASM_HELM_HYP
+                           ? -kr * kr * (sb.n[tt][0] * gs.n[0] + sb.n[tt][1] * gs.n[1] + sb.n[tt][2] * gs.n[2])
+                           : 0.0;
+#pragma unroll
+        for (int i = 0; i < NT; ++i) {
+            const double mt = prm.tmult[t * NT + i];
+            if (mt == 0.0) continue;
+            const int64_t row = prm.tl2g[t * NT + i];
+#pragma unroll
+            for (int j = 0; j < NS; ++j) {
+                const double ms = prm.smult[s * NS + j];
+                if (ms == 0.0) continue;
+                double vr = lre[i][j], vi = lim[i][j];
+                if (HYP) {
+                    const double cij = sb.curl[tt][i][0] * curl_s[j][0] + sb.curl[tt][i][1] * curl_s[j][1] +
+                                       sb.curl[tt][i][2] * curl_s[j][2];
+                    vr = fma(cij, sre, cpf * vr);
+                    vi = fma(cij, sim, cpf * vi);
+                }
+                if (PH) {
+                    const double tr = vr * ph_c - vi * ph_s;
+                    vi = fma(vr, ph_s, vi * ph_c);
+                    vr = tr;
+                }
+                const double m = mt * ms * scale;
+                const int64_t col = prm.sl2g[s * NS + j];
+                if (prm.is_complex) {
+                    double *o = reinterpret_cast<double *>(prm.result) + 2 * (row * prm.ld + col);
+                    atomicAdd(o, vr * m);
+                    atomicAdd(o + 1, vi * m);
+                } else {
+                    atomicAdd(reinterpret_cast<double *>(prm.result) + row * prm.ld + col, vr * m);
+                }
+            }
+        }
+    }
+}
+
+}  // namespace bc

@@ -23,6 +23,7 @@
 #include <cstdio>
 
 #include "dp0_sym.cuh"
+#include "p1.cuh"
 
 namespace bc {
 
@@ -311,6 +312,34 @@ static cudaError_t launch_dp0(const RegParams &prm, const QuadRule &rule, int mi
     return cudaGetLastError();
 }
 
+template <int ASM, int K, int NT, int NS>
+static void launch_p1_shapes(const RegParams &prm, const QuadRule &rule, int phase_class, dim3 grid, cudaStream_t st) {
+    if (phase_class == 2)
+        regular_p1<ASM, K, NT, NS, 2><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+    else if (phase_class == 1)
+        regular_p1<ASM, K, NT, NS, 1><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+    else
+        regular_p1<ASM, K, NT, NS, 0><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+}
+
+// Scalar and hypersingular operators on P1 / DP1 / P0 spaces with the 6-point
+// rule and a real wavenumber (p1.cuh).
+template <int ASM, int K>
+static cudaError_t launch_p1(const RegParams &prm, const QuadRule &rule, int phase_class, cudaStream_t st) {
+    dim3 grid((unsigned)((prm.ntrial + DP0_THREADS - 1) / DP0_THREADS),
+              (unsigned)((prm.ntest + P1_TCHUNK - 1) / P1_TCHUNK));
+    const int nt = prm.tnshape, ns = prm.snshape;
+    if (nt == 3 && ns == 3)
+        launch_p1_shapes<ASM, K, 3, 3>(prm, rule, phase_class, grid, st);
+    else if (nt == 3)
+        launch_p1_shapes<ASM, K, 3, 1>(prm, rule, phase_class, grid, st);
+    else if (ns == 3)
+        launch_p1_shapes<ASM, K, 1, 3>(prm, rule, phase_class, grid, st);
+    else
+        launch_p1_shapes<ASM, K, 1, 1>(prm, rule, phase_class, grid, st);
+    return cudaGetLastError();
+}
+
 template <int ASM, int K>
 static cudaError_t launch_generic(const RegParams &prm, const QuadRule &rule, cudaStream_t st) {
     dim3 grid((unsigned)((prm.ntrial + GEN_THREADS - 1) / GEN_THREADS), (unsigned)((prm.ntest + GEN_TCHUNK - 1) / GEN_TCHUNK));
@@ -396,6 +425,24 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
         case BEMPPCUDA_MODHELM_ADLP: err = launch_dp0<BEMPPCUDA_MODHELM_ADLP>(prm, rule, mixed, phase_class, sym, st); break;
         case BEMPPCUDA_HELMHOLTZ_COMBINED: err = launch_dp0<BEMPPCUDA_HELMHOLTZ_COMBINED>(prm, rule, mixed, phase_class, sym, st); break;
         default: bc_set_error("kernel %d not valid for boundary assembly", a->kernel); return BEMPPCUDA_ERR_INVALID;
+        }
+    } else if (a->nq == NQ6 && !a->overwrite && a->test.shapeset != BEMPPCUDA_SHAPE_RWG &&
+               a->trial.shapeset != BEMPPCUDA_SHAPE_RWG && a->params[1] == 0.0 &&
+               ((a->assembly == BEMPPCUDA_ASM_SCALAR && a->kernel <= BEMPPCUDA_HELMHOLTZ_ADLP) ||
+                a->assembly == BEMPPCUDA_ASM_LAPLACE_HYP || a->assembly == BEMPPCUDA_ASM_HELM_HYP)) {
+        if (a->assembly == BEMPPCUDA_ASM_LAPLACE_HYP) {
+            err = launch_p1<BEMPPCUDA_ASM_LAPLACE_HYP, BEMPPCUDA_LAPLACE_SLP>(prm, rule, phase_class, st);
+        } else if (a->assembly == BEMPPCUDA_ASM_HELM_HYP) {
+            err = launch_p1<BEMPPCUDA_ASM_HELM_HYP, BEMPPCUDA_HELMHOLTZ_SLP>(prm, rule, phase_class, st);
+        } else {
+            switch (a->kernel) {
+            case BEMPPCUDA_LAPLACE_SLP: err = launch_p1<0, BEMPPCUDA_LAPLACE_SLP>(prm, rule, phase_class, st); break;
+            case BEMPPCUDA_LAPLACE_DLP: err = launch_p1<0, BEMPPCUDA_LAPLACE_DLP>(prm, rule, phase_class, st); break;
+            case BEMPPCUDA_LAPLACE_ADLP: err = launch_p1<0, BEMPPCUDA_LAPLACE_ADLP>(prm, rule, phase_class, st); break;
+            case BEMPPCUDA_HELMHOLTZ_SLP: err = launch_p1<0, BEMPPCUDA_HELMHOLTZ_SLP>(prm, rule, phase_class, st); break;
+            case BEMPPCUDA_HELMHOLTZ_DLP: err = launch_p1<0, BEMPPCUDA_HELMHOLTZ_DLP>(prm, rule, phase_class, st); break;
+            default: err = launch_p1<0, BEMPPCUDA_HELMHOLTZ_ADLP>(prm, rule, phase_class, st); break;
+            }
         }
     } else {
         switch (a->assembly) {
