@@ -74,6 +74,21 @@ def _grids_identical(domain, dual_to_range):
     return domain.grid == dual_to_range.grid
 
 
+def same_space(a, b):
+    """True when two spaces are the same discretisation of one grid (so one device copy serves both)."""
+    if a is b:
+        return True
+    try:
+        if a.grid is not b.grid or a.shapeset.identifier != b.shapeset.identifier:
+            return False
+        if int(a.global_dof_count) != int(b.global_dof_count):
+            return False
+        return all(_np.array_equal(_np.asarray(getattr(a, f)), _np.asarray(getattr(b, f)))
+                   for f in ("support_elements", "local2global", "local_multipliers", "normal_multipliers"))
+    except AttributeError:
+        return False
+
+
 def regular_into(
     result, descriptor, domain, dual_to_range, parameters, precision=_lib.FP64, overwrite=False, stream=None,
     geometry=None, symmetric=True,
@@ -91,8 +106,10 @@ def regular_into(
     kernel, assembly = kernel_ids(descriptor)
     tgrid = geometry or device_grid(dual_to_range.grid)
     sgrid = geometry or device_grid(domain.grid)
-    tspace = device_space(dual_to_range)
     sspace = device_space(domain)
+    # an equal dual space shares the domain's device copy, which lets the
+    # library take the symmetric sweep (it compares the pointers)
+    tspace = sspace if same_space(domain, dual_to_range) else device_space(dual_to_range)
     points, weights = regular_rule(parameters.quadrature.regular)
     args = _lib.RegularArgs()
     args.kernel = kernel

@@ -12,6 +12,10 @@
 // (the P1 shape functions add up to 1), c = k^2 (Helmholtz), 0 (Laplace).
 // exp(ikr) is factored about the centroid distance as in the DP0 kernels.
 // The NT x NS block is added to the matrix with FP64 atomics (l2g, multipliers).
+// SYM (single layer and hypersingular, the same space on both sides): the
+// kernel is symmetric in x and y and so is the curl product, so the block of
+// the transposed pair is the transpose; only pairs i < j (support positions)
+// are evaluated and each block is added at (i, j) and (j, i).
 #pragma once
 
 #include "dp0.cuh"
@@ -29,7 +33,7 @@ struct TestBlockP1 {
     int v[P1_TCHUNK][3];
 };
 
-template <int ASM, int K, int NT, int NS, int PHC>
+template <int ASM, int K, int NT, int NS, int PHC, bool SYM>
 __global__ void __launch_bounds__(DP0_THREADS) regular_p1(RegParams prm, QuadRule rule) {
     constexpr bool HYP = (ASM == BEMPPCUDA_ASM_LAPLACE_HYP || ASM == BEMPPCUDA_ASM_HELM_HYP);
     constexpr bool HELM = (K == BEMPPCUDA_HELMHOLTZ_SLP || K == BEMPPCUDA_HELMHOLTZ_DLP ||
@@ -37,9 +41,12 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1(RegParams prm, QuadRul
     constexpr bool DL = (K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_HELMHOLTZ_DLP);
     constexpr bool AD = (K == BEMPPCUDA_LAPLACE_ADLP || K == BEMPPCUDA_HELMHOLTZ_ADLP);
     constexpr bool PH = HELM && PHC > 0;
+    static_assert(!SYM || (NT == NS && (K == BEMPPCUDA_LAPLACE_SLP || K == BEMPPCUDA_HELMHOLTZ_SLP)),
+                  "the symmetric sweep needs a symmetric operator on one space");
     __shared__ TestBlockP1 sb;
 
     const int64_t t0 = (int64_t)blockIdx.y * P1_TCHUNK;
+    if (SYM && t0 >= ((int64_t)blockIdx.x + 1) * DP0_THREADS) return;  // below the diagonal
     const int tcount = (int)min((int64_t)P1_TCHUNK, prm.ntest - t0);
     for (int idx = threadIdx.x; idx < tcount; idx += blockDim.x) {
         const int64_t t = prm.tsup[t0 + idx];
@@ -100,6 +107,7 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1(RegParams prm, QuadRul
             ynv[q] = fma(y[q][2] - gs.v0[2], gs.n[2], fma(y[q][1] - gs.v0[1], gs.n[1], (y[q][0] - gs.v0[0]) * gs.n[0]));
 
     for (int tt = 0; tt < tcount; ++tt) {
+        if (SYM && t0 + tt >= si) break;  // rows increase with tt
         if (prm.grids_identical && shares_vertex(sb.v[tt], sv0, sv1, sv2)) continue;
         const int64_t t = prm.tsup[t0 + tt];
         double rc = 0.0, ph_s = 0.0, ph_c = 1.0;
@@ -217,8 +225,14 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1(RegParams prm, QuadRul
                     double *o = reinterpret_cast<double *>(prm.result) + 2 * (row * prm.ld + col);
                     atomicAdd(o, vr * m);
                     atomicAdd(o + 1, vi * m);
+                    if (SYM) {
+                        double *ot = reinterpret_cast<double *>(prm.result) + 2 * (col * prm.ld + row);
+                        atomicAdd(ot, vr * m);
+                        atomicAdd(ot + 1, vi * m);
+                    }
                 } else {
                     atomicAdd(reinterpret_cast<double *>(prm.result) + row * prm.ld + col, vr * m);
+                    if (SYM) atomicAdd(reinterpret_cast<double *>(prm.result) + col * prm.ld + row, vr * m);
                 }
             }
         }

@@ -312,31 +312,44 @@ static cudaError_t launch_dp0(const RegParams &prm, const QuadRule &rule, int mi
     return cudaGetLastError();
 }
 
-template <int ASM, int K, int NT, int NS>
-static void launch_p1_shapes(const RegParams &prm, const QuadRule &rule, int phase_class, dim3 grid, cudaStream_t st) {
+template <int ASM, int K, int NT, int NS, bool SYM>
+static void launch_p1_phase(const RegParams &prm, const QuadRule &rule, int phase_class, dim3 grid, cudaStream_t st) {
     if (phase_class == 2)
-        regular_p1<ASM, K, NT, NS, 2><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+        regular_p1<ASM, K, NT, NS, 2, SYM><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
     else if (phase_class == 1)
-        regular_p1<ASM, K, NT, NS, 1><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+        regular_p1<ASM, K, NT, NS, 1, SYM><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
     else
-        regular_p1<ASM, K, NT, NS, 0><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+        regular_p1<ASM, K, NT, NS, 0, SYM><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+}
+
+template <int ASM, int K, int NT, int NS>
+static void launch_p1_shapes(const RegParams &prm, const QuadRule &rule, int phase_class, bool sym, dim3 grid,
+                             cudaStream_t st) {
+    constexpr bool SYMMETRIC_OP = NT == NS && (K == BEMPPCUDA_LAPLACE_SLP || K == BEMPPCUDA_HELMHOLTZ_SLP);
+    if constexpr (SYMMETRIC_OP) {
+        if (sym) {
+            launch_p1_phase<ASM, K, NT, NS, true>(prm, rule, phase_class, grid, st);
+            return;
+        }
+    }
+    launch_p1_phase<ASM, K, NT, NS, false>(prm, rule, phase_class, grid, st);
 }
 
 // Scalar and hypersingular operators on P1 / DP1 / P0 spaces with the 6-point
 // rule and a real wavenumber (p1.cuh).
 template <int ASM, int K>
-static cudaError_t launch_p1(const RegParams &prm, const QuadRule &rule, int phase_class, cudaStream_t st) {
+static cudaError_t launch_p1(const RegParams &prm, const QuadRule &rule, int phase_class, bool sym, cudaStream_t st) {
     dim3 grid((unsigned)((prm.ntrial + DP0_THREADS - 1) / DP0_THREADS),
               (unsigned)((prm.ntest + P1_TCHUNK - 1) / P1_TCHUNK));
     const int nt = prm.tnshape, ns = prm.snshape;
     if (nt == 3 && ns == 3)
-        launch_p1_shapes<ASM, K, 3, 3>(prm, rule, phase_class, grid, st);
+        launch_p1_shapes<ASM, K, 3, 3>(prm, rule, phase_class, sym, grid, st);
     else if (nt == 3)
-        launch_p1_shapes<ASM, K, 3, 1>(prm, rule, phase_class, grid, st);
+        launch_p1_shapes<ASM, K, 3, 1>(prm, rule, phase_class, false, grid, st);
     else if (ns == 3)
-        launch_p1_shapes<ASM, K, 1, 3>(prm, rule, phase_class, grid, st);
+        launch_p1_shapes<ASM, K, 1, 3>(prm, rule, phase_class, false, grid, st);
     else
-        launch_p1_shapes<ASM, K, 1, 1>(prm, rule, phase_class, grid, st);
+        launch_p1_shapes<ASM, K, 1, 1>(prm, rule, phase_class, sym, grid, st);
     return cudaGetLastError();
 }
 
@@ -426,22 +439,26 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
         case BEMPPCUDA_HELMHOLTZ_COMBINED: err = launch_dp0<BEMPPCUDA_HELMHOLTZ_COMBINED>(prm, rule, mixed, phase_class, sym, st); break;
         default: bc_set_error("kernel %d not valid for boundary assembly", a->kernel); return BEMPPCUDA_ERR_INVALID;
         }
-    } else if (a->nq == NQ6 && !a->overwrite && a->test.shapeset != BEMPPCUDA_SHAPE_RWG &&
+    } else if (const bool psym = !a->no_symmetry && a->grids_identical && a->test.support == a->trial.support &&
+                                 a->test.l2g == a->trial.l2g && a->test.mult == a->trial.mult &&
+                                 a->test.nsupport == a->trial.nsupport && a->test_grid.geom == a->trial_grid.geom &&
+                                 a->test.normal_mult == a->trial.normal_mult && prm.ntest == prm.ntrial;
+               a->nq == NQ6 && !a->overwrite && a->test.shapeset != BEMPPCUDA_SHAPE_RWG &&
                a->trial.shapeset != BEMPPCUDA_SHAPE_RWG && a->params[1] == 0.0 &&
                ((a->assembly == BEMPPCUDA_ASM_SCALAR && a->kernel <= BEMPPCUDA_HELMHOLTZ_ADLP) ||
                 a->assembly == BEMPPCUDA_ASM_LAPLACE_HYP || a->assembly == BEMPPCUDA_ASM_HELM_HYP)) {
         if (a->assembly == BEMPPCUDA_ASM_LAPLACE_HYP) {
-            err = launch_p1<BEMPPCUDA_ASM_LAPLACE_HYP, BEMPPCUDA_LAPLACE_SLP>(prm, rule, phase_class, st);
+            err = launch_p1<BEMPPCUDA_ASM_LAPLACE_HYP, BEMPPCUDA_LAPLACE_SLP>(prm, rule, phase_class, psym, st);
         } else if (a->assembly == BEMPPCUDA_ASM_HELM_HYP) {
-            err = launch_p1<BEMPPCUDA_ASM_HELM_HYP, BEMPPCUDA_HELMHOLTZ_SLP>(prm, rule, phase_class, st);
+            err = launch_p1<BEMPPCUDA_ASM_HELM_HYP, BEMPPCUDA_HELMHOLTZ_SLP>(prm, rule, phase_class, psym, st);
         } else {
             switch (a->kernel) {
-            case BEMPPCUDA_LAPLACE_SLP: err = launch_p1<0, BEMPPCUDA_LAPLACE_SLP>(prm, rule, phase_class, st); break;
-            case BEMPPCUDA_LAPLACE_DLP: err = launch_p1<0, BEMPPCUDA_LAPLACE_DLP>(prm, rule, phase_class, st); break;
-            case BEMPPCUDA_LAPLACE_ADLP: err = launch_p1<0, BEMPPCUDA_LAPLACE_ADLP>(prm, rule, phase_class, st); break;
-            case BEMPPCUDA_HELMHOLTZ_SLP: err = launch_p1<0, BEMPPCUDA_HELMHOLTZ_SLP>(prm, rule, phase_class, st); break;
-            case BEMPPCUDA_HELMHOLTZ_DLP: err = launch_p1<0, BEMPPCUDA_HELMHOLTZ_DLP>(prm, rule, phase_class, st); break;
-            default: err = launch_p1<0, BEMPPCUDA_HELMHOLTZ_ADLP>(prm, rule, phase_class, st); break;
+            case BEMPPCUDA_LAPLACE_SLP: err = launch_p1<0, BEMPPCUDA_LAPLACE_SLP>(prm, rule, phase_class, psym, st); break;
+            case BEMPPCUDA_LAPLACE_DLP: err = launch_p1<0, BEMPPCUDA_LAPLACE_DLP>(prm, rule, phase_class, psym, st); break;
+            case BEMPPCUDA_LAPLACE_ADLP: err = launch_p1<0, BEMPPCUDA_LAPLACE_ADLP>(prm, rule, phase_class, psym, st); break;
+            case BEMPPCUDA_HELMHOLTZ_SLP: err = launch_p1<0, BEMPPCUDA_HELMHOLTZ_SLP>(prm, rule, phase_class, psym, st); break;
+            case BEMPPCUDA_HELMHOLTZ_DLP: err = launch_p1<0, BEMPPCUDA_HELMHOLTZ_DLP>(prm, rule, phase_class, psym, st); break;
+            default: err = launch_p1<0, BEMPPCUDA_HELMHOLTZ_ADLP>(prm, rule, phase_class, psym, st); break;
             }
         }
     } else {

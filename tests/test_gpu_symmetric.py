@@ -75,3 +75,33 @@ def test_symmetric_sweep_odd_size():
         a = _assemble(grid, kernel, options, _lib.FP64, True)
         b = _assemble(grid, kernel, options, _lib.FP64, False)
         assert (torch.linalg.norm(a - b) / torch.linalg.norm(b)).item() < 1e-13
+
+
+@pytest.mark.parametrize("path,k", [("laplace.single_layer", None), ("helmholtz.single_layer", 4.0),
+                                    ("laplace.hypersingular", None), ("helmholtz.hypersingular", 4.0),
+                                    ("helmholtz.double_layer", 4.0)])
+def test_p1_symmetric_sweep_matches_entrywise(path, k):
+    """P1 operators: the symmetric sweep (single layer, hypersingular) against per-pair evaluation."""
+    from bempp_cuda import operators
+    from bempp_cuda.assembly import regular_into, singular_into_dense
+    from bempp_cuda.operators import Parameters
+    from bempp_cuda.shapes import ellipsoid
+    from bempp_cuda.space import function_space
+
+    grid = ellipsoid(3, 1.1, 0.9, 1.0)
+    sp = function_space(grid, "P", 1)
+    f = operators.boundary
+    for part in path.split("."):
+        f = getattr(f, part)
+    op = f(sp, sp, sp) if k is None else f(sp, sp, sp, k)
+    d = op.descriptor
+    n = sp.global_dof_count
+    dtype = torch.complex128 if d.is_complex else torch.float64
+    out = []
+    for sym in (True, False):
+        a = torch.zeros((n, n), dtype=dtype, device="cuda")
+        regular_into(a, d, sp, sp, Parameters(), symmetric=sym)
+        singular_into_dense(a, d, sp, sp, Parameters())
+        out.append(a)
+    torch.cuda.synchronize()
+    assert (torch.linalg.norm(out[0] - out[1]) / torch.linalg.norm(out[1])).item() < 1e-13
