@@ -100,6 +100,8 @@ class RegularArgs(_ct.Structure):
         ("overwrite", _i32),
         ("no_symmetry", _i32),
         ("phase_radius", _ct.c_double),
+        ("row_begin", _i64),
+        ("row_end", _i64),
     ]
 
 

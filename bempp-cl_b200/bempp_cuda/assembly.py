@@ -91,7 +91,7 @@ def same_space(a, b):
 
 def regular_into(
     result, descriptor, domain, dual_to_range, parameters, precision=_lib.FP64, overwrite=False, stream=None,
-    geometry=None, symmetric=True,
+    geometry=None, symmetric=True, rows=None,
 ):
     """Add (or with ``overwrite`` store) the regular part into the device tensor ``result``.
 
@@ -100,7 +100,8 @@ def regular_into(
     moved while its elements stayed the same.  With ``symmetric`` (default)
     the library computes A_ij and A_ji from one sweep when both spaces are the
     same DP0 space of one grid; ``symmetric=False`` evaluates every entry on
-    its own.
+    its own.  ``rows=(lo, hi)`` restricts a symmetric sweep to the pairs
+    (i, j), i <= j, with rows i in [lo, hi) (both entries written).
     """
     require_cuda()
     kernel, assembly = kernel_ids(descriptor)
@@ -129,6 +130,8 @@ def regular_into(
     args.ld = result.stride(0)
     args.overwrite = 1 if overwrite else 0
     args.no_symmetry = 0 if symmetric else 1
+    if rows is not None:
+        args.row_begin, args.row_end = int(rows[0]), int(rows[1])
     # a little slack over the exact bound keeps rounding of the radii on the safe side
     args.phase_radius = 1.0001 * (tgrid.radius + sgrid.radius)
     _lib.check(_lib.load().bemppcuda_assemble_regular(args, stream or current_stream()))
@@ -145,8 +148,12 @@ def dp0_fast_path(descriptor, domain, dual_to_range, parameters):
 
 
 def singular_into_dense(result, descriptor, domain, dual_to_range, parameters, diag_shift=0.0, stream=None,
-                        geometry=None):
-    """Scatter the Sauter-Schwab pairs into the dense device tensor ``result`` (``geometry`` as in regular_into)."""
+                        geometry=None, rows=None):
+    """Scatter the Sauter-Schwab pairs into the dense device tensor ``result`` (``geometry`` as in regular_into).
+
+    ``rows=(lo, hi)``: only the pairs whose test element is one of the support
+    elements lo .. hi-1 of ``dual_to_range`` (support in increasing order).
+    """
     kernel, assembly = kernel_ids(descriptor)
     grid = domain.grid
     rule = device_singular_rule(grid, parameters.quadrature.singular, dual_to_range.support, domain.support)
@@ -158,7 +165,11 @@ def singular_into_dense(result, descriptor, domain, dual_to_range, parameters, d
     args.grid = (geometry or device_grid(grid)).record()
     args.test = device_space(dual_to_range).record()
     args.trial = device_space(domain).record()
-    rule.fill(args)
+    if rows is None:
+        rule.fill(args)
+    else:
+        sup = _np.asarray(dual_to_range.support_elements)
+        rule.fill(args, rule.pair_range(int(sup[rows[0]]), int(sup[rows[1] - 1])))
     args.values = None
     args.dense = ptr(result)
     args.ld = result.stride(0)
@@ -195,6 +206,61 @@ def assemble_dense_device(domain, dual_to_range, parameters, descriptor, device_
     regular_into(out, descriptor, domain, dual_to_range, parameters, precision=precision, overwrite=fast)
     if _grids_identical(domain, dual_to_range):
         singular_into_dense(out, descriptor, domain, dual_to_range, parameters)
+    return out
+
+
+def symmetric_rows_eligible(descriptor, domain, dual_to_range, parameters):
+    """True when the library can run the symmetric sweep in row blocks (same DP0 space, real k)."""
+    if not (dp0_fast_path(descriptor, domain, dual_to_range, parameters) and same_space(domain, dual_to_range)):
+        return False
+    if descriptor.kernel_type not in ("laplace_single_layer", "laplace_double_layer", "laplace_adjoint_double_layer",
+                                      "helmholtz_single_layer", "helmholtz_double_layer",
+                                      "helmholtz_adjoint_double_layer", "helmholtz_combined_field"):
+        return False
+    p = kernel_params(descriptor.options)
+    return descriptor.kernel_type.startswith("laplace") or (p[1] == 0.0 and p[0] > 0.0)
+
+
+def assemble_dense_to_host(domain, dual_to_range, parameters, descriptor, device_interface="cuda", out=None,
+                           diag_shift=0.0, blocks=16):
+    """Dense DP0 weak form streamed into (pinned) host memory while it is assembled.
+
+    The symmetric sweep runs one row block at a time in row order: after the
+    block's upper-triangle tiles (which also write the transposes into later
+    rows) and its singular pairs, its rows are final, so their copy to the
+    host overlaps the next block's assembly on a second stream.  Other
+    operators are assembled whole and then copied.  Returns the host tensor.
+    """
+    require_cuda()
+    rows = int(dual_to_range.global_dof_count)
+    cols = int(domain.global_dof_count)
+    dtype = result_dtype(descriptor)
+    if out is None:
+        out = _torch.empty((rows, cols), dtype=dtype, pin_memory=True)
+    if not symmetric_rows_eligible(descriptor, domain, dual_to_range, parameters):
+        dev = assemble_dense_device(domain, dual_to_range, parameters, descriptor, device_interface)
+        out.copy_(dev, non_blocking=True)
+        _torch.cuda.current_stream().synchronize()
+        return out
+    precision = precision_of(device_interface)
+    dev = _torch.empty((rows, cols), dtype=dtype, device="cuda")
+    compute = _torch.cuda.current_stream()
+    copy = _torch.cuda.Stream()
+    bounds = [(rows * b) // blocks for b in range(blocks + 1)]
+    for lo, hi in zip(bounds[:-1], bounds[1:]):
+        if hi <= lo:
+            continue
+        regular_into(dev, descriptor, domain, dual_to_range, parameters, precision=precision, overwrite=True,
+                     rows=(lo, hi))
+        singular_into_dense(dev, descriptor, domain, dual_to_range, parameters, diag_shift=diag_shift, rows=(lo, hi))
+        done = _torch.cuda.Event()
+        done.record(compute)
+        copy.wait_event(done)
+        with _torch.cuda.stream(copy):
+            out[lo:hi].copy_(dev[lo:hi], non_blocking=True)
+    compute.wait_stream(copy)
+    copy.synchronize()
+    del dev
     return out
 
 

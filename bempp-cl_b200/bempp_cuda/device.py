@@ -143,20 +143,41 @@ class DeviceSingularRule(object):
         (self.test_elements, self.trial_elements, self.test_offsets, self.trial_offsets, self.weights_offsets,
          self.npoints) = [to_device(a, _torch.int32) for a in ints]
         self.h2d_bytes = tp.nbytes + sp.nbytes + 8 * len(w) + sum(a.nbytes for a in ints)
+        self._host_ints = ints
+        self._by_test = None
 
-    def fill(self, args):
-        args.npairs = self.npairs
+    def by_test(self):
+        """The pair arrays in test-element order (stable) on the device, and the sorted test elements (host)."""
+        if self._by_test is None:
+            order = _np.argsort(self._host_ints[0], kind="stable")
+            arrays = [to_device(a[order], _torch.int32) for a in self._host_ints]
+            self._by_test = (arrays, self._host_ints[0][order])
+        return self._by_test
+
+    def pair_range(self, first_element, last_element):
+        """[begin, end) of the pairs whose test element lies in [first_element, last_element] (test order)."""
+        te_sorted = self.by_test()[1]
+        return (int(_np.searchsorted(te_sorted, first_element, "left")),
+                int(_np.searchsorted(te_sorted, last_element, "right")))
+
+    def fill(self, args, pairs=None):
+        """Point the singular arguments at all pairs, or at pairs [begin, end) of the test-element order."""
         args.npoints_table = self.npoints_table
         args.test_points = ptr(self.test_points)
         args.trial_points = ptr(self.trial_points)
         args.weights = ptr(self.weights)
         args.nweights = self.nweights
-        args.test_elements = ptr(self.test_elements)
-        args.trial_elements = ptr(self.trial_elements)
-        args.test_offsets = ptr(self.test_offsets)
-        args.trial_offsets = ptr(self.trial_offsets)
-        args.weights_offsets = ptr(self.weights_offsets)
-        args.npoints = ptr(self.npoints)
+        if pairs is None:
+            args.npairs = self.npairs
+            arrays = (self.test_elements, self.trial_elements, self.test_offsets, self.trial_offsets,
+                      self.weights_offsets, self.npoints)
+            begin = 0
+        else:
+            begin, end = pairs
+            args.npairs = max(0, end - begin)
+            arrays = self.by_test()[0]
+        (args.test_elements, args.trial_elements, args.test_offsets, args.trial_offsets, args.weights_offsets,
+         args.npoints) = [_ct.c_void_p(a.data_ptr() + 4 * begin) for a in arrays]
 
 
 def device_grid(grid):

@@ -194,13 +194,9 @@ def linear_terms(op, coef=1.0):
     return [(coef, op)]
 
 
-def _fused_combined_field(op):
-    """Assemble a DP0 Helmholtz a*DLP + b*SLP + c*I in one pass, or return None.
-
-    The reference assembles each term and adds the dense weak forms
-    (boundary_operator.py:134-169); here the shared kernel work (distance,
-    exp(ikr)) is done once per quadrature pair (csrc/regular.cu).
-    """
+def _combined_field_parts(op):
+    """(a, eta, shift, dlp term) when ``op`` is a DP0 Helmholtz a*DLP + b*SLP + c*I with
+    eta = b / a and a real shift = c / a, else None."""
     terms = linear_terms(op)
     dlp = [(c, t) for c, t in terms if t.descriptor is not None and t.descriptor.kernel_type == "helmholtz_double_layer"]
     slp = [(c, t) for c, t in terms if t.descriptor is not None and t.descriptor.kernel_type == "helmholtz_single_layer"
@@ -220,17 +216,63 @@ def _fused_combined_field(op):
     c = ident[0][0] if ident else 0.0
     if ident and not (ident[0][1].domain == d.domain and ident[0][1].dual_to_range == d.dual_to_range):
         return None
-    from .assembly import assemble_combined_field_device
-
     eta = complex(b) / complex(a)
     shift = complex(c) / complex(a)
     if shift.imag != 0.0:
         return None
+    return complex(a), eta, shift.real, d
+
+
+def _fused_combined_field(op):
+    """Assemble a DP0 Helmholtz a*DLP + b*SLP + c*I in one pass, or return None.
+
+    The reference assembles each term and adds the dense weak forms
+    (boundary_operator.py:134-169); here the shared kernel work (distance,
+    exp(ikr)) is done once per quadrature pair (csrc/regular.cu).
+    """
+    parts = _combined_field_parts(op)
+    if parts is None:
+        return None
+    from .assembly import assemble_combined_field_device
+
+    a, eta, shift, d = parts
     mat = assemble_combined_field_device(d.domain, d.dual_to_range, d.parameters, d.descriptor.options, eta,
-                                         shift.real, d.device_interface)
-    if complex(a) != 1.0:
-        mat.mul_(complex(a))
+                                         shift, d.device_interface)
+    if a != 1.0:
+        mat.mul_(a)
     return DenseDeviceOperator(mat)
+
+
+def weak_form_to_host(op, out=None, blocks=16):
+    """The dense weak form of ``op`` as a host tensor (pinned unless ``out`` is given).
+
+    For a DP0 operator of one space (plain, or the fused combined field with
+    unit DLP coefficient) the copy to the host overlaps the assembly, one row
+    block at a time (assembly.assemble_dense_to_host); otherwise the weak form
+    is assembled on the device and copied.  The reference's weak form is a
+    host matrix (discrete_boundary_operator.py:177-252), so this is the call
+    that hands a user the same object.
+    """
+    from .assembly import assemble_dense_to_host
+
+    parts = _combined_field_parts(op) if isinstance(op, (_SumOperator, _ScaledOperator)) else None
+    if parts is not None and parts[0] == 1.0:
+        a, eta, shift, d = parts
+        opts = list(_np.asarray(d.descriptor.options, dtype=float)[:2]) + [eta.real, eta.imag]
+        desc = OperatorDescriptor("helmholtz_combined_field_boundary", opts, "helmholtz_combined_field",
+                                  "default_scalar", "double", True, None, 1)
+        return assemble_dense_to_host(d.domain, d.dual_to_range, d.parameters, desc, d.device_interface, out,
+                                      diag_shift=shift, blocks=blocks)
+    if getattr(op, "descriptor", None) is not None and not isinstance(
+            op, (_SumOperator, _ScaledOperator, IdentityOperator)):
+        return assemble_dense_to_host(op.domain, op.dual_to_range, op.parameters, op.descriptor,
+                                      op.device_interface, out, blocks=blocks)
+    w = op.weak_form()
+    t = _torch.diag(w.values) if isinstance(w, DiagonalOperator) else w.tensor
+    if out is None:
+        out = _torch.empty(tuple(t.shape), dtype=t.dtype, pin_memory=True)
+    out.copy_(t)
+    return out
 
 
 class _SumOperator(BoundaryOperator):

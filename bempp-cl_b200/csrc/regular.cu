@@ -231,11 +231,12 @@ __global__ void __launch_bounds__(GEN_THREADS) regular_generic(RegParams prm, Qu
 // that start below the block's last column have no pair i <= j and exit
 // before touching shared memory.
 template <int K, int PHC>
-__global__ void __launch_bounds__(DP0_THREADS) regular_dp0_fp64_sym(RegParams prm, QuadRule rule) {
-    const int64_t t0 = (int64_t)blockIdx.y * DP0_TCHUNK;
+__global__ void __launch_bounds__(DP0_THREADS) regular_dp0_fp64_sym(RegParams prm, QuadRule rule, int64_t row0,
+                                                                    int64_t row1) {
+    const int64_t t0 = row0 + (int64_t)blockIdx.y * DP0_TCHUNK;
     if (t0 >= ((int64_t)blockIdx.x + 1) * DP0_THREADS) return;
     __shared__ TestBlock64s sb;
-    regular_dp0_fp64_sym_tile<K, PHC>(prm, rule, blockIdx.x, t0, DP0_TCHUNK, sb);
+    regular_dp0_fp64_sym_tile<K, PHC>(prm, rule, blockIdx.x, t0, (int)min((int64_t)DP0_TCHUNK, row1 - t0), sb);
 }
 
 #ifndef BC_MSYM_MIN_BLOCKS
@@ -243,35 +244,37 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_dp0_fp64_sym(RegParams pr
 #endif
 
 template <int K, int PHC>
-__global__ void __launch_bounds__(DP0_THREADS, BC_MSYM_MIN_BLOCKS) regular_dp0_mixed_sym(RegParams prm, QuadRule rule) {
-    const int64_t t0 = (int64_t)blockIdx.y * DP0_TCHUNK;
+__global__ void __launch_bounds__(DP0_THREADS, BC_MSYM_MIN_BLOCKS) regular_dp0_mixed_sym(RegParams prm, QuadRule rule,
+                                                                                      int64_t row0, int64_t row1) {
+    const int64_t t0 = row0 + (int64_t)blockIdx.y * DP0_TCHUNK;
     if (t0 >= ((int64_t)blockIdx.x + 1) * DP0_THREADS) return;
     __shared__ TestBlock32p sb;
-    regular_dp0_mixed_sym_tile<K, PHC>(prm, rule, blockIdx.x, t0, DP0_TCHUNK, sb);
+    regular_dp0_mixed_sym_tile<K, PHC>(prm, rule, blockIdx.x, t0, (int)min((int64_t)DP0_TCHUNK, row1 - t0), sb);
 }
 
 template <int K>
 static cudaError_t launch_dp0(const RegParams &prm, const QuadRule &rule, int mixed, int phase_class, bool sym,
-                              cudaStream_t st) {
+                              int64_t row0, int64_t row1, cudaStream_t st) {
     dim3 grid((unsigned)((prm.ntrial + DP0_THREADS - 1) / DP0_THREADS), (unsigned)((prm.ntest + DP0_TCHUNK - 1) / DP0_TCHUNK));
     if constexpr (SymTraits<K>::supported) {
         // same DP0 space on both sides, real wavenumber (k > 0 for the scaled mixed path)
         const bool real_k = !KernelTraits<K>::helm || (prm.p[1] == 0.0 && (!mixed || prm.p[0] > 0.0));
         if (sym && real_k) {
+            const dim3 sgrid(grid.x, (unsigned)((row1 - row0 + DP0_TCHUNK - 1) / DP0_TCHUNK));
             if (mixed) {
                 if (phase_class == 2)
-                    regular_dp0_mixed_sym<K, 2><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+                    regular_dp0_mixed_sym<K, 2><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1);
                 else if (phase_class == 1)
-                    regular_dp0_mixed_sym<K, 1><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+                    regular_dp0_mixed_sym<K, 1><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1);
                 else
-                    regular_dp0_mixed_sym<K, 0><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+                    regular_dp0_mixed_sym<K, 0><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1);
             } else {
                 if (phase_class == 2)
-                    regular_dp0_fp64_sym<K, 2><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+                    regular_dp0_fp64_sym<K, 2><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1);
                 else if (phase_class == 1)
-                    regular_dp0_fp64_sym<K, 1><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+                    regular_dp0_fp64_sym<K, 1><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1);
                 else
-                    regular_dp0_fp64_sym<K, 0><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+                    regular_dp0_fp64_sym<K, 0><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1);
             }
             return cudaGetLastError();
         }
@@ -290,6 +293,7 @@ static cudaError_t launch_dp0(const RegParams &prm, const QuadRule &rule, int mi
             return cudaGetLastError();
         }
     }
+    if (row0 != 0 || row1 != prm.ntest) return cudaErrorInvalidValue;  // a row range needs the symmetric sweep
     if (mixed) {
         if (ck)
             regular_dp0_mixed<K, true, 0><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
@@ -425,18 +429,25 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
     const bool sym = dp0 && !a->no_symmetry && a->grids_identical && a->test.support == a->trial.support &&
                      a->test.nsupport == a->trial.nsupport && a->test_grid.geom == a->trial_grid.geom &&
                      a->test.normal_mult == a->trial.normal_mult && prm.ntest == prm.ntrial;
+    const bool ranged = a->row_begin != 0 || a->row_end != 0;
+    if (ranged && (!sym || a->row_begin < 0 || a->row_end > prm.ntest || a->row_begin >= a->row_end)) {
+        bc_set_error("row range [%lld, %lld) needs the symmetric sweep and 0 <= begin < end <= %lld rows",
+                     (long long)a->row_begin, (long long)a->row_end, (long long)prm.ntest);
+        return BEMPPCUDA_ERR_INVALID;
+    }
+    const int64_t row0 = ranged ? a->row_begin : 0, row1 = ranged ? a->row_end : prm.ntest;
     if (dp0) {
         switch (a->kernel) {
-        case BEMPPCUDA_LAPLACE_SLP: err = launch_dp0<BEMPPCUDA_LAPLACE_SLP>(prm, rule, mixed, phase_class, sym, st); break;
-        case BEMPPCUDA_LAPLACE_DLP: err = launch_dp0<BEMPPCUDA_LAPLACE_DLP>(prm, rule, mixed, phase_class, sym, st); break;
-        case BEMPPCUDA_LAPLACE_ADLP: err = launch_dp0<BEMPPCUDA_LAPLACE_ADLP>(prm, rule, mixed, phase_class, sym, st); break;
-        case BEMPPCUDA_HELMHOLTZ_SLP: err = launch_dp0<BEMPPCUDA_HELMHOLTZ_SLP>(prm, rule, mixed, phase_class, sym, st); break;
-        case BEMPPCUDA_HELMHOLTZ_DLP: err = launch_dp0<BEMPPCUDA_HELMHOLTZ_DLP>(prm, rule, mixed, phase_class, sym, st); break;
-        case BEMPPCUDA_HELMHOLTZ_ADLP: err = launch_dp0<BEMPPCUDA_HELMHOLTZ_ADLP>(prm, rule, mixed, phase_class, sym, st); break;
-        case BEMPPCUDA_MODHELM_SLP: err = launch_dp0<BEMPPCUDA_MODHELM_SLP>(prm, rule, mixed, phase_class, sym, st); break;
-        case BEMPPCUDA_MODHELM_DLP: err = launch_dp0<BEMPPCUDA_MODHELM_DLP>(prm, rule, mixed, phase_class, sym, st); break;
-        case BEMPPCUDA_MODHELM_ADLP: err = launch_dp0<BEMPPCUDA_MODHELM_ADLP>(prm, rule, mixed, phase_class, sym, st); break;
-        case BEMPPCUDA_HELMHOLTZ_COMBINED: err = launch_dp0<BEMPPCUDA_HELMHOLTZ_COMBINED>(prm, rule, mixed, phase_class, sym, st); break;
+        case BEMPPCUDA_LAPLACE_SLP: err = launch_dp0<BEMPPCUDA_LAPLACE_SLP>(prm, rule, mixed, phase_class, sym, row0, row1, st); break;
+        case BEMPPCUDA_LAPLACE_DLP: err = launch_dp0<BEMPPCUDA_LAPLACE_DLP>(prm, rule, mixed, phase_class, sym, row0, row1, st); break;
+        case BEMPPCUDA_LAPLACE_ADLP: err = launch_dp0<BEMPPCUDA_LAPLACE_ADLP>(prm, rule, mixed, phase_class, sym, row0, row1, st); break;
+        case BEMPPCUDA_HELMHOLTZ_SLP: err = launch_dp0<BEMPPCUDA_HELMHOLTZ_SLP>(prm, rule, mixed, phase_class, sym, row0, row1, st); break;
+        case BEMPPCUDA_HELMHOLTZ_DLP: err = launch_dp0<BEMPPCUDA_HELMHOLTZ_DLP>(prm, rule, mixed, phase_class, sym, row0, row1, st); break;
+        case BEMPPCUDA_HELMHOLTZ_ADLP: err = launch_dp0<BEMPPCUDA_HELMHOLTZ_ADLP>(prm, rule, mixed, phase_class, sym, row0, row1, st); break;
+        case BEMPPCUDA_MODHELM_SLP: err = launch_dp0<BEMPPCUDA_MODHELM_SLP>(prm, rule, mixed, phase_class, sym, row0, row1, st); break;
+        case BEMPPCUDA_MODHELM_DLP: err = launch_dp0<BEMPPCUDA_MODHELM_DLP>(prm, rule, mixed, phase_class, sym, row0, row1, st); break;
+        case BEMPPCUDA_MODHELM_ADLP: err = launch_dp0<BEMPPCUDA_MODHELM_ADLP>(prm, rule, mixed, phase_class, sym, row0, row1, st); break;
+        case BEMPPCUDA_HELMHOLTZ_COMBINED: err = launch_dp0<BEMPPCUDA_HELMHOLTZ_COMBINED>(prm, rule, mixed, phase_class, sym, row0, row1, st); break;
         default: bc_set_error("kernel %d not valid for boundary assembly", a->kernel); return BEMPPCUDA_ERR_INVALID;
         }
     } else if (const bool psym = !a->no_symmetry && a->grids_identical && a->test.support == a->trial.support &&

@@ -125,6 +125,9 @@ typedef struct {
     double phase_radius;        /* R_test + R_trial, R = largest centroid-to-vertex distance of a grid;
                                    lets the mixed path skip the phase range reduction when
                                    |k| * phase_radius <= 1; 0 = unknown (always reduce) */
+    int64_t row_begin;          /* symmetric sweep only: evaluate the pairs (i, j), i <= j, with rows i in */
+    int64_t row_end;            /* [row_begin, row_end) (writing A_ij and A_ji); 0, 0 = all rows.  Rows of
+                                   block [b, e) are complete once the blocks before it and this call ran */
 } bemppcuda_regular_args;
 
 /* Singular pairs (Sauter-Schwab), the arrays of

@@ -105,3 +105,31 @@ def test_p1_symmetric_sweep_matches_entrywise(path, k):
         out.append(a)
     torch.cuda.synchronize()
     assert (torch.linalg.norm(out[0] - out[1]) / torch.linalg.norm(out[1])).item() < 1e-13
+
+
+@pytest.mark.parametrize("blocks", [1, 5, 16])
+def test_weak_form_to_host_streams_row_blocks(blocks):
+    """Row-block symmetric assembly streamed to pinned host memory = the device weak form."""
+    from bempp_cuda import operators
+
+    from bempp_cuda.shapes import ellipsoid
+    from bempp_cuda.space import function_space
+
+    grid = ellipsoid(3, 1.0, 0.8, 1.2)
+    sp = function_space(grid, "DP", 0)
+    k = 6.0
+    for interface, tol in (("cuda", 1e-14), ("cuda_mixed", 1e-14)):
+        slp = operators.boundary.helmholtz.single_layer(sp, sp, sp, k, device_interface=interface)
+        dlp = operators.boundary.helmholtz.double_layer(sp, sp, sp, k, device_interface=interface)
+        ident = operators.boundary.sparse.identity(sp, sp, sp, device_interface=interface)
+        lhs = dlp - 0.5 * ident - 1j * k * slp
+        host = operators.weak_form_to_host(lhs, blocks=blocks)
+        assert host.is_pinned()
+        ref = lhs.weak_form().tensor.cpu()
+        assert (torch.linalg.norm(host - ref) / torch.linalg.norm(ref)).item() < tol
+    # a plain DP0 operator and a P1 operator (assembled whole, then copied)
+    for space in (sp, function_space(grid, "P", 1)):
+        op = operators.boundary.laplace.double_layer(space, space, space)
+        host = operators.weak_form_to_host(op, blocks=blocks)
+        ref = op.weak_form().tensor.cpu()
+        assert (torch.linalg.norm(host - ref) / torch.linalg.norm(ref)).item() < 1e-14
