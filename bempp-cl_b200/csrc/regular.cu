@@ -430,7 +430,13 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
                      a->test.nsupport == a->trial.nsupport && a->test_grid.geom == a->trial_grid.geom &&
                      a->test.normal_mult == a->trial.normal_mult && prm.ntest == prm.ntrial;
     const bool ranged = a->row_begin != 0 || a->row_end != 0;
-    if (ranged && (!sym || a->row_begin < 0 || a->row_end > prm.ntest || a->row_begin >= a->row_end)) {
+    // the kernels with a symmetric sweep, and its wavenumber condition (launch_dp0)
+    const bool laplace = a->kernel <= BEMPPCUDA_LAPLACE_ADLP;
+    const bool sym_kernel = laplace || a->kernel == BEMPPCUDA_HELMHOLTZ_SLP || a->kernel == BEMPPCUDA_HELMHOLTZ_DLP ||
+                            a->kernel == BEMPPCUDA_HELMHOLTZ_ADLP || a->kernel == BEMPPCUDA_HELMHOLTZ_COMBINED;
+    const bool sym_ok = sym && sym_kernel &&
+                        (laplace || (a->params[1] == 0.0 && (a->precision != BEMPPCUDA_MIXED || a->params[0] > 0.0)));
+    if (ranged && (!sym_ok || a->row_begin < 0 || a->row_end > prm.ntest || a->row_begin >= a->row_end)) {
         bc_set_error("row range [%lld, %lld) needs the symmetric sweep and 0 <= begin < end <= %lld rows",
                      (long long)a->row_begin, (long long)a->row_end, (long long)prm.ntest);
         return BEMPPCUDA_ERR_INVALID;

@@ -32,7 +32,17 @@ struct SingParams {
     const uint32_t *tl2g, *sl2g;
     const double *tmult, *smult;
     double diag_shift;
+    int64_t ntab, nw;  // point-table and weight-table lengths
 };
+
+// A pair whose element ids or table ranges fall outside the grid / tables is
+// skipped (caller-supplied tables are not trusted to be in range).
+__device__ __forceinline__ bool pair_in_range(const SingParams &prm, int64_t k) {
+    const int64_t t = prm.te[k], s = prm.se[k], n = prm.npts[k];
+    const int64_t toff = prm.toff[k], soff = prm.soff[k], woff = prm.woff[k];
+    return t >= 0 && t < prm.ne && s >= 0 && s < prm.ne && n >= 0 && toff >= 0 && soff >= 0 && woff >= 0 &&
+           toff + n <= prm.ntab && soff + n <= prm.ntab && woff + n <= prm.nw;
+}
 
 constexpr int SING_WARPS = 8;
 
@@ -40,7 +50,7 @@ template <int ASM, int K>
 __global__ void __launch_bounds__(32 * SING_WARPS) singular_pairs(SingParams prm) {
     const int lane = threadIdx.x & 31;
     const int64_t k = (int64_t)blockIdx.x * SING_WARPS + (threadIdx.x >> 5);
-    if (k >= prm.npairs) return;
+    if (k >= prm.npairs || !pair_in_range(prm, k)) return;
     const int64_t t = prm.te[k], s = prm.se[k];
     Geom gt, gs;
     load_geom(prm.g, prm.ne, t, prm.tnm ? (double)prm.tnm[t] : 1.0, gt);
@@ -212,7 +222,7 @@ template <int K, int PHC>
 __global__ void __launch_bounds__(32 * SING_WARPS) singular_dp0(SingParams prm) {
     const int lane = threadIdx.x & 31;
     const int64_t k = (int64_t)blockIdx.x * SING_WARPS + (threadIdx.x >> 5);
-    if (k >= prm.npairs) return;
+    if (k >= prm.npairs || !pair_in_range(prm, k)) return;
     const int64_t t = prm.te[k], s = prm.se[k];
     Geom gt, gs;
     load_geom(prm.g, prm.ne, t, prm.tnm ? (double)prm.tnm[t] : 1.0, gt);
@@ -301,6 +311,8 @@ int bc_singular_launch(const bemppcuda_singular_args *a, cudaStream_t st) {
     prm.tmult = a->test.mult;
     prm.smult = a->trial.mult;
     prm.diag_shift = a->diag_shift;
+    prm.ntab = a->npoints_table;
+    prm.nw = a->nweights;
     if (prm.npairs == 0) return BEMPPCUDA_OK;
     cudaError_t err = cudaSuccess;
     const bool real_k = a->params[1] == 0.0;

@@ -1,0 +1,188 @@
+"""Edge cases and corrupt inputs (run on a B200).
+
+Empty and tiny problems give the right (possibly empty) results; corrupt
+inputs — NaN or degenerate geometry, out-of-range indices, mismatched sizes,
+invalid row ranges, out-of-range singular pair tables — return an error status
+or are skipped without a GPU fault, and the context stays usable.
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def _usable():
+    torch.cuda.synchronize()
+    assert torch.ones(8, device="cuda").sum().item() == 8.0
+
+
+def _geometry_status(verts, elems):
+    from bempp_cuda import _lib
+    from bempp_cuda.device import current_stream, ptr
+
+    v = torch.as_tensor(np.asarray(verts, dtype=np.float64), device="cuda")
+    e = torch.as_tensor(np.asarray(elems, dtype=np.int32), device="cuda")
+    geom = torch.empty((_lib.GEOM_FIELDS, e.shape[0]), dtype=torch.float64, device="cuda")
+    rc = _lib.load().bemppcuda_grid_geometry(ptr(v), v.shape[0], ptr(e), e.shape[0], ptr(geom), current_stream())
+    return rc, _lib.last_error()
+
+
+def test_nan_and_degenerate_geometry_are_rejected():
+    from bempp_cuda import _lib
+
+    tri = [[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0]]
+    rc, msg = _geometry_status([[0.0, 0.0, np.nan], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0]], [[0, 1, 2]])
+    assert rc == _lib.ERR_INVALID and "non-finite" in msg
+    rc, msg = _geometry_status([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [2.0, 0.0, 0.0]], [[0, 1, 2]])  # collinear
+    assert rc == _lib.ERR_INVALID and "degenerate" in msg
+    rc, msg = _geometry_status(tri, [[0, 1, -1]])
+    assert rc == _lib.ERR_INVALID and "out of range" in msg
+    rc, msg = _geometry_status(tri, [[0, 1, 2]])
+    assert rc == _lib.OK
+    _usable()
+
+
+def test_mismatched_sizes_and_row_ranges_are_rejected():
+    from bempp_cuda import _lib, operators
+    from bempp_cuda.assembly import regular_into
+    from bempp_cuda.operators import Parameters
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+
+    grid = regular_sphere(2)
+    sp = function_space(grid, "DP", 0)
+    n = grid.number_of_elements
+    d = operators.boundary.helmholtz.single_layer(sp, sp, sp, 3.0).descriptor
+    narrow = torch.empty((n, n - 1), dtype=torch.complex128, device="cuda")
+    with pytest.raises(_lib.BemppCudaError) as exc:
+        regular_into(narrow, d, sp, sp, Parameters(), overwrite=True)
+    assert exc.value.status == _lib.ERR_INVALID
+    out = torch.empty((n, n), dtype=torch.complex128, device="cuda")
+    for rows in ((0, n + 1), (5, 5), (-1, 3)):
+        with pytest.raises(_lib.BemppCudaError) as exc:
+            regular_into(out, d, sp, sp, Parameters(), overwrite=True, rows=rows)
+        assert exc.value.status == _lib.ERR_INVALID
+    # a row range needs the symmetric sweep: complex wavenumber -> rejected, not ignored
+    dc = operators.boundary.helmholtz.single_layer(sp, sp, sp, 3.0 + 0.5j).descriptor
+    with pytest.raises(_lib.BemppCudaError) as exc:
+        regular_into(out, dc, sp, sp, Parameters(), overwrite=True, rows=(0, 8))
+    assert exc.value.status == _lib.ERR_INVALID
+    _usable()
+
+
+def test_out_of_range_singular_pairs_are_skipped():
+    """A caller table with a bad element id or offset: that pair is skipped, the others are assembled."""
+    from bempp_cuda import _lib, operators
+    from bempp_cuda.assembly import singular_into_dense
+    from bempp_cuda.device import device_singular_rule
+    from bempp_cuda.operators import Parameters
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+
+    grid = regular_sphere(1)
+    sp = function_space(grid, "DP", 0)
+    n = grid.number_of_elements
+    d = operators.boundary.laplace.single_layer(sp, sp, sp).descriptor
+    ref = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+    singular_into_dense(ref, d, sp, sp, Parameters())
+    rule = device_singular_rule(grid, 4, sp.support, sp.support)
+    saved = (rule.test_elements.clone(), rule.test_offsets.clone())
+    try:
+        rule.test_elements[0] = n + 1000  # element id past the grid
+        rule.test_offsets[1] = rule.npoints_table  # point range past the table
+        out = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+        singular_into_dense(out, d, sp, sp, Parameters())
+        _usable()
+    finally:
+        rule.test_elements.copy_(saved[0])
+        rule.test_offsets.copy_(saved[1])
+    diff = (out - ref).abs() > 1e-15 * ref.abs().max()
+    assert int(diff.sum().item()) <= 2  # only the two corrupted pairs are missing
+
+
+def test_empty_and_tiny_problems():
+    from bempp_cuda import operators
+    from bempp_cuda.grid import Grid
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+
+    # one triangle: a 1 x 1 DP0 matrix (the coincident pair only) against the oracle
+    from oracle import oracle as orc
+    from bempp_cuda.quadrature import SingularPairs, triangle_rule
+
+    g1 = Grid(np.array([[0.0, 1.0, 0.0], [0.0, 0.0, 1.0], [0.0, 0.0, 0.0]]), np.array([[0], [1], [2]], dtype=np.uint32))
+    sp1 = function_space(g1, "DP", 0)
+    for k in (None, 2.0):
+        op = (operators.boundary.laplace.single_layer(sp1, sp1, sp1) if k is None
+              else operators.boundary.helmholtz.single_layer(sp1, sp1, sp1, k))
+        a = op.weak_form().tensor.cpu().numpy()
+        qp, qw = triangle_rule(4)
+        rule = SingularPairs(g1, 4, sp1.support, sp1.support).arrays()
+        dsc = op.descriptor
+        b = orc.assemble_dense(dsc.kernel_type, dsc.assembly_type, dsc.options, dsc.is_complex, sp1, sp1, qp, qw, rule)
+        assert a.shape == (1, 1) and abs(a[0, 0] - b[0, 0]) <= 1e-13 * abs(b[0, 0])
+    # octahedron (8 elements): every symmetric tile is a diagonal tile
+    g0 = regular_sphere(0)
+    sp0 = function_space(g0, "DP", 0)
+    for sym in (True, False):
+        from bempp_cuda.assembly import regular_into
+        from bempp_cuda.operators import Parameters
+
+        out = torch.full((8, 8), np.nan, dtype=torch.complex128, device="cuda")
+        d = operators.boundary.helmholtz.double_layer(sp0, sp0, sp0, 1.5).descriptor
+        regular_into(out, d, sp0, sp0, Parameters(), overwrite=True, symmetric=sym)
+        assert torch.isfinite(torch.view_as_real(out)).all()
+    # potentials at zero points and an empty support
+    pot = operators.potential.laplace.single_layer(sp0, np.zeros((3, 0)))
+    assert pot.evaluate(np.ones(8)).shape == (1, 0)
+    empty = function_space(g0, "DP", 0, support_elements=np.arange(0))
+    assert empty.global_dof_count == 0
+    _usable()
+
+
+def test_batch_of_one_and_empty_batch():
+    from bempp_cuda import _lib
+    from bempp_cuda.batch import BatchAssembler
+    from bempp_cuda.shapes import regular_sphere
+
+    g = regular_sphere(2)
+    ba = BatchAssembler([g], [4.0])
+    ba.launch()
+    torch.cuda.synchronize()
+    assert torch.isfinite(torch.view_as_real(ba.outputs[0])).all()
+    with pytest.raises(ValueError):
+        BatchAssembler([], [])
+    ba.args.nproblems = 0
+    rc = _lib.load().bemppcuda_batch_launch(ctypes.byref(ba.args), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert rc == _lib.ERR_INVALID
+    _usable()
+
+
+def test_shape_gradient_on_the_octahedron():
+    """The smallest closed grid: every pair is adjacent except the opposite faces."""
+    from bempp_cuda.shape_gradient import FarFieldObjective, fibonacci_directions
+    from bempp_cuda.shapes import regular_sphere
+
+    obj = FarFieldObjective(regular_sphere(0), directions=fibonacci_directions(8))
+    x0 = obj.vertices.clone()
+    value, state = obj.evaluate(x0, 2.0, keep=True)
+    vgrad, kgrad = obj.gradient(state, 2.0)
+    h = 1e-6
+    for v, c in ((0, 0), (3, 2), (5, 1)):
+        xp = x0.clone()
+        xm = x0.clone()
+        xp[v, c] += h
+        xm[v, c] -= h
+        fd = (obj.evaluate(xp, 2.0).item() - obj.evaluate(xm, 2.0).item()) / (2 * h)
+        assert abs(vgrad[v, c].item() - fd) <= 1e-6 * vgrad.abs().max().item()

@@ -111,18 +111,19 @@ def test_full_gradient_against_central_differences(level):
     assert abs(kgrad.item() - fdk) <= 1e-6 * abs(fdk)
 
 
-def test_gradient_against_host_objective_differences():
+@pytest.mark.parametrize("level,count", [(2, 6), (3, 3)])
+def test_gradient_against_host_objective_differences(level, count):
     """Central differences of the oracle's J (host assembly, numpy solve) against the device adjoint."""
     from shape_oracle import host_objective
 
-    obj, k = _objective(2, seed=2)
+    obj, k = _objective(level, seed=2)
     x0 = obj.vertices.clone()
     value, state = obj.evaluate(x0, k, keep=True)
     vgrad, kgrad = obj.gradient(state, k)
     el = obj.base.elements.cpu().numpy()
     dirs = obj.directions.cpu().numpy()
     x0h = x0.cpu().numpy()
-    coords = _coords(obj.base.nvertices, 6, seed=11)
+    coords = _coords(obj.base.nvertices, count, seed=11)
     for v, c in coords:
         xp = x0h.copy()
         xm = x0h.copy()
