@@ -30,11 +30,17 @@ struct TestBlockP1 {
     double c[P1_TCHUNK][3];
     double curl[P1_TCHUNK][3][3];
     double ie[P1_TCHUNK];
+    double mult[P1_TCHUNK][3];  // local multipliers of the test functions
+    int64_t row[P1_TCHUNK][3];  // their global dofs
     int v[P1_TCHUNK][3];
 };
 
+#ifndef BC_P1_MIN_BLOCKS
+#define BC_P1_MIN_BLOCKS 1
+#endif
+
 template <int ASM, int K, int NT, int NS, int PHC, bool SYM>
-__global__ void __launch_bounds__(DP0_THREADS) regular_p1(RegParams prm, QuadRule rule) {
+__global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegParams prm, QuadRule rule) {
     constexpr bool HYP = (ASM == BEMPPCUDA_ASM_LAPLACE_HYP || ASM == BEMPPCUDA_ASM_HELM_HYP);
     constexpr bool HELM = (K == BEMPPCUDA_HELMHOLTZ_SLP || K == BEMPPCUDA_HELMHOLTZ_DLP ||
                            K == BEMPPCUDA_HELMHOLTZ_ADLP);
@@ -58,6 +64,11 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1(RegParams prm, QuadRul
             sb.n[idx][d] = g.n[d];
             sb.c[idx][d] = __ldg(prm.tg + (22 + d) * prm.tne + t);
             sb.v[idx][d] = __ldg(prm.tel + 3 * t + d);
+        }
+#pragma unroll
+        for (int i = 0; i < NT; ++i) {
+            sb.mult[idx][i] = prm.tmult[t * NT + i];
+            sb.row[idx][i] = prm.tl2g[t * NT + i];
         }
         if (HYP) {
             double cu[3][3];
@@ -99,6 +110,14 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1(RegParams prm, QuadRul
         }
     }
     const double kr = prm.p[0];
+    // the trial dofs and multipliers stay in registers for the whole tile
+    int64_t scol[NS];
+    double smul[NS];
+#pragma unroll
+    for (int j = 0; j < NS; ++j) {
+        scol[j] = prm.sl2g[s * NS + j];
+        smul[j] = prm.smult[s * NS + j];
+    }
     // (y_q - v0_s).n_s, the split of the double-layer normal term about the trial vertex 0
     double ynv[NQ6];
     if (DL)
@@ -200,12 +219,12 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1(RegParams prm, QuadRul
                            : 0.0;
 #pragma unroll
         for (int i = 0; i < NT; ++i) {
-            const double mt = prm.tmult[t * NT + i];
+            const double mt = sb.mult[tt][i];
             if (mt == 0.0) continue;
-            const int64_t row = prm.tl2g[t * NT + i];
+            const int64_t row = sb.row[tt][i];
 #pragma unroll
             for (int j = 0; j < NS; ++j) {
-                const double ms = prm.smult[s * NS + j];
+                const double ms = smul[j];
                 if (ms == 0.0) continue;
                 double vr = lre[i][j], vi = lim[i][j];
                 if (HYP) {
@@ -220,7 +239,7 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1(RegParams prm, QuadRul
                     vr = tr;
                 }
                 const double m = mt * ms * scale;
-                const int64_t col = prm.sl2g[s * NS + j];
+                const int64_t col = scol[j];
                 if (prm.is_complex) {
                     double *o = reinterpret_cast<double *>(prm.result) + 2 * (row * prm.ld + col);
                     atomicAdd(o, vr * m);

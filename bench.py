@@ -352,7 +352,7 @@ def gpu_arm(args, world, rank, local):
     breadth = None
     if not args.skip_breadth and world == 1:
         torch.cuda.empty_cache()
-        breadth = breadth_measure(args, torch)
+        breadth = breadth_measure(args, torch, peaks["fp64"])
     shape = None
     if not args.skip_shape and world == 1:
         torch.cuda.empty_cache()
@@ -625,19 +625,24 @@ def shape_measure(args, torch):
     return res
 
 
+# (name, factory path, domain space, dual space, level, wavenumber, algorithmic flops per point pair)
+# Flops per point pair (same convention as FLOPS_PER_QPE): kernels 13 (Laplace SLP), 20
+# (Helmholtz SLP), 30 (Helmholtz DLP / ADLP); a 3 x 3 shape product block adds 2 * 9 (P1);
+# the hypersingular form adds 2 * 9 more for the k^2 n.n term; Maxwell EFIE adds 9 x (5 for
+# the RWG dot product + 4 for the complex accumulation), MFIE 9 x (9 cross product + 5 dot
+# + 4 accumulation) on top of the Helmholtz DLP factor.
 BREADTH = [
-    # (name, factory path, domain space, dual space, level, wavenumber)
-    ("laplace.single_layer dp0", "laplace.single_layer", ("DP", 0), ("DP", 0), 4, None),
-    ("helmholtz.single_layer p1", "helmholtz.single_layer", ("P", 1), ("P", 1), 5, 5.0),
-    ("helmholtz.double_layer p1", "helmholtz.double_layer", ("P", 1), ("P", 1), 5, 5.0),
-    ("helmholtz.adjoint_double_layer p1", "helmholtz.adjoint_double_layer", ("P", 1), ("P", 1), 5, 5.0),
-    ("helmholtz.hypersingular p1", "helmholtz.hypersingular", ("P", 1), ("P", 1), 5, 5.0),
-    ("maxwell.electric_field rwg/snc", "maxwell.electric_field", ("RWG", 0), ("SNC", 0), 4, 2.0),
-    ("maxwell.magnetic_field rwg/snc", "maxwell.magnetic_field", ("RWG", 0), ("SNC", 0), 4, 2.0),
+    ("laplace.single_layer dp0", "laplace.single_layer", ("DP", 0), ("DP", 0), 4, None, 13),
+    ("helmholtz.single_layer p1", "helmholtz.single_layer", ("P", 1), ("P", 1), 5, 5.0, 38),
+    ("helmholtz.double_layer p1", "helmholtz.double_layer", ("P", 1), ("P", 1), 5, 5.0, 48),
+    ("helmholtz.adjoint_double_layer p1", "helmholtz.adjoint_double_layer", ("P", 1), ("P", 1), 5, 5.0, 48),
+    ("helmholtz.hypersingular p1", "helmholtz.hypersingular", ("P", 1), ("P", 1), 5, 5.0, 56),
+    ("maxwell.electric_field rwg/snc", "maxwell.electric_field", ("RWG", 0), ("SNC", 0), 4, 2.0, 101),
+    ("maxwell.magnetic_field rwg/snc", "maxwell.magnetic_field", ("RWG", 0), ("SNC", 0), 4, 2.0, 192),
 ]
 
 
-def breadth_measure(args, torch):
+def breadth_measure(args, torch, fp64_peak=None):
     """FP64 throughput of the other operator families (dense weak form through the operator API).
 
     GPU: CUDA events around the full assembly (regular + singular passes) of
@@ -676,7 +681,7 @@ def breadth_measure(args, torch):
         return (f(dom, dom, dual) if k is None else f(dom, dom, dual, k)), dom, dual
 
     out = []
-    for name, path, dsp, tsp, level, k in BREADTH:
+    for name, path, dsp, tsp, level, k, flops_pp in BREADTH:
         op, dom, dual = build(path, dsp, tsp, level, k)
         op._assemble()  # uploads and warms
         torch.cuda.synchronize()
@@ -693,6 +698,12 @@ def breadth_measure(args, torch):
         rows, cols = dual.global_dof_count, dom.global_dof_count
         entry = {"operator": name, "level": level, "k": k, "shape": [rows, cols],
                  "gpu_ms": float(np.median(ms)), "gpu_entries_per_s": rows * cols / (np.median(ms) * 1e-3)}
+        ne = dom.grid.number_of_elements
+        qpe = 36.0 * ne * ne  # regular point pairs of every element pair, counted per pair as the reference does
+        achieved = qpe * flops_pp / (np.median(ms) * 1e-3) / 1e12
+        entry["roofline"] = {"bound": "fp64", "flops_per_qpe": flops_pp, "qpe": qpe, "achieved": achieved,
+                             "unit": "TFLOP/s", "peak": fp64_peak,
+                             "frac": achieved / fp64_peak if fp64_peak else None}
         if not args.skip_cpu:
             op_c, dom_c, dual_c = build(path, dsp, tsp, level - 1, k)
             d = op_c.descriptor
@@ -744,8 +755,11 @@ def breadth_measure(args, torch):
     torch.cuda.synchronize()
     pms = e0.elapsed_time(e1) / max(args.steps, 1)
     qpe = 10000 * g.number_of_elements * 6
+    pach = qpe * 28 / (pms * 1e-3) / 1e12  # 20 (kernel) + 8 (complex multiply-accumulate) per point pair
     pentry = {"operator": "potential.helmholtz.single_layer p1", "level": 5, "k": 5.0, "points": 10000,
               "gpu_ms": pms, "gpu_qpe_per_s": qpe / (pms * 1e-3),
+              "roofline": {"bound": "fp64", "flops_per_qpe": 28, "qpe": qpe, "achieved": pach, "unit": "TFLOP/s",
+                           "peak": fp64_peak, "frac": pach / fp64_peak if fp64_peak else None},
               "note": "includes the host map_to_full_grid product and the coefficient upload"}
     if not args.skip_cpu:
         qp, qw = triangle_rule(4)
