@@ -238,7 +238,17 @@ def assemble_dense_to_host(domain, dual_to_range, parameters, descriptor, device
     if out is None:
         out = _torch.empty((rows, cols), dtype=dtype, pin_memory=True)
     if not symmetric_rows_eligible(descriptor, domain, dual_to_range, parameters):
-        dev = assemble_dense_device(domain, dual_to_range, parameters, descriptor, device_interface)
+        # whole operator on the device, then one copy (the fused-path steps of
+        # assemble_combined_field_device, with the identity shift)
+        fast = dp0_fast_path(descriptor, domain, dual_to_range, parameters)
+        dev = (_torch.empty if fast else _torch.zeros)((rows, cols), dtype=dtype, device="cuda")
+        precision = precision_of(device_interface)
+        regular_into(dev, descriptor, domain, dual_to_range, parameters,
+                     precision=precision if fast else _lib.FP64, overwrite=fast)
+        if _grids_identical(domain, dual_to_range):
+            singular_into_dense(dev, descriptor, domain, dual_to_range, parameters, diag_shift=diag_shift)
+        elif diag_shift != 0.0:
+            raise ValueError("an identity term needs identical domain and dual grids")
         out.copy_(dev, non_blocking=True)
         _torch.cuda.current_stream().synchronize()
         return out

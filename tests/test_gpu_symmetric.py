@@ -133,3 +133,27 @@ def test_weak_form_to_host_streams_row_blocks(blocks):
         host = operators.weak_form_to_host(op, blocks=blocks)
         ref = op.weak_form().tensor.cpu()
         assert (torch.linalg.norm(host - ref) / torch.linalg.norm(ref)).item() < 1e-14
+
+
+def test_weak_form_to_host_on_a_row_block():
+    """A row block of the combined field (dual restricted to some elements, as one rank assembles it)."""
+    import numpy as np
+
+    from bempp_cuda import operators
+    from bempp_cuda.shapes import ellipsoid
+    from bempp_cuda.space import function_space
+
+    grid = ellipsoid(3, 1.0, 0.8, 1.2)
+    d = function_space(grid, "DP", 0)
+    t = function_space(grid, "DP", 0, support_elements=np.arange(100, 300))
+    k = 5.0
+    slp = operators.boundary.helmholtz.single_layer(d, d, t, k)
+    dlp = operators.boundary.helmholtz.double_layer(d, d, t, k)
+    ident = operators.boundary.sparse.identity(d, d, t)
+    full_slp = operators.boundary.helmholtz.single_layer(d, d, d, k)
+    full_dlp = operators.boundary.helmholtz.double_layer(d, d, d, k)
+    full_id = operators.boundary.sparse.identity(d, d, d)
+    host = operators.weak_form_to_host(dlp - 0.5 * ident - 1j * k * slp)
+    ref = (full_dlp - 0.5 * full_id - 1j * k * full_slp).weak_form().tensor.cpu()[100:300]
+    assert host.shape == (200, grid.number_of_elements)
+    assert (torch.linalg.norm(host - ref) / torch.linalg.norm(ref)).item() < 1e-13
