@@ -401,6 +401,42 @@ def gpu_arm(args, world, rank, local):
     return line
 
 
+def hbm_peak():
+    """(GB/s, source): the driver's measured copy bandwidth, else the fallback figure of this pool."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured copy)"
+    except (OSError, ValueError, KeyError):
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def matvec_measure(torch, a64):
+    """GEMV on the resident matrix (the GMRES matvec): HBM-bound, one read of the matrix per product."""
+    peak, source = hbm_peak()
+    n = a64.shape[0]
+    out = {"peak_gbs": peak, "peak_source": source}
+    a32 = a64.to(torch.complex64)
+    for name, mat in (("complex128", a64), ("complex64", a32)):
+        x = torch.ones(n, dtype=mat.dtype, device="cuda")
+        for _ in range(3):
+            torch.mv(mat, x)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(10):
+            torch.mv(mat, x)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 10
+        nbytes = mat.numel() * mat.element_size()
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        out[name] = {"ms": ms, "bytes": nbytes, "gbs": gbs, "frac": gbs / peak}
+    del a32
+    torch.cuda.empty_cache()
+    return out
+
+
 def solve_measure(args, torch, grid, domain, a64, amx):
     """C3 solve: plane wave exp(i k z), FP64 GMRES vs mixed assembly + FP64-residual refinement."""
     from bempp_cuda.grid_function import GridFunction
@@ -418,6 +454,7 @@ def solve_measure(args, torch, grid, domain, a64, amx):
     torch.cuda.synchronize()
     t64 = time.perf_counter() - t0
     xmx, rinfo = solve_refined(amx, b, tol=1e-8, inner_tol=1e-4, restart=200)
+    matvec = matvec_measure(torch, a64)
     diff = float((torch.linalg.norm(xmx - x64) / torch.linalg.norm(x64)).item())
     res_true = float((torch.linalg.norm(b - torch.mv(a64, xmx)) / torch.linalg.norm(b)).item())
     return {"rhs": "projection of -exp(i k z) onto DP0", "tol": 1e-8,
@@ -425,7 +462,8 @@ def solve_measure(args, torch, grid, domain, a64, amx):
             "mixed_refined": {"refinements": rinfo["refinements"], "inner_iterations": rinfo["inner_iterations"],
                               "residuals": rinfo["relative_residuals"], "seconds": rinfo["seconds"],
                               "inner_dtype": "complex64"},
-            "solution_rel_diff_vs_fp64": diff, "mixed_solution_residual_in_fp64_operator": res_true}
+            "solution_rel_diff_vs_fp64": diff, "mixed_solution_residual_in_fp64_operator": res_true,
+            "matvec": matvec}
 
 
 def batch_measure(args, torch, world, rank, dist, count=64, levels=(3, 4, 5)):
