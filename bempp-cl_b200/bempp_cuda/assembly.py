@@ -105,6 +105,8 @@ def regular_into(
     """
     require_cuda()
     kernel, assembly = kernel_ids(descriptor)
+    if result.numel() == 0:
+        return result  # a space without dofs: nothing to assemble
     tgrid = geometry or device_grid(dual_to_range.grid)
     sgrid = geometry or device_grid(domain.grid)
     sspace = device_space(domain)
@@ -155,6 +157,8 @@ def singular_into_dense(result, descriptor, domain, dual_to_range, parameters, d
     elements lo .. hi-1 of ``dual_to_range`` (support in increasing order).
     """
     kernel, assembly = kernel_ids(descriptor)
+    if result.numel() == 0:
+        return result
     grid = domain.grid
     rule = device_singular_rule(grid, parameters.quadrature.singular, dual_to_range.support, domain.support)
     args = _lib.SingularArgs()

@@ -186,3 +186,33 @@ def test_shape_gradient_on_the_octahedron():
         xm[v, c] -= h
         fd = (obj.evaluate(xp, 2.0).item() - obj.evaluate(xm, 2.0).item()) / (2 * h)
         assert abs(vgrad[v, c].item() - fd) <= 1e-6 * vgrad.abs().max().item()
+
+
+def _two_element_grid():
+    from bempp_cuda.grid import Grid
+
+    verts = np.array([[0.0, 1.0, 0.0, 1.0], [0.0, 0.0, 1.0, 1.0], [0.0, 0.0, 0.0, 0.2]])
+    elems = np.array([[0, 1], [1, 3], [2, 2]], dtype=np.uint32)  # triangles (0,1,2) and (1,3,2) share an edge
+    return Grid(verts, elems)
+
+
+@pytest.mark.parametrize("which", ["octahedron", "two_elements"])
+def test_every_boundary_operator_on_extreme_adjacency(which, oracle):
+    """All operator x space cases where (almost) every element pair is adjacent: against the oracle."""
+    from cases import BOUNDARY, boundary_operator, oracle_dense
+
+    from bempp_cuda.shapes import regular_sphere
+
+    grid = regular_sphere(0) if which == "octahedron" else _two_element_grid()
+    for key in BOUNDARY:
+        if which == "two_elements" and key.startswith("maxwell"):
+            continue  # one interior edge: RWG / SNC have a single dof; covered on the octahedron
+        op, domain, dual = boundary_operator(key, grid)
+        got = op.weak_form().tensor.cpu().numpy()
+        if domain.global_dof_count == 0 or dual.global_dof_count == 0:
+            # P1 on the open two-element grid: every vertex is a boundary vertex, no dofs
+            assert got.shape == (dual.global_dof_count, domain.global_dof_count), key
+            continue
+        ref = oracle_dense(oracle, op, domain, dual)
+        scale = max(np.linalg.norm(ref), 1e-300)
+        assert np.linalg.norm(got - ref) <= 1e-12 * scale, key
