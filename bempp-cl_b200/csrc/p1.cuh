@@ -35,6 +35,8 @@ struct TestBlockP1 {
     int v[P1_TCHUNK][3];
 };
 
+// CTAs per SM the P1 kernel is compiled for: no cap (184-214 registers) beat
+// a cap of 3 on the double layer and hypersingular operators at L5.
 #ifndef BC_P1_MIN_BLOCKS
 #define BC_P1_MIN_BLOCKS 1
 #endif
