@@ -154,6 +154,7 @@ class PotentialArgs(_ct.Structure):
         ("result", _vp),
         ("workspace", _vp),
         ("workspace_bytes", _i64),
+        ("phase_radius", _ct.c_double),
     ]
 
 

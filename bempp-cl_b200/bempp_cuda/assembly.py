@@ -351,5 +351,6 @@ def evaluate_potential_device(space, descriptor, points, local_coefficients, par
     workspace = _torch.empty(max(need // 8, 1), dtype=_torch.float64, device="cuda")
     args.workspace = ptr(workspace)
     args.workspace_bytes = need
+    args.phase_radius = 1.0001 * dgrid.radius
     _lib.check(_lib.load().bemppcuda_evaluate_potential(args, stream or current_stream()))
     return result

@@ -110,7 +110,7 @@ __device__ __forceinline__ cplx greens(const double x[3], const double y[3], con
                                        const double p[4]) {
     double d0 = y[0] - x[0], d1 = y[1] - x[1], d2 = y[2] - x[2];
     double r2 = fma(d2, d2, fma(d1, d1, d0 * d0));
-    double rinv = rsqrt(r2);
+    double rinv = rsqrt64(r2);
     double r = r2 * rinv;
     if (K == BEMPPCUDA_LAPLACE_SLP) {
         return {BC_INV_4PI * rinv, 0.0};

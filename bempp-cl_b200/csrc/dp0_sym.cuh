@@ -124,7 +124,7 @@ __device__ __forceinline__ void regular_dp0_fp64_sym_tile(const RegParams &prm, 
                 for (int q = 0; q < NQ6; ++q) {
                     const double d0 = y[q][0] - x0, d1 = y[q][1] - x1, d2 = y[q][2] - x2;
                     const double r2 = fma(d2, d2, fma(d1, d1, d0 * d0));
-                    const double rinv = rsqrt(r2);
+                    const double rinv = rsqrt64(r2);
                     const double f = rule.w[q] * rinv;
                     if (!ST::helm) {
                         if (ST::slp_part) pr += f;

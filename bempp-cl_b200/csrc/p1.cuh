@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
             for (int q = 0; q < NQ6; ++q) {
                 const double d0 = y[q][0] - x0, d1 = y[q][1] - x1, d2 = y[q][2] - x2;
                 const double r2 = fma(d2, d2, fma(d1, d1, d0 * d0));
-                const double rinv = rsqrt(r2);
+                const double rinv = rsqrt64(r2);
                 double kre, kim = 0.0;  // kernel value without 1/(4 pi)
                 if (!HELM) {
                     if (K == BEMPPCUDA_LAPLACE_SLP) {

@@ -10,15 +10,22 @@
 //  1. potential_sources: one thread per (element, quadrature point) writes the
 //     source point, normal and weighted coefficient(s) field-major into the
 //     caller's workspace (the reference's `tmp` arrays).
-//  2. potential_eval: one warp owns PPW evaluation points; its lanes stride
-//     over the sources with coalesced loads, accumulate per point in FP64 and
-//     combine with xor-shuffle reductions; lane 0 writes.
+//  2. potential_scalar (Laplace and Helmholtz single / double layer with a
+//     real wavenumber): a thread per evaluation point walks the sources staged
+//     in shared memory; see the comment above the kernel.
+//     potential_eval (every other case): one warp owns PPW evaluation points;
+//     its lanes stride over the sources with coalesced loads, accumulate per
+//     point in FP64 and combine with xor-shuffle reductions; lane 0 writes.
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace bc {
 
-// workspace fields per source
-constexpr int SRC_FIELDS = 14;  // y(3) n(3) c0re c0im c1re c1im c2re c2im dre dim
+// workspace fields per source: y(3) n(3) then
+//   scalar:  cre cim, and fields 8-10 at index ei (< nsupport) hold element ei's centroid
+//   Maxwell: c0re c0im c1re c1im c2re c2im dre dim
+constexpr int SRC_FIELDS = 14;
 constexpr int POT_PPW = 4;
 constexpr int POT_WARPS = 4;
 
@@ -70,6 +77,13 @@ __global__ void potential_sources(PotParams prm, QuadRule rule) {
         }
         o[6 * n + k] = cr;
         o[7 * n + k] = ci;
+        if (q == 0) {
+            // element centroid, indexed by support position, for the phase factoring of potential_scalar
+            double c[3];
+            to_global(g, 1.0 / 3.0, 1.0 / 3.0, c);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) o[(8 + d) * n + ei] = c[d];
+        }
     } else {
         double b[3][3];
         rwg_values(g, rule.x[q], rule.y[q], b);
@@ -228,6 +242,217 @@ static cudaError_t launch_pot(const PotParams &prm, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+
+// ---------------------------------------------------------------------------
+// Scalar Laplace / Helmholtz potentials, a thread per evaluation point.
+//
+// Each thread owns PS_PPT points and walks the sources of its chunk, which the
+// block stages in shared memory PS_SOURCES at a time and reads back as
+// broadcasts.  The grid is (point blocks, source chunks): ten thousand points
+// make only a few dozen blocks of 256 points, so the support is split into
+// chunks of whole elements until the grid covers the SMs several times, and
+// the chunks' partial sums are added into the zeroed result with FP64
+// atomics (a single chunk stores directly).
+//
+// Helmholtz phase (real k): for a source y of element e with centroid c_e,
+//   k |x - y| = k |x - c_e| + k (|x - y| - |x - c_e|),
+// where |x - y| - |x - c_e| is at most |y - c_e| <= R, the grid's largest
+// centroid-to-vertex distance.  With k R <= 1/2 (PHC 2) or <= 1 (PHC 1) the
+// second part needs no range reduction (sincos_half64 / sincos_small64); the
+// element's partial sum is rotated once by exp(i k |x - c_e|) (sincos_cw64).
+// PHC 0 reduces the full phase per source.
+constexpr int PS_THREADS = 128;
+constexpr int PS_PPT = 2;
+constexpr int PS_SOURCES = 384;
+constexpr int PS_CHUNK_MIN = 16;  // fewest elements in a source chunk
+
+template <int PHC>
+__device__ __forceinline__ void phase_small(double t, double *s, double *c) {
+    if (PHC == 2)
+        sincos_half64(t, s, c);
+    else if (PHC == 1)
+        sincos_small64(t, s, c);
+    else
+        sincos_cw64(t, s, c);
+}
+
+template <int K, int PHC, int NQ>
+__global__ void __launch_bounds__(PS_THREADS) potential_scalar(PotParams prm, int64_t chunk_elems) {
+    constexpr bool HELM = (K == BEMPPCUDA_HELMHOLTZ_SLP || K == BEMPPCUDA_HELMHOLTZ_DLP);
+    constexpr bool DLP = (K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_HELMHOLTZ_DLP);
+    constexpr bool FACTOR = HELM && PHC > 0;
+    __shared__ double2 ssrc[PS_SOURCES * 4];        // {y0 y1} {y2 cre} {cim n0} {n1 n2}
+    __shared__ double2 scen[FACTOR ? PS_SOURCES * 2 : 2];  // {c0 c1} {c2 -} per element
+    const int nq = NQ ? NQ : prm.nq;
+    const int tile_elems = PS_SOURCES / nq;
+    const int64_t ebeg = (int64_t)blockIdx.y * chunk_elems;
+    const int64_t eend = min(ebeg + chunk_elems, prm.nsupport);
+    const int64_t pbase = (int64_t)blockIdx.x * (PS_THREADS * PS_PPT) + threadIdx.x;
+    double x[PS_PPT][3], ar[PS_PPT], ai[PS_PPT];
+#pragma unroll
+    for (int j = 0; j < PS_PPT; ++j) {
+        const int64_t pj = min(pbase + j * PS_THREADS, prm.npoints - 1);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) x[j][d] = prm.points[3 * pj + d];
+        ar[j] = ai[j] = 0.0;
+    }
+    const double k = prm.p[0];
+    const int64_t n = prm.nsrc;
+    const double *o = prm.src;
+    for (int64_t t0 = ebeg; t0 < eend; t0 += tile_elems) {
+        const int te = (int)min((int64_t)tile_elems, eend - t0);
+        const int ns = te * nq;
+        const int64_t s0 = t0 * nq;
+        __syncthreads();
+        for (int s = threadIdx.x; s < ns; s += PS_THREADS) {
+            const int64_t gs = s0 + s;
+            ssrc[4 * s + 0] = make_double2(o[gs], o[n + gs]);
+            ssrc[4 * s + 1] = make_double2(o[2 * n + gs], o[6 * n + gs]);
+            ssrc[4 * s + 2] = make_double2(o[7 * n + gs], DLP ? o[3 * n + gs] : 0.0);
+            if (DLP) ssrc[4 * s + 3] = make_double2(o[4 * n + gs], o[5 * n + gs]);
+        }
+        if (FACTOR) {
+            for (int e = threadIdx.x; e < te; e += PS_THREADS) {
+                const int64_t ge = t0 + e;
+                scen[2 * e] = make_double2(o[8 * n + ge], o[9 * n + ge]);
+                scen[2 * e + 1] = make_double2(o[10 * n + ge], 0.0);
+            }
+        }
+        __syncthreads();
+        for (int e = 0; e < te; ++e) {
+            double krc[PS_PPT], er[PS_PPT], ei[PS_PPT];
+#pragma unroll
+            for (int j = 0; j < PS_PPT; ++j) {
+                krc[j] = 0.0;
+                if (FACTOR) {
+                    const double2 c01 = scen[2 * e], c2 = scen[2 * e + 1];
+                    const double d0 = c01.x - x[j][0], d1 = c01.y - x[j][1], d2 = c2.x - x[j][2];
+                    const double rc2 = fma(d2, d2, fma(d1, d1, d0 * d0));
+                    krc[j] = rc2 > 0.0 ? k * (rc2 * rsqrt64(rc2)) : 0.0;  // a point may sit on a centroid
+                }
+                er[j] = ei[j] = 0.0;
+            }
+#pragma unroll 6
+            for (int q = 0; q < nq; ++q) {
+                const int s = e * nq + q;
+                const double2 y01 = ssrc[4 * s], y2c = ssrc[4 * s + 1], cin = ssrc[4 * s + 2];
+                double2 n12 = make_double2(0.0, 0.0);
+                if (DLP) n12 = ssrc[4 * s + 3];
+                const double cr = y2c.y, ci = cin.x;
+#pragma unroll
+                for (int j = 0; j < PS_PPT; ++j) {
+                    const double d0 = y01.x - x[j][0], d1 = y01.y - x[j][1], d2 = y2c.x - x[j][2];
+                    const double r2 = fma(d2, d2, fma(d1, d1, d0 * d0));
+                    const double rinv = rsqrt64(r2);
+                    // f: real factor of the kernel without 1/(4 pi) and phase
+                    double f = rinv;
+                    if (DLP) {
+                        const double dot = fma(d2, n12.y, fma(d1, n12.x, d0 * cin.y));
+                        f = dot * rinv * rinv * rinv;
+                    }
+                    if (!HELM) {
+                        if (DLP) f = -f;
+                        er[j] = fma(f, cr, er[j]);
+                        ei[j] = fma(f, ci, ei[j]);
+                    } else {
+                        const double r = r2 * rinv;
+                        double sn, cs;
+                        phase_small<PHC>(FACTOR ? fma(k, r, -krc[j]) : k * r, &sn, &cs);
+                        double wr = f * cr, wi = f * ci;  // f times the coefficient
+                        if (DLP) {
+                            // times (i k r - 1)
+                            const double b = k * r;
+                            const double tr = -fma(b, wi, wr), ti = fma(b, wr, -wi);
+                            wr = tr;
+                            wi = ti;
+                        }
+                        er[j] = fma(cs, wr, fma(-sn, wi, er[j]));
+                        ei[j] = fma(cs, wi, fma(sn, wr, ei[j]));
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < PS_PPT; ++j) {
+                if (FACTOR) {
+                    double sn, cs;
+                    sincos_cw64(krc[j], &sn, &cs);
+                    ar[j] = fma(cs, er[j], fma(-sn, ei[j], ar[j]));
+                    ai[j] = fma(cs, ei[j], fma(sn, er[j], ai[j]));
+                } else {
+                    ar[j] += er[j];
+                    ai[j] += ei[j];
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < PS_PPT; ++j) {
+        const int64_t pj = pbase + j * PS_THREADS;
+        if (pj >= prm.npoints) break;
+        double *out = prm.result + 2 * pj;
+        if (gridDim.y == 1) {
+            out[0] = BC_INV_4PI * ar[j];
+            out[1] = BC_INV_4PI * ai[j];
+        } else {
+            atomicAdd(out, BC_INV_4PI * ar[j]);
+            atomicAdd(out + 1, BC_INV_4PI * ai[j]);
+        }
+    }
+}
+
+template <int K, int PHC>
+static cudaError_t launch_scalar_nq(const PotParams &prm, dim3 grid, int64_t chunk_elems, cudaStream_t st) {
+    if (prm.nq == 6)
+        potential_scalar<K, PHC, 6><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems);
+    else
+        potential_scalar<K, PHC, 0><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems);
+    return cudaGetLastError();
+}
+
+// Number of SMs of the current device, looked up once per device.
+static int sm_count() {
+    static int cached[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (!cached[dev]) {
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+        cached[dev] = sms;
+    }
+    return cached[dev];
+}
+
+// Scalar Laplace / Helmholtz potential with a real wavenumber; phase_radius
+// bounds every source's distance from its element centroid (0: unknown).
+static cudaError_t launch_scalar(const PotParams &prm, int kernel, double phase_radius, cudaStream_t st) {
+    const int64_t pblocks = (prm.npoints + PS_THREADS * PS_PPT - 1) / (PS_THREADS * PS_PPT);
+    const int64_t target = (int64_t)sm_count() * 8;  // CTAs: several waves of 4 resident per SM
+    int64_t chunks = (target + pblocks - 1) / pblocks;
+    chunks = std::min(chunks, (prm.nsupport + PS_CHUNK_MIN - 1) / PS_CHUNK_MIN);
+    chunks = std::max<int64_t>(1, std::min<int64_t>(chunks, 65535));
+    const int64_t chunk_elems = (prm.nsupport + chunks - 1) / chunks;
+    chunks = (prm.nsupport + chunk_elems - 1) / chunk_elems;
+    if (chunks > 1) {
+        const cudaError_t err = cudaMemsetAsync(prm.result, 0, sizeof(double) * 2 * prm.npoints, st);
+        if (err != cudaSuccess) return err;
+    }
+    const dim3 grid((unsigned)pblocks, (unsigned)chunks);
+    const double kr = fabs(prm.p[0]) * phase_radius;
+    const int phc = (phase_radius > 0.0 && kr <= 0.5) ? 2 : (phase_radius > 0.0 && kr <= 1.0) ? 1 : 0;
+    switch (kernel) {
+    case BEMPPCUDA_LAPLACE_SLP: return launch_scalar_nq<BEMPPCUDA_LAPLACE_SLP, 0>(prm, grid, chunk_elems, st);
+    case BEMPPCUDA_LAPLACE_DLP: return launch_scalar_nq<BEMPPCUDA_LAPLACE_DLP, 0>(prm, grid, chunk_elems, st);
+    case BEMPPCUDA_HELMHOLTZ_SLP:
+        if (phc == 2) return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_SLP, 2>(prm, grid, chunk_elems, st);
+        if (phc == 1) return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_SLP, 1>(prm, grid, chunk_elems, st);
+        return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_SLP, 0>(prm, grid, chunk_elems, st);
+    default:  // BEMPPCUDA_HELMHOLTZ_DLP
+        if (phc == 2) return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_DLP, 2>(prm, grid, chunk_elems, st);
+        if (phc == 1) return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_DLP, 1>(prm, grid, chunk_elems, st);
+        return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_DLP, 0>(prm, grid, chunk_elems, st);
+    }
+}
+
 }  // namespace bc
 
 using namespace bc;
@@ -271,7 +496,12 @@ int bc_potential_launch(const bemppcuda_potential_args *a, double *workspace, cu
     }
     cudaError_t err = cudaGetLastError();
     if (err == cudaSuccess) {
-        if (!maxwell) {
+        const bool real_k = a->params[1] == 0.0;
+        const bool per_point = a->kernel == BEMPPCUDA_LAPLACE_SLP || a->kernel == BEMPPCUDA_LAPLACE_DLP ||
+                               ((a->kernel == BEMPPCUDA_HELMHOLTZ_SLP || a->kernel == BEMPPCUDA_HELMHOLTZ_DLP) && real_k);
+        if (!maxwell && per_point && prm.nsupport > 0) {
+            err = launch_scalar(prm, a->kernel, a->phase_radius, st);
+        } else if (!maxwell) {
             switch (a->kernel) {
             case BEMPPCUDA_LAPLACE_SLP: err = launch_pot<0, BEMPPCUDA_LAPLACE_SLP>(prm, st); break;
             case BEMPPCUDA_LAPLACE_DLP: err = launch_pot<0, BEMPPCUDA_LAPLACE_DLP>(prm, st); break;

@@ -77,8 +77,10 @@ struct ShapeParams {
     void *out;
 };
 
+// gd = a1 d / r^2 + a2 c_s is formed by the caller: the symmetric sweep adds
+// the two ordered pairs' gradients before multiplying by d.
 struct QpeTerms {
-    double gd[3];
+    double a1;  // a1 r^2
     double a2, ival, ere, kval;
 };
 
@@ -102,15 +104,12 @@ __device__ __forceinline__ void qpe_ordered(const double d[3], double r, double 
     const double reGzEta = Zr * P.eta_re - Zi * P.eta_im;
     const double t1 = fma(Gr, 3.0 - kr * kr, 3.0 * kr * Gi);  // Re(Gc (3 - k^2 r^2 - 3ikr))
     const double bu = bet * u;
-    const double a1 = fma(bu, t1, ies * reGzEta) * rinv2;
-    const double a2 = bet * Zr * rinv2;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) o.gd[c] = fma(a1, d[c], a2 * cs[c]);
-    o.a2 = a2;
+    o.a1 = fma(bu, t1, ies * reGzEta);
+    o.a2 = bet * Zr * rinv2;
     o.ival = fma(bu, Zr, ies * reGcEta);
     o.ere = reGcEta;
     const double er = P.deta_re - P.eta_im * r, ei = fma(P.eta_re, r, P.deta_im);
-    o.kval = fma(-bu * P.k * r * r, Gr, ies * (Gr * er - Gi * ei));
+    o.kval = fma(-bu * (kr * r), Gr, ies * (Gr * er - Gi * ei));
 }
 
 // exp(i theta) for the phase offset theta = k (r - r_c) of class PHC (0: any
@@ -184,8 +183,11 @@ __global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadR
 #pragma unroll
         for (int q = 0; q < SH_NQ; ++q) y[q][0] = y[q][1] = y[q][2] = 0.0;
     }
-    // column sums (layout of the workspace, fields 0-13)
-    double cT[3] = {0.0, 0.0, 0.0}, cX[3] = {0.0, 0.0, 0.0}, cY[3] = {0.0, 0.0, 0.0}, cC[3] = {0.0, 0.0, 0.0};
+    // column sums: dF/dy per column quadrature point (fields 0-8 are formed from
+    // them at the end), then fields 9-13 of the workspace layout
+    double cQ[SH_NQ][3], cC[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int q = 0; q < SH_NQ; ++q) cQ[q][0] = cQ[q][1] = cQ[q][2] = 0.0;
     double cI = 0.0, cK = 0.0;
 
     for (int tile = 0; tile < SH_TILES; ++tile) {
@@ -240,13 +242,13 @@ __global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadR
                 const double ct[3] = {sb.cr[tt][0], sb.cr[tt][1], sb.cr[tt][2]};
                 for (int p = 0; p < SH_NQ; ++p) {
                     const double x0 = sb.x[tt][p][0], x1 = sb.x[tt][p][1], x2 = sb.x[tt][p][2];
-                    const double wp = rule.w[p];
+                    const double wp = rule.w[p] * BC_INV_4PI;
                     double pp[3] = {0.0, 0.0, 0.0};  // row-element point derivative at x_p
 #pragma unroll
                     for (int q = 0; q < SH_NQ; ++q) {
                         const double d[3] = {y[q][0] - x0, y[q][1] - x1, y[q][2] - x2};
                         const double r2 = fma(d[2], d[2], fma(d[1], d[1], d[0] * d[0]));
-                        const double rinv = rsqrt(r2);
+                        const double rinv = rsqrt64(r2);
                         const double r = r2 * rinv;
                         const double rinv2 = rinv * rinv;
                         double sn, cn;
@@ -254,7 +256,7 @@ __global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadR
                             phase64<PHC>(P.k * (r - rc), &sn, &cn);
                         else
                             sincos_cw64(P.k * r, &sn, &cn);
-                        const double f = wp * rule.w[q] * rinv * BC_INV_4PI;
+                        const double f = (wp * rule.w[q]) * rinv;
                         const double gr = cn * f, gi = sn * f;
                         QpeTerms o1, o2;
                         // (i, j): x in i (test), y in j (trial), d = y - x
@@ -263,12 +265,12 @@ __global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadR
                         const double dn[3] = {-d[0], -d[1], -d[2]};
                         qpe_ordered(dn, r, rinv2, gr, gi, c2r, c2i, ct, iet, bett, P, o2);
                         // column element j: trial of (i, j) (+gd1), test of (j, i) (-gd2)
+                        // gd of (i, j) minus gd of (j, i): (a1_1 + a1_2) d / r^2 + a2_1 c_j - a2_2 c_i
+                        const double a1s = (o1.a1 + o2.a1) * rinv2;
 #pragma unroll
                         for (int c = 0; c < 3; ++c) {
-                            const double gj = o1.gd[c] - o2.gd[c];
-                            cT[c] += gj;
-                            cX[c] = fma(rule.x[q], gj, cX[c]);
-                            cY[c] = fma(rule.y[q], gj, cY[c]);
+                            const double gj = fma(a1s, d[c], fma(o1.a2, cs[c], -o2.a2 * ct[c]));
+                            cQ[q][c] += gj;
                             cC[c] = fma(o1.a2, d[c], cC[c]);
                             pp[c] -= gj;  // row element i: test of (i, j) (-gd1), trial of (j, i) (+gd2)
                             rs[9 + c] = fma(o2.a2, dn[c], rs[9 + c]);
@@ -304,9 +306,16 @@ __global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadR
         double *a = P.acc + s * SH_ACC;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            atomicAdd(a + c, cT[c]);
-            atomicAdd(a + 3 + c, cX[c]);
-            atomicAdd(a + 6 + c, cY[c]);
+            double cT = 0.0, cX = 0.0, cY = 0.0;
+#pragma unroll
+            for (int q = 0; q < SH_NQ; ++q) {
+                cT += cQ[q][c];
+                cX = fma(rule.x[q], cQ[q][c], cX);
+                cY = fma(rule.y[q], cQ[q][c], cY);
+            }
+            atomicAdd(a + c, cT);
+            atomicAdd(a + 3 + c, cX);
+            atomicAdd(a + 6 + c, cY);
             atomicAdd(a + 9 + c, cC[c]);
         }
         atomicAdd(a + 12, cI);
@@ -342,20 +351,23 @@ __global__ void __launch_bounds__(32 * SHS_WARPS) shape_singular(ShapeParams P) 
         to_global(gs, spm.x, spm.y, y);
         const double d[3] = {y[0] - x[0], y[1] - x[1], y[2] - x[2]};
         const double r2 = fma(d[2], d[2], fma(d[1], d[1], d[0] * d[0]));
-        const double rinv = rsqrt(r2);
+        const double rinv = rsqrt64(r2);
         const double r = r2 * rinv;
         double sn, cn;
         sincos_cw64(P.k * r, &sn, &cn);
         const double f = w * rinv * BC_INV_4PI;
         QpeTerms o;
-        qpe_ordered(d, r, rinv * rinv, cn * f, sn * f, cre, cim, cs, ies, bet, P, o);
+        const double rinv2 = rinv * rinv;
+        qpe_ordered(d, r, rinv2, cn * f, sn * f, cre, cim, cs, ies, bet, P, o);
+        const double a1 = o.a1 * rinv2;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            a[c] += o.gd[c];
-            a[3 + c] = fma(tpm.x, o.gd[c], a[3 + c]);
-            a[6 + c] = fma(tpm.y, o.gd[c], a[6 + c]);
-            a[9 + c] = fma(spm.x, o.gd[c], a[9 + c]);
-            a[12 + c] = fma(spm.y, o.gd[c], a[12 + c]);
+            const double gd = fma(a1, d[c], o.a2 * cs[c]);
+            a[c] += gd;
+            a[3 + c] = fma(tpm.x, gd, a[3 + c]);
+            a[6 + c] = fma(tpm.y, gd, a[6 + c]);
+            a[9 + c] = fma(spm.x, gd, a[9 + c]);
+            a[12 + c] = fma(spm.y, gd, a[12 + c]);
             a[15 + c] = fma(o.a2, d[c], a[15 + c]);
         }
         a[18] += o.ival;

@@ -53,7 +53,7 @@ __device__ __forceinline__ void sing_dp0_value(const double *__restrict__ g, int
         to_global(gs, spm.x, spm.y, y);
         const double d0 = y[0] - x[0], d1 = y[1] - x[1], d2 = y[2] - x[2];
         const double r2 = fma(d2, d2, fma(d1, d1, d0 * d0));
-        const double rinv = rsqrt(r2);
+        const double rinv = rsqrt64(r2);
         const double f = wm * rinv;
         double dot = 0.0;
         if (T::dl || T::ad) dot = (T::ad ? -1.0 : 1.0) * fma(d2, nv[2], fma(d1, nv[1], d0 * nv[0]));

@@ -183,6 +183,9 @@ typedef struct {
     void *result;               /* complex128 (kdim, npoints) */
     void *workspace;            /* bemppcuda_potential_workspace_bytes() bytes */
     int64_t workspace_bytes;
+    double phase_radius;  /* largest centroid-to-vertex distance of the source grid, or 0 (unknown):
+                             scalar potentials with a real wavenumber factor exp(ikr) about each
+                             element's centroid and skip the range reduction when |k| R <= 1 */
 } bemppcuda_potential_args;
 
 /* Batched DP0 assembly (many grids / wavenumbers in one persistent launch).

@@ -1,0 +1,170 @@
+"""The per-point scalar potential kernel against the oracle (run on a B200).
+
+Laplace and Helmholtz (real wavenumber) single / double layer potentials go
+through ``potential_scalar``: a thread per evaluation point, sources staged in
+shared memory, the support split into chunks added with atomics, and the
+Helmholtz phase factored about each element's centroid when k R <= 1
+(R = largest centroid-to-vertex distance).  The cases below reach every phase
+class (k R <= 1/2, <= 1, above 1, and R unknown), both rule branches (six
+points and a general rule size), a single chunk (direct store) and many
+chunks, ragged point counts, and points on element centroids and very close to
+the surface.  Tolerance: 1e-12 relative Frobenius norm, as for the other FP64
+paths.
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import rel_fro
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def _operator(name, space, points, k, parameters=None):
+    from bempp_cuda import operators
+
+    family = operators.potential.laplace if k is None else operators.potential.helmholtz
+    factory = getattr(family, name)
+    return factory(space, points, parameters=parameters) if k is None else factory(space, points, k,
+                                                                                   parameters=parameters)
+
+
+def _check(oracle, op, space, seed=5, tol=1e-12):
+    from cases import oracle_potential
+
+    rng = np.random.default_rng(seed)
+    n = space.global_dof_count
+    coeffs = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    got = op.evaluate_device(coeffs).cpu().numpy()
+    ref = oracle_potential(oracle, op, space, coeffs)
+    assert got.shape == ref.shape
+    assert np.all(np.isfinite(got))
+    assert rel_fro(got, ref) < tol
+    return got
+
+
+@pytest.mark.parametrize("kr", [0.3, 0.8, 3.0])
+@pytest.mark.parametrize("name", ["single_layer", "double_layer"])
+@pytest.mark.parametrize("family", ["DP0", "P1"])
+def test_helmholtz_every_phase_class(oracle, kr, name, family):
+    """k R = 0.3, 0.8, 3.0 select the three phase classes; 3000 shell points split into several chunks."""
+    from bempp_cuda.device import device_grid
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+    from cases import sphere_shell_points
+
+    grid = regular_sphere(3)
+    space = function_space(grid, "DP", 0) if family == "DP0" else function_space(grid, "P", 1)
+    k = kr / device_grid(grid).radius
+    points, _ = sphere_shell_points(3000, 17)
+    _check(oracle, _operator(name, space, points, k), space)
+
+
+@pytest.mark.parametrize("name", ["single_layer", "double_layer"])
+def test_laplace_points_near_the_surface(oracle, name):
+    """Points on element centroids, 1e-3 above the surface and far away, with a ragged count (257)."""
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+
+    grid = regular_sphere(3)
+    space = function_space(grid, "P", 1)
+    v = grid.vertices
+    e = grid.elements
+    cent = v[:, e].mean(axis=1)  # (3, ne) element centroids
+    rng = np.random.default_rng(3)
+    pick = rng.choice(cent.shape[1], 100, replace=False)
+    near = cent[:, pick[:50]] * 1.001
+    far = rng.standard_normal((3, 157)) * 5.0
+    points = np.concatenate([cent[:, pick[50:]], near, far], axis=1)
+    assert points.shape[1] == 257
+    _check(oracle, _operator(name, space, points, None), space)
+    _check(oracle, _operator(name, space, points, 4.0), space)
+
+
+@pytest.mark.parametrize("order", [2, 6])
+def test_general_rule_size(oracle, order):
+    """Rules with other than six points take the runtime-size branch of the kernel."""
+    from bempp_cuda.operators import Parameters
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+    from cases import sphere_shell_points
+
+    grid = regular_sphere(2)
+    space = function_space(grid, "P", 1)
+    prm = Parameters()
+    prm.quadrature.regular = order
+    points, _ = sphere_shell_points(700, 9)
+    for name in ("single_layer", "double_layer"):
+        for k in (None, 3.0):
+            _check(oracle, _operator(name, space, points, k, parameters=prm), space)
+
+
+def test_single_chunk_and_single_point(oracle):
+    """The octahedron (8 elements) is one chunk: the kernel stores instead of adding atomically."""
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+
+    grid = regular_sphere(0)
+    space = function_space(grid, "DP", 0)
+    for points in (np.array([[2.0], [0.5], [-0.3]]), np.random.default_rng(1).standard_normal((3, 600)) * 3.0):
+        for k in (None, 1.5):
+            for name in ("single_layer", "double_layer"):
+                _check(oracle, _operator(name, space, points, k), space)
+
+
+def test_unknown_phase_radius_matches_factored_result():
+    """A caller that leaves phase_radius at 0 gets the unfactored phase; both agree to FP64 accuracy."""
+    from bempp_cuda import _lib
+    from bempp_cuda.assembly import kernel_ids, potential_workspace_bytes, regular_rule
+    from bempp_cuda.device import current_stream, device_grid, device_space, ptr
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+    from cases import sphere_shell_points
+
+    grid = regular_sphere(3)
+    space = function_space(grid, "P", 1)
+    points, _ = sphere_shell_points(1000, 2)
+    pts = torch.as_tensor(np.ascontiguousarray(points.T), device="cuda")
+    rng = np.random.default_rng(4)
+    local = space.map_to_full_grid @ (rng.standard_normal(space.global_dof_count) + 0j)
+    coeff = torch.as_tensor(np.ascontiguousarray(local, dtype=np.complex128), device="cuda")
+    op = _operator("single_layer", space, points, 5.0)
+    kernel, assembly = kernel_ids(op.descriptor)
+    qp, qw = regular_rule(4)
+    results = []
+    for radius in (0.0, 1.0001 * device_grid(grid).radius):
+        out = torch.full((1, points.shape[1]), complex(np.nan, np.nan), dtype=torch.complex128, device="cuda")
+        args = _lib.PotentialArgs()
+        args.kernel = kernel
+        args.assembly = assembly
+        args.precision = _lib.FP64
+        args.params[0] = 5.0
+        args.grid = device_grid(grid).record()
+        args.space = device_space(space).record()
+        args.nq = len(qw)
+        args.quad_points = qp.ctypes.data
+        args.quad_weights = qw.ctypes.data
+        args.npoints = points.shape[1]
+        args.points = ptr(pts)
+        args.coefficients = ptr(coeff)
+        args.result = ptr(out)
+        need = potential_workspace_bytes(args)
+        ws = torch.empty(need // 8, dtype=torch.float64, device="cuda")
+        args.workspace = ptr(ws)
+        args.workspace_bytes = need
+        args.phase_radius = radius
+        _lib.check(_lib.load().bemppcuda_evaluate_potential(ctypes.byref(args), current_stream()))
+        torch.cuda.synchronize()
+        results.append(out.cpu().numpy())
+    assert np.all(np.isfinite(results[0]))
+    assert rel_fro(results[1], results[0]) < 1e-13
