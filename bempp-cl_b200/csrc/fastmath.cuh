@@ -7,8 +7,10 @@
 // few significant bits so that n * part is exact for the n that occur here.
 //
 // FP64: pi/2 = C1 + C2 + C3 with C1, C2 of 33 significant bits (n * C1 and
-// n * C2 exact for |n| < 2^20); Taylor series of sin to a^15 and cos to a^16
-// (first omitted terms a^17/17! < 5e-17 and a^18/18! < 2e-18 on |a| <= pi/4).
+// n * C2 exact for |n| < 2^20); then sin a = a + a^3 P(a^2) and
+// cos a = 1 + a^2 Q(a^2) with P, Q Chebyshev approximations on |a| <= pi/4
+// (degrees 13 and 14 in a; coefficients and error bounds from fit_sincos.py,
+// which also fits the reduction-free variants for |x| <= 1 and |x| <= 1/2).
 // Arguments with |x| >= 1e6 go to the CUDA library sincos.
 //
 // FP32: pi/2 = 1.5703125 + 4.838268e-4 (the first part has 8 significant
@@ -20,6 +22,38 @@
 #pragma once
 
 namespace bc {
+
+// Horner evaluation of sin x = x + x^3 P(x^2) and cos x = 1 + x^2 Q(x^2) with
+// the coefficient lists of fit_sincos.py (highest degree first).
+template <int NS, int NC>
+__device__ __forceinline__ void sincos_poly64(double x, const double (&ps)[NS], const double (&pc)[NC], double *s,
+                                              double *c) {
+    const double x2 = x * x;
+    double p = ps[0];
+#pragma unroll
+    for (int i = 1; i < NS; ++i) p = fma(p, x2, ps[i]);
+    *s = fma(x * x2, p, x);
+    double q = pc[0];
+#pragma unroll
+    for (int i = 1; i < NC; ++i) q = fma(q, x2, pc[i]);
+    *c = fma(x2, q, 1.0);
+}
+
+// Chebyshev coefficients (fit_sincos.py); maximum absolute errors of the
+// polynomials: cw 1.4e-17 / 4.2e-19 on |a| <= pi/4, small 9.0e-18 / 1.1e-17 on
+// |x| <= 1, half 3.7e-17 / 5.5e-19 on |x| <= 1/2 (sin / cos).
+#define BC_SIN_CW64 {1.5918129294866608e-10, -2.5051131845003624e-08, 2.755731610255244e-06, \
+                     -0.00019841269836758574, 0.008333333333330948, -0.16666666666666666}
+#define BC_COS_CW64 {-1.1367998654022494e-11, 2.0875886738047052e-09, -2.7557315566341895e-07, \
+                     2.480158729369346e-05, -0.0013888888888880775, 0.04166666666666664, -0.5}
+#define BC_SIN_SMALL64 {-7.549371704181243e-13, 1.6057701922579786e-10, -2.5052099244914114e-08, \
+                        2.755731919201122e-06, -0.00019841269841216566, 0.0083333333333333, -0.16666666666666666}
+#define BC_COS_SMALL64 {-1.1304620460700782e-11, 2.0874477943664777e-09, -2.755730370192223e-07, \
+                        2.4801587247292686e-05, -0.0013888888888798428, 0.0416666666666661, -0.5}
+#define BC_SIN_HALF64 {-2.4951933287704484e-08, 2.755710022606947e-06, -0.0001984126964579005, \
+                       0.008333333333272254, -0.16666666666666635}
+#define BC_COS_HALF64 {2.0790894217124703e-09, -2.7557077887523167e-07, 2.4801586988836374e-05, \
+                       -0.0013888888888705666, 0.041666666666666276, -0.5}
 
 __device__ __forceinline__ void sincos_cw64(double x, double *s, double *c) {
     if (!(fabs(x) < 1.0e6)) {
@@ -33,24 +67,10 @@ __device__ __forceinline__ void sincos_cw64(double x, double *s, double *c) {
     double a = fma(-n, 1.5707963267341256, x);
     a = fma(-n, 6.077100506303966e-11, a);
     a = fma(-n, 2.0222662487959506e-21, a);
-    const double a2 = a * a;
-    double ps = -7.647163731819816e-13;
-    ps = fma(ps, a2, 1.6059043836821613e-10);
-    ps = fma(ps, a2, -2.505210838544172e-08);
-    ps = fma(ps, a2, 2.7557319223985893e-06);
-    ps = fma(ps, a2, -0.0001984126984126984);
-    ps = fma(ps, a2, 0.008333333333333333);
-    ps = fma(ps, a2, -0.16666666666666666);
-    const double sa = fma(a * a2, ps, a);
-    double pc = 4.779477332387385e-14;
-    pc = fma(pc, a2, -1.1470745597729725e-11);
-    pc = fma(pc, a2, 2.08767569878681e-09);
-    pc = fma(pc, a2, -2.755731922398589e-07);
-    pc = fma(pc, a2, 2.48015873015873e-05);
-    pc = fma(pc, a2, -0.001388888888888889);
-    pc = fma(pc, a2, 0.041666666666666664);
-    pc = fma(pc, a2, -0.5);
-    const double ca = fma(a2, pc, 1.0);
+    constexpr double ps[] = BC_SIN_CW64;
+    constexpr double pc[] = BC_COS_CW64;
+    double sa, ca;
+    sincos_poly64(a, ps, pc, &sa, &ca);
     // quadrant q: sin = (s, c, -s, -c), cos = (c, -s, -c, s)
     const double ss = (q & 1) ? ca : sa;
     const double cc = (q & 1) ? sa : ca;
@@ -74,50 +94,18 @@ __device__ __forceinline__ double rsqrt64(double x) {
     return fma(y * e, fma(0.375, e, 0.5), y);
 }
 
-// |x| <= 1 without reduction: Taylor series of sin to x^17 and cos to x^18
-// (first omitted terms 1/19! < 9e-18 and 1/20! < 5e-19).
+// |x| <= 1 without reduction (callers know the bound).
 __device__ __forceinline__ void sincos_small64(double x, double *s, double *c) {
-    const double x2 = x * x;
-    double ps = 2.8114572543455206e-15;
-    ps = fma(ps, x2, -7.647163731819816e-13);
-    ps = fma(ps, x2, 1.6059043836821613e-10);
-    ps = fma(ps, x2, -2.505210838544172e-08);
-    ps = fma(ps, x2, 2.7557319223985893e-06);
-    ps = fma(ps, x2, -0.0001984126984126984);
-    ps = fma(ps, x2, 0.008333333333333333);
-    ps = fma(ps, x2, -0.16666666666666666);
-    *s = fma(x * x2, ps, x);
-    double pc = -1.5619206968586225e-16;
-    pc = fma(pc, x2, 4.779477332387385e-14);
-    pc = fma(pc, x2, -1.1470745597729725e-11);
-    pc = fma(pc, x2, 2.08767569878681e-09);
-    pc = fma(pc, x2, -2.755731922398589e-07);
-    pc = fma(pc, x2, 2.48015873015873e-05);
-    pc = fma(pc, x2, -0.001388888888888889);
-    pc = fma(pc, x2, 0.041666666666666664);
-    pc = fma(pc, x2, -0.5);
-    *c = fma(x2, pc, 1.0);
+    constexpr double ps[] = BC_SIN_SMALL64;
+    constexpr double pc[] = BC_COS_SMALL64;
+    sincos_poly64(x, ps, pc, s, c);
 }
 
-// |x| <= 1/2 without reduction: Taylor series of sin to x^13 and cos to x^14
-// (first omitted terms (1/2)^15/15! < 3e-17 and (1/2)^16/16! < 8e-19).
+// |x| <= 1/2 without reduction (callers know the bound).
 __device__ __forceinline__ void sincos_half64(double x, double *s, double *c) {
-    const double x2 = x * x;
-    double ps = 1.6059043836821613e-10;
-    ps = fma(ps, x2, -2.505210838544172e-08);
-    ps = fma(ps, x2, 2.7557319223985893e-06);
-    ps = fma(ps, x2, -0.0001984126984126984);
-    ps = fma(ps, x2, 0.008333333333333333);
-    ps = fma(ps, x2, -0.16666666666666666);
-    *s = fma(x * x2, ps, x);
-    double pc = -1.1470745597729725e-11;
-    pc = fma(pc, x2, 2.08767569878681e-09);
-    pc = fma(pc, x2, -2.755731922398589e-07);
-    pc = fma(pc, x2, 2.48015873015873e-05);
-    pc = fma(pc, x2, -0.001388888888888889);
-    pc = fma(pc, x2, 0.041666666666666664);
-    pc = fma(pc, x2, -0.5);
-    *c = fma(x2, pc, 1.0);
+    constexpr double ps[] = BC_SIN_HALF64;
+    constexpr double pc[] = BC_COS_HALF64;
+    sincos_poly64(x, ps, pc, s, c);
 }
 
 // |x| <= 1/2 in FP32: degree 5 (sin) and 6 (cos), coefficients fitted by

@@ -51,7 +51,7 @@ constexpr int SH_THREADS = 128;
 constexpr int SH_TCHUNK = 32;
 constexpr int SH_TILES = 8;  // row chunks per block
 constexpr int SH_WARPS = SH_THREADS / 32;
-constexpr int SHS_WARPS = 8;  // singular kernel: pairs per block
+constexpr int SHS_WARPS = 4;  // singular kernel: pairs per block (154 registers: 3 blocks per SM)
 constexpr int SH_NQ = 6;
 constexpr int SH_RED = 13;  // row-element sums reduced across a block
 
@@ -92,20 +92,22 @@ __device__ __forceinline__ void cross3(const double a[3], const double b[3], dou
 
 // One ordered quadrature-point pair of the combined kernel.  (gr, gi) = w
 // exp(ik(r - r_c)) / (4 pi r) and (cre, cim) = conj(lambda_t) phi_s ie_t
-// exp(ik r_c), so Gc = c' w G; d = y - x runs from the test point to the trial point.
+// exp(ik r_c), so Gc = c' w G; d = y - x runs from the test point to the trial
+// point.  bcs = beta c_s (the trial normal vector times beta), so the returned
+// a2 lacks its factor beta: callers multiply a2 d sums by beta and use a2 bcs
+// for a2 c_s.
 __device__ __forceinline__ void qpe_ordered(const double d[3], double r, double rinv2, double gr, double gi,
-                                            double cre, double cim, const double cs[3], double ies, double bet,
+                                            double cre, double cim, const double bcs[3], double ies,
                                             const ShapeParams &P, QpeTerms &o) {
     const double Gr = cre * gr - cim * gi, Gi = fma(cre, gi, cim * gr);
-    const double u = fma(d[2], cs[2], fma(d[1], cs[1], d[0] * cs[0])) * rinv2;
+    const double bu = fma(d[2], bcs[2], fma(d[1], bcs[1], d[0] * bcs[0])) * rinv2;
     const double kr = P.k * r;
     const double Zr = fma(-Gi, kr, -Gr), Zi = fma(Gr, kr, -Gi);  // Gc z
     const double reGcEta = Gr * P.eta_re - Gi * P.eta_im;
     const double reGzEta = Zr * P.eta_re - Zi * P.eta_im;
     const double t1 = fma(Gr, 3.0 - kr * kr, 3.0 * kr * Gi);  // Re(Gc (3 - k^2 r^2 - 3ikr))
-    const double bu = bet * u;
     o.a1 = fma(bu, t1, ies * reGzEta);
-    o.a2 = bet * Zr * rinv2;
+    o.a2 = Zr * rinv2;
     o.ival = fma(bu, Zr, ies * reGcEta);
     o.ere = reGcEta;
     const double er = P.deta_re - P.eta_im * r, ei = fma(P.eta_re, r, P.deta_im);
@@ -166,13 +168,13 @@ __global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadR
 #pragma unroll
         for (int q = 0; q < SH_NQ; ++q) to_global(gs, rule.x[q], rule.y[q], y[q]);
 #pragma unroll
+        bet = P.beta * (P.nm ? (double)P.nm[s] : 1.0);
         for (int c = 0; c < 3; ++c) {
-            cs[c] = gs.n[c] * gs.ie;
+            cs[c] = bet * gs.n[c] * gs.ie;
             sc[c] = __ldg(P.g + (22 + c) * P.ne + s);
         }
         ies = gs.ie;
         ies_inv = 1.0 / gs.ie;
-        bet = P.beta * (P.nm ? (double)P.nm[s] : 1.0);
         phs = P.phi[s];
         const double2 l = P.lam[s];
         ls = make_double2(l.x * gs.ie, -l.y * gs.ie);  // conj(lambda_j) ie_j
@@ -201,9 +203,10 @@ __global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadR
             load_geom(P.g, P.ne, t, 1.0, g);
 #pragma unroll
             for (int p = 0; p < SH_NQ; ++p) to_global(g, rule.x[p], rule.y[p], sb.x[idx][p]);
+            const double bi = P.beta * (P.nm ? (double)P.nm[t] : 1.0);
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                sb.cr[idx][c] = g.n[c] * g.ie;
+                sb.cr[idx][c] = bi * g.n[c] * g.ie;
                 sb.ce[idx][c] = __ldg(P.g + (22 + c) * P.ne + t);
                 sb.v[idx][c] = P.el[3 * t + c];
             }
@@ -211,7 +214,7 @@ __global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadR
             sb.lc[idx] = make_double2(l.x * g.ie, -l.y * g.ie);
             sb.ph[idx] = P.phi[t];
             sb.ie[idx] = g.ie;
-            sb.bet[idx] = P.beta * (P.nm ? (double)P.nm[t] : 1.0);
+            sb.bet[idx] = bi;
         }
         __syncthreads();
         for (int tt = 0; tt < tcount; ++tt) {
@@ -225,7 +228,8 @@ __global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadR
                 const double D0 = sc[0] - sb.ce[tt][0], D1 = sc[1] - sb.ce[tt][1], D2 = sc[2] - sb.ce[tt][2];
                 const double rc = sqrt(fma(D2, D2, fma(D1, D1, D0 * D0)));
                 double pcs = 1.0, psn = 0.0;
-                if (PHC > 0) sincos_cw64(P.k * rc, &psn, &pcs);
+                const double krc = P.k * rc;
+                if (PHC > 0) sincos_cw64(krc, &psn, &pcs);
                 const double2 lt = sb.lc[tt], pt = sb.ph[tt];
                 // ordered (i, j): conj(lambda_i) ie_i phi_j;  (j, i): conj(lambda_j) ie_j phi_i
                 double c1r = lt.x * phs.x - lt.y * phs.y, c1i = fma(lt.x, phs.y, lt.y * phs.x);
@@ -238,7 +242,7 @@ __global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadR
                     c2r = e;
                     c2i = f;
                 }
-                const double iet = sb.ie[tt], iet_inv = 1.0 / iet, bett = sb.bet[tt];
+                const double iet = sb.ie[tt], iet_inv = 1.0 / iet;
                 const double ct[3] = {sb.cr[tt][0], sb.cr[tt][1], sb.cr[tt][2]};
                 for (int p = 0; p < SH_NQ; ++p) {
                     const double x0 = sb.x[tt][p][0], x1 = sb.x[tt][p][1], x2 = sb.x[tt][p][2];
@@ -253,17 +257,17 @@ __global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadR
                         const double rinv2 = rinv * rinv;
                         double sn, cn;
                         if (PHC > 0)
-                            phase64<PHC>(P.k * (r - rc), &sn, &cn);
+                            phase64<PHC>(fma(P.k, r, -krc), &sn, &cn);
                         else
                             sincos_cw64(P.k * r, &sn, &cn);
                         const double f = (wp * rule.w[q]) * rinv;
                         const double gr = cn * f, gi = sn * f;
                         QpeTerms o1, o2;
                         // (i, j): x in i (test), y in j (trial), d = y - x
-                        qpe_ordered(d, r, rinv2, gr, gi, c1r, c1i, cs, ies, bet, P, o1);
+                        qpe_ordered(d, r, rinv2, gr, gi, c1r, c1i, cs, ies, P, o1);
                         // (j, i): test point y, trial point x, d' = -d
                         const double dn[3] = {-d[0], -d[1], -d[2]};
-                        qpe_ordered(dn, r, rinv2, gr, gi, c2r, c2i, ct, iet, bett, P, o2);
+                        qpe_ordered(dn, r, rinv2, gr, gi, c2r, c2i, ct, iet, P, o2);
                         // column element j: trial of (i, j) (+gd1), test of (j, i) (-gd2)
                         // gd of (i, j) minus gd of (j, i): (a1_1 + a1_2) d / r^2 + a2_1 c_j - a2_2 c_i
                         const double a1s = (o1.a1 + o2.a1) * rinv2;
@@ -287,6 +291,8 @@ __global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadR
                     }
                 }
             }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) rs[9 + c] *= sb.bet[tt];  // a2 d sums lack beta_i
 #pragma unroll
             for (int f = 0; f < SH_RED; ++f) rs[f] = warp_sum(rs[f]);
             if (lane == 0)
@@ -316,7 +322,7 @@ __global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadR
             atomicAdd(a + c, cT);
             atomicAdd(a + 3 + c, cX);
             atomicAdd(a + 6 + c, cY);
-            atomicAdd(a + 9 + c, cC[c]);
+            atomicAdd(a + 9 + c, bet * cC[c]);  // a2 d sums lack beta_j
         }
         atomicAdd(a + 12, cI);
         atomicAdd(a + 13, cK);
@@ -334,8 +340,8 @@ __global__ void __launch_bounds__(32 * SHS_WARPS) shape_singular(ShapeParams P) 
     load_geom(P.g, P.ne, s, 1.0, gs);
     const double2 l = P.lam[t], ph = P.phi[s];
     const double cre = (l.x * ph.x + l.y * ph.y) * gt.ie, cim = (l.x * ph.y - l.y * ph.x) * gt.ie;
-    const double cs[3] = {gs.n[0] * gs.ie, gs.n[1] * gs.ie, gs.n[2] * gs.ie};
     const double bet = P.beta * (P.nm ? (double)P.nm[s] : 1.0);
+    const double cs[3] = {bet * gs.n[0] * gs.ie, bet * gs.n[1] * gs.ie, bet * gs.n[2] * gs.ie};
     const double ies = gs.ie;
     // 0-2 sum gd, 3-5 xi(x) gd, 6-8 eta(x) gd, 9-11 xi(y) gd, 12-14 eta(y) gd, 15-17 a2 d, 18 ival, 19 ere, 20 k
     double a[21];
@@ -358,7 +364,7 @@ __global__ void __launch_bounds__(32 * SHS_WARPS) shape_singular(ShapeParams P) 
         const double f = w * rinv * BC_INV_4PI;
         QpeTerms o;
         const double rinv2 = rinv * rinv;
-        qpe_ordered(d, r, rinv2, cn * f, sn * f, cre, cim, cs, ies, bet, P, o);
+        qpe_ordered(d, r, rinv2, cn * f, sn * f, cre, cim, cs, ies, P, o);
         const double a1 = o.a1 * rinv2;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
@@ -386,7 +392,7 @@ __global__ void __launch_bounds__(32 * SHS_WARPS) shape_singular(ShapeParams P) 
         atomicAdd(as + c, a[c]);
         atomicAdd(as + 3 + c, a[9 + c]);
         atomicAdd(as + 6 + c, a[12 + c]);
-        atomicAdd(as + 9 + c, a[15 + c]);
+        atomicAdd(as + 9 + c, bet * a[15 + c]);
     }
     atomicAdd(at + 12, a[18] / gt.ie);
     atomicAdd(as + 12, a[19]);
