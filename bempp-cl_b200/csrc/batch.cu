@@ -361,14 +361,7 @@ extern "C" int bemppcuda_batch_launch(const bemppcuda_batch_args *a, void *strea
     for (int i = 0; i < a->nproblems; ++i)
         total_tiles += tiles_of(a->problems[i].grid.nelements, rows_of(a), sym_of(a->problems[i], rows_of(a)));
     QuadRule rule;
-    rule.nq = a->nq;
-    rule.pad = 0;
-    for (int i = 0; i < BEMPPCUDA_MAX_REGULAR_POINTS; ++i) {
-        rule.x[i] = i < a->nq ? a->quad_points[2 * i] : 0.0;
-        rule.y[i] = i < a->nq ? a->quad_points[2 * i + 1] : 0.0;
-        rule.w[i] = i < a->nq ? a->quad_weights[i] : 0.0;
-        rule.wf[i] = (float)rule.w[i];
-    }
+    fill_rule(rule, a->nq, a->quad_points, a->quad_weights);
     const int bps = a->blocks_per_sm > 0 ? a->blocks_per_sm : 4;
     const int blocks = bps * sms;
     char *ws = static_cast<char *>(a->workspace);

@@ -19,15 +19,32 @@ __device__ __forceinline__ cplx cmul(cplx a, cplx b) { return {a.re * b.re - a.i
 __device__ __forceinline__ cplx cadd(cplx a, cplx b) { return {a.re + b.re, a.im + b.im}; }
 __device__ __forceinline__ cplx cscale(cplx a, double s) { return {a.re * s, a.im * s}; }
 
-// Regular quadrature rule passed by value (lives in the constant parameter bank).
+// Regular quadrature rule passed by value (lives in the constant parameter bank,
+// so kernels use its entries as constant operands without holding registers).
 struct QuadRule {
     int nq;
     int pad;
     double x[BEMPPCUDA_MAX_REGULAR_POINTS];
     double y[BEMPPCUDA_MAX_REGULAR_POINTS];
     double w[BEMPPCUDA_MAX_REGULAR_POINTS];
-    float wf[BEMPPCUDA_MAX_REGULAR_POINTS];  // w rounded to FP32 for the mixed path
+    double sw[BEMPPCUDA_MAX_REGULAR_POINTS][3];  // w times the linear shape values (1 - x - y, x, y)
+    float wf[BEMPPCUDA_MAX_REGULAR_POINTS];      // w rounded to FP32 for the mixed path
 };
+
+// The first nq points (x, y pairs) and weights of a host rule; unused entries are zero.
+inline void fill_rule(QuadRule &rule, int nq, const double *points, const double *weights) {
+    rule.nq = nq;
+    rule.pad = 0;
+    for (int i = 0; i < BEMPPCUDA_MAX_REGULAR_POINTS; ++i) {
+        rule.x[i] = i < nq ? points[2 * i] : 0.0;
+        rule.y[i] = i < nq ? points[2 * i + 1] : 0.0;
+        rule.w[i] = i < nq ? weights[i] : 0.0;
+        rule.sw[i][0] = rule.w[i] * (1.0 - rule.x[i] - rule.y[i]);
+        rule.sw[i][1] = rule.w[i] * rule.x[i];
+        rule.sw[i][2] = rule.w[i] * rule.y[i];
+        rule.wf[i] = (float)rule.w[i];
+    }
+}
 
 // Geometry of one element read from the field-major record.
 struct Geom {

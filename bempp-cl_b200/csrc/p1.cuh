@@ -12,10 +12,15 @@
 // (the P1 shape functions add up to 1), c = k^2 (Helmholtz), 0 (Laplace).
 // exp(ikr) is factored about the centroid distance as in the DP0 kernels.
 // The NT x NS block is added to the matrix with FP64 atomics (l2g, multipliers).
-// SYM (single layer and hypersingular, the same space on both sides): the
-// kernel is symmetric in x and y and so is the curl product, so the block of
-// the transposed pair is the transpose; only pairs i < j (support positions)
-// are evaluated and each block is added at (i, j) and (j, i).
+// SYM (the same space on both sides): only pairs i < j (support positions) are
+// evaluated and each gives the blocks at (i, j) and (j, i).  Single layer and
+// hypersingular: the kernel is symmetric in x and y and so is the curl
+// product, so the second block is the transpose of the first.  Double and
+// adjoint double layer: with d = y - x, the double layer of the transposed
+// pair (test j, trial i) is the adjoint double layer of (i, j) --
+//   (ikr - 1) e^{ikr} ((x - y) . n_i) / r^3 = -(ikr - 1) e^{ikr} (d . n_i) / r^3
+// -- so both blocks share r, the phase and (ikr - 1) e^{ikr} / r^2 and differ
+// in the normal of the dot product (the trial normal for the double layer).
 #pragma once
 
 #include "dp0.cuh"
@@ -49,8 +54,8 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
     constexpr bool DL = (K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_HELMHOLTZ_DLP);
     constexpr bool AD = (K == BEMPPCUDA_LAPLACE_ADLP || K == BEMPPCUDA_HELMHOLTZ_ADLP);
     constexpr bool PH = HELM && PHC > 0;
-    static_assert(!SYM || (NT == NS && (K == BEMPPCUDA_LAPLACE_SLP || K == BEMPPCUDA_HELMHOLTZ_SLP)),
-                  "the symmetric sweep needs a symmetric operator on one space");
+    static_assert(!SYM || NT == NS, "the symmetric sweep needs one space on both sides");
+    constexpr bool SKEW = SYM && (DL || AD);  // the transposed block uses the other element's normal
     __shared__ TestBlockP1 sb;
 
     const int64_t t0 = (int64_t)blockIdx.y * P1_TCHUNK;
@@ -99,18 +104,8 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
         for (int d = 0; d < 3; ++d) sc[d] = __ldg(prm.sg + (22 + d) * prm.sne + s);
     double curl_s[3][3];
     if (HYP) surface_curls(prm.sg, prm.sne, s, gs.n, curl_s);
-    // trial shape values times the trial weights
-    double psw[NQ6][NS];
-#pragma unroll
-    for (int q = 0; q < NQ6; ++q) {
-        if (NS == 1) {
-            psw[q][0] = rule.w[q];
-        } else {
-            psw[q][0] = rule.w[q] * (1.0 - rule.x[q] - rule.y[q]);
-            psw[q][1 % NS] = rule.w[q] * rule.x[q];
-            psw[q][2 % NS] = rule.w[q] * rule.y[q];
-        }
-    }
+    // trial / test shape values times the weights (constant operands from the rule)
+    const auto psw = [&](int q, int j) -> double { return NS == 1 ? rule.w[q] : rule.sw[q][j]; };
     const double kr = prm.p[0];
     // the trial dofs and multipliers stay in registers for the whole tile
     int64_t scol[NS];
@@ -122,7 +117,7 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
     }
     // (y_q - v0_s).n_s, the split of the double-layer normal term about the trial vertex 0
     double ynv[NQ6];
-    if (DL)
+    if (DL || SKEW)
 #pragma unroll
         for (int q = 0; q < NQ6; ++q)
             ynv[q] = fma(y[q][2] - gs.v0[2], gs.n[2], fma(y[q][1] - gs.v0[1], gs.n[1], (y[q][0] - gs.v0[0]) * gs.n[0]));
@@ -131,32 +126,70 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
         if (SYM && t0 + tt >= si) break;  // rows increase with tt
         if (prm.grids_identical && shares_vertex(sb.v[tt], sv0, sv1, sv2)) continue;
         const int64_t t = prm.tsup[t0 + tt];
-        double rc = 0.0, ph_s = 0.0, ph_c = 1.0;
+        double rc = 0.0, krc = 0.0, ph_s = 0.0, ph_c = 1.0;
         if (PH) {
             const double D0 = sc[0] - sb.c[tt][0], D1 = sc[1] - sb.c[tt][1], D2 = sc[2] - sb.c[tt][2];
             rc = sqrt(fma(D2, D2, fma(D1, D1, D0 * D0)));
-            sincos_cw64(kr * rc, &ph_s, &ph_c);
+            krc = kr * rc;
+            sincos_cw64(krc, &ph_s, &ph_c);
         }
         double lre[NT][NS], lim[NT][NS];
+        double ure[SKEW ? NT : 1][SKEW ? NS : 1], uim[SKEW ? NT : 1][SKEW ? NS : 1];  // SKEW: block of (j, i)
 #pragma unroll
         for (int i = 0; i < NT; ++i)
 #pragma unroll
             for (int j = 0; j < NS; ++j) lre[i][j] = lim[i][j] = 0.0;
+        if (SKEW)
+#pragma unroll
+            for (int i = 0; i < NT; ++i)
+#pragma unroll
+                for (int j = 0; j < NS; ++j) ure[i % (SKEW ? NT : 1)][j % (SKEW ? NS : 1)] = uim[i % (SKEW ? NT : 1)][j % (SKEW ? NS : 1)] = 0.0;
         double sre = 0.0, sim = 0.0;  // HYP: sum_pq w G
         for (int p = 0; p < NQ6; ++p) {
             const double x0 = sb.x[tt][p][0], x1 = sb.x[tt][p][1], x2 = sb.x[tt][p][2];
             double xn = 0.0;
-            if (DL) xn = fma(gs.v0[2] - x2, gs.n[2], fma(gs.v0[1] - x1, gs.n[1], (gs.v0[0] - x0) * gs.n[0]));
-            double tre[NS], tim[NS];
+            if (DL || SKEW) xn = fma(gs.v0[2] - x2, gs.n[2], fma(gs.v0[1] - x1, gs.n[1], (gs.v0[0] - x0) * gs.n[0]));
+            double tre[NS], tim[NS], vre[SKEW ? NS : 1], vim[SKEW ? NS : 1];
 #pragma unroll
             for (int j = 0; j < NS; ++j) tre[j] = tim[j] = 0.0;
+            if (SKEW)
+#pragma unroll
+                for (int j = 0; j < NS; ++j) vre[j % (SKEW ? NS : 1)] = vim[j % (SKEW ? NS : 1)] = 0.0;
 #pragma unroll
             for (int q = 0; q < NQ6; ++q) {
                 const double d0 = y[q][0] - x0, d1 = y[q][1] - x1, d2 = y[q][2] - x2;
                 const double r2 = fma(d2, d2, fma(d1, d1, d0 * d0));
                 const double rinv = rsqrt64(r2);
                 double kre, kim = 0.0;  // kernel value without 1/(4 pi)
-                if (!HELM) {
+                double k2re = 0.0, k2im = 0.0;  // SKEW: the transposed pair's kernel
+                if (SKEW) {
+                    // dS = d . n_trial (split about the trial vertex 0), dT = d . n_test
+                    const double dS = ynv[q] + xn;
+                    const double dT = fma(d2, sb.n[tt][2], fma(d1, sb.n[tt][1], d0 * sb.n[tt][0]));
+                    double hre, him;  // double layer of trial normal n: (dot with n) (hre + i him)
+                    if (!HELM) {
+                        hre = -rinv * rinv * rinv;
+                        him = 0.0;
+                    } else {
+                        const double r = r2 * rinv;
+                        double sn, cs;
+                        if (PH && PHC == 2)
+                            sincos_half64(fma(kr, r, -krc), &sn, &cs);
+                        else if (PH)
+                            sincos_small64(fma(kr, r, -krc), &sn, &cs);
+                        else
+                            sincos_cw64(kr * r, &sn, &cs);
+                        const double rinv2 = rinv * rinv;
+                        hre = -rinv2 * fma(rinv, cs, kr * sn);
+                        him = rinv2 * fma(kr, cs, -rinv * sn);
+                    }
+                    // the double layer of (test, trial) uses the trial normal; its transpose the test normal
+                    const double a1 = DL ? dS : -dT, a2 = DL ? -dT : dS;
+                    kre = a1 * hre;
+                    kim = a1 * him;
+                    k2re = a2 * hre;
+                    k2im = a2 * him;
+                } else if (!HELM) {
                     if (K == BEMPPCUDA_LAPLACE_SLP) {
                         kre = rinv;
                     } else {
@@ -168,9 +201,9 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
                     const double r = r2 * rinv;
                     double sn, cs;
                     if (PH && PHC == 2)
-                        sincos_half64(kr * (r - rc), &sn, &cs);
+                        sincos_half64(fma(kr, r, -krc), &sn, &cs);
                     else if (PH)
-                        sincos_small64(kr * (r - rc), &sn, &cs);
+                        sincos_small64(fma(kr, r, -krc), &sn, &cs);
                     else
                         sincos_cw64(kr * r, &sn, &cs);
                     if (K == BEMPPCUDA_HELMHOLTZ_SLP) {
@@ -187,25 +220,30 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
                 }
 #pragma unroll
                 for (int j = 0; j < NS; ++j) {
-                    tre[j] = fma(kre, psw[q][j], tre[j]);
-                    tim[j] = fma(kim, psw[q][j], tim[j]);
+                    tre[j] = fma(kre, psw(q, j), tre[j]);
+                    tim[j] = fma(kim, psw(q, j), tim[j]);
                 }
+                if (SKEW)
+#pragma unroll
+                    for (int j = 0; j < NS; ++j) {
+                        vre[j % (SKEW ? NS : 1)] = fma(k2re, psw(q, j), vre[j % (SKEW ? NS : 1)]);
+                        vim[j % (SKEW ? NS : 1)] = fma(k2im, psw(q, j), vim[j % (SKEW ? NS : 1)]);
+                    }
             }
             const double wp = rule.w[p];
-            double phw[NT];
-            if (NT == 1) {
-                phw[0] = wp;
-            } else {
-                phw[0] = wp * (1.0 - rule.x[p] - rule.y[p]);
-                phw[1 % NT] = wp * rule.x[p];
-                phw[2 % NT] = wp * rule.y[p];
-            }
+            const auto phw = [&](int i) -> double { return NT == 1 ? wp : rule.sw[p][i]; };
 #pragma unroll
             for (int i = 0; i < NT; ++i)
 #pragma unroll
                 for (int j = 0; j < NS; ++j) {
-                    lre[i][j] = fma(phw[i], tre[j], lre[i][j]);
-                    lim[i][j] = fma(phw[i], tim[j], lim[i][j]);
+                    lre[i][j] = fma(phw(i), tre[j], lre[i][j]);
+                    lim[i][j] = fma(phw(i), tim[j], lim[i][j]);
+                    if (SKEW) {
+                        ure[i % (SKEW ? NT : 1)][j % (SKEW ? NS : 1)] =
+                            fma(phw(i), vre[j % (SKEW ? NS : 1)], ure[i % (SKEW ? NT : 1)][j % (SKEW ? NS : 1)]);
+                        uim[i % (SKEW ? NT : 1)][j % (SKEW ? NS : 1)] =
+                            fma(phw(i), vim[j % (SKEW ? NS : 1)], uim[i % (SKEW ? NT : 1)][j % (SKEW ? NS : 1)]);
+                    }
                 }
             if (HYP)
 #pragma unroll
@@ -235,10 +273,21 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
                     vr = fma(cij, sre, cpf * vr);
                     vi = fma(cij, sim, cpf * vi);
                 }
+                // SKEW: the transposed pair's own block, else the same block
+                double wr = SKEW ? ure[i % (SKEW ? NT : 1)][j % (SKEW ? NS : 1)] : vr;
+                double wi = SKEW ? uim[i % (SKEW ? NT : 1)][j % (SKEW ? NS : 1)] : vi;
                 if (PH) {
                     const double tr = vr * ph_c - vi * ph_s;
                     vi = fma(vr, ph_s, vi * ph_c);
                     vr = tr;
+                    if (SKEW) {
+                        const double ur = wr * ph_c - wi * ph_s;
+                        wi = fma(wr, ph_s, wi * ph_c);
+                        wr = ur;
+                    } else {
+                        wr = vr;
+                        wi = vi;
+                    }
                 }
                 const double m = mt * ms * scale;
                 const int64_t col = scol[j];
@@ -248,12 +297,12 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
                     atomicAdd(o + 1, vi * m);
                     if (SYM) {
                         double *ot = reinterpret_cast<double *>(prm.result) + 2 * (col * prm.ld + row);
-                        atomicAdd(ot, vr * m);
-                        atomicAdd(ot + 1, vi * m);
+                        atomicAdd(ot, wr * m);
+                        atomicAdd(ot + 1, wi * m);
                     }
                 } else {
                     atomicAdd(reinterpret_cast<double *>(prm.result) + row * prm.ld + col, vr * m);
-                    if (SYM) atomicAdd(reinterpret_cast<double *>(prm.result) + col * prm.ld + row, vr * m);
+                    if (SYM) atomicAdd(reinterpret_cast<double *>(prm.result) + col * prm.ld + row, wr * m);
                 }
             }
         }

@@ -477,14 +477,7 @@ int bc_potential_launch(const bemppcuda_potential_args *a, double *workspace, cu
     prm.result = reinterpret_cast<double *>(a->result);
     for (int i = 0; i < 4; ++i) prm.p[i] = a->params[i];
     QuadRule rule;
-    rule.nq = a->nq;
-    rule.pad = 0;
-    for (int i = 0; i < BEMPPCUDA_MAX_REGULAR_POINTS; ++i) {
-        rule.x[i] = i < a->nq ? a->quad_points[2 * i] : 0.0;
-        rule.y[i] = i < a->nq ? a->quad_points[2 * i + 1] : 0.0;
-        rule.w[i] = i < a->nq ? a->quad_weights[i] : 0.0;
-        rule.wf[i] = (float)rule.w[i];
-    }
+    fill_rule(rule, a->nq, a->quad_points, a->quad_weights);
     if (prm.npoints == 0) return BEMPPCUDA_OK;
     const bool maxwell = a->assembly != BEMPPCUDA_ASM_SCALAR;
     if (prm.nsrc > 0) {

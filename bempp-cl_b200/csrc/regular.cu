@@ -331,7 +331,9 @@ static void launch_p1_phase(const RegParams &prm, const QuadRule &rule, int phas
 template <int ASM, int K, int NT, int NS>
 static void launch_p1_shapes(const RegParams &prm, const QuadRule &rule, int phase_class, bool sym, dim3 grid,
                              cudaStream_t st) {
-    constexpr bool SYMMETRIC_OP = NT == NS && (K == BEMPPCUDA_LAPLACE_SLP || K == BEMPPCUDA_HELMHOLTZ_SLP);
+    // single layer and hypersingular: symmetric; double / adjoint double layer: each pair
+    // also gives the transposed pair's block from the other normal (p1.cuh)
+    constexpr bool SYMMETRIC_OP = NT == NS;
     if constexpr (SYMMETRIC_OP) {
         if (sym) {
             launch_p1_phase<ASM, K, NT, NS, true>(prm, rule, phase_class, grid, st);
@@ -401,14 +403,7 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
     if (prm.ntest == 0 || prm.ntrial == 0) return BEMPPCUDA_OK;
 
     QuadRule rule;
-    rule.nq = a->nq;
-    rule.pad = 0;
-    for (int i = 0; i < BEMPPCUDA_MAX_REGULAR_POINTS; ++i) {
-        rule.x[i] = i < a->nq ? a->quad_points[2 * i] : 0.0;
-        rule.y[i] = i < a->nq ? a->quad_points[2 * i + 1] : 0.0;
-        rule.w[i] = i < a->nq ? a->quad_weights[i] : 0.0;
-        rule.wf[i] = (float)rule.w[i];
-    }
+    fill_rule(rule, a->nq, a->quad_points, a->quad_weights);
 
     const bool dp0 = a->assembly == BEMPPCUDA_ASM_SCALAR && a->test.nshape == 1 && a->trial.nshape == 1 &&
                      a->test.dof_is_position && a->trial.dof_is_position && a->nq == NQ6 &&

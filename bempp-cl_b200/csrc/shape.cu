@@ -668,14 +668,7 @@ static int shape_setup(const bemppcuda_shape_args *a, ShapeParams &P, QuadRule &
     P.scale_ff = a->scale_farfield;
     P.scale_rhs = a->scale_rhs;
     P.out = a->out;
-    rule.nq = a->nq;
-    rule.pad = 0;
-    for (int i = 0; i < BEMPPCUDA_MAX_REGULAR_POINTS; ++i) {
-        rule.x[i] = i < a->nq ? a->quad_points[2 * i] : 0.0;
-        rule.y[i] = i < a->nq ? a->quad_points[2 * i + 1] : 0.0;
-        rule.w[i] = i < a->nq ? a->quad_weights[i] : 0.0;
-        rule.wf[i] = (float)rule.w[i];
-    }
+    fill_rule(rule, a->nq, a->quad_points, a->quad_weights);
     return BEMPPCUDA_OK;
 }
 
