@@ -85,6 +85,18 @@ class DeviceGrid(object):
         return _lib.GridRec(self.nvertices, self.nelements, ptr(self.geom), ptr(self.elements))
 
 
+def _shared_on_grid(grid, name, array, dtype):
+    """One device copy per distinct content on a grid: spaces with equal maps
+    (RWG and SNC on the same grid) get the same device buffers, which is what
+    the symmetric sweeps test for."""
+    cache = _cache(grid)
+    host = _np.ascontiguousarray(array)
+    key = ("space_array", _torch.cuda.current_device(), name, str(host.dtype), host.shape, host.tobytes())
+    if key not in cache:
+        cache[key] = to_device(host, dtype)
+    return cache[key]
+
+
 class DeviceSpace(object):
     """Support list and dof maps of one space on the device."""
 
@@ -104,11 +116,12 @@ class DeviceSpace(object):
             and _np.all(mult[support, 0] == 1.0)
         )
         self.dof_is_position = 1 if pos else 0
-        self.support = to_device(support.astype(_np.int32), _torch.int32)
-        self.l2g = to_device(l2g.astype(_np.int32), _torch.int32)
-        self.mult = to_device(mult, _torch.float64)
+        grid = space.grid
+        self.support = _shared_on_grid(grid, "support", support.astype(_np.int32), _torch.int32)
+        self.l2g = _shared_on_grid(grid, "l2g", l2g.astype(_np.int32), _torch.int32)
+        self.mult = _shared_on_grid(grid, "mult", mult, _torch.float64)
         nm = _np.asarray(space.normal_multipliers, dtype=_np.int32)
-        self.normal_mult = to_device(nm, _torch.int32)
+        self.normal_mult = _shared_on_grid(grid, "normal_mult", nm, _torch.int32)
         self.h2d_bytes = support.size * 4 + l2g.size * 4 + mult.nbytes + nm.nbytes
 
     def record(self):

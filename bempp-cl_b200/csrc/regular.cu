@@ -16,7 +16,11 @@
 //    per point only the offset r - r_c = (2 D.e + e.e) / (r + r_c) enters
 //    the FP32 phase, so the phase error stays ~1e-7 rad independently of
 //    k r.  The 6-point inner sums are FP32, the per-entry sum is FP64.
-//  * regular_generic<ASM, K>: any scalar / hypersingular / Maxwell
+//  * regular_p1<ASM, K, ...> (p1.cuh): scalar and hypersingular operators on
+//    P1 / DP1 / P0 spaces, 6-point rule, real wavenumber.
+//  * regular_rwg<ASM, ...> (rwg.cuh): Maxwell electric / magnetic field on
+//    RWG / SNC spaces, 6-point rule, real nonzero wavenumber.
+//  * regular_generic<ASM, K>: every other scalar / hypersingular / Maxwell
 //    assembly with 1 or 3 shape functions and any rule (<= 16 points).  One
 //    thread per element pair; the local nshape x nshape block is scattered
 //    with atomicAdd into the (pre-zeroed or accumulating) result.
@@ -24,6 +28,7 @@
 
 #include "dp0_sym.cuh"
 #include "p1.cuh"
+#include "rwg.cuh"
 
 namespace bc {
 
@@ -361,6 +366,30 @@ static cudaError_t launch_p1(const RegParams &prm, const QuadRule &rule, int pha
     return cudaGetLastError();
 }
 
+// Maxwell electric / magnetic field on RWG / SNC spaces, 6-point rule, real
+// nonzero wavenumber (rwg.cuh).
+template <int ASM>
+static cudaError_t launch_rwg(const RegParams &prm, const QuadRule &rule, int phase_class, bool sym, cudaStream_t st) {
+    dim3 grid((unsigned)((prm.ntrial + DP0_THREADS - 1) / DP0_THREADS),
+              (unsigned)((prm.ntest + RWG_TCHUNK - 1) / RWG_TCHUNK));
+    if (sym) {
+        if (phase_class == 2)
+            regular_rwg<ASM, 2, true><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+        else if (phase_class == 1)
+            regular_rwg<ASM, 1, true><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+        else
+            regular_rwg<ASM, 0, true><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+    } else {
+        if (phase_class == 2)
+            regular_rwg<ASM, 2, false><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+        else if (phase_class == 1)
+            regular_rwg<ASM, 1, false><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+        else
+            regular_rwg<ASM, 0, false><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+    }
+    return cudaGetLastError();
+}
+
 template <int ASM, int K>
 static cudaError_t launch_generic(const RegParams &prm, const QuadRule &rule, cudaStream_t st) {
     dim3 grid((unsigned)((prm.ntrial + GEN_THREADS - 1) / GEN_THREADS), (unsigned)((prm.ntest + GEN_TCHUNK - 1) / GEN_TCHUNK));
@@ -453,6 +482,19 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
         case BEMPPCUDA_HELMHOLTZ_COMBINED: err = launch_dp0<BEMPPCUDA_HELMHOLTZ_COMBINED>(prm, rule, mixed, phase_class, sym, row0, row1, st); break;
         default: bc_set_error("kernel %d not valid for boundary assembly", a->kernel); return BEMPPCUDA_ERR_INVALID;
         }
+    } else if ((a->assembly == BEMPPCUDA_ASM_EFIE || a->assembly == BEMPPCUDA_ASM_MFIE) && a->nq == NQ6 &&
+               !a->overwrite && a->kernel == BEMPPCUDA_HELMHOLTZ_SLP && a->params[1] == 0.0 && a->params[0] != 0.0 &&
+               a->test.shapeset == BEMPPCUDA_SHAPE_RWG && a->trial.shapeset == BEMPPCUDA_SHAPE_RWG &&
+               a->test.nshape == 3 && a->trial.nshape == 3) {
+        // RWG and SNC share their dof maps; the caller passes the same arrays for both
+        const bool rsym = !a->no_symmetry && a->grids_identical && a->test.support == a->trial.support &&
+                          a->test.l2g == a->trial.l2g && a->test.mult == a->trial.mult &&
+                          a->test.nsupport == a->trial.nsupport && a->test_grid.geom == a->trial_grid.geom &&
+                          prm.ntest == prm.ntrial;
+        if (a->assembly == BEMPPCUDA_ASM_EFIE)
+            err = launch_rwg<BEMPPCUDA_ASM_EFIE>(prm, rule, phase_class, rsym, st);
+        else
+            err = launch_rwg<BEMPPCUDA_ASM_MFIE>(prm, rule, phase_class, rsym, st);
     } else if (const bool psym = !a->no_symmetry && a->grids_identical && a->test.support == a->trial.support &&
                                  a->test.l2g == a->trial.l2g && a->test.mult == a->trial.mult &&
                                  a->test.nsupport == a->trial.nsupport && a->test_grid.geom == a->trial_grid.geom &&

@@ -1,0 +1,301 @@
+// Regular pairs of the Maxwell electric and magnetic field operators on RWG /
+// SNC spaces, 6-point rule, real wavenumber: the kernels of
+// numba_kernels.py:1853-1969 (maxwell_efield_regular_assembler) and
+// :2151-2280 (maxwell_mfield_regular_assembler).
+//
+// Basis: b_i = J r_i / |J| with the reference RWG functions
+// r_i = (xi - a_i, eta - b_i), (a, b) = (0, 1), (1, 0), (0, 0)
+// (shapesets.py:95-102; SNC evaluates the same values), so the integration
+// elements of the quadrature cancel and, with G = exp(ikr) / (4 pi r),
+//   EFIE_ij = sum_pq w_p w_q G [-ik (J_t r_i(p)) . (J_s r_j(q)) - 4 / (ik)]
+//   MFIE_ij = sum_pq w_p w_q G (ikr - 1) / r^2 (x - y) . (J_t r_i(p) x J_s r_j(q)),
+// each times the two edge lengths and multipliers.  Write J_t r_i(p) =
+// w_t(p) - c_ti with w_t(p) = x_p - v0_t = J_t (xi_p, eta_p) and
+// c_ti = J_t (a_i, b_i) (c_t2 = 0); likewise on the trial side.  Then no
+// per-function work is left inside the point loops:
+//  EFIE: with the nine moments M[u][v] = sum_pq w_p w_q G u(p) v(q),
+//        u, v in {1, xi, eta} (accumulated as the P1 kernel accumulates its sums),
+//          sum_pq w w G (J_t r_i) . (J_s r_j) = P - c_sj . V_t - c_ti . V_s + (c_ti . c_sj) M[1][1],
+//        P = sum_ab (J_ta . J_sb) M[e_a][e_b], V_t = sum_a J_ta M[e_a][1],
+//        V_s = sum_b J_sb M[1][e_b]  (e_0 = xi, e_1 = eta).
+//  MFIE: with H = w_p w_q G (ikr - 1) / r^2, d = x - y and d . (u x v) = u . (v x d),
+//          B(p) = sum_q H (w_s(q) x d),  C(p) = sum_q H d,
+//          MFIE_ij = PB - c_sj . PC - c_ti . QB + c_ti . (c_sj x QC),
+//        PB = sum_p w_t(p) . B(p), PC = sum_p C(p) x w_t(p), QB = sum_p B(p), QC = sum_p C(p).
+// exp(ikr) is factored about the centroid distance as in the DP0 / P1 kernels.
+// SYM (test and trial spaces with the same dof maps on one grid, as RWG and
+// SNC are): both operators are symmetric under exchanging the pair's
+// elements (G is symmetric; for MFIE both d and the cross product change
+// sign), so pairs i < j are evaluated once and added at (i, j) and (j, i).
+#pragma once
+
+#include "dp0.cuh"
+
+namespace bc {
+
+constexpr int RWG_TCHUNK = 32;
+
+struct TestBlockRWG {
+    double x[RWG_TCHUNK][NQ6][3];
+    double j0[RWG_TCHUNK][3];
+    double j1[RWG_TCHUNK][3];
+    double c[RWG_TCHUNK][3];
+    double fac[RWG_TCHUNK][3];  // edge length times multiplier of each test function
+    int64_t row[RWG_TCHUNK][3];
+    int v[RWG_TCHUNK][3];
+};
+
+__device__ __forceinline__ double dot3(const double a[3], const double b[3]) {
+    return fma(a[2], b[2], fma(a[1], b[1], a[0] * b[0]));
+}
+
+template <int ASM, int PHC, bool SYM>
+__global__ void __launch_bounds__(DP0_THREADS) regular_rwg(RegParams prm, QuadRule rule) {
+    constexpr bool EFIE = ASM == BEMPPCUDA_ASM_EFIE;
+    constexpr bool PH = PHC > 0;
+    __shared__ TestBlockRWG sb;
+
+    const int64_t t0 = (int64_t)blockIdx.y * RWG_TCHUNK;
+    if (SYM && t0 >= ((int64_t)blockIdx.x + 1) * DP0_THREADS) return;  // below the diagonal
+    const int tcount = (int)min((int64_t)RWG_TCHUNK, prm.ntest - t0);
+    for (int idx = threadIdx.x; idx < tcount; idx += blockDim.x) {
+        const int64_t t = prm.tsup[t0 + idx];
+        Geom g;
+        load_geom(prm.tg, prm.tne, t, 1.0, g);
+        for (int p = 0; p < NQ6; ++p) to_global(g, rule.x[p], rule.y[p], sb.x[idx][p]);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            sb.j0[idx][d] = g.j0[d];
+            sb.j1[idx][d] = g.j1[d];
+            sb.c[idx][d] = __ldg(prm.tg + (22 + d) * prm.tne + t);
+            sb.v[idx][d] = __ldg(prm.tel + 3 * t + d);
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            sb.fac[idx][i] = prm.tmult[t * 3 + i] * edge_length(prm.tg, prm.tne, t, i);
+            sb.row[idx][i] = prm.tl2g[t * 3 + i];
+        }
+    }
+    __syncthreads();
+
+    const int64_t si = (int64_t)blockIdx.x * DP0_THREADS + threadIdx.x;
+    if (si >= prm.ntrial) return;
+    const int64_t s = prm.ssup[si];
+    Geom gs;
+    load_geom(prm.sg, prm.sne, s, 1.0, gs);
+    const int sv0 = __ldg(prm.sel + 3 * s), sv1 = __ldg(prm.sel + 3 * s + 1), sv2 = __ldg(prm.sel + 3 * s + 2);
+    // trial points as offsets from the trial vertex 0: w_s(q) = J_s (xi_q, eta_q)
+    double ws[NQ6][3];
+#pragma unroll
+    for (int q = 0; q < NQ6; ++q)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) ws[q][d] = fma(gs.j1[d], rule.y[q], gs.j0[d] * rule.x[q]);
+    double sc[3] = {0.0, 0.0, 0.0};
+    if (PH)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) sc[d] = __ldg(prm.sg + (22 + d) * prm.sne + s);
+    int64_t scol[3];
+    double sfac[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        scol[j] = prm.sl2g[s * 3 + j];
+        sfac[j] = prm.smult[s * 3 + j] * edge_length(prm.sg, prm.sne, s, j);
+    }
+    const double kr = prm.p[0];
+
+    for (int tt = 0; tt < tcount; ++tt) {
+        if (SYM && t0 + tt >= si) break;  // rows increase with tt
+        if (prm.grids_identical && shares_vertex(sb.v[tt], sv0, sv1, sv2)) continue;
+        double krc = 0.0, ph_s = 0.0, ph_c = 1.0;
+        if (PH) {
+            const double D0 = sc[0] - sb.c[tt][0], D1 = sc[1] - sb.c[tt][1], D2 = sc[2] - sb.c[tt][2];
+            krc = kr * sqrt(fma(D2, D2, fma(D1, D1, D0 * D0)));
+            sincos_cw64(krc, &ph_s, &ph_c);
+        }
+        const double tj0[3] = {sb.j0[tt][0], sb.j0[tt][1], sb.j0[tt][2]};
+        const double tj1[3] = {sb.j1[tt][0], sb.j1[tt][1], sb.j1[tt][2]};
+        // EFIE: moments M[u][v]; MFIE: PB, PC, QB, QC (complex)
+        double mre[3][3], mim[3][3];
+        double pbr = 0.0, pbi = 0.0, pcr[3], pci[3], qbr[3], qbi[3], qcr[3], qci[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+#pragma unroll
+            for (int b = 0; b < 3; ++b) mre[a][b] = mim[a][b] = 0.0;
+            pcr[a] = pci[a] = qbr[a] = qbi[a] = qcr[a] = qci[a] = 0.0;
+        }
+        for (int p = 0; p < NQ6; ++p) {
+            // x_p relative to the trial vertex 0: d = xs - w_s(q)
+            const double xs[3] = {sb.x[tt][p][0] - gs.v0[0], sb.x[tt][p][1] - gs.v0[1], sb.x[tt][p][2] - gs.v0[2]};
+            double tre[3] = {0.0, 0.0, 0.0}, tim[3] = {0.0, 0.0, 0.0};  // EFIE: sum_q w_q G v(q)
+            double br[3] = {0.0, 0.0, 0.0}, bi[3] = {0.0, 0.0, 0.0};    // MFIE: B(p) / w_p
+            double cr[3] = {0.0, 0.0, 0.0}, ci[3] = {0.0, 0.0, 0.0};    // MFIE: C(p) / w_p
+#pragma unroll
+            for (int q = 0; q < NQ6; ++q) {
+                const double d[3] = {xs[0] - ws[q][0], xs[1] - ws[q][1], xs[2] - ws[q][2]};
+                const double r2 = dot3(d, d);
+                const double rinv = rsqrt64(r2);
+                const double r = r2 * rinv;
+                double sn, cs;
+                if (PH && PHC == 2)
+                    sincos_half64(fma(kr, r, -krc), &sn, &cs);
+                else if (PH)
+                    sincos_small64(fma(kr, r, -krc), &sn, &cs);
+                else
+                    sincos_cw64(kr * r, &sn, &cs);
+                if (EFIE) {
+                    // w_q G 4 pi (the phase exp(ik r_c) and 1 / (4 pi) are applied per pair)
+                    const double gr = cs * rinv, gi = sn * rinv;
+                    const double v[3] = {rule.w[q], rule.sw[q][1], rule.sw[q][2]};  // w_q (1, xi_q, eta_q)
+#pragma unroll
+                    for (int b = 0; b < 3; ++b) {
+                        tre[b] = fma(gr, v[b], tre[b]);
+                        tim[b] = fma(gi, v[b], tim[b]);
+                    }
+                } else {
+                    // w_q G (ikr - 1) / r^2 times 4 pi: (cs + i sn)(-1 + i k r) w_q / r^3
+                    const double f = rule.w[q] * (rinv * rinv * rinv);
+                    const double kq = kr * r;
+                    const double hr = -fma(kq, sn, cs) * f, hi = fma(kq, cs, -sn) * f;
+                    double wxd[3];
+                    wxd[0] = fma(ws[q][1], d[2], -ws[q][2] * d[1]);
+                    wxd[1] = fma(ws[q][2], d[0], -ws[q][0] * d[2]);
+                    wxd[2] = fma(ws[q][0], d[1], -ws[q][1] * d[0]);
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        br[c] = fma(hr, wxd[c], br[c]);
+                        bi[c] = fma(hi, wxd[c], bi[c]);
+                        cr[c] = fma(hr, d[c], cr[c]);
+                        ci[c] = fma(hi, d[c], ci[c]);
+                    }
+                }
+            }
+            if (EFIE) {
+                const double u[3] = {rule.w[p], rule.sw[p][1], rule.sw[p][2]};  // w_p (1, xi_p, eta_p)
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int b = 0; b < 3; ++b) {
+                        mre[a][b] = fma(u[a], tre[b], mre[a][b]);
+                        mim[a][b] = fma(u[a], tim[b], mim[a][b]);
+                    }
+            } else {
+                // w_p w_t(p) = J_t (w_p xi_p, w_p eta_p)
+                double wt[3];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) wt[c] = fma(tj1[c], rule.sw[p][2], tj0[c] * rule.sw[p][1]);
+                const double wp = rule.w[p];
+                pbr += dot3(wt, br);
+                pbi += dot3(wt, bi);
+                // C x w_t (w_p inside wt)
+                pcr[0] += fma(cr[1], wt[2], -cr[2] * wt[1]);
+                pcr[1] += fma(cr[2], wt[0], -cr[0] * wt[2]);
+                pcr[2] += fma(cr[0], wt[1], -cr[1] * wt[0]);
+                pci[0] += fma(ci[1], wt[2], -ci[2] * wt[1]);
+                pci[1] += fma(ci[2], wt[0], -ci[0] * wt[2]);
+                pci[2] += fma(ci[0], wt[1], -ci[1] * wt[0]);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    qbr[c] = fma(wp, br[c], qbr[c]);
+                    qbi[c] = fma(wp, bi[c], qbi[c]);
+                    qcr[c] = fma(wp, cr[c], qcr[c]);
+                    qci[c] = fma(wp, ci[c], qci[c]);
+                }
+            }
+        }
+        // c_t = (J_t (0, 1), J_t (1, 0), 0) = (j1_t, j0_t, 0); likewise c_s
+        const double *ctv[2] = {tj1, tj0};
+        const double *csv[2] = {gs.j1, gs.j0};
+        double blk_re[3][3], blk_im[3][3];
+        if (EFIE) {
+            // P, V_t, V_s from the moments (index 0 = 1, 1 = xi, 2 = eta)
+            const double D00 = dot3(tj0, gs.j0), D01 = dot3(tj0, gs.j1), D10 = dot3(tj1, gs.j0), D11 = dot3(tj1, gs.j1);
+            const double pr = D00 * mre[1][1] + D01 * mre[1][2] + D10 * mre[2][1] + D11 * mre[2][2];
+            const double pi = D00 * mim[1][1] + D01 * mim[1][2] + D10 * mim[2][1] + D11 * mim[2][2];
+            double vtr[3], vti[3], vsr[3], vsi[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                vtr[c] = fma(tj0[c], mre[1][0], tj1[c] * mre[2][0]);
+                vti[c] = fma(tj0[c], mim[1][0], tj1[c] * mim[2][0]);
+                vsr[c] = fma(gs.j0[c], mre[0][1], gs.j1[c] * mre[0][2]);
+                vsi[c] = fma(gs.j0[c], mim[0][1], gs.j1[c] * mim[0][2]);
+            }
+            // -ik E1 - 4 / (ik) M11, 1 / (ik) = -i / k
+            const double m11r = mre[0][0], m11i = mim[0][0];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    double er = pr, ei = pi;
+                    if (j < 2) {
+                        er -= dot3(csv[j], vtr);
+                        ei -= dot3(csv[j], vti);
+                    }
+                    if (i < 2) {
+                        er -= dot3(ctv[i], vsr);
+                        ei -= dot3(ctv[i], vsi);
+                    }
+                    if (i < 2 && j < 2) {
+                        const double cc = dot3(ctv[i], csv[j]);
+                        er = fma(cc, m11r, er);
+                        ei = fma(cc, m11i, ei);
+                    }
+                    // -ik (er + i ei) = k ei - i k er;  -(4 / (ik)) M11 = (4i / k) M11 = -4 m11i / k + i 4 m11r / k
+                    blk_re[i][j] = fma(kr, ei, -4.0 * m11i / kr);
+                    blk_im[i][j] = fma(-kr, er, 4.0 * m11r / kr);
+                }
+        } else {
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    double vr = pbr, vi = pbi;
+                    if (j < 2) {
+                        vr -= dot3(csv[j], pcr);
+                        vi -= dot3(csv[j], pci);
+                    }
+                    if (i < 2) {
+                        vr -= dot3(ctv[i], qbr);
+                        vi -= dot3(ctv[i], qbi);
+                        if (j < 2) {
+                            // c_ti . (c_sj x QC) = QC . (c_ti x c_sj)
+                            double cx[3];
+                            cx[0] = ctv[i][1] * csv[j][2] - ctv[i][2] * csv[j][1];
+                            cx[1] = ctv[i][2] * csv[j][0] - ctv[i][0] * csv[j][2];
+                            cx[2] = ctv[i][0] * csv[j][1] - ctv[i][1] * csv[j][0];
+                            vr += dot3(cx, qcr);
+                            vi += dot3(cx, qci);
+                        }
+                    }
+                    blk_re[i][j] = vr;
+                    blk_im[i][j] = vi;
+                }
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const double ft = sb.fac[tt][i] * BC_INV_4PI;
+            if (ft == 0.0) continue;
+            const int64_t row = sb.row[tt][i];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const double m = ft * sfac[j];
+                if (m == 0.0) continue;
+                double vr = blk_re[i][j], vi = blk_im[i][j];
+                if (PH) {
+                    const double tr = vr * ph_c - vi * ph_s;
+                    vi = fma(vr, ph_s, vi * ph_c);
+                    vr = tr;
+                }
+                double *o = reinterpret_cast<double *>(prm.result) + 2 * (row * prm.ld + scol[j]);
+                atomicAdd(o, vr * m);
+                atomicAdd(o + 1, vi * m);
+                if (SYM) {
+                    double *ot = reinterpret_cast<double *>(prm.result) + 2 * (scol[j] * prm.ld + row);
+                    atomicAdd(ot, vr * m);
+                    atomicAdd(ot + 1, vi * m);
+                }
+            }
+        }
+    }
+}
+
+}  // namespace bc
