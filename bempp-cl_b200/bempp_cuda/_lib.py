@@ -102,6 +102,8 @@ class RegularArgs(_ct.Structure):
         ("phase_radius", _ct.c_double),
         ("row_begin", _i64),
         ("row_end", _i64),
+        ("result_is_zero", _i32),
+        ("pad2", _i32),
     ]
 
 

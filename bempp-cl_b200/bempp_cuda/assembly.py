@@ -91,7 +91,7 @@ def same_space(a, b):
 
 def regular_into(
     result, descriptor, domain, dual_to_range, parameters, precision=_lib.FP64, overwrite=False, stream=None,
-    geometry=None, symmetric=True, rows=None,
+    geometry=None, symmetric=True, rows=None, result_is_zero=False,
 ):
     """Add (or with ``overwrite`` store) the regular part into the device tensor ``result``.
 
@@ -102,6 +102,9 @@ def regular_into(
     same DP0 space of one grid; ``symmetric=False`` evaluates every entry on
     its own.  ``rows=(lo, hi)`` restricts a symmetric sweep to the pairs
     (i, j), i <= j, with rows i in [lo, hi) (both entries written).
+    ``result_is_zero`` promises that ``result`` holds zeros, which lets
+    symmetric P1 single-layer and hypersingular sweeps add only the blocks
+    of the pairs i < j and symmetrise the matrix afterwards.
     """
     require_cuda()
     kernel, assembly = kernel_ids(descriptor)
@@ -132,6 +135,7 @@ def regular_into(
     args.ld = result.stride(0)
     args.overwrite = 1 if overwrite else 0
     args.no_symmetry = 0 if symmetric else 1
+    args.result_is_zero = 1 if result_is_zero else 0
     if rows is not None:
         args.row_begin, args.row_end = int(rows[0]), int(rows[1])
     # a little slack over the exact bound keeps rounding of the radii on the safe side
@@ -207,7 +211,8 @@ def assemble_dense_device(domain, dual_to_range, parameters, descriptor, device_
         out.zero_()
     if precision == _lib.MIXED and not fast:
         precision = _lib.FP64
-    regular_into(out, descriptor, domain, dual_to_range, parameters, precision=precision, overwrite=fast)
+    regular_into(out, descriptor, domain, dual_to_range, parameters, precision=precision, overwrite=fast,
+                 result_is_zero=not fast)
     if _grids_identical(domain, dual_to_range):
         singular_into_dense(out, descriptor, domain, dual_to_range, parameters)
     return out

@@ -101,10 +101,12 @@ def dense_assembler(device_interface, operator_descriptor, domain, dual_to_range
     if precision == _lib.MIXED and operator_descriptor.assembly_type != "default_scalar":
         precision = _lib.FP64
     try:
-        regular_into(dev, operator_descriptor, domain, dual_to_range, parameters, precision=precision)
+        regular_into(dev, operator_descriptor, domain, dual_to_range, parameters, precision=precision,
+                     result_is_zero=True)
     except _lib.BemppCudaError as exc:
         if exc.status == _lib.ERR_UNSUPPORTED and precision == _lib.MIXED:
-            regular_into(dev, operator_descriptor, domain, dual_to_range, parameters, precision=_lib.FP64)
+            regular_into(dev, operator_descriptor, domain, dual_to_range, parameters, precision=_lib.FP64,
+                         result_is_zero=True)
         else:
             raise
     result += dev.cpu().numpy().astype(result.dtype, copy=False)

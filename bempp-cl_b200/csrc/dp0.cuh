@@ -24,7 +24,7 @@ struct RegParams {
     int grids_identical;
     int is_complex;
     int overwrite;
-    int pad;
+    int defer_transpose;  // symmetric P1 sweep into a zeroed result: skip the (j, i) blocks (added later as U^T)
     double p[4];
     void *result;
     int64_t ld;

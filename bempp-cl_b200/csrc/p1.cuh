@@ -15,7 +15,10 @@
 // SYM (the same space on both sides): only pairs i < j (support positions) are
 // evaluated and each gives the blocks at (i, j) and (j, i).  Single layer and
 // hypersingular: the kernel is symmetric in x and y and so is the curl
-// product, so the second block is the transpose of the first.  Double and
+// product, so the second block is the transpose of the first; into a zeroed
+// result (defer_transpose) only the first is added and the host forms
+// A = U + U^T afterwards (the regular diagonal is zero: a pair that reaches
+// entry (I, I) shares vertex I and is singular).  Double and
 // adjoint double layer: with d = y - x, the double layer of the transposed
 // pair (test j, trial i) is the adjoint double layer of (i, j) --
 //   (ikr - 1) e^{ikr} ((x - y) . n_i) / r^3 = -(ikr - 1) e^{ikr} (d . n_i) / r^3
@@ -295,14 +298,15 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
                     double *o = reinterpret_cast<double *>(prm.result) + 2 * (row * prm.ld + col);
                     atomicAdd(o, vr * m);
                     atomicAdd(o + 1, vi * m);
-                    if (SYM) {
+                    if (SYM && (SKEW || !prm.defer_transpose)) {
                         double *ot = reinterpret_cast<double *>(prm.result) + 2 * (col * prm.ld + row);
                         atomicAdd(ot, wr * m);
                         atomicAdd(ot + 1, wi * m);
                     }
                 } else {
                     atomicAdd(reinterpret_cast<double *>(prm.result) + row * prm.ld + col, vr * m);
-                    if (SYM) atomicAdd(reinterpret_cast<double *>(prm.result) + col * prm.ld + row, wr * m);
+                    if (SYM && (SKEW || !prm.defer_transpose))
+                        atomicAdd(reinterpret_cast<double *>(prm.result) + col * prm.ld + row, wr * m);
                 }
             }
         }

@@ -366,6 +366,40 @@ static cudaError_t launch_p1(const RegParams &prm, const QuadRule &rule, int pha
     return cudaGetLastError();
 }
 
+// A <- A + A^T for an n x n matrix with row stride ld, in 32 x 32 tiles: the
+// block of tile pair (bi, bj), bi <= bj, reads both tiles and writes both sums.
+__device__ __forceinline__ double add_pair(double a, double b) { return a + b; }
+__device__ __forceinline__ double2 add_pair(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+
+template <typename T>
+__global__ void __launch_bounds__(256) add_transpose(T *a, int64_t n, int64_t ld) {
+    const int64_t bi = blockIdx.y, bj = blockIdx.x;
+    if (bi > bj) return;
+    __shared__ T s1[32][33], s2[32][33];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int64_t r0 = bi * 32, c0 = bj * 32;
+    for (int k = ty; k < 32; k += 8) {
+        if (r0 + k < n && c0 + tx < n) s1[k][tx] = a[(r0 + k) * ld + c0 + tx];  // tile (bi, bj)
+        if (c0 + k < n && r0 + tx < n) s2[k][tx] = a[(c0 + k) * ld + r0 + tx];  // tile (bj, bi)
+    }
+    __syncthreads();
+    for (int k = ty; k < 32; k += 8) {
+        if (r0 + k < n && c0 + tx < n) a[(r0 + k) * ld + c0 + tx] = add_pair(s1[k][tx], s2[tx][k]);
+        if (bi != bj && c0 + k < n && r0 + tx < n) a[(c0 + k) * ld + r0 + tx] = add_pair(s2[k][tx], s1[tx][k]);
+    }
+}
+
+static cudaError_t launch_add_transpose(void *a, int64_t n, int64_t ld, bool is_complex, cudaStream_t st) {
+    const int64_t tiles = (n + 31) / 32;
+    if (tiles == 0) return cudaSuccess;
+    const dim3 grid((unsigned)tiles, (unsigned)tiles), block(32, 8);
+    if (is_complex)
+        add_transpose<double2><<<grid, block, 0, st>>>(reinterpret_cast<double2 *>(a), n, ld);
+    else
+        add_transpose<double><<<grid, block, 0, st>>>(reinterpret_cast<double *>(a), n, ld);
+    return cudaGetLastError();
+}
+
 // Maxwell electric / magnetic field on RWG / SNC spaces, 6-point rule, real
 // nonzero wavenumber (rwg.cuh).
 template <int ASM>
@@ -425,7 +459,7 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
     prm.grids_identical = a->grids_identical;
     prm.is_complex = a->is_complex;
     prm.overwrite = a->overwrite;
-    prm.pad = 0;
+    prm.defer_transpose = 0;
     for (int i = 0; i < 4; ++i) prm.p[i] = a->params[i];
     prm.result = a->result;
     prm.ld = a->ld;
@@ -503,6 +537,13 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
                a->trial.shapeset != BEMPPCUDA_SHAPE_RWG && a->params[1] == 0.0 &&
                ((a->assembly == BEMPPCUDA_ASM_SCALAR && a->kernel <= BEMPPCUDA_HELMHOLTZ_ADLP) ||
                 a->assembly == BEMPPCUDA_ASM_LAPLACE_HYP || a->assembly == BEMPPCUDA_ASM_HELM_HYP)) {
+        // single layer / hypersingular on one space into a zeroed result: the pairs i < j add their
+        // blocks U, then A = U + U^T (the regular diagonal is zero), half the global atomics
+        const bool defer = psym && a->result_is_zero && a->test.nshape == a->trial.nshape &&
+                           a->test.ndofs == a->trial.ndofs && a->test.ndofs <= 32 * 65535LL &&
+                           (a->assembly != BEMPPCUDA_ASM_SCALAR || a->kernel == BEMPPCUDA_LAPLACE_SLP ||
+                            a->kernel == BEMPPCUDA_HELMHOLTZ_SLP);
+        prm.defer_transpose = defer ? 1 : 0;
         if (a->assembly == BEMPPCUDA_ASM_LAPLACE_HYP) {
             err = launch_p1<BEMPPCUDA_ASM_LAPLACE_HYP, BEMPPCUDA_LAPLACE_SLP>(prm, rule, phase_class, psym, st);
         } else if (a->assembly == BEMPPCUDA_ASM_HELM_HYP) {
@@ -517,6 +558,7 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
             default: err = launch_p1<0, BEMPPCUDA_HELMHOLTZ_ADLP>(prm, rule, phase_class, psym, st); break;
             }
         }
+        if (defer && err == cudaSuccess) err = launch_add_transpose(prm.result, a->test.ndofs, prm.ld, prm.is_complex, st);
     } else {
         switch (a->assembly) {
         case BEMPPCUDA_ASM_SCALAR:

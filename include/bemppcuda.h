@@ -128,6 +128,11 @@ typedef struct {
     int64_t row_begin;          /* symmetric sweep only: evaluate the pairs (i, j), i <= j, with rows i in */
     int64_t row_end;            /* [row_begin, row_end) (writing A_ij and A_ji); 0, 0 = all rows.  Rows of
                                    block [b, e) are complete once the blocks before it and this call ran */
+    int32_t result_is_zero;     /* 1: the caller guarantees that result holds zeros.  Symmetric P1 / P0
+                                   single-layer and hypersingular sweeps then store only the blocks of
+                                   the pairs i < j and form A = U + U^T in one pass over the matrix,
+                                   half the global atomics; 0: accumulate both blocks into result */
+    int32_t pad2;
 } bemppcuda_regular_args;
 
 /* Singular pairs (Sauter-Schwab), the arrays of

@@ -106,13 +106,23 @@ def test_p1_symmetric_sweep_matches_entrywise(path, k):
     n = sp.global_dof_count
     dtype = torch.complex128 if d.is_complex else torch.float64
     out = []
-    for sym in (True, False):
+    # symmetric (both blocks by atomics), per pair, and symmetric into a zeroed
+    # result (blocks of i < j, then A = U + U^T for single layer / hypersingular)
+    for sym, zero in ((True, False), (False, False), (True, True)):
         a = torch.zeros((n, n), dtype=dtype, device="cuda")
-        regular_into(a, d, sp, sp, Parameters(), symmetric=sym)
+        regular_into(a, d, sp, sp, Parameters(), symmetric=sym, result_is_zero=zero)
         singular_into_dense(a, d, sp, sp, Parameters())
         out.append(a)
     torch.cuda.synchronize()
     assert (torch.linalg.norm(out[0] - out[1]) / torch.linalg.norm(out[1])).item() < 1e-13
+    assert (torch.linalg.norm(out[2] - out[1]) / torch.linalg.norm(out[1])).item() < 1e-13
+    # accumulating into a matrix that already holds values (no zero promise): prior + A
+    prior = torch.randn((n, n), dtype=dtype, device="cuda")
+    acc = prior.clone()
+    regular_into(acc, d, sp, sp, Parameters())
+    singular_into_dense(acc, d, sp, sp, Parameters())
+    scale = (torch.linalg.norm(prior) + torch.linalg.norm(out[1])).item()
+    assert torch.linalg.norm(acc - prior - out[1]).item() < 1e-13 * scale
 
 
 @pytest.mark.parametrize("name", ["electric_field", "magnetic_field"])
