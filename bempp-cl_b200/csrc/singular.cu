@@ -44,7 +44,7 @@ __device__ __forceinline__ bool pair_in_range(const SingParams &prm, int64_t k) 
            toff + n <= prm.ntab && soff + n <= prm.ntab && woff + n <= prm.nw;
 }
 
-constexpr int SING_WARPS = 8;
+constexpr int SING_WARPS = 4;  // pairs per block: 128 threads let 3-5 blocks share an SM at 80-170 registers
 
 template <int ASM, int K>
 __global__ void __launch_bounds__(32 * SING_WARPS) singular_pairs(SingParams prm) {
