@@ -119,9 +119,10 @@ typedef struct {
     void *result;               /* (rows, ld) row-major float64 or complex128 */
     int64_t ld;                 /* row stride in entries */
     int32_t overwrite;          /* DP0 fast path only: store instead of add, zero for adjacent pairs */
-    int32_t no_symmetry;        /* 0: when test and trial are the same DP0 space of one grid (same support,
-                                   geometry and normal-multiplier pointers) and k is real, one sweep over the
-                                   pairs i < j gives A_ij and A_ji; 1: always evaluate every entry separately */
+    int32_t no_symmetry;        /* 0: when test and trial are the same space of one grid (same support, dof
+                                   map, multiplier, normal-multiplier and geometry pointers; DP0, P1 / DP1 /
+                                   P0, RWG with SNC) and k is real, one sweep over the pairs i < j gives
+                                   A_ij and A_ji; 1: always evaluate every entry separately */
     double phase_radius;        /* R_test + R_trial, R = largest centroid-to-vertex distance of a grid;
                                    lets the mixed path skip the phase range reduction when
                                    |k| * phase_radius <= 1; 0 = unknown (always reduce) */
