@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "../../include/bemppcuda.h"
 #include "fastmath.cuh"
 
@@ -30,6 +32,19 @@ struct QuadRule {
     double sw[BEMPPCUDA_MAX_REGULAR_POINTS][3];  // w times the linear shape values (1 - x - y, x, y)
     float wf[BEMPPCUDA_MAX_REGULAR_POINTS];      // w rounded to FP32 for the mixed path
 };
+
+// Number of SMs of the current device (148 on a B200 if the query fails), looked up once per device.
+inline int bc_sm_count() {
+    static std::atomic<int> cached[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    int sms = cached[dev].load(std::memory_order_relaxed);
+    if (sms <= 0) {
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+        cached[dev].store(sms, std::memory_order_relaxed);
+    }
+    return sms;
+}
 
 // The first nq points (x, y pairs) and weights of a host rule; unused entries are zero.
 inline void fill_rule(QuadRule &rule, int nq, const double *points, const double *weights) {

@@ -409,24 +409,12 @@ static cudaError_t launch_scalar_nq(const PotParams &prm, dim3 grid, int64_t chu
     return cudaGetLastError();
 }
 
-// Number of SMs of the current device, looked up once per device.
-static int sm_count() {
-    static int cached[64] = {0};
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
-    if (!cached[dev]) {
-        int sms = 0;
-        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
-        cached[dev] = sms;
-    }
-    return cached[dev];
-}
 
 // Scalar Laplace / Helmholtz potential with a real wavenumber; phase_radius
 // bounds every source's distance from its element centroid (0: unknown).
 static cudaError_t launch_scalar(const PotParams &prm, int kernel, double phase_radius, cudaStream_t st) {
     const int64_t pblocks = (prm.npoints + PS_THREADS * PS_PPT - 1) / (PS_THREADS * PS_PPT);
-    const int64_t target = (int64_t)sm_count() * 8;  // CTAs: several waves of 4 resident per SM
+    const int64_t target = (int64_t)bc_sm_count() * 8;  // CTAs: several waves of 4 resident per SM
     int64_t chunks = (target + pblocks - 1) / pblocks;
     chunks = std::min(chunks, (prm.nsupport + PS_CHUNK_MIN - 1) / PS_CHUNK_MIN);
     chunks = std::max<int64_t>(1, std::min<int64_t>(chunks, 65535));

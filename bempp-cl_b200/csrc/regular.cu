@@ -237,11 +237,11 @@ __global__ void __launch_bounds__(GEN_THREADS) regular_generic(RegParams prm, Qu
 // before touching shared memory.
 template <int K, int PHC>
 __global__ void __launch_bounds__(DP0_THREADS) regular_dp0_fp64_sym(RegParams prm, QuadRule rule, int64_t row0,
-                                                                    int64_t row1) {
-    const int64_t t0 = row0 + (int64_t)blockIdx.y * DP0_TCHUNK;
+                                                                    int64_t row1, int tile_rows) {
+    const int64_t t0 = row0 + (int64_t)blockIdx.y * tile_rows;
     if (t0 >= ((int64_t)blockIdx.x + 1) * DP0_THREADS) return;
     __shared__ TestBlock64s sb;
-    regular_dp0_fp64_sym_tile<K, PHC>(prm, rule, blockIdx.x, t0, (int)min((int64_t)DP0_TCHUNK, row1 - t0), sb);
+    regular_dp0_fp64_sym_tile<K, PHC>(prm, rule, blockIdx.x, t0, (int)min((int64_t)tile_rows, row1 - t0), sb);
 }
 
 // CTAs per SM the mixed symmetric sweep is compiled for (register cap 170 at
@@ -252,11 +252,12 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_dp0_fp64_sym(RegParams pr
 
 template <int K, int PHC>
 __global__ void __launch_bounds__(DP0_THREADS, BC_MSYM_MIN_BLOCKS) regular_dp0_mixed_sym(RegParams prm, QuadRule rule,
-                                                                                      int64_t row0, int64_t row1) {
-    const int64_t t0 = row0 + (int64_t)blockIdx.y * DP0_TCHUNK;
+                                                                                      int64_t row0, int64_t row1,
+                                                                                      int tile_rows) {
+    const int64_t t0 = row0 + (int64_t)blockIdx.y * tile_rows;
     if (t0 >= ((int64_t)blockIdx.x + 1) * DP0_THREADS) return;
     __shared__ TestBlock32p sb;
-    regular_dp0_mixed_sym_tile<K, PHC>(prm, rule, blockIdx.x, t0, (int)min((int64_t)DP0_TCHUNK, row1 - t0), sb);
+    regular_dp0_mixed_sym_tile<K, PHC>(prm, rule, blockIdx.x, t0, (int)min((int64_t)tile_rows, row1 - t0), sb);
 }
 
 template <int K>
@@ -267,21 +268,27 @@ static cudaError_t launch_dp0(const RegParams &prm, const QuadRule &rule, int mi
         // same DP0 space on both sides, real wavenumber (k > 0 for the scaled mixed path)
         const bool real_k = !KernelTraits<K>::helm || (prm.p[1] == 0.0 && (!mixed || prm.p[0] > 0.0));
         if (sym && real_k) {
-            const dim3 sgrid(grid.x, (unsigned)((row1 - row0 + DP0_TCHUNK - 1) / DP0_TCHUNK));
+            // rows per tile: 32, or 16 / 8 when 32-row tiles would leave the GPU under four waves of
+            // working CTAs (about half the tiles lie below the diagonal and exit; 3 CTAs per SM)
+            int tile_rows = DP0_TCHUNK;
+            const int64_t wave = (int64_t)bc_sm_count() * 3;
+            while (tile_rows > 8 && (int64_t)grid.x * ((row1 - row0 + tile_rows - 1) / tile_rows) / 2 < 4 * wave)
+                tile_rows /= 2;
+            const dim3 sgrid(grid.x, (unsigned)((row1 - row0 + tile_rows - 1) / tile_rows));
             if (mixed) {
                 if (phase_class == 2)
-                    regular_dp0_mixed_sym<K, 2><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1);
+                    regular_dp0_mixed_sym<K, 2><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
                 else if (phase_class == 1)
-                    regular_dp0_mixed_sym<K, 1><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1);
+                    regular_dp0_mixed_sym<K, 1><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
                 else
-                    regular_dp0_mixed_sym<K, 0><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1);
+                    regular_dp0_mixed_sym<K, 0><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
             } else {
                 if (phase_class == 2)
-                    regular_dp0_fp64_sym<K, 2><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1);
+                    regular_dp0_fp64_sym<K, 2><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
                 else if (phase_class == 1)
-                    regular_dp0_fp64_sym<K, 1><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1);
+                    regular_dp0_fp64_sym<K, 1><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
                 else
-                    regular_dp0_fp64_sym<K, 0><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1);
+                    regular_dp0_fp64_sym<K, 0><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
             }
             return cudaGetLastError();
         }
