@@ -33,7 +33,6 @@ struct SymTraits {
 
 struct TestBlock64s {
     double x[DP0_TCHUNK][NQ6][3];
-    double xn[DP0_TCHUNK][NQ6];  // (x_p - c_i).n_i: zero up to rounding, kept as the plain path keeps it
     double c[DP0_TCHUNK][3];
     double n[DP0_TCHUNK][3];
     double ie[DP0_TCHUNK];
@@ -59,7 +58,6 @@ __device__ __forceinline__ void regular_dp0_fp64_sym_tile(const RegParams &prm, 
             to_global(g, rule.x[p], rule.y[p], x);
 #pragma unroll
             for (int d = 0; d < 3; ++d) sb.x[idx][p][d] = x[d];
-            sb.xn[idx][p] = fma(x[2] - c[2], g.n[2], fma(x[1] - c[1], g.n[1], (x[0] - c[0]) * g.n[0]));
         }
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
@@ -85,12 +83,6 @@ __device__ __forceinline__ void regular_dp0_fp64_sym_tile(const RegParams &prm, 
 #pragma unroll
     for (int q = 0; q < NQ6; ++q) to_global(gs, rule.x[q], rule.y[q], y[q]);
     const double kr = prm.p[0], etar = prm.p[2], etai = prm.p[3];
-    // (y_q - v0_j).n_j, the plain path's split of the normal term of A_ij
-    double ynv[NQ6];
-    if (ST::dlp_part)
-#pragma unroll
-        for (int q = 0; q < NQ6; ++q)
-            ynv[q] = fma(y[q][2] - gs.v0[2], gs.n[2], fma(y[q][1] - gs.v0[1], gs.n[1], (y[q][0] - gs.v0[0]) * gs.n[0]));
 
     for (int tt = 0; tt < tcount; ++tt) {
         const int64_t row = t0 + tt;
@@ -104,7 +96,9 @@ __device__ __forceinline__ void regular_dp0_fp64_sym_tile(const RegParams &prm, 
                 rc = sqrt(fma(D2, D2, fma(D1, D1, D0 * D0)));
                 sincos_cw64(kr * rc, &ph_s, &ph_c);
             }
-            // (c_i - y_q).n_i: the transposed entry's normal term split about the test centroid
+            // Normal terms: (y - x).n_j = (v0_j - x).n_j since y lies in the plane of j (one value per
+            // test point, applied after the sum over q), and (x - y).n_i = (c_i - y).n_i since x lies in
+            // the plane of i (one value per trial point)
             double ynt[NQ6];
             if (ST::dlp_part)
 #pragma unroll
@@ -114,11 +108,9 @@ __device__ __forceinline__ void regular_dp0_fp64_sym_tile(const RegParams &prm, 
             double s0r = 0.0, s0i = 0.0, u_re = 0.0, u_im = 0.0, v_re = 0.0, v_im = 0.0;
             for (int p = 0; p < NQ6; ++p) {
                 const double x0 = sb.x[tt][p][0], x1 = sb.x[tt][p][1], x2 = sb.x[tt][p][2];
-                double xn = 0.0, xnt = 0.0;
-                if (ST::dlp_part) {
+                double xn = 0.0;
+                if (ST::dlp_part)
                     xn = fma(gs.v0[2] - x2, gs.n[2], fma(gs.v0[1] - x1, gs.n[1], (gs.v0[0] - x0) * gs.n[0]));
-                    xnt = sb.xn[tt][p];
-                }
                 double pr = 0.0, pi = 0.0, ur = 0.0, ui = 0.0, vr = 0.0, vi = 0.0;
 #pragma unroll
                 for (int q = 0; q < NQ6; ++q) {
@@ -130,8 +122,8 @@ __device__ __forceinline__ void regular_dp0_fp64_sym_tile(const RegParams &prm, 
                         if (ST::slp_part) pr += f;
                         if (ST::dlp_part) {
                             const double g3 = f * rinv * rinv;
-                            ur = fma(g3, ynv[q] + xn, ur);
-                            vr = fma(g3, ynt[q] + xnt, vr);
+                            ur += g3;
+                            vr = fma(g3, ynt[q], vr);
                         }
                     } else {
                         const double r = r2 * rinv;
@@ -150,19 +142,19 @@ __device__ __forceinline__ void regular_dp0_fp64_sym_tile(const RegParams &prm, 
                             // (ikr - 1) e^{ikr} / r^3: -h1 + i h2 per unit f (dot) / r
                             const double fr = f * rinv;
                             const double h1 = fma(rinv, cs, kr * sn), h2 = fma(kr, cs, -rinv * sn);
-                            const double g = fr * (ynv[q] + xn), gt = fr * (ynt[q] + xnt);
-                            ur = fma(g, h1, ur);
-                            ui = fma(g, h2, ui);
+                            const double gt = fr * ynt[q];
+                            ur = fma(fr, h1, ur);
+                            ui = fma(fr, h2, ui);
                             vr = fma(gt, h1, vr);
                             vi = fma(gt, h2, vi);
                         }
                     }
                 }
-                const double wp = rule.w[p];
+                const double wp = rule.w[p], wpn = wp * xn;
                 s0r = fma(wp, pr, s0r);
                 s0i = fma(wp, pi, s0i);
-                u_re = fma(wp, ur, u_re);
-                u_im = fma(wp, ui, u_im);
+                u_re = fma(wpn, ur, u_re);
+                u_im = fma(wpn, ui, u_im);
                 v_re = fma(wp, vr, v_re);
                 v_im = fma(wp, vi, v_im);
             }
@@ -264,7 +256,7 @@ __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm,
     double sc[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) sc[d] = __ldg(prm.sg + (22 + d) * prm.sne + s);
-    float2 yx[NP], yyy[NP], yz[NP], yy2[NP], yn2[NP], wq2[NP];
+    float2 yx[NP], yyy[NP], yz[NP], yy2[NP], wq2[NP];
     const float sn0 = (float)gs.n[0], sn1 = (float)gs.n[1], sn2 = (float)gs.n[2];
 #pragma unroll
     for (int j = 0; j < NP; ++j) {
@@ -280,7 +272,6 @@ __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm,
         yyy[j] = f2(o[0][1], o[1][1]);
         yz[j] = f2(o[0][2], o[1][2]);
         yy2[j] = fma2(yz[j], yz[j], fma2(yyy[j], yyy[j], mul2(yx[j], yx[j])));
-        yn2[j] = fma2(yz[j], b2(sn2), fma2(yyy[j], b2(sn1), mul2(yx[j], b2(sn0))));
         wq2[j] = f2(rule.wf[2 * j], rule.wf[2 * j + 1]);
     }
     const double ek_r = (K == BEMPPCUDA_HELMHOLTZ_COMBINED) ? kap * prm.p[2] : kap;
@@ -301,22 +292,20 @@ __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm,
             if (ST::helm) sincos_cw64(rc, &ph_s, &ph_c);
             const float D0f = (float)D0, D1f = (float)D1, D2f = (float)D2;
             const float2 rcf2 = b2((float)rc), rc2f2 = b2((float)rc2);
-            // k (y - x).n_j = cp_p + yn2_q and k (x - y).n_i = ct_p + ynt_q
-            float nh0 = 0.f, nh1 = 0.f, nh2 = 0.f, Dn = 0.f, th0 = 0.f, th1 = 0.f, th2 = 0.f, Dt = 0.f;
+            // k (y - x).n_j = cp_p (y lies in the plane of j, so (y - c_j).n_j = 0) and
+            // k (x - y).n_i = ynt_q ((x - c_i).n_i = 0): one factor per test point, one per trial point
+            float nh0 = 0.f, nh1 = 0.f, nh2 = 0.f, Dn = 0.f;
             float2 ynt[NP];
             if (ST::dlp_part) {
                 const float tn0 = sb.n[tt][0], tn1 = sb.n[tt][1], tn2 = sb.n[tt][2];
+                const float2 Dt = b2(-fmaf(D2f, tn2, fmaf(D1f, tn1, D0f * tn0)));
 #pragma unroll
                 for (int j = 0; j < NP; ++j)
-                    ynt[j] = fma2(yz[j], b2(-tn2), fma2(yyy[j], b2(-tn1), mul2(yx[j], b2(-tn0))));
+                    ynt[j] = fma2(yz[j], b2(-tn2), fma2(yyy[j], b2(-tn1), fma2(yx[j], b2(-tn0), Dt)));
                 Dn = fmaf(D2f, sn2, fmaf(D1f, sn1, D0f * sn0));
                 nh0 = 0.5f * sn0;
                 nh1 = 0.5f * sn1;
                 nh2 = 0.5f * sn2;
-                Dt = -fmaf(D2f, tn2, fmaf(D1f, tn1, D0f * tn0));
-                th0 = -0.5f * tn0;
-                th1 = -0.5f * tn1;
-                th2 = -0.5f * tn2;
             }
             const float2 D0d = b2(2.f * D0f), D1d = b2(2.f * D1f), D2d = b2(2.f * D2f);
             float2 A[NP];
@@ -328,11 +317,9 @@ __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm,
                 const float4 m = sb.m[tt][p];
                 const float Bp = fmaf(D2f, m.z, fmaf(D1f, m.y, fmaf(D0f, m.x, m.w)));
                 const float2 mx = b2(m.x), my = b2(m.y), mz = b2(m.z), Bp2 = b2(Bp);
-                float2 cp2 = b2(0.f), ct2 = b2(0.f);
-                if (ST::dlp_part) {
-                    cp2 = b2(fmaf(m.z, nh2, fmaf(m.y, nh1, fmaf(m.x, nh0, Dn))));
-                    ct2 = b2(fmaf(m.z, th2, fmaf(m.y, th1, fmaf(m.x, th0, Dt))));
-                }
+                float2 cp2 = b2(0.f);
+                if (ST::dlp_part) cp2 = b2(fmaf(m.z, nh2, fmaf(m.y, nh1, fmaf(m.x, nh0, Dn))));
+                float2 pur = b2(0.f), pui = b2(0.f);  // sum over q of the A_ij double-layer factor, times cp per p
 #pragma unroll
                 for (int j = 0; j < NP; ++j) {
                     const float2 sdot = fma2(yz[j], mz, fma2(yyy[j], my, fma2(yx[j], mx, add2(A[j], Bp2))));
@@ -343,8 +330,8 @@ __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm,
                         if (ST::slp_part) s0r = add2(f, s0r);
                         if (ST::dlp_part) {
                             const float2 fr = mul2(mul2(f, rinv), rinv);
-                            ur = fma2(fr, add2(cp2, yn2[j]), ur);
-                            vr = fma2(fr, add2(ct2, ynt[j]), vr);
+                            pur = add2(fr, pur);
+                            vr = fma2(fr, ynt[j], vr);
                         }
                     } else {
                         const float2 den = fma2(r2, rinv, rcf2);
@@ -359,13 +346,17 @@ __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm,
                             const float2 fr = mul2(f, rinv);
                             const float2 h1 = fma2(rinv, cs, sn);
                             const float2 h2 = fma2(mul2(rinv, b2(-1.f)), sn, cs);
-                            const float2 g = mul2(fr, add2(cp2, yn2[j])), gt = mul2(fr, add2(ct2, ynt[j]));
-                            ur = fma2(g, h1, ur);
-                            ui = fma2(g, h2, ui);
+                            const float2 gt = mul2(fr, ynt[j]);
+                            pur = fma2(fr, h1, pur);
+                            pui = fma2(fr, h2, pui);
                             vr = fma2(gt, h1, vr);
                             vi = fma2(gt, h2, vi);
                         }
                     }
+                }
+                if (ST::dlp_part) {
+                    ur = fma2(cp2, pur, ur);
+                    if (ST::helm) ui = fma2(cp2, pui, ui);
                 }
                 // flush where the test-point weight changes:
                 // entry += w_p [kappa eta S0 + kappa^2 (-h1 sum + i h2 sum)]
