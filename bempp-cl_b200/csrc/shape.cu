@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadR
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t s = col0 + threadIdx.x;
     const bool active = s < P.ne;
-    double y[SH_NQ][3], cs[3] = {0.0, 0.0, 0.0}, sc[3] = {0.0, 0.0, 0.0};
+    double y[SH_NQ][3], cs[3] = {0.0, 0.0, 0.0}, sc[3] = {0.0, 0.0, 0.0}, v0s[3] = {0.0, 0.0, 0.0};
     double ies = 0.0, ies_inv = 0.0, bet = 0.0;
     double2 phs = make_double2(0.0, 0.0), ls = make_double2(0.0, 0.0);
     int sv0 = -1, sv1 = -1, sv2 = -1;
@@ -172,6 +172,7 @@ __global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadR
         for (int c = 0; c < 3; ++c) {
             cs[c] = bet * gs.n[c] * gs.ie;
             sc[c] = __ldg(P.g + (22 + c) * P.ne + s);
+            v0s[c] = gs.v0[c];
         }
         ies = gs.ie;
         ies_inv = 1.0 / gs.ie;
@@ -244,9 +245,14 @@ __global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadR
                 }
                 const double iet = sb.ie[tt], iet_inv = 1.0 / iet;
                 const double ct[3] = {sb.cr[tt][0], sb.cr[tt][1], sb.cr[tt][2]};
+                // sums over the pair's points of G and r G (the eta and d eta / dk terms are linear in G
+                // with per-pair coefficients) and of the u-weighted terms of the area and k derivatives
+                double sgr = 0.0, sgi = 0.0, srgr = 0.0, srgi = 0.0, iz1 = 0.0, iz2 = 0.0, kz = 0.0;
                 for (int p = 0; p < SH_NQ; ++p) {
                     const double x0 = sb.x[tt][p][0], x1 = sb.x[tt][p][1], x2 = sb.x[tt][p][2];
                     const double wp = rule.w[p] * BC_INV_4PI;
+                    // (y - x).(beta_j c_j) = (v0_j - x).(beta_j c_j): y lies in the plane of j
+                    const double xs = fma(v0s[2] - x2, cs[2], fma(v0s[1] - x1, cs[1], (v0s[0] - x0) * cs[0]));
                     double pp[3] = {0.0, 0.0, 0.0};  // row-element point derivative at x_p
 #pragma unroll
                     for (int q = 0; q < SH_NQ; ++q) {
@@ -262,26 +268,38 @@ __global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadR
                             sincos_cw64(P.k * r, &sn, &cn);
                         const double f = (wp * rule.w[q]) * rinv;
                         const double gr = cn * f, gi = sn * f;
-                        QpeTerms o1, o2;
-                        // (i, j): x in i (test), y in j (trial), d = y - x
-                        qpe_ordered(d, r, rinv2, gr, gi, c1r, c1i, cs, ies, P, o1);
-                        // (j, i): test point y, trial point x, d' = -d
-                        const double dn[3] = {-d[0], -d[1], -d[2]};
-                        qpe_ordered(dn, r, rinv2, gr, gi, c2r, c2i, ct, iet, P, o2);
+                        sgr += gr;
+                        sgi += gi;
+                        srgr = fma(r, gr, srgr);
+                        srgi = fma(r, gi, srgi);
+                        const double kq = P.k * r;
+                        const double t13 = fma(-kq, kq, 3.0), k3 = 3.0 * kq;
+                        // (i, j): x in i (test), y in j (trial), d = y - x, Gc = c1 G, z = ikr - 1
+                        const double G1r = c1r * gr - c1i * gi, G1i = fma(c1r, gi, c1i * gr);
+                        const double Z1r = fma(-G1i, kq, -G1r), Z1i = fma(G1r, kq, -G1i);
+                        const double bu1 = xs * rinv2;
+                        const double a1_1 = fma(bu1, fma(G1r, t13, k3 * G1i), ies * (Z1r * P.eta_re - Z1i * P.eta_im));
+                        const double a2_1 = Z1r * rinv2;
+                        // (j, i): test point y, trial point x, d' = -d, Gc = c2 G
+                        const double G2r = c2r * gr - c2i * gi, G2i = fma(c2r, gi, c2i * gr);
+                        const double Z2r = fma(-G2i, kq, -G2r), Z2i = fma(G2r, kq, -G2i);
+                        const double bu2 = -fma(d[2], ct[2], fma(d[1], ct[1], d[0] * ct[0])) * rinv2;
+                        const double a1_2 = fma(bu2, fma(G2r, t13, k3 * G2i), iet * (Z2r * P.eta_re - Z2i * P.eta_im));
+                        const double a2_2 = Z2r * rinv2;
+                        iz1 = fma(bu1, Z1r, iz1);
+                        iz2 = fma(bu2, Z2r, iz2);
+                        kz = fma(fma(bu1, G1r, bu2 * G2r), kq * r, kz);
                         // column element j: trial of (i, j) (+gd1), test of (j, i) (-gd2)
                         // gd of (i, j) minus gd of (j, i): (a1_1 + a1_2) d / r^2 + a2_1 c_j - a2_2 c_i
-                        const double a1s = (o1.a1 + o2.a1) * rinv2;
+                        const double a1s = (a1_1 + a1_2) * rinv2;
 #pragma unroll
                         for (int c = 0; c < 3; ++c) {
-                            const double gj = fma(a1s, d[c], fma(o1.a2, cs[c], -o2.a2 * ct[c]));
+                            const double gj = fma(a1s, d[c], fma(a2_1, cs[c], -a2_2 * ct[c]));
                             cQ[q][c] += gj;
-                            cC[c] = fma(o1.a2, d[c], cC[c]);
+                            cC[c] = fma(a2_1, d[c], cC[c]);
                             pp[c] -= gj;  // row element i: test of (i, j) (-gd1), trial of (j, i) (+gd2)
-                            rs[9 + c] = fma(o2.a2, dn[c], rs[9 + c]);
+                            rs[9 + c] = fma(-a2_2, d[c], rs[9 + c]);
                         }
-                        cI = fma(o2.ival, ies_inv, cI + o1.ere);
-                        rs[12] = fma(o1.ival, iet_inv, rs[12] + o2.ere);
-                        cK += o1.kval + o2.kval;
                     }
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
@@ -290,6 +308,18 @@ __global__ void __launch_bounds__(SH_THREADS) shape_regular(ShapeParams P, QuadR
                         rs[6 + c] = fma(rule.y[p], pp[c], rs[6 + c]);
                     }
                 }
+                // ere_o = Re(eta c_o G) and ival_o = bu_o Re(c_o G z) + ie_o ere_o summed over the points:
+                // E_o = Re(eta c_o sum G); d/dk: Re(c_o (d eta + i r eta) G) = Re(dc_o sum G) - Im(ec_o sum r G)
+                const double ec1r = P.eta_re * c1r - P.eta_im * c1i, ec1i = fma(P.eta_re, c1i, P.eta_im * c1r);
+                const double ec2r = P.eta_re * c2r - P.eta_im * c2i, ec2i = fma(P.eta_re, c2i, P.eta_im * c2r);
+                const double dc1r = P.deta_re * c1r - P.deta_im * c1i, dc1i = fma(P.deta_re, c1i, P.deta_im * c1r);
+                const double dc2r = P.deta_re * c2r - P.deta_im * c2i, dc2i = fma(P.deta_re, c2i, P.deta_im * c2r);
+                const double e1 = ec1r * sgr - ec1i * sgi, e2 = ec2r * sgr - ec2i * sgi;
+                const double k1 = (dc1r * sgr - dc1i * sgi) - fma(ec1r, srgi, ec1i * srgr);
+                const double k2 = (dc2r * sgr - dc2i * sgi) - fma(ec2r, srgi, ec2i * srgr);
+                cI += fma(ies_inv, fma(iet, e2, iz2), e1);
+                rs[12] += fma(iet_inv, fma(ies, e1, iz1), e2);
+                cK += fma(ies, k1, fma(iet, k2, -kz));
             }
 #pragma unroll
             for (int c = 0; c < 3; ++c) rs[9 + c] *= sb.bet[tt];  // a2 d sums lack beta_i
