@@ -448,6 +448,8 @@ def solve_measure(args, torch, grid, domain, a64, amx):
         result[0] = -np.exp(1j * k * x[2])
 
     b = torch.as_tensor(GridFunction(domain, fun=minus_incident).projections(domain), device="cuda")
+    # warm-up (first-call costs of the solver's kernels and host loop), so both solves are timed warm
+    gmres_tensor(lambda v: torch.mv(a64, v), b, tol=1e-8, restart=200, maxiter=5)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     x64, info, res, its = gmres_tensor(lambda v: torch.mv(a64, v), b, tol=1e-8, restart=200, maxiter=2000)

@@ -144,7 +144,9 @@ def test_autograd_function():
     value, state = obj.evaluate(obj.vertices, k, keep=True)
     vgrad, kgrad = obj.gradient(state, k)
     assert abs(j.item() - value.item()) <= 1e-14 * value.item()
-    assert torch.allclose(x.grad, 3.0 * vgrad, rtol=1e-12, atol=1e-14 * vgrad.abs().max().item())
+    # the adjoint adds per-element partial sums with FP64 atomics, so two evaluations agree to
+    # rounding in summation order (measured ~1e-14 of the largest entry), not bit for bit
+    assert torch.allclose(x.grad, 3.0 * vgrad, rtol=1e-12, atol=1e-12 * vgrad.abs().max().item())
     assert abs(kt.grad.item() - 3.0 * kgrad.item()) <= 1e-12 * abs(kgrad.item())
 
 
