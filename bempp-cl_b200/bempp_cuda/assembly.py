@@ -187,6 +187,17 @@ def singular_into_dense(result, descriptor, domain, dual_to_range, parameters, d
     return result
 
 
+def _regular_with_fallback(result, descriptor, domain, dual_to_range, parameters, precision, **kw):
+    """``regular_into`` in ``precision``; where the library has no mixed-precision
+    kernel for the operator (it says so before launching anything) the FP64 one."""
+    try:
+        regular_into(result, descriptor, domain, dual_to_range, parameters, precision=precision, **kw)
+    except _lib.BemppCudaError as exc:
+        if exc.status != _lib.ERR_UNSUPPORTED or precision != _lib.MIXED:
+            raise
+        regular_into(result, descriptor, domain, dual_to_range, parameters, precision=_lib.FP64, **kw)
+
+
 def result_dtype(descriptor):
     return _torch.complex128 if descriptor.is_complex else _torch.float64
 
@@ -209,10 +220,8 @@ def assemble_dense_device(domain, dual_to_range, parameters, descriptor, device_
         )
     elif not fast:
         out.zero_()
-    if precision == _lib.MIXED and not fast:
-        precision = _lib.FP64
-    regular_into(out, descriptor, domain, dual_to_range, parameters, precision=precision, overwrite=fast,
-                 result_is_zero=not fast)
+    _regular_with_fallback(out, descriptor, domain, dual_to_range, parameters, precision, overwrite=fast,
+                           result_is_zero=not fast)
     if _grids_identical(domain, dual_to_range):
         singular_into_dense(out, descriptor, domain, dual_to_range, parameters)
     return out
@@ -251,9 +260,8 @@ def assemble_dense_to_host(domain, dual_to_range, parameters, descriptor, device
         # assemble_combined_field_device, with the identity shift)
         fast = dp0_fast_path(descriptor, domain, dual_to_range, parameters)
         dev = (_torch.empty if fast else _torch.zeros)((rows, cols), dtype=dtype, device="cuda")
-        precision = precision_of(device_interface)
-        regular_into(dev, descriptor, domain, dual_to_range, parameters,
-                     precision=precision if fast else _lib.FP64, overwrite=fast)
+        _regular_with_fallback(dev, descriptor, domain, dual_to_range, parameters, precision_of(device_interface),
+                               overwrite=fast, result_is_zero=not fast)
         if _grids_identical(domain, dual_to_range):
             singular_into_dense(dev, descriptor, domain, dual_to_range, parameters, diag_shift=diag_shift)
         elif diag_shift != 0.0:

@@ -98,8 +98,6 @@ def dense_assembler(device_interface, operator_descriptor, domain, dual_to_range
     require_cuda()
     precision = precision_of(device_interface)
     dev = _torch.zeros(result.shape, dtype=_torch_dtype(result.dtype), device="cuda")
-    if precision == _lib.MIXED and operator_descriptor.assembly_type != "default_scalar":
-        precision = _lib.FP64
     try:
         regular_into(dev, operator_descriptor, domain, dual_to_range, parameters, precision=precision,
                      result_is_zero=True)

@@ -30,6 +30,7 @@ struct QuadRule {
     double y[BEMPPCUDA_MAX_REGULAR_POINTS];
     double w[BEMPPCUDA_MAX_REGULAR_POINTS];
     double sw[BEMPPCUDA_MAX_REGULAR_POINTS][3];  // w times the linear shape values (1 - x - y, x, y)
+    float swf[BEMPPCUDA_MAX_REGULAR_POINTS][3];  // sw rounded to FP32 for the mixed path
     float wf[BEMPPCUDA_MAX_REGULAR_POINTS];      // w rounded to FP32 for the mixed path
 };
 
@@ -57,6 +58,7 @@ inline void fill_rule(QuadRule &rule, int nq, const double *points, const double
         rule.sw[i][0] = rule.w[i] * (1.0 - rule.x[i] - rule.y[i]);
         rule.sw[i][1] = rule.w[i] * rule.x[i];
         rule.sw[i][2] = rule.w[i] * rule.y[i];
+        for (int k = 0; k < 3; ++k) rule.swf[i][k] = (float)rule.sw[i][k];
         rule.wf[i] = (float)rule.w[i];
     }
 }

@@ -1,0 +1,221 @@
+// Mixed-precision regular pairs of the Helmholtz single layer and
+// hypersingular operators on P1 spaces (6-point rule, real k > 0): the FP32
+// counterpart of regular_p1 (p1.cuh) with the geometry of the mixed DP0
+// kernels (dp0.cuh).
+//
+// Lengths are in units of 1/k.  Per element pair the centroid offset
+// D = k (c_s - c_t), r_c' = |D| and exp(i r_c') are FP64; per point pair only
+//   r'^2 - r_c'^2 = A_q + B_p + yo_q . m_p,
+//   A_q = |yo_q|^2 + 2 D . yo_q,  B_p = |xo_p|^2 - 2 D . xo_p,  m_p = -2 xo_p,
+// (xo, yo: the points' offsets from their centroids, times k) is formed in
+// FP32, 1/r' by rsqrt.approx, the phase offset theta = (r'^2 - r_c'^2) /
+// (r' + r_c') without cancellation and its sine / cosine by the fitted FP32
+// polynomials; trial points q, q+1 travel together through packed f32x2 FMAs.
+// The trial sums T_j(p) = sum_q w_q psi_j(q) exp(i theta) / r' and the 3 x 3
+// block sum_p w_p phi_i(p) T_j(p) are FP32 (36 terms per entry); the block
+// is converted to FP64 once per element pair, where k / (4 pi), the
+// integration elements, exp(i r_c') and (hypersingular) the curl and normal
+// products are applied.  SYM as in regular_p1: pairs i < j, the block added
+// at (i, j) and, unless deferred to the transpose pass, at (j, i).
+#pragma once
+
+#include "p1.cuh"
+
+namespace bc {
+
+struct TestBlockP1m {
+    float4 m[P1_TCHUNK][NQ6];  // (-2 xo, |xo|^2), xo = k (x_p - c_t)
+    double c[P1_TCHUNK][3];
+    double n[P1_TCHUNK][3];
+    double curl[P1_TCHUNK][3][3];
+    double ie[P1_TCHUNK];
+    double mult[P1_TCHUNK][3];
+    int64_t row[P1_TCHUNK][3];
+    int v[P1_TCHUNK][3];
+};
+
+template <int ASM, int PHC, bool SYM>
+__global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, QuadRule rule) {
+    constexpr bool HYP = ASM == BEMPPCUDA_ASM_HELM_HYP;
+    constexpr int NP = NQ6 / 2;
+    __shared__ TestBlockP1m sb;
+    const double kap = prm.p[0];
+
+    const int64_t t0 = (int64_t)blockIdx.y * P1_TCHUNK;
+    if (SYM && t0 >= ((int64_t)blockIdx.x + 1) * DP0_THREADS) return;  // below the diagonal
+    const int tcount = (int)min((int64_t)P1_TCHUNK, prm.ntest - t0);
+    for (int idx = threadIdx.x; idx < tcount; idx += blockDim.x) {
+        const int64_t t = prm.tsup[t0 + idx];
+        Geom g;
+        load_geom(prm.tg, prm.tne, t, prm.tnm ? (double)prm.tnm[t] : 1.0, g);
+        double c[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) c[d] = __ldg(prm.tg + (22 + d) * prm.tne + t);
+        for (int p = 0; p < NQ6; ++p) {
+            double x[3];
+            to_global(g, rule.x[p], rule.y[p], x);
+            const float o0 = (float)(kap * (x[0] - c[0])), o1 = (float)(kap * (x[1] - c[1])),
+                        o2 = (float)(kap * (x[2] - c[2]));
+            sb.m[idx][p] = make_float4(-2.f * o0, -2.f * o1, -2.f * o2, fmaf(o2, o2, fmaf(o1, o1, o0 * o0)));
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            sb.c[idx][d] = c[d];
+            sb.n[idx][d] = g.n[d];
+            sb.v[idx][d] = __ldg(prm.tel + 3 * t + d);
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            sb.mult[idx][i] = prm.tmult[t * 3 + i];
+            sb.row[idx][i] = prm.tl2g[t * 3 + i];
+        }
+        if (HYP) {
+            double cu[3][3];
+            surface_curls(prm.tg, prm.tne, t, g.n, cu);
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) sb.curl[idx][i][d] = cu[i][d];
+        }
+        sb.ie[idx] = g.ie;
+    }
+    __syncthreads();
+
+    const int64_t si = (int64_t)blockIdx.x * DP0_THREADS + threadIdx.x;
+    if (si >= prm.ntrial) return;
+    const int64_t s = prm.ssup[si];
+    Geom gs;
+    load_geom(prm.sg, prm.sne, s, prm.snm ? (double)prm.snm[s] : 1.0, gs);
+    const int sv0 = __ldg(prm.sel + 3 * s), sv1 = __ldg(prm.sel + 3 * s + 1), sv2 = __ldg(prm.sel + 3 * s + 2);
+    double sc[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) sc[d] = __ldg(prm.sg + (22 + d) * prm.sne + s);
+    // trial offsets k (y_q - c_s), q = 2 jj, 2 jj + 1 packed
+    float2 yx[NP], yyy[NP], yz[NP], yy2[NP];
+#pragma unroll
+    for (int jj = 0; jj < NP; ++jj) {
+        float o[2][3];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            double v[3];
+            to_global(gs, rule.x[2 * jj + h], rule.y[2 * jj + h], v);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) o[h][d] = (float)(kap * (v[d] - sc[d]));
+        }
+        yx[jj] = f2(o[0][0], o[1][0]);
+        yyy[jj] = f2(o[0][1], o[1][1]);
+        yz[jj] = f2(o[0][2], o[1][2]);
+        yy2[jj] = fma2(yz[jj], yz[jj], fma2(yyy[jj], yyy[jj], mul2(yx[jj], yx[jj])));
+    }
+    double curl_s[3][3];
+    if (HYP) surface_curls(prm.sg, prm.sne, s, gs.n, curl_s);
+    int64_t scol[3];
+    double smul[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        scol[j] = prm.sl2g[s * 3 + j];
+        smul[j] = prm.smult[s * 3 + j];
+    }
+
+    for (int tt = 0; tt < tcount; ++tt) {
+        if (SYM && t0 + tt >= si) break;  // rows increase with tt
+        if (prm.grids_identical && shares_vertex(sb.v[tt], sv0, sv1, sv2)) continue;
+        const double D0 = kap * (sc[0] - sb.c[tt][0]), D1 = kap * (sc[1] - sb.c[tt][1]),
+                     D2 = kap * (sc[2] - sb.c[tt][2]);
+        const double rc2 = fma(D2, D2, fma(D1, D1, D0 * D0));
+        const double rc = sqrt(rc2);
+        double ph_s, ph_c;
+        sincos_cw64(rc, &ph_s, &ph_c);
+        const float D0f = (float)D0, D1f = (float)D1, D2f = (float)D2;
+        const float2 rcf2 = b2((float)rc), rc2f2 = b2((float)rc2);
+        const float2 D0d = b2(2.f * D0f), D1d = b2(2.f * D1f), D2d = b2(2.f * D2f);
+        float2 A[NP];
+#pragma unroll
+        for (int jj = 0; jj < NP; ++jj) A[jj] = fma2(D2d, yz[jj], fma2(D1d, yyy[jj], fma2(D0d, yx[jj], yy2[jj])));
+        float lre[3][3], lim[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) lre[i][j] = lim[i][j] = 0.f;
+#pragma unroll 2
+        for (int p = 0; p < NQ6; ++p) {
+            const float4 m = sb.m[tt][p];
+            const float Bp = fmaf(D2f, m.z, fmaf(D1f, m.y, fmaf(D0f, m.x, m.w)));
+            const float2 mx = b2(m.x), my = b2(m.y), mz = b2(m.z), Bp2 = b2(Bp);
+            float2 tre[3] = {b2(0.f), b2(0.f), b2(0.f)}, tim[3] = {b2(0.f), b2(0.f), b2(0.f)};
+#pragma unroll
+            for (int jj = 0; jj < NP; ++jj) {
+                const float2 sdot = fma2(yz[jj], mz, fma2(yyy[jj], my, fma2(yx[jj], mx, add2(A[jj], Bp2))));
+                const float2 r2 = add2(rc2f2, sdot);
+                const float2 rinv = f2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+                const float2 den = fma2(r2, rinv, rcf2);
+                const float2 th = mul2(sdot, f2(rcp_approx(den.x), rcp_approx(den.y)));
+                float2 sn, cs;
+                sincos2<PHC>(th, &sn, &cs);
+                const float2 kr = mul2(rinv, cs), ki = mul2(rinv, sn);
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const float2 w = f2(rule.swf[2 * jj][j], rule.swf[2 * jj + 1][j]);
+                    tre[j] = fma2(kr, w, tre[j]);
+                    tim[j] = fma2(ki, w, tim[j]);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const float ph = rule.swf[p][i];
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    lre[i][j] = fmaf(ph, tre[j].x + tre[j].y, lre[i][j]);
+                    lim[i][j] = fmaf(ph, tim[j].x + tim[j].y, lim[i][j]);
+                }
+            }
+        }
+        // k / (4 pi) |J_t| |J_s| exp(i r_c'), then the hypersingular combination
+        const double scale = kap * BC_INV_4PI * sb.ie[tt] * gs.ie;
+        double sre = 0.0, sim = 0.0, cpf = 0.0;
+        if (HYP) {
+            // S = sum_pq w_p w_q G: the P1 functions add up to 1 on each side
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    sre += (double)lre[i][j];
+                    sim += (double)lim[i][j];
+                }
+            cpf = -kap * kap * (sb.n[tt][0] * gs.n[0] + sb.n[tt][1] * gs.n[1] + sb.n[tt][2] * gs.n[2]);
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const double mt = sb.mult[tt][i];
+            if (mt == 0.0) continue;
+            const int64_t row = sb.row[tt][i];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const double ms = smul[j];
+                if (ms == 0.0) continue;
+                double vr = (double)lre[i][j], vi = (double)lim[i][j];
+                if (HYP) {
+                    const double cij = sb.curl[tt][i][0] * curl_s[j][0] + sb.curl[tt][i][1] * curl_s[j][1] +
+                                       sb.curl[tt][i][2] * curl_s[j][2];
+                    vr = fma(cij, sre, cpf * vr);
+                    vi = fma(cij, sim, cpf * vi);
+                }
+                const double tr = vr * ph_c - vi * ph_s;
+                vi = fma(vr, ph_s, vi * ph_c);
+                vr = tr;
+                const double mm = mt * ms * scale;
+                const int64_t col = scol[j];
+                double *o = reinterpret_cast<double *>(prm.result) + 2 * (row * prm.ld + col);
+                atomicAdd(o, vr * mm);
+                atomicAdd(o + 1, vi * mm);
+                if (SYM && !prm.defer_transpose) {
+                    double *ot = reinterpret_cast<double *>(prm.result) + 2 * (col * prm.ld + row);
+                    atomicAdd(ot, vr * mm);
+                    atomicAdd(ot + 1, vi * mm);
+                }
+            }
+        }
+    }
+}
+
+}  // namespace bc

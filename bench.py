@@ -352,7 +352,7 @@ def gpu_arm(args, world, rank, local):
     breadth = None
     if not args.skip_breadth and world == 1:
         torch.cuda.empty_cache()
-        breadth = breadth_measure(args, torch, peaks["fp64"])
+        breadth = breadth_measure(args, torch, peaks["fp64"], peaks["fp32"])
     shape = None
     if not args.skip_shape and world == 1:
         torch.cuda.empty_cache()
@@ -682,7 +682,7 @@ BREADTH = [
 ]
 
 
-def breadth_measure(args, torch, fp64_peak=None):
+def breadth_measure(args, torch, fp64_peak=None, fp32_peak=None):
     """FP64 throughput of the other operator families (dense weak form through the operator API).
 
     GPU: CUDA events around the full assembly (regular + singular passes) of
@@ -773,6 +773,40 @@ def breadth_measure(args, torch, fp64_peak=None):
             entry["matvec_note"] = "2048^2 f64 = 33.5 MB, resident in the 126 MB L2 between calls"
             del mat
         out.append(entry)
+        torch.cuda.empty_cache()
+
+    # mixed precision on P1 (device_interface "cuda_mixed"): FP32 regular pairs, against the FP64 weak form
+    for name, path, level, k, flops_pp in (("helmholtz.single_layer p1 mixed", "helmholtz.single_layer", 5, 5.0, 38),
+                                           ("helmholtz.hypersingular p1 mixed", "helmholtz.hypersingular", 5, 5.0, 56)):
+        g = grid_of(level)
+        sp = function_space(g, "P", 1)
+        f = factory(path)
+        op64, opmx = f(sp, sp, sp, k), f(sp, sp, sp, k, device_interface="cuda_mixed")
+        ref = op64._assemble()
+        opmx._assemble()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(max(args.steps, 1)):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            mat = opmx._assemble()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        err = float((torch.linalg.norm(mat.tensor - ref.tensor) / torch.linalg.norm(ref.tensor)).item())
+        rows = cols = sp.global_dof_count
+        ne = g.number_of_elements
+        qpe = 36.0 * ne * ne
+        gms = float(np.median(ms))
+        achieved = qpe * flops_pp / (gms * 1e-3) / 1e12
+        out.append({"operator": name, "level": level, "k": k, "shape": [rows, cols], "gpu_ms": gms,
+                    "gpu_entries_per_s": rows * cols / (gms * 1e-3), "rel_fro_err_vs_fp64": err,
+                    "roofline": {"bound": "fp32", "flops_per_qpe": flops_pp, "qpe": qpe, "achieved": achieved,
+                                 "unit": "TFLOP/s", "peak": fp32_peak,
+                                 "frac": achieved / fp32_peak if fp32_peak else None},
+                    "note": "FP32 regular pairs, FP64 singular pairs and per-pair blocks"})
+        del ref, mat
         torch.cuda.empty_cache()
 
     # potential: 10 000 shell points, P1 coefficients, k = 5

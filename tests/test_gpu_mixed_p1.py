@@ -1,0 +1,90 @@
+"""Mixed precision on P1 spaces (run on a B200).
+
+The Helmholtz single layer and hypersingular operators on P1 evaluate their
+regular pairs in FP32 (``regular_p1_mixed``) under ``device_interface=
+"cuda_mixed"``; their operator error against the FP64 path and the oracle is
+held to the mixed-precision bound (1e-6 relative Frobenius).  Operators
+without a mixed kernel (double layers, Laplace, complex k) run in FP64 under
+the same interface.
+"""
+
+import numpy as np
+import pytest
+
+from conftest import rel_fro
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def _op(path, sp, k, interface):
+    from bempp_cuda import operators
+
+    f = operators.boundary
+    for part in path.split("."):
+        f = getattr(f, part)
+    return f(sp, sp, sp, device_interface=interface) if k is None else f(sp, sp, sp, k, device_interface=interface)
+
+
+@pytest.mark.parametrize("k", [2.0, 4.0, 40.0])
+@pytest.mark.parametrize("path", ["helmholtz.single_layer", "helmholtz.hypersingular"])
+def test_mixed_p1_against_fp64_and_oracle(oracle, path, k):
+    """k = 2, 4, 40 on a 512-element ellipsoid reach the three phase classes."""
+    from cases import oracle_dense
+
+    from bempp_cuda.shapes import ellipsoid
+    from bempp_cuda.space import function_space
+
+    grid = ellipsoid(3, 1.1, 0.9, 1.0)
+    sp = function_space(grid, "P", 1)
+    a64 = _op(path, sp, k, "cuda").weak_form().tensor
+    amx = _op(path, sp, k, "cuda_mixed").weak_form().tensor
+    err = (torch.linalg.norm(amx - a64) / torch.linalg.norm(a64)).item()
+    assert 0.0 < err < 1e-6, err  # FP32 evaluation: close, not identical
+    ref = oracle_dense(oracle, _op(path, sp, k, "cuda"), sp, sp)
+    assert rel_fro(amx.cpu().numpy(), ref) < 1e-6
+
+
+@pytest.mark.parametrize("path", ["helmholtz.single_layer", "helmholtz.hypersingular"])
+def test_mixed_p1_sweeps_agree(path):
+    """Symmetric sweep (both blocks by atomics, or U + U^T into a zeroed result) and per-pair sweep."""
+    from bempp_cuda import _lib
+    from bempp_cuda.assembly import regular_into, singular_into_dense
+    from bempp_cuda.operators import Parameters
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+
+    grid = regular_sphere(3)
+    sp = function_space(grid, "P", 1)
+    d = _op(path, sp, 5.0, "cuda").descriptor
+    n = sp.global_dof_count
+    out = {}
+    for precision in (_lib.FP64, _lib.MIXED):
+        for sym, zero in ((True, False), (False, False), (True, True)):
+            a = torch.zeros((n, n), dtype=torch.complex128, device="cuda")
+            regular_into(a, d, sp, sp, Parameters(), precision=precision, symmetric=sym, result_is_zero=zero)
+            singular_into_dense(a, d, sp, sp, Parameters())
+            out[(precision, sym, zero)] = a
+    ref = out[(_lib.FP64, False, False)]
+    for key, a in out.items():
+        tol = 1e-13 if key[0] == _lib.FP64 else 1e-6
+        assert (torch.linalg.norm(a - ref) / torch.linalg.norm(ref)).item() < tol, key
+
+
+@pytest.mark.parametrize("path,k", [("helmholtz.double_layer", 3.0), ("laplace.single_layer", None),
+                                    ("helmholtz.single_layer", 3.0 + 0.5j)])
+def test_mixed_interface_without_mixed_kernel_is_fp64(path, k):
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+
+    sp = function_space(regular_sphere(2), "P", 1)
+    a64 = _op(path, sp, k, "cuda").weak_form().tensor
+    amx = _op(path, sp, k, "cuda_mixed").weak_form().tensor
+    assert (torch.linalg.norm(amx - a64) / torch.linalg.norm(a64)).item() < 1e-13
