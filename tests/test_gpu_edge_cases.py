@@ -216,3 +216,43 @@ def test_every_boundary_operator_on_extreme_adjacency(which, oracle):
         ref = oracle_dense(oracle, op, domain, dual)
         scale = max(np.linalg.norm(ref), 1e-300)
         assert np.linalg.norm(got - ref) <= 1e-12 * scale, key
+
+
+def _open_sphere(level, removed):
+    """regular_sphere(level) without its last ``removed`` elements: an open surface with boundary edges."""
+    from bempp_cuda.grid import Grid
+    from bempp_cuda.shapes import regular_sphere
+
+    g = regular_sphere(level)
+    keep = np.arange(g.number_of_elements - removed)
+    used = np.unique(g.elements[:, keep])
+    remap = -np.ones(g.vertices.shape[1], dtype=np.int64)
+    remap[used] = np.arange(len(used))
+    return Grid(g.vertices[:, used], remap[g.elements[:, keep]].astype(np.uint32))
+
+
+@pytest.mark.parametrize("key", ["maxwell_efie_rwg_snc", "maxwell_mfie_rwg_snc", "helmholtz_slp_p1_p1",
+                                 "helmholtz_hyp_p1_p1", "helmholtz_dlp_p1_p1"])
+def test_specialised_kernels_on_an_open_surface(oracle, key):
+    """Boundary edges / vertices carry no dof (zero multipliers): the RWG and P1 kernels skip them."""
+    from cases import BOUNDARY, boundary_operator, oracle_dense
+
+    if key not in BOUNDARY:
+        pytest.skip("case not defined")
+    grid = _open_sphere(3, 37)
+    op, domain, dual = boundary_operator(key, grid)
+    got = op.weak_form().tensor.cpu().numpy()
+    ref = oracle_dense(oracle, op, domain, dual)
+    assert np.linalg.norm(got - ref) <= 1e-12 * np.linalg.norm(ref), key
+
+
+def test_mixed_p1_on_an_open_surface():
+    from bempp_cuda import operators
+    from bempp_cuda.space import function_space
+
+    sp = function_space(_open_sphere(3, 37), "P", 1)
+    for name in ("single_layer", "hypersingular"):
+        f = getattr(operators.boundary.helmholtz, name)
+        a64 = f(sp, sp, sp, 4.0).weak_form().tensor
+        amx = f(sp, sp, sp, 4.0, device_interface="cuda_mixed").weak_form().tensor
+        assert (torch.linalg.norm(amx - a64) / torch.linalg.norm(a64)).item() < 1e-6, name
