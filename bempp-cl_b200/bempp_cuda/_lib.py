@@ -134,6 +134,7 @@ class SingularArgs(_ct.Structure):
         ("ld", _i64),
         ("diag_shift", _ct.c_double),
         ("phase_radius", _ct.c_double),
+        ("mirror_weights_offset", _i64),
     ]
 
 

@@ -24,7 +24,7 @@ from .device import (
     ptr,
     require_cuda,
 )
-from .quadrature import triangle_rule
+from .quadrature import number_of_duffy_points, triangle_rule
 
 _REG_CACHE = {}
 
@@ -154,11 +154,14 @@ def dp0_fast_path(descriptor, domain, dual_to_range, parameters):
 
 
 def singular_into_dense(result, descriptor, domain, dual_to_range, parameters, diag_shift=0.0, stream=None,
-                        geometry=None, rows=None):
+                        geometry=None, rows=None, mirror=True):
     """Scatter the Sauter-Schwab pairs into the dense device tensor ``result`` (``geometry`` as in regular_into).
 
     ``rows=(lo, hi)``: only the pairs whose test element is one of the support
     elements lo .. hi-1 of ``dual_to_range`` (support in increasing order).
+    ``mirror`` (default) lets the DP0 kernel evaluate each vertex-adjacent pair
+    once for both orders when both spaces are the same; ``mirror=False``
+    evaluates every ordered pair on its own.
     """
     kernel, assembly = kernel_ids(descriptor)
     if result.numel() == 0:
@@ -183,6 +186,13 @@ def singular_into_dense(result, descriptor, domain, dual_to_range, parameters, d
     args.ld = result.stride(0)
     args.diag_shift = float(diag_shift)
     args.phase_radius = 1.0001 * 2.0 * (geometry or device_grid(grid)).radius
+    if mirror and same_space(domain, dual_to_range):
+        # every pair is listed in both orders and the vertex-adjacent rule (its weights follow the
+        # coincident and edge-adjacent ones) is symmetric in test and trial points: the DP0 kernel
+        # evaluates each such pair once for both entries
+        order = parameters.quadrature.singular
+        args.mirror_weights_offset = (number_of_duffy_points(order, "coincident")
+                                      + number_of_duffy_points(order, "edge_adjacent"))
     _lib.check(_lib.load().bemppcuda_assemble_singular(args, stream or current_stream()))
     return result
 

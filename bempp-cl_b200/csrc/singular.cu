@@ -33,6 +33,7 @@ struct SingParams {
     const double *tmult, *smult;
     double diag_shift;
     int64_t ntab, nw;  // point-table and weight-table lengths
+    int64_t mirror_woff;  // > 0: pairs with this weights offset add both orders (test < trial) or nothing
 };
 
 // A pair whose element ids or table ranges fall outside the grid / tables is
@@ -224,17 +225,41 @@ __global__ void __launch_bounds__(32 * SING_WARPS) singular_dp0(SingParams prm) 
     const int64_t k = (int64_t)blockIdx.x * SING_WARPS + (threadIdx.x >> 5);
     if (k >= prm.npairs || !pair_in_range(prm, k)) return;
     const int64_t t = prm.te[k], s = prm.se[k];
+    // a vertex-adjacent pair in dense mode: the reverse pair's points are these points with the roles
+    // exchanged, so the pair with t < s gives both entries and the other one nothing
+    const bool mirror = !prm.values && prm.mirror_woff > 0 && (int64_t)prm.woff[k] == prm.mirror_woff;
+    if (mirror && t > s) return;
     Geom gt, gs;
     load_geom(prm.g, prm.ne, t, prm.tnm ? (double)prm.tnm[t] : 1.0, gt);
     load_geom(prm.g, prm.ne, s, prm.snm ? (double)prm.snm[s] : 1.0, gs);
-    double vr, vi;
-    sing_dp0_value<K, PHC>(prm.g, prm.ne, t, s, gt, gs, prm.p, reinterpret_cast<const double2 *>(prm.tp),
-                           reinterpret_cast<const double2 *>(prm.sp), prm.w, prm.toff[k], prm.soff[k],
-                           prm.woff[k], (int)prm.npts[k], &vr, &vi);
+    double vr, vi, ur = 0.0, ui = 0.0;
+    if (mirror)
+        sing_dp0_pair<K, PHC>(prm.g, prm.ne, t, s, gt, gs, prm.p, reinterpret_cast<const double2 *>(prm.tp),
+                              reinterpret_cast<const double2 *>(prm.sp), prm.w, prm.toff[k], prm.soff[k],
+                              prm.woff[k], (int)prm.npts[k], &vr, &vi, &ur, &ui);
+    else
+        sing_dp0_value<K, PHC>(prm.g, prm.ne, t, s, gt, gs, prm.p, reinterpret_cast<const double2 *>(prm.tp),
+                               reinterpret_cast<const double2 *>(prm.sp), prm.w, prm.toff[k], prm.soff[k],
+                               prm.woff[k], (int)prm.npts[k], &vr, &vi);
     if (lane != 0) return;
     const double scale = BC_INV_4PI * gt.ie * gs.ie;
     vr *= scale;
     vi *= scale;
+    if (mirror) {
+        // the (s, t) entry
+        const double mt = prm.tmult[s], ms = prm.smult[t];
+        if (mt != 0.0 && ms != 0.0) {
+            const int64_t row = prm.tl2g[s], col = prm.sl2g[t];
+            const double mm = mt * ms * scale;
+            if (prm.is_complex) {
+                double *o = reinterpret_cast<double *>(prm.dense) + 2 * (row * prm.ld + col);
+                atomicAdd(o, ur * mm);
+                atomicAdd(o + 1, ui * mm);
+            } else {
+                atomicAdd(reinterpret_cast<double *>(prm.dense) + row * prm.ld + col, ur * mm);
+            }
+        }
+    }
     if (prm.values) {
         if (prm.is_complex) {
             double *o = reinterpret_cast<double *>(prm.values) + 2 * k;
@@ -313,6 +338,7 @@ int bc_singular_launch(const bemppcuda_singular_args *a, cudaStream_t st) {
     prm.diag_shift = a->diag_shift;
     prm.ntab = a->npoints_table;
     prm.nw = a->nweights;
+    prm.mirror_woff = a->mirror_weights_offset;
     if (prm.npairs == 0) return BEMPPCUDA_OK;
     cudaError_t err = cudaSuccess;
     const bool real_k = a->params[1] == 0.0;

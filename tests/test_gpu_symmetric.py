@@ -155,6 +155,28 @@ def test_maxwell_rwg_kernel_against_oracle(oracle, name, k):
         assert np.linalg.norm(got - ref) <= 1e-12 * np.linalg.norm(ref), (name, k, sym)
 
 
+@pytest.mark.parametrize("kernel,options", KERNELS)
+def test_singular_vertex_pairs_mirrored(kernel, options):
+    """DP0 singular pass: each vertex-adjacent pair evaluated once for both orders = every ordered pair."""
+    from bempp_cuda.assembly import singular_into_dense
+    from bempp_cuda.operators import OperatorDescriptor, Parameters
+    from bempp_cuda.shapes import ellipsoid
+    from bempp_cuda.space import function_space
+
+    grid = ellipsoid(3, 1.0, 0.8, 1.2)
+    sp = function_space(grid, "DP", 0)
+    is_complex = not kernel.startswith("laplace")
+    desc = OperatorDescriptor("probe", options, kernel, "default_scalar", "double", is_complex, None, 1)
+    n = grid.number_of_elements
+    out = []
+    for mirror in (True, False):
+        a = torch.zeros((n, n), dtype=torch.complex128 if is_complex else torch.float64, device="cuda")
+        singular_into_dense(a, desc, sp, sp, Parameters(), diag_shift=-0.5, mirror=mirror)
+        out.append(a)
+    torch.cuda.synchronize()
+    assert (torch.linalg.norm(out[0] - out[1]) / torch.linalg.norm(out[1])).item() < 1e-13
+
+
 @pytest.mark.parametrize("blocks", [1, 5, 16])
 def test_weak_form_to_host_streams_row_blocks(blocks):
     """Row-block symmetric assembly streamed to pinned host memory = the device weak form."""
