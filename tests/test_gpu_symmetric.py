@@ -227,3 +227,31 @@ def test_weak_form_to_host_on_a_row_block():
     ref = (full_dlp - 0.5 * full_id - 1j * k * full_slp).weak_form().tensor.cpu()[100:300]
     assert host.shape == (200, grid.number_of_elements)
     assert (torch.linalg.norm(host - ref) / torch.linalg.norm(ref)).item() < 1e-13
+
+
+@pytest.mark.parametrize("world", [1, 3])
+def test_row_blocks_reproduce_the_operator(world):
+    """distributed.assemble_row_block: each rank's rows (a DP0 dual restricted to its block; its
+    singular pairs) equal those rows of the whole operator, identity shift included."""
+    from bempp_cuda import _lib
+    from bempp_cuda.assembly import regular_into, singular_into_dense
+    from bempp_cuda.distributed import assemble_row_block, row_block
+    from bempp_cuda.operators import OperatorDescriptor, Parameters
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+
+    grid = regular_sphere(3)
+    sp = function_space(grid, "DP", 0)
+    desc = OperatorDescriptor("probe", [6.0, 0.0, 0.0, -6.0], "helmholtz_combined_field", "default_scalar", "double",
+                              True, None, 1)
+    n = grid.number_of_elements
+    full = torch.empty((n, n), dtype=torch.complex128, device="cuda")
+    regular_into(full, desc, sp, sp, Parameters(), overwrite=True)
+    singular_into_dense(full, desc, sp, sp, Parameters(), diag_shift=-0.5)
+    for rank in range(world):
+        lo, hi = row_block(n, world, rank)
+        for precision, tol in ((None, 1e-13), (_lib.MIXED, 1e-6)):
+            block = assemble_row_block(grid, desc, world, rank, precision=precision, diag_shift=-0.5)
+            assert block.shape == (hi - lo, n)
+            ref = full[lo:hi]
+            assert (torch.linalg.norm(block - ref) / torch.linalg.norm(ref)).item() < tol, (rank, precision)
