@@ -10,7 +10,12 @@
 // layer sums: with constant surface curls per element,
 //   L_ij = (curl_i . curl_j) S - c (n_t . n_s) M_ij,  S = sum_j T_j summed over p
 // (the P1 shape functions add up to 1), c = k^2 (Helmholtz), 0 (Laplace).
-// exp(ikr) is factored about the centroid distance as in the DP0 kernels.
+// exp(ikr) is factored about the centroid distance as in the DP0 kernels
+// (phase classes 1, 2); class 3 is a complex wavenumber k = kr + i ki:
+// exp(i kr r) from the reduced sine / cosine times exp(-ki r), the double-layer
+// factor (ikr - 1) / r = (-1/r - ki) + i kr, and -k^2 complex in the
+// hypersingular operator.  The symmetric and skew sweeps hold for complex k
+// (G(x, y) = G(y, x)).
 // The NT x NS block is added to the matrix with FP64 atomics (l2g, multipliers).
 // SYM (the same space on both sides): only pairs i < j (support positions) are
 // evaluated and each gives the blocks at (i, j) and (j, i).  Single layer and
@@ -56,7 +61,8 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
                            K == BEMPPCUDA_HELMHOLTZ_ADLP);
     constexpr bool DL = (K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_HELMHOLTZ_DLP);
     constexpr bool AD = (K == BEMPPCUDA_LAPLACE_ADLP || K == BEMPPCUDA_HELMHOLTZ_ADLP);
-    constexpr bool PH = HELM && PHC > 0;
+    constexpr bool PH = HELM && (PHC == 1 || PHC == 2);
+    constexpr bool CK = HELM && PHC == 3;
     static_assert(!SYM || NT == NS, "the symmetric sweep needs one space on both sides");
     constexpr bool SKEW = SYM && (DL || AD);  // the transposed block uses the other element's normal
     __shared__ TestBlockP1 sb;
@@ -109,7 +115,7 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
     if (HYP) surface_curls(prm.sg, prm.sne, s, gs.n, curl_s);
     // trial / test shape values times the weights (constant operands from the rule)
     const auto psw = [&](int q, int j) -> double { return NS == 1 ? rule.w[q] : rule.sw[q][j]; };
-    const double kr = prm.p[0];
+    const double kr = prm.p[0], ki = CK ? prm.p[1] : 0.0;
     // the trial dofs and multipliers stay in registers for the whole tile
     int64_t scol[NS];
     double smul[NS];
@@ -182,9 +188,14 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
                             sincos_small64(fma(kr, r, -krc), &sn, &cs);
                         else
                             sincos_cw64(kr * r, &sn, &cs);
-                        const double rinv2 = rinv * rinv;
-                        hre = -rinv2 * fma(rinv, cs, kr * sn);
-                        him = rinv2 * fma(kr, cs, -rinv * sn);
+                        if (CK) {
+                            const double am = exp(-ki * r);
+                            sn *= am;
+                            cs *= am;
+                        }
+                        const double rinv2 = rinv * rinv, rk = rinv + ki;
+                        hre = -rinv2 * fma(rk, cs, kr * sn);
+                        him = rinv2 * fma(kr, cs, -rk * sn);
                     }
                     // the double layer of (test, trial) uses the trial normal; its transpose the test normal
                     const double a1 = DL ? dS : -dT, a2 = DL ? -dT : dS;
@@ -209,6 +220,11 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
                         sincos_small64(fma(kr, r, -krc), &sn, &cs);
                     else
                         sincos_cw64(kr * r, &sn, &cs);
+                    if (CK) {
+                        const double am = exp(-ki * r);
+                        sn *= am;
+                        cs *= am;
+                    }
                     if (K == BEMPPCUDA_HELMHOLTZ_SLP) {
                         kre = cs * rinv;
                         kim = sn * rinv;
@@ -216,9 +232,9 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
                         // (ikr - 1) e^{ikr} dot / r^3 = g (-h1 + i h2), g = dot / r^2
                         const double dot = DL ? ynv[q] + xn
                                               : -fma(d2, sb.n[tt][2], fma(d1, sb.n[tt][1], d0 * sb.n[tt][0]));
-                        const double g = dot * rinv * rinv;
-                        kre = -g * fma(rinv, cs, kr * sn);
-                        kim = g * fma(kr, cs, -rinv * sn);
+                        const double g = dot * rinv * rinv, rk = rinv + ki;
+                        kre = -g * fma(rk, cs, kr * sn);
+                        kim = g * fma(kr, cs, -rk * sn);
                     }
                 }
 #pragma unroll
@@ -256,10 +272,13 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
                 }
         }
         const double scale = BC_INV_4PI * sb.ie[tt] * gs.ie;
-        double cpf = 0.0;
-        if (HYP) cpf = ASM == BEMPPCUDA_ASM_HELM_HYP
-                           ? -kr * kr * (sb.n[tt][0] * gs.n[0] + sb.n[tt][1] * gs.n[1] + sb.n[tt][2] * gs.n[2])
-                           : 0.0;
+        // hypersingular: -k^2 (n_t . n_s), complex for a complex wavenumber
+        double cpf = 0.0, cpi = 0.0;
+        if (HYP && ASM == BEMPPCUDA_ASM_HELM_HYP) {
+            const double nn = sb.n[tt][0] * gs.n[0] + sb.n[tt][1] * gs.n[1] + sb.n[tt][2] * gs.n[2];
+            cpf = -(kr * kr - ki * ki) * nn;
+            cpi = -2.0 * kr * ki * nn;
+        }
 #pragma unroll
         for (int i = 0; i < NT; ++i) {
             const double mt = sb.mult[tt][i];
@@ -273,8 +292,9 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
                 if (HYP) {
                     const double cij = sb.curl[tt][i][0] * curl_s[j][0] + sb.curl[tt][i][1] * curl_s[j][1] +
                                        sb.curl[tt][i][2] * curl_s[j][2];
-                    vr = fma(cij, sre, cpf * vr);
-                    vi = fma(cij, sim, cpf * vi);
+                    const double lr = vr, li = vi;
+                    vr = fma(cij, sre, fma(cpf, lr, -cpi * li));
+                    vi = fma(cij, sim, fma(cpf, li, cpi * lr));
                 }
                 // SKEW: the transposed pair's own block, else the same block
                 double wr = SKEW ? ure[i % (SKEW ? NT : 1)][j % (SKEW ? NS : 1)] : vr;

@@ -333,7 +333,9 @@ static cudaError_t launch_dp0(const RegParams &prm, const QuadRule &rule, int mi
 
 template <int ASM, int K, int NT, int NS, bool SYM>
 static void launch_p1_phase(const RegParams &prm, const QuadRule &rule, int phase_class, dim3 grid, cudaStream_t st) {
-    if (phase_class == 2)
+    if (phase_class == 3)  // complex wavenumber
+        regular_p1<ASM, K, NT, NS, 3, SYM><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+    else if (phase_class == 2)
         regular_p1<ASM, K, NT, NS, 2, SYM><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
     else if (phase_class == 1)
         regular_p1<ASM, K, NT, NS, 1, SYM><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
@@ -573,7 +575,7 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
                                  a->test.nsupport == a->trial.nsupport && a->test_grid.geom == a->trial_grid.geom &&
                                  a->test.normal_mult == a->trial.normal_mult && prm.ntest == prm.ntrial;
                a->nq == NQ6 && !a->overwrite && a->test.shapeset != BEMPPCUDA_SHAPE_RWG &&
-               a->trial.shapeset != BEMPPCUDA_SHAPE_RWG && a->params[1] == 0.0 &&
+               a->trial.shapeset != BEMPPCUDA_SHAPE_RWG &&
                ((a->assembly == BEMPPCUDA_ASM_SCALAR && a->kernel <= BEMPPCUDA_HELMHOLTZ_ADLP) ||
                 a->assembly == BEMPPCUDA_ASM_LAPLACE_HYP || a->assembly == BEMPPCUDA_ASM_HELM_HYP)) {
         // single layer / hypersingular on one space into a zeroed result: the pairs i < j add their
@@ -583,23 +585,25 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
                            (a->assembly != BEMPPCUDA_ASM_SCALAR || a->kernel == BEMPPCUDA_LAPLACE_SLP ||
                             a->kernel == BEMPPCUDA_HELMHOLTZ_SLP);
         prm.defer_transpose = defer ? 1 : 0;
+        // a complex wavenumber takes phase class 3 (no centroid factoring, exp(-Im k r) per point)
+        const int p1_phase = a->params[1] != 0.0 ? 3 : phase_class;
         if (mixed && p1_mixed) {
             if (a->assembly == BEMPPCUDA_ASM_HELM_HYP)
                 err = launch_p1_mixed<BEMPPCUDA_ASM_HELM_HYP>(prm, rule, phase_class, psym, st);
             else
                 err = launch_p1_mixed<BEMPPCUDA_ASM_SCALAR>(prm, rule, phase_class, psym, st);
         } else if (a->assembly == BEMPPCUDA_ASM_LAPLACE_HYP) {
-            err = launch_p1<BEMPPCUDA_ASM_LAPLACE_HYP, BEMPPCUDA_LAPLACE_SLP>(prm, rule, phase_class, psym, st);
+            err = launch_p1<BEMPPCUDA_ASM_LAPLACE_HYP, BEMPPCUDA_LAPLACE_SLP>(prm, rule, p1_phase, psym, st);
         } else if (a->assembly == BEMPPCUDA_ASM_HELM_HYP) {
-            err = launch_p1<BEMPPCUDA_ASM_HELM_HYP, BEMPPCUDA_HELMHOLTZ_SLP>(prm, rule, phase_class, psym, st);
+            err = launch_p1<BEMPPCUDA_ASM_HELM_HYP, BEMPPCUDA_HELMHOLTZ_SLP>(prm, rule, p1_phase, psym, st);
         } else {
             switch (a->kernel) {
-            case BEMPPCUDA_LAPLACE_SLP: err = launch_p1<0, BEMPPCUDA_LAPLACE_SLP>(prm, rule, phase_class, psym, st); break;
-            case BEMPPCUDA_LAPLACE_DLP: err = launch_p1<0, BEMPPCUDA_LAPLACE_DLP>(prm, rule, phase_class, psym, st); break;
-            case BEMPPCUDA_LAPLACE_ADLP: err = launch_p1<0, BEMPPCUDA_LAPLACE_ADLP>(prm, rule, phase_class, psym, st); break;
-            case BEMPPCUDA_HELMHOLTZ_SLP: err = launch_p1<0, BEMPPCUDA_HELMHOLTZ_SLP>(prm, rule, phase_class, psym, st); break;
-            case BEMPPCUDA_HELMHOLTZ_DLP: err = launch_p1<0, BEMPPCUDA_HELMHOLTZ_DLP>(prm, rule, phase_class, psym, st); break;
-            default: err = launch_p1<0, BEMPPCUDA_HELMHOLTZ_ADLP>(prm, rule, phase_class, psym, st); break;
+            case BEMPPCUDA_LAPLACE_SLP: err = launch_p1<0, BEMPPCUDA_LAPLACE_SLP>(prm, rule, p1_phase, psym, st); break;
+            case BEMPPCUDA_LAPLACE_DLP: err = launch_p1<0, BEMPPCUDA_LAPLACE_DLP>(prm, rule, p1_phase, psym, st); break;
+            case BEMPPCUDA_LAPLACE_ADLP: err = launch_p1<0, BEMPPCUDA_LAPLACE_ADLP>(prm, rule, p1_phase, psym, st); break;
+            case BEMPPCUDA_HELMHOLTZ_SLP: err = launch_p1<0, BEMPPCUDA_HELMHOLTZ_SLP>(prm, rule, p1_phase, psym, st); break;
+            case BEMPPCUDA_HELMHOLTZ_DLP: err = launch_p1<0, BEMPPCUDA_HELMHOLTZ_DLP>(prm, rule, p1_phase, psym, st); break;
+            default: err = launch_p1<0, BEMPPCUDA_HELMHOLTZ_ADLP>(prm, rule, p1_phase, psym, st); break;
             }
         }
         if (defer && err == cudaSuccess) err = launch_add_transpose(prm.result, a->test.ndofs, prm.ld, prm.is_complex, st);

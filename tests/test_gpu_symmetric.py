@@ -81,14 +81,18 @@ def test_symmetric_sweep_odd_size():
                                     ("laplace.hypersingular", None), ("helmholtz.hypersingular", 4.0),
                                     ("laplace.double_layer", None), ("laplace.adjoint_double_layer", None),
                                     ("helmholtz.double_layer", 2.0), ("helmholtz.double_layer", 4.0),
-                                    ("helmholtz.double_layer", 40.0), ("helmholtz.adjoint_double_layer", 4.0)])
+                                    ("helmholtz.double_layer", 40.0), ("helmholtz.adjoint_double_layer", 4.0),
+                                    ("helmholtz.single_layer", 3.0 + 0.5j), ("helmholtz.double_layer", 3.0 + 0.5j),
+                                    ("helmholtz.adjoint_double_layer", 3.0 + 0.5j),
+                                    ("helmholtz.hypersingular", 3.0 + 0.5j)])
 def test_p1_symmetric_sweep_matches_entrywise(path, k):
     """P1 operators: the symmetric sweep against per-pair evaluation.
 
     Single layer and hypersingular add each block at (i, j) and its transpose;
     the double and adjoint double layer form the transposed pair's own block
     from the other element's normal.  k = 2, 4, 40 reach the three phase
-    classes (|k| (R_i + R_j) <= 1/2, <= 1, reduced).
+    classes (|k| (R_i + R_j) <= 1/2, <= 1, reduced); k = 3 + 0.5i the complex
+    wavenumber class (exp(-Im k r) per point pair).
     """
     from bempp_cuda import operators
     from bempp_cuda.assembly import regular_into, singular_into_dense
