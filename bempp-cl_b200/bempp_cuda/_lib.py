@@ -203,6 +203,30 @@ class BatchArgs(_ct.Structure):
     ]
 
 
+class MatmatProblem(_ct.Structure):
+    _fields_ = [
+        ("a", _vp),
+        ("x", _vp),
+        ("y", _vp),
+        ("rows", _i64),
+        ("cols", _i64),
+        ("lda", _i64),
+        ("ldx", _i64),
+        ("ldy", _i64),
+    ]
+
+
+class MatmatArgs(_ct.Structure):
+    _fields_ = [
+        ("nproblems", _i32),
+        ("nrhs", _i32),
+        ("problems", _ct.POINTER(MatmatProblem)),
+        ("workspace", _vp),
+        ("workspace_bytes", _i64),
+        ("blocks", _i64),
+    ]
+
+
 class ShapeArgs(_ct.Structure):
     _fields_ = [
         ("grid", GridRec),
@@ -261,6 +285,9 @@ SIGNATURES = {
     "bemppcuda_batch_workspace_bytes": (_i64, [_i32]),
     "bemppcuda_batch_prepare": (_ct.c_int, [_ct.POINTER(BatchArgs), _vp]),
     "bemppcuda_batch_launch": (_ct.c_int, [_ct.POINTER(BatchArgs), _vp]),
+    "bemppcuda_matmat_workspace_bytes": (_i64, [_i32]),
+    "bemppcuda_matmat_prepare": (_ct.c_int, [_ct.POINTER(MatmatArgs), _vp]),
+    "bemppcuda_matmat_launch": (_ct.c_int, [_ct.POINTER(MatmatArgs), _vp]),
     "bemppcuda_shape_workspace_bytes": (_i64, [_i64]),
     "bemppcuda_farfield_matrix_dp0": (_ct.c_int, [_ct.POINTER(ShapeArgs), _vp]),
     "bemppcuda_plane_wave_dp0": (_ct.c_int, [_ct.POINTER(ShapeArgs), _vp]),

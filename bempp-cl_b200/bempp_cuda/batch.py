@@ -10,8 +10,8 @@ is 64 separate assemblies there.
 
 * ``launch()`` queues device work only (counter reset and two kernels) and can
   be captured in a CUDA graph: ``capture()`` records launch (plus, optionally,
-  the multi-right-hand-side products) into a ``torch.cuda.CUDAGraph`` and
-  ``replay()`` runs it.
+  the multi-right-hand-side products of all problems, one batched launch of
+  csrc/matmat.cu) into a ``torch.cuda.CUDAGraph`` and ``replay()`` runs it.
 * ``autotune()`` times the launch for candidate tile shapes (test rows per
   work item) and persistent grid sizes (CTAs per SM) and keeps the fastest;
   results are cached per (kernel, precision mix, work-size bucket) in
@@ -29,6 +29,7 @@ import torch as _torch
 from . import _lib
 from .assembly import regular_rule
 from .device import current_stream, device_grid, device_space, ptr, require_cuda, singular_rule_arrays
+from .matmat import BatchedProduct
 from .shapes import ellipsoid
 from .space import function_space
 
@@ -131,6 +132,8 @@ class BatchAssembler(object):
         a.workspace = ptr(self._workspace)
         a.workspace_bytes = nbytes
         self._graph = None
+        self._product = None
+        self._product_key = None
         self.prepare()
 
     @property
@@ -195,19 +198,29 @@ class BatchAssembler(object):
                 pass
         return shape, timings
 
-    def capture(self, rhs=None, products=None):
-        """Record launch() (and products[i] = outputs[i] @ rhs[i]) in a CUDA graph."""
-        self.launch()  # warm up outside capture
+    def step(self, rhs=None, products=None):
+        """launch(), then products[i] = outputs[i] @ rhs[i]: the work capture() records, issued eagerly.
+
+        The products of all problems are one batched launch (``matmat.BatchedProduct``);
+        its problem table is uploaded on the first call with these tensors.
+        """
+        self.launch()
         if rhs is not None:
-            for a, x, y in zip(self.outputs, rhs, products):
-                _torch.matmul(a, x, out=y)
+            key = tuple(t.data_ptr() for t in rhs) + tuple(t.data_ptr() for t in products)
+            if self._product is None or self._product_key != key:
+                if _torch.cuda.is_current_stream_capturing():
+                    raise RuntimeError("call step(rhs, products) once before capturing it")
+                self._product = BatchedProduct(self.outputs, rhs, products)
+                self._product_key = key
+            self._product.launch()
+
+    def capture(self, rhs=None, products=None):
+        """Record step(rhs, products) in a CUDA graph."""
+        self.step(rhs, products)  # warm up outside capture
         _torch.cuda.synchronize()
         graph = _torch.cuda.CUDAGraph()
         with _torch.cuda.graph(graph):
-            self.launch()
-            if rhs is not None:
-                for a, x, y in zip(self.outputs, rhs, products):
-                    _torch.matmul(a, x, out=y)
+            self.step(rhs, products)
         self._graph = graph
         return graph
 

@@ -441,14 +441,18 @@ static cudaError_t launch_rwg(const RegParams &prm, const QuadRule &rule, int ph
     dim3 grid((unsigned)((prm.ntrial + DP0_THREADS - 1) / DP0_THREADS),
               (unsigned)((prm.ntest + RWG_TCHUNK - 1) / RWG_TCHUNK));
     if (sym) {
-        if (phase_class == 2)
+        if (phase_class == 3)  // complex wavenumber
+            regular_rwg<ASM, 3, true><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+        else if (phase_class == 2)
             regular_rwg<ASM, 2, true><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
         else if (phase_class == 1)
             regular_rwg<ASM, 1, true><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
         else
             regular_rwg<ASM, 0, true><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
     } else {
-        if (phase_class == 2)
+        if (phase_class == 3)
+            regular_rwg<ASM, 3, false><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+        else if (phase_class == 2)
             regular_rwg<ASM, 2, false><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
         else if (phase_class == 1)
             regular_rwg<ASM, 1, false><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
@@ -558,7 +562,7 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
         default: bc_set_error("kernel %d not valid for boundary assembly", a->kernel); return BEMPPCUDA_ERR_INVALID;
         }
     } else if ((a->assembly == BEMPPCUDA_ASM_EFIE || a->assembly == BEMPPCUDA_ASM_MFIE) && a->nq == NQ6 &&
-               !a->overwrite && a->kernel == BEMPPCUDA_HELMHOLTZ_SLP && a->params[1] == 0.0 && a->params[0] != 0.0 &&
+               !a->overwrite && a->kernel == BEMPPCUDA_HELMHOLTZ_SLP && (a->params[0] != 0.0 || a->params[1] != 0.0) &&
                a->test.shapeset == BEMPPCUDA_SHAPE_RWG && a->trial.shapeset == BEMPPCUDA_SHAPE_RWG &&
                a->test.nshape == 3 && a->trial.nshape == 3) {
         // RWG and SNC share their dof maps; the caller passes the same arrays for both
@@ -566,10 +570,12 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
                           a->test.l2g == a->trial.l2g && a->test.mult == a->trial.mult &&
                           a->test.nsupport == a->trial.nsupport && a->test_grid.geom == a->trial_grid.geom &&
                           prm.ntest == prm.ntrial;
+        // a complex wavenumber takes phase class 3 (exp(-Im k r) per point pair)
+        const int rwg_phase = a->params[1] != 0.0 ? 3 : phase_class;
         if (a->assembly == BEMPPCUDA_ASM_EFIE)
-            err = launch_rwg<BEMPPCUDA_ASM_EFIE>(prm, rule, phase_class, rsym, st);
+            err = launch_rwg<BEMPPCUDA_ASM_EFIE>(prm, rule, rwg_phase, rsym, st);
         else
-            err = launch_rwg<BEMPPCUDA_ASM_MFIE>(prm, rule, phase_class, rsym, st);
+            err = launch_rwg<BEMPPCUDA_ASM_MFIE>(prm, rule, rwg_phase, rsym, st);
     } else if (const bool psym = !a->no_symmetry && a->grids_identical && a->test.support == a->trial.support &&
                                  a->test.l2g == a->trial.l2g && a->test.mult == a->trial.mult &&
                                  a->test.nsupport == a->trial.nsupport && a->test_grid.geom == a->trial_grid.geom &&

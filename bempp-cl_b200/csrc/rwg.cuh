@@ -1,5 +1,5 @@
 // Regular pairs of the Maxwell electric and magnetic field operators on RWG /
-// SNC spaces, 6-point rule, real wavenumber: the kernels of
+// SNC spaces, 6-point rule: the kernels of
 // numba_kernels.py:1853-1969 (maxwell_efield_regular_assembler) and
 // :2151-2280 (maxwell_mfield_regular_assembler).
 //
@@ -22,7 +22,10 @@
 //          B(p) = sum_q H (w_s(q) x d),  C(p) = sum_q H d,
 //          MFIE_ij = PB - c_sj . PC - c_ti . QB + c_ti . (c_sj x QC),
 //        PB = sum_p w_t(p) . B(p), PC = sum_p C(p) x w_t(p), QB = sum_p B(p), QC = sum_p C(p).
-// exp(ikr) is factored about the centroid distance as in the DP0 / P1 kernels.
+// exp(ikr) is factored about the centroid distance as in the DP0 / P1 kernels
+// (phase classes 1, 2).  Class 3 is a complex wavenumber k = kr + i ki:
+// exp(ikr) = exp(i kr r) exp(-ki r) per point pair, (ikr - 1) = -(1 + ki r) + i kr r,
+// and -ik, -4 / (ik) = 4i conj(k) / |k|^2 as complex factors per element pair.
 // SYM (test and trial spaces with the same dof maps on one grid, as RWG and
 // SNC are): both operators are symmetric under exchanging the pair's
 // elements (G is symmetric; for MFIE both d and the cross product change
@@ -52,7 +55,8 @@ __device__ __forceinline__ double dot3(const double a[3], const double b[3]) {
 template <int ASM, int PHC, bool SYM>
 __global__ void __launch_bounds__(DP0_THREADS) regular_rwg(RegParams prm, QuadRule rule) {
     constexpr bool EFIE = ASM == BEMPPCUDA_ASM_EFIE;
-    constexpr bool PH = PHC > 0;
+    constexpr bool PH = PHC == 1 || PHC == 2;
+    constexpr bool CK = PHC == 3;
     __shared__ TestBlockRWG sb;
 
     const int64_t t0 = (int64_t)blockIdx.y * RWG_TCHUNK;
@@ -101,7 +105,7 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_rwg(RegParams prm, QuadRu
         scol[j] = prm.sl2g[s * 3 + j];
         sfac[j] = prm.smult[s * 3 + j] * edge_length(prm.sg, prm.sne, s, j);
     }
-    const double kr = prm.p[0];
+    const double kr = prm.p[0], ki = CK ? prm.p[1] : 0.0;
 
     for (int tt = 0; tt < tcount; ++tt) {
         if (SYM && t0 + tt >= si) break;  // rows increase with tt
@@ -142,6 +146,11 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_rwg(RegParams prm, QuadRu
                     sincos_small64(fma(kr, r, -krc), &sn, &cs);
                 else
                     sincos_cw64(kr * r, &sn, &cs);
+                if (CK) {
+                    const double am = exp(-ki * r);
+                    sn *= am;
+                    cs *= am;
+                }
                 if (EFIE) {
                     // w_q G 4 pi (the phase exp(ik r_c) and 1 / (4 pi) are applied per pair)
                     const double gr = cs * rinv, gi = sn * rinv;
@@ -155,7 +164,15 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_rwg(RegParams prm, QuadRu
                     // w_q G (ikr - 1) / r^2 times 4 pi: (cs + i sn)(-1 + i k r) w_q / r^3
                     const double f = rule.w[q] * (rinv * rinv * rinv);
                     const double kq = kr * r;
-                    const double hr = -fma(kq, sn, cs) * f, hi = fma(kq, cs, -sn) * f;
+                    double hr, hi;
+                    if (CK) {
+                        const double a = fma(ki, r, 1.0);  // -(ikr - 1) real part: 1 + ki r
+                        hr = -fma(kq, sn, a * cs) * f;
+                        hi = fma(kq, cs, -a * sn) * f;
+                    } else {
+                        hr = -fma(kq, sn, cs) * f;
+                        hi = fma(kq, cs, -sn) * f;
+                    }
                     double wxd[3];
                     wxd[0] = fma(ws[q][1], d[2], -ws[q][2] * d[1]);
                     wxd[1] = fma(ws[q][2], d[0], -ws[q][0] * d[2]);
@@ -221,6 +238,13 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_rwg(RegParams prm, QuadRu
             }
             // -ik E1 - 4 / (ik) M11, 1 / (ik) = -i / k
             const double m11r = mre[0][0], m11i = mim[0][0];
+            // complex k: -4 / (ik) M11 = 4 (ki + i kr) / |k|^2 M11, one value per pair
+            double c1r = 0.0, c1i = 0.0;
+            if (CK) {
+                const double g4 = 4.0 / fma(kr, kr, ki * ki);
+                c1r = g4 * fma(ki, m11r, -kr * m11i);
+                c1i = g4 * fma(kr, m11r, ki * m11i);
+            }
 #pragma unroll
             for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -240,8 +264,14 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_rwg(RegParams prm, QuadRu
                         ei = fma(cc, m11i, ei);
                     }
                     // -ik (er + i ei) = k ei - i k er;  -(4 / (ik)) M11 = (4i / k) M11 = -4 m11i / k + i 4 m11r / k
-                    blk_re[i][j] = fma(kr, ei, -4.0 * m11i / kr);
-                    blk_im[i][j] = fma(-kr, er, 4.0 * m11r / kr);
+                    if (CK) {
+                        // -ik (er + i ei) = (kr ei + ki er) + i (ki ei - kr er)
+                        blk_re[i][j] = fma(kr, ei, fma(ki, er, c1r));
+                        blk_im[i][j] = fma(ki, ei, fma(-kr, er, c1i));
+                    } else {
+                        blk_re[i][j] = fma(kr, ei, -4.0 * m11i / kr);
+                        blk_im[i][j] = fma(-kr, er, 4.0 * m11r / kr);
+                    }
                 }
         } else {
 #pragma unroll

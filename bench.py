@@ -527,12 +527,29 @@ def batch_measure(args, torch, world, rank, dist, count=64, levels=(3, 4, 5)):
         for _ in range(args.warmup):
             ba.replay()
         launch_ms = events_ms(ba.launch, args.steps)
+        # assembly + 8-RHS products: issued eagerly, then replayed from the graph
+        eager_ms = events_ms(lambda: ba.step(rhs, prods), args.steps)
         graph_ms = events_ms(ba.replay, args.steps)
         entry = {"rows_per_item": shape[0], "ctas_per_sm": shape[1], "autotune_s": tune_s,
-                 "shapes_timed": len(timings), "launch_ms": launch_ms, "graph_ms": graph_ms,
+                 "shapes_timed": len(timings), "launch_ms": launch_ms,
                  "entries_per_s": entries_all / (launch_ms * 1e-3),
-                 "graph_entries_per_s": entries_all / (graph_ms * 1e-3)}
+                 "step_with_products": {"eager_ms": eager_ms, "graph_ms": graph_ms,
+                                        "graph_speedup": eager_ms / graph_ms,
+                                        "products_ms": graph_ms - launch_ms,
+                                        "entries_per_s": entries_all / (graph_ms * 1e-3)}}
         if prec == "fp64":
+            # the batched 8-RHS product kernel alone against one library GEMM per problem
+            prod_ms = events_ms(ba._product.launch, args.steps)
+            torch_ms = events_ms(lambda: [torch.matmul(a, x, out=y) for a, x, y in zip(ba.outputs, rhs, prods)],
+                                 args.steps)
+            nbytes = sum(16 * (o.shape[0] * o.shape[1] + (o.shape[0] + o.shape[1]) * x.shape[1])
+                         for o, x in zip(ba.outputs, rhs))
+            peak, source = hbm_peak()
+            entry["products"] = {"kernel": "matmat_c128<8> (one launch, all problems)", "kernel_ms": prod_ms,
+                                 "torch_matmul_ms": torch_ms, "bytes": nbytes,
+                                 "gbs": nbytes / (prod_ms * 1e-3) / 1e9,
+                                 "frac": nbytes / (prod_ms * 1e-3) / 1e9 / peak, "peak_gbs": peak,
+                                 "peak_source": source}
             outputs64 = [o.clone() for o in ba.outputs]
         else:
             errs = [(torch.linalg.norm(a - b) / torch.linalg.norm(b)).item() for a, b in zip(ba.outputs, outputs64)]

@@ -242,6 +242,27 @@ typedef struct {
     int64_t workspace_bytes;
 } bemppcuda_batch_args;
 
+/* Batched multi-right-hand-side products Y_p = A_p X_p of dense complex128
+   operators (interleaved re / im, row-major), one launch for the whole list.
+   Replaces DenseDiscreteBoundaryOperator._matmat
+   (api/assembly/discrete_boundary_operator.py:192-198, a host ndarray.dot per
+   operator) for operators that stay on the device. */
+typedef struct {
+    const void *a;  /* complex128 (rows, cols), row stride lda elements; 16-byte aligned */
+    const void *x;  /* complex128 (cols, nrhs), row stride ldx */
+    void *y;        /* complex128 (rows, nrhs), row stride ldy; overwritten */
+    int64_t rows, cols, lda, ldx, ldy;
+} bemppcuda_matmat_problem;
+
+typedef struct {
+    int32_t nproblems;
+    int32_t nrhs;                             /* 1..8, the same for every problem */
+    const bemppcuda_matmat_problem *problems; /* HOST array of nproblems entries */
+    void *workspace;                          /* bemppcuda_matmat_workspace_bytes(nproblems) bytes */
+    int64_t workspace_bytes;
+    int64_t blocks;                           /* written by bemppcuda_matmat_prepare */
+} bemppcuda_matmat_args;
+
 int bemppcuda_version(void);
 int bemppcuda_last_error(char *buffer, int64_t length);
 
@@ -283,6 +304,16 @@ int bemppcuda_batch_prepare(const bemppcuda_batch_args *args, void *stream);
    (a memset and two launches), so it can be captured in a CUDA graph once
    bemppcuda_batch_prepare has run. */
 int bemppcuda_batch_launch(const bemppcuda_batch_args *args, void *stream);
+
+int64_t bemppcuda_matmat_workspace_bytes(int32_t nproblems);
+/* Check the list, upload it into the workspace (host-to-device copy, then a
+   stream synchronize) and set args->blocks; call again whenever it changes. */
+int bemppcuda_matmat_prepare(bemppcuda_matmat_args *args, void *stream);
+/* One kernel launch over every problem's rows (device work only, so it can be
+   captured in a CUDA graph once bemppcuda_matmat_prepare has run).  FP64
+   sums; the order differs from a BLAS product's, so results agree with it to
+   rounding, not bit for bit. */
+int bemppcuda_matmat_launch(const bemppcuda_matmat_args *args, void *stream);
 
 /* Measurement utility, no reference counterpart: launches `blocks` x 256
    threads that each run 32 independent FMAs per iteration in FP64

@@ -130,12 +130,12 @@ def test_p1_symmetric_sweep_matches_entrywise(path, k):
 
 
 @pytest.mark.parametrize("name", ["electric_field", "magnetic_field"])
-@pytest.mark.parametrize("k", [1.0, 3.0, 20.0])
+@pytest.mark.parametrize("k", [1.0, 3.0, 20.0, 3.0 + 0.5j, 1.0 + 2.0j])
 def test_maxwell_rwg_kernel_against_oracle(oracle, name, k):
     """Maxwell EFIE / MFIE (RWG domain, SNC dual) through the RWG kernel: the
     symmetric sweep (RWG and SNC share their dof maps) and the per-pair sweep
     against the oracle.  k = 1, 3, 20 on a 512-element ellipsoid reach the
-    three phase classes."""
+    three phase classes; 3 + 0.5i and 1 + 2i the complex wavenumber class."""
     from cases import oracle_dense
 
     from bempp_cuda import operators
