@@ -1,5 +1,5 @@
 // Regular pairs of scalar operators on linear (P1 / DP1) and mixed P0 / P1
-// spaces, 6-point rule, real wavenumber: the kernels of numba_kernels.py:980-1074
+// spaces, 6-point rule: the kernels of numba_kernels.py:980-1074
 // (default_scalar_regular_kernel) and the hypersingular ones of :1078-1467.
 //
 // One thread per trial element, 32 test elements staged in shared memory (as
@@ -15,7 +15,10 @@
 // exp(i kr r) from the reduced sine / cosine times exp(-ki r), the double-layer
 // factor (ikr - 1) / r = (-1/r - ki) + i kr, and -k^2 complex in the
 // hypersingular operator.  The symmetric and skew sweeps hold for complex k
-// (G(x, y) = G(y, x)).
+// (G(x, y) = G(y, x)).  Modified Helmholtz, G = exp(-w r) / (4 pi r) with
+// w = p[0] > 0, is real: the Laplace kernels times exp(-w r) (single layer) or
+// exp(-w r) (1 + w r) (double layers), and +w^2 (n_t . n_s) in the
+// hypersingular operator.
 // The NT x NS block is added to the matrix with FP64 atomics (l2g, multipliers).
 // SYM (the same space on both sides): only pairs i < j (support positions) are
 // evaluated and each gives the blocks at (i, j) and (j, i).  Single layer and
@@ -56,11 +59,13 @@ struct TestBlockP1 {
 
 template <int ASM, int K, int NT, int NS, int PHC, bool SYM>
 __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegParams prm, QuadRule rule) {
-    constexpr bool HYP = (ASM == BEMPPCUDA_ASM_LAPLACE_HYP || ASM == BEMPPCUDA_ASM_HELM_HYP);
+    constexpr bool HYP = (ASM == BEMPPCUDA_ASM_LAPLACE_HYP || ASM == BEMPPCUDA_ASM_HELM_HYP ||
+                          ASM == BEMPPCUDA_ASM_MODHELM_HYP);
     constexpr bool HELM = (K == BEMPPCUDA_HELMHOLTZ_SLP || K == BEMPPCUDA_HELMHOLTZ_DLP ||
                            K == BEMPPCUDA_HELMHOLTZ_ADLP);
-    constexpr bool DL = (K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_HELMHOLTZ_DLP);
-    constexpr bool AD = (K == BEMPPCUDA_LAPLACE_ADLP || K == BEMPPCUDA_HELMHOLTZ_ADLP);
+    constexpr bool MH = (K == BEMPPCUDA_MODHELM_SLP || K == BEMPPCUDA_MODHELM_DLP || K == BEMPPCUDA_MODHELM_ADLP);
+    constexpr bool DL = (K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_HELMHOLTZ_DLP || K == BEMPPCUDA_MODHELM_DLP);
+    constexpr bool AD = (K == BEMPPCUDA_LAPLACE_ADLP || K == BEMPPCUDA_HELMHOLTZ_ADLP || K == BEMPPCUDA_MODHELM_ADLP);
     constexpr bool PH = HELM && (PHC == 1 || PHC == 2);
     constexpr bool CK = HELM && PHC == 3;
     static_assert(!SYM || NT == NS, "the symmetric sweep needs one space on both sides");
@@ -178,6 +183,10 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
                     double hre, him;  // double layer of trial normal n: (dot with n) (hre + i him)
                     if (!HELM) {
                         hre = -rinv * rinv * rinv;
+                        if (MH) {
+                            const double r = r2 * rinv;
+                            hre *= exp(-kr * r) * fma(kr, r, 1.0);
+                        }
                         him = 0.0;
                     } else {
                         const double r = r2 * rinv;
@@ -206,10 +215,16 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
                 } else if (!HELM) {
                     if (K == BEMPPCUDA_LAPLACE_SLP) {
                         kre = rinv;
+                    } else if (K == BEMPPCUDA_MODHELM_SLP) {
+                        kre = exp(-kr * (r2 * rinv)) * rinv;
                     } else {
                         const double dot = DL ? ynv[q] + xn
                                               : fma(d2, sb.n[tt][2], fma(d1, sb.n[tt][1], d0 * sb.n[tt][0]));
                         kre = (DL ? -dot : dot) * rinv * rinv * rinv;
+                        if (MH) {
+                            const double r = r2 * rinv;
+                            kre *= exp(-kr * r) * fma(kr, r, 1.0);
+                        }
                     }
                 } else {
                     const double r = r2 * rinv;
@@ -272,12 +287,14 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
                 }
         }
         const double scale = BC_INV_4PI * sb.ie[tt] * gs.ie;
-        // hypersingular: -k^2 (n_t . n_s), complex for a complex wavenumber
+        // hypersingular: -k^2 (n_t . n_s), complex for a complex wavenumber; +w^2 (n_t . n_s) modified
         double cpf = 0.0, cpi = 0.0;
         if (HYP && ASM == BEMPPCUDA_ASM_HELM_HYP) {
             const double nn = sb.n[tt][0] * gs.n[0] + sb.n[tt][1] * gs.n[1] + sb.n[tt][2] * gs.n[2];
             cpf = -(kr * kr - ki * ki) * nn;
             cpi = -2.0 * kr * ki * nn;
+        } else if (HYP && ASM == BEMPPCUDA_ASM_MODHELM_HYP) {
+            cpf = kr * kr * (sb.n[tt][0] * gs.n[0] + sb.n[tt][1] * gs.n[1] + sb.n[tt][2] * gs.n[2]);
         }
 #pragma unroll
         for (int i = 0; i < NT; ++i) {

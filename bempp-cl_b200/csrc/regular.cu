@@ -333,14 +333,19 @@ static cudaError_t launch_dp0(const RegParams &prm, const QuadRule &rule, int mi
 
 template <int ASM, int K, int NT, int NS, bool SYM>
 static void launch_p1_phase(const RegParams &prm, const QuadRule &rule, int phase_class, dim3 grid, cudaStream_t st) {
-    if (phase_class == 3)  // complex wavenumber
-        regular_p1<ASM, K, NT, NS, 3, SYM><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
-    else if (phase_class == 2)
-        regular_p1<ASM, K, NT, NS, 2, SYM><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
-    else if (phase_class == 1)
-        regular_p1<ASM, K, NT, NS, 1, SYM><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
-    else
+    // the phase classes only concern exp(ikr): one instance for Laplace and modified Helmholtz
+    if constexpr (K != BEMPPCUDA_HELMHOLTZ_SLP && K != BEMPPCUDA_HELMHOLTZ_DLP && K != BEMPPCUDA_HELMHOLTZ_ADLP) {
         regular_p1<ASM, K, NT, NS, 0, SYM><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+    } else {
+        if (phase_class == 3)  // complex wavenumber
+            regular_p1<ASM, K, NT, NS, 3, SYM><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+        else if (phase_class == 2)
+            regular_p1<ASM, K, NT, NS, 2, SYM><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+        else if (phase_class == 1)
+            regular_p1<ASM, K, NT, NS, 1, SYM><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+        else
+            regular_p1<ASM, K, NT, NS, 0, SYM><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+    }
 }
 
 template <int ASM, int K, int NT, int NS>
@@ -359,7 +364,7 @@ static void launch_p1_shapes(const RegParams &prm, const QuadRule &rule, int pha
 }
 
 // Scalar and hypersingular operators on P1 / DP1 / P0 spaces with the 6-point
-// rule and a real wavenumber (p1.cuh).
+// rule (p1.cuh).
 template <int ASM, int K>
 static cudaError_t launch_p1(const RegParams &prm, const QuadRule &rule, int phase_class, bool sym, cudaStream_t st) {
     dim3 grid((unsigned)((prm.ntrial + DP0_THREADS - 1) / DP0_THREADS),
@@ -582,14 +587,15 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
                                  a->test.normal_mult == a->trial.normal_mult && prm.ntest == prm.ntrial;
                a->nq == NQ6 && !a->overwrite && a->test.shapeset != BEMPPCUDA_SHAPE_RWG &&
                a->trial.shapeset != BEMPPCUDA_SHAPE_RWG &&
-               ((a->assembly == BEMPPCUDA_ASM_SCALAR && a->kernel <= BEMPPCUDA_HELMHOLTZ_ADLP) ||
-                a->assembly == BEMPPCUDA_ASM_LAPLACE_HYP || a->assembly == BEMPPCUDA_ASM_HELM_HYP)) {
+               ((a->assembly == BEMPPCUDA_ASM_SCALAR && a->kernel <= BEMPPCUDA_MODHELM_ADLP) ||
+                a->assembly == BEMPPCUDA_ASM_LAPLACE_HYP || a->assembly == BEMPPCUDA_ASM_HELM_HYP ||
+                a->assembly == BEMPPCUDA_ASM_MODHELM_HYP)) {
         // single layer / hypersingular on one space into a zeroed result: the pairs i < j add their
         // blocks U, then A = U + U^T (the regular diagonal is zero), half the global atomics
         const bool defer = psym && a->result_is_zero && a->test.nshape == a->trial.nshape &&
                            a->test.ndofs == a->trial.ndofs && a->test.ndofs <= 32 * 65535LL &&
                            (a->assembly != BEMPPCUDA_ASM_SCALAR || a->kernel == BEMPPCUDA_LAPLACE_SLP ||
-                            a->kernel == BEMPPCUDA_HELMHOLTZ_SLP);
+                            a->kernel == BEMPPCUDA_HELMHOLTZ_SLP || a->kernel == BEMPPCUDA_MODHELM_SLP);
         prm.defer_transpose = defer ? 1 : 0;
         // a complex wavenumber takes phase class 3 (no centroid factoring, exp(-Im k r) per point)
         const int p1_phase = a->params[1] != 0.0 ? 3 : phase_class;
@@ -602,6 +608,8 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
             err = launch_p1<BEMPPCUDA_ASM_LAPLACE_HYP, BEMPPCUDA_LAPLACE_SLP>(prm, rule, p1_phase, psym, st);
         } else if (a->assembly == BEMPPCUDA_ASM_HELM_HYP) {
             err = launch_p1<BEMPPCUDA_ASM_HELM_HYP, BEMPPCUDA_HELMHOLTZ_SLP>(prm, rule, p1_phase, psym, st);
+        } else if (a->assembly == BEMPPCUDA_ASM_MODHELM_HYP) {
+            err = launch_p1<BEMPPCUDA_ASM_MODHELM_HYP, BEMPPCUDA_MODHELM_SLP>(prm, rule, p1_phase, psym, st);
         } else {
             switch (a->kernel) {
             case BEMPPCUDA_LAPLACE_SLP: err = launch_p1<0, BEMPPCUDA_LAPLACE_SLP>(prm, rule, p1_phase, psym, st); break;
@@ -609,7 +617,10 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
             case BEMPPCUDA_LAPLACE_ADLP: err = launch_p1<0, BEMPPCUDA_LAPLACE_ADLP>(prm, rule, p1_phase, psym, st); break;
             case BEMPPCUDA_HELMHOLTZ_SLP: err = launch_p1<0, BEMPPCUDA_HELMHOLTZ_SLP>(prm, rule, p1_phase, psym, st); break;
             case BEMPPCUDA_HELMHOLTZ_DLP: err = launch_p1<0, BEMPPCUDA_HELMHOLTZ_DLP>(prm, rule, p1_phase, psym, st); break;
-            default: err = launch_p1<0, BEMPPCUDA_HELMHOLTZ_ADLP>(prm, rule, p1_phase, psym, st); break;
+            case BEMPPCUDA_HELMHOLTZ_ADLP: err = launch_p1<0, BEMPPCUDA_HELMHOLTZ_ADLP>(prm, rule, p1_phase, psym, st); break;
+            case BEMPPCUDA_MODHELM_SLP: err = launch_p1<0, BEMPPCUDA_MODHELM_SLP>(prm, rule, p1_phase, psym, st); break;
+            case BEMPPCUDA_MODHELM_DLP: err = launch_p1<0, BEMPPCUDA_MODHELM_DLP>(prm, rule, p1_phase, psym, st); break;
+            default: err = launch_p1<0, BEMPPCUDA_MODHELM_ADLP>(prm, rule, p1_phase, psym, st); break;
             }
         }
         if (defer && err == cudaSuccess) err = launch_add_transpose(prm.result, a->test.ndofs, prm.ld, prm.is_complex, st);

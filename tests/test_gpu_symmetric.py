@@ -159,6 +159,34 @@ def test_maxwell_rwg_kernel_against_oracle(oracle, name, k):
         assert np.linalg.norm(got - ref) <= 1e-12 * np.linalg.norm(ref), (name, k, sym)
 
 
+@pytest.mark.parametrize("name", ["single_layer", "double_layer", "adjoint_double_layer", "hypersingular"])
+@pytest.mark.parametrize("omega", [1.5, 6.0])
+def test_modified_helmholtz_p1_kernel_against_oracle(oracle, name, omega):
+    """Modified Helmholtz (real kernel exp(-w r) / (4 pi r)) on P1 through regular_p1: the symmetric / skew
+    sweep, its deferred transpose and the per-pair sweep against the oracle."""
+    from cases import oracle_dense
+
+    from bempp_cuda import operators
+    from bempp_cuda.assembly import regular_into, singular_into_dense
+    from bempp_cuda.operators import Parameters
+    from bempp_cuda.shapes import ellipsoid
+    from bempp_cuda.space import function_space
+
+    grid = ellipsoid(3, 1.1, 0.9, 1.0)
+    sp = function_space(grid, "P", 1)
+    op = getattr(operators.boundary.modified_helmholtz, name)(sp, sp, sp, omega)
+    ref = oracle_dense(oracle, op, sp, sp)
+    d = op.descriptor
+    n = sp.global_dof_count
+    assert not d.is_complex
+    for sym, zero in ((True, False), (False, False), (True, True)):
+        a = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+        regular_into(a, d, sp, sp, Parameters(), symmetric=sym, result_is_zero=zero)
+        singular_into_dense(a, d, sp, sp, Parameters())
+        got = a.cpu().numpy()
+        assert np.linalg.norm(got - ref) <= 1e-12 * np.linalg.norm(ref), (name, omega, sym, zero)
+
+
 @pytest.mark.parametrize("kernel,options", KERNELS)
 def test_singular_vertex_pairs_mirrored(kernel, options):
     """DP0 singular pass: each vertex-adjacent pair evaluated once for both orders = every ordered pair."""
