@@ -39,12 +39,16 @@ struct TestBlock64s {
     int v[DP0_TCHUNK][3];
 };
 
-// FP64, real wavenumber.  PHC as in regular_dp0_fp64_tile.
+// FP64.  PHC 0-2 as in regular_dp0_fp64_tile (real wavenumber); PHC 3 is a complex wavenumber
+// k = kr + i ki: exp(i kr r) from the reduced sine / cosine times exp(-ki r) per point pair and
+// (ikr - 1) / r = -(1/r + ki) + i kr in the double layer (no centroid factoring: the amplitude
+// varies over the pair).  G(x, y) = G(y, x) for complex k too, so the sweep is unchanged.
 template <int K, int PHC>
 __device__ __forceinline__ void regular_dp0_fp64_sym_tile(const RegParams &prm, const QuadRule &rule,
                                                         int64_t tile_x, int64_t t0, int rows, TestBlock64s &sb) {
     using ST = SymTraits<K>;
-    constexpr bool PH = PHC > 0 && ST::helm;
+    constexpr bool PH = (PHC == 1 || PHC == 2) && ST::helm;
+    constexpr bool CK = PHC == 3 && ST::helm;
     const int tcount = (int)min((int64_t)rows, prm.ntest - t0);
     for (int idx = threadIdx.x; idx < tcount; idx += blockDim.x) {
         const int64_t t = prm.tsup[t0 + idx];
@@ -82,7 +86,7 @@ __device__ __forceinline__ void regular_dp0_fp64_sym_tile(const RegParams &prm, 
     double y[NQ6][3];
 #pragma unroll
     for (int q = 0; q < NQ6; ++q) to_global(gs, rule.x[q], rule.y[q], y[q]);
-    const double kr = prm.p[0], etar = prm.p[2], etai = prm.p[3];
+    const double kr = prm.p[0], ki = CK ? prm.p[1] : 0.0, etar = prm.p[2], etai = prm.p[3];
 
     for (int tt = 0; tt < tcount; ++tt) {
         const int64_t row = t0 + tt;
@@ -134,14 +138,19 @@ __device__ __forceinline__ void regular_dp0_fp64_sym_tile(const RegParams &prm, 
                             sincos_small64(kr * (r - rc), &sn, &cs);
                         else
                             sincos_cw64(kr * r, &sn, &cs);
+                        if (CK) {
+                            const double am = exp(-ki * r);
+                            sn *= am;
+                            cs *= am;
+                        }
                         if (ST::slp_part) {
                             pr = fma(f, cs, pr);
                             pi = fma(f, sn, pi);
                         }
                         if (ST::dlp_part) {
                             // (ikr - 1) e^{ikr} / r^3: -h1 + i h2 per unit f (dot) / r
-                            const double fr = f * rinv;
-                            const double h1 = fma(rinv, cs, kr * sn), h2 = fma(kr, cs, -rinv * sn);
+                            const double fr = f * rinv, rk = CK ? rinv + ki : rinv;
+                            const double h1 = fma(rk, cs, kr * sn), h2 = fma(kr, cs, -rk * sn);
                             const double gt = fr * ynt[q];
                             ur = fma(fr, h1, ur);
                             ui = fma(fr, h2, ui);

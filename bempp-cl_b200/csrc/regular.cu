@@ -266,9 +266,12 @@ static cudaError_t launch_dp0(const RegParams &prm, const QuadRule &rule, int mi
                               int64_t row0, int64_t row1, cudaStream_t st) {
     dim3 grid((unsigned)((prm.ntrial + DP0_THREADS - 1) / DP0_THREADS), (unsigned)((prm.ntest + DP0_TCHUNK - 1) / DP0_TCHUNK));
     if constexpr (SymTraits<K>::supported) {
-        // same DP0 space on both sides, real wavenumber (k > 0 for the scaled mixed path)
-        const bool real_k = !KernelTraits<K>::helm || (prm.p[1] == 0.0 && (!mixed || prm.p[0] > 0.0));
-        if (sym && real_k) {
+        // same DP0 space on both sides; the mixed tiles need a real wavenumber k > 0 (scaled units),
+        // the FP64 tiles take a complex one as phase class 3
+        const bool helm = KernelTraits<K>::helm;
+        const bool ck_sym = helm && prm.p[1] != 0.0;
+        const bool sweep_ok = !helm || (mixed ? (prm.p[1] == 0.0 && prm.p[0] > 0.0) : true);
+        if (sym && sweep_ok) {
             // rows per tile: 32, or 16 / 8 when 32-row tiles would leave the GPU under four waves of
             // working CTAs (about half the tiles lie below the diagonal and exit; 3 CTAs per SM)
             int tile_rows = DP0_TCHUNK;
@@ -284,7 +287,9 @@ static cudaError_t launch_dp0(const RegParams &prm, const QuadRule &rule, int mi
                 else
                     regular_dp0_mixed_sym<K, 0><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
             } else {
-                if (phase_class == 2)
+                if (ck_sym)
+                    regular_dp0_fp64_sym<K, 3><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
+                else if (phase_class == 2)
                     regular_dp0_fp64_sym<K, 2><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
                 else if (phase_class == 1)
                     regular_dp0_fp64_sym<K, 1><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
@@ -545,7 +550,7 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
     const bool sym_kernel = laplace || a->kernel == BEMPPCUDA_HELMHOLTZ_SLP || a->kernel == BEMPPCUDA_HELMHOLTZ_DLP ||
                             a->kernel == BEMPPCUDA_HELMHOLTZ_ADLP || a->kernel == BEMPPCUDA_HELMHOLTZ_COMBINED;
     const bool sym_ok = sym && sym_kernel &&
-                        (laplace || (a->params[1] == 0.0 && (a->precision != BEMPPCUDA_MIXED || a->params[0] > 0.0)));
+                        (laplace || a->precision != BEMPPCUDA_MIXED || (a->params[1] == 0.0 && a->params[0] > 0.0));
     if (ranged && (!sym_ok || a->row_begin < 0 || a->row_end > prm.ntest || a->row_begin >= a->row_end)) {
         bc_set_error("row range [%lld, %lld) needs the symmetric sweep and 0 <= begin < end <= %lld rows",
                      (long long)a->row_begin, (long long)a->row_end, (long long)prm.ntest);

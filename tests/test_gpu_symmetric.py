@@ -23,6 +23,11 @@ KERNELS = [
     ("helmholtz_adjoint_double_layer", [4.0, 0.0]),
     ("helmholtz_combined_field", [7.0, 0.0, 0.0, -7.0]),
     ("helmholtz_combined_field", [40.0, 0.0, 1.5, -40.0]),  # |k| (R_i + R_j) > 1: reduced phase
+    # complex wavenumbers: the FP64 sweep as phase class 3 (the mixed path runs per pair)
+    ("helmholtz_single_layer", [4.0, 0.7]),
+    ("helmholtz_double_layer", [4.0, 0.7]),
+    ("helmholtz_adjoint_double_layer", [4.0, 0.7]),
+    ("helmholtz_combined_field", [7.0, 0.5, 0.0, -7.0]),
 ]
 
 
@@ -155,6 +160,33 @@ def test_maxwell_rwg_kernel_against_oracle(oracle, name, k):
         a = torch.zeros((n, n), dtype=torch.complex128, device="cuda")
         regular_into(a, d, rwg, snc, Parameters(), symmetric=sym)
         singular_into_dense(a, d, rwg, snc, Parameters())
+        got = a.cpu().numpy()
+        assert np.linalg.norm(got - ref) <= 1e-12 * np.linalg.norm(ref), (name, k, sym)
+
+
+@pytest.mark.parametrize("name", ["single_layer", "double_layer", "adjoint_double_layer"])
+@pytest.mark.parametrize("k", [3.0 + 0.5j, 1.0 + 2.0j])
+def test_dp0_complex_wavenumber_against_oracle(oracle, name, k):
+    """DP0 Helmholtz operators with a complex wavenumber: symmetric sweep and per-pair evaluation against the
+    oracle."""
+    from cases import oracle_dense
+
+    from bempp_cuda import operators
+    from bempp_cuda.assembly import regular_into, singular_into_dense
+    from bempp_cuda.operators import Parameters
+    from bempp_cuda.shapes import ellipsoid
+    from bempp_cuda.space import function_space
+
+    grid = ellipsoid(3, 1.1, 0.9, 1.0)
+    sp = function_space(grid, "DP", 0)
+    op = getattr(operators.boundary.helmholtz, name)(sp, sp, sp, k)
+    ref = oracle_dense(oracle, op, sp, sp)
+    d = op.descriptor
+    n = sp.global_dof_count
+    for sym in (True, False):
+        a = torch.zeros((n, n), dtype=torch.complex128, device="cuda")
+        regular_into(a, d, sp, sp, Parameters(), symmetric=sym)
+        singular_into_dense(a, d, sp, sp, Parameters())
         got = a.cpu().numpy()
         assert np.linalg.norm(got - ref) <= 1e-12 * np.linalg.norm(ref), (name, k, sym)
 
