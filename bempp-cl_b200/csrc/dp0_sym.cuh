@@ -22,12 +22,15 @@ namespace bc {
 template <int K>
 struct SymTraits {
     static constexpr bool slp_part = (K == BEMPPCUDA_LAPLACE_SLP || K == BEMPPCUDA_HELMHOLTZ_SLP ||
-                                      K == BEMPPCUDA_HELMHOLTZ_COMBINED);
+                                      K == BEMPPCUDA_MODHELM_SLP || K == BEMPPCUDA_HELMHOLTZ_COMBINED);
     static constexpr bool dlp_part = (K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_LAPLACE_ADLP ||
                                       K == BEMPPCUDA_HELMHOLTZ_DLP || K == BEMPPCUDA_HELMHOLTZ_ADLP ||
+                                      K == BEMPPCUDA_MODHELM_DLP || K == BEMPPCUDA_MODHELM_ADLP ||
                                       K == BEMPPCUDA_HELMHOLTZ_COMBINED);
-    static constexpr bool swap = (K == BEMPPCUDA_LAPLACE_ADLP || K == BEMPPCUDA_HELMHOLTZ_ADLP);
+    static constexpr bool swap = (K == BEMPPCUDA_LAPLACE_ADLP || K == BEMPPCUDA_HELMHOLTZ_ADLP ||
+                                  K == BEMPPCUDA_MODHELM_ADLP);
     static constexpr bool helm = KernelTraits<K>::helm;
+    static constexpr bool modhelm = KernelTraits<K>::modhelm;  // FP64 tile only
     static constexpr bool supported = slp_part || dlp_part;
 };
 
@@ -43,6 +46,8 @@ struct TestBlock64s {
 // k = kr + i ki: exp(i kr r) from the reduced sine / cosine times exp(-ki r) per point pair and
 // (ikr - 1) / r = -(1/r + ki) + i kr in the double layer (no centroid factoring: the amplitude
 // varies over the pair).  G(x, y) = G(y, x) for complex k too, so the sweep is unchanged.
+// Modified Helmholtz (real, w = p[0]): the Laplace sums with exp(-w r) (single layer) and
+// exp(-w r) (1 + w r) (double layers) per point pair.
 template <int K, int PHC>
 __device__ __forceinline__ void regular_dp0_fp64_sym_tile(const RegParams &prm, const QuadRule &rule,
                                                         int64_t tile_x, int64_t t0, int rows, TestBlock64s &sb) {
@@ -123,9 +128,15 @@ __device__ __forceinline__ void regular_dp0_fp64_sym_tile(const RegParams &prm, 
                     const double rinv = rsqrt64(r2);
                     const double f = rule.w[q] * rinv;
                     if (!ST::helm) {
-                        if (ST::slp_part) pr += f;
+                        double e = 1.0, e1 = 1.0;  // modified Helmholtz: exp(-w r), exp(-w r) (1 + w r)
+                        if (ST::modhelm) {
+                            const double r = r2 * rinv;
+                            e = exp(-kr * r);
+                            e1 = e * fma(kr, r, 1.0);
+                        }
+                        if (ST::slp_part) pr = ST::modhelm ? fma(f, e, pr) : pr + f;
                         if (ST::dlp_part) {
-                            const double g3 = f * rinv * rinv;
+                            const double g3 = ST::modhelm ? f * rinv * rinv * e1 : f * rinv * rinv;
                             ur += g3;
                             vr = fma(g3, ynt[q], vr);
                         }

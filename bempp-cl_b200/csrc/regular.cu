@@ -268,9 +268,11 @@ static cudaError_t launch_dp0(const RegParams &prm, const QuadRule &rule, int mi
     if constexpr (SymTraits<K>::supported) {
         // same DP0 space on both sides; the mixed tiles need a real wavenumber k > 0 (scaled units),
         // the FP64 tiles take a complex one as phase class 3
+        // (modified Helmholtz: FP64 only)
         const bool helm = KernelTraits<K>::helm;
         const bool ck_sym = helm && prm.p[1] != 0.0;
-        const bool sweep_ok = !helm || (mixed ? (prm.p[1] == 0.0 && prm.p[0] > 0.0) : true);
+        const bool sweep_ok = helm ? (!mixed || (prm.p[1] == 0.0 && prm.p[0] > 0.0))
+                                   : !(KernelTraits<K>::modhelm && mixed);
         if (sym && sweep_ok) {
             // rows per tile: 32, or 16 / 8 when 32-row tiles would leave the GPU under four waves of
             // working CTAs (about half the tiles lie below the diagonal and exit; 3 CTAs per SM)
@@ -279,13 +281,19 @@ static cudaError_t launch_dp0(const RegParams &prm, const QuadRule &rule, int mi
             while (tile_rows > 8 && (int64_t)grid.x * ((row1 - row0 + tile_rows - 1) / tile_rows) / 2 < 4 * wave)
                 tile_rows /= 2;
             const dim3 sgrid(grid.x, (unsigned)((row1 - row0 + tile_rows - 1) / tile_rows));
-            if (mixed) {
-                if (phase_class == 2)
-                    regular_dp0_mixed_sym<K, 2><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
-                else if (phase_class == 1)
-                    regular_dp0_mixed_sym<K, 1><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
-                else
-                    regular_dp0_mixed_sym<K, 0><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
+            if constexpr (!KernelTraits<K>::modhelm) {
+                if (mixed) {
+                    if (phase_class == 2)
+                        regular_dp0_mixed_sym<K, 2><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
+                    else if (phase_class == 1)
+                        regular_dp0_mixed_sym<K, 1><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
+                    else
+                        regular_dp0_mixed_sym<K, 0><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
+                    return cudaGetLastError();
+                }
+            }
+            if constexpr (!KernelTraits<K>::helm) {  // no phase: one instance
+                regular_dp0_fp64_sym<K, 0><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
             } else {
                 if (ck_sym)
                     regular_dp0_fp64_sym<K, 3><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
@@ -547,10 +555,13 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
     const bool ranged = a->row_begin != 0 || a->row_end != 0;
     // the kernels with a symmetric sweep, and its wavenumber condition (launch_dp0)
     const bool laplace = a->kernel <= BEMPPCUDA_LAPLACE_ADLP;
-    const bool sym_kernel = laplace || a->kernel == BEMPPCUDA_HELMHOLTZ_SLP || a->kernel == BEMPPCUDA_HELMHOLTZ_DLP ||
-                            a->kernel == BEMPPCUDA_HELMHOLTZ_ADLP || a->kernel == BEMPPCUDA_HELMHOLTZ_COMBINED;
+    const bool modhelm = a->kernel >= BEMPPCUDA_MODHELM_SLP && a->kernel <= BEMPPCUDA_MODHELM_ADLP;
+    const bool sym_kernel = laplace || modhelm || a->kernel == BEMPPCUDA_HELMHOLTZ_SLP ||
+                            a->kernel == BEMPPCUDA_HELMHOLTZ_DLP || a->kernel == BEMPPCUDA_HELMHOLTZ_ADLP ||
+                            a->kernel == BEMPPCUDA_HELMHOLTZ_COMBINED;
     const bool sym_ok = sym && sym_kernel &&
-                        (laplace || a->precision != BEMPPCUDA_MIXED || (a->params[1] == 0.0 && a->params[0] > 0.0));
+                        (laplace || a->precision != BEMPPCUDA_MIXED ||
+                         (!modhelm && a->params[1] == 0.0 && a->params[0] > 0.0));
     if (ranged && (!sym_ok || a->row_begin < 0 || a->row_end > prm.ntest || a->row_begin >= a->row_end)) {
         bc_set_error("row range [%lld, %lld) needs the symmetric sweep and 0 <= begin < end <= %lld rows",
                      (long long)a->row_begin, (long long)a->row_end, (long long)prm.ntest);

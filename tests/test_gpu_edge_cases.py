@@ -73,11 +73,13 @@ def test_mismatched_sizes_and_row_ranges_are_rejected():
         with pytest.raises(_lib.BemppCudaError) as exc:
             regular_into(out, d, sp, sp, Parameters(), overwrite=True, rows=rows)
         assert exc.value.status == _lib.ERR_INVALID
-    # a row range needs the symmetric sweep: complex wavenumber -> rejected, not ignored
+    # a row range needs the symmetric sweep: the mixed tiles have none for a complex wavenumber ->
+    # rejected, not ignored; the FP64 tiles sweep complex wavenumbers (phase class 3) -> accepted
     dc = operators.boundary.helmholtz.single_layer(sp, sp, sp, 3.0 + 0.5j).descriptor
     with pytest.raises(_lib.BemppCudaError) as exc:
-        regular_into(out, dc, sp, sp, Parameters(), overwrite=True, rows=(0, 8))
+        regular_into(out, dc, sp, sp, Parameters(), precision=_lib.MIXED, overwrite=True, rows=(0, 8))
     assert exc.value.status == _lib.ERR_INVALID
+    regular_into(out, dc, sp, sp, Parameters(), overwrite=True, rows=(0, 8))
     _usable()
 
 

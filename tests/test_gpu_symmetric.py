@@ -28,6 +28,10 @@ KERNELS = [
     ("helmholtz_double_layer", [4.0, 0.7]),
     ("helmholtz_adjoint_double_layer", [4.0, 0.7]),
     ("helmholtz_combined_field", [7.0, 0.5, 0.0, -7.0]),
+    # modified Helmholtz (real kernel; FP64 sweep, the mixed path runs per pair)
+    ("modified_helmholtz_single_layer", [2.0]),
+    ("modified_helmholtz_double_layer", [2.0]),
+    ("modified_helmholtz_adjoint_double_layer", [6.0]),
 ]
 
 
@@ -38,7 +42,7 @@ def _assemble(grid, kernel, options, precision, symmetric):
     from bempp_cuda.space import function_space
 
     sp = function_space(grid, "DP", 0)
-    is_complex = not kernel.startswith("laplace")
+    is_complex = kernel.startswith("helmholtz")
     desc = OperatorDescriptor("probe", options, kernel, "default_scalar", "double", is_complex, None, 1)
     n = grid.number_of_elements
     out = torch.full((n, n), float("nan"), dtype=torch.complex128 if is_complex else torch.float64, device="cuda")
@@ -229,7 +233,7 @@ def test_singular_vertex_pairs_mirrored(kernel, options):
 
     grid = ellipsoid(3, 1.0, 0.8, 1.2)
     sp = function_space(grid, "DP", 0)
-    is_complex = not kernel.startswith("laplace")
+    is_complex = kernel.startswith("helmholtz")
     desc = OperatorDescriptor("probe", options, kernel, "default_scalar", "double", is_complex, None, 1)
     n = grid.number_of_elements
     out = []
