@@ -10,10 +10,10 @@
 //  1. potential_sources: one thread per (element, quadrature point) writes the
 //     source point, normal and weighted coefficient(s) field-major into the
 //     caller's workspace (the reference's `tmp` arrays).
-//  2. potential_scalar (Laplace and Helmholtz single / double layer with a
-//     real wavenumber): a thread per evaluation point walks the sources staged
+//  2. potential_scalar (Laplace, Helmholtz and modified Helmholtz single /
+//     double layer): a thread per evaluation point walks the sources staged
 //     in shared memory; see the comment above the kernel.
-//     potential_eval (every other case): one warp owns PPW evaluation points;
+//     potential_eval (far fields, Maxwell): one warp owns PPW evaluation points;
 //     its lanes stride over the sources with coalesced loads, accumulate per
 //     point in FP64 and combine with xor-shuffle reductions; lane 0 writes.
 #include <algorithm>
@@ -276,11 +276,16 @@ __device__ __forceinline__ void phase_small(double t, double *s, double *c) {
         sincos_cw64(t, s, c);
 }
 
+// PHC 0-2: real wavenumber (1, 2: factored about the element centroid); PHC 3: complex wavenumber
+// k = kr + i ki, exp(i kr r) exp(-ki r) per point-source pair and (ikr - 1) = -(1 + ki r) + i kr r.
+// Modified Helmholtz (real kernel, w = p[0]): the Laplace kernels times exp(-w r) or exp(-w r) (1 + w r).
 template <int K, int PHC, int NQ>
 __global__ void __launch_bounds__(PS_THREADS) potential_scalar(PotParams prm, int64_t chunk_elems) {
     constexpr bool HELM = (K == BEMPPCUDA_HELMHOLTZ_SLP || K == BEMPPCUDA_HELMHOLTZ_DLP);
-    constexpr bool DLP = (K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_HELMHOLTZ_DLP);
-    constexpr bool FACTOR = HELM && PHC > 0;
+    constexpr bool MH = (K == BEMPPCUDA_MODHELM_SLP || K == BEMPPCUDA_MODHELM_DLP);
+    constexpr bool DLP = (K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_HELMHOLTZ_DLP || K == BEMPPCUDA_MODHELM_DLP);
+    constexpr bool FACTOR = HELM && (PHC == 1 || PHC == 2);
+    constexpr bool CK = HELM && PHC == 3;
     __shared__ double2 ssrc[PS_SOURCES * 4];        // {y0 y1} {y2 cre} {cim n0} {n1 n2}
     __shared__ double2 scen[FACTOR ? PS_SOURCES * 2 : 2];  // {c0 c1} {c2 -} per element
     const int nq = NQ ? NQ : prm.nq;
@@ -296,7 +301,7 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar(PotParams prm, in
         for (int d = 0; d < 3; ++d) x[j][d] = prm.points[3 * pj + d];
         ar[j] = ai[j] = 0.0;
     }
-    const double k = prm.p[0];
+    const double k = prm.p[0], ki = CK ? prm.p[1] : 0.0;
     const int64_t n = prm.nsrc;
     const double *o = prm.src;
     for (int64_t t0 = ebeg; t0 < eend; t0 += tile_elems) {
@@ -352,17 +357,26 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar(PotParams prm, in
                     }
                     if (!HELM) {
                         if (DLP) f = -f;
+                        if (MH) {
+                            const double r = r2 * rinv, e = exp(-k * r);
+                            f *= DLP ? e * fma(k, r, 1.0) : e;
+                        }
                         er[j] = fma(f, cr, er[j]);
                         ei[j] = fma(f, ci, ei[j]);
                     } else {
                         const double r = r2 * rinv;
                         double sn, cs;
-                        phase_small<PHC>(FACTOR ? fma(k, r, -krc[j]) : k * r, &sn, &cs);
+                        phase_small<CK ? 0 : PHC>(FACTOR ? fma(k, r, -krc[j]) : k * r, &sn, &cs);
+                        if (CK) {
+                            const double am = exp(-ki * r);
+                            sn *= am;
+                            cs *= am;
+                        }
                         double wr = f * cr, wi = f * ci;  // f times the coefficient
                         if (DLP) {
-                            // times (i k r - 1)
-                            const double b = k * r;
-                            const double tr = -fma(b, wi, wr), ti = fma(b, wr, -wi);
+                            // times (i k r - 1) = -a + i b, a = 1 + ki r, b = kr r
+                            const double b = k * r, a = CK ? fma(ki, r, 1.0) : 1.0;
+                            const double tr = -fma(b, wi, a * wr), ti = fma(b, wr, -a * wi);
                             wr = tr;
                             wi = ti;
                         }
@@ -410,8 +424,8 @@ static cudaError_t launch_scalar_nq(const PotParams &prm, dim3 grid, int64_t chu
 }
 
 
-// Scalar Laplace / Helmholtz potential with a real wavenumber; phase_radius
-// bounds every source's distance from its element centroid (0: unknown).
+// Scalar Laplace, Helmholtz (real or complex wavenumber) and modified Helmholtz potentials;
+// phase_radius bounds every source's distance from its element centroid (0: unknown).
 static cudaError_t launch_scalar(const PotParams &prm, int kernel, double phase_radius, cudaStream_t st) {
     const int64_t pblocks = (prm.npoints + PS_THREADS * PS_PPT - 1) / (PS_THREADS * PS_PPT);
     const int64_t target = (int64_t)bc_sm_count() * 8;  // CTAs: several waves of 4 resident per SM
@@ -426,15 +440,20 @@ static cudaError_t launch_scalar(const PotParams &prm, int kernel, double phase_
     }
     const dim3 grid((unsigned)pblocks, (unsigned)chunks);
     const double kr = fabs(prm.p[0]) * phase_radius;
-    const int phc = (phase_radius > 0.0 && kr <= 0.5) ? 2 : (phase_radius > 0.0 && kr <= 1.0) ? 1 : 0;
+    const int phc = prm.p[1] != 0.0 ? 3
+                    : (phase_radius > 0.0 && kr <= 0.5) ? 2 : (phase_radius > 0.0 && kr <= 1.0) ? 1 : 0;
     switch (kernel) {
     case BEMPPCUDA_LAPLACE_SLP: return launch_scalar_nq<BEMPPCUDA_LAPLACE_SLP, 0>(prm, grid, chunk_elems, st);
     case BEMPPCUDA_LAPLACE_DLP: return launch_scalar_nq<BEMPPCUDA_LAPLACE_DLP, 0>(prm, grid, chunk_elems, st);
+    case BEMPPCUDA_MODHELM_SLP: return launch_scalar_nq<BEMPPCUDA_MODHELM_SLP, 0>(prm, grid, chunk_elems, st);
+    case BEMPPCUDA_MODHELM_DLP: return launch_scalar_nq<BEMPPCUDA_MODHELM_DLP, 0>(prm, grid, chunk_elems, st);
     case BEMPPCUDA_HELMHOLTZ_SLP:
+        if (phc == 3) return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_SLP, 3>(prm, grid, chunk_elems, st);
         if (phc == 2) return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_SLP, 2>(prm, grid, chunk_elems, st);
         if (phc == 1) return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_SLP, 1>(prm, grid, chunk_elems, st);
         return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_SLP, 0>(prm, grid, chunk_elems, st);
     default:  // BEMPPCUDA_HELMHOLTZ_DLP
+        if (phc == 3) return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_DLP, 3>(prm, grid, chunk_elems, st);
         if (phc == 2) return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_DLP, 2>(prm, grid, chunk_elems, st);
         if (phc == 1) return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_DLP, 1>(prm, grid, chunk_elems, st);
         return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_DLP, 0>(prm, grid, chunk_elems, st);
@@ -477,9 +496,9 @@ int bc_potential_launch(const bemppcuda_potential_args *a, double *workspace, cu
     }
     cudaError_t err = cudaGetLastError();
     if (err == cudaSuccess) {
-        const bool real_k = a->params[1] == 0.0;
         const bool per_point = a->kernel == BEMPPCUDA_LAPLACE_SLP || a->kernel == BEMPPCUDA_LAPLACE_DLP ||
-                               ((a->kernel == BEMPPCUDA_HELMHOLTZ_SLP || a->kernel == BEMPPCUDA_HELMHOLTZ_DLP) && real_k);
+                               a->kernel == BEMPPCUDA_HELMHOLTZ_SLP || a->kernel == BEMPPCUDA_HELMHOLTZ_DLP ||
+                               a->kernel == BEMPPCUDA_MODHELM_SLP || a->kernel == BEMPPCUDA_MODHELM_DLP;
         if (!maxwell && per_point && prm.nsupport > 0) {
             err = launch_scalar(prm, a->kernel, a->phase_radius, st);
         } else if (!maxwell) {

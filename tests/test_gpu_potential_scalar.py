@@ -1,7 +1,7 @@
 """The per-point scalar potential kernel against the oracle (run on a B200).
 
-Laplace and Helmholtz (real wavenumber) single / double layer potentials go
-through ``potential_scalar``: a thread per evaluation point, sources staged in
+Laplace, Helmholtz (real and complex wavenumber) and modified Helmholtz
+single / double layer potentials go through ``potential_scalar``: a thread per evaluation point, sources staged in
 shared memory, the support split into chunks added with atomics, and the
 Helmholtz phase factored about each element's centroid when k R <= 1
 (R = largest centroid-to-vertex distance).  The cases below reach every phase
@@ -68,6 +68,37 @@ def test_helmholtz_every_phase_class(oracle, kr, name, family):
     k = kr / device_grid(grid).radius
     points, _ = sphere_shell_points(3000, 17)
     _check(oracle, _operator(name, space, points, k), space)
+
+
+@pytest.mark.parametrize("k", [2.5 + 1.0j, 6.0 + 0.3j])
+@pytest.mark.parametrize("name", ["single_layer", "double_layer"])
+def test_helmholtz_complex_wavenumber(oracle, k, name):
+    """Complex wavenumbers (phase class 3: exp(-Im k r) per point-source pair, no centroid factoring)."""
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+    from cases import sphere_shell_points
+
+    grid = regular_sphere(3)
+    space = function_space(grid, "P", 1)
+    points, _ = sphere_shell_points(2000, 19)
+    _check(oracle, _operator(name, space, points, k), space)
+
+
+@pytest.mark.parametrize("omega", [0.7, 4.0])
+@pytest.mark.parametrize("name", ["single_layer", "double_layer"])
+@pytest.mark.parametrize("family", ["DP0", "P1"])
+def test_modified_helmholtz(oracle, omega, name, family):
+    """Modified Helmholtz potentials: the Laplace kernels times exp(-w r) (single) or exp(-w r) (1 + w r)."""
+    from bempp_cuda import operators
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+    from cases import sphere_shell_points
+
+    grid = regular_sphere(3)
+    space = function_space(grid, "DP", 0) if family == "DP0" else function_space(grid, "P", 1)
+    points, _ = sphere_shell_points(1500, 23)
+    op = getattr(operators.potential.modified_helmholtz, name)(space, points, omega)
+    _check(oracle, op, space)
 
 
 @pytest.mark.parametrize("name", ["single_layer", "double_layer"])
