@@ -203,6 +203,30 @@ class BatchArgs(_ct.Structure):
     ]
 
 
+BASIS_SCALAR = 0
+BASIS_RWG = 1
+BASIS_SNC = 2
+
+
+class IdentityArgs(_ct.Structure):
+    _fields_ = [
+        ("grid", GridRec),
+        ("test", Space),
+        ("trial", Space),
+        ("test_kind", _i32),
+        ("trial_kind", _i32),
+        ("nelements", _i64),
+        ("elements", _vp),
+        ("nq", _i32),
+        ("pad", _i32),
+        ("quad_points", _vp),
+        ("quad_weights", _vp),
+        ("rows", _vp),
+        ("cols", _vp),
+        ("values", _vp),
+    ]
+
+
 class MatmatProblem(_ct.Structure):
     _fields_ = [
         ("a", _vp),
@@ -285,6 +309,7 @@ SIGNATURES = {
     "bemppcuda_batch_workspace_bytes": (_i64, [_i32]),
     "bemppcuda_batch_prepare": (_ct.c_int, [_ct.POINTER(BatchArgs), _vp]),
     "bemppcuda_batch_launch": (_ct.c_int, [_ct.POINTER(BatchArgs), _vp]),
+    "bemppcuda_assemble_identity": (_ct.c_int, [_ct.POINTER(IdentityArgs), _vp]),
     "bemppcuda_matmat_workspace_bytes": (_i64, [_i32]),
     "bemppcuda_matmat_prepare": (_ct.c_int, [_ct.POINTER(MatmatArgs), _vp]),
     "bemppcuda_matmat_launch": (_ct.c_int, [_ct.POINTER(MatmatArgs), _vp]),

@@ -144,6 +144,58 @@ def regular_into(
     return result
 
 
+def basis_kind(space):
+    """BEMPPCUDA_BASIS_* of a space: RWG, SNC (n x RWG) or scalar."""
+    ident = getattr(space, "identifier", "")
+    if ident.startswith("rwg"):
+        return _lib.BASIS_RWG
+    if ident.startswith("snc"):
+        return _lib.BASIS_SNC
+    return _lib.BASIS_SCALAR
+
+
+def identity_triplets(domain, dual_to_range, parameters, stream=None):
+    """COO triplets (rows, cols, values) of the L2 identity on the device (csrc/identity.cu).
+
+    The reference (core/sparse_assembler.py:17-70) evaluates the same local
+    mass matrices on the elements of both supports and sums repeated (row,
+    col) pairs when it converts to CSR; the caller does that here.
+    """
+    require_cuda()
+    if domain.grid != dual_to_range.grid:
+        raise ValueError("For sparse operators the domain and dual_to_range grids must be identical.")
+    tk, sk = basis_kind(dual_to_range), basis_kind(domain)
+    if (tk == _lib.BASIS_SCALAR) != (sk == _lib.BASIS_SCALAR):
+        raise ValueError("the identity needs two scalar spaces or two RWG / SNC spaces")
+    elements = _np.flatnonzero(_np.asarray(domain.support) & _np.asarray(dual_to_range.support)).astype(_np.int32)
+    nt = int(dual_to_range.number_of_shape_functions)
+    ns = int(domain.number_of_shape_functions)
+    n = len(elements) * nt * ns
+    rows = _torch.empty(n, dtype=_torch.int64, device="cuda")
+    cols = _torch.empty(n, dtype=_torch.int64, device="cuda")
+    values = _torch.empty(n, dtype=_torch.float64, device="cuda")
+    if n == 0:
+        return rows, cols, values
+    el = _torch.as_tensor(elements).to("cuda")
+    grid = device_grid(domain.grid)
+    sspace = device_space(domain)
+    tspace = sspace if same_space(domain, dual_to_range) else device_space(dual_to_range)
+    points, weights = regular_rule(parameters.quadrature.regular)
+    args = _lib.IdentityArgs()
+    args.grid = grid.record()
+    args.test = tspace.record()
+    args.trial = sspace.record()
+    args.test_kind, args.trial_kind = tk, sk
+    args.nelements = len(elements)
+    args.elements = ptr(el)
+    args.nq = len(weights)
+    args.quad_points = points.ctypes.data
+    args.quad_weights = weights.ctypes.data
+    args.rows, args.cols, args.values = ptr(rows), ptr(cols), ptr(values)
+    _lib.check(_lib.load().bemppcuda_assemble_identity(args, stream or current_stream()))
+    return rows, cols, values
+
+
 def dp0_fast_path(descriptor, domain, dual_to_range, parameters):
     """True when the regular pass can overwrite every entry (no pre-zeroing needed)."""
     if descriptor.assembly_type != "default_scalar":

@@ -100,6 +100,12 @@ class DenseDeviceOperator(object):
                 out = out.to(_torch.complex128)
             out.diagonal().add_(b * vals.to(out.dtype))
             return DenseDeviceOperator(out)
+        if isinstance(other, SparseDeviceOperator):
+            out = self.tensor * a if a != 1 else self.tensor.clone()
+            if not out.is_complex() and (other._coo.is_complex() or isinstance(b, complex)):
+                out = out.to(_torch.complex128)
+            other.add_into(out, b)
+            return DenseDeviceOperator(out)
         return NotImplemented
 
     def __add__(self, other):
@@ -144,6 +150,89 @@ class DiagonalOperator(object):
 
     def __neg__(self):
         return DiagonalOperator(-self.values)
+
+
+class SparseDeviceOperator(object):
+    """Sparse discrete operator on the device: the counterpart of SparseDiscreteBoundaryOperator
+    (discrete_boundary_operator.py:255-330) with coalesced COO triplets and a CSR copy for products."""
+
+    def __init__(self, rows, cols, values, shape):
+        coo = _torch.sparse_coo_tensor(_torch.stack([rows, cols]), values, size=tuple(shape)).coalesce()
+        self._coo = coo
+        self.tensor = coo.to_sparse_csr()
+
+    @property
+    def shape(self):
+        return tuple(self._coo.shape)
+
+    @property
+    def dtype(self):
+        return _np.complex128 if self._coo.is_complex() else _np.float64
+
+    @property
+    def A(self):
+        return self._coo.to_dense().cpu().numpy()
+
+    def to_dense(self):
+        return self.A
+
+    def add_into(self, dense, coef=1.0):
+        """dense += coef * self, scattered on the device."""
+        idx = self._coo.indices()
+        vals = self._coo.values() * coef
+        if vals.is_complex() and not dense.is_complex():
+            raise TypeError("a complex sparse term needs a complex dense operator")
+        dense.index_put_((idx[0], idx[1]), vals.to(dense.dtype), accumulate=True)
+        return dense
+
+    def dot(self, x):
+        host = not isinstance(x, _torch.Tensor)
+        xt = _torch.as_tensor(_np.asarray(x)).to("cuda") if host else x
+        mat = self.tensor
+        if xt.is_complex() and not mat.is_complex():
+            mat = mat.to(xt.dtype)
+        elif mat.is_complex() and not xt.is_complex():
+            xt = xt.to(mat.dtype)
+        y = mat @ xt.to(mat.dtype)
+        return y.cpu().numpy() if host else y
+
+    def __matmul__(self, x):
+        return self.dot(x)
+
+    def __call__(self, x):
+        return self.dot(x)
+
+    def _scaled(self, alpha):
+        idx = self._coo.indices()
+        return SparseDeviceOperator(idx[0], idx[1], self._coo.values() * alpha, self.shape)
+
+    def __mul__(self, alpha):
+        if _np.isscalar(alpha):
+            return self._scaled(alpha)
+        return self.dot(alpha)
+
+    __rmul__ = __mul__
+
+    def __neg__(self):
+        return self._scaled(-1.0)
+
+    def _combine(self, other, a, b):
+        if isinstance(other, SparseDeviceOperator):
+            i1, i2 = self._coo.indices(), other._coo.indices()
+            v1, v2 = self._coo.values() * a, other._coo.values() * b
+            if v1.is_complex() != v2.is_complex():
+                v1, v2 = v1.to(_torch.complex128), v2.to(_torch.complex128)
+            idx = _torch.cat([i1, i2], dim=1)
+            return SparseDeviceOperator(idx[0], idx[1], _torch.cat([v1, v2]), self.shape)
+        if isinstance(other, DenseDeviceOperator):
+            return other._combine(self, b, a)
+        return NotImplemented
+
+    def __add__(self, other):
+        return self._combine(other, 1, 1)
+
+    def __sub__(self, other):
+        return self._combine(other, 1, -1)
 
 
 class BoundaryOperator(object):
@@ -268,7 +357,12 @@ def weak_form_to_host(op, out=None, blocks=16):
         return assemble_dense_to_host(op.domain, op.dual_to_range, op.parameters, op.descriptor,
                                       op.device_interface, out, blocks=blocks)
     w = op.weak_form()
-    t = _torch.diag(w.values) if isinstance(w, DiagonalOperator) else w.tensor
+    if isinstance(w, DiagonalOperator):
+        t = _torch.diag(w.values)
+    elif isinstance(w, SparseDeviceOperator):
+        t = w._coo.to_dense()
+    else:
+        t = w.tensor
     if out is None:
         out = _torch.empty(tuple(t.shape), dtype=t.dtype, pin_memory=True)
     out.copy_(t)
@@ -286,10 +380,12 @@ class _SumOperator(BoundaryOperator):
             return fused
         wa = self._a.weak_form()
         wb = self._b.weak_form()
-        if isinstance(wa, DiagonalOperator):
+        if isinstance(wa, (DiagonalOperator, SparseDeviceOperator)) and isinstance(wb, DenseDeviceOperator):
             wa, wb, ca, cb = wb, wa, self._cb, self._ca
         else:
             ca, cb = self._ca, self._cb
+        if isinstance(wa, SparseDeviceOperator):
+            return wa._combine(wb, ca, cb)
         if isinstance(wb, DiagonalOperator):
             return (wa * ca) + (wb * cb) if ca != 1 else wa + (wb * cb)
         return wa._combine(wb, ca, cb)
@@ -305,15 +401,28 @@ class _ScaledOperator(BoundaryOperator):
 
 
 class IdentityOperator(BoundaryOperator):
-    """L2 identity for DP0 spaces: diagonal of element areas (sparse.py:6-60)."""
+    """L2 identity (sparse.py:6-28): a diagonal of element areas when domain and dual are the same DP0
+    space, else the mass matrix of the two spaces as a device sparse operator (csrc/identity.cu)."""
 
     def _assemble(self):
-        if self.domain.number_of_shape_functions != 1 or self.dual_to_range.number_of_shape_functions != 1:
-            raise ValueError("the device identity is implemented for DP0 spaces")
-        if not (self.domain == self.dual_to_range):
-            raise ValueError("the device identity needs identical DP0 domain and dual spaces")
-        areas = _np.asarray(self.domain.grid.volumes)[self.domain.support_elements]
-        return DiagonalOperator(_torch.as_tensor(areas, dtype=_torch.float64, device="cuda"))
+        from .assembly import identity_triplets, same_space
+
+        if (self.domain.number_of_shape_functions == 1 and self.dual_to_range.number_of_shape_functions == 1
+                and same_space(self.domain, self.dual_to_range) and _dof_is_position(self.domain)):
+            areas = _np.asarray(self.domain.grid.volumes)[self.domain.support_elements]
+            return DiagonalOperator(_torch.as_tensor(areas, dtype=_torch.float64, device="cuda"))
+        rows, cols, values = identity_triplets(self.domain, self.dual_to_range, self.parameters)
+        return SparseDeviceOperator(rows, cols, values,
+                                    (self.dual_to_range.global_dof_count, self.domain.global_dof_count))
+
+
+def _dof_is_position(space):
+    """DP0 space whose dof i is its i-th support element with multiplier 1 (its mass matrix is diagonal)."""
+    l2g = _np.asarray(space.local2global).reshape(-1)
+    sup = _np.asarray(space.support_elements)
+    mult = _np.asarray(space.local_multipliers).reshape(-1)
+    return (len(sup) == int(space.global_dof_count) and _np.array_equal(l2g[sup], _np.arange(len(sup)))
+            and bool(_np.all(mult[sup] == 1.0)))
 
 
 def _create(identifier, domain, range_, dual_to_range, options, kernel_type, assembly_type, is_complex,

@@ -242,6 +242,36 @@ typedef struct {
     int64_t workspace_bytes;
 } bemppcuda_batch_args;
 
+/* L2 identity (mass matrix) of two spaces on one grid as COO triplets.
+   Replaces l2_identity_kernel (core/numba_kernels.py:713-769) with
+   default_sparse_kernel (:935-976) and the triplet assembly of
+   SparseAssembler.assemble (core/sparse_assembler.py:17-70): for every
+   element e of `elements` (the elements in both supports) and local
+   functions i (test), j (trial), entry e * nt * ns + i * ns + j holds
+       row = test.l2g[e, i], col = trial.l2g[e, j],
+       value = test.mult[e, i] * trial.mult[e, j] * |J_e| * sum_q w_q phi_i(q) . psi_j(q).
+   Repeated (row, col) pairs are to be summed by the caller (as coo -> csr). */
+#define BEMPPCUDA_BASIS_SCALAR 0 /* P0 / P1 / DP1 values */
+#define BEMPPCUDA_BASIS_RWG 1    /* l_i / |J| J r_i (maxwell_spaces.py:678-712) */
+#define BEMPPCUDA_BASIS_SNC 2    /* n x the RWG value, n times the normal multiplier (:716-757) */
+
+typedef struct {
+    bemppcuda_grid grid;
+    bemppcuda_space test;       /* dual_to_range */
+    bemppcuda_space trial;      /* domain */
+    int32_t test_kind;          /* BEMPPCUDA_BASIS_*: both scalar, or both RWG / SNC */
+    int32_t trial_kind;
+    int64_t nelements;
+    const uint32_t *elements;   /* (nelements,) device, elements in both supports */
+    int32_t nq;                 /* rule size <= BEMPPCUDA_MAX_REGULAR_POINTS */
+    int32_t pad;
+    const double *quad_points;  /* HOST (nq, 2) */
+    const double *quad_weights; /* HOST (nq,) */
+    int64_t *rows;              /* device outputs, nelements * nt * ns entries each */
+    int64_t *cols;
+    double *values;
+} bemppcuda_identity_args;
+
 /* Batched multi-right-hand-side products Y_p = A_p X_p of dense complex128
    operators (interleaved re / im, row-major), one launch for the whole list.
    Replaces DenseDiscreteBoundaryOperator._matmat
@@ -304,6 +334,8 @@ int bemppcuda_batch_prepare(const bemppcuda_batch_args *args, void *stream);
    (a memset and two launches), so it can be captured in a CUDA graph once
    bemppcuda_batch_prepare has run. */
 int bemppcuda_batch_launch(const bemppcuda_batch_args *args, void *stream);
+
+int bemppcuda_assemble_identity(const bemppcuda_identity_args *args, void *stream);
 
 int64_t bemppcuda_matmat_workspace_bytes(int32_t nproblems);
 /* Check the list, upload it into the workspace (host-to-device copy, then a

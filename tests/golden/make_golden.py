@@ -22,6 +22,11 @@ module) and writes small .npz files:
 * ``host_sphere_msh.npz``   reference host bookkeeping on sphere.msh: edge and
                             vertex adjacency, dof maps of every space, singular
                             pair arrays at order 4 and the order-4 triangle rule
+* ``identity.npz``          sparse L2 identities: the reference's golden
+                            test/data/sparse_identity_*.npy on sphere.msh and
+                            the live reference Numba path on regular_sphere(2)
+                            for more space pairs, as nonzero triplets
+                            (``--identity`` writes only this file)
 
 Nothing at test time reads the reference tree; only these fixtures.
 """
@@ -110,6 +115,58 @@ def fingerprint(mat, seed=1234):
         "entries": mat[ii, jj],
         "shape": np.array(mat.shape),
     }
+
+
+# (key, domain space, dual space, legacy file or None); the identity's range is its domain
+IDENTITY_CASES = [
+    ("p0_p0", ("DP", 0), ("DP", 0), "sparse_identity_p0_p0"),
+    ("p1_p1", ("P", 1), ("P", 1), "sparse_identity_p1_p1"),
+    ("p0_p1", ("P", 1), ("DP", 0), "sparse_identity_p0_p1"),
+    ("p1_p0", ("DP", 0), ("P", 1), "sparse_identity_p1_p0"),
+    ("snc_rwg", ("RWG", 0), ("SNC", 0), "sparse_identity_snc_rwg"),
+    ("dp1_dp1", ("DP", 1), ("DP", 1), None),
+    ("p1_dp1", ("DP", 1), ("P", 1), None),
+    ("rwg_rwg", ("RWG", 0), ("RWG", 0), None),
+    ("snc_snc", ("SNC", 0), ("SNC", 0), None),
+    ("rwg_snc", ("SNC", 0), ("RWG", 0), None),
+]
+
+
+def _triplets(mat):
+    mat = np.asarray(mat)
+    r, c = np.nonzero(mat)
+    return r.astype(np.int32), c.astype(np.int32), mat[r, c], np.array(mat.shape)
+
+
+def make_identity(ref_root):
+    sys.modules.setdefault("meshio", types.ModuleType("meshio"))
+    sys.path.insert(0, ref_root)
+    sys.path.insert(0, os.path.join(REPO, "bempp-cl_b200"))
+    import bempp_cl.api as api
+    from bempp_cl.api.grid.grid import Grid as RefGrid
+    from bempp_cl.api.operators.boundary.sparse import identity
+    from bempp_cuda import shapes
+
+    api.GLOBAL_PARAMETERS.quadrature.regular = 4
+    data = os.path.join(ref_root, "test", "data")
+    out = {}
+    for key, dsp, tsp, gold in IDENTITY_CASES:
+        if gold is None:
+            continue
+        for name, val in zip(("rows", "cols", "vals", "shape"), _triplets(np.load(os.path.join(data, gold + ".npy")))):
+            out["legacy_%s__%s" % (key, name)] = val
+    sv, se = shapes.sphere_arrays(2)
+    g = RefGrid(sv, se)
+    out["vertices"], out["elements"] = sv, se
+    for key, dsp, tsp, gold in IDENTITY_CASES:
+        d = api.function_space(g, *dsp)
+        t = api.function_space(g, *tsp)
+        mat = identity(d, d, t, device_interface="numba").weak_form().to_dense()
+        for name, val in zip(("rows", "cols", "vals", "shape"), _triplets(mat)):
+            out["live_%s__%s" % (key, name)] = val
+        out["live_%s__spaces" % key] = np.array([dsp[0], str(dsp[1]), tsp[0], str(tsp[1])])
+    np.savez_compressed(os.path.join(HERE, "identity.npz"), **out)
+    print("identity fixtures written to", HERE)
 
 
 def main(ref_root):
@@ -225,8 +282,14 @@ def main(ref_root):
     host["triangle4_points"] = qp
     host["triangle4_weights"] = qw
     np.savez_compressed(os.path.join(HERE, "host_sphere_msh.npz"), **host)
+    make_identity(ref_root)
     print("fixtures written to", HERE)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    argv = [a for a in sys.argv[1:] if not a.startswith("--")]
+    root = argv[0] if argv else "/root/reference"
+    if "--identity" in sys.argv[1:]:
+        make_identity(root)
+    else:
+        main(root)

@@ -40,7 +40,7 @@ def test_struct_layout_matches_header():
 #include <stddef.h>
 #include "bemppcuda.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(bemppcuda_regular_args), sizeof(bemppcuda_singular_args),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(bemppcuda_regular_args), sizeof(bemppcuda_singular_args),
          sizeof(bemppcuda_potential_args), sizeof(bemppcuda_space), offsetof(bemppcuda_regular_args, result),
          offsetof(bemppcuda_singular_args, diag_shift), offsetof(bemppcuda_potential_args, workspace_bytes),
          offsetof(bemppcuda_regular_args, phase_radius), sizeof(bemppcuda_batch_problem),
@@ -48,7 +48,9 @@ int main(void) {
          offsetof(bemppcuda_shape_args, incident), offsetof(bemppcuda_shape_args, lambda),
          offsetof(bemppcuda_shape_args, workspace_bytes), offsetof(bemppcuda_potential_args, phase_radius),
          offsetof(bemppcuda_regular_args, result_is_zero), offsetof(bemppcuda_singular_args, mirror_weights_offset),
-         sizeof(bemppcuda_matmat_problem), sizeof(bemppcuda_matmat_args), offsetof(bemppcuda_matmat_args, blocks));
+         sizeof(bemppcuda_matmat_problem), sizeof(bemppcuda_matmat_args), offsetof(bemppcuda_matmat_args, blocks),
+         sizeof(bemppcuda_identity_args), offsetof(bemppcuda_identity_args, nelements),
+         offsetof(bemppcuda_identity_args, values));
   return 0;
 }
 '''
@@ -65,7 +67,8 @@ int main(void) {
             ctypes.sizeof(_lib.ShapeArgs), _lib.ShapeArgs.incident.offset, _lib.ShapeArgs.lam.offset,
             _lib.ShapeArgs.workspace_bytes.offset, _lib.PotentialArgs.phase_radius.offset,
             _lib.RegularArgs.result_is_zero.offset, _lib.SingularArgs.mirror_weights_offset.offset,
-            ctypes.sizeof(_lib.MatmatProblem), ctypes.sizeof(_lib.MatmatArgs), _lib.MatmatArgs.blocks.offset]
+            ctypes.sizeof(_lib.MatmatProblem), ctypes.sizeof(_lib.MatmatArgs), _lib.MatmatArgs.blocks.offset,
+            ctypes.sizeof(_lib.IdentityArgs), _lib.IdentityArgs.nelements.offset, _lib.IdentityArgs.values.offset]
     assert [int(x) for x in out] == mine
 
 
