@@ -26,19 +26,89 @@ import numpy as _np
 import torch as _torch
 
 
-def _norm(v, allreduce=None):
+def _norm_t(v, allreduce=None):
+    """||v|| as a device scalar (float64), summed over the ranks with ``allreduce``."""
     if allreduce is None:
-        return float(_torch.linalg.vector_norm(v).item())
+        return _torch.linalg.vector_norm(v).to(_torch.float64)
     sq = (v.real.square().sum() + v.imag.square().sum()) if v.is_complex() else v.square().sum()
-    return float(_torch.sqrt(allreduce(sq.reshape(1).to(_torch.float64)))[0].item())
+    return _torch.sqrt(allreduce(sq.reshape(1).to(_torch.float64)))[0]
+
+
+def _norm(v, allreduce=None):
+    return float(_norm_t(v, allreduce).item())
+
+
+class _ArnoldiGraph(object):
+    """One Arnoldi step (classical Gram-Schmidt, one re-orthogonalisation) captured in a CUDA graph.
+
+    Shapes are fixed: the step orthogonalises against all restart + 1 rows of
+    the basis V, whose rows beyond the current step are zero, so the same
+    graph serves every step; the step index lives on the device.  A replay
+    reads V[j], writes V[j + 1] and column j of the Hessenberg matrix H and
+    advances j.  One launch per step instead of about twenty.
+    """
+
+    def __init__(self, matvec, n, restart, dtype, device):
+        self.V = _torch.zeros((restart + 1, n), dtype=dtype, device=device)
+        self.H = _torch.zeros((restart + 1, restart), dtype=_torch.complex128, device=device)
+        self.j = _torch.zeros(1, dtype=_torch.int64, device=device)
+        self._rows = _torch.arange(restart + 1, device=device)
+        self._matvec = matvec
+        side = _torch.cuda.Stream()
+        side.wait_stream(_torch.cuda.current_stream())
+        with _torch.cuda.stream(side):  # warm-up outside capture (library handles, workspaces)
+            self._step()
+        _torch.cuda.current_stream().wait_stream(side)
+        self.graph = _torch.cuda.CUDAGraph()
+        with _torch.cuda.graph(self.graph):
+            self._step()
+
+    def _dots(self, w):
+        return _torch.mv(self.V.conj(), w)  # V^H w (the conjugate view goes to the GEMV as a flag)
+
+    def _step(self):
+        V = self.V
+        w = self._matvec(V.index_select(0, self.j).squeeze(0))
+        h = self._dots(w)
+        w = w - _torch.mv(V.transpose(0, 1), h)
+        h2 = self._dots(w)
+        w = w - _torch.mv(V.transpose(0, 1), h2)
+        hn = _torch.linalg.vector_norm(w).to(_torch.float64)
+        V.index_copy_(0, self.j + 1, (w / hn.to(w.dtype)).unsqueeze(0))
+        col = (h + h2).to(_torch.complex128) + (self._rows == self.j + 1).to(_torch.complex128) * hn
+        self.H.index_copy_(1, self.j, col.unsqueeze(1))
+        self.j.add_(1)
+
+    def start(self, v0):
+        self.V.zero_()
+        self.V[0] = v0
+        self.H.zero_()
+        self.j.zero_()
+
+    def steps(self, count):
+        for _ in range(count):
+            self.graph.replay()
 
 
 def gmres_tensor(matvec, b, x0=None, tol=1e-5, restart=None, maxiter=None, callback=None, allreduce=None,
-                 global_size=None):
+                 global_size=None, check_every=1, graph=False):
     """Solve A x = b for one right-hand side; return (x, info, residuals, iterations).
 
     ``matvec(v)`` returns A v for a device vector of b's dtype.  ``info`` is 0
     on convergence, else the number of iterations done (scipy convention).
+
+    ``check_every``: Arnoldi steps run on the device without waiting for the
+    host (the Hessenberg columns stay in device memory); every
+    ``check_every`` steps the new columns come to the host in one transfer,
+    where the Givens rotations give the residual of each step.  The iterate
+    and the reported iteration count are those of the first step that meets
+    the tolerance; up to ``check_every - 1`` further steps may have been
+    computed and are discarded.  1 (default) checks after every step.
+
+    ``graph`` (CUDA tensors, one process): the Arnoldi step is captured once
+    in a CUDA graph (``_ArnoldiGraph``; ``matvec`` must be capturable, e.g.
+    a GEMV with a fixed matrix) and replayed ``check_every`` times between
+    host checks, so the step costs one launch.
 
     Distributed vectors: when every rank holds a block of rows of b and of the
     iterate, ``allreduce(t)`` must return the sum of ``t`` over the ranks (one
@@ -50,6 +120,7 @@ def gmres_tensor(matvec, b, x0=None, tol=1e-5, restart=None, maxiter=None, callb
     n = b.shape[0] if global_size is None else int(global_size)
     restart = min(restart or 100, n)
     maxiter = maxiter or 10 * n
+    check_every = max(1, int(check_every))
     dtype = b.dtype
     red = allreduce if allreduce is not None else (lambda t: t)
     x = _torch.zeros_like(b) if x0 is None else x0.clone()
@@ -61,58 +132,76 @@ def gmres_tensor(matvec, b, x0=None, tol=1e-5, restart=None, maxiter=None, callb
     beta = _norm(r, allreduce)
     residuals.append(beta / bnorm)
     iterations = 0
+    use_graph = bool(graph) and b.is_cuda and allreduce is None
+    arnoldi = _ArnoldiGraph(matvec, b.shape[0], restart, dtype, b.device) if use_graph else None
     while True:
         if beta <= tol * bnorm:
             return x, 0, residuals, iterations
-        V = _torch.empty((restart + 1, b.shape[0]), dtype=dtype, device=b.device)
-        V[0] = r / beta
-        H = _np.zeros((restart + 1, restart), dtype=_np.complex128)
+        if use_graph:
+            arnoldi.start(r / beta)
+            V, Hd = arnoldi.V, arnoldi.H
+        else:
+            V = _torch.empty((restart + 1, b.shape[0]), dtype=dtype, device=b.device)
+            V[0] = r / beta
+            Hd = _torch.zeros((restart + 1, restart), dtype=_torch.complex128, device=b.device)  # Arnoldi columns
+        H = _np.zeros((restart + 1, restart), dtype=_np.complex128)  # rotated (upper triangular)
         cs = _np.zeros(restart, dtype=_np.complex128)
         sn = _np.zeros(restart, dtype=_np.complex128)
         g = _np.zeros(restart + 1, dtype=_np.complex128)
         g[0] = beta
         j_done = 0
         converged = False
-        for j in range(restart):
-            w = matvec(V[j])
-            basis = V[: j + 1]
-            h = red(_torch.mv(basis.conj(), w))
-            w = w - _torch.mv(basis.transpose(0, 1), h)
-            h2 = red(_torch.mv(basis.conj(), w))
-            w = w - _torch.mv(basis.transpose(0, 1), h2)
-            h = (h + h2).to(_torch.complex128).cpu().numpy()
-            hn = _norm(w, allreduce)
-            if hn > 0.0:
-                V[j + 1] = w / hn
-            col = _np.zeros(restart + 1, dtype=_np.complex128)
-            col[: j + 1] = h
-            col[j + 1] = hn
-            for i in range(j):
-                t = cs[i] * col[i] + sn[i] * col[i + 1]
-                col[i + 1] = -_np.conj(sn[i]) * col[i] + _np.conj(cs[i]) * col[i + 1]
-                col[i] = t
-            # rotation G = [[c, s], [-conj(s), conj(c)]] with G (a, b)^T = (rho, 0)^T
-            a, bb = col[j], col[j + 1]
-            denom = _np.sqrt(abs(a) ** 2 + abs(bb) ** 2)
-            if denom == 0.0:
-                cs[j], sn[j] = 1.0, 0.0
-            else:
-                cs[j] = _np.conj(a) / denom
-                sn[j] = _np.conj(bb) / denom
-            col[j] = denom
-            col[j + 1] = 0.0
-            H[:, j] = col
-            g[j + 1] = -_np.conj(sn[j]) * g[j]
-            g[j] = cs[j] * g[j]
-            iterations += 1
-            j_done = j + 1
-            res = abs(g[j + 1])
-            residuals.append(res / bnorm)
-            if callback is not None:
-                callback(res / bnorm)
-            if res <= tol * bnorm or hn == 0.0 or iterations >= maxiter:
-                converged = res <= tol * bnorm or hn == 0.0
-                break
+        stop = False
+        j0 = 0
+        while j0 < restart and not stop:
+            j1 = min(j0 + check_every, restart, j0 + (maxiter - iterations))
+            if use_graph:
+                arnoldi.steps(j1 - j0)
+            for j in range(j0, j1) if not use_graph else ():
+                w = matvec(V[j])
+                basis = V[: j + 1]
+                h = red(_torch.mv(basis.conj(), w))
+                w = w - _torch.mv(basis.transpose(0, 1), h)
+                h2 = red(_torch.mv(basis.conj(), w))
+                w = w - _torch.mv(basis.transpose(0, 1), h2)
+                hn_t = _norm_t(w, allreduce)
+                V[j + 1] = w / hn_t.to(w.dtype)  # unused after a breakdown (hn == 0)
+                Hd[: j + 1, j] = (h + h2).to(_torch.complex128)
+                Hd[j + 1, j] = hn_t.to(_torch.complex128)
+            # the new columns reach the host in one transfer
+            cols = Hd[: j1 + 1, j0:j1].cpu().numpy()
+            for j in range(j0, j1):
+                col = _np.zeros(restart + 1, dtype=_np.complex128)
+                col[: j + 2] = cols[: j + 2, j - j0]
+                hn = float(col[j + 1].real)
+                for i in range(j):
+                    t = cs[i] * col[i] + sn[i] * col[i + 1]
+                    col[i + 1] = -_np.conj(sn[i]) * col[i] + _np.conj(cs[i]) * col[i + 1]
+                    col[i] = t
+                # rotation G = [[c, s], [-conj(s), conj(c)]] with G (a, b)^T = (rho, 0)^T
+                a, bb = col[j], col[j + 1]
+                denom = _np.sqrt(abs(a) ** 2 + abs(bb) ** 2)
+                if denom == 0.0:
+                    cs[j], sn[j] = 1.0, 0.0
+                else:
+                    cs[j] = _np.conj(a) / denom
+                    sn[j] = _np.conj(bb) / denom
+                col[j] = denom
+                col[j + 1] = 0.0
+                H[:, j] = col
+                g[j + 1] = -_np.conj(sn[j]) * g[j]
+                g[j] = cs[j] * g[j]
+                iterations += 1
+                j_done = j + 1
+                res = abs(g[j + 1])
+                residuals.append(res / bnorm)
+                if callback is not None:
+                    callback(res / bnorm)
+                if res <= tol * bnorm or hn == 0.0 or iterations >= maxiter:
+                    converged = res <= tol * bnorm or hn == 0.0
+                    stop = True
+                    break
+            j0 = j1
         # solve the triangular system and update x
         y = _np.zeros(j_done, dtype=_np.complex128)
         for i in range(j_done - 1, -1, -1):
@@ -202,33 +291,27 @@ def gmres_block(matmat, B, tol=1e-5, restart=None, maxiter=None):
     return X, infos, [int(v) for v in iters]
 
 
-def solve_refined(matrix, b, tol=1e-8, inner_tol=1e-4, restart=100, maxiter=2000, max_refinements=20,
-                  inner_dtype=_torch.complex64):
-    """Mixed-precision iterative refinement; returns (x, info dict).
-
-    ``matrix`` is the (complex128) device matrix; the inner solves use a
-    copy in ``inner_dtype``; residuals are formed in complex128.
-    """
+def refine_gmres(matvec, matvec_low, b, tol=1e-8, inner_tol=1e-4, restart=100, maxiter=2000, max_refinements=20,
+                 inner_dtype=_torch.complex64, check_every=1):
+    """Iterative refinement: inner GMRES with ``matvec_low`` (vectors in ``inner_dtype``), corrections
+    and residuals b - A x with ``matvec`` in b's precision; returns (x, info dict)."""
     t0 = _time.perf_counter()
-    low = matrix.to(inner_dtype)
-    b = b.to(matrix.dtype)
     bnorm = _norm(b)
     x = _torch.zeros_like(b)
     r = b.clone()
     history = []
     inner_iterations = []
     for _ in range(max_refinements):
-        res = _norm(r) / bnorm
+        res = _norm(r) / bnorm if bnorm > 0.0 else 0.0
         history.append(res)
         if res <= tol:
             break
-        rl = r.to(inner_dtype)
-        d, info, _, its = gmres_tensor(lambda v: _torch.mv(low, v), rl, tol=inner_tol, restart=restart,
-                                       maxiter=maxiter)
+        d, info, _, its = gmres_tensor(matvec_low, r.to(inner_dtype), tol=inner_tol, restart=restart,
+                                       maxiter=maxiter, check_every=check_every)
         inner_iterations.append(its)
-        x = x + d.to(matrix.dtype)
-        r = b - _torch.mv(matrix, x)
-    _torch.cuda.synchronize() if matrix.is_cuda else None
+        x = x + d.to(b.dtype)
+        r = b - matvec(x)
+    _torch.cuda.synchronize() if b.is_cuda else None
     info = {
         "refinements": len(inner_iterations),
         "inner_iterations": inner_iterations,
@@ -236,6 +319,31 @@ def solve_refined(matrix, b, tol=1e-8, inner_tol=1e-4, restart=100, maxiter=2000
         "converged": history[-1] <= tol,
         "seconds": _time.perf_counter() - t0,
     }
+    return x, info
+
+
+def adjoint_matvec(matrix):
+    """v -> A^H v through the transposed view (a GEMV with the transpose flag on the row-major matrix;
+    the conjugations touch vectors only, not the matrix)."""
+    at = matrix.transpose(0, 1)
+    return lambda v: _torch.mv(at, v.conj_physical()).conj_physical()
+
+
+def solve_refined(matrix, b, tol=1e-8, inner_tol=1e-4, restart=100, maxiter=2000, max_refinements=20,
+                  inner_dtype=_torch.complex64, adjoint=False, check_every=1):
+    """Mixed-precision iterative refinement of A x = b (or A^H x = b); returns (x, info dict).
+
+    ``matrix`` is the (complex128) device matrix; the inner solves use a
+    copy in ``inner_dtype``; residuals are formed in complex128.
+    """
+    low = matrix.to(inner_dtype)
+    b = b.to(matrix.dtype)
+    if adjoint:
+        hi, lo = adjoint_matvec(matrix), adjoint_matvec(low)
+    else:
+        hi, lo = (lambda v: _torch.mv(matrix, v)), (lambda v: _torch.mv(low, v))
+    x, info = refine_gmres(hi, lo, b, tol=tol, inner_tol=inner_tol, restart=restart, maxiter=maxiter,
+                           max_refinements=max_refinements, inner_dtype=inner_dtype, check_every=check_every)
     del low
     return x, info
 

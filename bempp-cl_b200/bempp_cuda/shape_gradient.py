@@ -16,8 +16,9 @@ solve, A^H lambda = F^H u, and
 
 evaluated by ``bemppcuda_shape_adjoint_dp0`` (csrc/shape.cu), which recomputes
 the quadrature of every element pair instead of forming dA/dx.  The dense
-solve is an LU factorisation on the device (torch.linalg), reused for the
-adjoint solve.  The reference has no derivatives; its forward path for this
+solves run on the device: an LU factorisation (torch.linalg) reused for the
+adjoint solve, or GMRES on a complex64 copy of the matrix refined with
+complex128 residuals (the adjoint through the transposed view).  The reference has no derivatives; its forward path for this
 objective is core/dense_assembler.py:49-98 (operators) and
 core/dense_potential_assembler.py:8-40 (far field).
 """
@@ -69,9 +70,10 @@ class ScatteringState(object):
     """What the backward pass needs from one forward evaluation.
 
     Holds either the LU factors (``lu``, ``pivots``) or, for the iterative
-    solver, the matrix itself (``matrix``)."""
+    solvers, the matrix itself (``matrix``) and its complex64 copy (``low``,
+    refined GMRES)."""
 
-    def __init__(self, geometry, lu, pivots, phi, u, farfield, matrix=None, iterations=None):
+    def __init__(self, geometry, lu, pivots, phi, u, farfield, matrix=None, iterations=None, low=None):
         self.geometry = geometry
         self.lu = lu
         self.pivots = pivots
@@ -80,6 +82,7 @@ class ScatteringState(object):
         self.farfield = farfield
         self.matrix = matrix
         self.iterations = iterations
+        self.low = low
 
 
 class FarFieldObjective(object):
@@ -87,13 +90,14 @@ class FarFieldObjective(object):
 
     def __init__(self, grid, directions=None, incident=(0.0, 0.0, 1.0), parameters=None, solver="lu", tol=1e-12):
         """``solver``: "lu" (dense complex128 LU on the device, factors reused for
-        the adjoint solve), "lu32" (complex64 LU, refined with complex128
+        the adjoint solve), "gmres32" (GMRES on a complex64 copy of the matrix,
+        refined with complex128 residuals, for both solves), "lu32" (complex64 LU, refined with complex128
         residuals b - A x of the FP64 matrix until ||b - A x|| <= tol ||b||; the
         same factors and refinement for the adjoint) or "gmres" (device GMRES on
         the resident matrix to relative residual ``tol`` for both solves)."""
         require_cuda()
-        if solver not in ("lu", "lu32", "gmres"):
-            raise ValueError("solver must be 'lu', 'lu32' or 'gmres'")
+        if solver not in ("lu", "lu32", "gmres", "gmres32"):
+            raise ValueError("solver must be 'lu', 'lu32', 'gmres' or 'gmres32'")
         self.solver = solver
         self.tol = float(tol)
         self.grid = grid
@@ -186,10 +190,21 @@ class FarFieldObjective(object):
     def _gmres(self, matvec, rhs):
         from .linalg import gmres_tensor
 
-        x, info, res, its = gmres_tensor(matvec, rhs, tol=self.tol, restart=300, maxiter=3000)
+        x, info, res, its = gmres_tensor(matvec, rhs, tol=self.tol, restart=300, maxiter=3000, check_every=16,
+                                         graph=True)
         if info != 0:
             raise RuntimeError("GMRES did not reach %g in %d iterations (last residual %g)" % (self.tol, its, res[-1]))
         return x, its
+
+    def _gmres32(self, matvec, matvec_low, rhs):
+        """Inner GMRES on the complex64 copy, complex128 residuals, to relative residual ``tol``."""
+        from .linalg import refine_gmres
+
+        x, info = refine_gmres(matvec, matvec_low, rhs, tol=self.tol, inner_tol=1e-5, restart=300, maxiter=3000,
+                               check_every=16)
+        if not info["converged"]:
+            raise RuntimeError("refined GMRES did not reach %g (residuals %s)" % (self.tol, info["relative_residuals"]))
+        return x, sum(info["inner_iterations"])
 
     def _refine(self, lu, pivots, matvec, rhs, adjoint=False, max_steps=20):
         """Solve with complex64 factors and complex128 residuals; returns (x, steps)."""
@@ -219,6 +234,10 @@ class FarFieldObjective(object):
             matrix = a
             lu, pivots = _torch.linalg.lu_factor(a.to(_torch.complex64))
             phi, its = self._refine(lu, pivots, lambda v: _torch.mv(matrix, v), b)
+        elif solver == "gmres32":
+            matrix = a
+            low = a.to(_torch.complex64)
+            phi, its = self._gmres32(lambda v: _torch.mv(matrix, v), lambda v: _torch.mv(low, v), b)
         else:
             matrix = a
             phi, its = self._gmres(lambda v: _torch.mv(matrix, v), b)
@@ -226,7 +245,9 @@ class FarFieldObjective(object):
         u = farfield @ phi
         value = (u.real ** 2 + u.imag ** 2).sum()
         if keep:
-            return value, ScatteringState(geometry, lu, pivots, phi, u, farfield, matrix, its)
+            # the complex64 copy (gmres32) serves the adjoint solve too
+            return value, ScatteringState(geometry, lu, pivots, phi, u, farfield, matrix, its,
+                                          low if solver == "gmres32" else None)
         return value
 
     def adjoint(self, state):
@@ -238,8 +259,12 @@ class FarFieldObjective(object):
             return lam
         if state.lu is not None:
             return _torch.linalg.lu_solve(state.lu, state.pivots, rhs.unsqueeze(1), adjoint=True).squeeze(1)
-        ah = state.matrix.mH
-        lam, its = self._gmres(lambda v: _torch.mv(ah, v), rhs)
+        from .linalg import adjoint_matvec
+
+        if getattr(state, "low", None) is not None:
+            lam, its = self._gmres32(adjoint_matvec(state.matrix), adjoint_matvec(state.low), rhs)
+            return lam
+        lam, its = self._gmres(adjoint_matvec(state.matrix), rhs)
         return lam
 
     def gradient(self, state, k, lam=None, scales=(-2.0, 2.0, 2.0)):

@@ -82,6 +82,7 @@ def parse():
     ap.add_argument("--skip-fd", action="store_true")
     ap.add_argument("--skip-breadth", action="store_true")
     ap.add_argument("--shape-level", type=int, default=5)
+    ap.add_argument("--shape-solver", choices=["lu32", "gmres", "gmres32"], default="lu32")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time per baseline sample")
     return ap.parse_args()
 
@@ -602,7 +603,8 @@ def shape_measure(args, torch):
     from bempp_cuda.shapes import perturbed_sphere
 
     grid, _ = perturbed_sphere(args.shape_level, seed=0)
-    obj = FarFieldObjective(grid, solver="lu32", tol=1e-12)
+    solver = args.shape_solver
+    obj = FarFieldObjective(grid, solver=solver, tol=1e-12)
     k = 6.0
     x0 = obj.vertices.clone()
     names = ("geometry", "assembly", "solve", "farfield", "adjoint_solve", "adjoint_kernels")
@@ -620,15 +622,26 @@ def shape_measure(args, torch):
         a = obj.assemble(geo, k)
         mark(2)
         b = obj.rhs(geo, k)
-        lu, piv = torch.linalg.lu_factor(a.to(torch.complex64))
-        phi, its = obj._refine(lu, piv, lambda v: torch.mv(a, v), b)
-        iters["forward_refinements"] = its
+        if solver == "lu32":
+            lu, piv = torch.linalg.lu_factor(a.to(torch.complex64))
+            phi, its = obj._refine(lu, piv, lambda v: torch.mv(a, v), b)
+            low = None
+            iters["forward_refinements"] = its
+        elif solver == "gmres32":
+            lu = piv = None
+            low = a.to(torch.complex64)
+            phi, its = obj._gmres32(lambda v: torch.mv(a, v), lambda v: torch.mv(low, v), b)
+            iters["forward_inner_iterations"] = its
+        else:  # gmres
+            lu = piv = low = None
+            phi, its = obj._gmres(lambda v: torch.mv(a, v), b)
+            iters["forward_iterations"] = its
         mark(3)
         ff = obj.farfield_matrix(geo, k)
         u = ff @ phi
         value = (u.real ** 2 + u.imag ** 2).sum()
         mark(4)
-        state = ScatteringState(geo, lu, piv, phi, u, ff, a, its)
+        state = ScatteringState(geo, lu, piv, phi, u, ff, a, its, low)
         lam = obj.adjoint(state)
         mark(5)
         vgrad, kgrad = obj.gradient(state, k, lam=lam)
@@ -656,8 +669,13 @@ def shape_measure(args, torch):
            "adjoint_kernels_over_forward_assembly": parts["adjoint_kernels"] / parts["assembly"],
            "backward_over_forward": (parts["adjoint_solve"] + parts["adjoint_kernels"])
            / (parts["geometry"] + parts["assembly"] + parts["solve"] + parts["farfield"]),
-           "solver": "complex64 LU (cuSOLVER via torch) refined with complex128 residuals of the FP64 matrix to "
-                     "relative residual 1e-12; the adjoint reuses the factors",
+           "solver": ("complex64 LU (cuSOLVER via torch) refined with complex128 residuals of the FP64 matrix to "
+                      "relative residual 1e-12; the adjoint reuses the factors") if solver == "lu32" else
+                     ("GMRES on a complex64 copy of the matrix (inner tolerance 1e-5) refined with complex128 "
+                      "residuals of the FP64 matrix to relative residual 1e-12, forward and adjoint (transposed "
+                      "view)") if solver == "gmres32" else
+                     ("GMRES on the complex128 matrix to relative residual 1e-12, forward and adjoint (transposed "
+                      "view); each Arnoldi step one CUDA-graph replay, convergence checked every 16 steps"),
            "refinements": dict(iters),
            "J": float(value.item())}
     if not args.skip_fd:

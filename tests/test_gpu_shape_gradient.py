@@ -190,13 +190,15 @@ def test_gmres_solver_gives_the_lu_gradient():
     assert s2.iterations is not None and s2.iterations > 0
 
 
-def test_lu32_refined_solver_gives_the_lu_gradient():
+@pytest.mark.parametrize("solver", ["lu32", "gmres32"])
+def test_refined_solvers_give_the_lu_gradient(solver):
+    """complex64 LU or complex64 GMRES (adjoint through the transposed view), refined in complex128."""
     from bempp_cuda.shape_gradient import FarFieldObjective, fibonacci_directions
     from bempp_cuda.shapes import perturbed_sphere
 
     grid, _ = perturbed_sphere(3, seed=6)
     lu = FarFieldObjective(grid, directions=fibonacci_directions(32))
-    lo = FarFieldObjective(grid, directions=fibonacci_directions(32), solver="lu32", tol=1e-13)
+    lo = FarFieldObjective(grid, directions=fibonacci_directions(32), solver=solver, tol=1e-13)
     v1, s1 = lu.evaluate(lu.vertices, 6.0, keep=True)
     v2, s2 = lo.evaluate(lo.vertices, 6.0, keep=True)
     g1, k1 = lu.gradient(s1, 6.0)

@@ -98,3 +98,33 @@ def test_block_gmres_eight_rhs_on_device():
     X, infos, iters = gmres_block(lambda V: a @ V, B, tol=1e-9, restart=60)
     assert infos == [0] * 8
     assert (torch.linalg.norm(a @ X - B) / torch.linalg.norm(B)).item() < 1e-8
+
+
+@pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64, torch.float64])
+@pytest.mark.parametrize("restart", [10, 200])
+def test_graph_arnoldi_matches_host_driven_gmres(dtype, restart):
+    """Arnoldi steps replayed from one CUDA graph (checked every 7 steps) = the step-by-step loop, with
+    restarts, for complex and real systems; and the adjoint through the transposed view."""
+    from bempp_cuda.linalg import adjoint_matvec, gmres_tensor
+
+    rng = np.random.default_rng(12)
+    n = 300
+    a = np.eye(n) * 4 + rng.standard_normal((n, n)) / np.sqrt(n)
+    b = rng.standard_normal(n)
+    if dtype.is_complex:
+        a = a + 1j * rng.standard_normal((n, n)) / np.sqrt(n)
+        b = b + 1j * rng.standard_normal(n)
+    A = torch.as_tensor(a, device="cuda").to(dtype)
+    bt = torch.as_tensor(b, device="cuda").to(dtype)
+    tol = 1e-5 if dtype == torch.complex64 else 1e-11
+    ref = gmres_tensor(lambda v: torch.mv(A, v), bt, tol=tol, restart=restart, maxiter=3000)
+    got = gmres_tensor(lambda v: torch.mv(A, v), bt, tol=tol, restart=restart, maxiter=3000, check_every=7,
+                       graph=True)
+    assert got[1] == ref[1] == 0 and got[3] == ref[3]
+    rtol = 1e-4 if dtype == torch.complex64 else 1e-9
+    assert torch.allclose(got[0], ref[0], rtol=rtol, atol=rtol * float(ref[0].abs().max()))
+    if dtype == torch.complex128:
+        adj = gmres_tensor(adjoint_matvec(A), bt, tol=1e-11, restart=restart, maxiter=3000, check_every=7, graph=True)
+        x = np.linalg.solve(a.conj().T, b)
+        assert adj[1] == 0
+        assert np.linalg.norm(adj[0].cpu().numpy() - x) <= 1e-9 * np.linalg.norm(x)

@@ -28,6 +28,33 @@ def test_gmres_matches_direct_solve(restart):
     assert res[-1] <= 1e-10 and its > 0
 
 
+@pytest.mark.parametrize("check_every", [3, 8, 50])
+@pytest.mark.parametrize("restart", [7, 200])
+def test_deferred_checks_give_the_same_iterate(check_every, restart):
+    """Arnoldi steps checked in chunks: same iterate, residual history and count as checking every step
+    (the extra steps of the last chunk are discarded); also with a restart length that is not a multiple."""
+    A, b, _, _ = _system(120, 9)
+    ref = gmres_tensor(lambda v: A @ v, b, tol=1e-10, restart=restart, maxiter=2000)
+    got = gmres_tensor(lambda v: A @ v, b, tol=1e-10, restart=restart, maxiter=2000, check_every=check_every)
+    assert got[1] == ref[1] == 0 and got[3] == ref[3]
+    assert np.allclose(got[2], ref[2], rtol=1e-10, atol=1e-14)
+    assert torch.allclose(got[0], ref[0], rtol=1e-12, atol=1e-14)
+
+
+def test_deferred_checks_respect_maxiter():
+    A, b, _, _ = _system(60, 10)
+    x, info, res, its = gmres_tensor(lambda v: A @ v, b, tol=1e-30, restart=20, maxiter=13, check_every=5)
+    assert info == 13 and its == 13 and len(res) == 14
+
+
+def test_adjoint_refinement():
+    A, b, a, bn = _system(100, 11)
+    x, info = solve_refined(A, b, tol=1e-12, inner_tol=1e-4, adjoint=True)
+    assert info["converged"]
+    ref = np.linalg.solve(a.conj().T, bn)
+    assert np.linalg.norm(x.numpy() - ref) <= 1e-10 * np.linalg.norm(ref)
+
+
 def test_gmres_real_system():
     rng = np.random.default_rng(3)
     a = np.eye(50) * 3 + rng.standard_normal((50, 50)) / 10
