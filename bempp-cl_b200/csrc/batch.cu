@@ -168,31 +168,16 @@ __global__ void __launch_bounds__(32 * SB_WARPS) singular_batch(const BatchDev *
     const double2 *tp = reinterpret_cast<const double2 *>(tab.tp), *sp = reinterpret_cast<const double2 *>(tab.sp);
     const int64_t toff = tab.toff[k], soff = tab.soff[k], woff = tab.woff[k];
     const int n = (int)tab.npts[k];
-    if (P.ck) {
-        // complex wavenumber: Green's function at every point
-        double are = 0.0, aim = 0.0;
-        for (int m = lane; m < n; m += 32) {
-            const double2 tpm = tp[toff + m], spm = sp[soff + m];
-            const double w = __ldg(tab.w + woff + m);
-            double x[3], y[3];
-            to_global(gt, tpm.x, tpm.y, x);
-            to_global(gs, spm.x, spm.y, y);
-            const cplx kv = greens<K>(x, y, gt.n, gs.n, prm.p);
-            are = fma(kv.re, w, are);
-            aim = fma(kv.im, w, aim);
-        }
-        vr = warp_sum(are);
-        vi = warp_sum(aim);
-    } else {
-        if (P.phase_class == 2)
-            sing_dp0_value<K, 2>(prm.tg, prm.tne, t, s, gt, gs, prm.p, tp, sp, tab.w, toff, soff, woff, n, &vr, &vi);
-        else if (P.phase_class == 1)
-            sing_dp0_value<K, 1>(prm.tg, prm.tne, t, s, gt, gs, prm.p, tp, sp, tab.w, toff, soff, woff, n, &vr, &vi);
-        else
-            sing_dp0_value<K, 0>(prm.tg, prm.tne, t, s, gt, gs, prm.p, tp, sp, tab.w, toff, soff, woff, n, &vr, &vi);
-        vr *= BC_INV_4PI;
-        vi *= BC_INV_4PI;
-    }
+    if (P.ck)
+        sing_dp0_value<K, 3>(prm.tg, prm.tne, t, s, gt, gs, prm.p, tp, sp, tab.w, toff, soff, woff, n, &vr, &vi);
+    else if (P.phase_class == 2)
+        sing_dp0_value<K, 2>(prm.tg, prm.tne, t, s, gt, gs, prm.p, tp, sp, tab.w, toff, soff, woff, n, &vr, &vi);
+    else if (P.phase_class == 1)
+        sing_dp0_value<K, 1>(prm.tg, prm.tne, t, s, gt, gs, prm.p, tp, sp, tab.w, toff, soff, woff, n, &vr, &vi);
+    else
+        sing_dp0_value<K, 0>(prm.tg, prm.tne, t, s, gt, gs, prm.p, tp, sp, tab.w, toff, soff, woff, n, &vr, &vi);
+    vr *= BC_INV_4PI;
+    vi *= BC_INV_4PI;
     if (lane == 0) {
         const double scale = gt.ie * gs.ie;
         vr *= scale;

@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(32 * SING_WARPS) singular_pairs(SingParams prm
     }
 }
 
-// DP0 scalar kernels with a real wavenumber (singular_dp0.cuh).
+// DP0 scalar kernels (singular_dp0.cuh).
 template <int K, int PHC>
 __global__ void __launch_bounds__(32 * SING_WARPS) singular_dp0(SingParams prm) {
     const int lane = threadIdx.x & 31;
@@ -287,12 +287,18 @@ __global__ void __launch_bounds__(32 * SING_WARPS) singular_dp0(SingParams prm) 
 template <int K>
 static cudaError_t launch_sing_dp0(const SingParams &prm, int phase_class, cudaStream_t st) {
     const unsigned blocks = (unsigned)((prm.npairs + SING_WARPS - 1) / SING_WARPS);
-    if (phase_class == 2)
-        singular_dp0<K, 2><<<blocks, 32 * SING_WARPS, 0, st>>>(prm);
-    else if (phase_class == 1)
-        singular_dp0<K, 1><<<blocks, 32 * SING_WARPS, 0, st>>>(prm);
-    else
+    if constexpr (!SingDp0Traits<K>::helm) {  // no phase: one instance
         singular_dp0<K, 0><<<blocks, 32 * SING_WARPS, 0, st>>>(prm);
+    } else {
+        if (phase_class == 3)  // complex wavenumber
+            singular_dp0<K, 3><<<blocks, 32 * SING_WARPS, 0, st>>>(prm);
+        else if (phase_class == 2)
+            singular_dp0<K, 2><<<blocks, 32 * SING_WARPS, 0, st>>>(prm);
+        else if (phase_class == 1)
+            singular_dp0<K, 1><<<blocks, 32 * SING_WARPS, 0, st>>>(prm);
+        else
+            singular_dp0<K, 0><<<blocks, 32 * SING_WARPS, 0, st>>>(prm);
+    }
     return cudaGetLastError();
 }
 
@@ -343,10 +349,11 @@ int bc_singular_launch(const bemppcuda_singular_args *a, cudaStream_t st) {
     cudaError_t err = cudaSuccess;
     const bool real_k = a->params[1] == 0.0;
     if (a->assembly == BEMPPCUDA_ASM_SCALAR && prm.nt == 1 && prm.ns == 1 &&
-        (a->kernel <= BEMPPCUDA_HELMHOLTZ_ADLP || a->kernel == BEMPPCUDA_HELMHOLTZ_COMBINED) &&
-        (real_k || a->kernel <= BEMPPCUDA_LAPLACE_ADLP)) {
+        (a->kernel <= BEMPPCUDA_MODHELM_ADLP || a->kernel == BEMPPCUDA_HELMHOLTZ_COMBINED)) {
+        // a complex wavenumber takes phase class 3 (no centroid factoring)
         const double theta = fabs(a->params[0]) * a->phase_radius;
-        const int phase_class = a->phase_radius > 0.0 ? (theta <= 0.5 ? 2 : (theta <= 1.0 ? 1 : 0)) : 0;
+        const int phase_class = !real_k ? 3
+                                : a->phase_radius > 0.0 ? (theta <= 0.5 ? 2 : (theta <= 1.0 ? 1 : 0)) : 0;
         switch (a->kernel) {
         case BEMPPCUDA_LAPLACE_SLP: err = launch_sing_dp0<BEMPPCUDA_LAPLACE_SLP>(prm, 0, st); break;
         case BEMPPCUDA_LAPLACE_DLP: err = launch_sing_dp0<BEMPPCUDA_LAPLACE_DLP>(prm, 0, st); break;
@@ -354,6 +361,9 @@ int bc_singular_launch(const bemppcuda_singular_args *a, cudaStream_t st) {
         case BEMPPCUDA_HELMHOLTZ_SLP: err = launch_sing_dp0<BEMPPCUDA_HELMHOLTZ_SLP>(prm, phase_class, st); break;
         case BEMPPCUDA_HELMHOLTZ_DLP: err = launch_sing_dp0<BEMPPCUDA_HELMHOLTZ_DLP>(prm, phase_class, st); break;
         case BEMPPCUDA_HELMHOLTZ_ADLP: err = launch_sing_dp0<BEMPPCUDA_HELMHOLTZ_ADLP>(prm, phase_class, st); break;
+        case BEMPPCUDA_MODHELM_SLP: err = launch_sing_dp0<BEMPPCUDA_MODHELM_SLP>(prm, 0, st); break;
+        case BEMPPCUDA_MODHELM_DLP: err = launch_sing_dp0<BEMPPCUDA_MODHELM_DLP>(prm, 0, st); break;
+        case BEMPPCUDA_MODHELM_ADLP: err = launch_sing_dp0<BEMPPCUDA_MODHELM_ADLP>(prm, 0, st); break;
         default: err = launch_sing_dp0<BEMPPCUDA_HELMHOLTZ_COMBINED>(prm, phase_class, st); break;
         }
         if (err != cudaSuccess) {

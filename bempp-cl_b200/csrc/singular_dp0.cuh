@@ -1,9 +1,12 @@
-// Singular (adjacent) DP0 pairs of the scalar kernels with a real
-// wavenumber: the 3 x 3 local block reduces to one value, and exp(ikr) is
-// factored about the centroid distance r_c as in the regular DP0 kernels: for
-// any x in element i and y in element j, |r - r_c| <= R_i + R_j, so phase
-// class PHC (|k|(R_i + R_j) <= 1 or 1/2) bounds the per-point phase offset
-// for adjacent pairs as well.  One warp per pair, lanes over the points.
+// Singular (adjacent) DP0 pairs of the scalar kernels: the 3 x 3 local block
+// reduces to one value, and for a real wavenumber exp(ikr) is factored about
+// the centroid distance r_c as in the regular DP0 kernels: for any x in
+// element i and y in element j, |r - r_c| <= R_i + R_j, so phase class PHC
+// (|k|(R_i + R_j) <= 1 or 1/2) bounds the per-point phase offset for adjacent
+// pairs as well.  PHC 3 is a complex wavenumber k = kr + i ki (exp(i kr r)
+// exp(-ki r) per point, (ikr - 1) / r = -(1/r + ki) + i kr); modified
+// Helmholtz (real, w = p[0]) scales the Laplace sums by exp(-w r) or
+// exp(-w r) (1 + w r).  One warp per pair, lanes over the points.
 // Used by the single-problem singular kernel and the batched one.
 #pragma once
 
@@ -15,12 +18,21 @@ template <int K>
 struct SingDp0Traits {
     static constexpr bool helm = (K == BEMPPCUDA_HELMHOLTZ_SLP || K == BEMPPCUDA_HELMHOLTZ_DLP ||
                                   K == BEMPPCUDA_HELMHOLTZ_ADLP || K == BEMPPCUDA_HELMHOLTZ_COMBINED);
+    static constexpr bool mh = (K == BEMPPCUDA_MODHELM_SLP || K == BEMPPCUDA_MODHELM_DLP ||
+                                K == BEMPPCUDA_MODHELM_ADLP);
     static constexpr bool sl = (K == BEMPPCUDA_LAPLACE_SLP || K == BEMPPCUDA_HELMHOLTZ_SLP ||
-                                K == BEMPPCUDA_HELMHOLTZ_COMBINED);
+                                K == BEMPPCUDA_MODHELM_SLP || K == BEMPPCUDA_HELMHOLTZ_COMBINED);
     static constexpr bool dl = (K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_HELMHOLTZ_DLP ||
-                                K == BEMPPCUDA_HELMHOLTZ_COMBINED);
-    static constexpr bool ad = (K == BEMPPCUDA_LAPLACE_ADLP || K == BEMPPCUDA_HELMHOLTZ_ADLP);
+                                K == BEMPPCUDA_MODHELM_DLP || K == BEMPPCUDA_HELMHOLTZ_COMBINED);
+    static constexpr bool ad = (K == BEMPPCUDA_LAPLACE_ADLP || K == BEMPPCUDA_HELMHOLTZ_ADLP ||
+                                K == BEMPPCUDA_MODHELM_ADLP);
 };
+
+// exp(-w r) for the single layer, exp(-w r) (1 + w r) for the double layers (modified Helmholtz)
+__device__ __forceinline__ void mh_factors(double w, double r, double *e, double *e1) {
+    *e = exp(-w * r);
+    *e1 = *e * fma(w, r, 1.0);
+}
 
 // Kernel sum of one adjacent pair over its Sauter-Schwab points, without the
 // integration elements and 1/(4 pi); every lane returns the warp total.
@@ -32,9 +44,10 @@ __device__ __forceinline__ void sing_dp0_value(const double *__restrict__ g, int
                                                const double *__restrict__ w, int64_t toff, int64_t soff,
                                                int64_t woff, int n, double *vr_out, double *vi_out) {
     using T = SingDp0Traits<K>;
-    constexpr bool PH = T::helm && PHC > 0;
+    constexpr bool PH = T::helm && (PHC == 1 || PHC == 2);
+    constexpr bool CK = T::helm && PHC == 3;
     const int lane = threadIdx.x & 31;
-    const double kr = p[0];
+    const double kr = p[0], ki = CK ? p[1] : 0.0;
     double rc = 0.0;
     if (PH) {
         const double D0 = __ldg(g + 22 * ne + s) - __ldg(g + 22 * ne + t);
@@ -58,8 +71,10 @@ __device__ __forceinline__ void sing_dp0_value(const double *__restrict__ g, int
         double dot = 0.0;
         if (T::dl || T::ad) dot = (T::ad ? -1.0 : 1.0) * fma(d2, nv[2], fma(d1, nv[1], d0 * nv[0]));
         if (!T::helm) {
-            if (T::sl) s0r += f;
-            if (T::dl || T::ad) s1r = fma(f * dot, rinv * rinv, s1r);
+            double e = 1.0, e1 = 1.0;
+            if (T::mh) mh_factors(kr, r2 * rinv, &e, &e1);
+            if (T::sl) s0r = T::mh ? fma(f, e, s0r) : s0r + f;
+            if (T::dl || T::ad) s1r = fma(f * dot * (T::mh ? e1 : 1.0), rinv * rinv, s1r);
         } else {
             const double r = r2 * rinv;
             double sn, cs;
@@ -69,15 +84,20 @@ __device__ __forceinline__ void sing_dp0_value(const double *__restrict__ g, int
                 sincos_small64(kr * (r - rc), &sn, &cs);
             else
                 sincos_cw64(kr * r, &sn, &cs);
+            if (CK) {
+                const double am = exp(-ki * r);
+                sn *= am;
+                cs *= am;
+            }
             if (T::sl) {
                 s0r = fma(f, cs, s0r);
                 s0i = fma(f, sn, s0i);
             }
             if (T::dl || T::ad) {
                 // (ikr - 1) e^{ikr} (dot) / r^3 = g (-h1 + i h2), g = f dot / r
-                const double gg = f * dot * rinv;
-                s1r = fma(gg, fma(rinv, cs, kr * sn), s1r);
-                s1i = fma(gg, fma(kr, cs, -rinv * sn), s1i);
+                const double gg = f * dot * rinv, rk = rinv + ki;
+                s1r = fma(gg, fma(rk, cs, kr * sn), s1r);
+                s1i = fma(gg, fma(kr, cs, -rk * sn), s1i);
             }
         }
     }
@@ -89,7 +109,7 @@ __device__ __forceinline__ void sing_dp0_value(const double *__restrict__ g, int
     }
     // SLP s0; Laplace DLP -s1r; Helmholtz DLP -s1r + i s1i; combined eta s0 + DLP
     double vr = 0.0, vi = 0.0;
-    if (K == BEMPPCUDA_LAPLACE_SLP || K == BEMPPCUDA_HELMHOLTZ_SLP) {
+    if (T::sl && K != BEMPPCUDA_HELMHOLTZ_COMBINED) {
         vr = s0r;
         vi = s0i;
     } else if (K == BEMPPCUDA_HELMHOLTZ_COMBINED) {
@@ -123,10 +143,11 @@ __device__ __forceinline__ void sing_dp0_pair(const double *__restrict__ g, int6
                                               int64_t woff, int n, double *vr_out, double *vi_out,
                                               double *ur_out, double *ui_out) {
     using T = SingDp0Traits<K>;
-    constexpr bool PH = T::helm && PHC > 0;
+    constexpr bool PH = T::helm && (PHC == 1 || PHC == 2);
+    constexpr bool CK = T::helm && PHC == 3;
     constexpr bool NORMAL = T::dl || T::ad;
     const int lane = threadIdx.x & 31;
-    const double kr = p[0];
+    const double kr = p[0], ki = CK ? p[1] : 0.0;
     double rc = 0.0;
     if (PH) {
         const double D0 = __ldg(g + 22 * ne + s) - __ldg(g + 22 * ne + t);
@@ -156,9 +177,11 @@ __device__ __forceinline__ void sing_dp0_pair(const double *__restrict__ g, int6
             dot2 = T::ad ? dns : -dnt;
         }
         if (!T::helm) {
-            if (T::sl) s0r += f;
+            double e = 1.0, e1 = 1.0;
+            if (T::mh) mh_factors(kr, r2 * rinv, &e, &e1);
+            if (T::sl) s0r = T::mh ? fma(f, e, s0r) : s0r + f;
             if (NORMAL) {
-                const double f3 = f * rinv * rinv;
+                const double f3 = f * rinv * rinv * (T::mh ? e1 : 1.0);
                 s1r = fma(f3, dot1, s1r);
                 s2r = fma(f3, dot2, s2r);
             }
@@ -171,13 +194,18 @@ __device__ __forceinline__ void sing_dp0_pair(const double *__restrict__ g, int6
                 sincos_small64(kr * (r - rc), &sn, &cs);
             else
                 sincos_cw64(kr * r, &sn, &cs);
+            if (CK) {
+                const double am = exp(-ki * r);
+                sn *= am;
+                cs *= am;
+            }
             if (T::sl) {
                 s0r = fma(f, cs, s0r);
                 s0i = fma(f, sn, s0i);
             }
             if (NORMAL) {
-                const double fr = f * rinv;
-                const double h1 = fma(rinv, cs, kr * sn), h2 = fma(kr, cs, -rinv * sn);
+                const double fr = f * rinv, rk = rinv + ki;
+                const double h1 = fma(rk, cs, kr * sn), h2 = fma(kr, cs, -rk * sn);
                 const double g1 = fr * dot1, g2 = fr * dot2;
                 s1r = fma(g1, h1, s1r);
                 s1i = fma(g1, h2, s1i);
@@ -201,7 +229,7 @@ __device__ __forceinline__ void sing_dp0_pair(const double *__restrict__ g, int6
 #pragma unroll
     for (int o = 0; o < 2; ++o) {
         double vr = 0.0, vi = 0.0;
-        if (K == BEMPPCUDA_LAPLACE_SLP || K == BEMPPCUDA_HELMHOLTZ_SLP) {
+        if (T::sl && K != BEMPPCUDA_HELMHOLTZ_COMBINED) {
             vr = s0r;
             vi = s0i;
         } else if (K == BEMPPCUDA_HELMHOLTZ_COMBINED) {

@@ -195,6 +195,32 @@ def test_dp0_complex_wavenumber_against_oracle(oracle, name, k):
         assert np.linalg.norm(got - ref) <= 1e-12 * np.linalg.norm(ref), (name, k, sym)
 
 
+@pytest.mark.parametrize("name", ["single_layer", "double_layer", "adjoint_double_layer"])
+@pytest.mark.parametrize("omega", [1.5, 5.0])
+def test_dp0_modified_helmholtz_against_oracle(oracle, name, omega):
+    """DP0 modified Helmholtz: symmetric sweep and per-pair evaluation, DP0 singular routine, against the oracle."""
+    from cases import oracle_dense
+
+    from bempp_cuda import operators
+    from bempp_cuda.assembly import regular_into, singular_into_dense
+    from bempp_cuda.operators import Parameters
+    from bempp_cuda.shapes import ellipsoid
+    from bempp_cuda.space import function_space
+
+    grid = ellipsoid(3, 1.1, 0.9, 1.0)
+    sp = function_space(grid, "DP", 0)
+    op = getattr(operators.boundary.modified_helmholtz, name)(sp, sp, sp, omega)
+    ref = oracle_dense(oracle, op, sp, sp)
+    d = op.descriptor
+    n = sp.global_dof_count
+    for sym in (True, False):
+        a = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+        regular_into(a, d, sp, sp, Parameters(), symmetric=sym)
+        singular_into_dense(a, d, sp, sp, Parameters())
+        got = a.cpu().numpy()
+        assert np.linalg.norm(got - ref) <= 1e-12 * np.linalg.norm(ref), (name, omega, sym)
+
+
 @pytest.mark.parametrize("name", ["single_layer", "double_layer", "adjoint_double_layer", "hypersingular"])
 @pytest.mark.parametrize("omega", [1.5, 6.0])
 def test_modified_helmholtz_p1_kernel_against_oracle(oracle, name, omega):
