@@ -387,12 +387,16 @@ def potential_workspace_bytes(args):
     return int(_lib.load().bemppcuda_potential_workspace_bytes(args))
 
 
-def evaluate_potential_device(space, descriptor, points, local_coefficients, parameters, stream=None):
+def evaluate_potential_device(space, descriptor, points, local_coefficients, parameters, stream=None,
+                              precision=_lib.FP64):
     """Potential (kdim, npoints) complex128 device tensor.
 
     ``local_coefficients`` are the element-local coefficients (nshape * ne,)
     complex128, i.e. ``space.map_to_full_grid @ x`` of the reference
     (dense_potential_assembler.py:30-34); ``points`` is a (3, npoints) array.
+    ``precision=MIXED`` evaluates the point-source pairs of Laplace and
+    Helmholtz (real k) single / double layer potentials in FP32; other
+    potentials then run in FP64.
     """
     require_cuda()
     kernel, assembly = kernel_ids(descriptor)
@@ -411,7 +415,6 @@ def evaluate_potential_device(space, descriptor, points, local_coefficients, par
     args = _lib.PotentialArgs()
     args.kernel = kernel
     args.assembly = assembly
-    args.precision = _lib.FP64
     _set_params(args, descriptor.options)
     args.grid = dgrid.record()
     args.space = dspace.record()
@@ -427,5 +430,11 @@ def evaluate_potential_device(space, descriptor, points, local_coefficients, par
     args.workspace = ptr(workspace)
     args.workspace_bytes = need
     args.phase_radius = 1.0001 * dgrid.radius
-    _lib.check(_lib.load().bemppcuda_evaluate_potential(args, stream or current_stream()))
+    args.precision = precision
+    lib = _lib.load()
+    rc = lib.bemppcuda_evaluate_potential(args, stream or current_stream())
+    if rc == _lib.ERR_UNSUPPORTED and precision == _lib.MIXED:
+        args.precision = _lib.FP64  # no mixed kernel for this potential
+        rc = lib.bemppcuda_evaluate_potential(args, stream or current_stream())
+    _lib.check(rc)
     return result

@@ -545,7 +545,10 @@ class PotentialOperator(object):
         from .assembly import evaluate_potential_device
 
         local = self.space.map_to_full_grid @ _np.asarray(coefficients)
-        return evaluate_potential_device(self.space, self.descriptor, self.points, local, self.parameters)
+        from .assembly import precision_of
+
+        return evaluate_potential_device(self.space, self.descriptor, self.points, local, self.parameters,
+                                         precision=precision_of(self.device_interface))
 
     def evaluate(self, grid_fun):
         coeffs = getattr(grid_fun, "coefficients", grid_fun)

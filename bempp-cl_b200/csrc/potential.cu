@@ -18,7 +18,7 @@
 //     point in FP64 and combine with xor-shuffle reductions; lane 0 writes.
 #include <algorithm>
 
-#include "common.cuh"
+#include "dp0.cuh"  // common.cuh, and the packed FP32 helpers of the mixed kernels
 
 namespace bc {
 
@@ -414,6 +414,161 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar(PotParams prm, in
     }
 }
 
+// Mixed precision (FP32 point-source pairs): Laplace and Helmholtz (real k)
+// single / double layer potentials.  Lengths are in units of 1/kappa
+// (kappa = k, or 1 for Laplace).  Per (evaluation point, source element) in
+// FP64: D = kappa (c_e - x), r_c' = |D| and exp(i r_c'); per source in FP32:
+// yo = kappa (y_q - c_e), |yo|^2 and yo . n_e; per pair in FP32:
+//   r'^2 - r_c'^2 = |yo|^2 + 2 D . yo,  theta = (r'^2 - r_c'^2) / (r' + r_c'),
+// 1/r' by rsqrt.approx, sin / cos of theta by the fitted polynomials (phase
+// class PHC bounds |theta| <= kappa R), and the complex product with the
+// source coefficient; the thread's two evaluation points travel together in
+// packed f32x2 operations.  The six-term sums per element are FP32; exp(i r_c'),
+// kappa (single layer) or kappa^2 (double layer) and the sum over elements are
+// FP64.  Single layer e^{ikr}/r = kappa e^{i theta} e^{i r_c'} / r'; double
+// layer (ikr - 1) e^{ikr} (d . n) / r^3 = kappa^2 (i r' - 1) e^{i theta}
+// e^{i r_c'} (d' . n) / r'^3 with d' = D + yo.
+template <int K, int PHC>
+__global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams prm, int64_t chunk_elems) {
+    constexpr bool HELM = (K == BEMPPCUDA_HELMHOLTZ_SLP || K == BEMPPCUDA_HELMHOLTZ_DLP);
+    constexpr bool DLP = (K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_HELMHOLTZ_DLP);
+    static_assert(PS_PPT == 2, "two evaluation points per thread, packed");
+    __shared__ float4 syo[PS_SOURCES];  // yo, |yo|^2
+    __shared__ float4 scf[PS_SOURCES];  // coefficient re, im, yo . n_e, -
+    __shared__ double scen[PS_SOURCES * 3];
+    __shared__ float snrm[DLP ? PS_SOURCES * 3 : 3];
+    const int nq = prm.nq;
+    const int tile_elems = PS_SOURCES / nq;
+    const int64_t ebeg = (int64_t)blockIdx.y * chunk_elems;
+    const int64_t eend = min(ebeg + chunk_elems, prm.nsupport);
+    const int64_t pbase = (int64_t)blockIdx.x * (PS_THREADS * PS_PPT) + threadIdx.x;
+    const double kap = HELM ? prm.p[0] : 1.0;
+    double x[PS_PPT][3], ar[PS_PPT], ai[PS_PPT];
+#pragma unroll
+    for (int j = 0; j < PS_PPT; ++j) {
+        const int64_t pj = min(pbase + j * PS_THREADS, prm.npoints - 1);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) x[j][d] = prm.points[3 * pj + d];
+        ar[j] = ai[j] = 0.0;
+    }
+    const int64_t n = prm.nsrc;
+    const double *o = prm.src;
+    for (int64_t t0 = ebeg; t0 < eend; t0 += tile_elems) {
+        const int te = (int)min((int64_t)tile_elems, eend - t0);
+        const int ns = te * nq;
+        const int64_t s0 = t0 * nq;
+        __syncthreads();
+        for (int e = threadIdx.x; e < te; e += PS_THREADS) {
+            const int64_t ge = t0 + e;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) scen[3 * e + d] = o[(8 + d) * n + ge];
+            if (DLP)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) snrm[3 * e + d] = (float)o[(3 + d) * n + ge * nq];
+        }
+        __syncthreads();
+        for (int s = threadIdx.x; s < ns; s += PS_THREADS) {
+            const int64_t gs = s0 + s;
+            const int e = s / nq;
+            const float y0 = (float)(kap * (o[gs] - scen[3 * e])), y1 = (float)(kap * (o[n + gs] - scen[3 * e + 1])),
+                        y2 = (float)(kap * (o[2 * n + gs] - scen[3 * e + 2]));
+            syo[s] = make_float4(y0, y1, y2, fmaf(y2, y2, fmaf(y1, y1, y0 * y0)));
+            float yn = 0.f;
+            if (DLP) yn = fmaf(y2, snrm[3 * e + 2], fmaf(y1, snrm[3 * e + 1], y0 * snrm[3 * e]));
+            scf[s] = make_float4((float)o[6 * n + gs], (float)o[7 * n + gs], yn, 0.f);
+        }
+        __syncthreads();
+        for (int e = 0; e < te; ++e) {
+            // per (point, element): D = kappa (c_e - x) in FP64, packed FP32 copies for the pairs
+            double rc[PS_PPT];
+            float dd[3][PS_PPT], rc2h[PS_PPT];
+#pragma unroll
+            for (int j = 0; j < PS_PPT; ++j) {
+                const double D0 = kap * (scen[3 * e] - x[j][0]), D1 = kap * (scen[3 * e + 1] - x[j][1]),
+                             D2 = kap * (scen[3 * e + 2] - x[j][2]);
+                const double rc2 = fma(D2, D2, fma(D1, D1, D0 * D0));
+                rc[j] = rc2 > 0.0 ? rc2 * rsqrt64(rc2) : 0.0;  // a point may sit on a centroid
+                rc2h[j] = (float)rc2;
+                dd[0][j] = (float)D0;
+                dd[1][j] = (float)D1;
+                dd[2][j] = (float)D2;
+            }
+            // D . n_e enters the double layer as a factor (no cancellation): FP32 is enough
+            const float2 Dh0 = f2(dd[0][0], dd[0][1]), Dh1 = f2(dd[1][0], dd[1][1]), Dh2 = f2(dd[2][0], dd[2][1]);
+            const float2 Dn = DLP ? fma2(Dh2, b2(snrm[3 * e + 2]), fma2(Dh1, b2(snrm[3 * e + 1]),
+                                                                       mul2(Dh0, b2(snrm[3 * e]))))
+                                  : b2(0.f);
+            const float2 Dx = add2(Dh0, Dh0), Dy = add2(Dh1, Dh1), Dz = add2(Dh2, Dh2);  // 2 D
+            const float2 rcf = f2((float)rc[0], (float)rc[1]);
+            const float2 rc2f = f2(rc2h[0], rc2h[1]);
+            float2 er = b2(0.f), ei = b2(0.f);
+            for (int q = 0; q < nq; ++q) {
+                const float4 yo = syo[e * nq + q];
+                const float4 cf = scf[e * nq + q];
+                const float2 sdot = fma2(Dz, b2(yo.z), fma2(Dy, b2(yo.y), fma2(Dx, b2(yo.x), b2(yo.w))));
+                const float2 r2 = add2(rc2f, sdot);
+                const float2 rinv = f2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+                const float2 cr = b2(cf.x), ci = b2(cf.y);
+                if (!HELM) {
+                    float2 f = rinv;
+                    if (DLP) {
+                        // -(d'.n) / r'^3
+                        const float2 dot = add2(Dn, b2(cf.z));
+                        f = mul2(mul2(rinv, rinv), mul2(rinv, mul2(dot, b2(-1.f))));
+                    }
+                    er = fma2(f, cr, er);
+                    ei = fma2(f, ci, ei);
+                } else {
+                    const float2 den = fma2(r2, rinv, rcf);  // r' + r_c'
+                    const float2 th = mul2(sdot, f2(rcp_approx(den.x), rcp_approx(den.y)));
+                    float2 sn, cs;
+                    sincos2<PHC>(th, &sn, &cs);
+                    float2 vr, vi;  // kernel value over kappa (SLP) or kappa^2 (DLP), phase e^{i r_c'} excluded
+                    if (!DLP) {
+                        vr = mul2(rinv, cs);
+                        vi = mul2(rinv, sn);
+                    } else {
+                        // (i r' - 1) e^{i theta} (d'.n) / r'^3: (-cs - r' sn, r' cs - sn) g
+                        const float2 rp = mul2(r2, rinv);
+                        const float2 g = mul2(add2(Dn, b2(cf.z)), mul2(rinv, mul2(rinv, rinv)));
+                        vr = mul2(g, mul2(fma2(rp, sn, cs), b2(-1.f)));
+                        vi = mul2(g, fma2(rp, cs, mul2(sn, b2(-1.f))));
+                    }
+                    er = fma2(vr, cr, fma2(mul2(vi, b2(-1.f)), ci, er));
+                    ei = fma2(vr, ci, fma2(vi, cr, ei));
+                }
+            }
+            const double sc = HELM ? (DLP ? kap * kap : kap) : 1.0;
+            const double erj[2] = {(double)er.x, (double)er.y}, eij[2] = {(double)ei.x, (double)ei.y};
+#pragma unroll
+            for (int j = 0; j < PS_PPT; ++j) {
+                if (HELM) {
+                    double sn, cs;
+                    sincos_cw64(rc[j], &sn, &cs);
+                    ar[j] = fma(sc, cs * erj[j] - sn * eij[j], ar[j]);
+                    ai[j] = fma(sc, fma(cs, eij[j], sn * erj[j]), ai[j]);
+                } else {
+                    ar[j] += erj[j];
+                    ai[j] += eij[j];
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < PS_PPT; ++j) {
+        const int64_t pj = pbase + j * PS_THREADS;
+        if (pj >= prm.npoints) break;
+        double *out = prm.result + 2 * pj;
+        if (gridDim.y == 1) {
+            out[0] = BC_INV_4PI * ar[j];
+            out[1] = BC_INV_4PI * ai[j];
+        } else {
+            atomicAdd(out, BC_INV_4PI * ar[j]);
+            atomicAdd(out + 1, BC_INV_4PI * ai[j]);
+        }
+    }
+}
+
 template <int K, int PHC>
 static cudaError_t launch_scalar_nq(const PotParams &prm, dim3 grid, int64_t chunk_elems, cudaStream_t st) {
     if (prm.nq == 6)
@@ -426,19 +581,60 @@ static cudaError_t launch_scalar_nq(const PotParams &prm, dim3 grid, int64_t chu
 
 // Scalar Laplace, Helmholtz (real or complex wavenumber) and modified Helmholtz potentials;
 // phase_radius bounds every source's distance from its element centroid (0: unknown).
-static cudaError_t launch_scalar(const PotParams &prm, int kernel, double phase_radius, cudaStream_t st) {
+// Grid of the per-point kernels: point blocks x source chunks, enough CTAs for several waves; with
+// more than one chunk the chunks add their sums with atomics into the zeroed result.
+static cudaError_t scalar_grid(const PotParams &prm, dim3 *grid, int64_t *chunk_elems, cudaStream_t st) {
     const int64_t pblocks = (prm.npoints + PS_THREADS * PS_PPT - 1) / (PS_THREADS * PS_PPT);
     const int64_t target = (int64_t)bc_sm_count() * 8;  // CTAs: several waves of 4 resident per SM
     int64_t chunks = (target + pblocks - 1) / pblocks;
     chunks = std::min(chunks, (prm.nsupport + PS_CHUNK_MIN - 1) / PS_CHUNK_MIN);
     chunks = std::max<int64_t>(1, std::min<int64_t>(chunks, 65535));
-    const int64_t chunk_elems = (prm.nsupport + chunks - 1) / chunks;
-    chunks = (prm.nsupport + chunk_elems - 1) / chunk_elems;
+    *chunk_elems = (prm.nsupport + chunks - 1) / chunks;
+    chunks = (prm.nsupport + *chunk_elems - 1) / *chunk_elems;
     if (chunks > 1) {
         const cudaError_t err = cudaMemsetAsync(prm.result, 0, sizeof(double) * 2 * prm.npoints, st);
         if (err != cudaSuccess) return err;
     }
-    const dim3 grid((unsigned)pblocks, (unsigned)chunks);
+    *grid = dim3((unsigned)pblocks, (unsigned)chunks);
+    return cudaSuccess;
+}
+
+// Mixed-precision Laplace / Helmholtz (real k) single / double layer potentials.
+static cudaError_t launch_scalar_mixed(const PotParams &prm, int kernel, double phase_radius, cudaStream_t st) {
+    dim3 grid;
+    int64_t chunk_elems = 0;
+    const cudaError_t err = scalar_grid(prm, &grid, &chunk_elems, st);
+    if (err != cudaSuccess) return err;
+    const double kr = fabs(prm.p[0]) * phase_radius;
+    const int phc = (phase_radius > 0.0 && kr <= 0.5) ? 2 : (phase_radius > 0.0 && kr <= 1.0) ? 1 : 0;
+    switch (kernel) {
+    case BEMPPCUDA_LAPLACE_SLP: potential_scalar_mixed<BEMPPCUDA_LAPLACE_SLP, 0><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems); break;
+    case BEMPPCUDA_LAPLACE_DLP: potential_scalar_mixed<BEMPPCUDA_LAPLACE_DLP, 0><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems); break;
+    case BEMPPCUDA_HELMHOLTZ_SLP:
+        if (phc == 2)
+            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_SLP, 2><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems);
+        else if (phc == 1)
+            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_SLP, 1><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems);
+        else
+            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_SLP, 0><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems);
+        break;
+    default:  // BEMPPCUDA_HELMHOLTZ_DLP
+        if (phc == 2)
+            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_DLP, 2><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems);
+        else if (phc == 1)
+            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_DLP, 1><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems);
+        else
+            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_DLP, 0><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems);
+        break;
+    }
+    return cudaGetLastError();
+}
+
+static cudaError_t launch_scalar(const PotParams &prm, int kernel, double phase_radius, cudaStream_t st) {
+    dim3 grid;
+    int64_t chunk_elems = 0;
+    const cudaError_t gerr = scalar_grid(prm, &grid, &chunk_elems, st);
+    if (gerr != cudaSuccess) return gerr;
     const double kr = fabs(prm.p[0]) * phase_radius;
     const int phc = prm.p[1] != 0.0 ? 3
                     : (phase_radius > 0.0 && kr <= 0.5) ? 2 : (phase_radius > 0.0 && kr <= 1.0) ? 1 : 0;
@@ -485,8 +681,22 @@ int bc_potential_launch(const bemppcuda_potential_args *a, double *workspace, cu
     for (int i = 0; i < 4; ++i) prm.p[i] = a->params[i];
     QuadRule rule;
     fill_rule(rule, a->nq, a->quad_points, a->quad_weights);
-    if (prm.npoints == 0) return BEMPPCUDA_OK;
     const bool maxwell = a->assembly != BEMPPCUDA_ASM_SCALAR;
+    // mixed precision: Laplace / Helmholtz (real k) single / double layer potentials
+    const bool mixed = a->precision == BEMPPCUDA_MIXED;
+    if (a->precision != BEMPPCUDA_FP64 && !mixed) {
+        bc_set_error("potential: precision must be BEMPPCUDA_FP64 or BEMPPCUDA_MIXED");
+        return BEMPPCUDA_ERR_INVALID;
+    }
+    if (mixed && (maxwell || a->params[1] != 0.0 || !(a->kernel == BEMPPCUDA_LAPLACE_SLP ||
+                                                       a->kernel == BEMPPCUDA_LAPLACE_DLP ||
+                                                       ((a->kernel == BEMPPCUDA_HELMHOLTZ_SLP ||
+                                                         a->kernel == BEMPPCUDA_HELMHOLTZ_DLP) &&
+                                                        a->params[0] > 0.0)))) {
+        bc_set_error("mixed-precision potentials: Laplace and Helmholtz (real k > 0) single / double layer only");
+        return BEMPPCUDA_ERR_UNSUPPORTED;
+    }
+    if (prm.npoints == 0) return BEMPPCUDA_OK;
     if (prm.nsrc > 0) {
         const unsigned blocks = (unsigned)((prm.nsrc + 255) / 256);
         if (maxwell)
@@ -499,7 +709,9 @@ int bc_potential_launch(const bemppcuda_potential_args *a, double *workspace, cu
         const bool per_point = a->kernel == BEMPPCUDA_LAPLACE_SLP || a->kernel == BEMPPCUDA_LAPLACE_DLP ||
                                a->kernel == BEMPPCUDA_HELMHOLTZ_SLP || a->kernel == BEMPPCUDA_HELMHOLTZ_DLP ||
                                a->kernel == BEMPPCUDA_MODHELM_SLP || a->kernel == BEMPPCUDA_MODHELM_DLP;
-        if (!maxwell && per_point && prm.nsupport > 0) {
+        if (mixed && prm.nsupport > 0) {
+            err = launch_scalar_mixed(prm, a->kernel, a->phase_radius, st);
+        } else if (!maxwell && per_point && prm.nsupport > 0) {
             err = launch_scalar(prm, a->kernel, a->phase_radius, st);
         } else if (!maxwell) {
             switch (a->kernel) {

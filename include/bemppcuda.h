@@ -179,7 +179,9 @@ typedef struct {
 typedef struct {
     int32_t kernel;   /* Green's function; far-field kernels treat points as directions */
     int32_t assembly; /* BEMPPCUDA_ASM_SCALAR, _EFIE or _MFIE */
-    int32_t precision;
+    int32_t precision; /* BEMPPCUDA_FP64, or BEMPPCUDA_MIXED (FP32 point-source pairs, FP64 per-element
+                          phase and sums) for Laplace / Helmholtz (real k > 0) single / double layer
+                          potentials; other kernels return BEMPPCUDA_ERR_UNSUPPORTED under MIXED */
     int32_t pad0;
     double params[4];
     bemppcuda_grid grid;

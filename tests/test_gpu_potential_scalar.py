@@ -101,6 +101,54 @@ def test_modified_helmholtz(oracle, omega, name, family):
     _check(oracle, op, space)
 
 
+@pytest.mark.parametrize("kr", [None, 0.3, 0.8, 3.0])
+@pytest.mark.parametrize("name", ["single_layer", "double_layer"])
+@pytest.mark.parametrize("family", ["DP0", "P1"])
+def test_mixed_precision_potentials(oracle, kr, name, family):
+    """``device_interface="cuda_mixed"``: FP32 point-source pairs (Laplace, and Helmholtz in each phase
+    class) within 1e-6 of the oracle and different from the FP64 path."""
+    from bempp_cuda import operators
+    from bempp_cuda.device import device_grid
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+    from cases import sphere_shell_points
+
+    grid = regular_sphere(3)
+    space = function_space(grid, "DP", 0) if family == "DP0" else function_space(grid, "P", 1)
+    points, _ = sphere_shell_points(3000, 29)
+    if kr is None:
+        family_ops, args = operators.potential.laplace, ()
+    else:
+        family_ops, args = operators.potential.helmholtz, (kr / device_grid(grid).radius,)
+    mixed = getattr(family_ops, name)(space, points, *args, device_interface="cuda_mixed")
+    fp64 = getattr(family_ops, name)(space, points, *args)
+    got = _check(oracle, mixed, space, tol=1e-6)
+    ref = _check(oracle, fp64, space)
+    assert 0.0 < rel_fro(got, ref) < 1e-6
+
+
+@pytest.mark.parametrize("case", ["complex", "modified"])
+def test_mixed_interface_without_mixed_kernel_runs_fp64(case):
+    """Complex wavenumbers and modified Helmholtz have no mixed potential kernel: the FP64 result (to
+    rounding: the source chunks add their sums with atomics, in no fixed order)."""
+    from bempp_cuda import operators
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+    from cases import sphere_shell_points
+
+    space = function_space(regular_sphere(2), "P", 1)
+    points, _ = sphere_shell_points(500, 31)
+    if case == "complex":
+        f, args = operators.potential.helmholtz.single_layer, (3.0 + 0.5j,)
+    else:
+        f, args = operators.potential.modified_helmholtz.double_layer, (2.0,)
+    rng = np.random.default_rng(8)
+    c = rng.standard_normal(space.global_dof_count) + 1j * rng.standard_normal(space.global_dof_count)
+    a = f(space, points, *args).evaluate_device(c)
+    b = f(space, points, *args, device_interface="cuda_mixed").evaluate_device(c)
+    assert (torch.linalg.norm(a - b) / torch.linalg.norm(a)).item() < 1e-13
+
+
 @pytest.mark.parametrize("name", ["single_layer", "double_layer"])
 def test_laplace_points_near_the_surface(oracle, name):
     """Points on element centroids, 1e-3 above the surface and far away, with a ragged count (257)."""
@@ -199,3 +247,59 @@ def test_unknown_phase_radius_matches_factored_result():
         results.append(out.cpu().numpy())
     assert np.all(np.isfinite(results[0]))
     assert rel_fro(results[1], results[0]) < 1e-13
+
+
+def test_mixed_precision_argument_checks():
+    """Through the C ABI: an unknown precision is invalid; MIXED for a Maxwell potential is unsupported
+    (the host layer then evaluates in FP64); MIXED with an unknown phase radius takes the reduced sincos."""
+    from bempp_cuda import _lib, operators
+    from bempp_cuda.assembly import kernel_ids, potential_workspace_bytes, regular_rule
+    from bempp_cuda.device import current_stream, device_grid, device_space, ptr
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+    from cases import sphere_shell_points
+
+    grid = regular_sphere(2)
+    points, _ = sphere_shell_points(300, 5)
+    pts = torch.as_tensor(np.ascontiguousarray(points.T), device="cuda")
+    qp, qw = regular_rule(4)
+
+    def args_for(space, op, k):
+        kernel, assembly = kernel_ids(op.descriptor)
+        nshape = space.number_of_shape_functions
+        coeff = torch.ones(grid.number_of_elements * nshape, dtype=torch.complex128, device="cuda")
+        kdim = 3 if assembly != _lib.ASM_SCALAR else 1
+        out = torch.zeros((kdim, points.shape[1]), dtype=torch.complex128, device="cuda")
+        a = _lib.PotentialArgs()
+        a.kernel, a.assembly = kernel, assembly
+        a.params[0] = k
+        a.grid = device_grid(grid).record()
+        a.space = device_space(space).record()
+        a.nq = len(qw)
+        a.quad_points, a.quad_weights = qp.ctypes.data, qw.ctypes.data
+        a.npoints = points.shape[1]
+        a.points, a.coefficients, a.result = ptr(pts), ptr(coeff), ptr(out)
+        need = potential_workspace_bytes(a)
+        ws = torch.empty(max(need // 8, 1), dtype=torch.float64, device="cuda")
+        a.workspace, a.workspace_bytes = ptr(ws), need
+        return a, (coeff, out, ws)
+
+    lib = _lib.load()
+    p1 = function_space(grid, "P", 1)
+    a, keep = args_for(p1, operators.potential.helmholtz.single_layer(p1, points, 4.0), 4.0)
+    a.precision = 7
+    assert lib.bemppcuda_evaluate_potential(ctypes.byref(a), current_stream()) == _lib.ERR_INVALID
+    a.precision = _lib.MIXED
+    a.phase_radius = 0.0  # unknown: phase class 0 (reduced sincos)
+    assert lib.bemppcuda_evaluate_potential(ctypes.byref(a), current_stream()) == _lib.OK
+    a.precision = _lib.FP64
+    b, keep_b = args_for(p1, operators.potential.helmholtz.single_layer(p1, points, 4.0), 4.0)
+    assert lib.bemppcuda_evaluate_potential(ctypes.byref(b), current_stream()) == _lib.OK
+    torch.cuda.synchronize()
+    assert rel_fro(keep[1].cpu().numpy(), keep_b[1].cpu().numpy()) < 1e-6
+    rwg = function_space(grid, "RWG", 0)
+    m, keep_m = args_for(rwg, operators.potential.maxwell.electric_field(rwg, points, 2.0), 2.0)
+    m.precision = _lib.MIXED
+    assert lib.bemppcuda_evaluate_potential(ctypes.byref(m), current_stream()) == _lib.ERR_UNSUPPORTED
+    assert "mixed-precision potentials" in _lib.last_error()
+    torch.cuda.synchronize()
