@@ -1,7 +1,7 @@
-// Mixed-precision regular pairs of the Helmholtz single layer and
-// hypersingular operators on P1 spaces (6-point rule, real k > 0): the FP32
-// counterpart of regular_p1 (p1.cuh) with the geometry of the mixed DP0
-// kernels (dp0.cuh).
+// Mixed-precision regular pairs of the Helmholtz single layer, double layer,
+// adjoint double layer and hypersingular operators on P1 spaces (6-point
+// rule, real k > 0): the FP32 counterpart of regular_p1 (p1.cuh) with the
+// geometry of the mixed DP0 kernels (dp0.cuh).
 //
 // Lengths are in units of 1/k.  Per element pair the centroid offset
 // D = k (c_s - c_t), r_c' = |D| and exp(i r_c') are FP64; per point pair only
@@ -11,12 +11,22 @@
 // FP32, 1/r' by rsqrt.approx, the phase offset theta = (r'^2 - r_c'^2) /
 // (r' + r_c') without cancellation and its sine / cosine by the fitted FP32
 // polynomials; trial points q, q+1 travel together through packed f32x2 FMAs.
-// The trial sums T_j(p) = sum_q w_q psi_j(q) exp(i theta) / r' and the 3 x 3
-// block sum_p w_p phi_i(p) T_j(p) are FP32 (36 terms per entry); the block
-// is converted to FP64 once per element pair, where k / (4 pi), the
-// integration elements, exp(i r_c') and (hypersingular) the curl and normal
-// products are applied.  SYM as in regular_p1: pairs i < j, the block added
-// at (i, j) and, unless deferred to the transpose pass, at (j, i).
+// Single layer: the trial sums T_j(p) = sum_q w_q psi_j(q) exp(i theta) / r'.
+// Double layers: with h = (i r' - 1) exp(i theta) / r'^3 and d' = k (y - x),
+// a quadrature point lies in its own element's plane, so
+//   d' . n_s = D . n_s - xo_p . n_s      (one value per test point)
+//   d' . n_t = D . n_t + yo_q . n_t      (one value per trial point);
+// the double layer (trial normal) sums T_j(p) = sum_q w_q psi_j(q) h and
+// multiplies by d'.n_s per test point, the adjoint double layer (test normal,
+// kernel -(d . n_t)) sums h (-d'.n_t) per pair.  The 3 x 3 block
+// sum_p w_p phi_i(p) T_j(p) is FP32 (36 terms per entry); it is converted to
+// FP64 once per element pair, where k / (4 pi) (single layer, hypersingular)
+// or k^2 / (4 pi) (double layers), the integration elements, exp(i r_c') and
+// (hypersingular) the curl and normal products are applied.  SYM as in
+// regular_p1: pairs i < j; single layer and hypersingular add the block at
+// (i, j) and, unless deferred to the transpose pass, at (j, i); the double
+// layers add at (j, i) the transposed pair's own block, which is the other
+// operator's kernel of (i, j) (skew sweep: both normal sums per pair).
 #pragma once
 
 #include "p1.cuh"
@@ -34,9 +44,14 @@ struct TestBlockP1m {
     int v[P1_TCHUNK][3];
 };
 
-template <int ASM, int PHC, bool SYM>
+template <int ASM, int K, int PHC, bool SYM>
 __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, QuadRule rule) {
     constexpr bool HYP = ASM == BEMPPCUDA_ASM_HELM_HYP;
+    constexpr bool DL = K == BEMPPCUDA_HELMHOLTZ_DLP;
+    constexpr bool AD = K == BEMPPCUDA_HELMHOLTZ_ADLP;
+    constexpr bool SKEW = SYM && (DL || AD);
+    constexpr bool NS_SUM = DL || SKEW;  // sums multiplied by d'.n_s per test point
+    constexpr bool NT_SUM = AD || SKEW;  // sums with -d'.n_t per pair
     constexpr int NP = NQ6 / 2;
     __shared__ TestBlockP1m sb;
     const double kap = prm.p[0];
@@ -107,6 +122,7 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
         yz[jj] = f2(o[0][2], o[1][2]);
         yy2[jj] = fma2(yz[jj], yz[jj], fma2(yyy[jj], yyy[jj], mul2(yx[jj], yx[jj])));
     }
+    const float sn0 = (float)gs.n[0], sn1 = (float)gs.n[1], sn2 = (float)gs.n[2];
     double curl_s[3][3];
     if (HYP) surface_curls(prm.sg, prm.sne, s, gs.n, curl_s);
     int64_t scol[3];
@@ -132,17 +148,31 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
         float2 A[NP];
 #pragma unroll
         for (int jj = 0; jj < NP; ++jj) A[jj] = fma2(D2d, yz[jj], fma2(D1d, yyy[jj], fma2(D0d, yx[jj], yy2[jj])));
-        float lre[3][3], lim[3][3];
+        // normal terms: D . n_s; -(d'.n_t) = -(D . n_t) - yo_q . n_t per trial point
+        const float tn0 = (float)sb.n[tt][0], tn1 = (float)sb.n[tt][1], tn2 = (float)sb.n[tt][2];
+        const float Dns = fmaf(D2f, sn2, fmaf(D1f, sn1, D0f * sn0));
+        float2 mdt[NP];
+        if (NT_SUM) {
+            const float2 mDnt = b2(-fmaf(D2f, tn2, fmaf(D1f, tn1, D0f * tn0)));
+#pragma unroll
+            for (int jj = 0; jj < NP; ++jj)
+                mdt[jj] = fma2(yz[jj], b2(-tn2), fma2(yyy[jj], b2(-tn1), fma2(yx[jj], b2(-tn0), mDnt)));
+        }
+        float lre[3][3], lim[3][3];              // block of (i, j): single layer, or the first double layer
+        float ure[3][3], uim[3][3];              // SKEW: the transposed pair's block
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
-            for (int j = 0; j < 3; ++j) lre[i][j] = lim[i][j] = 0.f;
+            for (int j = 0; j < 3; ++j) lre[i][j] = lim[i][j] = ure[i][j] = uim[i][j] = 0.f;
 #pragma unroll 2
         for (int p = 0; p < NQ6; ++p) {
             const float4 m = sb.m[tt][p];
             const float Bp = fmaf(D2f, m.z, fmaf(D1f, m.y, fmaf(D0f, m.x, m.w)));
             const float2 mx = b2(m.x), my = b2(m.y), mz = b2(m.z), Bp2 = b2(Bp);
+            // d'.n_s at this test point: D . n_s - xo . n_s = D . n_s + (m . n_s) / 2
+            const float dns = NS_SUM ? fmaf(0.5f, fmaf(m.z, sn2, fmaf(m.y, sn1, m.x * sn0)), Dns) : 0.f;
             float2 tre[3] = {b2(0.f), b2(0.f), b2(0.f)}, tim[3] = {b2(0.f), b2(0.f), b2(0.f)};
+            float2 vre[3] = {b2(0.f), b2(0.f), b2(0.f)}, vim[3] = {b2(0.f), b2(0.f), b2(0.f)};
 #pragma unroll
             for (int jj = 0; jj < NP; ++jj) {
                 const float2 sdot = fma2(yz[jj], mz, fma2(yyy[jj], my, fma2(yx[jj], mx, add2(A[jj], Bp2))));
@@ -152,26 +182,57 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
                 const float2 th = mul2(sdot, f2(rcp_approx(den.x), rcp_approx(den.y)));
                 float2 sn, cs;
                 sincos2<PHC>(th, &sn, &cs);
-                const float2 kr = mul2(rinv, cs), ki = mul2(rinv, sn);
+                float2 kr, ki;
+                if (!DL && !AD) {
+                    kr = mul2(rinv, cs);
+                    ki = mul2(rinv, sn);
+                } else {
+                    // h = (i r' - 1) e^{i theta} / r'^3 = ((-cs - r' sn) + i (r' cs - sn)) / r'^3
+                    const float2 rp = mul2(r2, rinv), r3 = mul2(rinv, mul2(rinv, rinv));
+                    kr = mul2(r3, mul2(fma2(rp, sn, cs), b2(-1.f)));
+                    ki = mul2(r3, fma2(rp, cs, mul2(sn, b2(-1.f))));
+                }
 #pragma unroll
                 for (int j = 0; j < 3; ++j) {
                     const float2 w = f2(rule.swf[2 * jj][j], rule.swf[2 * jj + 1][j]);
-                    tre[j] = fma2(kr, w, tre[j]);
-                    tim[j] = fma2(ki, w, tim[j]);
+                    if (!AD || SKEW) {  // plain sums (single layer; double layer: times d'.n_s below)
+                        tre[j] = fma2(kr, w, tre[j]);
+                        tim[j] = fma2(ki, w, tim[j]);
+                    }
+                    if (NT_SUM) {  // sums with -(d'.n_t)
+                        const float2 wd = mul2(w, mdt[jj]);
+                        vre[j] = fma2(kr, wd, vre[j]);
+                        vim[j] = fma2(ki, wd, vim[j]);
+                    }
                 }
             }
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
                 const float ph = rule.swf[p][i];
+                const float phs = NS_SUM ? ph * dns : ph;
 #pragma unroll
                 for (int j = 0; j < 3; ++j) {
-                    lre[i][j] = fmaf(ph, tre[j].x + tre[j].y, lre[i][j]);
-                    lim[i][j] = fmaf(ph, tim[j].x + tim[j].y, lim[i][j]);
+                    if (!DL && !AD) {
+                        lre[i][j] = fmaf(ph, tre[j].x + tre[j].y, lre[i][j]);
+                        lim[i][j] = fmaf(ph, tim[j].x + tim[j].y, lim[i][j]);
+                    } else {
+                        // (i, j): double layer -> n_s sums, adjoint -> n_t sums; SKEW: the other one at (j, i)
+                        const float2 first_r = DL ? tre[j] : vre[j], first_i = DL ? tim[j] : vim[j];
+                        const float f1 = DL ? phs : ph;
+                        lre[i][j] = fmaf(f1, first_r.x + first_r.y, lre[i][j]);
+                        lim[i][j] = fmaf(f1, first_i.x + first_i.y, lim[i][j]);
+                        if (SKEW) {
+                            const float2 sec_r = DL ? vre[j] : tre[j], sec_i = DL ? vim[j] : tim[j];
+                            const float f2_ = DL ? ph : phs;
+                            ure[i][j] = fmaf(f2_, sec_r.x + sec_r.y, ure[i][j]);
+                            uim[i][j] = fmaf(f2_, sec_i.x + sec_i.y, uim[i][j]);
+                        }
+                    }
                 }
             }
         }
-        // k / (4 pi) |J_t| |J_s| exp(i r_c'), then the hypersingular combination
-        const double scale = kap * BC_INV_4PI * sb.ie[tt] * gs.ie;
+        // k / (4 pi) or k^2 / (4 pi), |J_t| |J_s| exp(i r_c'), then the hypersingular combination
+        const double scale = (DL || AD ? kap * kap : kap) * BC_INV_4PI * sb.ie[tt] * gs.ie;
         double sre = 0.0, sim = 0.0, cpf = 0.0;
         if (HYP) {
             // S = sum_pq w_p w_q G: the P1 functions add up to 1 on each side
@@ -203,15 +264,21 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
                 const double tr = vr * ph_c - vi * ph_s;
                 vi = fma(vr, ph_s, vi * ph_c);
                 vr = tr;
+                double wr = vr, wi = vi;  // the (j, i) block: the same, or (SKEW) its own sums
+                if (SKEW) {
+                    const double ur = (double)ure[i][j], ui = (double)uim[i][j];
+                    wr = ur * ph_c - ui * ph_s;
+                    wi = fma(ur, ph_s, ui * ph_c);
+                }
                 const double mm = mt * ms * scale;
                 const int64_t col = scol[j];
                 double *o = reinterpret_cast<double *>(prm.result) + 2 * (row * prm.ld + col);
                 atomicAdd(o, vr * mm);
                 atomicAdd(o + 1, vi * mm);
-                if (SYM && !prm.defer_transpose) {
+                if (SYM && (SKEW || !prm.defer_transpose)) {
                     double *ot = reinterpret_cast<double *>(prm.result) + 2 * (col * prm.ld + row);
-                    atomicAdd(ot, vr * mm);
-                    atomicAdd(ot + 1, vi * mm);
+                    atomicAdd(ot, wr * mm);
+                    atomicAdd(ot + 1, wi * mm);
                 }
             }
         }

@@ -428,26 +428,26 @@ static cudaError_t launch_add_transpose(void *a, int64_t n, int64_t ld, bool is_
     return cudaGetLastError();
 }
 
-// Mixed-precision Helmholtz single layer / hypersingular on P1 spaces (p1_mixed.cuh).
-template <int ASM>
+// Mixed-precision Helmholtz single layer, double layers and hypersingular on P1 spaces (p1_mixed.cuh).
+template <int ASM, int K>
 static cudaError_t launch_p1_mixed(const RegParams &prm, const QuadRule &rule, int phase_class, bool sym,
                                    cudaStream_t st) {
     dim3 grid((unsigned)((prm.ntrial + DP0_THREADS - 1) / DP0_THREADS),
               (unsigned)((prm.ntest + P1_TCHUNK - 1) / P1_TCHUNK));
     if (sym) {
         if (phase_class == 2)
-            regular_p1_mixed<ASM, 2, true><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+            regular_p1_mixed<ASM, K, 2, true><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
         else if (phase_class == 1)
-            regular_p1_mixed<ASM, 1, true><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+            regular_p1_mixed<ASM, K, 1, true><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
         else
-            regular_p1_mixed<ASM, 0, true><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+            regular_p1_mixed<ASM, K, 0, true><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
     } else {
         if (phase_class == 2)
-            regular_p1_mixed<ASM, 2, false><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+            regular_p1_mixed<ASM, K, 2, false><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
         else if (phase_class == 1)
-            regular_p1_mixed<ASM, 1, false><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+            regular_p1_mixed<ASM, K, 1, false><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
         else
-            regular_p1_mixed<ASM, 0, false><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+            regular_p1_mixed<ASM, K, 0, false><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
     }
     return cudaGetLastError();
 }
@@ -531,15 +531,18 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
         bc_set_error("overwrite mode needs the DP0 fast path (DP0 spaces, identity dofs, 6-point rule)");
         return BEMPPCUDA_ERR_INVALID;
     }
-    // mixed precision: DP0 scalar kernels, and the Helmholtz single layer / hypersingular on P1
-    // spaces (6-point rule, real k > 0)
+    // mixed precision: DP0 scalar kernels, and the Helmholtz single / double / adjoint double layer and
+    // hypersingular operators on P1 spaces (6-point rule, real k > 0)
     const bool p1_mixed = a->nq == NQ6 && !a->overwrite && a->test.nshape == 3 && a->trial.nshape == 3 &&
                           a->test.shapeset == BEMPPCUDA_SHAPE_P1 && a->trial.shapeset == BEMPPCUDA_SHAPE_P1 &&
-                          a->params[1] == 0.0 && a->params[0] > 0.0 && a->kernel == BEMPPCUDA_HELMHOLTZ_SLP &&
-                          (a->assembly == BEMPPCUDA_ASM_SCALAR || a->assembly == BEMPPCUDA_ASM_HELM_HYP);
+                          a->params[1] == 0.0 && a->params[0] > 0.0 &&
+                          ((a->assembly == BEMPPCUDA_ASM_HELM_HYP && a->kernel == BEMPPCUDA_HELMHOLTZ_SLP) ||
+                           (a->assembly == BEMPPCUDA_ASM_SCALAR && (a->kernel == BEMPPCUDA_HELMHOLTZ_SLP ||
+                                                                    a->kernel == BEMPPCUDA_HELMHOLTZ_DLP ||
+                                                                    a->kernel == BEMPPCUDA_HELMHOLTZ_ADLP)));
     if (a->precision == BEMPPCUDA_MIXED && !dp0 && !p1_mixed) {
-        bc_set_error("mixed precision is implemented for DP0 scalar kernels and the P1 Helmholtz single layer / "
-                     "hypersingular with the 6-point rule and a real wavenumber");
+        bc_set_error("mixed precision is implemented for DP0 scalar kernels and the P1 Helmholtz single, double, "
+                     "adjoint double layer and hypersingular operators with the 6-point rule and a real wavenumber");
         return BEMPPCUDA_ERR_UNSUPPORTED;
     }
     cudaError_t err = cudaSuccess;
@@ -617,9 +620,13 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
         const int p1_phase = a->params[1] != 0.0 ? 3 : phase_class;
         if (mixed && p1_mixed) {
             if (a->assembly == BEMPPCUDA_ASM_HELM_HYP)
-                err = launch_p1_mixed<BEMPPCUDA_ASM_HELM_HYP>(prm, rule, phase_class, psym, st);
+                err = launch_p1_mixed<BEMPPCUDA_ASM_HELM_HYP, BEMPPCUDA_HELMHOLTZ_SLP>(prm, rule, phase_class, psym, st);
+            else if (a->kernel == BEMPPCUDA_HELMHOLTZ_DLP)
+                err = launch_p1_mixed<BEMPPCUDA_ASM_SCALAR, BEMPPCUDA_HELMHOLTZ_DLP>(prm, rule, phase_class, psym, st);
+            else if (a->kernel == BEMPPCUDA_HELMHOLTZ_ADLP)
+                err = launch_p1_mixed<BEMPPCUDA_ASM_SCALAR, BEMPPCUDA_HELMHOLTZ_ADLP>(prm, rule, phase_class, psym, st);
             else
-                err = launch_p1_mixed<BEMPPCUDA_ASM_SCALAR>(prm, rule, phase_class, psym, st);
+                err = launch_p1_mixed<BEMPPCUDA_ASM_SCALAR, BEMPPCUDA_HELMHOLTZ_SLP>(prm, rule, phase_class, psym, st);
         } else if (a->assembly == BEMPPCUDA_ASM_LAPLACE_HYP) {
             err = launch_p1<BEMPPCUDA_ASM_LAPLACE_HYP, BEMPPCUDA_LAPLACE_SLP>(prm, rule, p1_phase, psym, st);
         } else if (a->assembly == BEMPPCUDA_ASM_HELM_HYP) {

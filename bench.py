@@ -812,6 +812,9 @@ def breadth_measure(args, torch, fp64_peak=None, fp32_peak=None):
 
     # mixed precision on P1 (device_interface "cuda_mixed"): FP32 regular pairs, against the FP64 weak form
     for name, path, level, k, flops_pp in (("helmholtz.single_layer p1 mixed", "helmholtz.single_layer", 5, 5.0, 38),
+                                           ("helmholtz.double_layer p1 mixed", "helmholtz.double_layer", 5, 5.0, 48),
+                                           ("helmholtz.adjoint_double_layer p1 mixed",
+                                            "helmholtz.adjoint_double_layer", 5, 5.0, 48),
                                            ("helmholtz.hypersingular p1 mixed", "helmholtz.hypersingular", 5, 5.0, 56)):
         g = grid_of(level)
         sp = function_space(g, "P", 1)

@@ -1,11 +1,11 @@
 """Mixed precision on P1 spaces (run on a B200).
 
-The Helmholtz single layer and hypersingular operators on P1 evaluate their
-regular pairs in FP32 (``regular_p1_mixed``) under ``device_interface=
-"cuda_mixed"``; their operator error against the FP64 path and the oracle is
-held to the mixed-precision bound (1e-6 relative Frobenius).  Operators
-without a mixed kernel (double layers, Laplace, complex k) run in FP64 under
-the same interface.
+The Helmholtz single layer, double layer, adjoint double layer and
+hypersingular operators on P1 evaluate their regular pairs in FP32
+(``regular_p1_mixed``) under ``device_interface="cuda_mixed"``; their operator
+error against the FP64 path and the oracle is held to the mixed-precision
+bound (1e-6 relative Frobenius).  Operators without a mixed kernel (Laplace,
+complex k) run in FP64 under the same interface.
 """
 
 import numpy as np
@@ -34,7 +34,8 @@ def _op(path, sp, k, interface):
 
 
 @pytest.mark.parametrize("k", [2.0, 4.0, 40.0])
-@pytest.mark.parametrize("path", ["helmholtz.single_layer", "helmholtz.hypersingular"])
+@pytest.mark.parametrize("path", ["helmholtz.single_layer", "helmholtz.hypersingular", "helmholtz.double_layer",
+                                  "helmholtz.adjoint_double_layer"])
 def test_mixed_p1_against_fp64_and_oracle(oracle, path, k):
     """k = 2, 4, 40 on a 512-element ellipsoid reach the three phase classes."""
     from cases import oracle_dense
@@ -52,9 +53,11 @@ def test_mixed_p1_against_fp64_and_oracle(oracle, path, k):
     assert rel_fro(amx.cpu().numpy(), ref) < 1e-6
 
 
-@pytest.mark.parametrize("path", ["helmholtz.single_layer", "helmholtz.hypersingular"])
+@pytest.mark.parametrize("path", ["helmholtz.single_layer", "helmholtz.hypersingular", "helmholtz.double_layer",
+                                  "helmholtz.adjoint_double_layer"])
 def test_mixed_p1_sweeps_agree(path):
-    """Symmetric sweep (both blocks by atomics, or U + U^T into a zeroed result) and per-pair sweep."""
+    """Symmetric sweep (both blocks by atomics, U + U^T into a zeroed result, or for the double layers the
+    skew sweep) and per-pair sweep."""
     from bempp_cuda import _lib
     from bempp_cuda.assembly import regular_into, singular_into_dense
     from bempp_cuda.operators import Parameters
@@ -78,7 +81,7 @@ def test_mixed_p1_sweeps_agree(path):
         assert (torch.linalg.norm(a - ref) / torch.linalg.norm(ref)).item() < tol, key
 
 
-@pytest.mark.parametrize("path,k", [("helmholtz.double_layer", 3.0), ("laplace.single_layer", None),
+@pytest.mark.parametrize("path,k", [("laplace.double_layer", None), ("laplace.single_layer", None),
                                     ("helmholtz.single_layer", 3.0 + 0.5j)])
 def test_mixed_interface_without_mixed_kernel_is_fp64(path, k):
     from bempp_cuda.shapes import regular_sphere
