@@ -27,9 +27,16 @@
 // (i, j) and, unless deferred to the transpose pass, at (j, i); the double
 // layers add at (j, i) the transposed pair's own block, which is the other
 // operator's kernel of (i, j) (skew sweep: both normal sums per pair).
+// Maxwell electric field on RWG / SNC (ASM_EFIE): the nine moments
+// M[u][v] = sum_pq w_p w_q G u(p) v(q), u, v in {1, xi, eta}, that the EFIE
+// block needs (rwg.cuh) are a fixed linear map of the P1 single-layer block
+// (1 = phi_0 + phi_1 + phi_2, xi = phi_1, eta = phi_2), so the FP32 part is
+// the single layer's and the FP64 epilogue forms the moments and
+// efie_block; the integration elements cancel against the RWG basis.
 #pragma once
 
 #include "p1.cuh"
+#include "rwg.cuh"
 
 namespace bc {
 
@@ -47,6 +54,7 @@ struct TestBlockP1m {
 template <int ASM, int K, int PHC, bool SYM>
 __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, QuadRule rule) {
     constexpr bool HYP = ASM == BEMPPCUDA_ASM_HELM_HYP;
+    constexpr bool EFIE = ASM == BEMPPCUDA_ASM_EFIE;  // test curl slots hold J_t, multipliers edge lengths
     constexpr bool DL = K == BEMPPCUDA_HELMHOLTZ_DLP;
     constexpr bool AD = K == BEMPPCUDA_HELMHOLTZ_ADLP;
     constexpr bool SKEW = SYM && (DL || AD);
@@ -81,8 +89,15 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
         }
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
-            sb.mult[idx][i] = prm.tmult[t * 3 + i];
+            sb.mult[idx][i] = prm.tmult[t * 3 + i] * (EFIE ? edge_length(prm.tg, prm.tne, t, i) : 1.0);
             sb.row[idx][i] = prm.tl2g[t * 3 + i];
+        }
+        if (EFIE) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                sb.curl[idx][0][d] = g.j0[d];
+                sb.curl[idx][1][d] = g.j1[d];
+            }
         }
         if (HYP) {
             double cu[3][3];
@@ -130,7 +145,7 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
         scol[j] = prm.sl2g[s * 3 + j];
-        smul[j] = prm.smult[s * 3 + j];
+        smul[j] = prm.smult[s * 3 + j] * (EFIE ? edge_length(prm.sg, prm.sne, s, j) : 1.0);
     }
 
     for (int tt = 0; tt < tcount; ++tt) {
@@ -231,8 +246,40 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
                 }
             }
         }
-        // k / (4 pi) or k^2 / (4 pi), |J_t| |J_s| exp(i r_c'), then the hypersingular combination
-        const double scale = (DL || AD ? kap * kap : kap) * BC_INV_4PI * sb.ie[tt] * gs.ie;
+        // k / (4 pi) or k^2 / (4 pi), |J_t| |J_s| exp(i r_c'), then the hypersingular combination;
+        // EFIE: the moments, k (4 pi G = k e^{i theta} / r' in these units) and 1 / (4 pi), no |J|
+        double ere[3][3], eim[3][3];
+        if (EFIE) {
+            double mre[3][3], mim[3][3];
+            double rs[3] = {0.0, 0.0, 0.0}, is[3] = {0.0, 0.0, 0.0};  // sums over j (row sums)
+            double cs_[3] = {0.0, 0.0, 0.0}, ci_[3] = {0.0, 0.0, 0.0};  // sums over i (column sums)
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const double lr = kap * (double)lre[i][j], li = kap * (double)lim[i][j];
+                    rs[i] += lr;
+                    is[i] += li;
+                    cs_[j] += lr;
+                    ci_[j] += li;
+                }
+            mre[0][0] = rs[0] + rs[1] + rs[2];
+            mim[0][0] = is[0] + is[1] + is[2];
+#pragma unroll
+            for (int a = 1; a < 3; ++a) {
+                mre[a][0] = rs[a];
+                mim[a][0] = is[a];
+                mre[0][a] = cs_[a];
+                mim[0][a] = ci_[a];
+#pragma unroll
+                for (int b = 1; b < 3; ++b) {
+                    mre[a][b] = kap * (double)lre[a][b];
+                    mim[a][b] = kap * (double)lim[a][b];
+                }
+            }
+            efie_block<false>(mre, mim, sb.curl[tt][0], sb.curl[tt][1], gs.j0, gs.j1, kap, 0.0, ere, eim);
+        }
+        const double scale = EFIE ? BC_INV_4PI : (DL || AD ? kap * kap : kap) * BC_INV_4PI * sb.ie[tt] * gs.ie;
         double sre = 0.0, sim = 0.0, cpf = 0.0;
         if (HYP) {
             // S = sum_pq w_p w_q G: the P1 functions add up to 1 on each side
@@ -254,7 +301,7 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
             for (int j = 0; j < 3; ++j) {
                 const double ms = smul[j];
                 if (ms == 0.0) continue;
-                double vr = (double)lre[i][j], vi = (double)lim[i][j];
+                double vr = EFIE ? ere[i][j] : (double)lre[i][j], vi = EFIE ? eim[i][j] : (double)lim[i][j];
                 if (HYP) {
                     const double cij = sb.curl[tt][i][0] * curl_s[j][0] + sb.curl[tt][i][1] * curl_s[j][1] +
                                        sb.curl[tt][i][2] * curl_s[j][2];

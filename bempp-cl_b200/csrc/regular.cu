@@ -540,9 +540,15 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
                            (a->assembly == BEMPPCUDA_ASM_SCALAR && (a->kernel == BEMPPCUDA_HELMHOLTZ_SLP ||
                                                                     a->kernel == BEMPPCUDA_HELMHOLTZ_DLP ||
                                                                     a->kernel == BEMPPCUDA_HELMHOLTZ_ADLP)));
-    if (a->precision == BEMPPCUDA_MIXED && !dp0 && !p1_mixed) {
-        bc_set_error("mixed precision is implemented for DP0 scalar kernels and the P1 Helmholtz single, double, "
-                     "adjoint double layer and hypersingular operators with the 6-point rule and a real wavenumber");
+    // ... and the Maxwell electric field on RWG / SNC (same FP32 core; 6-point rule, real k > 0)
+    const bool rwg_mixed = a->nq == NQ6 && !a->overwrite && a->assembly == BEMPPCUDA_ASM_EFIE &&
+                           a->kernel == BEMPPCUDA_HELMHOLTZ_SLP && a->params[1] == 0.0 && a->params[0] > 0.0 &&
+                           a->test.shapeset == BEMPPCUDA_SHAPE_RWG && a->trial.shapeset == BEMPPCUDA_SHAPE_RWG &&
+                           a->test.nshape == 3 && a->trial.nshape == 3;
+    if (a->precision == BEMPPCUDA_MIXED && !dp0 && !p1_mixed && !rwg_mixed) {
+        bc_set_error("mixed precision is implemented for DP0 scalar kernels, the P1 Helmholtz single, double, "
+                     "adjoint double layer and hypersingular operators and the Maxwell electric field, with the "
+                     "6-point rule and a real wavenumber");
         return BEMPPCUDA_ERR_UNSUPPORTED;
     }
     cudaError_t err = cudaSuccess;
@@ -596,7 +602,9 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
                           prm.ntest == prm.ntrial;
         // a complex wavenumber takes phase class 3 (exp(-Im k r) per point pair)
         const int rwg_phase = a->params[1] != 0.0 ? 3 : phase_class;
-        if (a->assembly == BEMPPCUDA_ASM_EFIE)
+        if (mixed && rwg_mixed)
+            err = launch_p1_mixed<BEMPPCUDA_ASM_EFIE, BEMPPCUDA_HELMHOLTZ_SLP>(prm, rule, phase_class, rsym, st);
+        else if (a->assembly == BEMPPCUDA_ASM_EFIE)
             err = launch_rwg<BEMPPCUDA_ASM_EFIE>(prm, rule, rwg_phase, rsym, st);
         else
             err = launch_rwg<BEMPPCUDA_ASM_MFIE>(prm, rule, rwg_phase, rsym, st);

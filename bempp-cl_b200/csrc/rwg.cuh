@@ -52,6 +52,67 @@ __device__ __forceinline__ double dot3(const double a[3], const double b[3]) {
     return fma(a[2], b[2], fma(a[1], b[1], a[0] * b[0]));
 }
 
+// EFIE block of an element pair from its nine moments M[u][v] = sum_pq w_p w_q G u(p) v(q), u, v in
+// {1, xi, eta} (index 0, 1, 2; G times 4 pi, any phase factor of the pair left out): the formula of the
+// header comment, for real k (CK false) or complex k = kr + i ki.
+template <bool CK>
+__device__ __forceinline__ void efie_block(const double mre[3][3], const double mim[3][3], const double tj0[3],
+                                           const double tj1[3], const double sj0[3], const double sj1[3], double kr,
+                                           double ki, double blk_re[3][3], double blk_im[3][3]) {
+    // c_t = (J_t (0, 1), J_t (1, 0), 0) = (j1_t, j0_t, 0); likewise c_s
+    const double *ctv[2] = {tj1, tj0};
+    const double *csv[2] = {sj1, sj0};
+    // P, V_t, V_s from the moments (index 0 = 1, 1 = xi, 2 = eta)
+    const double D00 = dot3(tj0, sj0), D01 = dot3(tj0, sj1), D10 = dot3(tj1, sj0), D11 = dot3(tj1, sj1);
+    const double pr = D00 * mre[1][1] + D01 * mre[1][2] + D10 * mre[2][1] + D11 * mre[2][2];
+    const double pi = D00 * mim[1][1] + D01 * mim[1][2] + D10 * mim[2][1] + D11 * mim[2][2];
+    double vtr[3], vti[3], vsr[3], vsi[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        vtr[c] = fma(tj0[c], mre[1][0], tj1[c] * mre[2][0]);
+        vti[c] = fma(tj0[c], mim[1][0], tj1[c] * mim[2][0]);
+        vsr[c] = fma(sj0[c], mre[0][1], sj1[c] * mre[0][2]);
+        vsi[c] = fma(sj0[c], mim[0][1], sj1[c] * mim[0][2]);
+    }
+    // -ik E1 - 4 / (ik) M11, 1 / (ik) = -i / k
+    const double m11r = mre[0][0], m11i = mim[0][0];
+    // complex k: -4 / (ik) M11 = 4 (ki + i kr) / |k|^2 M11, one value per pair
+    double c1r = 0.0, c1i = 0.0;
+    if (CK) {
+        const double g4 = 4.0 / fma(kr, kr, ki * ki);
+        c1r = g4 * fma(ki, m11r, -kr * m11i);
+        c1i = g4 * fma(kr, m11r, ki * m11i);
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            double er = pr, ei = pi;
+            if (j < 2) {
+                er -= dot3(csv[j], vtr);
+                ei -= dot3(csv[j], vti);
+            }
+            if (i < 2) {
+                er -= dot3(ctv[i], vsr);
+                ei -= dot3(ctv[i], vsi);
+            }
+            if (i < 2 && j < 2) {
+                const double cc = dot3(ctv[i], csv[j]);
+                er = fma(cc, m11r, er);
+                ei = fma(cc, m11i, ei);
+            }
+            // -ik (er + i ei) = k ei - i k er;  -(4 / (ik)) M11 = (4i / k) M11 = -4 m11i / k + i 4 m11r / k
+            if (CK) {
+                // -ik (er + i ei) = (kr ei + ki er) + i (ki ei - kr er)
+                blk_re[i][j] = fma(kr, ei, fma(ki, er, c1r));
+                blk_im[i][j] = fma(ki, ei, fma(-kr, er, c1i));
+            } else {
+                blk_re[i][j] = fma(kr, ei, -4.0 * m11i / kr);
+                blk_im[i][j] = fma(-kr, er, 4.0 * m11r / kr);
+            }
+        }
+}
+
 template <int ASM, int PHC, bool SYM>
 __global__ void __launch_bounds__(DP0_THREADS) regular_rwg(RegParams prm, QuadRule rule) {
     constexpr bool EFIE = ASM == BEMPPCUDA_ASM_EFIE;
@@ -224,55 +285,7 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_rwg(RegParams prm, QuadRu
         const double *csv[2] = {gs.j1, gs.j0};
         double blk_re[3][3], blk_im[3][3];
         if (EFIE) {
-            // P, V_t, V_s from the moments (index 0 = 1, 1 = xi, 2 = eta)
-            const double D00 = dot3(tj0, gs.j0), D01 = dot3(tj0, gs.j1), D10 = dot3(tj1, gs.j0), D11 = dot3(tj1, gs.j1);
-            const double pr = D00 * mre[1][1] + D01 * mre[1][2] + D10 * mre[2][1] + D11 * mre[2][2];
-            const double pi = D00 * mim[1][1] + D01 * mim[1][2] + D10 * mim[2][1] + D11 * mim[2][2];
-            double vtr[3], vti[3], vsr[3], vsi[3];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                vtr[c] = fma(tj0[c], mre[1][0], tj1[c] * mre[2][0]);
-                vti[c] = fma(tj0[c], mim[1][0], tj1[c] * mim[2][0]);
-                vsr[c] = fma(gs.j0[c], mre[0][1], gs.j1[c] * mre[0][2]);
-                vsi[c] = fma(gs.j0[c], mim[0][1], gs.j1[c] * mim[0][2]);
-            }
-            // -ik E1 - 4 / (ik) M11, 1 / (ik) = -i / k
-            const double m11r = mre[0][0], m11i = mim[0][0];
-            // complex k: -4 / (ik) M11 = 4 (ki + i kr) / |k|^2 M11, one value per pair
-            double c1r = 0.0, c1i = 0.0;
-            if (CK) {
-                const double g4 = 4.0 / fma(kr, kr, ki * ki);
-                c1r = g4 * fma(ki, m11r, -kr * m11i);
-                c1i = g4 * fma(kr, m11r, ki * m11i);
-            }
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    double er = pr, ei = pi;
-                    if (j < 2) {
-                        er -= dot3(csv[j], vtr);
-                        ei -= dot3(csv[j], vti);
-                    }
-                    if (i < 2) {
-                        er -= dot3(ctv[i], vsr);
-                        ei -= dot3(ctv[i], vsi);
-                    }
-                    if (i < 2 && j < 2) {
-                        const double cc = dot3(ctv[i], csv[j]);
-                        er = fma(cc, m11r, er);
-                        ei = fma(cc, m11i, ei);
-                    }
-                    // -ik (er + i ei) = k ei - i k er;  -(4 / (ik)) M11 = (4i / k) M11 = -4 m11i / k + i 4 m11r / k
-                    if (CK) {
-                        // -ik (er + i ei) = (kr ei + ki er) + i (ki ei - kr er)
-                        blk_re[i][j] = fma(kr, ei, fma(ki, er, c1r));
-                        blk_im[i][j] = fma(ki, ei, fma(-kr, er, c1i));
-                    } else {
-                        blk_re[i][j] = fma(kr, ei, -4.0 * m11i / kr);
-                        blk_im[i][j] = fma(-kr, er, 4.0 * m11r / kr);
-                    }
-                }
+            efie_block<CK>(mre, mim, tj0, tj1, gs.j0, gs.j1, kr, ki, blk_re, blk_im);
         } else {
 #pragma unroll
             for (int i = 0; i < 3; ++i)

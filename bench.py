@@ -815,11 +815,16 @@ def breadth_measure(args, torch, fp64_peak=None, fp32_peak=None):
                                            ("helmholtz.double_layer p1 mixed", "helmholtz.double_layer", 5, 5.0, 48),
                                            ("helmholtz.adjoint_double_layer p1 mixed",
                                             "helmholtz.adjoint_double_layer", 5, 5.0, 48),
-                                           ("helmholtz.hypersingular p1 mixed", "helmholtz.hypersingular", 5, 5.0, 56)):
+                                           ("helmholtz.hypersingular p1 mixed", "helmholtz.hypersingular", 5, 5.0, 56),
+                                           ("maxwell.electric_field rwg/snc mixed", "maxwell.electric_field", 4, 2.0,
+                                            101)):
         g = grid_of(level)
-        sp = function_space(g, "P", 1)
+        if path.startswith("maxwell"):
+            sp, dual = function_space(g, "RWG", 0), function_space(g, "SNC", 0)
+        else:
+            sp = dual = function_space(g, "P", 1)
         f = factory(path)
-        op64, opmx = f(sp, sp, sp, k), f(sp, sp, sp, k, device_interface="cuda_mixed")
+        op64, opmx = f(sp, sp, dual, k), f(sp, sp, dual, k, device_interface="cuda_mixed")
         ref = op64._assemble()
         opmx._assemble()
         torch.cuda.synchronize()
@@ -833,7 +838,7 @@ def breadth_measure(args, torch, fp64_peak=None, fp32_peak=None):
             torch.cuda.synchronize()
             ms.append(e0.elapsed_time(e1))
         err = float((torch.linalg.norm(mat.tensor - ref.tensor) / torch.linalg.norm(ref.tensor)).item())
-        rows = cols = sp.global_dof_count
+        rows, cols = dual.global_dof_count, sp.global_dof_count
         ne = g.number_of_elements
         qpe = 36.0 * ne * ne
         gms = float(np.median(ms))
