@@ -428,8 +428,14 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar(PotParams prm, in
 // FP64.  Single layer e^{ikr}/r = kappa e^{i theta} e^{i r_c'} / r'; double
 // layer (ikr - 1) e^{ikr} (d . n) / r^3 = kappa^2 (i r' - 1) e^{i theta}
 // e^{i r_c'} (d' . n) / r'^3 with d' = D + yo.
+// Near elements: with r_c' >= 4 kappa R (R >= every source's distance from its
+// element centroid) the FP32 sums lose at most ~1.6e-7 relative in r'^2; a
+// point closer to an element than that (evaluation next to the surface)
+// takes that element's sources in FP64 instead (`near_r` = 4 kappa R, 0 when R
+// is unknown: no FP64 fallback).
 template <int K, int PHC>
-__global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams prm, int64_t chunk_elems) {
+__global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams prm, int64_t chunk_elems,
+                                                                      double near_r) {
     constexpr bool HELM = (K == BEMPPCUDA_HELMHOLTZ_SLP || K == BEMPPCUDA_HELMHOLTZ_DLP);
     constexpr bool DLP = (K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_HELMHOLTZ_DLP);
     static_assert(PS_PPT == 2, "two evaluation points per thread, packed");
@@ -542,7 +548,40 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams p
             const double erj[2] = {(double)er.x, (double)er.y}, eij[2] = {(double)ei.x, (double)ei.y};
 #pragma unroll
             for (int j = 0; j < PS_PPT; ++j) {
-                if (HELM) {
+                if (rc[j] < near_r) {
+                    // FP64 for this (point, element): the sources from the table in global memory
+                    double nr = 0.0, ni = 0.0;
+                    const int64_t g0 = s0 + (int64_t)e * nq;
+                    for (int q = 0; q < nq; ++q) {
+                        const int64_t gq = g0 + q;
+                        const double d0 = o[gq] - x[j][0], d1 = o[n + gq] - x[j][1], d2 = o[2 * n + gq] - x[j][2];
+                        const double r2 = fma(d2, d2, fma(d1, d1, d0 * d0));
+                        const double rinv = rsqrt64(r2);
+                        double f = rinv;
+                        if (DLP) f = fma(d2, o[5 * n + gq], fma(d1, o[4 * n + gq], d0 * o[3 * n + gq])) * rinv * rinv * rinv;
+                        const double cr = o[6 * n + gq], ci = o[7 * n + gq];
+                        if (!HELM) {
+                            if (DLP) f = -f;
+                            nr = fma(f, cr, nr);
+                            ni = fma(f, ci, ni);
+                        } else {
+                            const double r = r2 * rinv;
+                            double sn, cs;
+                            sincos_cw64(kap * r, &sn, &cs);
+                            double wr = f * cr, wi = f * ci;
+                            if (DLP) {  // times (i k r - 1)
+                                const double b = kap * r;
+                                const double tr = -fma(b, wi, wr), ti = fma(b, wr, -wi);
+                                wr = tr;
+                                wi = ti;
+                            }
+                            nr = fma(cs, wr, fma(-sn, wi, nr));
+                            ni = fma(cs, wi, fma(sn, wr, ni));
+                        }
+                    }
+                    ar[j] += nr;
+                    ai[j] += ni;
+                } else if (HELM) {
                     double sn, cs;
                     sincos_cw64(rc[j], &sn, &cs);
                     ar[j] = fma(sc, cs * erj[j] - sn * eij[j], ar[j]);
@@ -607,24 +646,26 @@ static cudaError_t launch_scalar_mixed(const PotParams &prm, int kernel, double 
     if (err != cudaSuccess) return err;
     const double kr = fabs(prm.p[0]) * phase_radius;
     const int phc = (phase_radius > 0.0 && kr <= 0.5) ? 2 : (phase_radius > 0.0 && kr <= 1.0) ? 1 : 0;
+    const bool helm = kernel == BEMPPCUDA_HELMHOLTZ_SLP || kernel == BEMPPCUDA_HELMHOLTZ_DLP;
+    const double near_r = 4.0 * (helm ? prm.p[0] : 1.0) * phase_radius;  // in the kernel's units of 1/kappa
     switch (kernel) {
-    case BEMPPCUDA_LAPLACE_SLP: potential_scalar_mixed<BEMPPCUDA_LAPLACE_SLP, 0><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems); break;
-    case BEMPPCUDA_LAPLACE_DLP: potential_scalar_mixed<BEMPPCUDA_LAPLACE_DLP, 0><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems); break;
+    case BEMPPCUDA_LAPLACE_SLP: potential_scalar_mixed<BEMPPCUDA_LAPLACE_SLP, 0><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems, near_r); break;
+    case BEMPPCUDA_LAPLACE_DLP: potential_scalar_mixed<BEMPPCUDA_LAPLACE_DLP, 0><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems, near_r); break;
     case BEMPPCUDA_HELMHOLTZ_SLP:
         if (phc == 2)
-            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_SLP, 2><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems);
+            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_SLP, 2><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems, near_r);
         else if (phc == 1)
-            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_SLP, 1><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems);
+            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_SLP, 1><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems, near_r);
         else
-            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_SLP, 0><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems);
+            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_SLP, 0><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems, near_r);
         break;
     default:  // BEMPPCUDA_HELMHOLTZ_DLP
         if (phc == 2)
-            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_DLP, 2><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems);
+            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_DLP, 2><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems, near_r);
         else if (phc == 1)
-            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_DLP, 1><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems);
+            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_DLP, 1><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems, near_r);
         else
-            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_DLP, 0><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems);
+            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_DLP, 0><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems, near_r);
         break;
     }
     return cudaGetLastError();

@@ -170,6 +170,27 @@ def test_laplace_points_near_the_surface(oracle, name):
     _check(oracle, _operator(name, space, points, 4.0), space)
 
 
+@pytest.mark.parametrize("name", ["single_layer", "double_layer"])
+@pytest.mark.parametrize("k", [None, 4.0])
+def test_mixed_points_near_the_surface(oracle, name, k):
+    """cuda_mixed with points on element centroids and 1e-3 above the surface: the elements next to a point
+    are evaluated in FP64 (the FP32 offsets would cancel there), so the result stays within 1e-6."""
+    from bempp_cuda import operators
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+
+    grid = regular_sphere(3)
+    space = function_space(grid, "P", 1)
+    cent = grid.vertices[:, grid.elements].mean(axis=1)
+    rng = np.random.default_rng(11)
+    pick = rng.choice(cent.shape[1], 100, replace=False)
+    points = np.concatenate([cent[:, pick[:50]], cent[:, pick[50:]] * 1.001, rng.standard_normal((3, 57)) * 5.0],
+                            axis=1)
+    family, args = (operators.potential.laplace, ()) if k is None else (operators.potential.helmholtz, (k,))
+    mixed = getattr(family, name)(space, points, *args, device_interface="cuda_mixed")
+    _check(oracle, mixed, space, tol=1e-6)
+
+
 @pytest.mark.parametrize("order", [2, 6])
 def test_general_rule_size(oracle, order):
     """Rules with other than six points take the runtime-size branch of the kernel."""
@@ -186,6 +207,13 @@ def test_general_rule_size(oracle, order):
     for name in ("single_layer", "double_layer"):
         for k in (None, 3.0):
             _check(oracle, _operator(name, space, points, k, parameters=prm), space)
+    # the mixed kernel with the same rule sizes
+    from bempp_cuda import operators
+
+    for k in (None, 3.0):
+        family, args = (operators.potential.laplace, ()) if k is None else (operators.potential.helmholtz, (k,))
+        op = family.double_layer(space, points, *args, parameters=prm, device_interface="cuda_mixed")
+        _check(oracle, op, space, tol=1e-6)
 
 
 def test_single_chunk_and_single_point(oracle):
