@@ -78,6 +78,7 @@ __global__ void __launch_bounds__(32 * SING_WARPS) singular_pairs(SingParams prm
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) are[i][j] = aim[i][j] = 0.0;
+    double sre = 0.0, sim = 0.0;  // Helmholtz / modified hypersingular: S = sum_p w G
 
     const int64_t toff = prm.toff[k], soff = prm.soff[k], woff = prm.woff[k];
     const int n = (int)prm.npts[k];
@@ -106,23 +107,20 @@ __global__ void __launch_bounds__(32 * SING_WARPS) singular_pairs(SingParams prm
         } else if (ASM == BEMPPCUDA_ASM_LAPLACE_HYP) {
             are[0][0] = fma(kv.re, w, are[0][0]);
         } else if (HYP) {
-            double k2r = 0.0, k2i = 0.0;
-            if (ASM == BEMPPCUDA_ASM_HELM_HYP) {
-                k2r = -(kr * kr - ki * ki);
-                k2i = -(2.0 * kr * ki);
-            } else {
-                k2r = kr * kr;
-            }
+            // the pair's value is curl_i.curl_j S + c (n_t.n_s) M_ij with S = sum_p w G and
+            // M_ij = sum_p w G phi_i psi_j (the curls and normals are constant per element pair)
             const cplx kw = cscale(kv, w);
+            sre += kw.re;
+            sim += kw.im;
 #pragma unroll
             for (int i = 0; i < 3; ++i)
 #pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    const double mm = pt[i] * ps[j] * normal_prod;
-                    const cplx v = cmul(kw, cplx{cp[i][j] + k2r * mm, k2i * mm});
-                    are[i][j] += v.re;
-                    aim[i][j] += v.im;
-                }
+                for (int j = 0; j < 3; ++j)
+                    if (i < nt && j < ns) {
+                        const double f = pt[i] * ps[j];
+                        are[i][j] = fma(kw.re, f, are[i][j]);
+                        aim[i][j] = fma(kw.im, f, aim[i][j]);
+                    }
         } else {
             double bt[3][3], bs[3][3];
             rwg_values(gt, tpm.x, tpm.y, bt);
@@ -163,6 +161,11 @@ __global__ void __launch_bounds__(32 * SING_WARPS) singular_pairs(SingParams prm
     }
 
     // reduce across the warp
+    constexpr bool HYP_K = HYP && ASM != BEMPPCUDA_ASM_LAPLACE_HYP;
+    if (HYP_K) {
+        sre = warp_sum(sre);
+        sim = warp_sum(sim);
+    }
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -185,6 +188,13 @@ __global__ void __launch_bounds__(32 * SING_WARPS) singular_pairs(SingParams prm
             if (ASM == BEMPPCUDA_ASM_LAPLACE_HYP) {
                 vr = are[0][0] * scale * cp[i][j];
                 vi = 0.0;
+            } else if (HYP_K) {
+                // c = -k^2 (Helmholtz, complex k allowed) or +omega^2 (modified Helmholtz)
+                const double k2r = ASM == BEMPPCUDA_ASM_HELM_HYP ? -(kr * kr - ki * ki) : kr * kr;
+                const double k2i = ASM == BEMPPCUDA_ASM_HELM_HYP ? -(2.0 * kr * ki) : 0.0;
+                const double mr = are[i][j] * normal_prod, mi = aim[i][j] * normal_prod;
+                vr = fma(cp[i][j], sre, fma(k2r, mr, -k2i * mi)) * scale;
+                vi = fma(cp[i][j], sim, fma(k2r, mi, k2i * mr)) * scale;
             } else {
                 double f = scale;
                 if (MAXWELL) f *= edge_length(prm.g, prm.ne, t, i) * edge_length(prm.g, prm.ne, s, j);
