@@ -11,6 +11,7 @@
 // reductions.  Always FP64.  Output either to the flat per-pair value array
 // of the reference interface or scattered straight into a dense matrix.
 #include "common.cuh"
+#include "rwg.cuh"  // efie_block
 #include "singular_dp0.cuh"
 
 namespace bc {
@@ -127,19 +128,17 @@ __global__ void __launch_bounds__(32 * SING_WARPS) singular_pairs(SingParams prm
             rwg_values(gs, spm.x, spm.y, bs);
             const cplx kw = cscale(kv, w);
             if (ASM == BEMPPCUDA_ASM_EFIE) {
-                const double kk = kr * kr + ki * ki;
-                const double div = 4.0 / (gt.ie * gs.ie);
-                const cplx inv_ik = {-ki / kk, -kr / kk};
+                // moments M[a][b] = sum w G u_a(x) v_b(y), u, v = (1, xi, eta): the EFIE block follows per pair
+                const double ut[3] = {1.0, tpm.x, tpm.y}, vs[3] = {1.0, spm.x, spm.y};
 #pragma unroll
-                for (int i = 0; i < 3; ++i)
+                for (int a = 0; a < 3; ++a) {
+                    const double wr = kw.re * ut[a], wi = kw.im * ut[a];
 #pragma unroll
-                    for (int j = 0; j < 3; ++j) {
-                        const double dot = bt[i][0] * bs[j][0] + bt[i][1] * bs[j][1] + bt[i][2] * bs[j][2];
-                        const cplx fac = {ki * dot - div * inv_ik.re, -kr * dot - div * inv_ik.im};
-                        const cplx v = cmul(kw, fac);
-                        are[i][j] += v.re;
-                        aim[i][j] += v.im;
+                    for (int b = 0; b < 3; ++b) {
+                        are[a][b] = fma(wr, vs[b], are[a][b]);
+                        aim[a][b] = fma(wi, vs[b], aim[a][b]);
                     }
+                }
             } else {
                 const double df[3] = {x[0] - y[0], x[1] - y[1], x[2] - y[2]};
                 const double d2 = df[0] * df[0] + df[1] * df[1] + df[2] * df[2];
@@ -178,6 +177,13 @@ __global__ void __launch_bounds__(32 * SING_WARPS) singular_pairs(SingParams prm
         }
     if (lane != 0) return;
     const double scale = gt.ie * gs.ie;
+    double eb_re[3][3], eb_im[3][3];  // EFIE block from the moments (the |J| factors cancel)
+    if (ASM == BEMPPCUDA_ASM_EFIE) {
+        if (ki != 0.0)
+            efie_block<true>(are, aim, gt.j0, gt.j1, gs.j0, gs.j1, kr, ki, eb_re, eb_im);
+        else
+            efie_block<false>(are, aim, gt.j0, gt.j1, gs.j0, gs.j1, kr, 0.0, eb_re, eb_im);
+    }
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
         if (i >= nt) continue;
@@ -195,6 +201,10 @@ __global__ void __launch_bounds__(32 * SING_WARPS) singular_pairs(SingParams prm
                 const double mr = are[i][j] * normal_prod, mi = aim[i][j] * normal_prod;
                 vr = fma(cp[i][j], sre, fma(k2r, mr, -k2i * mi)) * scale;
                 vi = fma(cp[i][j], sim, fma(k2r, mi, k2i * mr)) * scale;
+            } else if (ASM == BEMPPCUDA_ASM_EFIE) {
+                const double f = edge_length(prm.g, prm.ne, t, i) * edge_length(prm.g, prm.ne, s, j);
+                vr = eb_re[i][j] * f;
+                vi = eb_im[i][j] * f;
             } else {
                 double f = scale;
                 if (MAXWELL) f *= edge_length(prm.g, prm.ne, t, i) * edge_length(prm.g, prm.ne, s, j);
