@@ -113,6 +113,42 @@ __device__ __forceinline__ void efie_block(const double mre[3][3], const double 
         }
 }
 
+// MFIE block of an element pair from its four sums (any phase factor of the pair left out):
+// MFIE_ij = PB - c_sj . PC - c_ti . QB + c_ti . (c_sj x QC), the formula of the header comment.
+__device__ __forceinline__ void mfie_block(double pbr, double pbi, const double pcr[3], const double pci[3],
+                                           const double qbr[3], const double qbi[3], const double qcr[3],
+                                           const double qci[3], const double tj0[3], const double tj1[3],
+                                           const double sj0[3], const double sj1[3], double blk_re[3][3],
+                                           double blk_im[3][3]) {
+    const double *ctv[2] = {tj1, tj0};
+    const double *csv[2] = {sj1, sj0};
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            double vr = pbr, vi = pbi;
+            if (j < 2) {
+                vr -= dot3(csv[j], pcr);
+                vi -= dot3(csv[j], pci);
+            }
+            if (i < 2) {
+                vr -= dot3(ctv[i], qbr);
+                vi -= dot3(ctv[i], qbi);
+                if (j < 2) {
+                    // c_ti . (c_sj x QC) = QC . (c_ti x c_sj)
+                    double cx[3];
+                    cx[0] = ctv[i][1] * csv[j][2] - ctv[i][2] * csv[j][1];
+                    cx[1] = ctv[i][2] * csv[j][0] - ctv[i][0] * csv[j][2];
+                    cx[2] = ctv[i][0] * csv[j][1] - ctv[i][1] * csv[j][0];
+                    vr += dot3(cx, qcr);
+                    vi += dot3(cx, qci);
+                }
+            }
+            blk_re[i][j] = vr;
+            blk_im[i][j] = vi;
+        }
+}
+
 template <int ASM, int PHC, bool SYM>
 __global__ void __launch_bounds__(DP0_THREADS) regular_rwg(RegParams prm, QuadRule rule) {
     constexpr bool EFIE = ASM == BEMPPCUDA_ASM_EFIE;
@@ -287,31 +323,7 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_rwg(RegParams prm, QuadRu
         if (EFIE) {
             efie_block<CK>(mre, mim, tj0, tj1, gs.j0, gs.j1, kr, ki, blk_re, blk_im);
         } else {
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    double vr = pbr, vi = pbi;
-                    if (j < 2) {
-                        vr -= dot3(csv[j], pcr);
-                        vi -= dot3(csv[j], pci);
-                    }
-                    if (i < 2) {
-                        vr -= dot3(ctv[i], qbr);
-                        vi -= dot3(ctv[i], qbi);
-                        if (j < 2) {
-                            // c_ti . (c_sj x QC) = QC . (c_ti x c_sj)
-                            double cx[3];
-                            cx[0] = ctv[i][1] * csv[j][2] - ctv[i][2] * csv[j][1];
-                            cx[1] = ctv[i][2] * csv[j][0] - ctv[i][0] * csv[j][2];
-                            cx[2] = ctv[i][0] * csv[j][1] - ctv[i][1] * csv[j][0];
-                            vr += dot3(cx, qcr);
-                            vi += dot3(cx, qci);
-                        }
-                    }
-                    blk_re[i][j] = vr;
-                    blk_im[i][j] = vi;
-                }
+            mfie_block(pbr, pbi, pcr, pci, qbr, qbi, qcr, qci, tj0, tj1, gs.j0, gs.j1, blk_re, blk_im);
         }
 #pragma unroll
         for (int i = 0; i < 3; ++i) {

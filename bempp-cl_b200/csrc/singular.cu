@@ -80,6 +80,9 @@ __global__ void __launch_bounds__(32 * SING_WARPS) singular_pairs(SingParams prm
 #pragma unroll
         for (int j = 0; j < 3; ++j) are[i][j] = aim[i][j] = 0.0;
     double sre = 0.0, sim = 0.0;  // Helmholtz / modified hypersingular: S = sum_p w G
+    // MFIE: the four sums of the pair (MFIE block of rwg.cuh)
+    double pbr = 0.0, pbi = 0.0, pcr[3] = {0.0, 0.0, 0.0}, pci[3] = {0.0, 0.0, 0.0};
+    double qbr[3] = {0.0, 0.0, 0.0}, qbi[3] = {0.0, 0.0, 0.0}, qcr[3] = {0.0, 0.0, 0.0}, qci[3] = {0.0, 0.0, 0.0};
 
     const int64_t toff = prm.toff[k], soff = prm.soff[k], woff = prm.woff[k];
     const int n = (int)prm.npts[k];
@@ -140,36 +143,64 @@ __global__ void __launch_bounds__(32 * SING_WARPS) singular_pairs(SingParams prm
                     }
                 }
             } else {
+                // H = w G (ikr - 1) / r^2 and d = x - y; with w_t = J_t (xi, eta), w_s likewise, the four sums
+                // PB = sum w_t . (H w_s x d), PC = sum (H d) x w_t, QB = sum H w_s x d, QC = sum H d
                 const double df[3] = {x[0] - y[0], x[1] - y[1], x[2] - y[2]};
                 const double d2 = df[0] * df[0] + df[1] * df[1] + df[2] * df[2];
                 const double d = sqrt(d2);
                 const cplx f = cmul(kw, cplx{(-ki * d - 1.0) / d2, kr * d / d2});
+                double wt[3], ws[3];
 #pragma unroll
-                for (int i = 0; i < 3; ++i)
+                for (int c = 0; c < 3; ++c) {
+                    wt[c] = fma(gt.j1[c], tpm.y, gt.j0[c] * tpm.x);
+                    ws[c] = fma(gs.j1[c], spm.y, gs.j0[c] * spm.x);
+                }
+                const double wxd[3] = {fma(ws[1], df[2], -ws[2] * df[1]), fma(ws[2], df[0], -ws[0] * df[2]),
+                                       fma(ws[0], df[1], -ws[1] * df[0])};
+                const double dxw[3] = {fma(df[1], wt[2], -df[2] * wt[1]), fma(df[2], wt[0], -df[0] * wt[2]),
+                                       fma(df[0], wt[1], -df[1] * wt[0])};
+                const double pb = fma(wt[2], wxd[2], fma(wt[1], wxd[1], wt[0] * wxd[0]));
+                pbr = fma(f.re, pb, pbr);
+                pbi = fma(f.im, pb, pbi);
 #pragma unroll
-                    for (int j = 0; j < 3; ++j) {
-                        const double c0 = bt[i][1] * bs[j][2] - bt[i][2] * bs[j][1];
-                        const double c1 = bt[i][2] * bs[j][0] - bt[i][0] * bs[j][2];
-                        const double c2 = bt[i][0] * bs[j][1] - bt[i][1] * bs[j][0];
-                        const double tr = df[0] * c0 + df[1] * c1 + df[2] * c2;
-                        are[i][j] += f.re * tr;
-                        aim[i][j] += f.im * tr;
-                    }
+                for (int c = 0; c < 3; ++c) {
+                    pcr[c] = fma(f.re, dxw[c], pcr[c]);
+                    pci[c] = fma(f.im, dxw[c], pci[c]);
+                    qbr[c] = fma(f.re, wxd[c], qbr[c]);
+                    qbi[c] = fma(f.im, wxd[c], qbi[c]);
+                    qcr[c] = fma(f.re, df[c], qcr[c]);
+                    qci[c] = fma(f.im, df[c], qci[c]);
+                }
             }
         }
     }
 
     // reduce across the warp
     constexpr bool HYP_K = HYP && ASM != BEMPPCUDA_ASM_LAPLACE_HYP;
+    constexpr bool MFIE = ASM == BEMPPCUDA_ASM_MFIE;
     if (HYP_K) {
         sre = warp_sum(sre);
         sim = warp_sum(sim);
+    }
+    if (MFIE) {
+        pbr = warp_sum(pbr);
+        pbi = warp_sum(pbi);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            pcr[c] = warp_sum(pcr[c]);
+            pci[c] = warp_sum(pci[c]);
+            qbr[c] = warp_sum(qbr[c]);
+            qbi[c] = warp_sum(qbi[c]);
+            qcr[c] = warp_sum(qcr[c]);
+            qci[c] = warp_sum(qci[c]);
+        }
     }
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
-            const bool live = (ASM == BEMPPCUDA_ASM_LAPLACE_HYP) ? (i == 0 && j == 0) : (i < nt && j < ns);
+            const bool live = MFIE ? false : (ASM == BEMPPCUDA_ASM_LAPLACE_HYP) ? (i == 0 && j == 0)
+                                                                             : (i < nt && j < ns);
             if (live) {
                 are[i][j] = warp_sum(are[i][j]);
                 aim[i][j] = warp_sum(aim[i][j]);
@@ -177,7 +208,8 @@ __global__ void __launch_bounds__(32 * SING_WARPS) singular_pairs(SingParams prm
         }
     if (lane != 0) return;
     const double scale = gt.ie * gs.ie;
-    double eb_re[3][3], eb_im[3][3];  // EFIE block from the moments (the |J| factors cancel)
+    double eb_re[3][3], eb_im[3][3];  // EFIE / MFIE block from the moments or sums (the |J| factors cancel)
+    if (MFIE) mfie_block(pbr, pbi, pcr, pci, qbr, qbi, qcr, qci, gt.j0, gt.j1, gs.j0, gs.j1, eb_re, eb_im);
     if (ASM == BEMPPCUDA_ASM_EFIE) {
         if (ki != 0.0)
             efie_block<true>(are, aim, gt.j0, gt.j1, gs.j0, gs.j1, kr, ki, eb_re, eb_im);
@@ -201,7 +233,7 @@ __global__ void __launch_bounds__(32 * SING_WARPS) singular_pairs(SingParams prm
                 const double mr = are[i][j] * normal_prod, mi = aim[i][j] * normal_prod;
                 vr = fma(cp[i][j], sre, fma(k2r, mr, -k2i * mi)) * scale;
                 vi = fma(cp[i][j], sim, fma(k2r, mi, k2i * mr)) * scale;
-            } else if (ASM == BEMPPCUDA_ASM_EFIE) {
+            } else if (MAXWELL) {
                 const double f = edge_length(prm.g, prm.ne, t, i) * edge_length(prm.g, prm.ne, s, j);
                 vr = eb_re[i][j] * f;
                 vi = eb_im[i][j] * f;
