@@ -433,17 +433,19 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar(PotParams prm, in
 // point closer to an element than that (evaluation next to the surface)
 // takes that element's sources in FP64 instead (`near_r` = 4 kappa R, 0 when R
 // is unknown: no FP64 fallback).
-template <int K, int PHC>
+// NQ > 0 fixes the sources per element at compile time (the pair loop unrolls);
+// NQ = 0 reads it from prm.nq.
+template <int K, int PHC, int NQ>
 __global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams prm, int64_t chunk_elems,
                                                                       double near_r) {
     constexpr bool HELM = (K == BEMPPCUDA_HELMHOLTZ_SLP || K == BEMPPCUDA_HELMHOLTZ_DLP);
     constexpr bool DLP = (K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_HELMHOLTZ_DLP);
     static_assert(PS_PPT == 2, "two evaluation points per thread, packed");
     __shared__ float4 syo[PS_SOURCES];  // yo, |yo|^2
-    __shared__ float4 scf[PS_SOURCES];  // coefficient re, im, yo . n_e, -
+    __shared__ float4 scf[PS_SOURCES];  // coefficient re, im, yo . n_e, -im
     __shared__ double scen[PS_SOURCES * 3];
     __shared__ float snrm[DLP ? PS_SOURCES * 3 : 3];
-    const int nq = prm.nq;
+    const int nq = NQ > 0 ? NQ : prm.nq;
     const int tile_elems = PS_SOURCES / nq;
     const int64_t ebeg = (int64_t)blockIdx.y * chunk_elems;
     const int64_t eend = min(ebeg + chunk_elems, prm.nsupport);
@@ -481,7 +483,8 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams p
             syo[s] = make_float4(y0, y1, y2, fmaf(y2, y2, fmaf(y1, y1, y0 * y0)));
             float yn = 0.f;
             if (DLP) yn = fmaf(y2, snrm[3 * e + 2], fmaf(y1, snrm[3 * e + 1], y0 * snrm[3 * e]));
-            scf[s] = make_float4((float)o[6 * n + gs], (float)o[7 * n + gs], yn, 0.f);
+            const float cim = (float)o[7 * n + gs];
+            scf[s] = make_float4((float)o[6 * n + gs], cim, yn, -cim);
         }
         __syncthreads();
         for (int e = 0; e < te; ++e) {
@@ -508,6 +511,7 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams p
             const float2 rcf = f2((float)rc[0], (float)rc[1]);
             const float2 rc2f = f2(rc2h[0], rc2h[1]);
             float2 er = b2(0.f), ei = b2(0.f);
+#pragma unroll(NQ > 0 ? NQ : 1)
             for (int q = 0; q < nq; ++q) {
                 const float4 yo = syo[e * nq + q];
                 const float4 cf = scf[e * nq + q];
@@ -540,7 +544,7 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams p
                         vr = mul2(g, mul2(fma2(rp, sn, cs), b2(-1.f)));
                         vi = mul2(g, fma2(rp, cs, mul2(sn, b2(-1.f))));
                     }
-                    er = fma2(vr, cr, fma2(mul2(vi, b2(-1.f)), ci, er));
+                    er = fma2(vr, cr, fma2(vi, b2(cf.w), er));  // cf.w = -im, exact
                     ei = fma2(vr, ci, fma2(vi, cr, ei));
                 }
             }
@@ -608,92 +612,103 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams p
     }
 }
 
-template <int K, int PHC>
-static cudaError_t launch_scalar_nq(const PotParams &prm, dim3 grid, int64_t chunk_elems, cudaStream_t st) {
-    if (prm.nq == 6)
-        potential_scalar<K, PHC, 6><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems);
-    else
-        potential_scalar<K, PHC, 0><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems);
-    return cudaGetLastError();
-}
-
-
-// Scalar Laplace, Helmholtz (real or complex wavenumber) and modified Helmholtz potentials;
-// phase_radius bounds every source's distance from its element centroid (0: unknown).
-// Grid of the per-point kernels: point blocks x source chunks, enough CTAs for several waves; with
-// more than one chunk the chunks add their sums with atomics into the zeroed result.
-static cudaError_t scalar_grid(const PotParams &prm, dim3 *grid, int64_t *chunk_elems, cudaStream_t st) {
+// Grid of the per-point kernels: point blocks x source chunks; with more than one chunk the
+// chunks add their sums with atomics into the zeroed result.  The chunk count c minimises
+//   ceil(pblocks c / slots) (1/c + 1/64),
+// slots = SMs x resident CTAs of the kernel being launched (occupancy query): the number of
+// waves times the work of one CTA (1/c of its point block's sources) plus a small fixed cost
+// per CTA, so that the grid ends on a full wave rather than on a few CTAs of a second one.
+static cudaError_t scalar_grid(const PotParams &prm, const void *fn, dim3 *grid, int64_t *chunk_elems,
+                               cudaStream_t st) {
+    int resident = 0;
+    cudaError_t err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, fn, PS_THREADS, 0);
+    if (err != cudaSuccess) return err;
+    const int64_t slots = (int64_t)bc_sm_count() * std::max(resident, 1);
     const int64_t pblocks = (prm.npoints + PS_THREADS * PS_PPT - 1) / (PS_THREADS * PS_PPT);
-    const int64_t target = (int64_t)bc_sm_count() * 8;  // CTAs: several waves of 4 resident per SM
-    int64_t chunks = (target + pblocks - 1) / pblocks;
-    chunks = std::min(chunks, (prm.nsupport + PS_CHUNK_MIN - 1) / PS_CHUNK_MIN);
-    chunks = std::max<int64_t>(1, std::min<int64_t>(chunks, 65535));
+    int64_t cmax = std::min<int64_t>((prm.nsupport + PS_CHUNK_MIN - 1) / PS_CHUNK_MIN, 65535);
+    cmax = std::max<int64_t>(1, std::min<int64_t>(cmax, 8 * ((slots + pblocks - 1) / pblocks)));
+    int64_t chunks = 1;
+    double best = 0.0;
+    for (int64_t c = 1; c <= cmax; ++c) {
+        const double t = (double)((pblocks * c + slots - 1) / slots) * (1.0 / (double)c + 1.0 / 64.0);
+        if (c == 1 || t < best) {
+            best = t;
+            chunks = c;
+        }
+    }
     *chunk_elems = (prm.nsupport + chunks - 1) / chunks;
     chunks = (prm.nsupport + *chunk_elems - 1) / *chunk_elems;
     if (chunks > 1) {
-        const cudaError_t err = cudaMemsetAsync(prm.result, 0, sizeof(double) * 2 * prm.npoints, st);
+        err = cudaMemsetAsync(prm.result, 0, sizeof(double) * 2 * prm.npoints, st);
         if (err != cudaSuccess) return err;
     }
     *grid = dim3((unsigned)pblocks, (unsigned)chunks);
     return cudaSuccess;
 }
 
-// Mixed-precision Laplace / Helmholtz (real k) single / double layer potentials.
-static cudaError_t launch_scalar_mixed(const PotParams &prm, int kernel, double phase_radius, cudaStream_t st) {
+template <int K, int PHC>
+static cudaError_t launch_scalar_nq(const PotParams &prm, cudaStream_t st) {
+    auto fn = prm.nq == 6 ? potential_scalar<K, PHC, 6> : potential_scalar<K, PHC, 0>;
     dim3 grid;
     int64_t chunk_elems = 0;
-    const cudaError_t err = scalar_grid(prm, &grid, &chunk_elems, st);
+    const cudaError_t err = scalar_grid(prm, (const void *)fn, &grid, &chunk_elems, st);
     if (err != cudaSuccess) return err;
+    fn<<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems);
+    return cudaGetLastError();
+}
+
+template <int K, int PHC>
+static cudaError_t launch_mixed_nq(const PotParams &prm, double near_r, cudaStream_t st) {
+    auto fn = prm.nq == 6 ? potential_scalar_mixed<K, PHC, 6> : potential_scalar_mixed<K, PHC, 0>;
+    dim3 grid;
+    int64_t chunk_elems = 0;
+    const cudaError_t err = scalar_grid(prm, (const void *)fn, &grid, &chunk_elems, st);
+    if (err != cudaSuccess) return err;
+    fn<<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems, near_r);
+    return cudaGetLastError();
+}
+
+// Scalar Laplace, Helmholtz (real or complex wavenumber) and modified Helmholtz potentials;
+// phase_radius bounds every source's distance from its element centroid (0: unknown).
+// Mixed-precision Laplace / Helmholtz (real k) single / double layer potentials.
+static cudaError_t launch_scalar_mixed(const PotParams &prm, int kernel, double phase_radius, cudaStream_t st) {
     const double kr = fabs(prm.p[0]) * phase_radius;
     const int phc = (phase_radius > 0.0 && kr <= 0.5) ? 2 : (phase_radius > 0.0 && kr <= 1.0) ? 1 : 0;
     const bool helm = kernel == BEMPPCUDA_HELMHOLTZ_SLP || kernel == BEMPPCUDA_HELMHOLTZ_DLP;
     const double near_r = 4.0 * (helm ? prm.p[0] : 1.0) * phase_radius;  // in the kernel's units of 1/kappa
     switch (kernel) {
-    case BEMPPCUDA_LAPLACE_SLP: potential_scalar_mixed<BEMPPCUDA_LAPLACE_SLP, 0><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems, near_r); break;
-    case BEMPPCUDA_LAPLACE_DLP: potential_scalar_mixed<BEMPPCUDA_LAPLACE_DLP, 0><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems, near_r); break;
+    case BEMPPCUDA_LAPLACE_SLP: return launch_mixed_nq<BEMPPCUDA_LAPLACE_SLP, 0>(prm, near_r, st);
+    case BEMPPCUDA_LAPLACE_DLP: return launch_mixed_nq<BEMPPCUDA_LAPLACE_DLP, 0>(prm, near_r, st);
     case BEMPPCUDA_HELMHOLTZ_SLP:
-        if (phc == 2)
-            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_SLP, 2><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems, near_r);
-        else if (phc == 1)
-            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_SLP, 1><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems, near_r);
-        else
-            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_SLP, 0><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems, near_r);
-        break;
+        if (phc == 2) return launch_mixed_nq<BEMPPCUDA_HELMHOLTZ_SLP, 2>(prm, near_r, st);
+        if (phc == 1) return launch_mixed_nq<BEMPPCUDA_HELMHOLTZ_SLP, 1>(prm, near_r, st);
+        return launch_mixed_nq<BEMPPCUDA_HELMHOLTZ_SLP, 0>(prm, near_r, st);
     default:  // BEMPPCUDA_HELMHOLTZ_DLP
-        if (phc == 2)
-            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_DLP, 2><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems, near_r);
-        else if (phc == 1)
-            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_DLP, 1><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems, near_r);
-        else
-            potential_scalar_mixed<BEMPPCUDA_HELMHOLTZ_DLP, 0><<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems, near_r);
-        break;
+        if (phc == 2) return launch_mixed_nq<BEMPPCUDA_HELMHOLTZ_DLP, 2>(prm, near_r, st);
+        if (phc == 1) return launch_mixed_nq<BEMPPCUDA_HELMHOLTZ_DLP, 1>(prm, near_r, st);
+        return launch_mixed_nq<BEMPPCUDA_HELMHOLTZ_DLP, 0>(prm, near_r, st);
     }
-    return cudaGetLastError();
 }
 
 static cudaError_t launch_scalar(const PotParams &prm, int kernel, double phase_radius, cudaStream_t st) {
-    dim3 grid;
-    int64_t chunk_elems = 0;
-    const cudaError_t gerr = scalar_grid(prm, &grid, &chunk_elems, st);
-    if (gerr != cudaSuccess) return gerr;
     const double kr = fabs(prm.p[0]) * phase_radius;
     const int phc = prm.p[1] != 0.0 ? 3
                     : (phase_radius > 0.0 && kr <= 0.5) ? 2 : (phase_radius > 0.0 && kr <= 1.0) ? 1 : 0;
     switch (kernel) {
-    case BEMPPCUDA_LAPLACE_SLP: return launch_scalar_nq<BEMPPCUDA_LAPLACE_SLP, 0>(prm, grid, chunk_elems, st);
-    case BEMPPCUDA_LAPLACE_DLP: return launch_scalar_nq<BEMPPCUDA_LAPLACE_DLP, 0>(prm, grid, chunk_elems, st);
-    case BEMPPCUDA_MODHELM_SLP: return launch_scalar_nq<BEMPPCUDA_MODHELM_SLP, 0>(prm, grid, chunk_elems, st);
-    case BEMPPCUDA_MODHELM_DLP: return launch_scalar_nq<BEMPPCUDA_MODHELM_DLP, 0>(prm, grid, chunk_elems, st);
+    case BEMPPCUDA_LAPLACE_SLP: return launch_scalar_nq<BEMPPCUDA_LAPLACE_SLP, 0>(prm, st);
+    case BEMPPCUDA_LAPLACE_DLP: return launch_scalar_nq<BEMPPCUDA_LAPLACE_DLP, 0>(prm, st);
+    case BEMPPCUDA_MODHELM_SLP: return launch_scalar_nq<BEMPPCUDA_MODHELM_SLP, 0>(prm, st);
+    case BEMPPCUDA_MODHELM_DLP: return launch_scalar_nq<BEMPPCUDA_MODHELM_DLP, 0>(prm, st);
     case BEMPPCUDA_HELMHOLTZ_SLP:
-        if (phc == 3) return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_SLP, 3>(prm, grid, chunk_elems, st);
-        if (phc == 2) return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_SLP, 2>(prm, grid, chunk_elems, st);
-        if (phc == 1) return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_SLP, 1>(prm, grid, chunk_elems, st);
-        return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_SLP, 0>(prm, grid, chunk_elems, st);
+        if (phc == 3) return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_SLP, 3>(prm, st);
+        if (phc == 2) return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_SLP, 2>(prm, st);
+        if (phc == 1) return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_SLP, 1>(prm, st);
+        return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_SLP, 0>(prm, st);
     default:  // BEMPPCUDA_HELMHOLTZ_DLP
-        if (phc == 3) return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_DLP, 3>(prm, grid, chunk_elems, st);
-        if (phc == 2) return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_DLP, 2>(prm, grid, chunk_elems, st);
-        if (phc == 1) return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_DLP, 1>(prm, grid, chunk_elems, st);
-        return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_DLP, 0>(prm, grid, chunk_elems, st);
+        if (phc == 3) return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_DLP, 3>(prm, st);
+        if (phc == 2) return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_DLP, 2>(prm, st);
+        if (phc == 1) return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_DLP, 1>(prm, st);
+        return launch_scalar_nq<BEMPPCUDA_HELMHOLTZ_DLP, 0>(prm, st);
     }
 }
 
