@@ -250,9 +250,9 @@ static cudaError_t launch_pot(const PotParams &prm, cudaStream_t st) {
 // block stages in shared memory PS_SOURCES at a time and reads back as
 // broadcasts.  The grid is (point blocks, source chunks): ten thousand points
 // make only a few dozen blocks of 256 points, so the support is split into
-// chunks of whole elements until the grid covers the SMs several times, and
-// the chunks' partial sums are added into the zeroed result with FP64
-// atomics (a single chunk stores directly).
+// chunks of whole elements, as many as fill the SMs' resident CTA slots in
+// whole waves (scalar_grid), and the chunks' partial sums are added into the
+// zeroed result with FP64 atomics (a single chunk stores directly).
 //
 // Helmholtz phase (real k): for a source y of element e with centroid c_e,
 //   k |x - y| = k |x - c_e| + k (|x - y| - |x - c_e|),
