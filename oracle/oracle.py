@@ -240,6 +240,59 @@ def assemble_dense(
     return result
 
 
+class _RowSample(object):
+    """The dual space seen through a row sample: only the test elements that touch a sampled dof
+    are in the support, and ``local2global`` sends every dof to its position in the sample, or to
+    one discard row (index ``len(rows)``) for dofs outside it.  A sampled row then receives every
+    contribution the full assembly gives it, regular and singular, since all its test elements
+    are kept."""
+
+    def __init__(self, space, rows):
+        rows = _np.asarray(rows, dtype=_np.int64)
+        nshape = space.number_of_shape_functions
+        rowmap = _np.full(space.global_dof_count, len(rows), dtype=_np.int64)
+        rowmap[rows] = _np.arange(len(rows))
+        l2g = _np.asarray(space.local2global, dtype=_np.int64).reshape(-1, nshape)
+        support = _np.asarray(space.support, dtype=bool)
+        touch = support & _np.isin(l2g, rows).any(axis=1)
+        self.grid = space.grid
+        self.support = touch
+        self.support_elements = _np.flatnonzero(touch).astype(_np.uint32)
+        self.local2global = _np.where(support[:, None], rowmap[_np.where(support[:, None], l2g, 0)],
+                                      len(rows)).astype(_np.uint32)
+        self.local_multipliers = space.local_multipliers
+        self.normal_multipliers = space.normal_multipliers
+        self.number_of_shape_functions = nshape
+        self.global_dof_count = len(rows) + 1
+        self.localised_space = space.localised_space
+        idx, ptr = space.get_elements_by_color()
+        idx = _np.asarray(idx)
+        keep = touch[idx]
+        counts = _np.add.reduceat(keep.astype(_np.int64), _np.asarray(ptr[:-1])) if len(idx) else []
+        self._colors = (idx[keep], _np.concatenate([[0], _np.cumsum(counts)]).astype(_np.int64))
+
+    def get_elements_by_color(self):
+        return self._colors
+
+
+def assemble_rows(kernel_type, assembly_type, options, is_complex, domain, dual_to_range, rows, quad_points,
+                  quad_weights, singular_order=4):
+    """Rows ``rows`` (global dofs of ``dual_to_range``) of the dense weak form, regular plus singular part.
+
+    Equal to ``assemble_dense(...)[rows]`` (dense_assembler.py:49-98) at the cost of the sampled rows only:
+    a parity check of a matrix too large for the oracle to assemble whole.
+    """
+    from bempp_cuda.quadrature import SingularPairs
+
+    view = _RowSample(dual_to_range, rows)
+    rule = None
+    if domain.grid == dual_to_range.grid:
+        rule = SingularPairs(domain.grid, singular_order, view.support, domain.support).arrays()
+    full = assemble_dense(kernel_type, assembly_type, options, is_complex, domain, view, quad_points, quad_weights,
+                          rule)
+    return full[: len(rows)]
+
+
 def evaluate_potential(kernel_type, assembly_type, options, space, points, coefficients, quad_points, quad_weights):
     """Potential values (kdim, npoints) for global coefficients ``coefficients``."""
     kdim = 3 if assembly_type.startswith("maxwell") else 1
