@@ -54,12 +54,47 @@ def to_device(array, dtype):
     return _torch.as_tensor(_np.ascontiguousarray(array)).to(device="cuda", dtype=dtype, non_blocking=False)
 
 
+def host_grid_arrays(grid):
+    """(vertices (nv, 3) f64, elements (ne, 3) i32) in the device layout, from a ``bempp_cuda`` or
+    ``bempp_cl`` grid (both store (3, nv) vertices and (3, ne) elements, grid.py:24-60)."""
+    vertices = _np.ascontiguousarray(_np.asarray(grid.vertices, dtype=_np.float64).T)
+    elements = _np.ascontiguousarray(_np.asarray(grid.elements).T.astype(_np.int32))
+    return vertices, elements
+
+
+def host_space_arrays(space):
+    """The host arrays a space uploads, from a ``bempp_cuda`` or ``bempp_cl`` function space
+    (space.py:444-459 of the reference): shapeset id, shape count, support (i32), local2global
+    (ne, nshape) i32, local multipliers (ne, nshape) f64, normal multipliers (ne,) i32, dof count,
+    and whether DP0 dof i is support element i with multiplier 1."""
+    nshape = int(space.number_of_shape_functions)
+    support = _np.asarray(space.support_elements, dtype=_np.int64)
+    l2g = _np.asarray(space.local2global).reshape(-1, nshape)
+    mult = _np.asarray(space.local_multipliers, dtype=_np.float64).reshape(-1, nshape)
+    ndofs = int(space.global_dof_count)
+    pos = (
+        nshape == 1
+        and len(support) == ndofs
+        and _np.array_equal(l2g[support, 0], _np.arange(len(support)))
+        and _np.all(mult[support, 0] == 1.0)
+    )
+    return {
+        "shapeset": _lib.SHAPESET_IDS[space.shapeset.identifier],
+        "nshape": nshape,
+        "support": _np.ascontiguousarray(support.astype(_np.int32)),
+        "l2g": _np.ascontiguousarray(l2g.astype(_np.int32)),
+        "mult": _np.ascontiguousarray(mult),
+        "normal_mult": _np.ascontiguousarray(_np.asarray(space.normal_multipliers, dtype=_np.int32)),
+        "ndofs": ndofs,
+        "dof_is_position": 1 if pos else 0,
+    }
+
+
 class DeviceGrid(object):
     """Vertices, elements and the per-element geometry record on the device."""
 
     def __init__(self, grid):
-        vertices = _np.ascontiguousarray(_np.asarray(grid.vertices, dtype=_np.float64).T)
-        elements = _np.ascontiguousarray(_np.asarray(grid.elements).T.astype(_np.int32))
+        vertices, elements = host_grid_arrays(grid)
         self.nvertices = vertices.shape[0]
         self.nelements = elements.shape[0]
         self.vertices = to_device(vertices, _torch.float64)
@@ -101,28 +136,18 @@ class DeviceSpace(object):
     """Support list and dof maps of one space on the device."""
 
     def __init__(self, space):
-        nshape = int(space.number_of_shape_functions)
-        self.nshape = nshape
-        self.shapeset = _lib.SHAPESET_IDS[space.shapeset.identifier]
-        support = _np.asarray(space.support_elements, dtype=_np.int64)
-        l2g = _np.asarray(space.local2global).reshape(-1, nshape)
-        mult = _np.asarray(space.local_multipliers, dtype=_np.float64).reshape(-1, nshape)
-        self.nsupport = len(support)
-        self.ndofs = int(space.global_dof_count)
-        pos = (
-            nshape == 1
-            and self.nsupport == self.ndofs
-            and _np.array_equal(l2g[support, 0], _np.arange(self.nsupport))
-            and _np.all(mult[support, 0] == 1.0)
-        )
-        self.dof_is_position = 1 if pos else 0
+        h = host_space_arrays(space)
+        self.nshape = h["nshape"]
+        self.shapeset = h["shapeset"]
+        self.nsupport = len(h["support"])
+        self.ndofs = h["ndofs"]
+        self.dof_is_position = h["dof_is_position"]
         grid = space.grid
-        self.support = _shared_on_grid(grid, "support", support.astype(_np.int32), _torch.int32)
-        self.l2g = _shared_on_grid(grid, "l2g", l2g.astype(_np.int32), _torch.int32)
-        self.mult = _shared_on_grid(grid, "mult", mult, _torch.float64)
-        nm = _np.asarray(space.normal_multipliers, dtype=_np.int32)
-        self.normal_mult = _shared_on_grid(grid, "normal_mult", nm, _torch.int32)
-        self.h2d_bytes = support.size * 4 + l2g.size * 4 + mult.nbytes + nm.nbytes
+        self.support = _shared_on_grid(grid, "support", h["support"], _torch.int32)
+        self.l2g = _shared_on_grid(grid, "l2g", h["l2g"], _torch.int32)
+        self.mult = _shared_on_grid(grid, "mult", h["mult"], _torch.float64)
+        self.normal_mult = _shared_on_grid(grid, "normal_mult", h["normal_mult"], _torch.int32)
+        self.h2d_bytes = sum(h[name].nbytes for name in ("support", "l2g", "mult", "normal_mult"))
 
     def record(self):
         return _lib.Space(
