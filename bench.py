@@ -17,8 +17,11 @@ pairs + Sauter-Schwab singular pairs + identity), matrix resident in HBM.
 * ``roofline``: the regular-pair kernel (the dominant launch), algorithmic
   flops / CUDA-event time against the FP32 (or FP64) FMA peak measured in the
   same run by ``bemppcuda_fma_probe``.
-* ``cpu_baseline``: the oracle (a C/OpenMP restatement of the reference Numba
-  kernels) on a bounded row sample of the same operator, all host cores.
+* ``cpu_baseline``: the reference's own Numba path (bempp_cl installed under
+  baseline/_ref, through its public API) on a seeded random row sample of the
+  same operator, all host cores; the oracle port when the reference is not
+  importable.  ``parity`` compares the GPU matrices with it on those rows, and
+  the breadth operators with the oracle on 48 rows at their own sizes.
 * ``shape_gradient``: gradients/s of the far-field objective of a perturbed
   L5 sphere (k = 6) with respect to all vertex coordinates and k, with the
   adjoint-kernel cost relative to one forward assembly and a central
@@ -37,8 +40,8 @@ pairs + Sauter-Schwab singular pairs + identity), matrix resident in HBM.
 
 Multi-GPU (torchrun): the rows (test elements) are split into one contiguous
 block per rank; each rank assembles its block with no collective (strong
-scaling, total work fixed).  ``--impl reference`` times the oracle port of the
-reference CPU path on rank 0 only.
+scaling, total work fixed).  ``--impl reference`` times the reference's CPU
+path (as ``cpu_baseline``) on rank 0 only.
 """
 
 import argparse
@@ -65,7 +68,7 @@ FLOPS_PER_QPE = {
 }
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -84,7 +87,7 @@ def parse():
     ap.add_argument("--shape-level", type=int, default=5)
     ap.add_argument("--shape-solver", choices=["lu32", "gmres", "gmres32"], default="lu32")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time per baseline sample")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 def dist_setup(args):
@@ -301,6 +304,13 @@ def gpu_arm(args, world, rank, local):
         ref64 = out.clone() if rows * cols * 16 * 3 < torch.cuda.get_device_properties(local).total_memory * 0.85 else None
     tmx, regmx, singmx, clocks = timed(_lib.MIXED, args.steps, args.warmup, True)
     value = total_entries * args.steps / (tmx * 1e-3)
+    # seeded rows of both matrices for the parity check against the CPU reference (after timing)
+    gpu_rows = None
+    if world == 1:
+        idx = torch.as_tensor(parity_rows(rows), device="cuda")
+        gpu_rows = {"mixed": out.index_select(0, idx).cpu().numpy()}
+        if ref64 is not None:
+            gpu_rows["fp64"] = ref64.index_select(0, idx).cpu().numpy()
     solve = None
     if fp64 is not None:
         fp64["mixed_over_fp64"] = value / fp64["value"]
@@ -329,8 +339,8 @@ def gpu_arm(args, world, rank, local):
                                 "work); the symmetric sweep evaluates each point pair once for A_ij and A_ji, "
                                 "so the hardware evaluates qpe_per_launch / 2 point pairs",
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the same kernel at "
-                              "regular_sphere(5) (profiles/regular_dp0_symmetric_combined_l5.md), scaled by "
-                              "the entry count; the output write is the whole traffic",
+                              "regular_sphere(5), scaled by the entry count; the output write is the whole "
+                              "traffic",
             "peak_source": "bemppcuda_fma_probe, measured in this run"}
     if fp64 is not None:
         a64 = flops / (fp64["regular_ms"] * 1e-3) / 1e12
@@ -360,7 +370,7 @@ def gpu_arm(args, world, rank, local):
         shape = shape_measure(args, torch)
 
     line = {
-        "metric": "entries/s Helmholtz assembly, mixed vs FP64 GPU at rel err <=1e-6; shape-grads/s",
+        "metric": METRIC,
         "value": value,
         "unit": "entries/s",
         "n_gpus": world,
@@ -372,15 +382,9 @@ def gpu_arm(args, world, rank, local):
         "vs_baseline": None,
         "dtype": "f32+f64",
         "data": "synthetic: regular_sphere(%d) unit sphere, generated by octahedron subdivision" % args.level,
-        "config": {
-            "workload": "Helmholtz combined-field DLP - 1/2 I - i k SLP, DP0, regular_sphere(%d), %d x %d complex128, "
-                        "k=%g, regular order 4, singular order 4" % (args.level, grid.number_of_elements,
-                                                                      grid.number_of_elements, args.k),
-            "elements": int(grid.number_of_elements),
-            "precision": "mixed: FP32 regular pairs, FP64 singular pairs and per-entry sums",
-            "parallelism": "row blocks x%d" % world,
-            "l2": "output %.1f GB per step > 126 MB L2; compute-bound kernel" % (total_entries * 16 / 1e9),
-        },
+        "config": bench_config(args),
+        "precision": "mixed: FP32 regular pairs, FP64 singular pairs and per-entry sums",
+        "parallelism": "row blocks x%d" % world,
         "gpu_launches": 2 * args.steps,
         "clocks": clocks,
         "roofline": roof,
@@ -399,7 +403,12 @@ def gpu_arm(args, world, rank, local):
         line["shape_gradient"] = shape
     if breadth is not None:
         line["breadth"] = breadth
-    return line
+        checks = {e["operator"]: e["parity_rel_fro_vs_oracle"] for e in breadth if "parity_rel_fro_vs_oracle" in e}
+        if checks:
+            line["parity"] = {"breadth_fp64_vs_oracle": checks, "bound": 1e-12,
+                              "sample": "48 seeded rows per operator at its configured level; 500 of the 10 000 "
+                                        "potential points"}
+    return line, gpu_rows
 
 
 def hbm_peak():
@@ -721,12 +730,12 @@ def breadth_measure(args, torch, fp64_peak=None, fp32_peak=None):
     """FP64 throughput of the other operator families (dense weak form through the operator API).
 
     GPU: CUDA events around the full assembly (regular + singular passes) of
-    each operator on its configuration, inputs resident.  CPU: the oracle on
-    the same operator one level coarser (4x fewer elements), with all host
-    cores, scaled to the measured level by the number of element pairs (x16);
-    the singular pairs grow only 4x, so the scaled CPU time is an upper bound.
-    Potential: 10 000 points in the shell 1.5 < r < 3 from complex N(0,1) P1
-    coefficients on the level-5 sphere.
+    each operator on its configuration, inputs resident.  CPU: the oracle
+    (port) on 48 seeded rows of the same operator at the same level, with all
+    host cores; the same rows of the GPU matrix are its FP64 parity check
+    (``parity_rel_fro_vs_oracle``, bound 1e-12).  Potential: 10 000 points in
+    the shell 1.5 < r < 3 from complex N(0,1) P1 coefficients on the level-5
+    sphere; the oracle evaluates 500 seeded points of them.
     """
     from bempp_cuda import operators
     from bempp_cuda.quadrature import SingularPairs, triangle_rule
@@ -780,16 +789,19 @@ def breadth_measure(args, torch, fp64_peak=None, fp32_peak=None):
                              "unit": "TFLOP/s", "peak": fp64_peak,
                              "frac": achieved / fp64_peak if fp64_peak else None}
         if not args.skip_cpu:
-            op_c, dom_c, dual_c = build(path, dsp, tsp, level - 1, k)
-            d = op_c.descriptor
+            # oracle (port) on a seeded sample of rows of the same operator: CPU rate and FP64 parity
+            d = op.descriptor
             qp, qw = triangle_rule(4)
-            rule = SingularPairs(dom_c.grid, 4, dual_c.support, dom_c.support).arrays()
+            sample = np.sort(np.random.default_rng(48).choice(rows, min(48, rows), replace=False))
             t0 = time.perf_counter()
-            orc.assemble_dense(d.kernel_type, d.assembly_type, d.options, d.is_complex, dom_c, dual_c, qp, qw, rule)
-            tc = (time.perf_counter() - t0) * 16.0
-            entry["cpu_s_scaled"] = tc
-            entry["cpu_entries_per_s"] = rows * cols / tc
+            ref_rows = orc.assemble_rows(d.kernel_type, d.assembly_type, d.options, d.is_complex, dom, dual, sample,
+                                         qp, qw, 4)
+            tc = time.perf_counter() - t0
+            got = op._assemble().tensor.index_select(0, torch.as_tensor(sample, device="cuda")).cpu().numpy()
+            entry["cpu_rows"] = int(len(sample))
+            entry["cpu_entries_per_s"] = len(sample) * cols / tc
             entry["gpu_over_cpu"] = entry["gpu_entries_per_s"] / entry["cpu_entries_per_s"]
+            entry["parity_rel_fro_vs_oracle"] = float(np.linalg.norm(got - ref_rows) / np.linalg.norm(ref_rows))
         if name.startswith("laplace"):
             # C1 matvec: HBM-bound GEMV on the resident matrix
             mat = op._assemble()
@@ -894,13 +906,18 @@ def breadth_measure(args, torch, fp64_peak=None, fp32_peak=None):
               "note": "gpu_ms: public API call with the host map_to_full_grid product and coefficient upload; "
                       "kernel_ms: device-resident points and element coefficients (source table + evaluation)"}
     if not args.skip_cpu:
+        # oracle (port) at 500 seeded points of the 10 000: CPU rate (scaled to 10 000) and FP64 parity
         qp, qw = triangle_rule(4)
         d = pot.descriptor
+        pick = np.sort(np.random.default_rng(500).choice(10000, 500, replace=False))
         t0 = time.perf_counter()
-        orc.evaluate_potential(d.kernel_type, d.assembly_type, d.options, sp, pts[:, :1000], coeffs, qp, qw)
-        tc = (time.perf_counter() - t0) * 10.0
+        ref_pts = orc.evaluate_potential(d.kernel_type, d.assembly_type, d.options, sp, pts[:, pick], coeffs, qp, qw)
+        tc = (time.perf_counter() - t0) * 20.0
+        got = pot.evaluate(coeffs)[:, pick]
         pentry["cpu_s_scaled"] = tc
         pentry["gpu_over_cpu"] = tc / (pms * 1e-3)
+        pentry["parity_points"] = 500
+        pentry["parity_rel_fro_vs_oracle"] = float(np.linalg.norm(got - ref_pts) / np.linalg.norm(ref_pts))
     out.append(pentry)
     # the same potential with FP32 point-source pairs (device_interface="cuda_mixed")
     from bempp_cuda import _lib
@@ -1020,53 +1037,120 @@ def e2e_measure(args, torch, grid, domain, dual, world, dist, clear_cache, total
 
 
 # ----------------------------------------------------------------------------- CPU arm
-def cpu_sample(args, target_seconds):
-    """Oracle (C/OpenMP port of the reference kernels) on the first R rows of the operator.
+METRIC = "entries/s Helmholtz assembly, mixed vs FP64 GPU at rel err <=1e-6; shape-grads/s"
+PARITY_ROWS = 512  # seeded rows of the benchmark operator kept from the GPU matrices for the CPU comparison
 
-    Returns (entries/s, description).  R is calibrated so one sample takes
-    about ``target_seconds`` on this host.
+
+def bench_config(args):
+    """The workload description both arms print (identical dicts)."""
+    n = 8 * 4**args.level
+    return {
+        "workload": "Helmholtz combined-field DLP - 1/2 I - i k SLP, DP0, regular_sphere(%d), %d x %d complex128, "
+                    "k=%g, regular order 4, singular order 4" % (args.level, n, n, args.k),
+        "elements": n,
+        "k": args.k,
+        "l2": "output %.1f GB per step > 126 MB L2; compute-bound kernel" % (n * n * 16 / 1e9),
+    }
+
+
+def parity_rows(n):
+    """The seeded random rows (test elements) used for CPU timing samples and parity checks."""
+    return np.random.default_rng(20240).permutation(n)[: min(PARITY_ROWS, n)]
+
+
+class CpuReference(object):
+    """The reference's CPU path on a row sample of the benchmark operator.
+
+    With the unmodified bempp_cl importable (installed under baseline/_ref,
+    oracle/reference.py): its own public API with device_interface="numba"
+    -- ``(dlp - 0.5 * identity - 1j * k * slp).weak_form()`` with the dual space
+    restricted to the sampled elements (``support_elements``), so every step
+    runs the reference's regular, singular and sparse assemblers on those rows
+    (kind "reference").  Otherwise the oracle, the C/OpenMP restatement of the
+    reference Numba kernels (kind "port").  Rows are a seeded random sample of
+    the test elements, sized so one step takes about ``target_seconds``.
     """
-    from oracle import oracle as orc
 
-    from bempp_cuda.quadrature import SingularPairs, triangle_rule
-    from bempp_cuda.shapes import regular_sphere
-    from bempp_cuda.space import function_space
+    def __init__(self, args):
+        self.args = args
+        self.n = 8 * 4**args.level
+        from oracle import reference
 
-    grid = regular_sphere(args.level)
-    n = grid.number_of_elements
-    domain = function_space(grid, "DP", 0)
-    qp, qw = triangle_rule(4)
-    eta = -1j * args.k
-    options = [args.k, 0.0, eta.real, eta.imag]
+        self.bempp_cl = reference.load()
+        self.kind = "reference" if self.bempp_cl is not None else "port"
+        self.why_port = None if self.bempp_cl is not None else reference.reason()
+        var = "NUMBA_NUM_THREADS" if self.bempp_cl is not None else "OMP_NUM_THREADS"
+        self.cores = int(os.environ.get(var, os.cpu_count() or 1))
+        from bempp_cuda.shapes import regular_sphere
 
-    def run(r):
-        dual = function_space(grid, "DP", 0, support_elements=np.arange(r))
-        rule = SingularPairs(grid, 4, dual.support, domain.support).arrays()
+        self.grid = regular_sphere(args.level)
+        self._ref_grid = None
+
+    def rows(self, rows):
+        """(matrix rows of ``sorted(rows)``, seconds of the timed call)."""
+        rows = np.sort(np.asarray(rows))
+        k = self.args.k
+        if self.bempp_cl is not None:
+            from oracle import reference
+
+            api = self.bempp_cl.api
+            if self._ref_grid is None:
+                self._ref_grid = reference.grid_from(self.grid)
+            g = self._ref_grid
+            d = api.function_space(g, "DP", 0)
+            t = api.function_space(g, "DP", 0, support_elements=rows)
+            H = api.operators.boundary.helmholtz
+            t0 = time.perf_counter()
+            slp = H.single_layer(d, d, t, k, assembler="dense", device_interface="numba")
+            dlp = H.double_layer(d, d, t, k, assembler="dense", device_interface="numba")
+            ident = api.operators.boundary.sparse.identity(d, d, t)
+            mat = (dlp - 0.5 * ident - 1j * k * slp).weak_form().to_dense()
+            return np.asarray(mat), time.perf_counter() - t0
+        from oracle import oracle as orc
+
+        from bempp_cuda.quadrature import triangle_rule
+        from bempp_cuda.space import function_space
+
+        domain = function_space(self.grid, "DP", 0)
+        qp, qw = triangle_rule(4)
+        eta = -1j * k
         t0 = time.perf_counter()
-        mat = orc.assemble_dense("helmholtz_combined_field", "default_scalar", options, True, domain, dual, qp, qw, rule)
-        mat[np.arange(r), np.arange(r)] += -0.5 * grid.volumes[:r]
-        return time.perf_counter() - t0
+        mat = orc.assemble_rows("helmholtz_combined_field", "default_scalar", [k, 0.0, eta.real, eta.imag], True,
+                                domain, domain, rows, qp, qw, 4)
+        mat[np.arange(len(rows)), rows] += -0.5 * self.grid.volumes[rows]
+        return mat, time.perf_counter() - t0
 
-    orc.lib()
-    t = run(8)
-    r = int(min(n, max(8, 8 * target_seconds / max(t, 1e-3))))
-    return r, run
+    def calibrate(self, target_seconds):
+        """Warm the path (Numba compiles on its first call) and pick the sample size."""
+        sample = parity_rows(self.n)
+        self.rows(sample[:8])
+        _, t = self.rows(sample[:32])
+        self.count = int(min(len(sample), max(32, 32 * target_seconds / max(t, 1e-3))))
+        self.sample = sample[: self.count]
+        return self.count
+
+    def describe(self):
+        if self.bempp_cl is not None:
+            what = ("bempp_cl %s Numba path through its public API (weak_form of the combined field with the "
+                    "dual space on the sampled elements)" % getattr(self.bempp_cl, "__version__", ""))
+        else:
+            what = "oracle port (C/OpenMP restatement of the reference Numba kernels; %s)" % self.why_port
+        return ("%d seeded random rows x %d columns of the %d x %d operator per step, regular + singular + "
+                "identity: %s" % (self.count, self.n, self.n, self.n, what))
 
 
 def reference_arm(args, world, rank):
     if rank != 0:
         return None
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    r, run = cpu_sample(args, args.cpu_seconds)
-    n = 8 * 4**args.level
-    for _ in range(min(args.warmup, 1)):
-        run(max(8, r // 8))
-    times = [run(r) for _ in range(args.steps)]
+    cpu = CpuReference(args)
+    cpu.calibrate(args.cpu_seconds)
+    for _ in range(max(0, args.warmup - 1)):
+        cpu.rows(cpu.sample[: max(8, cpu.count // 8)])
+    times = [cpu.rows(cpu.sample)[1] for _ in range(args.steps)]
     total = sum(times)
-    value = r * n * args.steps / total
-    sample = "%d rows x %d columns of the %d x %d operator per step (regular + singular + identity)" % (r, n, n, n)
+    value = cpu.count * cpu.n * args.steps / total
     return {
-        "metric": "entries/s Helmholtz assembly, mixed vs FP64 GPU at rel err <=1e-6; shape-grads/s",
+        "metric": METRIC,
         "value": value,
         "unit": "entries/s",
         "n_gpus": world,
@@ -1077,13 +1161,30 @@ def reference_arm(args, world, rank):
         "scaling": "strong",
         "vs_baseline": None,
         "dtype": "f64",
-        "data": "synthetic: regular_sphere(%d) unit sphere" % args.level,
-        "config": {"workload": "Helmholtz combined-field DLP - 1/2 I - i k SLP, DP0, regular_sphere(%d), k=%g"
-                               % (args.level, args.k), "elements": n},
+        "data": "synthetic: regular_sphere(%d) unit sphere, generated by octahedron subdivision" % args.level,
+        "config": bench_config(args),
         "impl": "reference",
-        "cpu_baseline": {"value": value, "unit": "entries/s", "cores": cores, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": "entries/s", "cores": cpu.cores, "kind": cpu.kind,
+                         "sample": cpu.describe()},
         "e2e": {"value": value, "unit": "entries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+
+
+def cpu_leg(args, line, gpu_rows):
+    """cpu_baseline of the GPU arm, and the parity of the GPU matrices on the same rows."""
+    cpu = CpuReference(args)
+    cpu.calibrate(args.cpu_seconds)
+    mat, t = cpu.rows(cpu.sample)
+    line["cpu_baseline"] = {"value": cpu.count * cpu.n / t, "unit": "entries/s", "cores": cpu.cores,
+                            "kind": cpu.kind, "sample": cpu.describe()}
+    if gpu_rows is None:
+        return
+    order = np.argsort(cpu.sample)
+    parity = {"rows": int(cpu.count), "against": cpu.kind, "bound_fp64": 1e-12, "bound_mixed": 1e-6}
+    for name, rows in gpu_rows.items():
+        got = rows[: cpu.count][order]
+        parity[name + "_rel_fro"] = float(np.linalg.norm(got - mat) / np.linalg.norm(mat))
+    line.setdefault("parity", {})["benchmark_operator"] = parity
 
 
 def main():
@@ -1098,15 +1199,9 @@ def main():
 
             dist.destroy_process_group()
         return
-    line = gpu_arm(args, world, rank, local)
+    line, gpu_rows = gpu_arm(args, world, rank, local)
     if rank == 0 and world == 1 and not args.skip_cpu:
-        cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-        r, run = cpu_sample(args, args.cpu_seconds)
-        t = run(r)
-        n = 8 * 4**args.level
-        line["cpu_baseline"] = {"value": r * n / t, "unit": "entries/s", "cores": cores, "kind": "port",
-                                "sample": "%d rows x %d columns of the same operator, oracle (C/OpenMP restatement "
-                                          "of the reference Numba kernels)" % (r, n)}
+        cpu_leg(args, line, gpu_rows)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
