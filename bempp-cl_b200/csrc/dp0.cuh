@@ -463,19 +463,17 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __
 template <int PHC>
 __device__ __forceinline__ void sincos2(float2 x, float2 *s, float2 *c) {
     if (PHC == 2) {
+        constexpr float ps[] = BC_SIN_HALF32;
+        constexpr float pc[] = BC_COS_HALF32;
         const float2 x2 = mul2(x, x);
-        *s = fma2(mul2(x, x2), fma2(b2(0.008264548145234585f), x2, b2(-0.1666613519191742f)), x);
-        *c = fma2(x2, fma2(fma2(b2(-0.001377025037072599f), x2, b2(0.04166495054960251f)), x2, b2(-0.4999999403953552f)),
-                  b2(1.0f));
+        *s = fma2(mul2(x, x2), fma2(b2(ps[0]), x2, b2(ps[1])), x);
+        *c = fma2(x2, fma2(fma2(b2(pc[0]), x2, b2(pc[1])), x2, b2(pc[2])), b2(1.0f));
     } else if (PHC == 1) {
+        constexpr float ps[] = BC_SIN_SMALL32;
+        constexpr float pc[] = BC_COS_SMALL32;
         const float2 x2 = mul2(x, x);
-        float2 ps = fma2(b2(-0.00019318617705721408f), x2, b2(0.008330317214131355f));
-        ps = fma2(ps, x2, b2(-0.1666661649942398f));
-        *s = fma2(mul2(x, x2), ps, x);
-        float2 pc = fma2(b2(2.4138245862559415e-05f), x2, b2(-0.0013883339706808329f));
-        pc = fma2(pc, x2, b2(0.041666481643915176f));
-        pc = fma2(pc, x2, b2(-0.4999999701976776f));
-        *c = fma2(x2, pc, b2(1.0f));
+        *s = fma2(mul2(x, x2), fma2(fma2(b2(ps[0]), x2, b2(ps[1])), x2, b2(ps[2])), x);
+        *c = fma2(x2, fma2(fma2(fma2(b2(pc[0]), x2, b2(pc[1])), x2, b2(pc[2])), x2, b2(pc[3])), b2(1.0f));
     } else {
         sincos_cw32(x.x, &s->x, &c->x);
         sincos_cw32(x.y, &s->y, &c->y);

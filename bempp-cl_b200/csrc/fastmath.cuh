@@ -55,6 +55,17 @@ __device__ __forceinline__ void sincos_poly64(double x, const double (&ps)[NS], 
 #define BC_COS_HALF64 {2.0790894217124703e-09, -2.7557077887523167e-07, 2.4801586988836374e-05, \
                        -0.0013888888888705666, 0.041666666666666276, -0.5}
 
+// FP32 minimax coefficients (fit_sincos.py, Lawson's algorithm; highest degree first); maximum
+// absolute errors evaluated in float with fused multiply-adds: half 5.6e-8 / 3.7e-8 on |x| <= 1/2,
+// small 5.7e-8 / 6.1e-8 on |x| <= 1, cw 3.6e-8 / 5.2e-8 on |a| <= pi/4 (sin / cos).
+#define BC_SIN_HALF32 {0.008259795606136322f, -0.16666032373905182f}
+#define BC_COS_HALF32 {-0.001377024920657277f, 0.04166495054960251f, -0.4999999403953552f}
+#define BC_SIN_SMALL32 {-0.00019283789151813835f, 0.00832979753613472f, -0.16666598618030548f}
+#define BC_COS_SMALL32 {2.4138245862559415e-05f, -0.0013883339706808329f, 0.041666481643915176f, \
+                        -0.4999999701976776f}
+#define BC_SIN_CW32 {-0.000194956359337084f, 0.00833197869360447f, -0.16666650772094727f}
+#define BC_COS_CW32 {2.4390450562350452e-05f, -0.0013886763481423259f, 0.04166662320494652f, -0.5f}
+
 __device__ __forceinline__ void sincos_cw64(double x, double *s, double *c) {
     if (!(fabs(x) < 1.0e6)) {
         sincos(x, s, c);
@@ -108,13 +119,13 @@ __device__ __forceinline__ void sincos_half64(double x, double *s, double *c) {
     sincos_poly64(x, ps, pc, s, c);
 }
 
-// |x| <= 1/2 in FP32: degree 5 (sin) and 6 (cos), coefficients fitted by
-// weighted least squares on Chebyshev nodes of [-1/2, 1/2] (max abs error
-// 8e-8 / 5e-8 in FP32 arithmetic).
+// |x| <= 1/2 in FP32: degree 5 (sin) and 6 (cos), BC_*_HALF32.
 __device__ __forceinline__ void sincos_half32(float x, float *s, float *c) {
+    constexpr float ps[] = BC_SIN_HALF32;
+    constexpr float pc[] = BC_COS_HALF32;
     const float x2 = x * x;
-    *s = fmaf(x * x2, fmaf(0.008264548145234585f, x2, -0.1666613519191742f), x);
-    *c = fmaf(x2, fmaf(fmaf(-0.001377025037072599f, x2, 0.04166495054960251f), x2, -0.4999999403953552f), 1.0f);
+    *s = fmaf(x * x2, fmaf(ps[0], x2, ps[1]), x);
+    *c = fmaf(x2, fmaf(fmaf(pc[0], x2, pc[1]), x2, pc[2]), 1.0f);
 }
 
 // Single-instruction FP32 approximations (PTX rsqrt.approx / rcp.approx with
@@ -133,15 +144,13 @@ __device__ __forceinline__ float rcp_approx(float x) {
     return y;
 }
 
+// |x| <= 1 in FP32: degree 7 (sin) and 8 (cos), BC_*_SMALL32.
 __device__ __forceinline__ void sincos_small32(float x, float *s, float *c) {
+    constexpr float ps[] = BC_SIN_SMALL32;
+    constexpr float pc[] = BC_COS_SMALL32;
     const float x2 = x * x;
-    float ps = fmaf(-0.00019318617705721408f, x2, 0.008330317214131355f);
-    ps = fmaf(ps, x2, -0.1666661649942398f);
-    *s = fmaf(x * x2, ps, x);
-    float pc = fmaf(2.4138245862559415e-05f, x2, -0.0013883339706808329f);
-    pc = fmaf(pc, x2, 0.041666481643915176f);
-    pc = fmaf(pc, x2, -0.4999999701976776f);
-    *c = fmaf(x2, pc, 1.0f);
+    *s = fmaf(x * x2, fmaf(fmaf(ps[0], x2, ps[1]), x2, ps[2]), x);
+    *c = fmaf(x2, fmaf(fmaf(fmaf(pc[0], x2, pc[1]), x2, pc[2]), x2, pc[3]), 1.0f);
 }
 
 __device__ __forceinline__ void sincos_cw32(float x, float *s, float *c) {
@@ -151,14 +160,11 @@ __device__ __forceinline__ void sincos_cw32(float x, float *s, float *c) {
     const int q = __float_as_int(t);
     float a = fmaf(-n, 1.5703125f, x);
     a = fmaf(-n, 0.0004838267923332751f, a);
+    constexpr float ps[] = BC_SIN_CW32;
+    constexpr float pc[] = BC_COS_CW32;
     const float a2 = a * a;
-    float ps = fmaf(-0.0001951729936990887f, a2, 0.008332177996635437f);
-    ps = fmaf(ps, a2, -0.16666655242443085f);
-    const float sa = fmaf(a * a2, ps, a);
-    float pc = fmaf(2.4390450562350452e-05f, a2, -0.0013886763481423259f);
-    pc = fmaf(pc, a2, 0.04166662320494652f);
-    pc = fmaf(pc, a2, -0.5f);
-    const float ca = fmaf(a2, pc, 1.0f);
+    const float sa = fmaf(a * a2, fmaf(fmaf(ps[0], a2, ps[1]), a2, ps[2]), a);
+    const float ca = fmaf(a2, fmaf(fmaf(fmaf(pc[0], a2, pc[1]), a2, pc[2]), a2, pc[3]), 1.0f);
     const float ss = (q & 1) ? ca : sa;
     const float cc = (q & 1) ? sa : ca;
     *s = (q & 2) ? -ss : ss;
