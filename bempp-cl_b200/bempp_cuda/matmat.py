@@ -107,37 +107,3 @@ def matmat(mats, xs, ys=None):
               for a, x in zip(mats, xs)]
     BatchedProduct(mats, xs, ys).launch()
     return ys
-
-
-def _main(argv=None):
-    """Time the batched product on `count` random n x n operators with 8 right-hand sides."""
-    import argparse
-
-    ap = argparse.ArgumentParser(description=_main.__doc__)
-    ap.add_argument("--count", type=int, default=3)
-    ap.add_argument("--n", type=int, default=8192)
-    ap.add_argument("--nrhs", type=int, default=8)
-    ap.add_argument("--repeats", type=int, default=5)
-    a = ap.parse_args(argv)
-    gen = _torch.Generator(device="cuda").manual_seed(0)
-    mats = [_torch.randn((a.n, a.n), dtype=_torch.complex128, device="cuda", generator=gen) for _ in range(a.count)]
-    xs = [_torch.randn((a.n, a.nrhs), dtype=_torch.complex128, device="cuda", generator=gen) for _ in range(a.count)]
-    ys = [_torch.empty_like(x) for x in xs]
-    bp = BatchedProduct(mats, xs, ys)
-    bp.launch()
-    _torch.cuda.synchronize()
-    err = max(((y - m @ x).norm() / (m @ x).norm()).item() for m, x, y in zip(mats, xs, ys))
-    e0, e1 = _torch.cuda.Event(enable_timing=True), _torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(a.repeats):
-        bp.launch()
-    e1.record()
-    _torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / a.repeats
-    nbytes = a.count * 16 * (a.n * a.n + 2 * a.n * a.nrhs)
-    print("%d x %d^2, %d rhs: %.3f ms, %.0f GB/s, max rel err vs torch.matmul %.2e"
-          % (a.count, a.n, a.nrhs, ms, nbytes / ms / 1e6, err))
-
-
-if __name__ == "__main__":
-    _main()

@@ -258,7 +258,8 @@ int bemppcuda_assemble_singular(const bemppcuda_singular_args *a, void *stream) 
 
 int64_t bemppcuda_potential_workspace_bytes(const bemppcuda_potential_args *a) {
     if (!a || a->space.nsupport < 0 || a->nq < 1) return 0;
-    return 8 * bc_potential_workspace_doubles(a->space.nsupport, a->nq);
+    const int64_t doubles = bc_potential_workspace_doubles(a->space.nsupport, a->nq);
+    return (doubles < 0 || doubles > INT64_MAX / 8) ? -1 : 8 * doubles;
 }
 
 int bemppcuda_evaluate_potential(const bemppcuda_potential_args *a, void *stream) {
@@ -285,6 +286,11 @@ int bemppcuda_evaluate_potential(const bemppcuda_potential_args *a, void *stream
         return BEMPPCUDA_ERR_INVALID;
     }
     const int64_t need = bemppcuda_potential_workspace_bytes(a);
+    if (need < 0) {
+        bc_set_error("potential: %lld support elements x %d points overflow the workspace size",
+                     (long long)a->space.nsupport, a->nq);
+        return BEMPPCUDA_ERR_INVALID;
+    }
     if (need > 0 && (!a->workspace || a->workspace_bytes < need)) {
         bc_set_error("potential workspace too small: need %lld bytes, got %lld", (long long)need,
                      (long long)a->workspace_bytes);

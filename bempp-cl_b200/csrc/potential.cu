@@ -716,7 +716,11 @@ static cudaError_t launch_scalar(const PotParams &prm, int kernel, double phase_
 
 using namespace bc;
 
-int64_t bc_potential_workspace_doubles(int64_t nsupport, int nq) { return (int64_t)SRC_FIELDS * nsupport * nq; }
+// Doubles of the source table, or -1 when nsupport * nq * SRC_FIELDS does not fit in int64.
+int64_t bc_potential_workspace_doubles(int64_t nsupport, int nq) {
+    if (nsupport < 0 || nq < 1 || nsupport > INT64_MAX / ((int64_t)SRC_FIELDS * nq)) return -1;
+    return (int64_t)SRC_FIELDS * nsupport * nq;
+}
 
 // `workspace` must hold bc_potential_workspace_doubles() doubles.
 int bc_potential_launch(const bemppcuda_potential_args *a, double *workspace, cudaStream_t st) {
@@ -751,6 +755,12 @@ int bc_potential_launch(const bemppcuda_potential_args *a, double *workspace, cu
                                                         a->params[0] > 0.0)))) {
         bc_set_error("mixed-precision potentials: Laplace and Helmholtz (real k > 0) single / double layer only");
         return BEMPPCUDA_ERR_UNSUPPORTED;
+    }
+    // the FP64 treatment of points next to the surface needs the bound R on source offsets
+    if (mixed && !(a->phase_radius > 0.0)) {
+        bc_set_error("mixed-precision potentials need phase_radius > 0 (the largest centroid-to-vertex distance "
+                     "of the grid): points near the surface take FP64 sources within 4 k R of an element");
+        return BEMPPCUDA_ERR_INVALID;
     }
     if (prm.npoints == 0) return BEMPPCUDA_OK;
     if (prm.nsrc > 0) {

@@ -20,9 +20,14 @@
 //    race on it; order them on one stream or with events;
 //  * each call rewrites every workspace entry it reads, so nothing has to
 //    start at zero and the contents left by the previous call do no harm;
-//  * the first call on a device looks up the array's device address with
-//    cudaGetSymbolAddress; make that first call before any stream capture
-//    begins on that device.
+//  * the array's device address comes from cudaGetSymbolAddress on the
+//    current device.  It is looked up again on every call made outside a
+//    stream capture, so a call after cudaDeviceReset (or anything else that
+//    recreates the primary context and reloads the module) uses the array's
+//    new address; a call made while its stream is capturing uses the address
+//    of the last uncaptured call on that device, so make at least one call on
+//    a device before any stream capture begins there, and none across a
+//    context reset inside one capture.
 #include <mutex>
 
 #include "common.cuh"
@@ -38,16 +43,23 @@ constexpr int kMaxDevices = 256;
 std::mutex g_setup_mutex;
 double *g_scratch_address[kMaxDevices] = {nullptr};
 
-// Device address of the scratch array on the current device, looked up once.
-int scratch_address(double **out) {
+// Device address of the scratch array on the current device: looked up on every call outside a
+// stream capture (the address changes when the context is recreated), cached for captured calls.
+int scratch_address(cudaStream_t stream, double **out) {
     int dev = 0;
     cudaError_t err = cudaGetDevice(&dev);
     if (err != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
         bc_set_error("evaluate_potential_noalloc: no usable current device (%s)", cudaGetErrorString(err));
         return BEMPPCUDA_ERR_CUDA;
     }
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    err = cudaStreamIsCapturing(stream, &capture);
+    if (err != cudaSuccess) {
+        bc_set_error("evaluate_potential_noalloc: cudaStreamIsCapturing failed: %s", cudaGetErrorString(err));
+        return BEMPPCUDA_ERR_CUDA;
+    }
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_address[dev]) {
+    if (capture == cudaStreamCaptureStatusNone) {
         void *addr = nullptr;
         err = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
         if (err != cudaSuccess || !addr) {
@@ -56,6 +68,10 @@ int scratch_address(double **out) {
             return BEMPPCUDA_ERR_CUDA;
         }
         g_scratch_address[dev] = static_cast<double *>(addr);
+    } else if (!g_scratch_address[dev]) {
+        bc_set_error("evaluate_potential_noalloc: the first call on device %d is inside a stream capture; make "
+                     "one call on the device before capturing", dev);
+        return BEMPPCUDA_ERR_INVALID;
     }
     *out = g_scratch_address[dev];
     return BEMPPCUDA_OK;
@@ -73,7 +89,7 @@ extern "C" int bemppcuda_evaluate_potential_noalloc(const bemppcuda_potential_ar
         return BEMPPCUDA_ERR_INVALID;
     }
     const int64_t need = bc_potential_workspace_doubles(a->space.nsupport, a->nq);
-    if (need > (int64_t)BEMPPCUDA_NOALLOC_SCRATCH_DOUBLES) {
+    if (need < 0 || need > (int64_t)BEMPPCUDA_NOALLOC_SCRATCH_DOUBLES) {
         bc_set_error(
             "evaluate_potential_noalloc: %lld support elements x %d points need %lld workspace doubles, above the "
             "fixed maximum of %lld; use bemppcuda_evaluate_potential with a caller workspace",
@@ -83,7 +99,7 @@ extern "C" int bemppcuda_evaluate_potential_noalloc(const bemppcuda_potential_ar
     // same argument checks as the allocating entry point, with the fixed array as workspace
     bemppcuda_potential_args local = *a;
     double *scratch = nullptr;
-    int rc = scratch_address(&scratch);
+    int rc = scratch_address((cudaStream_t)stream, &scratch);
     if (rc) return rc;
     local.workspace = scratch;
     local.workspace_bytes = (int64_t)sizeof(double) * (int64_t)BEMPPCUDA_NOALLOC_SCRATCH_DOUBLES;

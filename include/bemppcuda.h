@@ -196,9 +196,13 @@ typedef struct {
     void *result;               /* complex128 (kdim, npoints) */
     void *workspace;            /* bemppcuda_potential_workspace_bytes() bytes */
     int64_t workspace_bytes;
-    double phase_radius;  /* largest centroid-to-vertex distance of the source grid, or 0 (unknown):
+    double phase_radius;  /* largest centroid-to-vertex distance R of the source grid, or 0 (unknown):
                              scalar potentials with a real wavenumber factor exp(ikr) about each
-                             element's centroid and skip the range reduction when |k| R <= 1 */
+                             element's centroid and skip the range reduction when |k| R <= 1.
+                             Required (> 0) under BEMPPCUDA_MIXED, which evaluates an element's
+                             sources in FP64 for points within 4 k R of its centroid (FP32 r^2 of a
+                             point next to the surface would lose accuracy); BEMPPCUDA_ERR_INVALID
+                             otherwise */
 } bemppcuda_potential_args;
 
 /* Batched DP0 assembly (many grids / wavenumbers in one persistent launch).
@@ -306,6 +310,8 @@ int bemppcuda_grid_geometry(const double *vertices, int64_t nvertices, const int
 int bemppcuda_assemble_regular(const bemppcuda_regular_args *args, void *stream);
 int bemppcuda_assemble_singular(const bemppcuda_singular_args *args, void *stream);
 
+/* Bytes of the source table (0 for no sources; -1 when the size overflows int64, which
+   bemppcuda_evaluate_potential rejects with BEMPPCUDA_ERR_INVALID). */
 int64_t bemppcuda_potential_workspace_bytes(const bemppcuda_potential_args *args);
 int bemppcuda_evaluate_potential(const bemppcuda_potential_args *args, void *stream);
 
@@ -322,8 +328,10 @@ int bemppcuda_evaluate_potential(const bemppcuda_potential_args *args, void *str
    Problems whose table exceeds the array (space.nsupport * nq * 14 doubles)
    are rejected with BEMPPCUDA_ERR_WORKSPACE.  All calls on a device share
    the array: calls that can overlap on the GPU race, so order them on one
-   stream.  The first call on a device looks up the array's address; make it
-   before any stream capture starts on that device. */
+   stream.  Every call made outside a stream capture looks the array's device
+   address up again (it moves when the context is recreated, e.g. after
+   cudaDeviceReset); a captured call reuses the last looked-up address, so
+   make one call on a device before any stream capture starts there. */
 #define BEMPPCUDA_NOALLOC_SCRATCH_DOUBLES (3 * 1024 * 1024)
 int bemppcuda_evaluate_potential_noalloc(const bemppcuda_potential_args *args, void *stream);
 

@@ -288,7 +288,9 @@ def main(ref_root):
 
 if __name__ == "__main__":
     argv = [a for a in sys.argv[1:] if not a.startswith("--")]
-    root = argv[0] if argv else "/root/reference"
+    if not argv:
+        sys.exit("usage: make_golden.py REFERENCE_CHECKOUT [--identity]")
+    root = argv[0]
     if "--identity" in sys.argv[1:]:
         make_identity(root)
     else:

@@ -279,7 +279,8 @@ def test_unknown_phase_radius_matches_factored_result():
 
 def test_mixed_precision_argument_checks():
     """Through the C ABI: an unknown precision is invalid; MIXED for a Maxwell potential is unsupported
-    (the host layer then evaluates in FP64); MIXED with an unknown phase radius takes the reduced sincos."""
+    (the host layer then evaluates in FP64); MIXED needs the grid's phase radius (it bounds the points
+    that take FP64 sources next to the surface) and refuses an unknown one."""
     from bempp_cuda import _lib, operators
     from bempp_cuda.assembly import kernel_ids, potential_workspace_bytes, regular_rule
     from bempp_cuda.device import current_stream, device_grid, device_space, ptr
@@ -318,7 +319,10 @@ def test_mixed_precision_argument_checks():
     a.precision = 7
     assert lib.bemppcuda_evaluate_potential(ctypes.byref(a), current_stream()) == _lib.ERR_INVALID
     a.precision = _lib.MIXED
-    a.phase_radius = 0.0  # unknown: phase class 0 (reduced sincos)
+    a.phase_radius = 0.0  # unknown: the near-surface FP64 treatment has no bound, so MIXED refuses it
+    assert lib.bemppcuda_evaluate_potential(ctypes.byref(a), current_stream()) == _lib.ERR_INVALID
+    assert "phase_radius" in _lib.last_error()
+    a.phase_radius = 1.0001 * device_grid(grid).radius
     assert lib.bemppcuda_evaluate_potential(ctypes.byref(a), current_stream()) == _lib.OK
     a.precision = _lib.FP64
     b, keep_b = args_for(p1, operators.potential.helmholtz.single_layer(p1, points, 4.0), 4.0)
