@@ -301,6 +301,7 @@ SIGNATURES = {
     "bemppcuda_last_error": (_ct.c_int, [_ct.c_char_p, _i64]),
     "bemppcuda_grid_geometry": (_ct.c_int, [_vp, _i64, _vp, _i64, _vp, _vp]),
     "bemppcuda_assemble_regular": (_ct.c_int, [_ct.POINTER(RegularArgs), _vp]),
+    "bemppcuda_apply_regular": (_ct.c_int, [_ct.POINTER(RegularArgs), _vp, _vp, _vp]),
     "bemppcuda_assemble_singular": (_ct.c_int, [_ct.POINTER(SingularArgs), _vp]),
     "bemppcuda_potential_workspace_bytes": (_i64, [_ct.POINTER(PotentialArgs)]),
     "bemppcuda_evaluate_potential": (_ct.c_int, [_ct.POINTER(PotentialArgs), _vp]),

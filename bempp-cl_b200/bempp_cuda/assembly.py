@@ -144,6 +144,55 @@ def regular_into(
     return result
 
 
+def apply_regular(y, x, descriptor, domain, dual_to_range, parameters, stream=None):
+    """y += A_reg x in FP64, A_reg the regular part evaluated on the fly (bemppcuda_apply_regular).
+
+    One DP0 space of one grid on both sides (Laplace / Helmholtz single, double,
+    adjoint double layer, combined field); ``x``, ``y`` complex128 device
+    vectors.  The adjacent pairs (the singular part) contribute nothing.
+    """
+    require_cuda()
+    if not same_space(domain, dual_to_range):
+        raise ValueError("apply_regular needs the same DP0 space on both sides")
+    kernel, assembly = kernel_ids(descriptor)
+    space = device_space(domain)
+    grid = device_grid(domain.grid)
+    points, weights = regular_rule(parameters.quadrature.regular)
+    args = _lib.RegularArgs()
+    args.kernel = kernel
+    args.assembly = assembly
+    args.precision = _lib.FP64
+    args.is_complex = 1
+    _set_params(args, descriptor.options)
+    args.test_grid = args.trial_grid = grid.record()
+    args.test = args.trial = space.record()
+    args.grids_identical = 1
+    args.nq = len(weights)
+    args.quad_points = points.ctypes.data
+    args.quad_weights = weights.ctypes.data
+    args.phase_radius = 1.0001 * 2.0 * grid.radius
+    _lib.check(_lib.load().bemppcuda_apply_regular(args, ptr(x), ptr(y), stream or current_stream()))
+    return y
+
+
+def adjacent_part(matrix, domain, dual_to_range, parameters):
+    """The entries of a dense DP0 weak form at the adjacent element pairs (the singular part, with any
+    identity term), as a device CSR matrix.  Both spaces map element e to dof e (same DP0 space)."""
+    grid = domain.grid
+    n = grid.number_of_elements
+    if not (same_space(domain, dual_to_range) and device_space(domain).dof_is_position
+            and int(domain.global_dof_count) == n and tuple(matrix.shape) == (n, n)):
+        raise ValueError("adjacent_part needs one DP0 space on every element of the grid on both sides")
+    rule = device_singular_rule(grid, parameters.quadrature.singular, dual_to_range.support, domain.support)
+    te, se = (_torch.as_tensor(a.astype(_np.int64), device=matrix.device) for a in rule._host_ints[:2])
+    keys = _torch.unique(te * matrix.shape[1] + se)
+    rows, cols = keys // matrix.shape[1], keys % matrix.shape[1]
+    vals = matrix[rows, cols]
+    crow = _torch.zeros(matrix.shape[0] + 1, dtype=_torch.int64, device=matrix.device)
+    crow[1:] = _torch.cumsum(_torch.bincount(rows, minlength=matrix.shape[0]), 0)
+    return _torch.sparse_csr_tensor(crow, cols, vals, size=tuple(matrix.shape))
+
+
 def basis_kind(space):
     """BEMPPCUDA_BASIS_* of a space: RWG, SNC (n x RWG) or scalar."""
     ident = getattr(space, "identifier", "")

@@ -16,8 +16,11 @@ relative-residual test of scipy's gmres).
 
 ``solve_refined`` is mixed-precision iterative refinement: an inner GMRES on
 a complex64 copy of the matrix, corrections accumulated in complex128, and
-the residual b - A x recomputed in complex128 with the complex128 matrix
-after every inner solve, until ||b - A x|| <= tol ||b||.
+the residual b - A x recomputed in complex128 after every inner solve, until
+||b - A x|| <= tol ||b||: with the complex128 matrix, or with the FP64
+operator evaluated matrix-free (``operators.fp64_matvec``) when the matrix is
+a mixed-precision weak form, so that the iterate converges to the FP64
+operator's solution.
 """
 
 import time as _time
@@ -330,18 +333,25 @@ def adjoint_matvec(matrix):
 
 
 def solve_refined(matrix, b, tol=1e-8, inner_tol=1e-4, restart=100, maxiter=2000, max_refinements=20,
-                  inner_dtype=_torch.complex64, adjoint=False, check_every=1):
+                  inner_dtype=_torch.complex64, adjoint=False, check_every=1, residual=None):
     """Mixed-precision iterative refinement of A x = b (or A^H x = b); returns (x, info dict).
 
     ``matrix`` is the (complex128) device matrix; the inner solves use a
-    copy in ``inner_dtype``; residuals are formed in complex128.
+    copy in ``inner_dtype``; residuals are formed in complex128, with
+    ``residual`` (v -> A v, e.g. operators.fp64_matvec: the FP64 operator
+    evaluated matrix-free) when given, else with ``matrix``.  With a mixed
+    precision ``matrix`` and the FP64 ``residual`` the iterate converges to
+    the FP64 operator's solution; the mixed matrix only preconditions.
     """
     low = matrix.to(inner_dtype)
     b = b.to(matrix.dtype)
     if adjoint:
+        if residual is not None:
+            raise ValueError("a residual operator is supported for A x = b only")
         hi, lo = adjoint_matvec(matrix), adjoint_matvec(low)
     else:
-        hi, lo = (lambda v: _torch.mv(matrix, v)), (lambda v: _torch.mv(low, v))
+        hi = residual if residual is not None else (lambda v: _torch.mv(matrix, v))
+        lo = lambda v: _torch.mv(low, v)  # noqa: E731
     x, info = refine_gmres(hi, lo, b, tol=tol, inner_tol=inner_tol, restart=restart, maxiter=maxiter,
                            max_refinements=max_refinements, inner_dtype=inner_dtype, check_every=check_every)
     del low

@@ -332,6 +332,49 @@ def _fused_combined_field(op):
     return DenseDeviceOperator(mat)
 
 
+def fp64_matvec(op, matrix):
+    """v -> A v with A the FP64 weak form of ``op``, given ``matrix``, a dense weak form of ``op`` held in
+    lower precision (``device_interface="cuda_mixed"``): the adjacent element pairs (singular part and
+    identity, FP64 in every precision) are taken from ``matrix`` once, the regular part is evaluated
+    on the fly in FP64 by the matrix-free apply (csrc/apply.cu), never stored.
+
+    ``op``: a DP0 Helmholtz combined field a*DLP + b*SLP + c*I, or a Laplace / Helmholtz single,
+    double or adjoint double layer, on one DP0 space of one grid.  This is the residual product of
+    the refined solve (linalg.solve_refined), whose corrections then converge to the FP64 solution.
+    """
+    parts = _combined_field_parts(op) if isinstance(op, (_SumOperator, _ScaledOperator)) else None
+    if parts is not None:
+        a, eta, _, d = parts
+        opts = list(_np.asarray(d.descriptor.options, dtype=float)[:2]) + [eta.real, eta.imag]
+        desc = OperatorDescriptor("helmholtz_combined_field_boundary", opts, "helmholtz_combined_field",
+                                  "default_scalar", "double", True, None, 1)
+        leaf = d
+    elif getattr(op, "descriptor", None) is not None and not isinstance(op, IdentityOperator):
+        a, desc, leaf = 1.0, op.descriptor, op
+    else:
+        raise ValueError("fp64_matvec: a DP0 combined field or a single DP0 boundary operator is required")
+    tensor = matrix.tensor if isinstance(matrix, DenseDeviceOperator) else matrix
+    return fp64_matvec_of(desc, a, leaf.domain, leaf.parameters, tensor)
+
+
+def fp64_matvec_of(descriptor, coefficient, space, parameters, matrix):
+    """``fp64_matvec`` from its parts: v -> S v + coefficient * A_reg v, S the entries of ``matrix`` at
+    the adjacent element pairs of the DP0 ``space``, A_reg the regular part of ``descriptor`` on it."""
+    from .assembly import adjacent_part, apply_regular
+
+    singular = adjacent_part(matrix, space, space, parameters)
+
+    def matvec(v):
+        v = v.to(_torch.complex128)
+        y = _torch.zeros(matrix.shape[0], dtype=_torch.complex128, device=v.device)
+        apply_regular(y, v, descriptor, space, space, parameters)
+        if coefficient != 1.0:
+            y.mul_(coefficient)
+        return y + _torch.mv(singular, v)
+
+    return matvec
+
+
 def weak_form_to_host(op, out=None, blocks=16):
     """The dense weak form of ``op`` as a host tensor (pinned unless ``out`` is given).
 

@@ -8,6 +8,7 @@
 #include "common.cuh"
 
 int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st);
+int bc_apply_launch(const bemppcuda_regular_args *a, const void *x, void *y, cudaStream_t st);
 int bc_singular_launch(const bemppcuda_singular_args *a, cudaStream_t st);
 int bc_potential_launch(const bemppcuda_potential_args *a, double *workspace, cudaStream_t st);
 int64_t bc_potential_workspace_doubles(int64_t nsupport, int nq);
@@ -228,6 +229,25 @@ int bemppcuda_assemble_regular(const bemppcuda_regular_args *a, void *stream) {
         return BEMPPCUDA_ERR_INVALID;
     }
     return bc_regular_launch(a, (cudaStream_t)stream);
+}
+
+int bemppcuda_apply_regular(const bemppcuda_regular_args *a, const void *x, void *y, void *stream) {
+    if (!a) {
+        bc_set_error("null argument struct");
+        return BEMPPCUDA_ERR_INVALID;
+    }
+    if (bad_grid(a->test_grid, "test grid") || bad_grid(a->trial_grid, "trial grid")) return BEMPPCUDA_ERR_INVALID;
+    if (bad_space(a->test, "test space", true) || bad_space(a->trial, "trial space", true)) return BEMPPCUDA_ERR_INVALID;
+    if (bad_params(a->params, a->kernel, a->assembly)) return BEMPPCUDA_ERR_INVALID;
+    if (a->nq < 1 || a->nq > BEMPPCUDA_MAX_REGULAR_POINTS || !a->quad_points || !a->quad_weights) {
+        bc_set_error("regular rule: 1 <= nq <= %d host points and weights required", BEMPPCUDA_MAX_REGULAR_POINTS);
+        return BEMPPCUDA_ERR_INVALID;
+    }
+    if ((a->trial.nsupport > 0 && !x) || (a->test.nsupport > 0 && !y)) {
+        bc_set_error("apply_regular: x / y missing");
+        return BEMPPCUDA_ERR_INVALID;
+    }
+    return bc_apply_launch(a, x, y, (cudaStream_t)stream);
 }
 
 int bemppcuda_assemble_singular(const bemppcuda_singular_args *a, void *stream) {

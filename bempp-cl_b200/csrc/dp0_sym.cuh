@@ -48,13 +48,14 @@ struct TestBlock64s {
 // varies over the pair).  G(x, y) = G(y, x) for complex k too, so the sweep is unchanged.
 // Modified Helmholtz (real, w = p[0]): the Laplace sums with exp(-w r) (single layer) and
 // exp(-w r) (1 + w r) (double layers) per point pair.
-template <int K, int PHC>
-__device__ __forceinline__ void regular_dp0_fp64_sym_tile(const RegParams &prm, const QuadRule &rule,
-                                                        int64_t tile_x, int64_t t0, int rows, TestBlock64s &sb) {
-    using ST = SymTraits<K>;
-    constexpr bool PH = (PHC == 1 || PHC == 2) && ST::helm;
-    constexpr bool CK = PHC == 3 && ST::helm;
-    const int tcount = (int)min((int64_t)rows, prm.ntest - t0);
+//
+// The tile is split into three steps shared by the assembly (stores A_ij, A_ji) and the
+// matrix-free apply (accumulates A x): staging the test block, loading a thread's trial
+// element, and the sweep over the 36 point pairs of one element pair.
+
+// Stage test elements t0 .. t0 + tcount - 1 (points, centroids, normals, areas, vertex ids).
+__device__ __forceinline__ void stage_sym64(const RegParams &prm, const QuadRule &rule, int64_t t0, int tcount,
+                                            TestBlock64s &sb) {
     for (int idx = threadIdx.x; idx < tcount; idx += blockDim.x) {
         const int64_t t = prm.tsup[t0 + idx];
         Geom g;
@@ -76,154 +77,184 @@ __device__ __forceinline__ void regular_dp0_fp64_sym_tile(const RegParams &prm, 
         }
         sb.ie[idx] = g.ie;
     }
+}
+
+// One thread's trial element: geometry, vertex ids, centroid (phase classes 1, 2) and points.
+struct SymTrial64 {
+    Geom gs;
+    int sv0, sv1, sv2;
+    double sc[3];
+    double y[NQ6][3];
+};
+
+template <int K, int PHC>
+__device__ __forceinline__ void load_trial_sym64(const RegParams &prm, const QuadRule &rule, int64_t si,
+                                                 SymTrial64 &tr) {
+    constexpr bool PH = (PHC == 1 || PHC == 2) && SymTraits<K>::helm;
+    const int64_t s = prm.ssup[si];
+    load_geom(prm.sg, prm.sne, s, prm.snm ? (double)prm.snm[s] : 1.0, tr.gs);
+    tr.sv0 = __ldg(prm.sel + 3 * s);
+    tr.sv1 = __ldg(prm.sel + 3 * s + 1);
+    tr.sv2 = __ldg(prm.sel + 3 * s + 2);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) tr.sc[d] = PH ? __ldg(prm.sg + (22 + d) * prm.sne + s) : 0.0;
+#pragma unroll
+    for (int q = 0; q < NQ6; ++q) to_global(tr.gs, rule.x[q], rule.y[q], tr.y[q]);
+}
+
+// A_ij and A_ji of the non-adjacent pair (test element tt of the block, the thread's trial element).
+template <int K, int PHC>
+__device__ __forceinline__ void pair_sym64(const RegParams &prm, const QuadRule &rule, const TestBlock64s &sb,
+                                           int tt, const SymTrial64 &tr, double &a_re, double &a_im, double &b_re,
+                                           double &b_im) {
+    using ST = SymTraits<K>;
+    constexpr bool PH = (PHC == 1 || PHC == 2) && ST::helm;
+    constexpr bool CK = PHC == 3 && ST::helm;
+    const Geom &gs = tr.gs;
+    const double kr = prm.p[0], ki = CK ? prm.p[1] : 0.0, etar = prm.p[2], etai = prm.p[3];
+    double rc = 0.0, ph_s = 0.0, ph_c = 1.0;
+    if (PH) {
+        const double D0 = tr.sc[0] - sb.c[tt][0], D1 = tr.sc[1] - sb.c[tt][1], D2 = tr.sc[2] - sb.c[tt][2];
+        rc = sqrt(fma(D2, D2, fma(D1, D1, D0 * D0)));
+        sincos_cw64(kr * rc, &ph_s, &ph_c);
+    }
+    // Normal terms: (y - x).n_j = (v0_j - x).n_j since y lies in the plane of j (one value per
+    // test point, applied after the sum over q), and (x - y).n_i = (c_i - y).n_i since x lies in
+    // the plane of i (one value per trial point)
+    double ynt[NQ6];
+    if (ST::dlp_part)
+#pragma unroll
+        for (int q = 0; q < NQ6; ++q)
+            ynt[q] = fma(sb.c[tt][2] - tr.y[q][2], sb.n[tt][2],
+                         fma(sb.c[tt][1] - tr.y[q][1], sb.n[tt][1], (sb.c[tt][0] - tr.y[q][0]) * sb.n[tt][0]));
+    double s0r = 0.0, s0i = 0.0, u_re = 0.0, u_im = 0.0, v_re = 0.0, v_im = 0.0;
+    for (int p = 0; p < NQ6; ++p) {
+        const double x0 = sb.x[tt][p][0], x1 = sb.x[tt][p][1], x2 = sb.x[tt][p][2];
+        double xn = 0.0;
+        if (ST::dlp_part)
+            xn = fma(gs.v0[2] - x2, gs.n[2], fma(gs.v0[1] - x1, gs.n[1], (gs.v0[0] - x0) * gs.n[0]));
+        double pr = 0.0, pi = 0.0, ur = 0.0, ui = 0.0, vr = 0.0, vi = 0.0;
+#pragma unroll
+        for (int q = 0; q < NQ6; ++q) {
+            const double d0 = tr.y[q][0] - x0, d1 = tr.y[q][1] - x1, d2 = tr.y[q][2] - x2;
+            const double r2 = fma(d2, d2, fma(d1, d1, d0 * d0));
+            const double rinv = rsqrt64(r2);
+            const double f = rule.w[q] * rinv;
+            if (!ST::helm) {
+                double e = 1.0, e1 = 1.0;  // modified Helmholtz: exp(-w r), exp(-w r) (1 + w r)
+                if (ST::modhelm) {
+                    const double r = r2 * rinv;
+                    e = exp(-kr * r);
+                    e1 = e * fma(kr, r, 1.0);
+                }
+                if (ST::slp_part) pr = ST::modhelm ? fma(f, e, pr) : pr + f;
+                if (ST::dlp_part) {
+                    const double g3 = ST::modhelm ? f * rinv * rinv * e1 : f * rinv * rinv;
+                    ur += g3;
+                    vr = fma(g3, ynt[q], vr);
+                }
+            } else {
+                const double r = r2 * rinv;
+                double sn, cs;
+                if (PH && PHC == 2)
+                    sincos_half64(kr * (r - rc), &sn, &cs);
+                else if (PH)
+                    sincos_small64(kr * (r - rc), &sn, &cs);
+                else
+                    sincos_cw64(kr * r, &sn, &cs);
+                if (CK) {
+                    const double am = exp(-ki * r);
+                    sn *= am;
+                    cs *= am;
+                }
+                if (ST::slp_part) {
+                    pr = fma(f, cs, pr);
+                    pi = fma(f, sn, pi);
+                }
+                if (ST::dlp_part) {
+                    // (ikr - 1) e^{ikr} / r^3: -h1 + i h2 per unit f (dot) / r
+                    const double fr = f * rinv, rk = CK ? rinv + ki : rinv;
+                    const double h1 = fma(rk, cs, kr * sn), h2 = fma(kr, cs, -rk * sn);
+                    const double gt = fr * ynt[q];
+                    ur = fma(fr, h1, ur);
+                    ui = fma(fr, h2, ui);
+                    vr = fma(gt, h1, vr);
+                    vi = fma(gt, h2, vi);
+                }
+            }
+        }
+        const double wp = rule.w[p], wpn = wp * xn;
+        s0r = fma(wp, pr, s0r);
+        s0i = fma(wp, pi, s0i);
+        u_re = fma(wpn, ur, u_re);
+        u_im = fma(wpn, ui, u_im);
+        v_re = fma(wp, vr, v_re);
+        v_im = fma(wp, vi, v_im);
+    }
+    // kernel values: Laplace DLP -sum f dot / r^2; Helmholtz DLP -u_re + i u_im
+    double dr = 0.0, di = 0.0, er = 0.0, ei = 0.0;  // double-layer parts of A_ij, A_ji
+    if (ST::dlp_part) {
+        dr = -u_re;
+        di = ST::helm ? u_im : 0.0;
+        er = -v_re;
+        ei = ST::helm ? v_im : 0.0;
+    }
+    if (K == BEMPPCUDA_HELMHOLTZ_COMBINED) {
+        const double sr = fma(etar, s0r, -etai * s0i), sim = fma(etar, s0i, etai * s0r);
+        a_re = dr + sr;
+        a_im = di + sim;
+        b_re = er + sr;
+        b_im = ei + sim;
+    } else if (ST::slp_part) {
+        a_re = b_re = s0r;
+        a_im = b_im = s0i;
+    } else if (ST::swap) {
+        a_re = er;
+        a_im = ei;
+        b_re = dr;
+        b_im = di;
+    } else {
+        a_re = dr;
+        a_im = di;
+        b_re = er;
+        b_im = ei;
+    }
+    const double scale = BC_INV_4PI * sb.ie[tt] * gs.ie;
+    if (PH) {
+        double t = a_re * ph_c - a_im * ph_s;
+        a_im = (a_re * ph_s + a_im * ph_c) * scale;
+        a_re = t * scale;
+        t = b_re * ph_c - b_im * ph_s;
+        b_im = (b_re * ph_s + b_im * ph_c) * scale;
+        b_re = t * scale;
+    } else {
+        a_re *= scale;
+        a_im *= scale;
+        b_re *= scale;
+        b_im *= scale;
+    }
+}
+
+template <int K, int PHC>
+__device__ __forceinline__ void regular_dp0_fp64_sym_tile(const RegParams &prm, const QuadRule &rule,
+                                                        int64_t tile_x, int64_t t0, int rows, TestBlock64s &sb) {
+    const int tcount = (int)min((int64_t)rows, prm.ntest - t0);
+    stage_sym64(prm, rule, t0, tcount, sb);
     __syncthreads();
 
     const int64_t si = tile_x * DP0_THREADS + threadIdx.x;
     if (si < prm.ntrial && t0 <= si) {
-    const int64_t s = prm.ssup[si];
-    Geom gs;
-    load_geom(prm.sg, prm.sne, s, prm.snm ? (double)prm.snm[s] : 1.0, gs);
-    const int sv0 = __ldg(prm.sel + 3 * s), sv1 = __ldg(prm.sel + 3 * s + 1), sv2 = __ldg(prm.sel + 3 * s + 2);
-    double sc[3] = {0.0, 0.0, 0.0};
-    if (PH)
-#pragma unroll
-        for (int d = 0; d < 3; ++d) sc[d] = __ldg(prm.sg + (22 + d) * prm.sne + s);
-    double y[NQ6][3];
-#pragma unroll
-    for (int q = 0; q < NQ6; ++q) to_global(gs, rule.x[q], rule.y[q], y[q]);
-    const double kr = prm.p[0], ki = CK ? prm.p[1] : 0.0, etar = prm.p[2], etai = prm.p[3];
-
-    for (int tt = 0; tt < tcount; ++tt) {
-        const int64_t row = t0 + tt;
-        if (row > si) break;  // rows increase with tt: the rest of this column lies below the diagonal
-        const bool adj = row == si || (prm.grids_identical && shares_vertex(sb.v[tt], sv0, sv1, sv2));
-        double a_re = 0.0, a_im = 0.0, b_re = 0.0, b_im = 0.0;  // A_ij, A_ji
-        if (!adj) {
-            double rc = 0.0, ph_s = 0.0, ph_c = 1.0;
-            if (PH) {
-                const double D0 = sc[0] - sb.c[tt][0], D1 = sc[1] - sb.c[tt][1], D2 = sc[2] - sb.c[tt][2];
-                rc = sqrt(fma(D2, D2, fma(D1, D1, D0 * D0)));
-                sincos_cw64(kr * rc, &ph_s, &ph_c);
-            }
-            // Normal terms: (y - x).n_j = (v0_j - x).n_j since y lies in the plane of j (one value per
-            // test point, applied after the sum over q), and (x - y).n_i = (c_i - y).n_i since x lies in
-            // the plane of i (one value per trial point)
-            double ynt[NQ6];
-            if (ST::dlp_part)
-#pragma unroll
-                for (int q = 0; q < NQ6; ++q)
-                    ynt[q] = fma(sb.c[tt][2] - y[q][2], sb.n[tt][2],
-                                 fma(sb.c[tt][1] - y[q][1], sb.n[tt][1], (sb.c[tt][0] - y[q][0]) * sb.n[tt][0]));
-            double s0r = 0.0, s0i = 0.0, u_re = 0.0, u_im = 0.0, v_re = 0.0, v_im = 0.0;
-            for (int p = 0; p < NQ6; ++p) {
-                const double x0 = sb.x[tt][p][0], x1 = sb.x[tt][p][1], x2 = sb.x[tt][p][2];
-                double xn = 0.0;
-                if (ST::dlp_part)
-                    xn = fma(gs.v0[2] - x2, gs.n[2], fma(gs.v0[1] - x1, gs.n[1], (gs.v0[0] - x0) * gs.n[0]));
-                double pr = 0.0, pi = 0.0, ur = 0.0, ui = 0.0, vr = 0.0, vi = 0.0;
-#pragma unroll
-                for (int q = 0; q < NQ6; ++q) {
-                    const double d0 = y[q][0] - x0, d1 = y[q][1] - x1, d2 = y[q][2] - x2;
-                    const double r2 = fma(d2, d2, fma(d1, d1, d0 * d0));
-                    const double rinv = rsqrt64(r2);
-                    const double f = rule.w[q] * rinv;
-                    if (!ST::helm) {
-                        double e = 1.0, e1 = 1.0;  // modified Helmholtz: exp(-w r), exp(-w r) (1 + w r)
-                        if (ST::modhelm) {
-                            const double r = r2 * rinv;
-                            e = exp(-kr * r);
-                            e1 = e * fma(kr, r, 1.0);
-                        }
-                        if (ST::slp_part) pr = ST::modhelm ? fma(f, e, pr) : pr + f;
-                        if (ST::dlp_part) {
-                            const double g3 = ST::modhelm ? f * rinv * rinv * e1 : f * rinv * rinv;
-                            ur += g3;
-                            vr = fma(g3, ynt[q], vr);
-                        }
-                    } else {
-                        const double r = r2 * rinv;
-                        double sn, cs;
-                        if (PH && PHC == 2)
-                            sincos_half64(kr * (r - rc), &sn, &cs);
-                        else if (PH)
-                            sincos_small64(kr * (r - rc), &sn, &cs);
-                        else
-                            sincos_cw64(kr * r, &sn, &cs);
-                        if (CK) {
-                            const double am = exp(-ki * r);
-                            sn *= am;
-                            cs *= am;
-                        }
-                        if (ST::slp_part) {
-                            pr = fma(f, cs, pr);
-                            pi = fma(f, sn, pi);
-                        }
-                        if (ST::dlp_part) {
-                            // (ikr - 1) e^{ikr} / r^3: -h1 + i h2 per unit f (dot) / r
-                            const double fr = f * rinv, rk = CK ? rinv + ki : rinv;
-                            const double h1 = fma(rk, cs, kr * sn), h2 = fma(kr, cs, -rk * sn);
-                            const double gt = fr * ynt[q];
-                            ur = fma(fr, h1, ur);
-                            ui = fma(fr, h2, ui);
-                            vr = fma(gt, h1, vr);
-                            vi = fma(gt, h2, vi);
-                        }
-                    }
-                }
-                const double wp = rule.w[p], wpn = wp * xn;
-                s0r = fma(wp, pr, s0r);
-                s0i = fma(wp, pi, s0i);
-                u_re = fma(wpn, ur, u_re);
-                u_im = fma(wpn, ui, u_im);
-                v_re = fma(wp, vr, v_re);
-                v_im = fma(wp, vi, v_im);
-            }
-            // kernel values: Laplace DLP -sum f dot / r^2; Helmholtz DLP -u_re + i u_im
-            double dr = 0.0, di = 0.0, er = 0.0, ei = 0.0;  // double-layer parts of A_ij, A_ji
-            if (ST::dlp_part) {
-                dr = -u_re;
-                di = ST::helm ? u_im : 0.0;
-                er = -v_re;
-                ei = ST::helm ? v_im : 0.0;
-            }
-            if (K == BEMPPCUDA_HELMHOLTZ_COMBINED) {
-                const double sr = fma(etar, s0r, -etai * s0i), sim = fma(etar, s0i, etai * s0r);
-                a_re = dr + sr;
-                a_im = di + sim;
-                b_re = er + sr;
-                b_im = ei + sim;
-            } else if (ST::slp_part) {
-                a_re = b_re = s0r;
-                a_im = b_im = s0i;
-            } else if (ST::swap) {
-                a_re = er;
-                a_im = ei;
-                b_re = dr;
-                b_im = di;
-            } else {
-                a_re = dr;
-                a_im = di;
-                b_re = er;
-                b_im = ei;
-            }
-            const double scale = BC_INV_4PI * sb.ie[tt] * gs.ie;
-            if (PH) {
-                double tr = a_re * ph_c - a_im * ph_s;
-                a_im = (a_re * ph_s + a_im * ph_c) * scale;
-                a_re = tr * scale;
-                tr = b_re * ph_c - b_im * ph_s;
-                b_im = (b_re * ph_s + b_im * ph_c) * scale;
-                b_re = tr * scale;
-            } else {
-                a_re *= scale;
-                a_im *= scale;
-                b_re *= scale;
-                b_im *= scale;
-            }
+        SymTrial64 tr;
+        load_trial_sym64<K, PHC>(prm, rule, si, tr);
+        for (int tt = 0; tt < tcount; ++tt) {
+            const int64_t row = t0 + tt;
+            if (row > si) break;  // rows increase with tt: the rest of this column lies below the diagonal
+            const bool adj = row == si || (prm.grids_identical && shares_vertex(sb.v[tt], tr.sv0, tr.sv1, tr.sv2));
+            double a_re = 0.0, a_im = 0.0, b_re = 0.0, b_im = 0.0;  // A_ij, A_ji
+            if (!adj) pair_sym64<K, PHC>(prm, rule, sb, tt, tr, a_re, a_im, b_re, b_im);
+            store_entry(prm, row, si, adj, a_re, a_im);
+            if (row != si) store_entry(prm, si, row, adj, b_re, b_im);
         }
-        store_entry(prm, row, si, adj, a_re, a_im);
-        if (row != si) store_entry(prm, si, row, adj, b_re, b_im);
-    }
     }
     __syncthreads();  // the shared block is reused by the next tile of a persistent loop
 }

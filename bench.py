@@ -319,7 +319,7 @@ def gpu_arm(args, world, rank, local):
             fp64["mixed_rel_fro_err"] = float(err.item())
             if not args.skip_solve:
                 if world == 1:
-                    solve = solve_measure(args, torch, grid, domain, ref64, out)
+                    solve = solve_measure(args, torch, grid, domain, ref64, out, desc, params)
                 else:
                     solve = solve_measure_distributed(args, torch, grid, domain, ref64, world, rank, dist)
             del ref64
@@ -447,10 +447,14 @@ def matvec_measure(torch, a64):
     return out
 
 
-def solve_measure(args, torch, grid, domain, a64, amx):
-    """C3 solve: plane wave exp(i k z), FP64 GMRES vs mixed assembly + FP64-residual refinement."""
+def solve_measure(args, torch, grid, domain, a64, amx, desc, params):
+    """C3 solve: plane wave exp(i k z).  FP64 GMRES on the FP64 matrix against the mixed matrix with
+    iterative refinement whose residuals use the FP64 operator, evaluated matrix-free (the mixed
+    matrix only preconditions the corrections), both to relative residual 1e-8; then both again to
+    1e-11, where the two solutions must agree to 1e-8."""
     from bempp_cuda.grid_function import GridFunction
     from bempp_cuda.linalg import gmres_tensor, solve_refined
+    from bempp_cuda.operators import fp64_matvec_of
 
     k = args.k
 
@@ -458,24 +462,47 @@ def solve_measure(args, torch, grid, domain, a64, amx):
         result[0] = -np.exp(1j * k * x[2])
 
     b = torch.as_tensor(GridFunction(domain, fun=minus_incident).projections(domain), device="cuda")
+    fp64_apply = fp64_matvec_of(desc, 1.0, domain, params, amx)
     # warm-up (first-call costs of the solver's kernels and host loop), so both solves are timed warm
     gmres_tensor(lambda v: torch.mv(a64, v), b, tol=1e-8, restart=200, maxiter=5)
+    fp64_apply(b)
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    x64, info, res, its = gmres_tensor(lambda v: torch.mv(a64, v), b, tol=1e-8, restart=200, maxiter=2000)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(3):
+        fp64_apply(b)
+    e1.record()
     torch.cuda.synchronize()
-    t64 = time.perf_counter() - t0
-    xmx, rinfo = solve_refined(amx, b, tol=1e-8, inner_tol=1e-4, restart=200)
-    matvec = matvec_measure(torch, a64)
-    diff = float((torch.linalg.norm(xmx - x64) / torch.linalg.norm(x64)).item())
-    res_true = float((torch.linalg.norm(b - torch.mv(a64, xmx)) / torch.linalg.norm(b)).item())
-    return {"rhs": "projection of -exp(i k z) onto DP0", "tol": 1e-8,
+    apply_ms = e0.elapsed_time(e1) / 3
+    out = {"rhs": "projection of -exp(i k z) onto DP0", "fp64_residual_apply_ms": apply_ms,
+           "fp64_residual_apply_note": "FP64 operator product without the FP64 matrix: regular pairs evaluated "
+                                       "on the fly (bemppcuda_apply_regular) + adjacent entries of the mixed matrix"}
+    solutions = {}
+    for tol in (1e-8, 1e-11):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        x64, info, res, its = gmres_tensor(lambda v: torch.mv(a64, v), b, tol=tol, restart=200, maxiter=2000)
+        torch.cuda.synchronize()
+        t64 = time.perf_counter() - t0
+        xmx, rinfo = solve_refined(amx, b, tol=tol, inner_tol=1e-4, restart=200, residual=fp64_apply)
+        res_true = float((torch.linalg.norm(b - torch.mv(a64, xmx)) / torch.linalg.norm(b)).item())
+        out["tol_%g" % tol] = {
             "fp64": {"iterations": its, "info": info, "seconds": t64, "final_residual": res[-1]},
             "mixed_refined": {"refinements": rinfo["refinements"], "inner_iterations": rinfo["inner_iterations"],
                               "residuals": rinfo["relative_residuals"], "seconds": rinfo["seconds"],
-                              "inner_dtype": "complex64"},
-            "solution_rel_diff_vs_fp64": diff, "mixed_solution_residual_in_fp64_operator": res_true,
-            "matvec": matvec}
+                              "inner_dtype": "complex64", "residual_operator": "FP64, matrix-free"},
+            "mixed_solution_residual_in_fp64_matrix": res_true,
+        }
+        solutions[tol] = (x64, xmx)
+    x64, xmx = solutions[1e-11]
+    out["solution_rel_diff_vs_fp64"] = float((torch.linalg.norm(xmx - x64) / torch.linalg.norm(x64)).item())
+    x64, xmx = solutions[1e-8]
+    out["solution_rel_diff_vs_fp64_at_tol_1e-8"] = float(
+        (torch.linalg.norm(xmx - x64) / torch.linalg.norm(x64)).item())
+    out["note"] = ("solution_rel_diff_vs_fp64 compares both solves run to relative residual 1e-11 (bound 1e-8); "
+                   "at 1e-8 each solution carries its own GMRES error of about cond x 1e-8")
+    out["matvec"] = matvec_measure(torch, a64)
+    return out
 
 
 def batch_measure(args, torch, world, rank, dist, count=64, levels=(3, 4, 5)):

@@ -310,6 +310,19 @@ int bemppcuda_grid_geometry(const double *vertices, int64_t nvertices, const int
 int bemppcuda_assemble_regular(const bemppcuda_regular_args *args, void *stream);
 int bemppcuda_assemble_singular(const bemppcuda_singular_args *args, void *stream);
 
+/* Matrix-free FP64 apply of the regular part: y += A_reg x, complex128 vectors (x: trial.nsupport
+   entries, y: test.nsupport), A_reg the Galerkin matrix of the non-adjacent element pairs evaluated on
+   the fly (never stored).  Adjacent pairs and the diagonal contribute nothing here: they are the
+   singular part.  Replaces the residual product of the reference's solve, b - A x with the assembled
+   weak form (api/linalg/iterative_solvers.py:47-93, discrete_boundary_operator.py:192-198), for a
+   matrix that is held in lower precision: same regular entries as bemppcuda_assemble_regular in
+   FP64, summed in another order.  Scope: Laplace / Helmholtz single, double, adjoint double layer
+   and the combined field (params as for the assembly) on one DP0 space of one grid (identity dof
+   map, the same device arrays on both sides) with the 6-point rule and precision FP64; anything else
+   returns BEMPPCUDA_ERR_UNSUPPORTED.  result / ld / overwrite / row_begin / row_end are ignored.
+   y is updated with atomics: the summation order is not deterministic. */
+int bemppcuda_apply_regular(const bemppcuda_regular_args *args, const void *x, void *y, void *stream);
+
 /* Bytes of the source table (0 for no sources; -1 when the size overflows int64, which
    bemppcuda_evaluate_potential rejects with BEMPPCUDA_ERR_INVALID). */
 int64_t bemppcuda_potential_workspace_bytes(const bemppcuda_potential_args *args);

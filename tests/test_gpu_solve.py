@@ -63,26 +63,33 @@ def test_device_gmres_matches_direct_solve():
 
 
 def test_mixed_refinement_matches_fp64_solve():
-    """Mixed-precision assembly + FP64-residual refinement against the FP64 solve (L4, k = 10)."""
+    """Mixed-precision assembly + refinement with FP64 residuals (the FP64 operator evaluated
+    matrix-free) against the FP64 solve (L4, k = 10): within 1e-8, the bound of the benchmark's
+    precision configuration; residuals with the mixed matrix instead stop at its own solution."""
     from bempp_cuda.grid_function import GridFunction
     from bempp_cuda.linalg import gmres_tensor, solve_refined
+    from bempp_cuda.operators import fp64_matvec
     from bempp_cuda.shapes import regular_sphere
     from bempp_cuda.space import function_space
 
     k = 10.0
     sp = function_space(regular_sphere(4), "DP", 0)
     a64 = _combined(sp, k, "cuda").weak_form().tensor
-    amx = _combined(sp, k, "cuda_mixed").weak_form().tensor
+    opmx = _combined(sp, k, "cuda_mixed")
+    amx = opmx.weak_form().tensor
     op_err = (torch.linalg.norm(amx - a64) / torch.linalg.norm(a64)).item()
     assert op_err < 1e-6
     b = torch.as_tensor(GridFunction(sp, fun=_plane_wave(k)).projections(sp), device="cuda")
-    x64, info, _, _ = gmres_tensor(lambda v: torch.mv(a64, v), b, tol=1e-10, restart=200)
+    x64, info, _, _ = gmres_tensor(lambda v: torch.mv(a64, v), b, tol=1e-12, restart=200)
     assert info == 0
-    xmx, rinfo = solve_refined(amx, b, tol=1e-10, inner_tol=1e-4)
+    xmx, rinfo = solve_refined(amx, b, tol=1e-10, inner_tol=1e-4, residual=fp64_matvec(opmx, amx))
     assert rinfo["converged"]
-    # the mixed system differs from the FP64 one by op_err; the solutions by about cond * op_err
     diff = (torch.linalg.norm(xmx - x64) / torch.linalg.norm(x64)).item()
-    assert diff < 100 * op_err + 1e-9, (diff, op_err)
+    assert diff < 1e-8, (diff, op_err)
+    # residuals with the mixed matrix converge to the mixed operator's solution instead
+    xm2, _ = solve_refined(amx, b, tol=1e-10, inner_tol=1e-4)
+    diff_mixed = (torch.linalg.norm(xm2 - x64) / torch.linalg.norm(x64)).item()
+    assert diff < diff_mixed
 
 
 def test_block_gmres_eight_rhs_on_device():
