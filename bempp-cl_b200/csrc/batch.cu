@@ -35,6 +35,7 @@ union TileShared {
     TestBlock64s b64s;
     TestBlock32 b32;
     TestBlock32p b32p;
+    TestBlock32q b32q;
 };
 
 template <int K>
@@ -81,11 +82,11 @@ __device__ __forceinline__ void run_tile_sym(const BatchDev &P, const QuadRule &
             regular_dp0_fp64_sym_tile<K, 0>(P.prm, rule, tx, t0, rows, sh.b64s);
     } else {
         if (P.phase_class == 2)
-            regular_dp0_mixed_sym_tile<K, 2>(P.prm, rule, tx, t0, rows, sh.b32p);
+            regular_dp0_mixed_sym_tile<K, 2>(P.prm, rule, tx, t0, rows, sh.b32q);
         else if (P.phase_class == 1)
-            regular_dp0_mixed_sym_tile<K, 1>(P.prm, rule, tx, t0, rows, sh.b32p);
+            regular_dp0_mixed_sym_tile<K, 1>(P.prm, rule, tx, t0, rows, sh.b32q);
         else
-            regular_dp0_mixed_sym_tile<K, 0>(P.prm, rule, tx, t0, rows, sh.b32p);
+            regular_dp0_mixed_sym_tile<K, 0>(P.prm, rule, tx, t0, rows, sh.b32q);
     }
 }
 
@@ -294,6 +295,7 @@ extern "C" int bemppcuda_batch_prepare(const bemppcuda_batch_args *a, void *stre
         tiles += tiles_of(p.grid.nelements, d.rows, d.sym != 0);
         d.pair_begin = p.pair_begin;
         d.precision = p.precision;
+        r.near_r = p.phase_radius > 0.0 ? p.phase_radius : 0.0;  // 2 R bounds adjacent centroid distances
         const double theta = fabs(p.params[0]) * p.phase_radius;
         d.phase_class = p.phase_radius > 0.0 ? (theta <= 0.5 ? 2 : (theta <= 1.0 ? 1 : 0)) : 0;
         d.ck = p.params[1] != 0.0;

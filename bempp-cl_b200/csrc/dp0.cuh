@@ -28,6 +28,7 @@ struct RegParams {
     double p[4];
     void *result;
     int64_t ld;
+    double near_r;  // bound on the centroid distance of vertex-sharing pairs (0: unknown, test every pair)
 };
 
 constexpr int DP0_THREADS = 128;

@@ -263,13 +263,89 @@ __device__ __forceinline__ void regular_dp0_fp64_sym_tile(const RegParams &prm, 
 
 namespace bc {
 
+// Test block of the packed symmetric sweep: per test point the scaled offset
+// o = kappa (x_p - c_t) as -2 o, each component stored twice so that it is an
+// f32x2 operand straight from shared memory, and |o|^2.
+struct TestBlock32q {
+    float4 mxy[DP0_TCHUNK][NQ6];  // (-2 o_x, -2 o_x, -2 o_y, -2 o_y)
+    float4 mzw[DP0_TCHUNK][NQ6];  // (-2 o_z, -2 o_z, |o|^2, |o|^2)
+    double c[DP0_TCHUNK][3];      // centroid
+    float4 n[DP0_TCHUNK];         // unit normal (fourth entry unused)
+    double ie[DP0_TCHUNK];
+    int v[DP0_TCHUNK][3];
+};
+
+// exp(i x) for the centroid distance x >= 0 of an element pair (units of 1/k, below 1e6): Cody-Waite
+// reduction by pi/2 in FP64 (two-part constant), then the FP32 minimax polynomials on |a| <= pi/4.
+// The reduced argument keeps its FP64 accuracy until it is rounded to FP32, so the phase is
+// within 1e-7 of exp(i x) for any x in range; the FP32 sums it multiplies carry errors of the
+// same size.
+__device__ __forceinline__ void phase_reduced32(double x, float *s, float *c) {
+    const double magic = 6755399441055744.0;  // 1.5 * 2^52: adding it rounds to an integer
+    const double t = fma(x, 0.6366197723675814, magic);
+    const double n = t - magic;
+    const int q = __double2loint(t);
+    double a = fma(-n, 1.5707963267948966, x);
+    a = fma(-n, 6.123233995736766e-17, a);
+    const float af = (float)a;
+    constexpr float ps[] = BC_SIN_CW32;
+    constexpr float pc[] = BC_COS_CW32;
+    const float a2 = af * af;
+    const float sa = fmaf(af * a2, fmaf(fmaf(ps[0], a2, ps[1]), a2, ps[2]), af);
+    const float ca = fmaf(a2, fmaf(fmaf(fmaf(pc[0], a2, pc[1]), a2, pc[2]), a2, pc[3]), 1.0f);
+    // quadrant q: sin = (s, c, -s, -c), cos = (c, -s, -c, s)
+    const float ss = (q & 1) ? ca : sa;
+    const float cc = (q & 1) ? sa : ca;
+    *s = (q & 2) ? -ss : ss;
+    *c = ((q + 1) & 2) ? -cc : cc;
+}
+
+// sin / cos of the point-pair phase offsets of the symmetric sweep (|x| <= 1/2 for phase class
+// 2, |x| <= 1 for class 1): the sine by the FP32 minimax polynomial, the cosine by the hardware
+// approximation cos.approx.f32 (absolute error below 1e-6 on these ranges; the operator error of
+// the sweep measured against FP64 is 1.3e-8 either way).  The cosine moves from the FMA pipe
+// to the special-function unit, which this kernel leaves partly idle (its reciprocal and
+// reciprocal square root are the other users); the sine stays a polynomial, since both
+// functions on that unit saturate it.  Class 0 reduces the argument first (sincos2).
+__device__ __forceinline__ float hw_cos(float x) {
+    float y;
+    asm("cos.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+template <int PHC>
+__device__ __forceinline__ void sincos2_sym(float2 x, float2 *s, float2 *c) {
+    if (PHC == 2 || PHC == 1) {
+        const float2 x2 = mul2(x, x);
+        if (PHC == 2) {
+            constexpr float ps[] = BC_SIN_HALF32;
+            *s = fma2(mul2(x, x2), fma2(b2(ps[0]), x2, b2(ps[1])), x);
+        } else {
+            constexpr float ps[] = BC_SIN_SMALL32;
+            *s = fma2(mul2(x, x2), fma2(fma2(b2(ps[0]), x2, b2(ps[1])), x2, b2(ps[2])), x);
+        }
+        *c = f2(hw_cos(x.x), hw_cos(x.y));
+    } else {
+        sincos2<PHC>(x, s, c);
+    }
+}
+
 // Packed mixed precision in wavenumber-scaled units (as regular_dp0_mixed2_tile).
 // Per point pair, with g = w (d'.n) / r'^2 and the shared factors
 // h1 = cos / r' + sin, h2 = cos - sin / r', the double-layer part of an entry
 // is -g h1 + i g h2 (times kappa^2); the two entries differ only in (d'.n).
+//
+// Per element pair: the centroid offset D and |D|^2 in FP64 (r_c' for the
+// phase), FP32 copies for the point-pair terms; elements whose centroids are
+// farther apart than prm.near_r cannot share a vertex, so the vertex test
+// runs only for near pairs; the pair phase exp(i r_c') by phase_reduced32.
+// The six test points form two orbits of equal weight (w_a for points 0-2,
+// w_b for 3-5, the order-4 rule): the FP32 sums of the first orbit are scaled
+// by w_a / w_b when the second begins, and everything is converted to FP64
+// once, times w_b.
 template <int K, int PHC>
 __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm, const QuadRule &rule,
-                                                         int64_t tile_x, int64_t t0, int rows, TestBlock32p &sb) {
+                                                         int64_t tile_x, int64_t t0, int rows, TestBlock32q &sb) {
     using ST = SymTraits<K>;
     constexpr int NP = NQ6 / 2;
     const double kap = ST::helm ? prm.p[0] : 1.0;  // callers guarantee k > 0 for the Helmholtz family
@@ -286,14 +362,16 @@ __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm,
             to_global(g, rule.x[p], rule.y[p], x);
             const float o0 = (float)(kap * (x[0] - c[0])), o1 = (float)(kap * (x[1] - c[1])),
                         o2 = (float)(kap * (x[2] - c[2]));
-            sb.m[idx][p] = make_float4(-2.f * o0, -2.f * o1, -2.f * o2, fmaf(o2, o2, fmaf(o1, o1, o0 * o0)));
+            const float m2 = fmaf(o2, o2, fmaf(o1, o1, o0 * o0));
+            sb.mxy[idx][p] = make_float4(-2.f * o0, -2.f * o0, -2.f * o1, -2.f * o1);
+            sb.mzw[idx][p] = make_float4(-2.f * o2, -2.f * o2, m2, m2);
         }
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             sb.c[idx][d] = c[d];
-            sb.n[idx][d] = (float)g.n[d];
             sb.v[idx][d] = __ldg(prm.tel + 3 * t + d);
         }
+        sb.n[idx] = make_float4((float)g.n[0], (float)g.n[1], (float)g.n[2], 0.f);
         sb.ie[idx] = g.ie;
     }
     __syncthreads();
@@ -328,19 +406,25 @@ __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm,
     const double ek_r = (K == BEMPPCUDA_HELMHOLTZ_COMBINED) ? kap * prm.p[2] : kap;
     const double ek_i = (K == BEMPPCUDA_HELMHOLTZ_COMBINED) ? kap * prm.p[3] : 0.0;
     const double k2d = kap * kap;
+    // test-point weights: w_b for the second orbit, w_a / w_b applied in FP32 to the first
+    const double wb = rule.w[NQ6 - 1];
+    const float2 rho2 = b2((float)(rule.w[0] / wb));
+    // centroid distances below near_r (scaled) may belong to vertex-sharing pairs
+    const double near2 = prm.near_r > 0.0 ? (kap * prm.near_r) * (kap * prm.near_r) : 1e300;
 
     for (int tt = 0; tt < tcount; ++tt) {
         const int64_t row = t0 + tt;
         if (row > si) break;
-        const bool adj = row == si || (prm.grids_identical && shares_vertex(sb.v[tt], sv0, sv1, sv2));
+        const double D0 = kap * (sc[0] - sb.c[tt][0]), D1 = kap * (sc[1] - sb.c[tt][1]),
+                     D2 = kap * (sc[2] - sb.c[tt][2]);
+        const double rc2 = fma(D2, D2, fma(D1, D1, D0 * D0));
+        const bool adj = row == si ||
+                         (prm.grids_identical && rc2 <= near2 && shares_vertex(sb.v[tt], sv0, sv1, sv2));
         double a_re = 0.0, a_im = 0.0, b_re = 0.0, b_im = 0.0;  // A_ij, A_ji
         if (!adj) {
-            const double D0 = kap * (sc[0] - sb.c[tt][0]), D1 = kap * (sc[1] - sb.c[tt][1]),
-                         D2 = kap * (sc[2] - sb.c[tt][2]);
-            const double rc2 = fma(D2, D2, fma(D1, D1, D0 * D0));
-            const double rc = sqrt(rc2);
-            double ph_s = 0.0, ph_c = 1.0;
-            if (ST::helm) sincos_cw64(rc, &ph_s, &ph_c);
+            const double rc = rc2 * rsqrt64(rc2);
+            float ph_s = 0.f, ph_c = 1.f;
+            if (ST::helm) phase_reduced32(rc, &ph_s, &ph_c);
             const float D0f = (float)D0, D1f = (float)D1, D2f = (float)D2;
             const float2 rcf2 = b2((float)rc), rc2f2 = b2((float)rc2);
             // k (y - x).n_j = cp_p (y lies in the plane of j, so (y - c_j).n_j = 0) and
@@ -348,11 +432,11 @@ __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm,
             float nh0 = 0.f, nh1 = 0.f, nh2 = 0.f, Dn = 0.f;
             float2 ynt[NP];
             if (ST::dlp_part) {
-                const float tn0 = sb.n[tt][0], tn1 = sb.n[tt][1], tn2 = sb.n[tt][2];
-                const float2 Dt = b2(-fmaf(D2f, tn2, fmaf(D1f, tn1, D0f * tn0)));
+                const float4 tn = sb.n[tt];
+                const float2 Dt = b2(-fmaf(D2f, tn.z, fmaf(D1f, tn.y, D0f * tn.x)));
 #pragma unroll
                 for (int j = 0; j < NP; ++j)
-                    ynt[j] = fma2(yz[j], b2(-tn2), fma2(yyy[j], b2(-tn1), fma2(yx[j], b2(-tn0), Dt)));
+                    ynt[j] = fma2(yz[j], b2(-tn.z), fma2(yyy[j], b2(-tn.y), fma2(yx[j], b2(-tn.x), Dt)));
                 Dn = fmaf(D2f, sn2, fmaf(D1f, sn1, D0f * sn0));
                 nh0 = 0.5f * sn0;
                 nh1 = 0.5f * sn1;
@@ -363,13 +447,21 @@ __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm,
 #pragma unroll
             for (int j = 0; j < NP; ++j) A[j] = fma2(D2d, yz[j], fma2(D1d, yyy[j], fma2(D0d, yx[j], yy2[j])));
             float2 s0r = b2(0.f), s0i = b2(0.f), ur = b2(0.f), ui = b2(0.f), vr = b2(0.f), vi = b2(0.f);
-#pragma unroll 2
+#pragma unroll
             for (int p = 0; p < NQ6; ++p) {
-                const float4 m = sb.m[tt][p];
-                const float Bp = fmaf(D2f, m.z, fmaf(D1f, m.y, fmaf(D0f, m.x, m.w)));
-                const float2 mx = b2(m.x), my = b2(m.y), mz = b2(m.z), Bp2 = b2(Bp);
+                if (p == NQ6 / 2) {  // second orbit: the first orbit's sums times w_a / w_b
+                    s0r = mul2(s0r, rho2);
+                    s0i = mul2(s0i, rho2);
+                    ur = mul2(ur, rho2);
+                    ui = mul2(ui, rho2);
+                    vr = mul2(vr, rho2);
+                    vi = mul2(vi, rho2);
+                }
+                const float4 mxy = sb.mxy[tt][p], mzw = sb.mzw[tt][p];
+                const float2 mx = f2(mxy.x, mxy.y), my = f2(mxy.z, mxy.w), mz = f2(mzw.x, mzw.y);
+                const float2 Bp2 = b2(fmaf(D2f, mzw.x, fmaf(D1f, mxy.z, fmaf(D0f, mxy.x, mzw.z))));
                 float2 cp2 = b2(0.f);
-                if (ST::dlp_part) cp2 = b2(fmaf(m.z, nh2, fmaf(m.y, nh1, fmaf(m.x, nh0, Dn))));
+                if (ST::dlp_part) cp2 = b2(fmaf(mzw.x, nh2, fmaf(mxy.z, nh1, fmaf(mxy.x, nh0, Dn))));
                 float2 pur = b2(0.f), pui = b2(0.f);  // sum over q of the A_ij double-layer factor, times cp per p
 #pragma unroll
                 for (int j = 0; j < NP; ++j) {
@@ -388,7 +480,7 @@ __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm,
                         const float2 den = fma2(r2, rinv, rcf2);
                         const float2 th = mul2(sdot, f2(rcp_approx(den.x), rcp_approx(den.y)));
                         float2 sn, cs;
-                        sincos2<PHC>(th, &sn, &cs);
+                        sincos2_sym<PHC>(th, &sn, &cs);
                         if (ST::slp_part) {
                             s0r = fma2(f, cs, s0r);
                             s0i = fma2(f, sn, s0i);
@@ -396,7 +488,7 @@ __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm,
                         if (ST::dlp_part) {
                             const float2 fr = mul2(f, rinv);
                             const float2 h1 = fma2(rinv, cs, sn);
-                            const float2 h2 = fma2(mul2(rinv, b2(-1.f)), sn, cs);
+                            const float2 h2 = fma2(f2(-rinv.x, -rinv.y), sn, cs);
                             const float2 gt = mul2(fr, ynt[j]);
                             pur = fma2(fr, h1, pur);
                             pui = fma2(fr, h2, pui);
@@ -409,46 +501,41 @@ __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm,
                     ur = fma2(cp2, pur, ur);
                     if (ST::helm) ui = fma2(cp2, pui, ui);
                 }
-                // flush where the test-point weight changes:
-                // entry += w_p [kappa eta S0 + kappa^2 (-h1 sum + i h2 sum)]
-                if (p == NQ6 - 1 || rule.w[p + 1] != rule.w[p]) {
-                    const double wp = rule.w[p];
-                    double sr = 0.0, sim = 0.0;
-                    if (ST::slp_part) {
-                        const double xr = (double)(s0r.x + s0r.y), xi = (double)(s0i.x + s0i.y);
-                        sr = fma(ek_r, xr, -ek_i * xi);
-                        sim = fma(ek_r, xi, ek_i * xr);
-                        s0r = s0i = b2(0.f);
-                    }
-                    double dr = 0.0, di = 0.0, er = 0.0, ei = 0.0;
-                    if (ST::dlp_part) {
-                        dr = -k2d * (double)(ur.x + ur.y);
-                        er = -k2d * (double)(vr.x + vr.y);
-                        if (ST::helm) {
-                            di = k2d * (double)(ui.x + ui.y);
-                            ei = k2d * (double)(vi.x + vi.y);
-                        }
-                        ur = ui = vr = vi = b2(0.f);
-                    }
-                    if (ST::swap) {
-                        a_re = fma(wp, er, a_re);
-                        a_im = fma(wp, ei, a_im);
-                        b_re = fma(wp, dr, b_re);
-                        b_im = fma(wp, di, b_im);
-                    } else {
-                        a_re = fma(wp, sr + dr, a_re);
-                        a_im = fma(wp, sim + di, a_im);
-                        b_re = fma(wp, sr + er, b_re);
-                        b_im = fma(wp, sim + ei, b_im);
-                    }
+            }
+            // entry = w_b [kappa eta S0 + kappa^2 (-h1 sum + i h2 sum)], rotated by exp(i r_c') and scaled
+            double sr = 0.0, sim = 0.0;
+            if (ST::slp_part) {
+                const double xr = (double)(s0r.x + s0r.y), xi = (double)(s0i.x + s0i.y);
+                sr = fma(ek_r, xr, -ek_i * xi);
+                sim = fma(ek_r, xi, ek_i * xr);
+            }
+            double dr = 0.0, di = 0.0, er = 0.0, ei = 0.0;
+            if (ST::dlp_part) {
+                dr = -k2d * (double)(ur.x + ur.y);
+                er = -k2d * (double)(vr.x + vr.y);
+                if (ST::helm) {
+                    di = k2d * (double)(ui.x + ui.y);
+                    ei = k2d * (double)(vi.x + vi.y);
                 }
             }
-            const double scale = BC_INV_4PI * sb.ie[tt] * gs.ie;
-            double tr = a_re * ph_c - a_im * ph_s;
-            a_im = (a_re * ph_s + a_im * ph_c) * scale;
+            if (ST::swap) {
+                a_re = er;
+                a_im = ei;
+                b_re = dr;
+                b_im = di;
+            } else {
+                a_re = sr + dr;
+                a_im = sim + di;
+                b_re = sr + er;
+                b_im = sim + ei;
+            }
+            const double scale = BC_INV_4PI * sb.ie[tt] * gs.ie * wb;
+            const double pc = (double)ph_c, ps = (double)ph_s;
+            double tr = a_re * pc - a_im * ps;
+            a_im = (a_re * ps + a_im * pc) * scale;
             a_re = tr * scale;
-            tr = b_re * ph_c - b_im * ph_s;
-            b_im = (b_re * ph_s + b_im * ph_c) * scale;
+            tr = b_re * pc - b_im * ps;
+            b_im = (b_re * ps + b_im * pc) * scale;
             b_re = tr * scale;
         }
         store_entry(prm, row, si, adj, a_re, a_im);

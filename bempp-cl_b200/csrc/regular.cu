@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_MSYM_MIN_BLOCKS) regular_dp0_m
                                                                                       int tile_rows) {
     const int64_t t0 = row0 + (int64_t)blockIdx.y * tile_rows;
     if (t0 >= ((int64_t)blockIdx.x + 1) * DP0_THREADS) return;
-    __shared__ TestBlock32p sb;
+    __shared__ TestBlock32q sb;
     regular_dp0_mixed_sym_tile<K, PHC>(prm, rule, blockIdx.x, t0, (int)min((int64_t)tile_rows, row1 - t0), sb);
 }
 
@@ -519,6 +519,8 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
     for (int i = 0; i < 4; ++i) prm.p[i] = a->params[i];
     prm.result = a->result;
     prm.ld = a->ld;
+    // R_test + R_trial bounds the centroid distance of two elements that share a vertex
+    prm.near_r = a->phase_radius > 0.0 ? a->phase_radius : 0.0;
     if (prm.ntest == 0 || prm.ntrial == 0) return BEMPPCUDA_OK;
 
     QuadRule rule;
