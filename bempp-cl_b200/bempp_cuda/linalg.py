@@ -6,7 +6,9 @@ against the projections onto the dual space and returns a grid function in
 the domain (plus the info code, and optionally residuals / iteration count).
 The reference hands the weak form to scipy's GMRES with ``ndarray.dot``
 matvecs on the host; here the matrix stays in HBM and every matvec is a
-device GEMV (matmat for several right-hand sides, cuBLAS through torch).
+device GEMV (the library's own kernel, bemppcuda_gemv; the batched product for
+several right-hand sides); the small orthogonalisation products against the
+Krylov basis go through torch (cuBLAS).
 
 ``gmres_tensor`` is restarted GMRES on torch tensors: Arnoldi with classical
 Gram-Schmidt and one re-orthogonalisation (two GEMVs against the basis per
@@ -350,8 +352,10 @@ def solve_refined(matrix, b, tol=1e-8, inner_tol=1e-4, restart=100, maxiter=2000
             raise ValueError("a residual operator is supported for A x = b only")
         hi, lo = adjoint_matvec(matrix), adjoint_matvec(low)
     else:
-        hi = residual if residual is not None else (lambda v: _torch.mv(matrix, v))
-        lo = lambda v: _torch.mv(low, v)  # noqa: E731
+        from .matmat import matvec_of
+
+        hi = residual if residual is not None else matvec_of(matrix)
+        lo = matvec_of(low)
     x, info = refine_gmres(hi, lo, b, tol=tol, inner_tol=inner_tol, restart=restart, maxiter=maxiter,
                            max_refinements=max_refinements, inner_dtype=inner_dtype, check_every=check_every)
     del low
@@ -370,7 +374,9 @@ def gmres(A, b, tol=1e-5, restart=None, maxiter=None, use_strong_form=False, ret
     dtype = mat.tensor.dtype if mat.tensor.is_complex() or not _np.iscomplexobj(rhs) else _torch.complex128
     M = mat.tensor.to(dtype)
     bt = _torch.as_tensor(_np.asarray(rhs)).to(device=M.device, dtype=dtype)
-    x, info, residuals, its = gmres_tensor(lambda v: _torch.mv(M, v), bt, tol=tol, restart=restart,
+    from .matmat import matvec_of
+
+    x, info, residuals, its = gmres_tensor(matvec_of(M), bt, tol=tol, restart=restart,
                                            maxiter=maxiter)
     sol = GridFunction(A.domain, coefficients=x.cpu().numpy())
     out = [sol, info]

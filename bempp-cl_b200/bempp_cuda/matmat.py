@@ -10,7 +10,12 @@ a list of them (the batched assembly's outputs, each with its own right-hand
 sides) costs one launch instead of one library GEMM per operator.
 
 The problem table is uploaded once by the constructor; ``launch()`` queues
-device work only and can be captured in a CUDA graph.
+device work only and can be captured in a CUDA graph.  Two to eight
+right-hand sides run on the FP64 tensor cores.
+
+``gemv(a, x)`` is the one-right-hand-side product y = A x of the solves
+(``bemppcuda_gemv``): complex128 or complex64 row-major matrices, streamed
+from HBM by the library's own kernel.
 """
 
 import ctypes as _ct
@@ -107,3 +112,31 @@ def matmat(mats, xs, ys=None):
               for a, x in zip(mats, xs)]
     BatchedProduct(mats, xs, ys).launch()
     return ys
+
+
+def gemv(a, x, out=None, stream=None):
+    """y = a @ x for a complex128 / complex64 device matrix with unit column stride and a vector of
+    the same dtype (bemppcuda_gemv); ``out`` (rows,) receives the result when given."""
+    require_cuda()
+    if a.dim() != 2 or a.dtype not in (_torch.complex128, _torch.complex64):
+        raise ValueError("gemv: a must be a 2-D complex128 or complex64 tensor (got %s)" % (a.dtype,))
+    if a.stride(1) != 1 or (a.shape[0] > 1 and a.stride(0) < a.shape[1]):
+        raise ValueError("gemv: a must have unit column stride (row-major rows)")
+    if x.dim() != 1 or x.shape[0] != a.shape[1]:
+        raise ValueError("gemv: x must be a vector of length %d" % a.shape[1])
+    x = x.to(a.dtype).contiguous()
+    if out is None:
+        out = _torch.empty(a.shape[0], dtype=a.dtype, device=a.device)
+    elif out.dtype != a.dtype or not out.is_contiguous() or out.shape != (a.shape[0],):
+        raise ValueError("gemv: out must be a contiguous (rows,) tensor of the matrix dtype")
+    lda = a.stride(0) if a.shape[0] > 1 else a.shape[1]
+    _lib.check(_lib.load().bemppcuda_gemv(ptr(a), a.shape[0], a.shape[1], lda, ptr(x), ptr(out),
+                                          1 if a.dtype == _torch.complex64 else 0, stream or current_stream()))
+    return out
+
+
+def matvec_of(a):
+    """v -> a @ v on the device: the library GEMV for complex matrices, torch.mv for real ones."""
+    if a.is_complex() and a.stride(1) == 1:
+        return lambda v: gemv(a, v)
+    return lambda v: _torch.mv(a, v)

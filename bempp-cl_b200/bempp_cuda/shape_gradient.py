@@ -32,6 +32,7 @@ import torch as _torch
 from . import _lib
 from .assembly import regular_into, regular_rule, singular_into_dense
 from .device import current_stream, device_grid, device_singular_rule, device_space, ptr, require_cuda
+from .matmat import matvec_of
 from .operators import OperatorDescriptor, Parameters
 from .space import function_space
 
@@ -233,14 +234,14 @@ class FarFieldObjective(object):
         elif solver == "lu32":
             matrix = a
             lu, pivots = _torch.linalg.lu_factor(a.to(_torch.complex64))
-            phi, its = self._refine(lu, pivots, lambda v: _torch.mv(matrix, v), b)
+            phi, its = self._refine(lu, pivots, matvec_of(matrix), b)
         elif solver == "gmres32":
             matrix = a
             low = a.to(_torch.complex64)
-            phi, its = self._gmres32(lambda v: _torch.mv(matrix, v), lambda v: _torch.mv(low, v), b)
+            phi, its = self._gmres32(matvec_of(matrix), matvec_of(low), b)
         else:
             matrix = a
-            phi, its = self._gmres(lambda v: _torch.mv(matrix, v), b)
+            phi, its = self._gmres(matvec_of(matrix), b)
         farfield = self.farfield_matrix(geometry, k)
         u = farfield @ phi
         value = (u.real ** 2 + u.imag ** 2).sum()

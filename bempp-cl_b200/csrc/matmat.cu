@@ -2,23 +2,24 @@
 // operators: the device counterpart of DenseDiscreteBoundaryOperator._matmat
 // (api/assembly/discrete_boundary_operator.py:192-198, ndarray.dot on the
 // host) for a list of operators with up to 8 right-hand sides each, in one
-// launch.
+// launch; and the one-right-hand-side product of the solves (bemppcuda_gemv).
 //
 // With 8 right-hand sides each 16-byte matrix entry meets 8 complex FMAs
 // (64 flops), so the product sits at the FP64 ridge of a B200 (4 flop / byte
-// at HBM bandwidth is ~26 TFLOP/s, the FP64 pipe ~36): the kernel must keep
-// enough of A in flight to stream it at HBM rate while the FP64 pipe and
-// shared memory stay under their limits.  Layout: a CTA of 8 warps owns 16
-// rows of one problem (2 rows per warp); columns go in tiles of 64.  A
-// three-stage pipeline of asynchronous 16-byte copies (cp.async, L2 only)
-// brings each tile of A (16 x 64, 16 KB) and the matching rows of X
-// (transposed to xs[c][j], one padding element per row so the transposing
-// stores spread over the banks) into shared memory two tiles ahead, about
-// 32 KB in flight per CTA.  Each lane reads A(r, j) for its 2 rows and
-// j = lane + 32 m, and every X(j, c) once for both rows; one barrier per
-// tile.  Partial sums are reduced across the warp with shuffles at the end.
-// A CTA's problem is found by binary search over the problems' first row
-// blocks.
+// at HBM bandwidth is ~26 TFLOP/s, the FP64 pipe ~36).  2 to 8 right-hand
+// sides run on the FP64 tensor cores (matmat_c128_tc below), which take the
+// multiply-adds off the FP64 pipe and out of the issue slots, so the kernel
+// is left to stream A.  One right-hand side of the batched call keeps the
+// FP64-pipe kernel matmat_c128: a CTA of 8 warps owns 16 rows of one problem
+// (2 rows per warp); columns go in tiles of 64.  A three-stage pipeline of
+// asynchronous 16-byte copies (cp.async, L2 only) brings each tile of A
+// (16 x 64, 16 KB) and the matching rows of X (transposed to xs[c][j], one
+// padding element per row so the transposing stores spread over the banks)
+// into shared memory two tiles ahead, about 32 KB in flight per CTA.  Each
+// lane reads A(r, j) for its 2 rows and j = lane + 32 m, and every X(j, c)
+// once for both rows; one barrier per tile.  Partial sums are reduced across
+// the warp with shuffles at the end.  In both kernels a CTA's problem is
+// found by binary search over the problems' first row blocks.
 #include "common.cuh"
 
 namespace bc {
@@ -190,9 +191,219 @@ __global__ void __launch_bounds__(MM_THREADS, 2) matmat_c128(const MatmatDev *__
             if (lane == r * NR + c && rw + r < P.rows) P.y[(rw + r) * P.ldy + c] = make_double2(sr[r][c], si[r][c]);
 }
 
+// ---------------------------------------------------------------------------------------------
+// FP64 tensor cores (mma.sync m8n8k4 .f64; Blackwell's tcgen05 has no FP64 form).  The complex
+// product is one real GEMM: a row of A read as its interleaved (re, im) doubles is a real row of
+// length 2K, and X becomes the real 2K x 2N matrix B with, for complex column j of A and column c
+// of X,
+//   B[2j][2c] = Re X[j][c],   B[2j][2c+1] = Im X[j][c],
+//   B[2j+1][2c] = -Im X[j][c], B[2j+1][2c+1] = Re X[j][c],
+// so that (A B)[r][2c] = Re Y[r][c] and (A B)[r][2c+1] = Im Y[r][c].  A warp owns MT tiles of 8
+// rows; per group of 4 complex columns lane (g, t) = (lane / 4, lane % 4) loads A[row g][j0 + t]
+// as one 16-byte (re, im) pair straight from global memory (8 rows x 64 contiguous bytes per warp
+// load, streamed past L1) and uses re as its A fragment of one k4 step and im as that of a second,
+// the k index of both steps being t (the sum over k may be taken in any order, B follows it).  The
+// B fragments (B[k = t][n = g]) come from X[j0 + t][c] with c = g / 2 (output columns 0-7 =
+// complex columns 0-3) and 4 + g / 2 (columns 4-7, when NR > 4), cached in L1 since every warp of
+// the problem reads the same X.  The accumulator fragment of lane (g, t), C[g][2t], C[g][2t + 1],
+// is the complex entry Y[row g][4 n + t]: stored directly.  Columns beyond NR read zero.
+constexpr int TC_WARPS = 4;
+
+__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
+
+// A is read once: keep it out of L1 (X and the other operands use it)
+__device__ __forceinline__ double2 ld_stream(const double2 *p) {
+    double2 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v2.f64 {%0,%1}, [%2];\n" : "=d"(v.x), "=d"(v.y) : "l"(p));
+    return v;
+}
+
+__device__ __forceinline__ float2 ld_stream(const float2 *p) {
+    float2 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v2.f32 {%0,%1}, [%2];\n" : "=f"(v.x), "=f"(v.y) : "l"(p));
+    return v;
+}
+
+template <int NR, int MT>
+struct TcLayout {
+    static constexpr int NT = NR > 4 ? 2 : 1;  // n8 tiles of the real output (2 NR columns)
+    static constexpr int ROWS = TC_WARPS * 8 * MT;
+};
+
+// One group of 4 complex columns j0 .. j0 + 3: lane (g, t) takes column j0 + t (one 16-byte load
+// per row and m-tile; a warp reads 64 contiguous bytes of each of its rows); two k4 steps.  (Two
+// adjacent columns per lane, 128 bytes per row and load, measured 10 % slower.)
+template <int NR, int MT, bool MASK>
+__device__ __forceinline__ void tc_group(const MatmatDev &P, const double2 *const (&arow)[MT], int64_t j0, int g,
+                                         int t, double (&acc)[MT][TcLayout<NR, MT>::NT][2]) {
+    constexpr int NT = TcLayout<NR, MT>::NT;
+    constexpr int H = 1;
+    const int c0 = g >> 1;
+    const bool odd = g & 1;
+    double2 av[H][MT];
+    double bre[H][NT], bim[H][NT];
+#pragma unroll
+    for (int h = 0; h < H; ++h) {
+        const int64_t j = j0 + H * t + h;
+        const bool jok = !MASK || j < P.cols;
+#pragma unroll
+        for (int n = 0; n < NT; ++n) {
+            const int c = 4 * n + c0;
+            const double2 xv = (jok && c < NR) ? __ldg(P.x + j * P.ldx + c) : make_double2(0.0, 0.0);
+            bre[h][n] = odd ? xv.y : xv.x;   // B[2j][g]
+            bim[h][n] = odd ? xv.x : -xv.y;  // B[2j + 1][g]
+        }
+#pragma unroll
+        for (int m = 0; m < MT; ++m) av[h][m] = jok ? ld_stream(arow[m] + j) : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int h = 0; h < H; ++h)
+#pragma unroll
+        for (int m = 0; m < MT; ++m)
+#pragma unroll
+            for (int n = 0; n < NT; ++n) {
+                dmma(acc[m][n], av[h][m].x, bre[h][n]);
+                dmma(acc[m][n], av[h][m].y, bim[h][n]);
+            }
+}
+
+template <int NR, int MT>
+__global__ void __launch_bounds__(TC_WARPS * 32) matmat_c128_tc(const MatmatDev *__restrict__ probs, int nproblems) {
+    using L = TcLayout<NR, MT>;
+    constexpr int GW = 4;  // columns per group
+    const int64_t b = blockIdx.x;
+    int lo = 0, hi = nproblems - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (probs[mid].block_begin <= b)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const MatmatDev P = probs[lo];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int64_t r0 = (b - P.block_begin) * L::ROWS + (int64_t)warp * 8 * MT;
+    if (r0 >= P.rows) return;  // whole warp: the mma instructions below need all 32 lanes
+    const double2 *arow[MT];
+#pragma unroll
+    for (int m = 0; m < MT; ++m) arow[m] = P.a + min(r0 + 8 * m + g, P.rows - 1) * P.lda;
+    double acc[MT][L::NT][2];
+#pragma unroll
+    for (int m = 0; m < MT; ++m)
+#pragma unroll
+        for (int n = 0; n < L::NT; ++n) acc[m][n][0] = acc[m][n][1] = 0.0;
+    const int64_t full = P.cols / (4 * GW) * (4 * GW);  // four groups per step
+    for (int64_t j0 = 0; j0 < full; j0 += 4 * GW) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) tc_group<NR, MT, false>(P, arow, j0 + u * GW, g, t, acc);
+    }
+    for (int64_t j0 = full; j0 < P.cols; j0 += GW) tc_group<NR, MT, true>(P, arow, j0, g, t, acc);
+#pragma unroll
+    for (int m = 0; m < MT; ++m) {
+        const int64_t r = r0 + 8 * m + g;
+#pragma unroll
+        for (int n = 0; n < L::NT; ++n) {
+            const int c = 4 * n + t;
+            if (r < P.rows && c < NR) P.y[r * P.ldy + c] = make_double2(acc[m][n][0], acc[m][n][1]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// One right-hand side (the GMRES matvec): y = A x for a row-major complex matrix, HBM-bound.  The
+// matrix is read like a copy reads its source: CTA b takes segment b % S of row b / S (S segments
+// of GV_SEG entries per row), so consecutive CTAs stream consecutive memory; each thread loads
+// GV_PER entries GV_THREADS apart (coalesced, all in flight at once, streamed past L1), multiplies
+// by x (through L1), and the CTA's sum goes to y[row] with one atomic add per component, y having
+// been zeroed.  Sums in the matrix's precision; the order of the atomic adds is not fixed.
+template <typename C>
+struct GemvTraits;
+template <>
+struct GemvTraits<double2> {
+    using R = double;
+};
+template <>
+struct GemvTraits<float2> {
+    using R = float;
+};
+
+constexpr int GV_THREADS = 256;
+constexpr int GV_PER = 8;  // 32 KB segments for complex128 (4 and 16 measured slower)
+constexpr int64_t GV_SEG = (int64_t)GV_THREADS * GV_PER;
+
+template <typename C>
+__global__ void __launch_bounds__(GV_THREADS) gemv_segments(const C *__restrict__ a, int64_t cols, int64_t lda,
+                                                             int64_t segs, int64_t block0, const C *__restrict__ x,
+                                                             C *y) {
+    using R = typename GemvTraits<C>::R;
+    const int64_t blk = block0 + blockIdx.x;
+    const int64_t row = blk / segs, j0 = (blk - row * segs) * GV_SEG + threadIdx.x;
+    const C *ar = a + row * lda;
+    C av[GV_PER], xv[GV_PER];
+#pragma unroll
+    for (int u = 0; u < GV_PER; ++u) {
+        const int64_t j = j0 + (int64_t)u * GV_THREADS;
+        if (j < cols) {
+            av[u] = ld_stream(ar + j);
+            xv[u] = __ldg(x + j);
+        } else {
+            av[u].x = av[u].y = xv[u].x = xv[u].y = 0;
+        }
+    }
+    R sr = 0, si = 0;
+#pragma unroll
+    for (int u = 0; u < GV_PER; ++u) {
+        sr = fma(av[u].x, xv[u].x, fma(-av[u].y, xv[u].y, sr));
+        si = fma(av[u].x, xv[u].y, fma(av[u].y, xv[u].x, si));
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        sr += __shfl_xor_sync(0xffffffffu, sr, off);
+        si += __shfl_xor_sync(0xffffffffu, si, off);
+    }
+    __shared__ R part[2][GV_THREADS / 32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        part[0][warp] = sr;
+        part[1][warp] = si;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        R tr = 0, ti = 0;
+#pragma unroll
+        for (int w = 0; w < GV_THREADS / 32; ++w) {
+            tr += part[0][w];
+            ti += part[1][w];
+        }
+        atomicAdd(&y[row].x, tr);
+        atomicAdd(&y[row].y, ti);
+    }
+}
+
 }  // namespace bc
 
 using namespace bc;
+
+// m8 tiles per warp: 4 (32 rows per warp, 128 per CTA) measured fastest against 1 and 2 on
+// 25 x 8192^2 (2 wins on 64 x 2048^2 by 10 %)
+#ifndef BC_MATMAT_TC_MT
+#define BC_MATMAT_TC_MT 4
+#endif
+
+// rows per CTA of the kernel that serves nrhs right-hand sides: tensor cores from 2 up
+static int64_t matmat_rows_per_block(int nrhs) {
+    return nrhs >= 2 ? (int64_t)TC_WARPS * 8 * BC_MATMAT_TC_MT : (int64_t)MM_ROWS;
+}
+
+template <int NR>
+static cudaError_t launch_matmat_tc(const MatmatDev *probs, int nproblems, int64_t blocks, cudaStream_t st) {
+    matmat_c128_tc<NR, BC_MATMAT_TC_MT><<<dim3((unsigned)blocks), TC_WARPS * 32, 0, st>>>(probs, nproblems);
+    return cudaGetLastError();
+}
 
 template <int NR>
 static cudaError_t launch_matmat(const MatmatDev *probs, int nproblems, int64_t blocks, cudaStream_t st) {
@@ -262,7 +473,8 @@ extern "C" int bemppcuda_matmat_prepare(bemppcuda_matmat_args *a, void *stream) 
         d.ldx = p.ldx;
         d.ldy = p.ldy;
         d.block_begin = blocks;
-        blocks += (p.rows + MM_ROWS - 1) / MM_ROWS;
+        const int64_t rpb = matmat_rows_per_block(a->nrhs);
+        blocks += (p.rows + rpb - 1) / rpb;
     }
     cudaError_t err = blocks > 0x7fffffffLL ? cudaErrorInvalidValue
                                             : cudaMemcpyAsync(a->workspace, host, sizeof(MatmatDev) * a->nproblems,
@@ -284,19 +496,56 @@ extern "C" int bemppcuda_matmat_launch(const bemppcuda_matmat_args *a, void *str
     }
     const MatmatDev *probs = static_cast<const MatmatDev *>(a->workspace);
     cudaError_t err = cudaSuccess;
+    const cudaStream_t st = (cudaStream_t)stream;
     switch (a->nrhs) {
-    case 1: err = launch_matmat<1>(probs, a->nproblems, a->blocks, (cudaStream_t)stream); break;
-    case 2: err = launch_matmat<2>(probs, a->nproblems, a->blocks, (cudaStream_t)stream); break;
-    case 3: err = launch_matmat<3>(probs, a->nproblems, a->blocks, (cudaStream_t)stream); break;
-    case 4: err = launch_matmat<4>(probs, a->nproblems, a->blocks, (cudaStream_t)stream); break;
-    case 5: err = launch_matmat<5>(probs, a->nproblems, a->blocks, (cudaStream_t)stream); break;
-    case 6: err = launch_matmat<6>(probs, a->nproblems, a->blocks, (cudaStream_t)stream); break;
-    case 7: err = launch_matmat<7>(probs, a->nproblems, a->blocks, (cudaStream_t)stream); break;
-    default: err = launch_matmat<8>(probs, a->nproblems, a->blocks, (cudaStream_t)stream); break;
+    case 1: err = launch_matmat<1>(probs, a->nproblems, a->blocks, st); break;
+    case 2: err = launch_matmat_tc<2>(probs, a->nproblems, a->blocks, st); break;
+    case 3: err = launch_matmat_tc<3>(probs, a->nproblems, a->blocks, st); break;
+    case 4: err = launch_matmat_tc<4>(probs, a->nproblems, a->blocks, st); break;
+    case 5: err = launch_matmat_tc<5>(probs, a->nproblems, a->blocks, st); break;
+    case 6: err = launch_matmat_tc<6>(probs, a->nproblems, a->blocks, st); break;
+    case 7: err = launch_matmat_tc<7>(probs, a->nproblems, a->blocks, st); break;
+    default: err = launch_matmat_tc<8>(probs, a->nproblems, a->blocks, st); break;
     }
     if (err != cudaSuccess) {
         bc_set_error("matmat_launch: %s", cudaGetErrorString(err));
         return BEMPPCUDA_ERR_CUDA;
     }
     return BEMPPCUDA_OK;
+}
+
+extern "C" int bemppcuda_gemv(const void *a, int64_t rows, int64_t cols, int64_t lda, const void *x, void *y,
+                              int32_t complex64, void *stream) {
+    if (rows < 0 || cols < 0 || lda < cols || ((rows > 0 && cols > 0) && (!a || !x)) || (rows > 0 && !y)) {
+        bc_set_error("gemv: missing pointers or inconsistent sizes (rows %lld, cols %lld, lda %lld)",
+                     (long long)rows, (long long)cols, (long long)lda);
+        return BEMPPCUDA_ERR_INVALID;
+    }
+    const size_t elem = complex64 ? 8 : 16;
+    if ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) % elem) {
+        bc_set_error("gemv: arrays must be aligned to their element size");
+        return BEMPPCUDA_ERR_INVALID;
+    }
+    if (rows == 0) return BEMPPCUDA_OK;
+    const cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t err = cudaMemsetAsync(y, 0, (size_t)rows * elem, st);
+    if (err != cudaSuccess) {
+        bc_set_error("gemv: %s", cudaGetErrorString(err));
+        return BEMPPCUDA_ERR_CUDA;
+    }
+    if (cols == 0) return BEMPPCUDA_OK;
+    const int64_t segs = (cols + GV_SEG - 1) / GV_SEG;
+    const int64_t total = rows * segs;
+    constexpr int64_t kMaxGrid = 0x7fffffffLL;
+    for (int64_t b0 = 0; b0 < total; b0 += kMaxGrid) {
+        const unsigned n = (unsigned)min(total - b0, kMaxGrid);
+        if (complex64)
+            gemv_segments<float2><<<n, GV_THREADS, 0, st>>>(static_cast<const float2 *>(a), cols, lda, segs, b0,
+                                                            static_cast<const float2 *>(x), static_cast<float2 *>(y));
+        else
+            gemv_segments<double2><<<n, GV_THREADS, 0, st>>>(static_cast<const double2 *>(a), cols, lda, segs, b0,
+                                                             static_cast<const double2 *>(x),
+                                                             static_cast<double2 *>(y));
+    }
+    return bc_check_launch("gemv");
 }

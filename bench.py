@@ -421,27 +421,35 @@ def hbm_peak():
 
 
 def matvec_measure(torch, a64):
-    """GEMV on the resident matrix (the GMRES matvec): HBM-bound, one read of the matrix per product."""
+    """GEMV on the resident matrix (the GMRES matvec): HBM-bound, one read of the matrix per product.
+    The library's kernel (bemppcuda_gemv, used by the solves) beside cuBLAS through torch.mv."""
+    from bempp_cuda.matmat import gemv
+
     peak, source = hbm_peak()
     n = a64.shape[0]
     out = {"peak_gbs": peak, "peak_source": source}
     a32 = a64.to(torch.complex64)
     for name, mat in (("complex128", a64), ("complex64", a32)):
         x = torch.ones(n, dtype=mat.dtype, device="cuda")
-        for _ in range(3):
-            torch.mv(mat, x)
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(10):
-            torch.mv(mat, x)
-        e1.record()
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / 10
         nbytes = mat.numel() * mat.element_size()
-        gbs = nbytes / (ms * 1e-3) / 1e9
-        out[name] = {"ms": ms, "bytes": nbytes, "gbs": gbs, "frac": gbs / peak}
+        entry = {"bytes": nbytes}
+        for impl, fn in (("library", lambda: gemv(mat, x)), ("cublas", lambda: torch.mv(mat, x))):
+            for _ in range(3):
+                fn()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(10):
+                fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / 10
+            gbs = nbytes / (ms * 1e-3) / 1e9
+            entry[impl] = {"ms": ms, "gbs": gbs, "frac": gbs / peak}
+        ref = torch.mv(mat, x)
+        entry["library_rel_diff_vs_cublas"] = float((torch.linalg.norm(gemv(mat, x) - ref) / torch.linalg.norm(ref)).item())
+        out[name] = entry
     del a32
     torch.cuda.empty_cache()
     return out
@@ -454,6 +462,7 @@ def solve_measure(args, torch, grid, domain, a64, amx, desc, params):
     1e-11, where the two solutions must agree to 1e-8."""
     from bempp_cuda.grid_function import GridFunction
     from bempp_cuda.linalg import gmres_tensor, solve_refined
+    from bempp_cuda.matmat import matvec_of
     from bempp_cuda.operators import fp64_matvec_of
 
     k = args.k
@@ -464,7 +473,8 @@ def solve_measure(args, torch, grid, domain, a64, amx, desc, params):
     b = torch.as_tensor(GridFunction(domain, fun=minus_incident).projections(domain), device="cuda")
     fp64_apply = fp64_matvec_of(desc, 1.0, domain, params, amx)
     # warm-up (first-call costs of the solver's kernels and host loop), so both solves are timed warm
-    gmres_tensor(lambda v: torch.mv(a64, v), b, tol=1e-8, restart=200, maxiter=5)
+    gemv64 = matvec_of(a64)
+    gmres_tensor(gemv64, b, tol=1e-8, restart=200, maxiter=5)
     fp64_apply(b)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -481,7 +491,7 @@ def solve_measure(args, torch, grid, domain, a64, amx, desc, params):
     for tol in (1e-8, 1e-11):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        x64, info, res, its = gmres_tensor(lambda v: torch.mv(a64, v), b, tol=tol, restart=200, maxiter=2000)
+        x64, info, res, its = gmres_tensor(gemv64, b, tol=tol, restart=200, maxiter=2000)
         torch.cuda.synchronize()
         t64 = time.perf_counter() - t0
         xmx, rinfo = solve_refined(amx, b, tol=tol, inner_tol=1e-4, restart=200, residual=fp64_apply)
@@ -582,7 +592,7 @@ def batch_measure(args, torch, world, rank, dist, count=64, levels=(3, 4, 5)):
             nbytes = sum(16 * (o.shape[0] * o.shape[1] + (o.shape[0] + o.shape[1]) * x.shape[1])
                          for o, x in zip(ba.outputs, rhs))
             peak, source = hbm_peak()
-            entry["products"] = {"kernel": "matmat_c128<8> (one launch, all problems)", "kernel_ms": prod_ms,
+            entry["products"] = {"kernel": "matmat_c128_tc<8> (FP64 tensor cores, one launch, all problems)", "kernel_ms": prod_ms,
                                  "torch_matmul_ms": torch_ms, "bytes": nbytes,
                                  "gbs": nbytes / (prod_ms * 1e-3) / 1e9,
                                  "frac": nbytes / (prod_ms * 1e-3) / 1e9 / peak, "peak_gbs": peak,
@@ -635,6 +645,7 @@ def shape_measure(args, torch):
     Central differences (h = 1e-6) on 20 seeded coordinates and on k check
     the gradient at this size.
     """
+    from bempp_cuda.matmat import matvec_of
     from bempp_cuda.shape_gradient import FarFieldObjective
     from bempp_cuda.shapes import perturbed_sphere
 
@@ -660,17 +671,17 @@ def shape_measure(args, torch):
         b = obj.rhs(geo, k)
         if solver == "lu32":
             lu, piv = torch.linalg.lu_factor(a.to(torch.complex64))
-            phi, its = obj._refine(lu, piv, lambda v: torch.mv(a, v), b)
+            phi, its = obj._refine(lu, piv, matvec_of(a), b)
             low = None
             iters["forward_refinements"] = its
         elif solver == "gmres32":
             lu = piv = None
             low = a.to(torch.complex64)
-            phi, its = obj._gmres32(lambda v: torch.mv(a, v), lambda v: torch.mv(low, v), b)
+            phi, its = obj._gmres32(matvec_of(a), matvec_of(low), b)
             iters["forward_inner_iterations"] = its
         else:  # gmres
             lu = piv = low = None
-            phi, its = obj._gmres(lambda v: torch.mv(a, v), b)
+            phi, its = obj._gmres(matvec_of(a), b)
             iters["forward_iterations"] = its
         mark(3)
         ff = obj.farfield_matrix(geo, k)

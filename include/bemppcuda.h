@@ -367,8 +367,19 @@ int bemppcuda_matmat_prepare(bemppcuda_matmat_args *args, void *stream);
 /* One kernel launch over every problem's rows (device work only, so it can be
    captured in a CUDA graph once bemppcuda_matmat_prepare has run).  FP64
    sums; the order differs from a BLAS product's, so results agree with it to
-   rounding, not bit for bit. */
+   rounding, not bit for bit.  2 to 8 right-hand sides run on the FP64 tensor
+   cores (mma.sync m8n8k4 .f64), 1 on the FP64 pipe. */
 int bemppcuda_matmat_launch(const bemppcuda_matmat_args *args, void *stream);
+
+/* y = A x, one right-hand side: the matvec of the solve (DenseDiscreteBoundaryOperator._matvec,
+   api/assembly/discrete_boundary_operator.py:192-198, ndarray.dot on the host; scipy's GMRES calls
+   it once per iteration, api/linalg/iterative_solvers.py:47-93).  A row-major (rows, cols) with row
+   stride lda >= cols, x (cols,), y (rows,), all device arrays of complex128 (complex64 = 0) or
+   complex64 (complex64 = 1), aligned to their element size.  HBM-bound stream of A; y is zeroed
+   and receives the sums of row segments with atomic adds, in the matrix's precision: equal to a
+   BLAS GEMV to rounding, not bit for bit, and not bit-reproducible from call to call. */
+int bemppcuda_gemv(const void *a, int64_t rows, int64_t cols, int64_t lda, const void *x, void *y, int32_t complex64,
+                   void *stream);
 
 /* Measurement utility, no reference counterpart: launches `blocks` x 256
    threads that each run 32 independent FMAs per iteration in FP64

@@ -113,3 +113,38 @@ def test_library_rejects_bad_tables():
     args.workspace_bytes = ws.numel()
     assert lib.bemppcuda_matmat_prepare(ctypes.byref(args), current_stream()) == _lib.OK
     assert args.blocks == 1
+
+
+@pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
+@pytest.mark.parametrize("shape", [(1, 1), (3, 200), (257, 129), (1000, 4097), (4096, 4096)])
+def test_gemv_matches_mv(dtype, shape):
+    """The solves' one-right-hand-side product (bemppcuda_gemv) = torch.mv to rounding: 1e-14 relative
+    (complex128) / 1e-6 (complex64), ragged sizes around the 4-row / 128-column steps."""
+    from bempp_cuda.matmat import gemv
+
+    rng = np.random.default_rng(shape[0] + shape[1])
+    a = _c128(rng, shape).to(dtype)
+    x = _c128(rng, (shape[1],)).to(dtype)
+    y = gemv(a, x)
+    ref = torch.mv(a.to(torch.complex128), x.to(torch.complex128))
+    assert y.dtype == dtype
+    assert _rel(y.to(torch.complex128), ref) < (1e-14 if dtype == torch.complex128 else 1e-6)
+
+
+def test_gemv_strided_rows_and_operator_dot():
+    """Row stride wider than the row (a view), and DenseDeviceOperator @ vector taking this path."""
+    from bempp_cuda.matmat import gemv
+    from bempp_cuda.operators import DenseDeviceOperator
+
+    rng = np.random.default_rng(9)
+    big = _c128(rng, (400, 900))
+    a = big[7:307, 11:611]
+    x = _c128(rng, (600,))
+    out = torch.empty(300, dtype=torch.complex128, device="cuda")
+    gemv(a, x, out=out)
+    assert _rel(out, a @ x) < 1e-14
+    op = DenseDeviceOperator(big.contiguous())
+    v = _c128(rng, (900,))
+    assert _rel(op @ v, big @ v) < 1e-14
+    with pytest.raises(ValueError):
+        gemv(big.transpose(0, 1), v)
