@@ -231,12 +231,9 @@ __device__ __forceinline__ float2 ld_stream(const float2 *p) {
 template <int NR, int MT>
 struct TcLayout {
     static constexpr int NT = NR > 4 ? 2 : 1;  // n8 tiles of the real output (2 NR columns)
-    static constexpr int ROWS = TC_WARPS * 8 * MT;
+    static constexpr int ROWS = 8 * MT;        // rows per CTA: its warps split the columns
 };
 
-// One group of 4 complex columns j0 .. j0 + 3: lane (g, t) takes column j0 + t (one 16-byte load
-// per row and m-tile; a warp reads 64 contiguous bytes of each of its rows); two k4 steps.  (Two
-// adjacent columns per lane, 128 bytes per row and load, measured 10 % slower.)
 template <int NR, int MT, bool MASK>
 __device__ __forceinline__ void tc_group(const MatmatDev &P, const double2 *const (&arow)[MT], int64_t j0, int g,
                                          int t, double (&acc)[MT][TcLayout<NR, MT>::NT][2]) {
@@ -271,10 +268,17 @@ __device__ __forceinline__ void tc_group(const MatmatDev &P, const double2 *cons
             }
 }
 
+// A CTA owns 8 MT rows of one problem; its TC_WARPS warps split the columns in steps of
+// 16 TC_WARPS (warp w takes columns 16 w .. 16 w + 15 of each step, so a step reads one contiguous
+// 256-byte-per-warp stretch of every row), then add their accumulators in shared memory in a fixed
+// order.  Splitting the columns instead of the rows keeps four times as many CTAs for the same
+// matrix (problems of a few thousand rows still fill the GPU) without atomics.
 template <int NR, int MT>
 __global__ void __launch_bounds__(TC_WARPS * 32) matmat_c128_tc(const MatmatDev *__restrict__ probs, int nproblems) {
     using L = TcLayout<NR, MT>;
-    constexpr int GW = 4;  // columns per group
+    constexpr int GW = 4;                 // columns per group
+    constexpr int STEP = 16 * TC_WARPS;  // columns per step of the CTA
+    __shared__ double red[TC_WARPS - 1][MT][L::NT][2][32];
     const int64_t b = blockIdx.x;
     int lo = 0, hi = nproblems - 1;
     while (lo < hi) {
@@ -286,8 +290,7 @@ __global__ void __launch_bounds__(TC_WARPS * 32) matmat_c128_tc(const MatmatDev 
     }
     const MatmatDev P = probs[lo];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    const int64_t r0 = (b - P.block_begin) * L::ROWS + (int64_t)warp * 8 * MT;
-    if (r0 >= P.rows) return;  // whole warp: the mma instructions below need all 32 lanes
+    const int64_t r0 = (b - P.block_begin) * L::ROWS;  // < P.rows by construction of the blocks
     const double2 *arow[MT];
 #pragma unroll
     for (int m = 0; m < MT; ++m) arow[m] = P.a + min(r0 + 8 * m + g, P.rows - 1) * P.lda;
@@ -296,19 +299,41 @@ __global__ void __launch_bounds__(TC_WARPS * 32) matmat_c128_tc(const MatmatDev 
     for (int m = 0; m < MT; ++m)
 #pragma unroll
         for (int n = 0; n < L::NT; ++n) acc[m][n][0] = acc[m][n][1] = 0.0;
-    const int64_t full = P.cols / (4 * GW) * (4 * GW);  // four groups per step
-    for (int64_t j0 = 0; j0 < full; j0 += 4 * GW) {
+    const int64_t full = P.cols / STEP * STEP;
+    for (int64_t j0 = 16 * warp; j0 < full; j0 += STEP) {
 #pragma unroll
         for (int u = 0; u < 4; ++u) tc_group<NR, MT, false>(P, arow, j0 + u * GW, g, t, acc);
     }
-    for (int64_t j0 = full; j0 < P.cols; j0 += GW) tc_group<NR, MT, true>(P, arow, j0, g, t, acc);
+    for (int64_t j0 = full + 16 * warp; j0 < P.cols; j0 += STEP)
+        for (int u = 0; u < 4 && j0 + u * GW < P.cols; ++u) tc_group<NR, MT, true>(P, arow, j0 + u * GW, g, t, acc);
+    if (warp > 0) {
 #pragma unroll
-    for (int m = 0; m < MT; ++m) {
-        const int64_t r = r0 + 8 * m + g;
+        for (int m = 0; m < MT; ++m)
 #pragma unroll
-        for (int n = 0; n < L::NT; ++n) {
-            const int c = 4 * n + t;
-            if (r < P.rows && c < NR) P.y[r * P.ldy + c] = make_double2(acc[m][n][0], acc[m][n][1]);
+            for (int n = 0; n < L::NT; ++n) {
+                red[warp - 1][m][n][0][lane] = acc[m][n][0];
+                red[warp - 1][m][n][1][lane] = acc[m][n][1];
+            }
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int w = 0; w < TC_WARPS - 1; ++w)
+#pragma unroll
+            for (int m = 0; m < MT; ++m)
+#pragma unroll
+                for (int n = 0; n < L::NT; ++n) {
+                    acc[m][n][0] += red[w][m][n][0][lane];
+                    acc[m][n][1] += red[w][m][n][1][lane];
+                }
+#pragma unroll
+        for (int m = 0; m < MT; ++m) {
+            const int64_t r = r0 + 8 * m + g;
+#pragma unroll
+            for (int n = 0; n < L::NT; ++n) {
+                const int c = 4 * n + t;
+                if (r < P.rows && c < NR) P.y[r * P.ldy + c] = make_double2(acc[m][n][0], acc[m][n][1]);
+            }
         }
     }
 }
@@ -388,15 +413,15 @@ __global__ void __launch_bounds__(GV_THREADS) gemv_segments(const C *__restrict_
 
 using namespace bc;
 
-// m8 tiles per warp: 4 (32 rows per warp, 128 per CTA) measured fastest against 1 and 2 on
-// 25 x 8192^2 (2 wins on 64 x 2048^2 by 10 %)
+// m8 tiles per warp (rows per CTA = 8 x this): 2 measured fastest against 4 on 25 x 8192^2, 64 x
+// 2048^2, 3 x 8192^2 and 1 x 4096^2 with eight right-hand sides
 #ifndef BC_MATMAT_TC_MT
-#define BC_MATMAT_TC_MT 4
+#define BC_MATMAT_TC_MT 2
 #endif
 
 // rows per CTA of the kernel that serves nrhs right-hand sides: tensor cores from 2 up
 static int64_t matmat_rows_per_block(int nrhs) {
-    return nrhs >= 2 ? (int64_t)TC_WARPS * 8 * BC_MATMAT_TC_MT : (int64_t)MM_ROWS;
+    return nrhs >= 2 ? (int64_t)8 * BC_MATMAT_TC_MT : (int64_t)MM_ROWS;
 }
 
 template <int NR>

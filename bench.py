@@ -87,6 +87,8 @@ def parse(argv=None):
     ap.add_argument("--shape-level", type=int, default=5)
     ap.add_argument("--shape-solver", choices=["lu32", "gmres", "gmres32"], default="lu32")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time per baseline sample")
+    ap.add_argument("--profile-case", choices=sorted(PROFILE_CASES), default=None,
+                    help="run one kernel on a few-GB case (for ncu captures; prints its CUDA-event time) and exit")
     return ap.parse_args(argv)
 
 
@@ -1225,8 +1227,89 @@ def cpu_leg(args, line, gpu_rows):
     line.setdefault("parity", {})["benchmark_operator"] = parity
 
 
+# ----------------------------------------------------------------------------- single-kernel cases
+def _case_matmat(torch):
+    """The FP64 tensor-core product: 3 x (8192 x 8192) complex128 times 8 right-hand sides (3.2 GB)."""
+    from bempp_cuda.matmat import BatchedProduct
+
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    mats = [torch.randn((8192, 8192), dtype=torch.complex128, device="cuda", generator=gen) for _ in range(3)]
+    xs = [torch.randn((8192, 8), dtype=torch.complex128, device="cuda", generator=gen) for _ in range(3)]
+    ys = [torch.empty_like(x) for x in xs]
+    bp = BatchedProduct(mats, xs, ys)
+    return bp.launch, 3 * 16 * (8192 * 8192 + 2 * 8192 * 8)
+
+
+def _case_gemv(torch):
+    """The solves' one-right-hand-side product on a 16384 x 16384 complex128 matrix (4.3 GB)."""
+    from bempp_cuda.matmat import gemv
+
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    a = torch.randn((16384, 16384), dtype=torch.complex128, device="cuda", generator=gen)
+    x = torch.randn(16384, dtype=torch.complex128, device="cuda", generator=gen)
+    return (lambda: gemv(a, x)), a.numel() * 16
+
+
+def _combined_l5(torch, args):
+    from bempp_cuda.operators import Parameters
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+
+    grid = regular_sphere(5)
+    sp = function_space(grid, "DP", 0)
+    return sp, Parameters(), combined_descriptor(5.0)
+
+
+def _case_mixed_sym(torch, args=None):
+    """The mixed symmetric combined-field sweep on regular_sphere(5), k = 5 (1.07 GB output)."""
+    from bempp_cuda import _lib
+    from bempp_cuda.assembly import regular_into
+
+    sp, prm, desc = _combined_l5(torch, args)
+    out = torch.empty((8192, 8192), dtype=torch.complex128, device="cuda")
+    return (lambda: regular_into(out, desc, sp, sp, prm, precision=_lib.MIXED, overwrite=True)), out.numel() * 16
+
+
+def _case_apply(torch, args=None):
+    """The FP64 matrix-free apply of the combined field's regular part on regular_sphere(5), k = 5."""
+    from bempp_cuda.assembly import apply_regular
+
+    sp, prm, desc = _combined_l5(torch, args)
+    x = torch.ones(8192, dtype=torch.complex128, device="cuda")
+    y = torch.zeros(8192, dtype=torch.complex128, device="cuda")
+    return (lambda: apply_regular(y, x, desc, sp, sp, prm)), 0
+
+
+PROFILE_CASES = {"matmat_3x8192": _case_matmat, "gemv_16384": _case_gemv, "mixed_sym_l5": _case_mixed_sym,
+                 "apply_l5": _case_apply}
+
+
+def profile_case(args):
+    import torch
+
+    from bempp_cuda import _lib
+
+    _lib.load()
+    fn, nbytes = PROFILE_CASES[args.profile_case](torch)
+    for _ in range(max(1, args.warmup)):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    print(json.dumps({"profile_case": args.profile_case, "ms": ms, "bytes": nbytes,
+                      "gbs": nbytes / (ms * 1e-3) / 1e9 if nbytes else None}))
+
+
 def main():
     args = parse()
+    if args.profile_case:
+        profile_case(args)
+        return
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         line = reference_arm(args, world, rank)
