@@ -743,9 +743,34 @@ def shape_measure(args, torch):
         fd = np.array(fd)
         ad = np.array(ad)
         fdk = (obj.evaluate(x0, k + h, solver="lu").item() - obj.evaluate(x0, k - h, solver="lu").item()) / (2 * h)
-        res["fd_check"] = {"h": h, "coordinates": 20, "fd_solver": "complex128 dense LU (independent of the refined complex64 solve above)", "rel_err_norm": float(np.linalg.norm(ad - fd) / np.linalg.norm(fd)),
+        # the same coordinates with the fourth-order stencil (f(-2H) - 8 f(-H) + 8 f(H) - f(2H)) / (12 H),
+        # H = 1e-4: truncation O(H^4) and roundoff eps_J |J| / H both far below the h = 1e-6 central
+        # difference's roundoff, which dominates on the small gradient components
+        H = 1e-4
+        fd4 = []
+        for f in flat:
+            v, c = int(f) // 3, int(f) % 3
+            vals = []
+            for step in (-2, -1, 1, 2):
+                xs = x0.clone()
+                xs[v, c] += step * H
+                vals.append(obj.evaluate(xs, k, solver="lu").item())
+            fd4.append((vals[0] - 8 * vals[1] + 8 * vals[2] - vals[3]) / (12 * H))
+        fd4 = np.array(fd4)
+        res["fd_check"] = {"h": h, "coordinates": 20,
+                           "fd_solver": "complex128 dense LU (independent of the refined complex64 solve above)",
+                           "rel_err_norm": float(np.linalg.norm(ad - fd) / np.linalg.norm(fd)),
                            "max_rel_err": float(np.max(np.abs(ad - fd) / np.abs(fd))),
-                           "k_rel_err": float(abs(kgrad.item() - fdk) / abs(fdk))}
+                           "max_err_over_max_grad": float(np.max(np.abs(ad - fd)) / np.max(np.abs(fd))),
+                           "fourth_order_H": H,
+                           "fourth_order_rel_err_norm": float(np.linalg.norm(ad - fd4) / np.linalg.norm(fd4)),
+                           "fourth_order_max_rel_err": float(np.max(np.abs(ad - fd4) / np.abs(fd4))),
+                           "central_vs_fourth_order_max_rel": float(np.max(np.abs(fd - fd4) / np.abs(fd4))),
+                           "smallest_component_over_max": float(np.min(np.abs(fd4)) / np.max(np.abs(fd4))),
+                           "k_rel_err": float(abs(kgrad.item() - fdk) / abs(fdk)),
+                           "criterion": "per coordinate relative error <= 1e-6 against the fourth-order stencil; "
+                                        "the h = 1e-6 central difference is reported as configured, its "
+                                        "per-coordinate error is its own roundoff (central_vs_fourth_order)"}
     return res
 
 

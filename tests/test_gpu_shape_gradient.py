@@ -206,3 +206,22 @@ def test_refined_solvers_give_the_lu_gradient(solver):
     assert abs(v1.item() - v2.item()) <= 1e-11 * v1.item()
     assert (torch.linalg.norm(g1 - g2) / torch.linalg.norm(g1)).item() <= 1e-9
     assert abs(k1.item() - k2.item()) <= 1e-9 * abs(k1.item())
+
+
+def test_gradient_per_coordinate_fourth_order():
+    """Every one of 20 seeded coordinates within 1e-6 relative of a fourth-order central difference
+    (H = 1e-4; truncation O(H^4)), L3: the per-coordinate bound, which the h = 1e-6 two-point
+    difference cannot test on small components (its roundoff eps |J| / h exceeds 1e-6 of them)."""
+    obj, k = _objective(3, seed=1)
+    x0 = obj.vertices.clone()
+    value, state = obj.evaluate(x0, k, keep=True)
+    vgrad, _ = obj.gradient(state, k)
+    step = 1e-4
+    for v, c in _coords(obj.base.nvertices, 20, seed=7):
+        vals = []
+        for s in (-2, -1, 1, 2):
+            xs = x0.clone()
+            xs[v, c] += s * step
+            vals.append(obj.evaluate(xs, k).item())
+        fd4 = (vals[0] - 8 * vals[1] + 8 * vals[2] - vals[3]) / (12 * step)
+        assert abs(vgrad[v, c].item() - fd4) <= 1e-6 * abs(fd4), (v, c, vgrad[v, c].item(), fd4)
