@@ -298,6 +298,25 @@ def singular_into_dense(result, descriptor, domain, dual_to_range, parameters, d
     return result
 
 
+class MixedPrecisionFallback(UserWarning):
+    """device_interface="cuda_mixed" asked for an operator that has no mixed-precision kernel: it is
+    assembled / evaluated in FP64 (same values as "cuda")."""
+
+
+FP64_FALLBACKS = set()
+
+
+def note_fp64_fallback(descriptor, what):
+    """Record (and warn once per operator kind) that a mixed-precision request ran in FP64."""
+    import warnings
+
+    key = (what, getattr(descriptor, "kernel_type", None), getattr(descriptor, "assembly_type", None))
+    if key not in FP64_FALLBACKS:
+        FP64_FALLBACKS.add(key)
+        warnings.warn("cuda_mixed: no mixed-precision %s kernel for %s / %s; evaluated in FP64"
+                      % (what, key[1], key[2]), MixedPrecisionFallback, stacklevel=3)
+
+
 def _regular_with_fallback(result, descriptor, domain, dual_to_range, parameters, precision, **kw):
     """``regular_into`` in ``precision``; where the library has no mixed-precision
     kernel for the operator (it says so before launching anything) the FP64 one."""
@@ -306,6 +325,7 @@ def _regular_with_fallback(result, descriptor, domain, dual_to_range, parameters
     except _lib.BemppCudaError as exc:
         if exc.status != _lib.ERR_UNSUPPORTED or precision != _lib.MIXED:
             raise
+        note_fp64_fallback(descriptor, "regular-pair")
         regular_into(result, descriptor, domain, dual_to_range, parameters, precision=_lib.FP64, **kw)
 
 
@@ -483,6 +503,7 @@ def evaluate_potential_device(space, descriptor, points, local_coefficients, par
     lib = _lib.load()
     rc = lib.bemppcuda_evaluate_potential(args, stream or current_stream())
     if rc == _lib.ERR_UNSUPPORTED and precision == _lib.MIXED:
+        note_fp64_fallback(descriptor, "potential")
         args.precision = _lib.FP64  # no mixed kernel for this potential
         rc = lib.bemppcuda_evaluate_potential(args, stream or current_stream())
     _lib.check(rc)

@@ -27,6 +27,7 @@ from .assembly import (
     evaluate_potential_device,
     kernel_ids,
     kernel_params,
+    note_fp64_fallback,
     precision_of,
     regular_into,
     result_dtype,
@@ -103,6 +104,7 @@ def dense_assembler(device_interface, operator_descriptor, domain, dual_to_range
                      result_is_zero=True)
     except _lib.BemppCudaError as exc:
         if exc.status == _lib.ERR_UNSUPPORTED and precision == _lib.MIXED:
+            note_fp64_fallback(operator_descriptor, "regular-pair")
             regular_into(dev, operator_descriptor, domain, dual_to_range, parameters, precision=_lib.FP64,
                          result_is_zero=True)
         else:

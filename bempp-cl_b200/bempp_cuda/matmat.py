@@ -136,7 +136,8 @@ def gemv(a, x, out=None, stream=None):
 
 
 def matvec_of(a):
-    """v -> a @ v on the device: the library GEMV for complex matrices, torch.mv for real ones."""
-    if a.is_complex() and a.stride(1) == 1:
+    """v -> a @ v: the library GEMV for complex device matrices; torch.mv for real ones and for host
+    tensors (the solvers' host-side tests and tools; the product path's matrices are on the device)."""
+    if a.is_cuda and a.is_complex() and a.stride(1) == 1:
         return lambda v: gemv(a, v)
     return lambda v: _torch.mv(a, v)

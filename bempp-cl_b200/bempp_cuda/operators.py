@@ -75,7 +75,7 @@ class DenseDeviceOperator(object):
     def dot(self, x):
         if isinstance(x, _torch.Tensor):
             xt = x.to(self.tensor.dtype) if not self.tensor.is_complex() or x.is_complex() else x.to(self.tensor.dtype)
-            if xt.dim() == 1 and self.tensor.is_complex() and self.tensor.stride(1) == 1:
+            if xt.dim() == 1 and self.tensor.is_cuda and self.tensor.is_complex() and self.tensor.stride(1) == 1:
                 from .matmat import gemv
 
                 return gemv(self.tensor, xt)

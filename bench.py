@@ -894,7 +894,9 @@ def breadth_measure(args, torch, fp64_peak=None, fp32_peak=None):
                                             "helmholtz.adjoint_double_layer", 5, 5.0, 48),
                                            ("helmholtz.hypersingular p1 mixed", "helmholtz.hypersingular", 5, 5.0, 56),
                                            ("maxwell.electric_field rwg/snc mixed", "maxwell.electric_field", 4, 2.0,
-                                            101)):
+                                            101),
+                                           ("maxwell.magnetic_field rwg/snc mixed", "maxwell.magnetic_field", 4, 2.0,
+                                            192)):
         g = grid_of(level)
         if path.startswith("maxwell"):
             sp, dual = function_space(g, "RWG", 0), function_space(g, "SNC", 0)
@@ -920,12 +922,19 @@ def breadth_measure(args, torch, fp64_peak=None, fp32_peak=None):
         qpe = 36.0 * ne * ne
         gms = float(np.median(ms))
         achieved = qpe * flops_pp / (gms * 1e-3) / 1e12
+        from bempp_cuda.assembly import FP64_FALLBACKS
+
+        fallback = any(key[1] == opmx.descriptor.kernel_type and key[2] == opmx.descriptor.assembly_type
+                       for key in FP64_FALLBACKS)
         out.append({"operator": name, "level": level, "k": k, "shape": [rows, cols], "gpu_ms": gms,
                     "gpu_entries_per_s": rows * cols / (gms * 1e-3), "rel_fro_err_vs_fp64": err,
-                    "roofline": {"bound": "fp32", "flops_per_qpe": flops_pp, "qpe": qpe, "achieved": achieved,
-                                 "unit": "TFLOP/s", "peak": fp32_peak,
-                                 "frac": achieved / fp32_peak if fp32_peak else None},
-                    "note": "FP32 regular pairs, FP64 singular pairs and per-pair blocks"})
+                    "roofline": {"bound": "fp64" if fallback else "fp32", "flops_per_qpe": flops_pp, "qpe": qpe,
+                                 "achieved": achieved, "unit": "TFLOP/s",
+                                 "peak": fp64_peak if fallback else fp32_peak,
+                                 "frac": achieved / (fp64_peak if fallback else fp32_peak)
+                                 if (fp64_peak if fallback else fp32_peak) else None},
+                    "note": ("no mixed-precision kernel: FP64 under cuda_mixed" if fallback else
+                             "FP32 regular pairs, FP64 singular pairs and per-pair blocks")})
         del ref, mat
         torch.cuda.empty_cache()
 

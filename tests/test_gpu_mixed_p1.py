@@ -136,3 +136,24 @@ def test_mixed_interface_maxwell_mfie_is_fp64():
     a64 = operators.boundary.maxwell.magnetic_field(rwg, rwg, snc, 2.0).weak_form().tensor
     amx = operators.boundary.maxwell.magnetic_field(rwg, rwg, snc, 2.0, device_interface="cuda_mixed").weak_form().tensor
     assert (torch.linalg.norm(amx - a64) / torch.linalg.norm(a64)).item() < 1e-13
+
+
+def test_operators_without_mixed_kernel_warn_and_run_fp64():
+    """cuda_mixed on an operator without a mixed-precision kernel (the Maxwell magnetic field) warns
+    once (MixedPrecisionFallback) and gives the FP64 weak form."""
+    import warnings
+
+    from bempp_cuda import assembly, operators
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+
+    grid = regular_sphere(2)
+    rwg, snc = function_space(grid, "RWG", 0), function_space(grid, "SNC", 0)
+    assembly.FP64_FALLBACKS.clear()
+    with warnings.catch_warnings(record=True) as caught:
+        warnings.simplefilter("always")
+        mixed = operators.boundary.maxwell.magnetic_field(rwg, rwg, snc, 2.0,
+                                                          device_interface="cuda_mixed").weak_form().A
+    assert any(issubclass(w.category, assembly.MixedPrecisionFallback) for w in caught)
+    fp64 = operators.boundary.maxwell.magnetic_field(rwg, rwg, snc, 2.0).weak_form().A
+    assert np.array_equal(mixed, fp64) or np.linalg.norm(mixed - fp64) <= 1e-15 * np.linalg.norm(fp64)
