@@ -303,6 +303,9 @@ SIGNATURES = {
     "bemppcuda_assemble_regular": (_ct.c_int, [_ct.POINTER(RegularArgs), _vp]),
     "bemppcuda_apply_regular": (_ct.c_int, [_ct.POINTER(RegularArgs), _vp, _vp, _vp]),
     "bemppcuda_gemv": (_ct.c_int, [_vp, _i64, _i64, _i64, _vp, _vp, _i32, _vp]),
+    "bemppcuda_quadrature_points": (_ct.c_int, [_ct.POINTER(GridRec), _ct.POINTER(Space), _i32, _vp, _vp, _vp, _vp,
+                                                _vp]),
+    "bemppcuda_project": (_ct.c_int, [_ct.POINTER(GridRec), _ct.POINTER(Space), _i32, _vp, _vp, _vp, _vp, _vp]),
     "bemppcuda_assemble_singular": (_ct.c_int, [_ct.POINTER(SingularArgs), _vp]),
     "bemppcuda_potential_workspace_bytes": (_i64, [_ct.POINTER(PotentialArgs)]),
     "bemppcuda_evaluate_potential": (_ct.c_int, [_ct.POINTER(PotentialArgs), _vp]),

@@ -11,17 +11,16 @@ w_q * phi_i(q) * f(x_q) * |J|.
 Callables are vectorized numpy functions ``fun(x, n, domain_index, result)``
 with x, n of shape (3, npoints), domain_index (npoints,) and result
 (codomain_dimension, npoints) filled in place (the reference's vectorized
-callable convention).
+callable convention), or functions marked with ``device_callable``, which
+take the same arguments as CUDA tensors and return the values (npoints,) as
+a tensor.  Both go through the device kernels (``bemppcuda_quadrature_points``,
+``bemppcuda_project``): the points and normals of the rule are formed on the
+device, a device callable is evaluated there (the whole projection stays in
+HBM), a host callable on copies of them; the weighted sums and the scatter
+onto the dofs run on the device.
 """
 
 import numpy as _np
-
-from .quadrature import triangle_rule
-
-
-def _local_values(space, points):
-    """Shape values (codomain, nshape, npoints) on every support element."""
-    return space.shapeset.evaluate(points)
 
 
 class GridFunction(object):
@@ -37,7 +36,8 @@ class GridFunction(object):
         self._projections = None if projections is None else _np.asarray(projections)
         order = parameters.quadrature.regular if parameters is not None else 4
         if fun is not None:
-            self._projections = project_callable(fun, self.dual_space, order, complex)
+            proj = project_callable_device(fun, self.dual_space, order)
+            self._projections = proj.cpu().numpy() if complex else proj.real.cpu().numpy()
 
     @property
     def coefficients(self):
@@ -60,29 +60,49 @@ class GridFunction(object):
         raise ValueError("projections onto a different space are implemented for identical DP0 spaces")
 
 
-def project_callable(fun, dual_space, order=4, complex=True):
-    """Vector of projections <fun, phi_i> onto ``dual_space`` (grid_function.py:824-863)."""
+def device_callable(fun):
+    """Mark ``fun(x, n, domain_index) -> values`` as a device callable: x, n (3, npoints) float64 and
+    domain_index (npoints,) int32 CUDA tensors in, the (npoints,) values (real or complex) out."""
+    fun.bempp_cuda_device = True
+    return fun
+
+
+def project_callable_device(fun, dual_space, order=4):
+    """Projections <fun, phi_i> onto the scalar ``dual_space`` as a complex128 CUDA tensor
+    (grid_function.py, _project_function_vectorized, on the device)."""
+    import torch
+
+    from . import _lib
+    from .assembly import regular_rule
+    from .device import current_stream, device_grid, device_space, ptr, require_cuda
+
+    require_cuda()
+    if dual_space.codomain_dimension != 1:
+        raise ValueError("callable projection is implemented for scalar spaces")
     grid = dual_space.grid
-    points, weights = triangle_rule(order)
+    dgrid = device_grid(grid)
+    dspace = device_space(dual_space)
+    qp, qw = regular_rule(order)
+    nq = len(qw)
+    nsup = dspace.nsupport
+    grec, srec = dgrid.record(), dspace.record()
+    lib = _lib.load()
+    points = torch.empty((3, nsup * nq), dtype=torch.float64, device="cuda")
+    normals = torch.empty((3, nsup * nq), dtype=torch.float64, device="cuda")
+    _lib.check(lib.bemppcuda_quadrature_points(grec, srec, nq, qp.ctypes.data, qw.ctypes.data, ptr(points),
+                                               ptr(normals), current_stream()))
     sup = _np.asarray(dual_space.support_elements, dtype=_np.int64)
-    e = grid.elements.astype(_np.int64)[:, sup]
-    v = grid.vertices
-    b0 = 1.0 - points[0] - points[1]
-    # global points (3, nsup, nq) as barycentric combinations of the corners
-    gp = (v[:, e[0]][:, :, None] * b0 + v[:, e[1]][:, :, None] * points[0] + v[:, e[2]][:, :, None] * points[1])
-    nq = len(weights)
-    normals = (grid.normals[sup] * dual_space.normal_multipliers[sup][:, None]).T
-    x = gp.reshape(3, -1)
-    n = _np.repeat(normals, nq, axis=1)
-    dom = _np.repeat(grid.domain_indices[sup], nq)
-    values = _np.zeros((1, x.shape[1]), dtype=_np.complex128 if complex else _np.float64)
-    fun(x, n, dom, values)
-    values = values.reshape(len(sup), nq)
-    shape = _local_values(dual_space, points)[0]  # (nshape, nq)
-    ie = grid.integration_elements[sup]
-    local = _np.einsum("eq,iq,q->ei", values, shape, weights) * ie[:, None]
-    out = _np.zeros(dual_space.global_dof_count, dtype=values.dtype)
-    l2g = dual_space.local2global[sup]
-    mult = dual_space.local_multipliers[sup]
-    _np.add.at(out, l2g.ravel(), (local * mult).ravel())
+    dom = _np.repeat(_np.asarray(grid.domain_indices)[sup], nq).astype(_np.int32)
+    if getattr(fun, "bempp_cuda_device", False):
+        values = fun(points, normals, torch.as_tensor(dom, device="cuda"))
+        values = torch.as_tensor(values, device="cuda").reshape(-1).to(torch.complex128).contiguous()
+    else:
+        host = _np.zeros((1, nsup * nq), dtype=_np.complex128)
+        fun(points.cpu().numpy(), normals.cpu().numpy(), dom, host)
+        values = torch.as_tensor(host[0], device="cuda")
+    if values.numel() != nsup * nq:
+        raise ValueError("the callable returned %d values for %d points" % (values.numel(), nsup * nq))
+    out = torch.empty(int(dual_space.global_dof_count), dtype=torch.complex128, device="cuda")
+    _lib.check(lib.bemppcuda_project(grec, srec, nq, qp.ctypes.data, qw.ctypes.data, ptr(values), ptr(out),
+                                     current_stream()))
     return out

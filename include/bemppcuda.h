@@ -323,6 +323,22 @@ int bemppcuda_assemble_singular(const bemppcuda_singular_args *args, void *strea
    y is updated with atomics: the summation order is not deterministic. */
 int bemppcuda_apply_regular(const bemppcuda_regular_args *args, const void *x, void *y, void *stream);
 
+/* Projections of a function onto a scalar space (P0 / P1 shapesets): the vectorized projection of
+   GridFunction (api/assembly/grid_function.py, _project_function_vectorized), on the device.
+   bemppcuda_quadrature_points writes the global points and the unit normals (times the normal
+   multipliers) of every (support element, point) of the nq-point rule, in the reference's
+   vectorized-callable layout: points / normals (3, nsupport * nq), component-major, point index
+   k * nq + q for support element k; normals may be NULL.  The caller evaluates its function there
+   (on the device or the host) and passes the complex128 values (nsupport * nq);
+   bemppcuda_project zeroes out (ndofs complex128) and adds
+   mult(e, i) |J_e| sum_q w_q phi_i(q) f(e, q) at l2g(e, i) with FP64 atomics (order not fixed). */
+int bemppcuda_quadrature_points(const bemppcuda_grid *grid, const bemppcuda_space *space, int32_t nq,
+                                const double *quad_points, const double *quad_weights, double *points,
+                                double *normals, void *stream);
+int bemppcuda_project(const bemppcuda_grid *grid, const bemppcuda_space *space, int32_t nq,
+                      const double *quad_points, const double *quad_weights, const void *values, void *out,
+                      void *stream);
+
 /* Bytes of the source table (0 for no sources; -1 when the size overflows int64, which
    bemppcuda_evaluate_potential rejects with BEMPPCUDA_ERR_INVALID). */
 int64_t bemppcuda_potential_workspace_bytes(const bemppcuda_potential_args *args);
