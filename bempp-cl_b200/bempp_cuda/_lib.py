@@ -104,6 +104,8 @@ class RegularArgs(_ct.Structure):
         ("row_end", _i64),
         ("result_is_zero", _i32),
         ("pad2", _i32),
+        ("tresult", _vp),
+        ("col_begin", _i64),
     ]
 
 

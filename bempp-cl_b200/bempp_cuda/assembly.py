@@ -91,7 +91,7 @@ def same_space(a, b):
 
 def regular_into(
     result, descriptor, domain, dual_to_range, parameters, precision=_lib.FP64, overwrite=False, stream=None,
-    geometry=None, symmetric=True, rows=None, result_is_zero=False,
+    geometry=None, symmetric=True, rows=None, result_is_zero=False, tresult=None, col_begin=0,
 ):
     """Add (or with ``overwrite`` store) the regular part into the device tensor ``result``.
 
@@ -104,7 +104,11 @@ def regular_into(
     (i, j), i <= j, with rows i in [lo, hi) (both entries written).
     ``result_is_zero`` promises that ``result`` holds zeros, which lets
     symmetric P1 single-layer and hypersingular sweeps add only the blocks
-    of the pairs i < j and symmetrise the matrix afterwards.
+    of the pairs i < j and symmetrise the matrix afterwards.  ``tresult``
+    (with ``rows``, DP0 symmetric sweep): stripe mode, ``result`` and
+    ``tresult`` hold rows [lo, hi) and columns [col_begin, n): A_ij of the
+    swept pairs i <= j at result[i - lo, j - col_begin], A_ji at
+    tresult[i - lo, j - col_begin].
     """
     require_cuda()
     kernel, assembly = kernel_ids(descriptor)
@@ -138,6 +142,11 @@ def regular_into(
     args.result_is_zero = 1 if result_is_zero else 0
     if rows is not None:
         args.row_begin, args.row_end = int(rows[0]), int(rows[1])
+    if tresult is not None:
+        if tresult.shape != result.shape or tresult.dtype != result.dtype or tresult.stride() != result.stride():
+            raise ValueError("tresult must have the shape, dtype and strides of result")
+        args.tresult = ptr(tresult)
+        args.col_begin = int(col_begin)
     # a little slack over the exact bound keeps rounding of the radii on the safe side
     args.phase_radius = 1.0001 * (tgrid.radius + sgrid.radius)
     _lib.check(_lib.load().bemppcuda_assemble_regular(args, stream or current_stream()))

@@ -204,7 +204,7 @@ int bemppcuda_assemble_regular(const bemppcuda_regular_args *a, void *stream) {
         bc_set_error("regular rule: 1 <= nq <= %d host points and weights required", BEMPPCUDA_MAX_REGULAR_POINTS);
         return BEMPPCUDA_ERR_INVALID;
     }
-    if (!a->result || a->ld < a->trial.ndofs) {
+    if (!a->result || a->ld < a->trial.ndofs - (a->tresult ? a->col_begin : 0)) {
         bc_set_error("result pointer missing or ld (%lld) < columns (%lld)", (long long)a->ld,
                      (long long)a->trial.ndofs);
         return BEMPPCUDA_ERR_INVALID;

@@ -29,6 +29,8 @@ struct RegParams {
     void *result;
     int64_t ld;
     double near_r;  // bound on the centroid distance of vertex-sharing pairs (0: unknown, test every pair)
+    void *tresult;  // stripe mode of the symmetric DP0 sweeps (store_pair): transposed entries, local rows
+    int64_t row0, col0;
 };
 
 constexpr int DP0_THREADS = 128;
@@ -93,6 +95,46 @@ __device__ __forceinline__ void store_entry(const RegParams &prm, int64_t row, i
         else if (!adj)
             *out += re;
     }
+}
+
+// Both entries of a symmetric-sweep pair (row i <= column j): A_ij at (i, j) and A_ji at (j, i) of the
+// matrix, or in stripe mode (STRIPE, prm.tresult set) A_ij at (i - row0, j - col0) of result and A_ji
+// at the same position of tresult, so both stores of a warp are coalesced.  A template switch, so the
+// single-GPU sweeps carry no stripe branch.
+template <bool STRIPE>
+__device__ __forceinline__ void store_pair(const RegParams &prm, int64_t row, int64_t col, bool adj, double a_re,
+                                           double a_im, double b_re, double b_im) {
+    if (STRIPE) {
+        const int64_t at = (row - prm.row0) * prm.ld + (col - prm.col0);
+        if (prm.is_complex) {
+            double2 *o = reinterpret_cast<double2 *>(prm.result) + at;
+            double2 *ot = reinterpret_cast<double2 *>(prm.tresult) + at;
+            if (prm.overwrite) {
+                *o = make_double2(a_re, a_im);
+                if (row != col) *ot = make_double2(b_re, b_im);
+            } else if (!adj) {
+                const double2 u = *o;
+                *o = make_double2(u.x + a_re, u.y + a_im);
+                if (row != col) {
+                    const double2 v = *ot;
+                    *ot = make_double2(v.x + b_re, v.y + b_im);
+                }
+            }
+        } else {
+            double *o = reinterpret_cast<double *>(prm.result) + at;
+            double *ot = reinterpret_cast<double *>(prm.tresult) + at;
+            if (prm.overwrite) {
+                *o = a_re;
+                if (row != col) *ot = b_re;
+            } else if (!adj) {
+                *o += a_re;
+                if (row != col) *ot += b_re;
+            }
+        }
+        return;
+    }
+    store_entry(prm, row, col, adj, a_re, a_im);
+    if (row != col) store_entry(prm, col, row, adj, b_re, b_im);
 }
 
 // FP64: one thread per (trial element, block of 32 test elements).

@@ -235,7 +235,7 @@ __device__ __forceinline__ void pair_sym64(const RegParams &prm, const QuadRule 
     }
 }
 
-template <int K, int PHC>
+template <int K, int PHC, bool STRIPE = false>
 __device__ __forceinline__ void regular_dp0_fp64_sym_tile(const RegParams &prm, const QuadRule &rule,
                                                         int64_t tile_x, int64_t t0, int rows, TestBlock64s &sb) {
     const int tcount = (int)min((int64_t)rows, prm.ntest - t0);
@@ -252,8 +252,7 @@ __device__ __forceinline__ void regular_dp0_fp64_sym_tile(const RegParams &prm, 
             const bool adj = row == si || (prm.grids_identical && shares_vertex(sb.v[tt], tr.sv0, tr.sv1, tr.sv2));
             double a_re = 0.0, a_im = 0.0, b_re = 0.0, b_im = 0.0;  // A_ij, A_ji
             if (!adj) pair_sym64<K, PHC>(prm, rule, sb, tt, tr, a_re, a_im, b_re, b_im);
-            store_entry(prm, row, si, adj, a_re, a_im);
-            if (row != si) store_entry(prm, si, row, adj, b_re, b_im);
+            store_pair<STRIPE>(prm, row, si, adj, a_re, a_im, b_re, b_im);
         }
     }
     __syncthreads();  // the shared block is reused by the next tile of a persistent loop
@@ -343,7 +342,7 @@ __device__ __forceinline__ void sincos2_sym(float2 x, float2 *s, float2 *c) {
 // w_b for 3-5, the order-4 rule): the FP32 sums of the first orbit are scaled
 // by w_a / w_b when the second begins, and everything is converted to FP64
 // once, times w_b.
-template <int K, int PHC>
+template <int K, int PHC, bool STRIPE = false>
 __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm, const QuadRule &rule,
                                                          int64_t tile_x, int64_t t0, int rows, TestBlock32q &sb) {
     using ST = SymTraits<K>;
@@ -538,8 +537,7 @@ __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm,
             b_im = (b_re * ps + b_im * pc) * scale;
             b_re = tr * scale;
         }
-        store_entry(prm, row, si, adj, a_re, a_im);
-        if (row != si) store_entry(prm, si, row, adj, b_re, b_im);
+        store_pair<STRIPE>(prm, row, si, adj, a_re, a_im, b_re, b_im);
     }
     }
     __syncthreads();

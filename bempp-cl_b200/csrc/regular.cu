@@ -236,13 +236,14 @@ __global__ void __launch_bounds__(GEN_THREADS) regular_generic(RegParams prm, Qu
 // Symmetric sweeps: blockIdx.x = column block, blockIdx.y = row chunk; chunks
 // that start below the block's last column have no pair i <= j and exit
 // before touching shared memory.
-template <int K, int PHC>
+template <int K, int PHC, bool STRIPE = false>
 __global__ void __launch_bounds__(DP0_THREADS) regular_dp0_fp64_sym(RegParams prm, QuadRule rule, int64_t row0,
                                                                     int64_t row1, int tile_rows) {
     const int64_t t0 = row0 + (int64_t)blockIdx.y * tile_rows;
     if (t0 >= ((int64_t)blockIdx.x + 1) * DP0_THREADS) return;
     __shared__ TestBlock64s sb;
-    regular_dp0_fp64_sym_tile<K, PHC>(prm, rule, blockIdx.x, t0, (int)min((int64_t)tile_rows, row1 - t0), sb);
+    regular_dp0_fp64_sym_tile<K, PHC, STRIPE>(prm, rule, blockIdx.x, t0, (int)min((int64_t)tile_rows, row1 - t0),
+                                              sb);
 }
 
 // CTAs per SM the mixed symmetric sweep is compiled for (register cap 170 at
@@ -251,14 +252,52 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_dp0_fp64_sym(RegParams pr
 #define BC_MSYM_MIN_BLOCKS 3
 #endif
 
-template <int K, int PHC>
+template <int K, int PHC, bool STRIPE = false>
 __global__ void __launch_bounds__(DP0_THREADS, BC_MSYM_MIN_BLOCKS) regular_dp0_mixed_sym(RegParams prm, QuadRule rule,
                                                                                       int64_t row0, int64_t row1,
                                                                                       int tile_rows) {
     const int64_t t0 = row0 + (int64_t)blockIdx.y * tile_rows;
     if (t0 >= ((int64_t)blockIdx.x + 1) * DP0_THREADS) return;
     __shared__ TestBlock32q sb;
-    regular_dp0_mixed_sym_tile<K, PHC>(prm, rule, blockIdx.x, t0, (int)min((int64_t)tile_rows, row1 - t0), sb);
+    regular_dp0_mixed_sym_tile<K, PHC, STRIPE>(prm, rule, blockIdx.x, t0, (int)min((int64_t)tile_rows, row1 - t0),
+                                               sb);
+}
+
+// Kernels with a stripe-mode instance (the multi-GPU symmetric stripes): the Helmholtz family, the
+// combined field and the Laplace single layer.
+template <int K>
+constexpr bool stripe_kernel() {
+    return K == BEMPPCUDA_HELMHOLTZ_SLP || K == BEMPPCUDA_HELMHOLTZ_DLP || K == BEMPPCUDA_HELMHOLTZ_ADLP ||
+           K == BEMPPCUDA_HELMHOLTZ_COMBINED || K == BEMPPCUDA_LAPLACE_SLP;
+}
+
+// The symmetric sweep of launch_dp0 in stripe mode (real wavenumber; mixed or FP64).
+template <int K>
+static cudaError_t launch_dp0_stripe(const RegParams &prm, const QuadRule &rule, int mixed, int phase_class,
+                                     int64_t row0, int64_t row1, int tile_rows, dim3 sgrid, cudaStream_t st) {
+    if constexpr (stripe_kernel<K>()) {
+        if (mixed) {
+            if (phase_class == 2)
+                regular_dp0_mixed_sym<K, 2, true><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
+            else if (phase_class == 1)
+                regular_dp0_mixed_sym<K, 1, true><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
+            else
+                regular_dp0_mixed_sym<K, 0, true><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
+        } else if (!KernelTraits<K>::helm) {
+            regular_dp0_fp64_sym<K, 0, true><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
+        } else if (prm.p[1] != 0.0) {
+            regular_dp0_fp64_sym<K, 3, true><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
+        } else if (phase_class == 2) {
+            regular_dp0_fp64_sym<K, 2, true><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
+        } else if (phase_class == 1) {
+            regular_dp0_fp64_sym<K, 1, true><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
+        } else {
+            regular_dp0_fp64_sym<K, 0, true><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
+        }
+        return cudaGetLastError();
+    } else {
+        return cudaErrorInvalidValue;
+    }
 }
 
 template <int K>
@@ -281,6 +320,7 @@ static cudaError_t launch_dp0(const RegParams &prm, const QuadRule &rule, int mi
             while (tile_rows > 8 && (int64_t)grid.x * ((row1 - row0 + tile_rows - 1) / tile_rows) / 2 < 4 * wave)
                 tile_rows /= 2;
             const dim3 sgrid(grid.x, (unsigned)((row1 - row0 + tile_rows - 1) / tile_rows));
+            if (prm.tresult) return launch_dp0_stripe<K>(prm, rule, mixed, phase_class, row0, row1, tile_rows, sgrid, st);
             if constexpr (!KernelTraits<K>::modhelm) {
                 if (mixed) {
                     if (phase_class == 2)
@@ -521,6 +561,8 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
     prm.ld = a->ld;
     // R_test + R_trial bounds the centroid distance of two elements that share a vertex
     prm.near_r = a->phase_radius > 0.0 ? a->phase_radius : 0.0;
+    prm.tresult = nullptr;
+    prm.row0 = prm.col0 = 0;
     if (prm.ntest == 0 || prm.ntrial == 0) return BEMPPCUDA_OK;
 
     QuadRule rule;
@@ -579,6 +621,26 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
         return BEMPPCUDA_ERR_INVALID;
     }
     const int64_t row0 = ranged ? a->row_begin : 0, row1 = ranged ? a->row_end : prm.ntest;
+    if (a->tresult) {
+        // stripe mode: only the DP0 symmetric sweep over a row range stores into local buffers
+        if (!ranged || !dp0 || !sym_ok || a->col_begin < 0 || a->col_begin > a->row_begin ||
+            a->ld < prm.ntrial - a->col_begin) {
+            bc_set_error("tresult needs the DP0 symmetric sweep over a row range, 0 <= col_begin <= row_begin "
+                         "and ld >= columns - col_begin");
+            return BEMPPCUDA_ERR_INVALID;
+        }
+        const bool kernel_ok = a->kernel == BEMPPCUDA_HELMHOLTZ_SLP || a->kernel == BEMPPCUDA_HELMHOLTZ_DLP ||
+                               a->kernel == BEMPPCUDA_HELMHOLTZ_ADLP || a->kernel == BEMPPCUDA_HELMHOLTZ_COMBINED ||
+                               a->kernel == BEMPPCUDA_LAPLACE_SLP;
+        if (!kernel_ok) {
+            bc_set_error("tresult (stripe mode): Helmholtz single, double, adjoint double layer, combined field "
+                         "and Laplace single layer only");
+            return BEMPPCUDA_ERR_UNSUPPORTED;
+        }
+        prm.tresult = a->tresult;
+        prm.row0 = a->row_begin;
+        prm.col0 = a->col_begin;
+    }
     if (dp0) {
         switch (a->kernel) {
         case BEMPPCUDA_LAPLACE_SLP: err = launch_dp0<BEMPPCUDA_LAPLACE_SLP>(prm, rule, mixed, phase_class, sym, row0, row1, st); break;

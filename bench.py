@@ -38,9 +38,11 @@ pairs + Sauter-Schwab singular pairs + identity), matrix resident in HBM.
   ``batch.many_small`` repeats this for 256 problems of 128 / 512 elements,
   where separate launches cannot fill the GPU.
 
-Multi-GPU (torchrun): the rows (test elements) are split into one contiguous
-block per rank; each rank assembles its block with no collective (strong
-scaling, total work fixed).  ``--impl reference`` times the reference's CPU
+Multi-GPU (torchrun): symmetric stripes -- rank r sweeps the element pairs
+(i, j), i <= j, of its rows [lo_r, hi_r) (equal pair counts over the ranks),
+keeping A_ij and the transposed A_ji in two local buffers, with no collective
+(strong scaling, total work fixed, each pair's kernel work done once as on
+one GPU); the distributed solve runs on the stripes.  ``--impl reference`` times the reference's CPU
 path (as ``cpu_baseline``) on rank 0 only.
 """
 
@@ -245,17 +247,39 @@ def gpu_arm(args, world, rank, local):
     device_grid(grid)
     device_space(domain)
     device_space(dual)
-    rule = device_singular_rule(grid, params.quadrature.singular, dual.support, domain.support)
-    npairs_singular = rule.npairs
-    out = torch.empty((rows, cols), dtype=torch.complex128, device="cuda")
+    n_el = int(grid.number_of_elements)
+    stripe = None
+    if world == 1:
+        rule = device_singular_rule(grid, params.quadrature.singular, dual.support, domain.support)
+        npairs_singular = rule.npairs
+        out = torch.empty((rows, cols), dtype=torch.complex128, device="cuda")
+        rank_entries = rows * cols
+    else:
+        # symmetric stripes: this rank sweeps the pairs (i, j), i <= j, of rows [lo, hi) (equal pair counts
+        # over the ranks) into U (A_ij) and L (A_ji), both (hi - lo) x (n - lo)
+        from bempp_cuda.distributed import singular_into_stripe, stripe_bounds, stripe_entries, stripe_singular_pairs
+
+        lo, hi = stripe_bounds(n_el, world)[rank]
+        stripe = (lo, hi)
+        out = torch.zeros((hi - lo, n_el - lo), dtype=torch.complex128, device="cuda")
+        out_t = torch.zeros_like(out)
+        rank_entries = stripe_entries(n_el, lo, hi)
+        npairs_singular = stripe_singular_pairs(domain, params, lo, hi)  # builds the stripe's pair list
 
     def one_step(precision, events=None):
         if events is not None:
             events[0].record()
-        regular_into(out, desc, domain, dual, params, precision=precision, overwrite=True)
+        if stripe is None:
+            regular_into(out, desc, domain, dual, params, precision=precision, overwrite=True)
+        else:
+            regular_into(out, desc, domain, domain, params, precision=precision, overwrite=True, rows=stripe,
+                         tresult=out_t, col_begin=stripe[0])
         if events is not None:
             events[1].record()
-        singular_into_dense(out, desc, domain, dual, params, diag_shift=-0.5)
+        if stripe is None:
+            singular_into_dense(out, desc, domain, dual, params, diag_shift=-0.5)
+        else:
+            singular_into_stripe(out, out_t, stripe[0], stripe[1], desc, domain, params, diag_shift=-0.5)
         if events is not None:
             events[2].record()
 
@@ -303,7 +327,8 @@ def gpu_arm(args, world, rank, local):
         t64, reg64, sing64, _ = timed(_lib.FP64, args.steps, args.warmup, False)
         fp64 = {"value": total_entries * args.steps / (t64 * 1e-3), "unit": "entries/s",
                 "ms_per_step": t64 / args.steps, "regular_ms": reg64, "singular_ms": sing64}
-        ref64 = out.clone() if rows * cols * 16 * 3 < torch.cuda.get_device_properties(local).total_memory * 0.85 else None
+        fits = rank_entries * 16 * 3 < torch.cuda.get_device_properties(local).total_memory * 0.85
+        ref64 = (out.clone() if stripe is None else (out.clone(), out_t.clone())) if fits else None
     tmx, regmx, singmx, clocks = timed(_lib.MIXED, args.steps, args.warmup, True)
     value = total_entries * args.steps / (tmx * 1e-3)
     # seeded rows of both matrices for the parity check against the CPU reference (after timing)
@@ -317,7 +342,11 @@ def gpu_arm(args, world, rank, local):
     if fp64 is not None:
         fp64["mixed_over_fp64"] = value / fp64["value"]
         if ref64 is not None:
-            err = torch.linalg.norm(out - ref64) / torch.linalg.norm(ref64)
+            if stripe is None:
+                err = torch.linalg.norm(out - ref64) / torch.linalg.norm(ref64)
+            else:
+                err = torch.sqrt((torch.linalg.norm(out - ref64[0]) ** 2 + torch.linalg.norm(out_t - ref64[1]) ** 2)
+                                 / (torch.linalg.norm(ref64[0]) ** 2 + torch.linalg.norm(ref64[1]) ** 2))
             fp64["mixed_rel_fro_err"] = float(err.item())
             if not args.skip_solve:
                 if world == 1:
@@ -327,15 +356,14 @@ def gpu_arm(args, world, rank, local):
             del ref64
         torch.cuda.empty_cache()
 
-    # roofline of the regular-pair kernel (mixed precision)
-    regular_pairs = rows * cols - npairs_singular
+    # roofline of the regular-pair kernel (mixed precision); entries of this rank's block or stripe
+    regular_pairs = rank_entries - npairs_singular
     qpe = 36 * regular_pairs
     flops = qpe * FLOPS_PER_QPE["helmholtz_combined_field"]
     achieved = flops / (regmx * 1e-3) / 1e12
     roof = {"bound": "fp32", "achieved": achieved, "peak": peaks["fp32"], "unit": "TFLOP/s",
-            "frac": achieved / peaks["fp32"], "traffic": traffic_estimate(rows, cols),
-            "kernel": "regular_dp0_mixed_sym<HELMHOLTZ_COMBINED>" if rows == cols else
-                      "regular_dp0_mixed2<HELMHOLTZ_COMBINED>", "kernel_ms": regmx,
+            "frac": achieved / peaks["fp32"], "traffic": traffic_estimate(rank_entries, 1),
+            "kernel": "regular_dp0_mixed_sym<HELMHOLTZ_COMBINED>", "kernel_ms": regmx,
             "flops_per_qpe": FLOPS_PER_QPE["helmholtz_combined_field"], "qpe_per_launch": qpe,
             "flops_convention": "algorithmic flops of evaluating every entry on its own (the reference's "
                                 "work); the symmetric sweep evaluates each point pair once for A_ij and A_ji, "
@@ -386,7 +414,8 @@ def gpu_arm(args, world, rank, local):
         "data": "synthetic: regular_sphere(%d) unit sphere, generated by octahedron subdivision" % args.level,
         "config": bench_config(args),
         "precision": "mixed: FP32 regular pairs, FP64 singular pairs and per-entry sums",
-        "parallelism": "row blocks x%d" % world,
+        "parallelism": ("symmetric stripes x%d (equal pair counts; U and L per rank)" % world) if world > 1
+                       else "one GPU",
         "gpu_launches": 2 * args.steps,
         "clocks": clocks,
         "roofline": roof,
@@ -1018,9 +1047,10 @@ def breadth_measure(args, torch, fp64_peak=None, fp32_peak=None):
     return out
 
 
-def solve_measure_distributed(args, torch, grid, domain, a_local, world, rank, dist):
-    """C3 solve on row blocks: FP64 GMRES with one all-gather of the iterate per matvec (NCCL)."""
-    from bempp_cuda.distributed import RowBlockOperator, gmres_distributed
+def solve_measure_distributed(args, torch, grid, domain, stripes, world, rank, dist):
+    """C3 solve on symmetric stripes: FP64 GMRES, per matvec one all-gather of the iterate and one
+    all-reduce of the product (NCCL)."""
+    from bempp_cuda.distributed import StripeOperator, gmres_distributed
     from bempp_cuda.grid_function import GridFunction
 
     k = args.k
@@ -1029,7 +1059,7 @@ def solve_measure_distributed(args, torch, grid, domain, a_local, world, rank, d
         result[0] = -np.exp(1j * k * x[2])
 
     n = grid.number_of_elements
-    op = RowBlockOperator(a_local, n, world, rank)
+    op = StripeOperator(stripes[0], stripes[1], n, world, rank)
     lo, hi = op.local_range
     b = GridFunction(domain, fun=minus_incident).projections(domain)
     b_local = torch.as_tensor(b[lo:hi], device="cuda")
@@ -1050,8 +1080,9 @@ def solve_measure_distributed(args, torch, grid, domain, a_local, world, rank, d
             "fp64_distributed": {"iterations": its, "info": info, "seconds": float(t.item()) / 1e3,
                                  "final_residual": res[-1],
                                  "true_residual": float(torch.sqrt(rr[0] / rr[1]).item()),
-                                 "collectives": "per iteration: all-gather of the iterate (NCCL), all-reduce of "
-                                                "the orthogonalisation coefficients and norms"}}
+                                 "collectives": "per iteration: all-gather of the iterate and all-reduce of the "
+                                                "stripe products (NCCL), all-reduce of the orthogonalisation "
+                                                "coefficients and norms"}}
 
 
 def e2e_measure(args, torch, grid, domain, dual, world, dist, clear_cache, total_entries):

@@ -134,6 +134,14 @@ typedef struct {
                                    the pairs i < j and form A = U + U^T in one pass over the matrix,
                                    half the global atomics; 0: accumulate both blocks into result */
     int32_t pad2;
+    void *tresult;              /* NULL, or with row_begin / row_end (the DP0 symmetric sweep): a stripe
+                                   of the upper triangle into two local buffers of the same layout,
+                                   A_ij at result[(i - row_begin) * ld + (j - col_begin)] and the
+                                   transposed entry A_ji at tresult[(i - row_begin) * ld + (j - col_begin)],
+                                   for the swept pairs i <= j (entries with j < i are not written);
+                                   Helmholtz single / double / adjoint double layer, combined field and
+                                   Laplace single layer (others: BEMPPCUDA_ERR_UNSUPPORTED) */
+    int64_t col_begin;          /* first column held by result / tresult (<= row_begin) */
 } bemppcuda_regular_args;
 
 /* Singular pairs (Sauter-Schwab), the arrays of

@@ -98,3 +98,91 @@ def test_row_block_operator_rejects_wrong_block():
 
     with pytest.raises(ValueError):
         RowBlockOperator(torch.zeros((4, 10)), 10, 2, 0)  # rank 0 of 2 owns rows [0, 5)
+
+
+def _stripes(a, world, rank):
+    """The stripe (U, L) of rank ``rank`` cut from a full matrix, as the stripe assembly leaves it."""
+    from bempp_cuda.distributed import stripe_bounds
+
+    n = a.shape[0]
+    lo, hi = stripe_bounds(n, world)[rank]
+    U = np.zeros((hi - lo, n - lo), dtype=a.dtype)
+    L = np.zeros_like(U)
+    for i in range(lo, hi):
+        U[i - lo, i - lo:] = a[i, i:]       # A_ij, j >= i
+        L[i - lo, i + 1 - lo:] = a[i + 1:, i]  # A_ji, j > i
+    return U, L
+
+
+def _stripe_worker(rank, world, port, n, restart, result_path):
+    import datetime
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, os.path.join(root, "bempp-cl_b200"))
+    import torch.distributed as dist
+
+    from bempp_cuda.distributed import StripeOperator, gmres_distributed, stripe_bounds
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        a, b = _matrix(n)
+        U, L = _stripes(a, world, rank)
+        op = StripeOperator(torch.as_tensor(U), torch.as_tensor(L), n, world, rank)
+        lo, hi = stripe_bounds(n, world)[rank]
+        x = np.random.default_rng(3).standard_normal(n) + 0j
+        ax = op.matvec(torch.as_tensor(x[lo:hi]))
+        x_local, info, residuals, its = gmres_distributed(op, torch.as_tensor(b[lo:hi]), tol=1e-12, restart=restart)
+        full = op.gather(x_local)
+        np.savez(result_path % rank, x=full.numpy(), info=info, its=its, ax=ax.numpy(), lo=lo, hi=hi)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_stripe_operator_matvec_and_gmres(tmp_path, world):
+    """Symmetric stripes on gloo ranks: the stripe matvec (all-gather + all-reduce) equals A x row by row, and
+    the distributed GMRES reproduces the single-process solve."""
+    import torch.multiprocessing as mp
+
+    n = 61
+    path = str(tmp_path / "stripe%d.npz")
+    mp.spawn(_stripe_worker, args=(world, _free_port(), n, 30, path), nprocs=world, join=True)
+    a, b = _matrix(n)
+    x = np.random.default_rng(3).standard_normal(n) + 0j
+    x_ref = np.linalg.solve(a, b)
+    for r in range(world):
+        o = np.load(path % r)
+        lo, hi = int(o["lo"]), int(o["hi"])
+        np.testing.assert_allclose(o["ax"], (a @ x)[lo:hi], rtol=0, atol=1e-12 * np.abs(a @ x).max())
+        assert int(o["info"]) == 0
+        assert np.linalg.norm(o["x"] - x_ref) <= 1e-10 * np.linalg.norm(x_ref)
+
+
+def test_stripe_bounds_balance_the_upper_triangle():
+    from bempp_cuda.distributed import stripe_bounds
+
+    for n in (1, 5, 97, 32768):
+        for world in (1, 2, 3, 8):
+            b = stripe_bounds(n, world)
+            assert b[0][0] == 0 and b[-1][1] == n and all(b[r][1] == b[r + 1][0] for r in range(world - 1))
+            work = [(h - l) * (n - l) - (h - l) * (h - l - 1) // 2 for l, h in b]
+            if n >= 97:
+                assert max(work) - min(work) <= n + 1  # within one row of the equal share
+
+
+def test_stripe_partial_products_sum_to_the_matrix_product():
+    """Without collectives: the ranks' partial products of the stripes add up to A x."""
+    from bempp_cuda.distributed import StripeOperator
+
+    n = 40
+    a, _ = _matrix(n, seed=9)
+    x = torch.as_tensor(np.random.default_rng(2).standard_normal(n) + 1j * np.random.default_rng(5).standard_normal(n))
+    for world in (1, 2, 4):
+        total = torch.zeros(n, dtype=torch.complex128)
+        for r in range(world):
+            U, L = _stripes(a, world, r)
+            total += StripeOperator(torch.as_tensor(U), torch.as_tensor(L), n, world, r).partial_product(x)
+        assert np.allclose(total.numpy(), a @ x.numpy(), rtol=0, atol=1e-12)
