@@ -274,31 +274,6 @@ struct TestBlock32q {
     int v[DP0_TCHUNK][3];
 };
 
-// exp(i x) for the centroid distance x >= 0 of an element pair (units of 1/k, below 1e6): Cody-Waite
-// reduction by pi/2 in FP64 (two-part constant), then the FP32 minimax polynomials on |a| <= pi/4.
-// The reduced argument keeps its FP64 accuracy until it is rounded to FP32, so the phase is
-// within 1e-7 of exp(i x) for any x in range; the FP32 sums it multiplies carry errors of the
-// same size.
-__device__ __forceinline__ void phase_reduced32(double x, float *s, float *c) {
-    const double magic = 6755399441055744.0;  // 1.5 * 2^52: adding it rounds to an integer
-    const double t = fma(x, 0.6366197723675814, magic);
-    const double n = t - magic;
-    const int q = __double2loint(t);
-    double a = fma(-n, 1.5707963267948966, x);
-    a = fma(-n, 6.123233995736766e-17, a);
-    const float af = (float)a;
-    constexpr float ps[] = BC_SIN_CW32;
-    constexpr float pc[] = BC_COS_CW32;
-    const float a2 = af * af;
-    const float sa = fmaf(af * a2, fmaf(fmaf(ps[0], a2, ps[1]), a2, ps[2]), af);
-    const float ca = fmaf(a2, fmaf(fmaf(fmaf(pc[0], a2, pc[1]), a2, pc[2]), a2, pc[3]), 1.0f);
-    // quadrant q: sin = (s, c, -s, -c), cos = (c, -s, -c, s)
-    const float ss = (q & 1) ? ca : sa;
-    const float cc = (q & 1) ? sa : ca;
-    *s = (q & 2) ? -ss : ss;
-    *c = ((q + 1) & 2) ? -cc : cc;
-}
-
 // sin / cos of the point-pair phase offsets of the symmetric sweep (|x| <= 1/2 for phase class
 // 2, |x| <= 1 for class 1): the sine by the FP32 minimax polynomial, the cosine by the hardware
 // approximation cos.approx.f32 (absolute error below 1e-6 on these ranges; the operator error of

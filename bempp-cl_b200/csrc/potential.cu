@@ -417,15 +417,20 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar(PotParams prm, in
 // Mixed precision (FP32 point-source pairs): Laplace and Helmholtz (real k)
 // single / double layer potentials.  Lengths are in units of 1/kappa
 // (kappa = k, or 1 for Laplace).  Per (evaluation point, source element) in
-// FP64: D = kappa (c_e - x), r_c' = |D| and exp(i r_c'); per source in FP32:
+// FP64: D = kappa c_e - kappa x (one FMA per coordinate, kappa c_e staged),
+// r_c' = |D| (FP32 rsqrt, one FP64 Newton step) and the argument reduction of
+// exp(i r_c'); per source in FP32:
 // yo = kappa (y_q - c_e), |yo|^2 and yo . n_e; per pair in FP32:
 //   r'^2 - r_c'^2 = |yo|^2 + 2 D . yo,  theta = (r'^2 - r_c'^2) / (r' + r_c'),
 // 1/r' by rsqrt.approx, sin / cos of theta by the fitted polynomials (phase
 // class PHC bounds |theta| <= kappa R), and the complex product with the
 // source coefficient; the thread's two evaluation points travel together in
-// packed f32x2 operations.  The six-term sums per element are FP32; exp(i r_c'),
-// kappa (single layer) or kappa^2 (double layer) and the sum over elements are
-// FP64.  Single layer e^{ikr}/r = kappa e^{i theta} e^{i r_c'} / r'; double
+// packed f32x2 operations.  The six-term sums per element, exp(i r_c') (FP32
+// polynomials after the FP64 reduction, phase_reduced32) and their product are
+// FP32; the sum over elements is FP64, in units of kappa (single layer) or
+// kappa^2 (double layer), which multiply once at the end.  B200 runs FP64 at
+// half the FP32 rate, so every FP64 operation per (point, element) costs about
+// as much as the FP32 work of one pair: the FP64 part is kept to ~20 of them.  Single layer e^{ikr}/r = kappa e^{i theta} e^{i r_c'} / r'; double
 // layer (ikr - 1) e^{ikr} (d . n) / r^3 = kappa^2 (i r' - 1) e^{i theta}
 // e^{i r_c'} (d' . n) / r'^3 with d' = D + yo.
 // Near elements: with r_c' >= 4 kappa R (R >= every source's distance from its
@@ -443,7 +448,7 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams p
     static_assert(PS_PPT == 2, "two evaluation points per thread, packed");
     __shared__ float4 syo[PS_SOURCES];  // yo, |yo|^2
     __shared__ float4 scf[PS_SOURCES];  // coefficient re, im, yo . n_e, -im
-    __shared__ double scen[PS_SOURCES * 3];
+    __shared__ double scen[PS_SOURCES * 3];  // kappa c_e
     __shared__ float snrm[DLP ? PS_SOURCES * 3 : 3];
     const int nq = NQ > 0 ? NQ : prm.nq;
     const int tile_elems = PS_SOURCES / nq;
@@ -451,6 +456,8 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams p
     const int64_t eend = min(ebeg + chunk_elems, prm.nsupport);
     const int64_t pbase = (int64_t)blockIdx.x * (PS_THREADS * PS_PPT) + threadIdx.x;
     const double kap = HELM ? prm.p[0] : 1.0;
+    const double sc = HELM ? (DLP ? kap * kap : kap) : 1.0;  // the sums ar, ai are in units of sc
+    const double inv_sc = __drcp_rn(sc);
     double x[PS_PPT][3], ar[PS_PPT], ai[PS_PPT];
 #pragma unroll
     for (int j = 0; j < PS_PPT; ++j) {
@@ -469,7 +476,7 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams p
         for (int e = threadIdx.x; e < te; e += PS_THREADS) {
             const int64_t ge = t0 + e;
 #pragma unroll
-            for (int d = 0; d < 3; ++d) scen[3 * e + d] = o[(8 + d) * n + ge];
+            for (int d = 0; d < 3; ++d) scen[3 * e + d] = kap * o[(8 + d) * n + ge];
             if (DLP)
 #pragma unroll
                 for (int d = 0; d < 3; ++d) snrm[3 * e + d] = (float)o[(3 + d) * n + ge * nq];
@@ -478,8 +485,8 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams p
         for (int s = threadIdx.x; s < ns; s += PS_THREADS) {
             const int64_t gs = s0 + s;
             const int e = s / nq;
-            const float y0 = (float)(kap * (o[gs] - scen[3 * e])), y1 = (float)(kap * (o[n + gs] - scen[3 * e + 1])),
-                        y2 = (float)(kap * (o[2 * n + gs] - scen[3 * e + 2]));
+            const float y0 = (float)fma(kap, o[gs], -scen[3 * e]), y1 = (float)fma(kap, o[n + gs], -scen[3 * e + 1]),
+                        y2 = (float)fma(kap, o[2 * n + gs], -scen[3 * e + 2]);
             syo[s] = make_float4(y0, y1, y2, fmaf(y2, y2, fmaf(y1, y1, y0 * y0)));
             float yn = 0.f;
             if (DLP) yn = fmaf(y2, snrm[3 * e + 2], fmaf(y1, snrm[3 * e + 1], y0 * snrm[3 * e]));
@@ -493,11 +500,15 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams p
             float dd[3][PS_PPT], rc2h[PS_PPT];
 #pragma unroll
             for (int j = 0; j < PS_PPT; ++j) {
-                const double D0 = kap * (scen[3 * e] - x[j][0]), D1 = kap * (scen[3 * e + 1] - x[j][1]),
-                             D2 = kap * (scen[3 * e + 2] - x[j][2]);
+                const double D0 = fma(-kap, x[j][0], scen[3 * e]), D1 = fma(-kap, x[j][1], scen[3 * e + 1]),
+                             D2 = fma(-kap, x[j][2], scen[3 * e + 2]);
                 const double rc2 = fma(D2, D2, fma(D1, D1, D0 * D0));
-                rc[j] = rc2 > 0.0 ? rc2 * rsqrt64(rc2) : 0.0;  // a point may sit on a centroid
                 rc2h[j] = (float)rc2;
+                // r_c' from the FP32 rsqrt and one FP64 Newton step (relative error ~1e-13); the clamp
+                // keeps a point on a centroid (rc2 = 0) at r_c' = 0
+                const double y0 = (double)rsqrt_approx(fmaxf(rc2h[j], 1e-30f));
+                const double r0 = rc2 * y0;
+                rc[j] = fma(r0, 0.5 * fma(-r0, y0, 1.0), r0);
                 dd[0][j] = (float)D0;
                 dd[1][j] = (float)D1;
                 dd[2][j] = (float)D2;
@@ -548,8 +559,18 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams p
                     ei = fma2(vr, ci, fma2(vi, cr, ei));
                 }
             }
-            const double sc = HELM ? (DLP ? kap * kap : kap) : 1.0;
-            const double erj[2] = {(double)er.x, (double)er.y}, eij[2] = {(double)ei.x, (double)ei.y};
+            // times exp(i r_c') in packed FP32 (the phase and the sums carry FP32 errors alike); the
+            // FP64 sums over elements leave out kappa (single layer) or kappa^2 (double layer)
+            float2 pr = er, pi = ei;
+            if (HELM) {
+                float s0f, c0f, s1f, c1f;  // FP64 reduction, FP32 polynomials (phase_reduced32)
+                phase_reduced32(rc[0], &s0f, &c0f);
+                phase_reduced32(rc[1], &s1f, &c1f);
+                const float2 cs = f2(c0f, c1f), sn = f2(s0f, s1f);
+                pr = fma2(cs, er, mul2(sn, mul2(ei, b2(-1.f))));
+                pi = fma2(cs, ei, mul2(sn, er));
+            }
+            const double prj[2] = {(double)pr.x, (double)pr.y}, pij[2] = {(double)pi.x, (double)pi.y};
 #pragma unroll
             for (int j = 0; j < PS_PPT; ++j) {
                 if (rc[j] < near_r) {
@@ -583,16 +604,11 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams p
                             ni = fma(cs, wi, fma(sn, wr, ni));
                         }
                     }
-                    ar[j] += nr;
-                    ai[j] += ni;
-                } else if (HELM) {
-                    double sn, cs;
-                    sincos_cw64(rc[j], &sn, &cs);
-                    ar[j] = fma(sc, cs * erj[j] - sn * eij[j], ar[j]);
-                    ai[j] = fma(sc, fma(cs, eij[j], sn * erj[j]), ai[j]);
+                    ar[j] = fma(nr, inv_sc, ar[j]);
+                    ai[j] = fma(ni, inv_sc, ai[j]);
                 } else {
-                    ar[j] += erj[j];
-                    ai[j] += eij[j];
+                    ar[j] += prj[j];
+                    ai[j] += pij[j];
                 }
             }
         }
@@ -602,12 +618,13 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams p
         const int64_t pj = pbase + j * PS_THREADS;
         if (pj >= prm.npoints) break;
         double *out = prm.result + 2 * pj;
+        const double scale = BC_INV_4PI * sc;
         if (gridDim.y == 1) {
-            out[0] = BC_INV_4PI * ar[j];
-            out[1] = BC_INV_4PI * ai[j];
+            out[0] = scale * ar[j];
+            out[1] = scale * ai[j];
         } else {
-            atomicAdd(out, BC_INV_4PI * ar[j]);
-            atomicAdd(out + 1, BC_INV_4PI * ai[j]);
+            atomicAdd(out, scale * ar[j]);
+            atomicAdd(out + 1, scale * ai[j]);
         }
     }
 }
