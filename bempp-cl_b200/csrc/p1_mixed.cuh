@@ -33,10 +33,16 @@
 // (1 = phi_0 + phi_1 + phi_2, xi = phi_1, eta = phi_2), so the FP32 part is
 // the single layer's and the FP64 epilogue forms the moments and
 // efie_block; the integration elements cancel against the RWG basis.
+// Scatter: the FP64 block entries of a warp's 32 pairs (one test element,
+// 32 consecutive trial elements) are summed per distinct trial dof in shared
+// memory and added to the matrix once per (test dof, trial dof)
+// (warp_cols.cuh): ~3.5x fewer FP64 L2 atomics, which bound the double-layer
+// sweep (each pair adds two blocks).
 #pragma once
 
 #include "p1.cuh"
 #include "rwg.cuh"
+#include "warp_cols.cuh"
 
 namespace bc {
 
@@ -44,7 +50,6 @@ struct TestBlockP1m {
     float4 m[P1_TCHUNK][NQ6];  // (-2 xo, |xo|^2), xo = k (x_p - c_t)
     double c[P1_TCHUNK][3];
     double n[P1_TCHUNK][3];
-    double curl[P1_TCHUNK][3][3];
     double ie[P1_TCHUNK];
     double mult[P1_TCHUNK][3];
     int64_t row[P1_TCHUNK][3];
@@ -62,6 +67,11 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
     constexpr bool NT_SUM = AD || SKEW;  // sums with -d'.n_t per pair
     constexpr int NP = NQ6 / 2;
     __shared__ TestBlockP1m sb;
+    __shared__ double scurl[HYP || EFIE ? P1_TCHUNK : 1][3][3];  // curls (HYP) or J_t (EFIE)
+    __shared__ WarpColumns swc[DP0_THREADS / 32];
+    // staged block entries per warp: [block row][staging position]; SKEW: the (j, i) blocks too
+    __shared__ double2 sst[DP0_THREADS / 32][3][WC_SLOTS];
+    __shared__ double2 sst_t[SKEW ? DP0_THREADS / 32 : 1][3][SKEW ? WC_SLOTS : 1];
     const double kap = prm.p[0];
 
     const int64_t t0 = (int64_t)blockIdx.y * P1_TCHUNK;
@@ -95,8 +105,8 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
         if (EFIE) {
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
-                sb.curl[idx][0][d] = g.j0[d];
-                sb.curl[idx][1][d] = g.j1[d];
+                scurl[idx][0][d] = g.j0[d];
+                scurl[idx][1][d] = g.j1[d];
             }
         }
         if (HYP) {
@@ -105,15 +115,16 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
 #pragma unroll
             for (int i = 0; i < 3; ++i)
 #pragma unroll
-                for (int d = 0; d < 3; ++d) sb.curl[idx][i][d] = cu[i][d];
+                for (int d = 0; d < 3; ++d) scurl[idx][i][d] = cu[i][d];
         }
         sb.ie[idx] = g.ie;
     }
     __syncthreads();
 
     const int64_t si = (int64_t)blockIdx.x * DP0_THREADS + threadIdx.x;
-    if (si >= prm.ntrial) return;
-    const int64_t s = prm.ssup[si];
+    const bool active = si < prm.ntrial;  // lanes past the last trial element stage nothing
+    if (__all_sync(0xffffffffu, !active)) return;
+    const int64_t s = prm.ssup[active ? si : prm.ntrial - 1];
     Geom gs;
     load_geom(prm.sg, prm.sne, s, prm.snm ? (double)prm.snm[s] : 1.0, gs);
     const int sv0 = __ldg(prm.sel + 3 * s), sv1 = __ldg(prm.sel + 3 * s + 1), sv2 = __ldg(prm.sel + 3 * s + 2);
@@ -147,10 +158,34 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
         scol[j] = prm.sl2g[s * 3 + j];
         smul[j] = prm.smult[s * 3 + j] * (EFIE ? edge_length(prm.sg, prm.sne, s, j) : 1.0);
     }
+    // the warp's columns (distinct trial dofs) and this lane's staging positions
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    WarpColumns &wc = swc[warp];
+    int pos[3];
+    {
+        int dof[3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) dof[j] = active && scol[j] >= 0 && scol[j] < INT32_MAX ? (int)scol[j] : -1;
+        static_assert(sizeof(sst[0]) >= 2 * WC_TABLE * sizeof(int), "column table scratch");
+        wc_build(wc, reinterpret_cast<int *>(&sst[warp][0][0]), dof, pos);
+    }
+    double2(&st)[3][WC_SLOTS] = sst[warp];
+    double2(&st_t)[3][SKEW ? WC_SLOTS : 1] = sst_t[SKEW ? warp : 0];
 
     for (int tt = 0; tt < tcount; ++tt) {
-        if (SYM && t0 + tt >= si) break;  // rows increase with tt
-        if (prm.grids_identical && shares_vertex(sb.v[tt], sv0, sv1, sv2)) continue;
+        const bool done = !active || (SYM && t0 + tt >= si);  // rows increase with tt
+        if (__all_sync(0xffffffffu, done)) break;
+        if (done || (prm.grids_identical && shares_vertex(sb.v[tt], sv0, sv1, sv2))) {
+            // no pair: zeros in this lane's staging positions
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+                    if (pos[j] >= 0) {
+                        st[i][pos[j]] = make_double2(0.0, 0.0);
+                        if (SKEW) st_t[i][pos[j]] = make_double2(0.0, 0.0);
+                    }
+        } else {
         const double D0 = kap * (sc[0] - sb.c[tt][0]), D1 = kap * (sc[1] - sb.c[tt][1]),
                      D2 = kap * (sc[2] - sb.c[tt][2]);
         const double rc2 = fma(D2, D2, fma(D1, D1, D0 * D0));
@@ -277,7 +312,7 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
                     mim[a][b] = kap * (double)lim[a][b];
                 }
             }
-            efie_block<false>(mre, mim, sb.curl[tt][0], sb.curl[tt][1], gs.j0, gs.j1, kap, 0.0, ere, eim);
+            efie_block<false>(mre, mim, scurl[tt][0], scurl[tt][1], gs.j0, gs.j1, kap, 0.0, ere, eim);
         }
         const double scale = EFIE ? BC_INV_4PI : (DL || AD ? kap * kap : kap) * BC_INV_4PI * sb.ie[tt] * gs.ie;
         double sre = 0.0, sim = 0.0, cpf = 0.0;
@@ -295,16 +330,19 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
             const double mt = sb.mult[tt][i];
-            if (mt == 0.0) continue;
-            const int64_t row = sb.row[tt][i];
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
                 const double ms = smul[j];
-                if (ms == 0.0) continue;
+                if (pos[j] < 0) continue;
+                if (mt == 0.0 || ms == 0.0) {
+                    st[i][pos[j]] = make_double2(0.0, 0.0);
+                    if (SKEW) st_t[i][pos[j]] = make_double2(0.0, 0.0);
+                    continue;
+                }
                 double vr = EFIE ? ere[i][j] : (double)lre[i][j], vi = EFIE ? eim[i][j] : (double)lim[i][j];
                 if (HYP) {
-                    const double cij = sb.curl[tt][i][0] * curl_s[j][0] + sb.curl[tt][i][1] * curl_s[j][1] +
-                                       sb.curl[tt][i][2] * curl_s[j][2];
+                    const double cij = scurl[tt][i][0] * curl_s[j][0] + scurl[tt][i][1] * curl_s[j][1] +
+                                       scurl[tt][i][2] * curl_s[j][2];
                     vr = fma(cij, sre, cpf * vr);
                     vi = fma(cij, sim, cpf * vi);
                 }
@@ -318,17 +356,51 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
                     wi = fma(ur, ph_s, ui * ph_c);
                 }
                 const double mm = mt * ms * scale;
-                const int64_t col = scol[j];
-                double *o = reinterpret_cast<double *>(prm.result) + 2 * (row * prm.ld + col);
-                atomicAdd(o, vr * mm);
-                atomicAdd(o + 1, vi * mm);
-                if (SYM && (SKEW || !prm.defer_transpose)) {
-                    double *ot = reinterpret_cast<double *>(prm.result) + 2 * (col * prm.ld + row);
-                    atomicAdd(ot, wr * mm);
-                    atomicAdd(ot + 1, wi * mm);
+                st[i][pos[j]] = make_double2(vr * mm, vi * mm);
+                if (SKEW) st_t[i][pos[j]] = make_double2(wr * mm, wi * mm);
+            }
+        }
+        }  // pair
+        __syncwarp();
+        // per (test dof, column): the sum of the column's staged entries, one complex atomic
+        // (and, for the symmetric sweep, one at the transposed position)
+        const int ncols = wc.ncols;
+        double *res = reinterpret_cast<double *>(prm.result);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const int64_t row = sb.row[tt][i];
+            for (int c = (int)lane; c < ncols; c += 32) {
+                const int b = wc.start[c], e = wc.start[c + 1];
+                double ar = 0.0, ai = 0.0, br = 0.0, bi = 0.0;
+                for (int k = b; k < e; ++k) {
+                    const double2 v = st[i][k];
+                    ar += v.x;
+                    ai += v.y;
+                    if (SKEW) {
+                        const double2 w = st_t[i][k];
+                        br += w.x;
+                        bi += w.y;
+                    }
+                }
+                const int64_t col = wc.col[c];
+                if (ar != 0.0 || ai != 0.0) {
+                    double *o = res + 2 * (row * prm.ld + col);
+                    atomicAdd(o, ar);
+                    atomicAdd(o + 1, ai);
+                    if (SYM && !SKEW && !prm.defer_transpose) {
+                        double *ot = res + 2 * (col * prm.ld + row);
+                        atomicAdd(ot, ar);
+                        atomicAdd(ot + 1, ai);
+                    }
+                }
+                if (SKEW && (br != 0.0 || bi != 0.0)) {
+                    double *ot = res + 2 * (col * prm.ld + row);
+                    atomicAdd(ot, br);
+                    atomicAdd(ot + 1, bi);
                 }
             }
         }
+        __syncwarp();  // the staging arrays are rewritten by the next test element
     }
 }
 
