@@ -1,7 +1,8 @@
-// Mixed-precision regular pairs of the Helmholtz single layer, double layer,
-// adjoint double layer and hypersingular operators on P1 spaces (6-point
-// rule, real k > 0): the FP32 counterpart of regular_p1 (p1.cuh) with the
-// geometry of the mixed DP0 kernels (dp0.cuh).
+// Mixed-precision regular pairs of the single layer, double layer, adjoint
+// double layer and hypersingular operators on P1 spaces (6-point rule) for the
+// Helmholtz (Re k > 0, real or complex k), Laplace and modified Helmholtz
+// kernels: the FP32 counterpart of regular_p1 (p1.cuh) with the geometry of
+// the mixed DP0 kernels (dp0.cuh).
 //
 // Lengths are in units of 1/k.  Per element pair the centroid offset
 // D = k (c_s - c_t), r_c' = |D| and exp(i r_c') are FP64; per point pair only
@@ -27,6 +28,15 @@
 // (i, j) and, unless deferred to the transpose pass, at (j, i); the double
 // layers add at (j, i) the transposed pair's own block, which is the other
 // operator's kernel of (i, j) (skew sweep: both normal sums per pair).
+// Other kernels, in units of 1/kappa (kappa = Re k, omega, or 1 for Laplace):
+// Laplace has no phase (1/r', -1/r'^3 in the double layers); modified
+// Helmholtz exp(-r') = exp(-r_c') exp(-theta), the first FP64 per element
+// pair, the second __expf per point pair, double-layer factor -(1 + r'); a
+// complex wavenumber k = kr + i ki adds exp(-beta r'), beta = ki / kr, split
+// the same way beside exp(i r'), the double-layer factor
+// (i k r - 1) = -(1 + beta r') + i r', and -k^2 complex in the hypersingular
+// operator.  Laplace and modified Helmholtz blocks are real and go to a real
+// matrix.
 // Maxwell electric field on RWG / SNC (ASM_EFIE): the nine moments
 // M[u][v] = sum_pq w_p w_q G u(p) v(q), u, v in {1, xi, eta}, that the EFIE
 // block needs (rwg.cuh) are a fixed linear map of the P1 single-layer block
@@ -56,12 +66,17 @@ struct TestBlockP1m {
     int v[P1_TCHUNK][3];
 };
 
-template <int ASM, int K, int PHC, bool SYM>
+template <int ASM, int K, int PHC, bool SYM, bool CK = false>
 __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, QuadRule rule) {
-    constexpr bool HYP = ASM == BEMPPCUDA_ASM_HELM_HYP;
+    constexpr bool LAP = K == BEMPPCUDA_LAPLACE_SLP || K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_LAPLACE_ADLP;
+    constexpr bool MH = K == BEMPPCUDA_MODHELM_SLP || K == BEMPPCUDA_MODHELM_DLP || K == BEMPPCUDA_MODHELM_ADLP;
+    constexpr bool REAL = LAP || MH;  // real kernel, real result
+    constexpr bool HYP = ASM == BEMPPCUDA_ASM_HELM_HYP || ASM == BEMPPCUDA_ASM_LAPLACE_HYP ||
+                         ASM == BEMPPCUDA_ASM_MODHELM_HYP;
     constexpr bool EFIE = ASM == BEMPPCUDA_ASM_EFIE;  // test curl slots hold J_t, multipliers edge lengths
-    constexpr bool DL = K == BEMPPCUDA_HELMHOLTZ_DLP;
-    constexpr bool AD = K == BEMPPCUDA_HELMHOLTZ_ADLP;
+    constexpr bool DL = K == BEMPPCUDA_HELMHOLTZ_DLP || K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_MODHELM_DLP;
+    constexpr bool AD = K == BEMPPCUDA_HELMHOLTZ_ADLP || K == BEMPPCUDA_LAPLACE_ADLP || K == BEMPPCUDA_MODHELM_ADLP;
+    static_assert(!CK || (!REAL && !EFIE), "complex wavenumber: the Helmholtz scalar operators");
     constexpr bool SKEW = SYM && (DL || AD);
     constexpr bool NS_SUM = DL || SKEW;  // sums multiplied by d'.n_s per test point
     constexpr bool NT_SUM = AD || SKEW;  // sums with -d'.n_t per pair
@@ -72,7 +87,11 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
     // staged block entries per warp: [block row][staging position]; SKEW: the (j, i) blocks too
     __shared__ double2 sst[DP0_THREADS / 32][3][WC_SLOTS];
     __shared__ double2 sst_t[SKEW ? DP0_THREADS / 32 : 1][3][SKEW ? WC_SLOTS : 1];
-    const double kap = prm.p[0];
+    // units of 1/kappa: kappa = k (Helmholtz; Re k for a complex wavenumber), omega (modified), 1 (Laplace)
+    const double kap = LAP ? 1.0 : prm.p[0];
+    // exp(-beta r') beside exp(i r'): beta = Im k / Re k (complex k), 1 (modified: exp(-r') alone)
+    const double betd = CK ? prm.p[1] / prm.p[0] : (MH ? 1.0 : 0.0);
+    const float bet = (float)betd;
 
     const int64_t t0 = (int64_t)blockIdx.y * P1_TCHUNK;
     if (SYM && t0 >= ((int64_t)blockIdx.x + 1) * DP0_THREADS) return;  // below the diagonal
@@ -190,8 +209,16 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
                      D2 = kap * (sc[2] - sb.c[tt][2]);
         const double rc2 = fma(D2, D2, fma(D1, D1, D0 * D0));
         const double rc = sqrt(rc2);
-        double ph_s, ph_c;
-        sincos_cw64(rc, &ph_s, &ph_c);
+        // the element pair's factor: exp(i r_c'), times exp(-beta r_c') (complex k); exp(-r_c') (modified)
+        double ph_s = 0.0, ph_c = 1.0;
+        if (!LAP) {
+            if (!MH) sincos_cw64(rc, &ph_s, &ph_c);
+            if (MH || CK) {
+                const double am = exp(-betd * rc);
+                ph_c *= am;
+                ph_s *= am;
+            }
+        }
         const float D0f = (float)D0, D1f = (float)D1, D2f = (float)D2;
         const float2 rcf2 = b2((float)rc), rc2f2 = b2((float)rc2);
         const float2 D0d = b2(2.f * D0f), D1d = b2(2.f * D1f), D2d = b2(2.f * D2f);
@@ -228,31 +255,51 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
                 const float2 sdot = fma2(yz[jj], mz, fma2(yyy[jj], my, fma2(yx[jj], mx, add2(A[jj], Bp2))));
                 const float2 r2 = add2(rc2f2, sdot);
                 const float2 rinv = f2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
-                const float2 den = fma2(r2, rinv, rcf2);
-                const float2 th = mul2(sdot, f2(rcp_approx(den.x), rcp_approx(den.y)));
-                float2 sn, cs;
-                sincos2<PHC>(th, &sn, &cs);
-                float2 kr, ki;
+                // cs + i sn: exp(i theta) (Helmholtz), times exp(-beta theta) (complex k); exp(-theta)
+                // (modified, sn = 0); 1 (Laplace)
+                float2 sn = b2(0.f), cs = b2(1.f);
+                if (!LAP) {
+                    const float2 den = fma2(r2, rinv, rcf2);
+                    const float2 th = mul2(sdot, f2(rcp_approx(den.x), rcp_approx(den.y)));
+                    if (!MH) sincos2<PHC>(th, &sn, &cs);
+                    if (MH || CK) {
+                        const float2 am = f2(__expf(-bet * th.x), __expf(-bet * th.y));
+                        cs = mul2(cs, am);
+                        if (CK) sn = mul2(sn, am);
+                    }
+                }
+                float2 kr, ki = b2(0.f);
                 if (!DL && !AD) {
                     kr = mul2(rinv, cs);
-                    ki = mul2(rinv, sn);
+                    if (!REAL) ki = mul2(rinv, sn);
+                } else if (LAP) {
+                    kr = mul2(rinv, mul2(rinv, mul2(rinv, b2(-1.f))));  // -1 / r'^3
                 } else {
-                    // h = (i r' - 1) e^{i theta} / r'^3 = ((-cs - r' sn) + i (r' cs - sn)) / r'^3
+                    // h = (i k r - 1) e^{ikr} / r^3 in units of 1/kappa: ((-a cs - r' sn) + i (r' cs - a sn)) / r'^3,
+                    // a = 1 + beta r' (a = 1 for real k); modified: -(1 + r') e^{-r'} / r'^3
                     const float2 rp = mul2(r2, rinv), r3 = mul2(rinv, mul2(rinv, rinv));
-                    kr = mul2(r3, mul2(fma2(rp, sn, cs), b2(-1.f)));
-                    ki = mul2(r3, fma2(rp, cs, mul2(sn, b2(-1.f))));
+                    if (MH) {
+                        kr = mul2(mul2(r3, cs), mul2(add2(rp, b2(1.f)), b2(-1.f)));
+                    } else if (CK) {
+                        const float2 a = fma2(b2(bet), rp, b2(1.f));
+                        kr = mul2(r3, mul2(fma2(rp, sn, mul2(a, cs)), b2(-1.f)));
+                        ki = mul2(r3, fma2(rp, cs, mul2(mul2(a, sn), b2(-1.f))));
+                    } else {
+                        kr = mul2(r3, mul2(fma2(rp, sn, cs), b2(-1.f)));
+                        ki = mul2(r3, fma2(rp, cs, mul2(sn, b2(-1.f))));
+                    }
                 }
 #pragma unroll
                 for (int j = 0; j < 3; ++j) {
                     const float2 w = f2(rule.swf[2 * jj][j], rule.swf[2 * jj + 1][j]);
                     if (!AD || SKEW) {  // plain sums (single layer; double layer: times d'.n_s below)
                         tre[j] = fma2(kr, w, tre[j]);
-                        tim[j] = fma2(ki, w, tim[j]);
+                        if (!REAL) tim[j] = fma2(ki, w, tim[j]);
                     }
                     if (NT_SUM) {  // sums with -(d'.n_t)
                         const float2 wd = mul2(w, mdt[jj]);
                         vre[j] = fma2(kr, wd, vre[j]);
-                        vim[j] = fma2(ki, wd, vim[j]);
+                        if (!REAL) vim[j] = fma2(ki, wd, vim[j]);
                     }
                 }
             }
@@ -264,18 +311,18 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
                 for (int j = 0; j < 3; ++j) {
                     if (!DL && !AD) {
                         lre[i][j] = fmaf(ph, tre[j].x + tre[j].y, lre[i][j]);
-                        lim[i][j] = fmaf(ph, tim[j].x + tim[j].y, lim[i][j]);
+                        if (!REAL) lim[i][j] = fmaf(ph, tim[j].x + tim[j].y, lim[i][j]);
                     } else {
                         // (i, j): double layer -> n_s sums, adjoint -> n_t sums; SKEW: the other one at (j, i)
                         const float2 first_r = DL ? tre[j] : vre[j], first_i = DL ? tim[j] : vim[j];
                         const float f1 = DL ? phs : ph;
                         lre[i][j] = fmaf(f1, first_r.x + first_r.y, lre[i][j]);
-                        lim[i][j] = fmaf(f1, first_i.x + first_i.y, lim[i][j]);
+                        if (!REAL) lim[i][j] = fmaf(f1, first_i.x + first_i.y, lim[i][j]);
                         if (SKEW) {
                             const float2 sec_r = DL ? vre[j] : tre[j], sec_i = DL ? vim[j] : tim[j];
                             const float f2_ = DL ? ph : phs;
                             ure[i][j] = fmaf(f2_, sec_r.x + sec_r.y, ure[i][j]);
-                            uim[i][j] = fmaf(f2_, sec_i.x + sec_i.y, uim[i][j]);
+                            if (!REAL) uim[i][j] = fmaf(f2_, sec_i.x + sec_i.y, uim[i][j]);
                         }
                     }
                 }
@@ -315,7 +362,7 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
             efie_block<false>(mre, mim, scurl[tt][0], scurl[tt][1], gs.j0, gs.j1, kap, 0.0, ere, eim);
         }
         const double scale = EFIE ? BC_INV_4PI : (DL || AD ? kap * kap : kap) * BC_INV_4PI * sb.ie[tt] * gs.ie;
-        double sre = 0.0, sim = 0.0, cpf = 0.0;
+        double sre = 0.0, sim = 0.0, cpf = 0.0, cpi = 0.0;
         if (HYP) {
             // S = sum_pq w_p w_q G: the P1 functions add up to 1 on each side
 #pragma unroll
@@ -325,7 +372,15 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
                     sre += (double)lre[i][j];
                     sim += (double)lim[i][j];
                 }
-            cpf = -kap * kap * (sb.n[tt][0] * gs.n[0] + sb.n[tt][1] * gs.n[1] + sb.n[tt][2] * gs.n[2]);
+            // -k^2 (n_t . n_s), complex for a complex wavenumber; +w^2 (n_t . n_s) modified; 0 Laplace
+            const double nn = sb.n[tt][0] * gs.n[0] + sb.n[tt][1] * gs.n[1] + sb.n[tt][2] * gs.n[2];
+            if (MH) {
+                cpf = kap * kap * nn;
+            } else if (!LAP) {
+                const double ki = CK ? prm.p[1] : 0.0;
+                cpf = -(kap * kap - ki * ki) * nn;
+                cpi = -2.0 * kap * ki * nn;
+            }
         }
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
@@ -343,8 +398,9 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
                 if (HYP) {
                     const double cij = scurl[tt][i][0] * curl_s[j][0] + scurl[tt][i][1] * curl_s[j][1] +
                                        scurl[tt][i][2] * curl_s[j][2];
-                    vr = fma(cij, sre, cpf * vr);
-                    vi = fma(cij, sim, cpf * vi);
+                    const double lr = vr, li = vi;
+                    vr = fma(cij, sre, fma(cpf, lr, -cpi * li));
+                    vi = fma(cij, sim, fma(cpf, li, cpi * lr));
                 }
                 const double tr = vr * ph_c - vi * ph_s;
                 vi = fma(vr, ph_s, vi * ph_c);
@@ -366,6 +422,15 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
         // (and, for the symmetric sweep, one at the transposed position)
         const int ncols = wc.ncols;
         double *res = reinterpret_cast<double *>(prm.result);
+        // one entry into the matrix: complex (two atomics) or, for the real kernels, real
+        const auto add_entry = [](double *m, int64_t ld, int64_t r, int64_t c, double re, double im) {
+            if (REAL) {
+                atomicAdd(m + r * ld + c, re);
+            } else {
+                atomicAdd(m + 2 * (r * ld + c), re);
+                atomicAdd(m + 2 * (r * ld + c) + 1, im);
+            }
+        };
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
             const int64_t row = sb.row[tt][i];
@@ -384,20 +449,10 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
                 }
                 const int64_t col = wc.col[c];
                 if (ar != 0.0 || ai != 0.0) {
-                    double *o = res + 2 * (row * prm.ld + col);
-                    atomicAdd(o, ar);
-                    atomicAdd(o + 1, ai);
-                    if (SYM && !SKEW && !prm.defer_transpose) {
-                        double *ot = res + 2 * (col * prm.ld + row);
-                        atomicAdd(ot, ar);
-                        atomicAdd(ot + 1, ai);
-                    }
+                    add_entry(res, prm.ld, row, col, ar, ai);
+                    if (SYM && !SKEW && !prm.defer_transpose) add_entry(res, prm.ld, col, row, ar, ai);
                 }
-                if (SKEW && (br != 0.0 || bi != 0.0)) {
-                    double *ot = res + 2 * (col * prm.ld + row);
-                    atomicAdd(ot, br);
-                    atomicAdd(ot + 1, bi);
-                }
+                if (SKEW && (br != 0.0 || bi != 0.0)) add_entry(res, prm.ld, col, row, br, bi);
             }
         }
         __syncwarp();  // the staging arrays are rewritten by the next test element

@@ -468,26 +468,41 @@ static cudaError_t launch_add_transpose(void *a, int64_t n, int64_t ld, bool is_
     return cudaGetLastError();
 }
 
-// Mixed-precision Helmholtz single layer, double layers and hypersingular on P1 spaces (p1_mixed.cuh).
+// Mixed-precision single layer, double layers and hypersingular on P1 spaces (p1_mixed.cuh): Helmholtz
+// (phase classes, real or complex k), Laplace and modified Helmholtz (no phase classes).
+template <int ASM, int K, bool SYM, bool CK>
+static void p1_mixed_phase(const RegParams &prm, const QuadRule &rule, int phase_class, dim3 grid, cudaStream_t st) {
+    if constexpr (K != BEMPPCUDA_HELMHOLTZ_SLP && K != BEMPPCUDA_HELMHOLTZ_DLP && K != BEMPPCUDA_HELMHOLTZ_ADLP) {
+        regular_p1_mixed<ASM, K, 0, SYM, false><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+    } else {
+        if (phase_class == 2)
+            regular_p1_mixed<ASM, K, 2, SYM, CK><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+        else if (phase_class == 1)
+            regular_p1_mixed<ASM, K, 1, SYM, CK><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+        else
+            regular_p1_mixed<ASM, K, 0, SYM, CK><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+    }
+}
+
 template <int ASM, int K>
 static cudaError_t launch_p1_mixed(const RegParams &prm, const QuadRule &rule, int phase_class, bool sym,
                                    cudaStream_t st) {
     dim3 grid((unsigned)((prm.ntrial + DP0_THREADS - 1) / DP0_THREADS),
               (unsigned)((prm.ntest + P1_TCHUNK - 1) / P1_TCHUNK));
-    if (sym) {
-        if (phase_class == 2)
-            regular_p1_mixed<ASM, K, 2, true><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
-        else if (phase_class == 1)
-            regular_p1_mixed<ASM, K, 1, true><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
-        else
-            regular_p1_mixed<ASM, K, 0, true><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+    constexpr bool helm = (K == BEMPPCUDA_HELMHOLTZ_SLP || K == BEMPPCUDA_HELMHOLTZ_DLP ||
+                           K == BEMPPCUDA_HELMHOLTZ_ADLP) && ASM != BEMPPCUDA_ASM_EFIE;
+    const bool ck = helm && prm.p[1] != 0.0;
+    if (ck) {
+        if constexpr (helm) {
+            if (sym)
+                p1_mixed_phase<ASM, K, true, true>(prm, rule, phase_class, grid, st);
+            else
+                p1_mixed_phase<ASM, K, false, true>(prm, rule, phase_class, grid, st);
+        }
+    } else if (sym) {
+        p1_mixed_phase<ASM, K, true, false>(prm, rule, phase_class, grid, st);
     } else {
-        if (phase_class == 2)
-            regular_p1_mixed<ASM, K, 2, false><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
-        else if (phase_class == 1)
-            regular_p1_mixed<ASM, K, 1, false><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
-        else
-            regular_p1_mixed<ASM, K, 0, false><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+        p1_mixed_phase<ASM, K, false, false>(prm, rule, phase_class, grid, st);
     }
     return cudaGetLastError();
 }
@@ -575,24 +590,32 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
         bc_set_error("overwrite mode needs the DP0 fast path (DP0 spaces, identity dofs, 6-point rule)");
         return BEMPPCUDA_ERR_INVALID;
     }
-    // mixed precision: DP0 scalar kernels, and the Helmholtz single / double / adjoint double layer and
-    // hypersingular operators on P1 spaces (6-point rule, real k > 0)
+    // mixed precision: DP0 scalar kernels, and the single / double / adjoint double layer and
+    // hypersingular operators on P1 spaces (6-point rule): Helmholtz with Re k > 0 (complex result),
+    // Laplace and modified Helmholtz with w > 0 (real result)
+    const bool helm_k = a->kernel == BEMPPCUDA_HELMHOLTZ_SLP || a->kernel == BEMPPCUDA_HELMHOLTZ_DLP ||
+                        a->kernel == BEMPPCUDA_HELMHOLTZ_ADLP;
+    const bool lap_k = a->kernel <= BEMPPCUDA_LAPLACE_ADLP;
+    const bool mh_k = a->kernel >= BEMPPCUDA_MODHELM_SLP && a->kernel <= BEMPPCUDA_MODHELM_ADLP;
+    const bool p1_family =
+        (a->assembly == BEMPPCUDA_ASM_SCALAR && (helm_k || lap_k || mh_k)) ||
+        (a->assembly == BEMPPCUDA_ASM_HELM_HYP && a->kernel == BEMPPCUDA_HELMHOLTZ_SLP) ||
+        (a->assembly == BEMPPCUDA_ASM_LAPLACE_HYP && a->kernel == BEMPPCUDA_LAPLACE_SLP) ||
+        (a->assembly == BEMPPCUDA_ASM_MODHELM_HYP && a->kernel == BEMPPCUDA_MODHELM_SLP);
+    const bool p1_params = (helm_k && a->params[0] > 0.0 && a->is_complex) ||
+                           (lap_k && !a->is_complex) || (mh_k && a->params[0] > 0.0 && !a->is_complex);
     const bool p1_mixed = a->nq == NQ6 && !a->overwrite && a->test.nshape == 3 && a->trial.nshape == 3 &&
                           a->test.shapeset == BEMPPCUDA_SHAPE_P1 && a->trial.shapeset == BEMPPCUDA_SHAPE_P1 &&
-                          a->params[1] == 0.0 && a->params[0] > 0.0 &&
-                          ((a->assembly == BEMPPCUDA_ASM_HELM_HYP && a->kernel == BEMPPCUDA_HELMHOLTZ_SLP) ||
-                           (a->assembly == BEMPPCUDA_ASM_SCALAR && (a->kernel == BEMPPCUDA_HELMHOLTZ_SLP ||
-                                                                    a->kernel == BEMPPCUDA_HELMHOLTZ_DLP ||
-                                                                    a->kernel == BEMPPCUDA_HELMHOLTZ_ADLP)));
+                          p1_family && p1_params;
     // ... and the Maxwell electric field on RWG / SNC (same FP32 core; 6-point rule, real k > 0)
     const bool rwg_mixed = a->nq == NQ6 && !a->overwrite && a->assembly == BEMPPCUDA_ASM_EFIE &&
                            a->kernel == BEMPPCUDA_HELMHOLTZ_SLP && a->params[1] == 0.0 && a->params[0] > 0.0 &&
                            a->test.shapeset == BEMPPCUDA_SHAPE_RWG && a->trial.shapeset == BEMPPCUDA_SHAPE_RWG &&
                            a->test.nshape == 3 && a->trial.nshape == 3;
     if (a->precision == BEMPPCUDA_MIXED && !dp0 && !p1_mixed && !rwg_mixed) {
-        bc_set_error("mixed precision is implemented for DP0 scalar kernels, the P1 Helmholtz single, double, "
-                     "adjoint double layer and hypersingular operators and the Maxwell electric field, with the "
-                     "6-point rule and a real wavenumber");
+        bc_set_error("mixed precision is implemented for DP0 scalar kernels, the P1 single, double, adjoint "
+                     "double layer and hypersingular operators (Helmholtz with Re k > 0, Laplace, modified "
+                     "Helmholtz) and the Maxwell electric field (real k), with the 6-point rule");
         return BEMPPCUDA_ERR_UNSUPPORTED;
     }
     cudaError_t err = cudaSuccess;
@@ -693,6 +716,22 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
         if (mixed && p1_mixed) {
             if (a->assembly == BEMPPCUDA_ASM_HELM_HYP)
                 err = launch_p1_mixed<BEMPPCUDA_ASM_HELM_HYP, BEMPPCUDA_HELMHOLTZ_SLP>(prm, rule, phase_class, psym, st);
+            else if (a->assembly == BEMPPCUDA_ASM_LAPLACE_HYP)
+                err = launch_p1_mixed<BEMPPCUDA_ASM_LAPLACE_HYP, BEMPPCUDA_LAPLACE_SLP>(prm, rule, 0, psym, st);
+            else if (a->assembly == BEMPPCUDA_ASM_MODHELM_HYP)
+                err = launch_p1_mixed<BEMPPCUDA_ASM_MODHELM_HYP, BEMPPCUDA_MODHELM_SLP>(prm, rule, 0, psym, st);
+            else if (a->kernel == BEMPPCUDA_LAPLACE_SLP)
+                err = launch_p1_mixed<BEMPPCUDA_ASM_SCALAR, BEMPPCUDA_LAPLACE_SLP>(prm, rule, 0, psym, st);
+            else if (a->kernel == BEMPPCUDA_LAPLACE_DLP)
+                err = launch_p1_mixed<BEMPPCUDA_ASM_SCALAR, BEMPPCUDA_LAPLACE_DLP>(prm, rule, 0, psym, st);
+            else if (a->kernel == BEMPPCUDA_LAPLACE_ADLP)
+                err = launch_p1_mixed<BEMPPCUDA_ASM_SCALAR, BEMPPCUDA_LAPLACE_ADLP>(prm, rule, 0, psym, st);
+            else if (a->kernel == BEMPPCUDA_MODHELM_SLP)
+                err = launch_p1_mixed<BEMPPCUDA_ASM_SCALAR, BEMPPCUDA_MODHELM_SLP>(prm, rule, 0, psym, st);
+            else if (a->kernel == BEMPPCUDA_MODHELM_DLP)
+                err = launch_p1_mixed<BEMPPCUDA_ASM_SCALAR, BEMPPCUDA_MODHELM_DLP>(prm, rule, 0, psym, st);
+            else if (a->kernel == BEMPPCUDA_MODHELM_ADLP)
+                err = launch_p1_mixed<BEMPPCUDA_ASM_SCALAR, BEMPPCUDA_MODHELM_ADLP>(prm, rule, 0, psym, st);
             else if (a->kernel == BEMPPCUDA_HELMHOLTZ_DLP)
                 err = launch_p1_mixed<BEMPPCUDA_ASM_SCALAR, BEMPPCUDA_HELMHOLTZ_DLP>(prm, rule, phase_class, psym, st);
             else if (a->kernel == BEMPPCUDA_HELMHOLTZ_ADLP)

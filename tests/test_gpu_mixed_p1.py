@@ -1,11 +1,12 @@
 """Mixed precision on P1 spaces (run on a B200).
 
-The Helmholtz single layer, double layer, adjoint double layer and
-hypersingular operators on P1 evaluate their regular pairs in FP32
-(``regular_p1_mixed``) under ``device_interface="cuda_mixed"``; their operator
-error against the FP64 path and the oracle is held to the mixed-precision
-bound (1e-6 relative Frobenius).  Operators without a mixed kernel (Laplace,
-complex k) run in FP64 under the same interface.
+The single layer, double layer, adjoint double layer and hypersingular
+operators on P1 -- Helmholtz (real and complex k), Laplace and modified
+Helmholtz -- evaluate their regular pairs in FP32 (``regular_p1_mixed``) under
+``device_interface="cuda_mixed"``; their operator error against the FP64 path
+and the oracle is held to the mixed-precision bound (1e-6 relative
+Frobenius).  Operators without a mixed kernel (a P1 domain with a DP0 dual
+space, the Maxwell magnetic field) run in FP64 under the same interface.
 """
 
 import numpy as np
@@ -53,9 +54,42 @@ def test_mixed_p1_against_fp64_and_oracle(oracle, path, k):
     assert rel_fro(amx.cpu().numpy(), ref) < 1e-6
 
 
-@pytest.mark.parametrize("path", ["helmholtz.single_layer", "helmholtz.hypersingular", "helmholtz.double_layer",
-                                  "helmholtz.adjoint_double_layer"])
-def test_mixed_p1_sweeps_agree(path):
+OPS = ["single_layer", "hypersingular", "double_layer", "adjoint_double_layer"]
+# (family, parameter): complex wavenumbers in the three phase classes of Re k, modified Helmholtz at a small
+# and a large omega, Laplace
+FAMILIES = [("laplace", None), ("modified_helmholtz", 1.5), ("modified_helmholtz", 12.0),
+            ("helmholtz", 2.0 + 0.5j), ("helmholtz", 4.0 + 1.0j), ("helmholtz", 40.0 + 2.0j)]
+
+
+@pytest.mark.parametrize("family,k", FAMILIES)
+@pytest.mark.parametrize("name", OPS)
+def test_mixed_p1_other_kernels_against_fp64_and_oracle(oracle, family, name, k):
+    """Laplace, modified Helmholtz and complex-k Helmholtz on a 512-element ellipsoid: FP32 pairs within 1e-6
+    of the FP64 weak form and of the oracle; real kernels give real matrices."""
+    from cases import oracle_dense
+
+    from bempp_cuda import assembly
+    from bempp_cuda.shapes import ellipsoid
+    from bempp_cuda.space import function_space
+
+    grid = ellipsoid(3, 1.1, 0.9, 1.0)
+    sp = function_space(grid, "P", 1)
+    path = family + "." + name
+    a64 = _op(path, sp, k, "cuda").weak_form().tensor
+    assembly.FP64_FALLBACKS.clear()
+    amx = _op(path, sp, k, "cuda_mixed").weak_form().tensor
+    assert not assembly.FP64_FALLBACKS  # a mixed kernel ran
+    assert amx.dtype == a64.dtype == (torch.complex128 if family == "helmholtz" else torch.float64)
+    err = (torch.linalg.norm(amx - a64) / torch.linalg.norm(a64)).item()
+    assert 0.0 < err < 1e-6, err
+    ref = oracle_dense(oracle, _op(path, sp, k, "cuda"), sp, sp)
+    assert rel_fro(amx.cpu().numpy(), ref) < 1e-6
+
+
+@pytest.mark.parametrize("family,k", [("helmholtz", 5.0), ("helmholtz", 5.0 + 1.0j), ("laplace", None),
+                                      ("modified_helmholtz", 3.0)])
+@pytest.mark.parametrize("name", OPS)
+def test_mixed_p1_sweeps_agree(family, name, k):
     """Symmetric sweep (both blocks by atomics, U + U^T into a zeroed result, or for the double layers the
     skew sweep) and per-pair sweep."""
     from bempp_cuda import _lib
@@ -66,12 +100,13 @@ def test_mixed_p1_sweeps_agree(path):
 
     grid = regular_sphere(3)
     sp = function_space(grid, "P", 1)
-    d = _op(path, sp, 5.0, "cuda").descriptor
+    d = _op(family + "." + name, sp, k, "cuda").descriptor
     n = sp.global_dof_count
+    dtype = torch.complex128 if family == "helmholtz" else torch.float64
     out = {}
     for precision in (_lib.FP64, _lib.MIXED):
         for sym, zero in ((True, False), (False, False), (True, True)):
-            a = torch.zeros((n, n), dtype=torch.complex128, device="cuda")
+            a = torch.zeros((n, n), dtype=dtype, device="cuda")
             regular_into(a, d, sp, sp, Parameters(), precision=precision, symmetric=sym, result_is_zero=zero)
             singular_into_dense(a, d, sp, sp, Parameters())
             out[(precision, sym, zero)] = a
@@ -81,15 +116,21 @@ def test_mixed_p1_sweeps_agree(path):
         assert (torch.linalg.norm(a - ref) / torch.linalg.norm(ref)).item() < tol, key
 
 
-@pytest.mark.parametrize("path,k", [("laplace.double_layer", None), ("laplace.single_layer", None),
-                                    ("helmholtz.single_layer", 3.0 + 0.5j)])
+@pytest.mark.parametrize("path,k", [("laplace.double_layer", None), ("helmholtz.single_layer", 3.0 + 0.5j)])
 def test_mixed_interface_without_mixed_kernel_is_fp64(path, k):
+    """A P1 domain with a DP0 dual space has no mixed kernel: FP64 under cuda_mixed."""
+    from bempp_cuda import operators
     from bempp_cuda.shapes import regular_sphere
     from bempp_cuda.space import function_space
 
-    sp = function_space(regular_sphere(2), "P", 1)
-    a64 = _op(path, sp, k, "cuda").weak_form().tensor
-    amx = _op(path, sp, k, "cuda_mixed").weak_form().tensor
+    grid = regular_sphere(2)
+    p1, dp0 = function_space(grid, "P", 1), function_space(grid, "DP", 0)
+    f = operators.boundary
+    for part in path.split("."):
+        f = getattr(f, part)
+    args = (p1, p1, dp0) if k is None else (p1, p1, dp0, k)
+    a64 = f(*args, device_interface="cuda").weak_form().tensor
+    amx = f(*args, device_interface="cuda_mixed").weak_form().tensor
     assert (torch.linalg.norm(amx - a64) / torch.linalg.norm(a64)).item() < 1e-13
 
 
