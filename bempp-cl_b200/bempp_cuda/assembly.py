@@ -472,9 +472,10 @@ def evaluate_potential_device(space, descriptor, points, local_coefficients, par
     ``local_coefficients`` are the element-local coefficients (nshape * ne,)
     complex128, i.e. ``space.map_to_full_grid @ x`` of the reference
     (dense_potential_assembler.py:30-34); ``points`` is a (3, npoints) array.
-    ``precision=MIXED`` evaluates the point-source pairs of Laplace and
-    Helmholtz (real k) single / double layer potentials in FP32; other
-    potentials then run in FP64.
+    ``precision=MIXED`` evaluates the point-source pairs of Laplace,
+    Helmholtz (real or complex k) and modified Helmholtz single / double
+    layer potentials in FP32; the library refuses it for the others (Maxwell
+    potentials, far fields), which the operator layer then runs in FP64.
     """
     require_cuda()
     kernel, assembly = kernel_ids(descriptor)

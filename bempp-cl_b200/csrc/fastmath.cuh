@@ -196,4 +196,16 @@ __device__ __forceinline__ void phase_reduced32(double x, float *s, float *c) {
     *c = ((q + 1) & 2) ? -cc : cc;
 }
 
+// e^{-x} (any real x, |x| below ~700) for the mixed-precision kernels: t = -x log2(e) in FP64, split
+// t = n + f with n = rint(t), |f| <= 1/2; 2^f by exp2f in FP32 (relative error ~1e-7, the size of the
+// FP32 sums it multiplies) and 2^n built exactly in FP64, so a factor far below the FP32 range stays
+// exact in scale.  0 below 2^-1022.
+__device__ __forceinline__ double exp_neg_reduced(double x) {
+    const double t = -x * 1.4426950408889634;  // log2(e)
+    const double n = fmin(rint(t), 1023.0);
+    if (n < -1022.0) return 0.0;
+    const double two_n = __longlong_as_double((long long)(n + 1023.0) << 52);
+    return (double)exp2f((float)(t - n)) * two_n;
+}
+
 }  // namespace bc

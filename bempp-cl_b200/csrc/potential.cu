@@ -414,9 +414,14 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar(PotParams prm, in
     }
 }
 
-// Mixed precision (FP32 point-source pairs): Laplace and Helmholtz (real k)
-// single / double layer potentials.  Lengths are in units of 1/kappa
-// (kappa = k, or 1 for Laplace).  Per (evaluation point, source element) in
+// Mixed precision (FP32 point-source pairs): Laplace, Helmholtz and modified
+// Helmholtz single / double layer potentials.  Lengths are in units of
+// 1/kappa (kappa = Re k, omega, or 1 for Laplace).  A complex wavenumber
+// (CK) adds the amplitude e^{-beta r'}, beta = Im k / Re k, and modified
+// Helmholtz has e^{-r'} alone (real kernel): e^{-beta theta} per pair by
+// __expf, e^{-beta r_c'} per (point, element) by exp_neg_reduced; the
+// double-layer factor (i k r - 1) becomes -(1 + beta r') + i r', and
+// -(1 + r') for modified Helmholtz.  Per (evaluation point, source element) in
 // FP64: D = kappa c_e - kappa x (one FMA per coordinate, kappa c_e staged),
 // r_c' = |D| (FP32 rsqrt, one FP64 Newton step) and the argument reduction of
 // exp(i r_c'); per source in FP32:
@@ -440,11 +445,14 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar(PotParams prm, in
 // is unknown: no FP64 fallback).
 // NQ > 0 fixes the sources per element at compile time (the pair loop unrolls);
 // NQ = 0 reads it from prm.nq.
-template <int K, int PHC, int NQ>
+template <int K, int PHC, int NQ, bool CK = false>
 __global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams prm, int64_t chunk_elems,
                                                                       double near_r) {
     constexpr bool HELM = (K == BEMPPCUDA_HELMHOLTZ_SLP || K == BEMPPCUDA_HELMHOLTZ_DLP);
-    constexpr bool DLP = (K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_HELMHOLTZ_DLP);
+    constexpr bool MH = (K == BEMPPCUDA_MODHELM_SLP || K == BEMPPCUDA_MODHELM_DLP);
+    constexpr bool DLP = (K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_HELMHOLTZ_DLP || K == BEMPPCUDA_MODHELM_DLP);
+    constexpr bool EXPO = MH || CK;  // an amplitude exp(-beta r') beside (or instead of) the phase
+    static_assert(!CK || HELM, "complex wavenumber: Helmholtz potentials");
     static_assert(PS_PPT == 2, "two evaluation points per thread, packed");
     __shared__ float4 syo[PS_SOURCES];  // yo, |yo|^2
     __shared__ float4 scf[PS_SOURCES];  // coefficient re, im, yo . n_e, -im
@@ -455,8 +463,11 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams p
     const int64_t ebeg = (int64_t)blockIdx.y * chunk_elems;
     const int64_t eend = min(ebeg + chunk_elems, prm.nsupport);
     const int64_t pbase = (int64_t)blockIdx.x * (PS_THREADS * PS_PPT) + threadIdx.x;
-    const double kap = HELM ? prm.p[0] : 1.0;
-    const double sc = HELM ? (DLP ? kap * kap : kap) : 1.0;  // the sums ar, ai are in units of sc
+    const double kap = HELM || MH ? prm.p[0] : 1.0;
+    // exp(-beta r'): beta = Im k / Re k (complex k), 1 (modified Helmholtz, units of 1/omega)
+    const double betd = CK ? prm.p[1] / prm.p[0] : (MH ? 1.0 : 0.0);
+    const float bet = (float)betd;
+    const double sc = HELM || MH ? (DLP ? kap * kap : kap) : 1.0;  // the sums ar, ai are in units of sc
     const double inv_sc = __drcp_rn(sc);
     double x[PS_PPT][3], ar[PS_PPT], ai[PS_PPT];
 #pragma unroll
@@ -530,7 +541,7 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams p
                 const float2 r2 = add2(rc2f, sdot);
                 const float2 rinv = f2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
                 const float2 cr = b2(cf.x), ci = b2(cf.y);
-                if (!HELM) {
+                if (!HELM && !MH) {
                     float2 f = rinv;
                     if (DLP) {
                         // -(d'.n) / r'^3
@@ -542,26 +553,53 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams p
                 } else {
                     const float2 den = fma2(r2, rinv, rcf);  // r' + r_c'
                     const float2 th = mul2(sdot, f2(rcp_approx(den.x), rcp_approx(den.y)));
-                    float2 sn, cs;
-                    sincos2<PHC>(th, &sn, &cs);
-                    float2 vr, vi;  // kernel value over kappa (SLP) or kappa^2 (DLP), phase e^{i r_c'} excluded
+                    // cs + i sn: e^{i theta} (Helmholtz), times e^{-beta theta} (complex k); e^{-theta} (modified)
+                    float2 sn = b2(0.f), cs = b2(1.f);
+                    if (HELM) sincos2<PHC>(th, &sn, &cs);
+                    if (EXPO) {
+                        const float2 am = f2(__expf(-bet * th.x), __expf(-bet * th.y));
+                        cs = mul2(cs, am);
+                        if (HELM) sn = mul2(sn, am);
+                    }
+                    // kernel value over kappa (SLP) or kappa^2 (DLP), the element factor e^{(i - beta) r_c'} excluded
+                    float2 vr, vi = b2(0.f);
                     if (!DLP) {
                         vr = mul2(rinv, cs);
-                        vi = mul2(rinv, sn);
+                        if (HELM) vi = mul2(rinv, sn);
                     } else {
-                        // (i r' - 1) e^{i theta} (d'.n) / r'^3: (-cs - r' sn, r' cs - sn) g
                         const float2 rp = mul2(r2, rinv);
                         const float2 g = mul2(add2(Dn, b2(cf.z)), mul2(rinv, mul2(rinv, rinv)));
-                        vr = mul2(g, mul2(fma2(rp, sn, cs), b2(-1.f)));
-                        vi = mul2(g, fma2(rp, cs, mul2(sn, b2(-1.f))));
+                        if (MH) {
+                            // -(1 + r') e^{-theta} (d'.n) / r'^3
+                            vr = mul2(g, mul2(mul2(add2(rp, b2(1.f)), cs), b2(-1.f)));
+                        } else if (CK) {
+                            // (i k r - 1) = -(1 + beta r') + i r': (-a cs - r' sn, r' cs - a sn) g
+                            const float2 a = fma2(b2(bet), rp, b2(1.f));
+                            vr = mul2(g, mul2(fma2(rp, sn, mul2(a, cs)), b2(-1.f)));
+                            vi = mul2(g, fma2(rp, cs, mul2(mul2(a, sn), b2(-1.f))));
+                        } else {
+                            // (i r' - 1) e^{i theta} (d'.n) / r'^3: (-cs - r' sn, r' cs - sn) g
+                            vr = mul2(g, mul2(fma2(rp, sn, cs), b2(-1.f)));
+                            vi = mul2(g, fma2(rp, cs, mul2(sn, b2(-1.f))));
+                        }
                     }
-                    er = fma2(vr, cr, fma2(vi, b2(cf.w), er));  // cf.w = -im, exact
-                    ei = fma2(vr, ci, fma2(vi, cr, ei));
+                    if (MH) {  // real kernel
+                        er = fma2(vr, cr, er);
+                        ei = fma2(vr, ci, ei);
+                    } else {
+                        er = fma2(vr, cr, fma2(vi, b2(cf.w), er));  // cf.w = -im, exact
+                        ei = fma2(vr, ci, fma2(vi, cr, ei));
+                    }
                 }
             }
             // times exp(i r_c') in packed FP32 (the phase and the sums carry FP32 errors alike); the
             // FP64 sums over elements leave out kappa (single layer) or kappa^2 (double layer)
             float2 pr = er, pi = ei;
+            double amp[2] = {1.0, 1.0};  // e^{-beta r_c'} (complex k, modified Helmholtz)
+            if (EXPO) {
+                amp[0] = exp_neg_reduced(betd * rc[0]);
+                amp[1] = exp_neg_reduced(betd * rc[1]);
+            }
             if (HELM) {
                 float s0f, c0f, s1f, c1f;  // FP64 reduction, FP32 polynomials (phase_reduced32)
                 phase_reduced32(rc[0], &s0f, &c0f);
@@ -585,18 +623,30 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams p
                         double f = rinv;
                         if (DLP) f = fma(d2, o[5 * n + gq], fma(d1, o[4 * n + gq], d0 * o[3 * n + gq])) * rinv * rinv * rinv;
                         const double cr = o[6 * n + gq], ci = o[7 * n + gq];
-                        if (!HELM) {
+                        if (!HELM && !MH) {
                             if (DLP) f = -f;
                             nr = fma(f, cr, nr);
                             ni = fma(f, ci, ni);
+                        } else if (MH) {
+                            // the Laplace kernels times e^{-w r} (single layer), e^{-w r} (1 + w r) (double layer)
+                            const double r = r2 * rinv;
+                            double w = f * exp(-kap * r);
+                            if (DLP) w = -w * fma(kap, r, 1.0);
+                            nr = fma(w, cr, nr);
+                            ni = fma(w, ci, ni);
                         } else {
                             const double r = r2 * rinv;
                             double sn, cs;
                             sincos_cw64(kap * r, &sn, &cs);
+                            if (CK) {
+                                const double am = exp(-prm.p[1] * r);
+                                sn *= am;
+                                cs *= am;
+                            }
                             double wr = f * cr, wi = f * ci;
-                            if (DLP) {  // times (i k r - 1)
-                                const double b = kap * r;
-                                const double tr = -fma(b, wi, wr), ti = fma(b, wr, -wi);
+                            if (DLP) {  // times (i k r - 1) = -(1 + Im k r) + i Re k r
+                                const double b = kap * r, c0 = CK ? -fma(prm.p[1], r, 1.0) : -1.0;
+                                const double tr = fma(c0, wr, -b * wi), ti = fma(c0, wi, b * wr);
                                 wr = tr;
                                 wi = ti;
                             }
@@ -606,6 +656,9 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams p
                     }
                     ar[j] = fma(nr, inv_sc, ar[j]);
                     ai[j] = fma(ni, inv_sc, ai[j]);
+                } else if (EXPO) {
+                    ar[j] = fma(amp[j], prj[j], ar[j]);
+                    ai[j] = fma(amp[j], pij[j], ai[j]);
                 } else {
                     ar[j] += prj[j];
                     ai[j] += pij[j];
@@ -674,9 +727,9 @@ static cudaError_t launch_scalar_nq(const PotParams &prm, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-template <int K, int PHC>
+template <int K, int PHC, bool CK = false>
 static cudaError_t launch_mixed_nq(const PotParams &prm, double near_r, cudaStream_t st) {
-    auto fn = prm.nq == 6 ? potential_scalar_mixed<K, PHC, 6> : potential_scalar_mixed<K, PHC, 0>;
+    auto fn = prm.nq == 6 ? potential_scalar_mixed<K, PHC, 6, CK> : potential_scalar_mixed<K, PHC, 0, CK>;
     dim3 grid;
     int64_t chunk_elems = 0;
     const cudaError_t err = scalar_grid(prm, (const void *)fn, &grid, &chunk_elems, st);
@@ -687,23 +740,33 @@ static cudaError_t launch_mixed_nq(const PotParams &prm, double near_r, cudaStre
 
 // Scalar Laplace, Helmholtz (real or complex wavenumber) and modified Helmholtz potentials;
 // phase_radius bounds every source's distance from its element centroid (0: unknown).
-// Mixed-precision Laplace / Helmholtz (real k) single / double layer potentials.
+// Mixed-precision Laplace, Helmholtz (Re k > 0, real or complex k) and modified Helmholtz single / double
+// layer potentials.
+template <int K, bool CK>
+static cudaError_t launch_mixed_phase(const PotParams &prm, int phc, double near_r, cudaStream_t st) {
+    if (phc == 2) return launch_mixed_nq<K, 2, CK>(prm, near_r, st);
+    if (phc == 1) return launch_mixed_nq<K, 1, CK>(prm, near_r, st);
+    return launch_mixed_nq<K, 0, CK>(prm, near_r, st);
+}
+
 static cudaError_t launch_scalar_mixed(const PotParams &prm, int kernel, double phase_radius, cudaStream_t st) {
     const double kr = fabs(prm.p[0]) * phase_radius;
     const int phc = (phase_radius > 0.0 && kr <= 0.5) ? 2 : (phase_radius > 0.0 && kr <= 1.0) ? 1 : 0;
-    const bool helm = kernel == BEMPPCUDA_HELMHOLTZ_SLP || kernel == BEMPPCUDA_HELMHOLTZ_DLP;
-    const double near_r = 4.0 * (helm ? prm.p[0] : 1.0) * phase_radius;  // in the kernel's units of 1/kappa
+    const bool scaled = kernel == BEMPPCUDA_HELMHOLTZ_SLP || kernel == BEMPPCUDA_HELMHOLTZ_DLP ||
+                        kernel == BEMPPCUDA_MODHELM_SLP || kernel == BEMPPCUDA_MODHELM_DLP;
+    const double near_r = 4.0 * (scaled ? prm.p[0] : 1.0) * phase_radius;  // in the kernel's units of 1/kappa
+    const bool ck = prm.p[1] != 0.0;
     switch (kernel) {
     case BEMPPCUDA_LAPLACE_SLP: return launch_mixed_nq<BEMPPCUDA_LAPLACE_SLP, 0>(prm, near_r, st);
     case BEMPPCUDA_LAPLACE_DLP: return launch_mixed_nq<BEMPPCUDA_LAPLACE_DLP, 0>(prm, near_r, st);
+    case BEMPPCUDA_MODHELM_SLP: return launch_mixed_nq<BEMPPCUDA_MODHELM_SLP, 0>(prm, near_r, st);
+    case BEMPPCUDA_MODHELM_DLP: return launch_mixed_nq<BEMPPCUDA_MODHELM_DLP, 0>(prm, near_r, st);
     case BEMPPCUDA_HELMHOLTZ_SLP:
-        if (phc == 2) return launch_mixed_nq<BEMPPCUDA_HELMHOLTZ_SLP, 2>(prm, near_r, st);
-        if (phc == 1) return launch_mixed_nq<BEMPPCUDA_HELMHOLTZ_SLP, 1>(prm, near_r, st);
-        return launch_mixed_nq<BEMPPCUDA_HELMHOLTZ_SLP, 0>(prm, near_r, st);
+        return ck ? launch_mixed_phase<BEMPPCUDA_HELMHOLTZ_SLP, true>(prm, phc, near_r, st)
+                  : launch_mixed_phase<BEMPPCUDA_HELMHOLTZ_SLP, false>(prm, phc, near_r, st);
     default:  // BEMPPCUDA_HELMHOLTZ_DLP
-        if (phc == 2) return launch_mixed_nq<BEMPPCUDA_HELMHOLTZ_DLP, 2>(prm, near_r, st);
-        if (phc == 1) return launch_mixed_nq<BEMPPCUDA_HELMHOLTZ_DLP, 1>(prm, near_r, st);
-        return launch_mixed_nq<BEMPPCUDA_HELMHOLTZ_DLP, 0>(prm, near_r, st);
+        return ck ? launch_mixed_phase<BEMPPCUDA_HELMHOLTZ_DLP, true>(prm, phc, near_r, st)
+                  : launch_mixed_phase<BEMPPCUDA_HELMHOLTZ_DLP, false>(prm, phc, near_r, st);
     }
 }
 
@@ -759,18 +822,21 @@ int bc_potential_launch(const bemppcuda_potential_args *a, double *workspace, cu
     QuadRule rule;
     fill_rule(rule, a->nq, a->quad_points, a->quad_weights);
     const bool maxwell = a->assembly != BEMPPCUDA_ASM_SCALAR;
-    // mixed precision: Laplace / Helmholtz (real k) single / double layer potentials
+    // mixed precision: Laplace, Helmholtz (Re k > 0) and modified Helmholtz (w > 0) single / double layer
+    // potentials
     const bool mixed = a->precision == BEMPPCUDA_MIXED;
     if (a->precision != BEMPPCUDA_FP64 && !mixed) {
         bc_set_error("potential: precision must be BEMPPCUDA_FP64 or BEMPPCUDA_MIXED");
         return BEMPPCUDA_ERR_INVALID;
     }
-    if (mixed && (maxwell || a->params[1] != 0.0 || !(a->kernel == BEMPPCUDA_LAPLACE_SLP ||
-                                                       a->kernel == BEMPPCUDA_LAPLACE_DLP ||
-                                                       ((a->kernel == BEMPPCUDA_HELMHOLTZ_SLP ||
-                                                         a->kernel == BEMPPCUDA_HELMHOLTZ_DLP) &&
-                                                        a->params[0] > 0.0)))) {
-        bc_set_error("mixed-precision potentials: Laplace and Helmholtz (real k > 0) single / double layer only");
+    const bool mixed_kernel =
+        a->kernel == BEMPPCUDA_LAPLACE_SLP || a->kernel == BEMPPCUDA_LAPLACE_DLP ||
+        ((a->kernel == BEMPPCUDA_HELMHOLTZ_SLP || a->kernel == BEMPPCUDA_HELMHOLTZ_DLP ||
+          a->kernel == BEMPPCUDA_MODHELM_SLP || a->kernel == BEMPPCUDA_MODHELM_DLP) &&
+         a->params[0] > 0.0);
+    if (mixed && (maxwell || !mixed_kernel)) {
+        bc_set_error("mixed-precision potentials: Laplace, Helmholtz (Re k > 0) and modified Helmholtz (w > 0) "
+                     "single / double layer only");
         return BEMPPCUDA_ERR_UNSUPPORTED;
     }
     // the FP64 treatment of points next to the surface needs the bound R on source offsets

@@ -105,7 +105,10 @@ typedef struct {
 typedef struct {
     int32_t kernel;     /* BEMPPCUDA_* Green's function */
     int32_t assembly;   /* BEMPPCUDA_ASM_* */
-    int32_t precision;  /* BEMPPCUDA_FP64 or BEMPPCUDA_MIXED */
+    int32_t precision;  /* BEMPPCUDA_FP64 or BEMPPCUDA_MIXED: DP0 scalar kernels; P1 single, double,
+                           adjoint double layer and hypersingular (Helmholtz with Re k > 0, Laplace,
+                           modified Helmholtz); Maxwell electric field (real k > 0); 6-point rule.
+                           Other operators return BEMPPCUDA_ERR_UNSUPPORTED under MIXED */
     int32_t is_complex; /* result is complex128 (1) or float64 (0) */
     double params[4];   /* kernel parameters: (Re k, Im k) or (omega) */
     bemppcuda_grid test_grid;
@@ -188,8 +191,9 @@ typedef struct {
     int32_t kernel;   /* Green's function; far-field kernels treat points as directions */
     int32_t assembly; /* BEMPPCUDA_ASM_SCALAR, _EFIE or _MFIE */
     int32_t precision; /* BEMPPCUDA_FP64, or BEMPPCUDA_MIXED (FP32 point-source pairs, FP64 per-element
-                          phase and sums) for Laplace / Helmholtz (real k > 0) single / double layer
-                          potentials; other kernels return BEMPPCUDA_ERR_UNSUPPORTED under MIXED */
+                          phase, amplitude and sums) for Laplace, Helmholtz (Re k > 0, real or complex k)
+                          and modified Helmholtz (omega > 0) single / double layer potentials; other
+                          kernels return BEMPPCUDA_ERR_UNSUPPORTED under MIXED */
     int32_t pad0;
     double params[4];
     bemppcuda_grid grid;

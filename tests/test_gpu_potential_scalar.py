@@ -127,26 +127,36 @@ def test_mixed_precision_potentials(oracle, kr, name, family):
     assert 0.0 < rel_fro(got, ref) < 1e-6
 
 
-@pytest.mark.parametrize("case", ["complex", "modified"])
-def test_mixed_interface_without_mixed_kernel_runs_fp64(case):
-    """Complex wavenumbers and modified Helmholtz have no mixed potential kernel: the FP64 result (to
-    rounding: the source chunks add their sums with atomics, in no fixed order)."""
-    from bempp_cuda import operators
+@pytest.mark.parametrize("k", [0.3 + 0.1j, 0.8 + 0.4j, 3.0 + 0.5j, 6.0 + 3.0j, "w1.5", "w12"])
+@pytest.mark.parametrize("name", ["single_layer", "double_layer"])
+@pytest.mark.parametrize("family", ["DP0", "P1"])
+def test_mixed_potentials_complex_and_modified(oracle, family, name, k):
+    """cuda_mixed for complex wavenumbers (Re k R in each phase class, Im k up to Re k / 2) and modified
+    Helmholtz (w = 1.5, 12): FP32 point-source pairs with the amplitude e^{-beta r'} split about the element
+    centroids, within 1e-6 of the oracle and of the FP64 path; points on centroids and 1e-3 above the
+    surface take the FP64 branch."""
+    from bempp_cuda import assembly, operators
+    from bempp_cuda.device import device_grid
     from bempp_cuda.shapes import regular_sphere
     from bempp_cuda.space import function_space
     from cases import sphere_shell_points
 
-    space = function_space(regular_sphere(2), "P", 1)
-    points, _ = sphere_shell_points(500, 31)
-    if case == "complex":
-        f, args = operators.potential.helmholtz.single_layer, (3.0 + 0.5j,)
+    grid = regular_sphere(3)
+    space = function_space(grid, "DP", 0) if family == "DP0" else function_space(grid, "P", 1)
+    shell, _ = sphere_shell_points(1500, 37)
+    cent = grid.vertices[:, grid.elements].mean(axis=1)
+    pick = np.random.default_rng(13).choice(cent.shape[1], 40, replace=False)
+    points = np.concatenate([shell, cent[:, pick[:20]], cent[:, pick[20:]] * 1.001], axis=1)
+    if isinstance(k, str):
+        fam, args = operators.potential.modified_helmholtz, (float(k[1:]),)
     else:
-        f, args = operators.potential.modified_helmholtz.double_layer, (2.0,)
-    rng = np.random.default_rng(8)
-    c = rng.standard_normal(space.global_dof_count) + 1j * rng.standard_normal(space.global_dof_count)
-    a = f(space, points, *args).evaluate_device(c)
-    b = f(space, points, *args, device_interface="cuda_mixed").evaluate_device(c)
-    assert (torch.linalg.norm(a - b) / torch.linalg.norm(a)).item() < 1e-13
+        fam, args = operators.potential.helmholtz, (k.real / device_grid(grid).radius + 1j * k.imag / device_grid(grid).radius,)
+    assembly.FP64_FALLBACKS.clear()
+    mixed = getattr(fam, name)(space, points, *args, device_interface="cuda_mixed")
+    got = _check(oracle, mixed, space, tol=1e-6)
+    assert not assembly.FP64_FALLBACKS  # the mixed kernel ran
+    ref = _check(oracle, getattr(fam, name)(space, points, *args), space)
+    assert 0.0 < rel_fro(got, ref) < 1e-6
 
 
 @pytest.mark.parametrize("name", ["single_layer", "double_layer"])
