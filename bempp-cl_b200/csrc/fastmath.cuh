@@ -171,7 +171,8 @@ __device__ __forceinline__ void sincos_cw32(float x, float *s, float *c) {
     *c = ((q + 1) & 2) ? -cc : cc;
 }
 
-// exp(i x) for a centroid distance x >= 0 in units of 1/k (below 1e6) of the mixed-precision kernels:
+// exp(i x) for a phase |x| below 1e6 (a centroid distance in units of 1/k, a far-field phase) of the
+// mixed-precision kernels:
 // Cody-Waite reduction by pi/2 in FP64 (two-part constant), then the FP32 minimax polynomials on
 // |a| <= pi/4.  The reduced argument keeps its FP64 accuracy until it is rounded to FP32, so the
 // phase is within 1e-7 of exp(i x) for any x in range; the FP32 sums it multiplies carry errors of

@@ -682,6 +682,118 @@ __global__ void __launch_bounds__(PS_THREADS) potential_scalar_mixed(PotParams p
     }
 }
 
+// Mixed-precision scalar far fields (helmholtz_far_field_{single,double}_layer,
+// numba_kernels.py:402-449): u(x) = (1/4 pi) sum_y e^{-i k x . y} c_y (single
+// layer), each term times -k (x . n_y) i (double layer), for unit directions x
+// and k = Re k, as the reference evaluates them.  The phase is split about the
+// source's element centroid: per (direction, element) in FP64
+// phi = -x . (k c_e) and its reduction (phase_reduced32); per source in FP32
+// theta = -x . k (y - c_e), |theta| <= k R (phase class PHC), the fitted sine /
+// cosine and the complex product with the coefficient; the thread's two
+// directions share each source in packed f32x2 operations.  The six-term sums
+// per element are FP32, their product with e^{i phi} too; the sum over
+// elements is FP64.  No near field: the kernel is smooth.
+template <int K, int PHC, int NQ>
+__global__ void __launch_bounds__(PS_THREADS) farfield_scalar_mixed(PotParams prm, int64_t chunk_elems) {
+    constexpr bool DLP = K == BEMPPCUDA_FARFIELD_DLP;
+    static_assert(PS_PPT == 2, "two directions per thread, packed");
+    __shared__ float4 syo[PS_SOURCES];                 // -k (y - c_e)
+    __shared__ float4 scf[PS_SOURCES];                 // coefficient re, im, -im
+    __shared__ double scen[PS_SOURCES * 3];            // k c_e
+    __shared__ float snrm[DLP ? PS_SOURCES * 3 : 3];  // n_e
+    const int nq = NQ > 0 ? NQ : prm.nq;
+    const int tile_elems = PS_SOURCES / nq;
+    const int64_t ebeg = (int64_t)blockIdx.y * chunk_elems;
+    const int64_t eend = min(ebeg + chunk_elems, prm.nsupport);
+    const int64_t pbase = (int64_t)blockIdx.x * (PS_THREADS * PS_PPT) + threadIdx.x;
+    const double kap = prm.p[0];
+    double x[PS_PPT][3], ar[PS_PPT], ai[PS_PPT];
+#pragma unroll
+    for (int j = 0; j < PS_PPT; ++j) {
+        const int64_t pj = min(pbase + j * PS_THREADS, prm.npoints - 1);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) x[j][d] = prm.points[3 * pj + d];
+        ar[j] = ai[j] = 0.0;
+    }
+    const float2 xx = f2((float)x[0][0], (float)x[1][0]), xy = f2((float)x[0][1], (float)x[1][1]),
+                 xz = f2((float)x[0][2], (float)x[1][2]);
+    const int64_t n = prm.nsrc;
+    const double *o = prm.src;
+    for (int64_t t0 = ebeg; t0 < eend; t0 += tile_elems) {
+        const int te = (int)min((int64_t)tile_elems, eend - t0);
+        const int ns = te * nq;
+        const int64_t s0 = t0 * nq;
+        __syncthreads();
+        for (int e = threadIdx.x; e < te; e += PS_THREADS) {
+            const int64_t ge = t0 + e;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) scen[3 * e + d] = kap * o[(8 + d) * n + ge];
+            if (DLP)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) snrm[3 * e + d] = (float)o[(3 + d) * n + ge * nq];
+        }
+        __syncthreads();
+        for (int s = threadIdx.x; s < ns; s += PS_THREADS) {
+            const int64_t gs = s0 + s;
+            const int e = s / nq;
+            syo[s] = make_float4((float)fma(-kap, o[gs], scen[3 * e]), (float)fma(-kap, o[n + gs], scen[3 * e + 1]),
+                                 (float)fma(-kap, o[2 * n + gs], scen[3 * e + 2]), 0.f);
+            const float cim = (float)o[7 * n + gs];
+            scf[s] = make_float4((float)o[6 * n + gs], cim, -cim, 0.f);
+        }
+        __syncthreads();
+        for (int e = 0; e < te; ++e) {
+            float2 er = b2(0.f), ei = b2(0.f);
+#pragma unroll(NQ > 0 ? NQ : 1)
+            for (int q = 0; q < nq; ++q) {
+                const float4 yo = syo[e * nq + q];
+                const float4 cf = scf[e * nq + q];
+                const float2 th = fma2(xz, b2(yo.z), fma2(xy, b2(yo.y), mul2(xx, b2(yo.x))));
+                float2 sn, cs;
+                sincos2<PHC>(th, &sn, &cs);
+                const float2 cr = b2(cf.x), ci = b2(cf.y);
+                er = fma2(cs, cr, fma2(sn, b2(cf.z), er));  // cf.z = -im, exact
+                ei = fma2(cs, ci, fma2(sn, cr, ei));
+            }
+            // times e^{i phi}, phi = -x . (k c_e): FP64 reduction, FP32 polynomials
+            float s0f, c0f, s1f, c1f;
+            phase_reduced32(-fma(x[0][2], scen[3 * e + 2], fma(x[0][1], scen[3 * e + 1], x[0][0] * scen[3 * e])),
+                            &s0f, &c0f);
+            phase_reduced32(-fma(x[1][2], scen[3 * e + 2], fma(x[1][1], scen[3 * e + 1], x[1][0] * scen[3 * e])),
+                            &s1f, &c1f);
+            const float2 cs = f2(c0f, c1f), sn = f2(s0f, s1f);
+            float2 pr = fma2(cs, er, mul2(sn, mul2(ei, b2(-1.f))));
+            float2 pi = fma2(cs, ei, mul2(sn, er));
+            if (DLP) {
+                // times -(x . n_e) i (k applied at the store)
+                const float2 f = mul2(fma2(xz, b2(snrm[3 * e + 2]), fma2(xy, b2(snrm[3 * e + 1]),
+                                                                       mul2(xx, b2(snrm[3 * e])))), b2(-1.f));
+                const float2 tr = mul2(mul2(f, pi), b2(-1.f));
+                pi = mul2(f, pr);
+                pr = tr;
+            }
+            ar[0] += (double)pr.x;
+            ar[1] += (double)pr.y;
+            ai[0] += (double)pi.x;
+            ai[1] += (double)pi.y;
+        }
+    }
+    const double scale = BC_INV_4PI * (DLP ? kap : 1.0);
+#pragma unroll
+    for (int j = 0; j < PS_PPT; ++j) {
+        const int64_t pj = pbase + j * PS_THREADS;
+        if (pj >= prm.npoints) break;
+        double *out = prm.result + 2 * pj;
+        if (gridDim.y == 1) {
+            out[0] = scale * ar[j];
+            out[1] = scale * ai[j];
+        } else {
+            atomicAdd(out, scale * ar[j]);
+            atomicAdd(out + 1, scale * ai[j]);
+        }
+    }
+}
+
 // Grid of the per-point kernels: point blocks x source chunks; with more than one chunk the
 // chunks add their sums with atomics into the zeroed result.  The chunk count c minimises
 //   ceil(pblocks c / slots) (1/c + 1/64),
@@ -742,6 +854,24 @@ static cudaError_t launch_mixed_nq(const PotParams &prm, double near_r, cudaStre
 // phase_radius bounds every source's distance from its element centroid (0: unknown).
 // Mixed-precision Laplace, Helmholtz (Re k > 0, real or complex k) and modified Helmholtz single / double
 // layer potentials.
+template <int K, int PHC>
+static cudaError_t launch_far_mixed_nq(const PotParams &prm, cudaStream_t st) {
+    auto fn = prm.nq == 6 ? farfield_scalar_mixed<K, PHC, 6> : farfield_scalar_mixed<K, PHC, 0>;
+    dim3 grid;
+    int64_t chunk_elems = 0;
+    const cudaError_t err = scalar_grid(prm, (const void *)fn, &grid, &chunk_elems, st);
+    if (err != cudaSuccess) return err;
+    fn<<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems);
+    return cudaGetLastError();
+}
+
+template <int K>
+static cudaError_t launch_far_mixed(const PotParams &prm, int phc, cudaStream_t st) {
+    if (phc == 2) return launch_far_mixed_nq<K, 2>(prm, st);
+    if (phc == 1) return launch_far_mixed_nq<K, 1>(prm, st);
+    return launch_far_mixed_nq<K, 0>(prm, st);
+}
+
 template <int K, bool CK>
 static cudaError_t launch_mixed_phase(const PotParams &prm, int phc, double near_r, cudaStream_t st) {
     if (phc == 2) return launch_mixed_nq<K, 2, CK>(prm, near_r, st);
@@ -757,6 +887,8 @@ static cudaError_t launch_scalar_mixed(const PotParams &prm, int kernel, double 
     const double near_r = 4.0 * (scaled ? prm.p[0] : 1.0) * phase_radius;  // in the kernel's units of 1/kappa
     const bool ck = prm.p[1] != 0.0;
     switch (kernel) {
+    case BEMPPCUDA_FARFIELD_SLP: return launch_far_mixed<BEMPPCUDA_FARFIELD_SLP>(prm, phc, st);
+    case BEMPPCUDA_FARFIELD_DLP: return launch_far_mixed<BEMPPCUDA_FARFIELD_DLP>(prm, phc, st);
     case BEMPPCUDA_LAPLACE_SLP: return launch_mixed_nq<BEMPPCUDA_LAPLACE_SLP, 0>(prm, near_r, st);
     case BEMPPCUDA_LAPLACE_DLP: return launch_mixed_nq<BEMPPCUDA_LAPLACE_DLP, 0>(prm, near_r, st);
     case BEMPPCUDA_MODHELM_SLP: return launch_mixed_nq<BEMPPCUDA_MODHELM_SLP, 0>(prm, near_r, st);
@@ -832,11 +964,12 @@ int bc_potential_launch(const bemppcuda_potential_args *a, double *workspace, cu
     const bool mixed_kernel =
         a->kernel == BEMPPCUDA_LAPLACE_SLP || a->kernel == BEMPPCUDA_LAPLACE_DLP ||
         ((a->kernel == BEMPPCUDA_HELMHOLTZ_SLP || a->kernel == BEMPPCUDA_HELMHOLTZ_DLP ||
-          a->kernel == BEMPPCUDA_MODHELM_SLP || a->kernel == BEMPPCUDA_MODHELM_DLP) &&
+          a->kernel == BEMPPCUDA_MODHELM_SLP || a->kernel == BEMPPCUDA_MODHELM_DLP ||
+          a->kernel == BEMPPCUDA_FARFIELD_SLP || a->kernel == BEMPPCUDA_FARFIELD_DLP) &&
          a->params[0] > 0.0);
     if (mixed && (maxwell || !mixed_kernel)) {
         bc_set_error("mixed-precision potentials: Laplace, Helmholtz (Re k > 0) and modified Helmholtz (w > 0) "
-                     "single / double layer only");
+                     "single / double layer potentials and Helmholtz far fields (k > 0) only");
         return BEMPPCUDA_ERR_UNSUPPORTED;
     }
     // the FP64 treatment of points next to the surface needs the bound R on source offsets

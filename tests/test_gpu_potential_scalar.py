@@ -345,3 +345,29 @@ def test_mixed_precision_argument_checks():
     assert lib.bemppcuda_evaluate_potential(ctypes.byref(m), current_stream()) == _lib.ERR_UNSUPPORTED
     assert "mixed-precision potentials" in _lib.last_error()
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("kr", [0.3, 0.8, 3.0])
+@pytest.mark.parametrize("name", ["single_layer", "double_layer"])
+@pytest.mark.parametrize("family", ["DP0", "P1"])
+def test_mixed_far_fields(oracle, family, name, kr):
+    """cuda_mixed Helmholtz far fields: e^{-i k x . y} split about the element centroids (FP64 phase per
+    direction and element, FP32 offsets per source) within 1e-6 of the oracle and of the FP64 path, k R in
+    each phase class, 2000 random directions plus the coordinate axes."""
+    from bempp_cuda import assembly, operators
+    from bempp_cuda.device import device_grid
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+
+    grid = regular_sphere(3)
+    space = function_space(grid, "DP", 0) if family == "DP0" else function_space(grid, "P", 1)
+    rng = np.random.default_rng(17)
+    dirs = rng.standard_normal((3, 2000))
+    dirs = np.concatenate([dirs / np.linalg.norm(dirs, axis=0), np.eye(3), -np.eye(3)], axis=1)
+    k = kr / device_grid(grid).radius
+    f = getattr(operators.far_field.helmholtz, name)
+    assembly.FP64_FALLBACKS.clear()
+    got = _check(oracle, f(space, dirs, k, device_interface="cuda_mixed"), space, tol=1e-6)
+    assert not assembly.FP64_FALLBACKS  # the mixed kernel ran
+    ref = _check(oracle, f(space, dirs, k), space)
+    assert 0.0 < rel_fro(got, ref) < 1e-6
