@@ -37,6 +37,17 @@
 // (i k r - 1) = -(1 + beta r') + i r', and -k^2 complex in the hypersingular
 // operator.  Laplace and modified Helmholtz blocks are real and go to a real
 // matrix.
+// Maxwell magnetic field on RWG / SNC (ASM_MFIE): with u_i(p) = J_t r_i(p) =
+// x_p - P_ti and v_j(q) = y_q - P_sj (P: the vertex each RWG function points
+// away from), (x - y) . (u x v) = (P_ti - P_sj) . (u x v), so
+//   MFIE_ij = sum_ab det(P_ti - P_sj, J_t^a, J_s^b) N_ab,
+//   N_ab = sum_pq w_p w_q H (zeta_a(p) - o_ia)(zeta_b(q) - o_jb),
+// zeta = (xi, eta), o_i = (a_i, b_i), H = e^{ikr} (ikr - 1) / r^3: the N are
+// shifts of the nine moments of H, which the FP32 core gives as it gives
+// the EFIE's moments of G (the double layer's kernel value h without its
+// normal factor).  The determinants are FP64 geometry, so pairs of nearly
+// coplanar elements, whose triple products nearly vanish, keep the FP32
+// moments' relative accuracy (mfie_block_moments).
 // Maxwell electric field on RWG / SNC (ASM_EFIE): the nine moments
 // M[u][v] = sum_pq w_p w_q G u(p) v(q), u, v in {1, xi, eta}, that the EFIE
 // block needs (rwg.cuh) are a fixed linear map of the P1 single-layer block
@@ -66,6 +77,75 @@ struct TestBlockP1m {
     int v[P1_TCHUNK][3];
 };
 
+// MFIE block of an element pair from the nine moments M[u][v] = sum_pq w_p w_q H u(p) v(q), u, v in
+// {1, xi, eta} (index 0, 1, 2; H = e^{ikr} (ikr - 1) / r^3 times 4 pi, any phase factor of the pair left
+// out) and the two elements' vertex 0 and Jacobian columns: the formula of the header comment.
+__device__ __forceinline__ void mfie_block_moments(const double mre[3][3], const double mim[3][3],
+                                                   const double tv0[3], const double tj0[3], const double tj1[3],
+                                                   const double sv0[3], const double sj0[3], const double sj1[3],
+                                                   double blk_re[3][3], double blk_im[3][3]) {
+    const double *tJ[2] = {tj0, tj1}, *sJ[2] = {sj0, sj1};
+    // C_ab = J_t^a x J_s^b, and the vertex offsets P - v0 = J (a_i, b_i): (j1, j0, 0) per function
+    double C[2][2][3];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            C[a][b][0] = tJ[a][1] * sJ[b][2] - tJ[a][2] * sJ[b][1];
+            C[a][b][1] = tJ[a][2] * sJ[b][0] - tJ[a][0] * sJ[b][2];
+            C[a][b][2] = tJ[a][0] * sJ[b][1] - tJ[a][1] * sJ[b][0];
+        }
+    constexpr int oa[3] = {0, 1, 0}, ob[3] = {1, 0, 0};  // (a_i, b_i)
+    // det(P_ti - P_sj, C_ab) = (v0_t - v0_s + J_t o_i - J_s o_j) . C_ab
+    double e[2][2], ti[3][2][2], sj[3][2][2];
+    const double dv[3] = {tv0[0] - sv0[0], tv0[1] - sv0[1], tv0[2] - sv0[2]};
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            e[a][b] = dot3(dv, C[a][b]);
+            const double t0 = dot3(tj1, C[a][b]), t1 = dot3(tj0, C[a][b]);
+            const double s0 = dot3(sj1, C[a][b]), s1 = dot3(sj0, C[a][b]);
+            ti[0][a][b] = t0;
+            ti[1][a][b] = t1;
+            ti[2][a][b] = 0.0;
+            sj[0][a][b] = s0;
+            sj[1][a][b] = s1;
+            sj[2][a][b] = 0.0;
+        }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        // test side shifted moments: Mt[a][v] = M[1 + a][v] - o_ia M[0][v]
+        double mtr[2][3], mti[2][3];
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+            const int o = a == 0 ? oa[i] : ob[i];
+#pragma unroll
+            for (int v = 0; v < 3; ++v) {
+                mtr[a][v] = o ? mre[1 + a][v] - mre[0][v] : mre[1 + a][v];
+                mti[a][v] = o ? mim[1 + a][v] - mim[0][v] : mim[1 + a][v];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            double vr = 0.0, vi = 0.0;
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int b = 0; b < 2; ++b) {
+                    const int o = b == 0 ? oa[j] : ob[j];
+                    const double nr = o ? mtr[a][1 + b] - mtr[a][0] : mtr[a][1 + b];
+                    const double ni = o ? mti[a][1 + b] - mti[a][0] : mti[a][1 + b];
+                    const double det = e[a][b] + ti[i][a][b] - sj[j][a][b];
+                    vr = fma(det, nr, vr);
+                    vi = fma(det, ni, vi);
+                }
+            blk_re[i][j] = vr;
+            blk_im[i][j] = vi;
+        }
+    }
+}
+
 template <int ASM, int K, int PHC, bool SYM, bool CK = false>
 __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, QuadRule rule) {
     constexpr bool LAP = K == BEMPPCUDA_LAPLACE_SLP || K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_LAPLACE_ADLP;
@@ -74,15 +154,17 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
     constexpr bool HYP = ASM == BEMPPCUDA_ASM_HELM_HYP || ASM == BEMPPCUDA_ASM_LAPLACE_HYP ||
                          ASM == BEMPPCUDA_ASM_MODHELM_HYP;
     constexpr bool EFIE = ASM == BEMPPCUDA_ASM_EFIE;  // test curl slots hold J_t, multipliers edge lengths
+    constexpr bool MFIE = ASM == BEMPPCUDA_ASM_MFIE;  // the same, and v0_t in the third slot
+    constexpr bool RWG = EFIE || MFIE;
     constexpr bool DL = K == BEMPPCUDA_HELMHOLTZ_DLP || K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_MODHELM_DLP;
     constexpr bool AD = K == BEMPPCUDA_HELMHOLTZ_ADLP || K == BEMPPCUDA_LAPLACE_ADLP || K == BEMPPCUDA_MODHELM_ADLP;
-    static_assert(!CK || (!REAL && !EFIE), "complex wavenumber: the Helmholtz scalar operators");
+    static_assert(!CK || (!REAL && !RWG), "complex wavenumber: the Helmholtz scalar operators");
     constexpr bool SKEW = SYM && (DL || AD);
     constexpr bool NS_SUM = DL || SKEW;  // sums multiplied by d'.n_s per test point
     constexpr bool NT_SUM = AD || SKEW;  // sums with -d'.n_t per pair
     constexpr int NP = NQ6 / 2;
     __shared__ TestBlockP1m sb;
-    __shared__ double scurl[HYP || EFIE ? P1_TCHUNK : 1][3][3];  // curls (HYP) or J_t (EFIE)
+    __shared__ double scurl[HYP || RWG ? P1_TCHUNK : 1][3][3];  // curls (HYP) or J_t, v0_t (RWG)
     __shared__ WarpColumns swc[DP0_THREADS / 32];
     // staged block entries per warp: [block row][staging position]; SKEW: the (j, i) blocks too
     __shared__ double2 sst[DP0_THREADS / 32][3][WC_SLOTS];
@@ -118,14 +200,15 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
         }
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
-            sb.mult[idx][i] = prm.tmult[t * 3 + i] * (EFIE ? edge_length(prm.tg, prm.tne, t, i) : 1.0);
+            sb.mult[idx][i] = prm.tmult[t * 3 + i] * (RWG ? edge_length(prm.tg, prm.tne, t, i) : 1.0);
             sb.row[idx][i] = prm.tl2g[t * 3 + i];
         }
-        if (EFIE) {
+        if (RWG) {
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 scurl[idx][0][d] = g.j0[d];
                 scurl[idx][1][d] = g.j1[d];
+                scurl[idx][2][d] = g.v0[d];
             }
         }
         if (HYP) {
@@ -175,7 +258,7 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
         scol[j] = prm.sl2g[s * 3 + j];
-        smul[j] = prm.smult[s * 3 + j] * (EFIE ? edge_length(prm.sg, prm.sne, s, j) : 1.0);
+        smul[j] = prm.smult[s * 3 + j] * (RWG ? edge_length(prm.sg, prm.sne, s, j) : 1.0);
     }
     // the warp's columns (distinct trial dofs) and this lane's staging positions
     const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
@@ -269,7 +352,7 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
                     }
                 }
                 float2 kr, ki = b2(0.f);
-                if (!DL && !AD) {
+                if (!DL && !AD && !MFIE) {
                     kr = mul2(rinv, cs);
                     if (!REAL) ki = mul2(rinv, sn);
                 } else if (LAP) {
@@ -360,8 +443,38 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
                 }
             }
             efie_block<false>(mre, mim, scurl[tt][0], scurl[tt][1], gs.j0, gs.j1, kap, 0.0, ere, eim);
+        } else if (MFIE) {
+            // the moments of H = k^3 h (units of 1/k), then the block from the FP64 geometry
+            const double k3 = kap * kap * kap;
+            double mre[3][3], mim[3][3];
+            double rs[3] = {0.0, 0.0, 0.0}, is[3] = {0.0, 0.0, 0.0};
+            double cs_[3] = {0.0, 0.0, 0.0}, ci_[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const double lr = k3 * (double)lre[i][j], li = k3 * (double)lim[i][j];
+                    rs[i] += lr;
+                    is[i] += li;
+                    cs_[j] += lr;
+                    ci_[j] += li;
+                    if (i > 0 && j > 0) {
+                        mre[i][j] = lr;
+                        mim[i][j] = li;
+                    }
+                }
+            mre[0][0] = rs[0] + rs[1] + rs[2];
+            mim[0][0] = is[0] + is[1] + is[2];
+#pragma unroll
+            for (int a = 1; a < 3; ++a) {
+                mre[a][0] = rs[a];
+                mim[a][0] = is[a];
+                mre[0][a] = cs_[a];
+                mim[0][a] = ci_[a];
+            }
+            mfie_block_moments(mre, mim, scurl[tt][2], scurl[tt][0], scurl[tt][1], gs.v0, gs.j0, gs.j1, ere, eim);
         }
-        const double scale = EFIE ? BC_INV_4PI : (DL || AD ? kap * kap : kap) * BC_INV_4PI * sb.ie[tt] * gs.ie;
+        const double scale = RWG ? BC_INV_4PI : (DL || AD ? kap * kap : kap) * BC_INV_4PI * sb.ie[tt] * gs.ie;
         double sre = 0.0, sim = 0.0, cpf = 0.0, cpi = 0.0;
         if (HYP) {
             // S = sum_pq w_p w_q G: the P1 functions add up to 1 on each side
@@ -394,7 +507,7 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
                     if (SKEW) st_t[i][pos[j]] = make_double2(0.0, 0.0);
                     continue;
                 }
-                double vr = EFIE ? ere[i][j] : (double)lre[i][j], vi = EFIE ? eim[i][j] : (double)lim[i][j];
+                double vr = RWG ? ere[i][j] : (double)lre[i][j], vi = RWG ? eim[i][j] : (double)lim[i][j];
                 if (HYP) {
                     const double cij = scurl[tt][i][0] * curl_s[j][0] + scurl[tt][i][1] * curl_s[j][1] +
                                        scurl[tt][i][2] * curl_s[j][2];

@@ -490,7 +490,7 @@ static cudaError_t launch_p1_mixed(const RegParams &prm, const QuadRule &rule, i
     dim3 grid((unsigned)((prm.ntrial + DP0_THREADS - 1) / DP0_THREADS),
               (unsigned)((prm.ntest + P1_TCHUNK - 1) / P1_TCHUNK));
     constexpr bool helm = (K == BEMPPCUDA_HELMHOLTZ_SLP || K == BEMPPCUDA_HELMHOLTZ_DLP ||
-                           K == BEMPPCUDA_HELMHOLTZ_ADLP) && ASM != BEMPPCUDA_ASM_EFIE;
+                           K == BEMPPCUDA_HELMHOLTZ_ADLP) && ASM != BEMPPCUDA_ASM_EFIE && ASM != BEMPPCUDA_ASM_MFIE;
     const bool ck = helm && prm.p[1] != 0.0;
     if (ck) {
         if constexpr (helm) {
@@ -607,15 +607,17 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
     const bool p1_mixed = a->nq == NQ6 && !a->overwrite && a->test.nshape == 3 && a->trial.nshape == 3 &&
                           a->test.shapeset == BEMPPCUDA_SHAPE_P1 && a->trial.shapeset == BEMPPCUDA_SHAPE_P1 &&
                           p1_family && p1_params;
-    // ... and the Maxwell electric field on RWG / SNC (same FP32 core; 6-point rule, real k > 0)
-    const bool rwg_mixed = a->nq == NQ6 && !a->overwrite && a->assembly == BEMPPCUDA_ASM_EFIE &&
+    // ... and the Maxwell electric and magnetic fields on RWG / SNC (same FP32 core; 6-point rule,
+    // real k > 0)
+    const bool rwg_mixed = a->nq == NQ6 && !a->overwrite &&
+                           (a->assembly == BEMPPCUDA_ASM_EFIE || a->assembly == BEMPPCUDA_ASM_MFIE) &&
                            a->kernel == BEMPPCUDA_HELMHOLTZ_SLP && a->params[1] == 0.0 && a->params[0] > 0.0 &&
                            a->test.shapeset == BEMPPCUDA_SHAPE_RWG && a->trial.shapeset == BEMPPCUDA_SHAPE_RWG &&
                            a->test.nshape == 3 && a->trial.nshape == 3;
     if (a->precision == BEMPPCUDA_MIXED && !dp0 && !p1_mixed && !rwg_mixed) {
         bc_set_error("mixed precision is implemented for DP0 scalar kernels, the P1 single, double, adjoint "
                      "double layer and hypersingular operators (Helmholtz with Re k > 0, Laplace, modified "
-                     "Helmholtz) and the Maxwell electric field (real k), with the 6-point rule");
+                     "Helmholtz) and the Maxwell electric and magnetic fields (real k), with the 6-point rule");
         return BEMPPCUDA_ERR_UNSUPPORTED;
     }
     cudaError_t err = cudaSuccess;
@@ -689,8 +691,10 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
                           prm.ntest == prm.ntrial;
         // a complex wavenumber takes phase class 3 (exp(-Im k r) per point pair)
         const int rwg_phase = a->params[1] != 0.0 ? 3 : phase_class;
-        if (mixed && rwg_mixed)
+        if (mixed && rwg_mixed && a->assembly == BEMPPCUDA_ASM_EFIE)
             err = launch_p1_mixed<BEMPPCUDA_ASM_EFIE, BEMPPCUDA_HELMHOLTZ_SLP>(prm, rule, phase_class, rsym, st);
+        else if (mixed && rwg_mixed)
+            err = launch_p1_mixed<BEMPPCUDA_ASM_MFIE, BEMPPCUDA_HELMHOLTZ_SLP>(prm, rule, phase_class, rsym, st);
         else if (a->assembly == BEMPPCUDA_ASM_EFIE)
             err = launch_rwg<BEMPPCUDA_ASM_EFIE>(prm, rule, rwg_phase, rsym, st);
         else

@@ -5,8 +5,9 @@ operators on P1 -- Helmholtz (real and complex k), Laplace and modified
 Helmholtz -- evaluate their regular pairs in FP32 (``regular_p1_mixed``) under
 ``device_interface="cuda_mixed"``; their operator error against the FP64 path
 and the oracle is held to the mixed-precision bound (1e-6 relative
-Frobenius).  Operators without a mixed kernel (a P1 domain with a DP0 dual
-space, the Maxwell magnetic field) run in FP64 under the same interface.
+Frobenius); so do the Maxwell electric and magnetic fields on RWG / SNC.
+Operators without a mixed kernel (a P1 domain with a DP0 dual space) run in
+FP64 under the same interface.
 """
 
 import numpy as np
@@ -166,21 +167,43 @@ def test_mixed_maxwell_efie_against_fp64_and_oracle(oracle, k):
     assert (torch.linalg.norm(outs[0] - a64) / torch.linalg.norm(a64)).item() < 1e-6
 
 
-def test_mixed_interface_maxwell_mfie_is_fp64():
-    from bempp_cuda import operators
-    from bempp_cuda.shapes import regular_sphere
+@pytest.mark.parametrize("k", [1.0, 3.0, 20.0])
+def test_mixed_maxwell_mfie_against_fp64_and_oracle(oracle, k):
+    """MFIE (RWG domain, SNC dual) under cuda_mixed: the nine FP32 moments of e^{ikr}(ikr - 1)/r^3 and the
+    FP64 determinants det(P_ti - P_sj, J_t^a, J_s^b); k = 1, 3, 20 on a 512-element ellipsoid reach the three
+    phase classes.  Symmetric and per-pair sweeps agree."""
+    from cases import oracle_dense
+
+    from bempp_cuda import _lib, assembly, operators
+    from bempp_cuda.assembly import regular_into, singular_into_dense
+    from bempp_cuda.operators import Parameters
+    from bempp_cuda.shapes import ellipsoid
     from bempp_cuda.space import function_space
 
-    grid = regular_sphere(2)
+    grid = ellipsoid(3, 1.1, 0.9, 1.0)
     rwg = function_space(grid, "RWG", 0)
     snc = function_space(grid, "SNC", 0)
-    a64 = operators.boundary.maxwell.magnetic_field(rwg, rwg, snc, 2.0).weak_form().tensor
-    amx = operators.boundary.maxwell.magnetic_field(rwg, rwg, snc, 2.0, device_interface="cuda_mixed").weak_form().tensor
-    assert (torch.linalg.norm(amx - a64) / torch.linalg.norm(a64)).item() < 1e-13
+    a64 = operators.boundary.maxwell.magnetic_field(rwg, rwg, snc, k).weak_form().tensor
+    op = operators.boundary.maxwell.magnetic_field(rwg, rwg, snc, k, device_interface="cuda_mixed")
+    assembly.FP64_FALLBACKS.clear()
+    amx = op.weak_form().tensor
+    assert not assembly.FP64_FALLBACKS  # the mixed kernel ran
+    err = (torch.linalg.norm(amx - a64) / torch.linalg.norm(a64)).item()
+    assert 0.0 < err < 1e-6, err
+    assert rel_fro(amx.cpu().numpy(), oracle_dense(oracle, op, rwg, snc)) < 1e-6
+    n = rwg.global_dof_count
+    outs = []
+    for sym in (True, False):
+        a = torch.zeros((n, n), dtype=torch.complex128, device="cuda")
+        regular_into(a, op.descriptor, rwg, snc, Parameters(), precision=_lib.MIXED, symmetric=sym)
+        singular_into_dense(a, op.descriptor, rwg, snc, Parameters())
+        outs.append(a)
+    assert (torch.linalg.norm(outs[0] - outs[1]) / torch.linalg.norm(outs[1])).item() < 1e-6
+    assert (torch.linalg.norm(outs[0] - a64) / torch.linalg.norm(a64)).item() < 1e-6
 
 
 def test_operators_without_mixed_kernel_warn_and_run_fp64():
-    """cuda_mixed on an operator without a mixed-precision kernel (the Maxwell magnetic field) warns
+    """cuda_mixed on an operator without a mixed-precision kernel (a P1 domain with a DP0 dual space) warns
     once (MixedPrecisionFallback) and gives the FP64 weak form."""
     import warnings
 
@@ -189,12 +212,12 @@ def test_operators_without_mixed_kernel_warn_and_run_fp64():
     from bempp_cuda.space import function_space
 
     grid = regular_sphere(2)
-    rwg, snc = function_space(grid, "RWG", 0), function_space(grid, "SNC", 0)
+    p1, dp0 = function_space(grid, "P", 1), function_space(grid, "DP", 0)
     assembly.FP64_FALLBACKS.clear()
     with warnings.catch_warnings(record=True) as caught:
         warnings.simplefilter("always")
-        mixed = operators.boundary.maxwell.magnetic_field(rwg, rwg, snc, 2.0,
+        mixed = operators.boundary.helmholtz.single_layer(p1, p1, dp0, 2.0,
                                                           device_interface="cuda_mixed").weak_form().A
     assert any(issubclass(w.category, assembly.MixedPrecisionFallback) for w in caught)
-    fp64 = operators.boundary.maxwell.magnetic_field(rwg, rwg, snc, 2.0).weak_form().A
+    fp64 = operators.boundary.helmholtz.single_layer(p1, p1, dp0, 2.0).weak_form().A
     assert np.array_equal(mixed, fp64) or np.linalg.norm(mixed - fp64) <= 1e-15 * np.linalg.norm(fp64)
