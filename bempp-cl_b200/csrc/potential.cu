@@ -794,6 +794,155 @@ __global__ void __launch_bounds__(PS_THREADS) farfield_scalar_mixed(PotParams pr
     }
 }
 
+// Mixed-precision Maxwell far fields (maxwell_{e,m}field_far_field, numba_kernels.py:2437-2570): with
+// kv = e^{-i k x . y} / (4 pi) (k = Re k in the phase, as potential_eval evaluates it) and per source the
+// weighted basis value v (3 complex) and divergence dv,
+//   electric: u = i k V - x W,  magnetic: u = i k (x x V),  V = sum_y kv v,  W = sum_y kv dv,
+// i k with the complex wavenumber.  V and W are sums of e^{-i k x . y} against per-source coefficients,
+// split about the element centroids as in farfield_scalar_mixed: FP64 phase per (direction, element),
+// FP32 offsets, polynomials and complex products per source, FP64 sums over elements.
+// Only the magnetic field is dispatched here: in W the two triangles of each RWG function add
+// divergences of opposite sign, so neighbouring elements' contributions cancel to O(k h) and the FP32
+// rounding of each element's sum is amplified by ~1 / (k h) (6e-7 relative at 8192 elements, k = 5,
+// growing with refinement); the electric far field stays FP64.
+template <int ASM, int PHC, int NQ>
+__global__ void __launch_bounds__(PS_THREADS) farfield_maxwell_mixed(PotParams prm, int64_t chunk_elems) {
+    constexpr bool EF = ASM == BEMPPCUDA_ASM_EFIE;
+    static_assert(PS_PPT == 2, "two directions per thread, packed");
+    __shared__ float4 syo[PS_SOURCES];         // -k (y - c_e)
+    __shared__ float4 sv01[PS_SOURCES];        // v_0, v_1 (re, im)
+    __shared__ float4 sv2d[PS_SOURCES];        // v_2, dv (re, im)
+    __shared__ double scen[PS_SOURCES * 3];    // k c_e
+    const int nq = NQ > 0 ? NQ : prm.nq;
+    const int tile_elems = PS_SOURCES / nq;
+    const int64_t ebeg = (int64_t)blockIdx.y * chunk_elems;
+    const int64_t eend = min(ebeg + chunk_elems, prm.nsupport);
+    const int64_t pbase = (int64_t)blockIdx.x * (PS_THREADS * PS_PPT) + threadIdx.x;
+    const double kap = prm.p[0];
+    double x[PS_PPT][3], vr[PS_PPT][3], vi[PS_PPT][3], wr[PS_PPT], wi[PS_PPT];
+#pragma unroll
+    for (int j = 0; j < PS_PPT; ++j) {
+        const int64_t pj = min(pbase + j * PS_THREADS, prm.npoints - 1);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            x[j][d] = prm.points[3 * pj + d];
+            vr[j][d] = vi[j][d] = 0.0;
+        }
+        wr[j] = wi[j] = 0.0;
+    }
+    const float2 xx = f2((float)x[0][0], (float)x[1][0]), xy = f2((float)x[0][1], (float)x[1][1]),
+                 xz = f2((float)x[0][2], (float)x[1][2]);
+    const int64_t n = prm.nsrc;
+    const double *o = prm.src;
+    for (int64_t t0 = ebeg; t0 < eend; t0 += tile_elems) {
+        const int te = (int)min((int64_t)tile_elems, eend - t0);
+        const int ns = te * nq;
+        const int64_t s0 = t0 * nq;
+        __syncthreads();
+        for (int e = threadIdx.x; e < te; e += PS_THREADS) {
+            const int64_t el = prm.support[t0 + e];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) scen[3 * e + d] = kap * __ldg(prm.g + (22 + d) * prm.ne + el);
+        }
+        __syncthreads();
+        for (int s = threadIdx.x; s < ns; s += PS_THREADS) {
+            const int64_t gs = s0 + s;
+            const int e = s / nq;
+            syo[s] = make_float4((float)fma(-kap, o[gs], scen[3 * e]), (float)fma(-kap, o[n + gs], scen[3 * e + 1]),
+                                 (float)fma(-kap, o[2 * n + gs], scen[3 * e + 2]), 0.f);
+            sv01[s] = make_float4((float)o[6 * n + gs], (float)o[7 * n + gs], (float)o[8 * n + gs],
+                                  (float)o[9 * n + gs]);
+            sv2d[s] = make_float4((float)o[10 * n + gs], (float)o[11 * n + gs], EF ? (float)o[12 * n + gs] : 0.f,
+                                  EF ? (float)o[13 * n + gs] : 0.f);
+        }
+        __syncthreads();
+        for (int e = 0; e < te; ++e) {
+            float2 ar[3] = {b2(0.f), b2(0.f), b2(0.f)}, ai[3] = {b2(0.f), b2(0.f), b2(0.f)};
+            float2 br = b2(0.f), bi = b2(0.f);
+#pragma unroll(NQ > 0 ? NQ : 1)
+            for (int q = 0; q < nq; ++q) {
+                const float4 yo = syo[e * nq + q];
+                const float4 va = sv01[e * nq + q], vb = sv2d[e * nq + q];
+                const float2 th = fma2(xz, b2(yo.z), fma2(xy, b2(yo.y), mul2(xx, b2(yo.x))));
+                float2 sn, cs;
+                sincos2<PHC>(th, &sn, &cs);
+                const float2 msn = mul2(sn, b2(-1.f));
+                const float cre[4] = {va.x, va.z, vb.x, vb.z}, cim[4] = {va.y, va.w, vb.y, vb.w};
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    ar[d] = fma2(cs, b2(cre[d]), fma2(msn, b2(cim[d]), ar[d]));
+                    ai[d] = fma2(cs, b2(cim[d]), fma2(sn, b2(cre[d]), ai[d]));
+                }
+                if (EF) {
+                    br = fma2(cs, b2(cre[3]), fma2(msn, b2(cim[3]), br));
+                    bi = fma2(cs, b2(cim[3]), fma2(sn, b2(cre[3]), bi));
+                }
+            }
+            // times e^{i phi}, phi = -x . (k c_e)
+            float s0f, c0f, s1f, c1f;
+            phase_reduced32(-fma(x[0][2], scen[3 * e + 2], fma(x[0][1], scen[3 * e + 1], x[0][0] * scen[3 * e])),
+                            &s0f, &c0f);
+            phase_reduced32(-fma(x[1][2], scen[3 * e + 2], fma(x[1][1], scen[3 * e + 1], x[1][0] * scen[3 * e])),
+                            &s1f, &c1f);
+            const float2 cs = f2(c0f, c1f), sn = f2(s0f, s1f), msn = mul2(sn, b2(-1.f));
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const float2 pr = fma2(cs, ar[d], mul2(msn, ai[d])), pi = fma2(cs, ai[d], mul2(sn, ar[d]));
+                vr[0][d] += (double)pr.x;
+                vr[1][d] += (double)pr.y;
+                vi[0][d] += (double)pi.x;
+                vi[1][d] += (double)pi.y;
+            }
+            if (EF) {
+                const float2 pr = fma2(cs, br, mul2(msn, bi)), pi = fma2(cs, bi, mul2(sn, br));
+                wr[0] += (double)pr.x;
+                wr[1] += (double)pr.y;
+                wi[0] += (double)pi.x;
+                wi[1] += (double)pi.y;
+            }
+        }
+    }
+    // i k with the complex wavenumber, 1 / (4 pi)
+    const double ikr = -prm.p[1] * BC_INV_4PI, iki = prm.p[0] * BC_INV_4PI;
+#pragma unroll
+    for (int j = 0; j < PS_PPT; ++j) {
+        const int64_t pj = pbase + j * PS_THREADS;
+        if (pj >= prm.npoints) break;
+        double ur[3], ui[3];
+        if (EF) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                ur[d] = ikr * vr[j][d] - iki * vi[j][d] - BC_INV_4PI * x[j][d] * wr[j];
+                ui[d] = ikr * vi[j][d] + iki * vr[j][d] - BC_INV_4PI * x[j][d] * wi[j];
+            }
+        } else {
+            double cr[3], ci[3];  // x x V
+            cr[0] = x[j][1] * vr[j][2] - x[j][2] * vr[j][1];
+            cr[1] = x[j][2] * vr[j][0] - x[j][0] * vr[j][2];
+            cr[2] = x[j][0] * vr[j][1] - x[j][1] * vr[j][0];
+            ci[0] = x[j][1] * vi[j][2] - x[j][2] * vi[j][1];
+            ci[1] = x[j][2] * vi[j][0] - x[j][0] * vi[j][2];
+            ci[2] = x[j][0] * vi[j][1] - x[j][1] * vi[j][0];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                ur[d] = ikr * cr[d] - iki * ci[d];
+                ui[d] = ikr * ci[d] + iki * cr[d];
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            double *out = prm.result + 2 * (d * prm.npoints + pj);
+            if (gridDim.y == 1) {
+                out[0] = ur[d];
+                out[1] = ui[d];
+            } else {
+                atomicAdd(out, ur[d]);
+                atomicAdd(out + 1, ui[d]);
+            }
+        }
+    }
+}
+
 // Grid of the per-point kernels: point blocks x source chunks; with more than one chunk the
 // chunks add their sums with atomics into the zeroed result.  The chunk count c minimises
 //   ceil(pblocks c / slots) (1/c + 1/64),
@@ -801,7 +950,7 @@ __global__ void __launch_bounds__(PS_THREADS) farfield_scalar_mixed(PotParams pr
 // waves times the work of one CTA (1/c of its point block's sources) plus a small fixed cost
 // per CTA, so that the grid ends on a full wave rather than on a few CTAs of a second one.
 static cudaError_t scalar_grid(const PotParams &prm, const void *fn, dim3 *grid, int64_t *chunk_elems,
-                               cudaStream_t st) {
+                               cudaStream_t st, int kdim = 1) {
     int resident = 0;
     cudaError_t err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, fn, PS_THREADS, 0);
     if (err != cudaSuccess) return err;
@@ -821,7 +970,7 @@ static cudaError_t scalar_grid(const PotParams &prm, const void *fn, dim3 *grid,
     *chunk_elems = (prm.nsupport + chunks - 1) / chunks;
     chunks = (prm.nsupport + *chunk_elems - 1) / *chunk_elems;
     if (chunks > 1) {
-        err = cudaMemsetAsync(prm.result, 0, sizeof(double) * 2 * prm.npoints, st);
+        err = cudaMemsetAsync(prm.result, 0, sizeof(double) * 2 * kdim * prm.npoints, st);
         if (err != cudaSuccess) return err;
     }
     *grid = dim3((unsigned)pblocks, (unsigned)chunks);
@@ -863,6 +1012,31 @@ static cudaError_t launch_far_mixed_nq(const PotParams &prm, cudaStream_t st) {
     if (err != cudaSuccess) return err;
     fn<<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems);
     return cudaGetLastError();
+}
+
+template <int ASM, int PHC>
+static cudaError_t launch_far_maxwell_nq(const PotParams &prm, cudaStream_t st) {
+    auto fn = prm.nq == 6 ? farfield_maxwell_mixed<ASM, PHC, 6> : farfield_maxwell_mixed<ASM, PHC, 0>;
+    dim3 grid;
+    int64_t chunk_elems = 0;
+    const cudaError_t err = scalar_grid(prm, (const void *)fn, &grid, &chunk_elems, st, 3);
+    if (err != cudaSuccess) return err;
+    fn<<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems);
+    return cudaGetLastError();
+}
+
+// Mixed-precision Maxwell far fields (electric: ASM_EFIE, magnetic: ASM_MFIE).
+static cudaError_t launch_far_maxwell(const PotParams &prm, int assembly, double phase_radius, cudaStream_t st) {
+    const double kr = fabs(prm.p[0]) * phase_radius;
+    const int phc = (phase_radius > 0.0 && kr <= 0.5) ? 2 : (phase_radius > 0.0 && kr <= 1.0) ? 1 : 0;
+    if (assembly == BEMPPCUDA_ASM_EFIE) {
+        if (phc == 2) return launch_far_maxwell_nq<BEMPPCUDA_ASM_EFIE, 2>(prm, st);
+        if (phc == 1) return launch_far_maxwell_nq<BEMPPCUDA_ASM_EFIE, 1>(prm, st);
+        return launch_far_maxwell_nq<BEMPPCUDA_ASM_EFIE, 0>(prm, st);
+    }
+    if (phc == 2) return launch_far_maxwell_nq<BEMPPCUDA_ASM_MFIE, 2>(prm, st);
+    if (phc == 1) return launch_far_maxwell_nq<BEMPPCUDA_ASM_MFIE, 1>(prm, st);
+    return launch_far_maxwell_nq<BEMPPCUDA_ASM_MFIE, 0>(prm, st);
 }
 
 template <int K>
@@ -967,9 +1141,13 @@ int bc_potential_launch(const bemppcuda_potential_args *a, double *workspace, cu
           a->kernel == BEMPPCUDA_MODHELM_SLP || a->kernel == BEMPPCUDA_MODHELM_DLP ||
           a->kernel == BEMPPCUDA_FARFIELD_SLP || a->kernel == BEMPPCUDA_FARFIELD_DLP) &&
          a->params[0] > 0.0);
-    if (mixed && (maxwell || !mixed_kernel)) {
+    // Maxwell: the magnetic far field (the electric one's divergence sum cancels between neighbouring
+    // elements, which FP32 element sums do not survive; farfield_maxwell_mixed)
+    const bool maxwell_far = maxwell && a->assembly == BEMPPCUDA_ASM_MFIE && a->kernel == BEMPPCUDA_FARFIELD_SLP &&
+                             a->params[0] > 0.0;
+    if (mixed && (maxwell ? !maxwell_far : !mixed_kernel)) {
         bc_set_error("mixed-precision potentials: Laplace, Helmholtz (Re k > 0) and modified Helmholtz (w > 0) "
-                     "single / double layer potentials and Helmholtz far fields (k > 0) only");
+                     "single / double layer potentials, Helmholtz and Maxwell magnetic far fields (Re k > 0) only");
         return BEMPPCUDA_ERR_UNSUPPORTED;
     }
     // the FP64 treatment of points next to the surface needs the bound R on source offsets
@@ -991,7 +1169,9 @@ int bc_potential_launch(const bemppcuda_potential_args *a, double *workspace, cu
         const bool per_point = a->kernel == BEMPPCUDA_LAPLACE_SLP || a->kernel == BEMPPCUDA_LAPLACE_DLP ||
                                a->kernel == BEMPPCUDA_HELMHOLTZ_SLP || a->kernel == BEMPPCUDA_HELMHOLTZ_DLP ||
                                a->kernel == BEMPPCUDA_MODHELM_SLP || a->kernel == BEMPPCUDA_MODHELM_DLP;
-        if (mixed && prm.nsupport > 0) {
+        if (mixed && maxwell && prm.nsupport > 0) {
+            err = launch_far_maxwell(prm, a->assembly, a->phase_radius, st);
+        } else if (mixed && prm.nsupport > 0) {
             err = launch_scalar_mixed(prm, a->kernel, a->phase_radius, st);
         } else if (!maxwell && per_point && prm.nsupport > 0) {
             err = launch_scalar(prm, a->kernel, a->phase_radius, st);
