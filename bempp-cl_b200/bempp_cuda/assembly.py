@@ -474,9 +474,9 @@ def evaluate_potential_device(space, descriptor, points, local_coefficients, par
     (dense_potential_assembler.py:30-34); ``points`` is a (3, npoints) array.
     ``precision=MIXED`` evaluates the point-source pairs of Laplace,
     Helmholtz (real or complex k) and modified Helmholtz single / double
-    layer potentials and Helmholtz far fields in FP32; the library refuses it
-    for the Maxwell potentials and far fields, which the operator layer then
-    runs in FP64.
+    layer potentials, Helmholtz far fields and the Maxwell magnetic far field
+    in FP32; the library refuses it for the Maxwell potentials and electric
+    far field, which the operator layer then runs in FP64.
     """
     require_cuda()
     kernel, assembly = kernel_ids(descriptor)
