@@ -8,8 +8,13 @@ reference's own descriptor / space / parameter objects (duck-typed: a
 ``bempp_cl`` object and the matching ``bempp_cuda`` object both work).
 
 Precision: ``device_interface`` "cuda" is FP64 end to end; "cuda_mixed"
-evaluates regular DP0 pairs in FP32 (see csrc/regular.cu) and keeps the
-singular pairs in FP64.  Everything else in "cuda_mixed" stays FP64.
+evaluates the regular pairs in FP32 where the library has a mixed kernel
+(DP0 scalar kernels; P1 single, double, adjoint double layer and
+hypersingular operators; the Maxwell electric and magnetic fields; scalar
+potentials, Helmholtz far fields and the Maxwell magnetic far field) and
+keeps the singular pairs, per-entry sums and element-pair factors in FP64.
+Operators without a mixed kernel run in FP64 and say so once
+(``MixedPrecisionFallback``).
 """
 
 import numpy as _np
