@@ -221,3 +221,33 @@ def test_operators_without_mixed_kernel_warn_and_run_fp64():
     assert any(issubclass(w.category, assembly.MixedPrecisionFallback) for w in caught)
     fp64 = operators.boundary.helmholtz.single_layer(p1, p1, dp0, 2.0).weak_form().A
     assert np.array_equal(mixed, fp64) or np.linalg.norm(mixed - fp64) <= 1e-15 * np.linalg.norm(fp64)
+
+
+@pytest.mark.parametrize("family,name,k", [("helmholtz", "single_layer", 4.0), ("helmholtz", "double_layer", 4.0),
+                                           ("laplace", "adjoint_double_layer", None),
+                                           ("modified_helmholtz", "hypersingular", 2.0)])
+@pytest.mark.parametrize("kind", ["DP1", "P1 half sphere"])
+def test_mixed_p1_other_spaces(oracle, kind, family, name, k):
+    """The mixed P1 kernels on DP1 (no shared dofs: each warp's 96 slots are 96 columns) and on a P1 space
+    restricted to half the sphere (its boundary vertices carry zero multipliers): within 1e-6 of FP64 and
+    the oracle."""
+    from cases import oracle_dense
+
+    from bempp_cuda import assembly
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+
+    grid = regular_sphere(3)
+    if kind == "DP1":
+        sp = function_space(grid, "DP", 1)
+    else:
+        cent = grid.vertices[:, grid.elements].mean(axis=1)
+        sp = function_space(grid, "P", 1, support_elements=np.flatnonzero(cent[2] > 0.0))
+    path = family + "." + name
+    a64 = _op(path, sp, k, "cuda").weak_form().tensor
+    assembly.FP64_FALLBACKS.clear()
+    amx = _op(path, sp, k, "cuda_mixed").weak_form().tensor
+    assert not assembly.FP64_FALLBACKS  # a mixed kernel ran
+    err = (torch.linalg.norm(amx - a64) / torch.linalg.norm(a64)).item()
+    assert 0.0 < err < 1e-6, err
+    assert rel_fro(amx.cpu().numpy(), oracle_dense(oracle, _op(path, sp, k, "cuda"), sp, sp)) < 1e-6
