@@ -1360,8 +1360,43 @@ def _case_p1_mixed_dlp(torch, args=None):
     return (lambda: regular_into(out, op.descriptor, sp, sp, op.parameters, precision=_lib.MIXED)), out.numel() * 16
 
 
+def _points_case(torch, path, k, directions):
+    """A mixed-precision potential or far field of P1 coefficients on regular_sphere(5) at 10 000 seeded points
+    (the shell 1.5 < r < 3) or directions, inputs on the device."""
+    from bempp_cuda import _lib, operators
+    from bempp_cuda.assembly import evaluate_potential_device
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+
+    sp = function_space(regular_sphere(5), "P", 1)
+    rng = np.random.default_rng(1)
+    dirs = rng.standard_normal((3, 10000))
+    dirs /= np.linalg.norm(dirs, axis=0)
+    pts = dirs if directions else dirs * (1.5**3 + rng.random(10000) * (3.0**3 - 1.5**3)) ** (1.0 / 3.0)
+    f = operators
+    for part in path.split("."):
+        f = getattr(f, part)
+    op = f(sp, pts, k)
+    coeffs = rng.standard_normal(sp.global_dof_count) + 1j * rng.standard_normal(sp.global_dof_count)
+    local = torch.as_tensor(sp.map_to_full_grid @ coeffs, device="cuda")
+    pdev = torch.as_tensor(np.ascontiguousarray(pts.T), device="cuda")
+    return (lambda: evaluate_potential_device(sp, op.descriptor, pdev, local, op.parameters,
+                                              precision=_lib.MIXED)), 0
+
+
+def _case_potential_mixed(torch, args=None):
+    """The mixed Helmholtz single-layer potential, 10 000 points, P1 on regular_sphere(5), k = 5."""
+    return _points_case(torch, "potential.helmholtz.single_layer", 5.0, False)
+
+
+def _case_farfield_mixed(torch, args=None):
+    """The mixed Helmholtz single-layer far field, 10 000 directions, P1 on regular_sphere(5), k = 5."""
+    return _points_case(torch, "far_field.helmholtz.single_layer", 5.0, True)
+
+
 PROFILE_CASES = {"matmat_3x8192": _case_matmat, "gemv_16384": _case_gemv, "mixed_sym_l5": _case_mixed_sym,
-                 "apply_l5": _case_apply, "p1_mixed_dlp_l5": _case_p1_mixed_dlp}
+                 "apply_l5": _case_apply, "p1_mixed_dlp_l5": _case_p1_mixed_dlp,
+                 "potential_mixed_l5": _case_potential_mixed, "farfield_mixed_l5": _case_farfield_mixed}
 
 
 def profile_case(args):
