@@ -1345,19 +1345,40 @@ def _case_apply(torch, args=None):
     return (lambda: apply_regular(y, x, desc, sp, sp, prm)), 0
 
 
-def _case_p1_mixed_dlp(torch, args=None):
-    """The mixed Helmholtz double layer on P1 of regular_sphere(5), k = 5: the skew sweep's regular pass,
-    added into a 4098 x 4098 complex128 matrix (269 MB)."""
-    from bempp_cuda import _lib, operators
+def _p1_case(torch, name, precision):
+    """The regular pass of a Helmholtz operator on P1 of regular_sphere(5), k = 5, added into a 4098 x 4098
+    complex128 matrix (269 MB)."""
+    from bempp_cuda import operators
     from bempp_cuda.assembly import regular_into
     from bempp_cuda.shapes import regular_sphere
     from bempp_cuda.space import function_space
 
     sp = function_space(regular_sphere(5), "P", 1)
-    op = operators.boundary.helmholtz.double_layer(sp, sp, sp, 5.0, device_interface="cuda_mixed")
+    op = getattr(operators.boundary.helmholtz, name)(sp, sp, sp, 5.0)
     n = sp.global_dof_count
     out = torch.zeros((n, n), dtype=torch.complex128, device="cuda")
-    return (lambda: regular_into(out, op.descriptor, sp, sp, op.parameters, precision=_lib.MIXED)), out.numel() * 16
+    return (lambda: regular_into(out, op.descriptor, sp, sp, op.parameters, precision=precision)), out.numel() * 16
+
+
+def _case_p1_mixed_dlp(torch, args=None):
+    """The mixed Helmholtz double layer on P1 of regular_sphere(5), k = 5 (the skew sweep)."""
+    from bempp_cuda import _lib
+
+    return _p1_case(torch, "double_layer", _lib.MIXED)
+
+
+def _case_p1_fp64_dlp(torch, args=None):
+    """The FP64 Helmholtz double layer on P1 of regular_sphere(5), k = 5 (the skew sweep)."""
+    from bempp_cuda import _lib
+
+    return _p1_case(torch, "double_layer", _lib.FP64)
+
+
+def _case_p1_fp64_slp(torch, args=None):
+    """The FP64 Helmholtz single layer on P1 of regular_sphere(5), k = 5 (the symmetric sweep)."""
+    from bempp_cuda import _lib
+
+    return _p1_case(torch, "single_layer", _lib.FP64)
 
 
 def _points_case(torch, path, k, directions):
@@ -1395,7 +1416,8 @@ def _case_farfield_mixed(torch, args=None):
 
 
 PROFILE_CASES = {"matmat_3x8192": _case_matmat, "gemv_16384": _case_gemv, "mixed_sym_l5": _case_mixed_sym,
-                 "apply_l5": _case_apply, "p1_mixed_dlp_l5": _case_p1_mixed_dlp,
+                 "apply_l5": _case_apply, "p1_mixed_dlp_l5": _case_p1_mixed_dlp, "p1_fp64_dlp_l5": _case_p1_fp64_dlp,
+                 "p1_fp64_slp_l5": _case_p1_fp64_slp,
                  "potential_mixed_l5": _case_potential_mixed, "farfield_mixed_l5": _case_farfield_mixed}
 
 
