@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
     }
     // (y_q - v0_s).n_s, the split of the double-layer normal term about the trial vertex 0
     double ynv[NQ6];
-    if (DL || SKEW)
+    if (DL && !SKEW)
 #pragma unroll
         for (int q = 0; q < NQ6; ++q)
             ynv[q] = fma(y[q][2] - gs.v0[2], gs.n[2], fma(y[q][1] - gs.v0[1], gs.n[1], (y[q][0] - gs.v0[0]) * gs.n[0]));
@@ -140,6 +140,16 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
         if (SYM && t0 + tt >= si) break;  // rows increase with tt
         if (prm.grids_identical && shares_vertex(sb.v[tt], sv0, sv1, sv2)) continue;
         const int64_t t = prm.tsup[t0 + tt];
+        // SKEW: the normal factors by the plane property (a quadrature point lies in its own element's
+        // plane): (y_q - x_p).n_s = (v0_s - x_p).n_s, one value per test point (xn below), and
+        // (x_p - y_q).n_t = (c_t - y_q).n_t, one value per trial point
+        double mdt[SKEW ? NQ6 : 1];
+        if (SKEW)
+#pragma unroll
+            for (int q = 0; q < NQ6; ++q)
+                mdt[q % (SKEW ? NQ6 : 1)] =
+                    fma(sb.c[tt][2] - y[q][2], sb.n[tt][2],
+                        fma(sb.c[tt][1] - y[q][1], sb.n[tt][1], (sb.c[tt][0] - y[q][0]) * sb.n[tt][0]));
         double rc = 0.0, krc = 0.0, ph_s = 0.0, ph_c = 1.0;
         if (PH) {
             const double D0 = sc[0] - sb.c[tt][0], D1 = sc[1] - sb.c[tt][1], D2 = sc[2] - sb.c[tt][2];
@@ -177,9 +187,6 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
                 double kre, kim = 0.0;  // kernel value without 1/(4 pi)
                 double k2re = 0.0, k2im = 0.0;  // SKEW: the transposed pair's kernel
                 if (SKEW) {
-                    // dS = d . n_trial (split about the trial vertex 0), dT = d . n_test
-                    const double dS = ynv[q] + xn;
-                    const double dT = fma(d2, sb.n[tt][2], fma(d1, sb.n[tt][1], d0 * sb.n[tt][0]));
                     double hre, him;  // double layer of trial normal n: (dot with n) (hre + i him)
                     if (!HELM) {
                         hre = -rinv * rinv * rinv;
@@ -202,16 +209,16 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
                             sn *= am;
                             cs *= am;
                         }
-                        const double rinv2 = rinv * rinv, rk = rinv + ki;
+                        const double rinv2 = rinv * rinv, rk = CK ? rinv + ki : rinv;
                         hre = -rinv2 * fma(rk, cs, kr * sn);
                         him = rinv2 * fma(kr, cs, -rk * sn);
                     }
-                    // the double layer of (test, trial) uses the trial normal; its transpose the test normal
-                    const double a1 = DL ? dS : -dT, a2 = DL ? -dT : dS;
-                    kre = a1 * hre;
-                    kim = a1 * him;
-                    k2re = a2 * hre;
-                    k2im = a2 * him;
+                    // h alone (its trial-normal factor xn is applied per test point), and h times the
+                    // test-normal factor of this trial point
+                    kre = hre;
+                    kim = him;
+                    k2re = mdt[q % (SKEW ? NQ6 : 1)] * hre;
+                    k2im = mdt[q % (SKEW ? NQ6 : 1)] * him;
                 } else if (!HELM) {
                     if (K == BEMPPCUDA_LAPLACE_SLP) {
                         kre = rinv;
@@ -267,18 +274,28 @@ __global__ void __launch_bounds__(DP0_THREADS, BC_P1_MIN_BLOCKS) regular_p1(RegP
             const double wp = rule.w[p];
             const auto phw = [&](int i) -> double { return NT == 1 ? wp : rule.sw[p][i]; };
 #pragma unroll
-            for (int i = 0; i < NT; ++i)
+            for (int i = 0; i < NT; ++i) {
+                // SKEW: the sums of h take the trial-normal factor xn of this test point; they form the
+                // (i, j) block of the double layer and the transposed block of the adjoint double layer
+                const double px = SKEW ? phw(i) * xn : phw(i);
 #pragma unroll
                 for (int j = 0; j < NS; ++j) {
-                    lre[i][j] = fma(phw(i), tre[j], lre[i][j]);
-                    lim[i][j] = fma(phw(i), tim[j], lim[i][j]);
-                    if (SKEW) {
-                        ure[i % (SKEW ? NT : 1)][j % (SKEW ? NS : 1)] =
-                            fma(phw(i), vre[j % (SKEW ? NS : 1)], ure[i % (SKEW ? NT : 1)][j % (SKEW ? NS : 1)]);
-                        uim[i % (SKEW ? NT : 1)][j % (SKEW ? NS : 1)] =
-                            fma(phw(i), vim[j % (SKEW ? NS : 1)], uim[i % (SKEW ? NT : 1)][j % (SKEW ? NS : 1)]);
+                    if (!SKEW) {
+                        lre[i][j] = fma(phw(i), tre[j], lre[i][j]);
+                        lim[i][j] = fma(phw(i), tim[j], lim[i][j]);
+                    } else {
+                        constexpr int a = SKEW ? NT : 1, b = SKEW ? NS : 1;
+                        // (weight, sum) of the (i, j) block and of the transposed pair's block
+                        const double w1 = DL ? px : phw(i), w2 = DL ? phw(i) : px;
+                        const double s1r = DL ? tre[j] : vre[j % b], s1i = DL ? tim[j] : vim[j % b];
+                        const double s2r = DL ? vre[j % b] : tre[j], s2i = DL ? vim[j % b] : tim[j];
+                        lre[i][j] = fma(w1, s1r, lre[i][j]);
+                        lim[i][j] = fma(w1, s1i, lim[i][j]);
+                        ure[i % a][j % b] = fma(w2, s2r, ure[i % a][j % b]);
+                        uim[i % a][j % b] = fma(w2, s2i, uim[i % a][j % b]);
                     }
                 }
+            }
             if (HYP)
 #pragma unroll
                 for (int j = 0; j < NS; ++j) {
