@@ -717,6 +717,10 @@ __global__ void __launch_bounds__(PS_THREADS) farfield_scalar_mixed(PotParams pr
     }
     const float2 xx = f2((float)x[0][0], (float)x[1][0]), xy = f2((float)x[0][1], (float)x[1][1]),
                  xz = f2((float)x[0][2], (float)x[1][2]);
+    // the phase class bounds |theta| <= k R for unit directions; a longer direction takes the reduced
+    // polynomials, which hold for any argument
+    const bool unit = fmax(fma(x[0][2], x[0][2], fma(x[0][1], x[0][1], x[0][0] * x[0][0])),
+                           fma(x[1][2], x[1][2], fma(x[1][1], x[1][1], x[1][0] * x[1][0]))) <= 1.0 + 1e-6;
     const int64_t n = prm.nsrc;
     const double *o = prm.src;
     for (int64_t t0 = ebeg; t0 < eend; t0 += tile_elems) {
@@ -750,7 +754,10 @@ __global__ void __launch_bounds__(PS_THREADS) farfield_scalar_mixed(PotParams pr
                 const float4 cf = scf[e * nq + q];
                 const float2 th = fma2(xz, b2(yo.z), fma2(xy, b2(yo.y), mul2(xx, b2(yo.x))));
                 float2 sn, cs;
-                sincos2<PHC>(th, &sn, &cs);
+                if (unit)
+                    sincos2<PHC>(th, &sn, &cs);
+                else
+                    sincos2<0>(th, &sn, &cs);
                 const float2 cr = b2(cf.x), ci = b2(cf.y);
                 er = fma2(cs, cr, fma2(sn, b2(cf.z), er));  // cf.z = -im, exact
                 ei = fma2(cs, ci, fma2(sn, cr, ei));
@@ -832,6 +839,10 @@ __global__ void __launch_bounds__(PS_THREADS) farfield_maxwell_mixed(PotParams p
     }
     const float2 xx = f2((float)x[0][0], (float)x[1][0]), xy = f2((float)x[0][1], (float)x[1][1]),
                  xz = f2((float)x[0][2], (float)x[1][2]);
+    // the phase class bounds |theta| <= k R for unit directions; a longer direction takes the reduced
+    // polynomials, which hold for any argument
+    const bool unit = fmax(fma(x[0][2], x[0][2], fma(x[0][1], x[0][1], x[0][0] * x[0][0])),
+                           fma(x[1][2], x[1][2], fma(x[1][1], x[1][1], x[1][0] * x[1][0]))) <= 1.0 + 1e-6;
     const int64_t n = prm.nsrc;
     const double *o = prm.src;
     for (int64_t t0 = ebeg; t0 < eend; t0 += tile_elems) {
@@ -865,7 +876,10 @@ __global__ void __launch_bounds__(PS_THREADS) farfield_maxwell_mixed(PotParams p
                 const float4 va = sv01[e * nq + q], vb = sv2d[e * nq + q];
                 const float2 th = fma2(xz, b2(yo.z), fma2(xy, b2(yo.y), mul2(xx, b2(yo.x))));
                 float2 sn, cs;
-                sincos2<PHC>(th, &sn, &cs);
+                if (unit)
+                    sincos2<PHC>(th, &sn, &cs);
+                else
+                    sincos2<0>(th, &sn, &cs);
                 const float2 msn = mul2(sn, b2(-1.f));
                 const float cre[4] = {va.x, va.z, vb.x, vb.z}, cim[4] = {va.y, va.w, vb.y, vb.w};
 #pragma unroll
@@ -1025,15 +1039,10 @@ static cudaError_t launch_far_maxwell_nq(const PotParams &prm, cudaStream_t st) 
     return cudaGetLastError();
 }
 
-// Mixed-precision Maxwell far fields (electric: ASM_EFIE, magnetic: ASM_MFIE).
-static cudaError_t launch_far_maxwell(const PotParams &prm, int assembly, double phase_radius, cudaStream_t st) {
+// Mixed-precision Maxwell magnetic far field (the electric one stays FP64: farfield_maxwell_mixed).
+static cudaError_t launch_far_maxwell(const PotParams &prm, double phase_radius, cudaStream_t st) {
     const double kr = fabs(prm.p[0]) * phase_radius;
     const int phc = (phase_radius > 0.0 && kr <= 0.5) ? 2 : (phase_radius > 0.0 && kr <= 1.0) ? 1 : 0;
-    if (assembly == BEMPPCUDA_ASM_EFIE) {
-        if (phc == 2) return launch_far_maxwell_nq<BEMPPCUDA_ASM_EFIE, 2>(prm, st);
-        if (phc == 1) return launch_far_maxwell_nq<BEMPPCUDA_ASM_EFIE, 1>(prm, st);
-        return launch_far_maxwell_nq<BEMPPCUDA_ASM_EFIE, 0>(prm, st);
-    }
     if (phc == 2) return launch_far_maxwell_nq<BEMPPCUDA_ASM_MFIE, 2>(prm, st);
     if (phc == 1) return launch_far_maxwell_nq<BEMPPCUDA_ASM_MFIE, 1>(prm, st);
     return launch_far_maxwell_nq<BEMPPCUDA_ASM_MFIE, 0>(prm, st);
@@ -1170,7 +1179,7 @@ int bc_potential_launch(const bemppcuda_potential_args *a, double *workspace, cu
                                a->kernel == BEMPPCUDA_HELMHOLTZ_SLP || a->kernel == BEMPPCUDA_HELMHOLTZ_DLP ||
                                a->kernel == BEMPPCUDA_MODHELM_SLP || a->kernel == BEMPPCUDA_MODHELM_DLP;
         if (mixed && maxwell && prm.nsupport > 0) {
-            err = launch_far_maxwell(prm, a->assembly, a->phase_radius, st);
+            err = launch_far_maxwell(prm, a->phase_radius, st);
         } else if (mixed && prm.nsupport > 0) {
             err = launch_scalar_mixed(prm, a->kernel, a->phase_radius, st);
         } else if (!maxwell && per_point && prm.nsupport > 0) {

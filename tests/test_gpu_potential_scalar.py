@@ -371,3 +371,24 @@ def test_mixed_far_fields(oracle, family, name, kr):
     assert not assembly.FP64_FALLBACKS  # the mixed kernel ran
     ref = _check(oracle, f(space, dirs, k), space)
     assert 0.0 < rel_fro(got, ref) < 1e-6
+
+
+@pytest.mark.parametrize("scale", [3.0, 0.5])
+def test_mixed_far_field_non_unit_directions(oracle, scale):
+    """Directions scaled away from unit length: the mixed far field leaves the phase-class polynomials
+    (whose range assumes |x| <= 1) for the reduced ones and stays within 1e-6 of the oracle and FP64."""
+    from bempp_cuda import operators
+    from bempp_cuda.device import device_grid
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+
+    grid = regular_sphere(3)
+    space = function_space(grid, "P", 1)
+    rng = np.random.default_rng(23)
+    dirs = rng.standard_normal((3, 700))
+    dirs = scale * dirs / np.linalg.norm(dirs, axis=0)
+    k = 0.4 / device_grid(grid).radius  # k R = 0.4: the short polynomials for unit directions
+    f = operators.far_field.helmholtz.double_layer
+    got = _check(oracle, f(space, dirs, k, device_interface="cuda_mixed"), space, tol=1e-6)
+    ref = _check(oracle, f(space, dirs, k), space)
+    assert rel_fro(got, ref) < 1e-6
