@@ -317,12 +317,19 @@ __device__ __forceinline__ void sincos2_sym(float2 x, float2 *s, float2 *c) {
 // w_b for 3-5, the order-4 rule): the FP32 sums of the first orbit are scaled
 // by w_a / w_b when the second begins, and everything is converted to FP64
 // once, times w_b.
-template <int K, int PHC, bool STRIPE = false>
+// CK: a complex wavenumber k = kr + i ki in units of 1/kr: the amplitude e^{-beta r'} (beta = ki / kr)
+// split like the phase, e^{-beta theta} per point pair by __expf and e^{-beta r_c'} per element pair by
+// exp_neg_reduced; the double-layer factor (i k r - 1) = -(1 + beta r') + i r' turns 1 / r' into
+// 1 / r' + beta in h1 and h2.
+template <int K, int PHC, bool STRIPE = false, bool CK = false>
 __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm, const QuadRule &rule,
                                                          int64_t tile_x, int64_t t0, int rows, TestBlock32q &sb) {
     using ST = SymTraits<K>;
+    static_assert(!CK || ST::helm, "complex wavenumber: the Helmholtz kernels");
     constexpr int NP = NQ6 / 2;
-    const double kap = ST::helm ? prm.p[0] : 1.0;  // callers guarantee k > 0 for the Helmholtz family
+    const double kap = ST::helm ? prm.p[0] : 1.0;  // callers guarantee Re k > 0 for the Helmholtz family
+    const double betd = CK ? prm.p[1] / prm.p[0] : 0.0;
+    const float2 bet2 = b2((float)betd);
     const int tcount = (int)min((int64_t)rows, prm.ntest - t0);
     for (int idx = threadIdx.x; idx < tcount; idx += blockDim.x) {
         const int64_t t = prm.tsup[t0 + idx];
@@ -399,6 +406,7 @@ __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm,
             const double rc = rc2 * rsqrt64(rc2);
             float ph_s = 0.f, ph_c = 1.f;
             if (ST::helm) phase_reduced32(rc, &ph_s, &ph_c);
+            const double amp = CK ? exp_neg_reduced(betd * rc) : 1.0;  // e^{-beta r_c'}
             const float D0f = (float)D0, D1f = (float)D1, D2f = (float)D2;
             const float2 rcf2 = b2((float)rc), rc2f2 = b2((float)rc2);
             // k (y - x).n_j = cp_p (y lies in the plane of j, so (y - c_j).n_j = 0) and
@@ -455,14 +463,20 @@ __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm,
                         const float2 th = mul2(sdot, f2(rcp_approx(den.x), rcp_approx(den.y)));
                         float2 sn, cs;
                         sincos2_sym<PHC>(th, &sn, &cs);
+                        if (CK) {
+                            const float2 am = f2(__expf(-bet2.x * th.x), __expf(-bet2.x * th.y));
+                            cs = mul2(cs, am);
+                            sn = mul2(sn, am);
+                        }
                         if (ST::slp_part) {
                             s0r = fma2(f, cs, s0r);
                             s0i = fma2(f, sn, s0i);
                         }
                         if (ST::dlp_part) {
                             const float2 fr = mul2(f, rinv);
-                            const float2 h1 = fma2(rinv, cs, sn);
-                            const float2 h2 = fma2(f2(-rinv.x, -rinv.y), sn, cs);
+                            const float2 rb = CK ? add2(rinv, bet2) : rinv;  // 1 / r' (+ beta)
+                            const float2 h1 = fma2(rb, cs, sn);
+                            const float2 h2 = fma2(f2(-rb.x, -rb.y), sn, cs);
                             const float2 gt = mul2(fr, ynt[j]);
                             pur = fma2(fr, h1, pur);
                             pui = fma2(fr, h2, pui);
@@ -503,7 +517,7 @@ __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm,
                 b_re = sr + er;
                 b_im = sim + ei;
             }
-            const double scale = BC_INV_4PI * sb.ie[tt] * gs.ie * wb;
+            const double scale = BC_INV_4PI * sb.ie[tt] * gs.ie * wb * amp;
             const double pc = (double)ph_c, ps = (double)ph_s;
             double tr = a_re * pc - a_im * ps;
             a_im = (a_re * ps + a_im * pc) * scale;

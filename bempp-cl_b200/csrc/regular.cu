@@ -252,15 +252,39 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_dp0_fp64_sym(RegParams pr
 #define BC_MSYM_MIN_BLOCKS 3
 #endif
 
-template <int K, int PHC, bool STRIPE = false>
+template <int K, int PHC, bool STRIPE = false, bool CK = false>
 __global__ void __launch_bounds__(DP0_THREADS, BC_MSYM_MIN_BLOCKS) regular_dp0_mixed_sym(RegParams prm, QuadRule rule,
                                                                                       int64_t row0, int64_t row1,
                                                                                       int tile_rows) {
     const int64_t t0 = row0 + (int64_t)blockIdx.y * tile_rows;
     if (t0 >= ((int64_t)blockIdx.x + 1) * DP0_THREADS) return;
     __shared__ TestBlock32q sb;
-    regular_dp0_mixed_sym_tile<K, PHC, STRIPE>(prm, rule, blockIdx.x, t0, (int)min((int64_t)tile_rows, row1 - t0),
-                                               sb);
+    regular_dp0_mixed_sym_tile<K, PHC, STRIPE, CK>(prm, rule, blockIdx.x, t0,
+                                                   (int)min((int64_t)tile_rows, row1 - t0), sb);
+}
+
+// The mixed symmetric sweep in its phase class, real or (Helmholtz) complex wavenumber.
+template <int K, bool STRIPE, bool CK>
+static void mixed_sym_phase(const RegParams &prm, const QuadRule &rule, int phase_class, int64_t row0, int64_t row1,
+                            int tile_rows, dim3 sgrid, cudaStream_t st) {
+    if (phase_class == 2)
+        regular_dp0_mixed_sym<K, 2, STRIPE, CK><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
+    else if (phase_class == 1)
+        regular_dp0_mixed_sym<K, 1, STRIPE, CK><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
+    else
+        regular_dp0_mixed_sym<K, 0, STRIPE, CK><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
+}
+
+template <int K, bool STRIPE>
+static void launch_mixed_sym(const RegParams &prm, const QuadRule &rule, int phase_class, int64_t row0, int64_t row1,
+                             int tile_rows, dim3 sgrid, cudaStream_t st) {
+    if constexpr (KernelTraits<K>::helm) {
+        if (prm.p[1] != 0.0) {
+            mixed_sym_phase<K, STRIPE, true>(prm, rule, phase_class, row0, row1, tile_rows, sgrid, st);
+            return;
+        }
+    }
+    mixed_sym_phase<K, STRIPE, false>(prm, rule, phase_class, row0, row1, tile_rows, sgrid, st);
 }
 
 // Kernels with a stripe-mode instance (the multi-GPU symmetric stripes): the Helmholtz family, the
@@ -277,12 +301,7 @@ static cudaError_t launch_dp0_stripe(const RegParams &prm, const QuadRule &rule,
                                      int64_t row0, int64_t row1, int tile_rows, dim3 sgrid, cudaStream_t st) {
     if constexpr (stripe_kernel<K>()) {
         if (mixed) {
-            if (phase_class == 2)
-                regular_dp0_mixed_sym<K, 2, true><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
-            else if (phase_class == 1)
-                regular_dp0_mixed_sym<K, 1, true><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
-            else
-                regular_dp0_mixed_sym<K, 0, true><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
+            launch_mixed_sym<K, true>(prm, rule, phase_class, row0, row1, tile_rows, sgrid, st);
         } else if (!KernelTraits<K>::helm) {
             regular_dp0_fp64_sym<K, 0, true><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
         } else if (prm.p[1] != 0.0) {
@@ -305,13 +324,12 @@ static cudaError_t launch_dp0(const RegParams &prm, const QuadRule &rule, int mi
                               int64_t row0, int64_t row1, cudaStream_t st) {
     dim3 grid((unsigned)((prm.ntrial + DP0_THREADS - 1) / DP0_THREADS), (unsigned)((prm.ntest + DP0_TCHUNK - 1) / DP0_TCHUNK));
     if constexpr (SymTraits<K>::supported) {
-        // same DP0 space on both sides; the mixed tiles need a real wavenumber k > 0 (scaled units),
-        // the FP64 tiles take a complex one as phase class 3
+        // same DP0 space on both sides; the mixed tiles need Re k > 0 (scaled units; a complex k adds
+        // the amplitude split), the FP64 tiles take a complex k as phase class 3
         // (modified Helmholtz: FP64 only)
         const bool helm = KernelTraits<K>::helm;
         const bool ck_sym = helm && prm.p[1] != 0.0;
-        const bool sweep_ok = helm ? (!mixed || (prm.p[1] == 0.0 && prm.p[0] > 0.0))
-                                   : !(KernelTraits<K>::modhelm && mixed);
+        const bool sweep_ok = helm ? (!mixed || prm.p[0] > 0.0) : !(KernelTraits<K>::modhelm && mixed);
         if (sym && sweep_ok) {
             // rows per tile: 32, or 16 / 8 when 32-row tiles would leave the GPU under four waves of
             // working CTAs (about half the tiles lie below the diagonal and exit; 3 CTAs per SM)
@@ -323,12 +341,7 @@ static cudaError_t launch_dp0(const RegParams &prm, const QuadRule &rule, int mi
             if (prm.tresult) return launch_dp0_stripe<K>(prm, rule, mixed, phase_class, row0, row1, tile_rows, sgrid, st);
             if constexpr (!KernelTraits<K>::modhelm) {
                 if (mixed) {
-                    if (phase_class == 2)
-                        regular_dp0_mixed_sym<K, 2><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
-                    else if (phase_class == 1)
-                        regular_dp0_mixed_sym<K, 1><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
-                    else
-                        regular_dp0_mixed_sym<K, 0><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
+                    launch_mixed_sym<K, false>(prm, rule, phase_class, row0, row1, tile_rows, sgrid, st);
                     return cudaGetLastError();
                 }
             }
@@ -638,8 +651,7 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
                             a->kernel == BEMPPCUDA_HELMHOLTZ_DLP || a->kernel == BEMPPCUDA_HELMHOLTZ_ADLP ||
                             a->kernel == BEMPPCUDA_HELMHOLTZ_COMBINED;
     const bool sym_ok = sym && sym_kernel &&
-                        (laplace || a->precision != BEMPPCUDA_MIXED ||
-                         (!modhelm && a->params[1] == 0.0 && a->params[0] > 0.0));
+                        (laplace || a->precision != BEMPPCUDA_MIXED || (!modhelm && a->params[0] > 0.0));
     if (ranged && (!sym_ok || a->row_begin < 0 || a->row_end > prm.ntest || a->row_begin >= a->row_end)) {
         bc_set_error("row range [%lld, %lld) needs the symmetric sweep and 0 <= begin < end <= %lld rows",
                      (long long)a->row_begin, (long long)a->row_end, (long long)prm.ntest);

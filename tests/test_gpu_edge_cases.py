@@ -73,12 +73,15 @@ def test_mismatched_sizes_and_row_ranges_are_rejected():
         with pytest.raises(_lib.BemppCudaError) as exc:
             regular_into(out, d, sp, sp, Parameters(), overwrite=True, rows=rows)
         assert exc.value.status == _lib.ERR_INVALID
-    # a row range needs the symmetric sweep: the mixed tiles have none for a complex wavenumber ->
-    # rejected, not ignored; the FP64 tiles sweep complex wavenumbers (phase class 3) -> accepted
-    dc = operators.boundary.helmholtz.single_layer(sp, sp, sp, 3.0 + 0.5j).descriptor
+    # a row range needs the symmetric sweep: the mixed tiles have none for modified Helmholtz ->
+    # rejected, not ignored; complex wavenumbers sweep in both precisions -> accepted
+    dm = operators.boundary.modified_helmholtz.single_layer(sp, sp, sp, 2.0).descriptor
+    real_out = torch.empty((n, n), dtype=torch.float64, device="cuda")
     with pytest.raises(_lib.BemppCudaError) as exc:
-        regular_into(out, dc, sp, sp, Parameters(), precision=_lib.MIXED, overwrite=True, rows=(0, 8))
+        regular_into(real_out, dm, sp, sp, Parameters(), precision=_lib.MIXED, overwrite=True, rows=(0, 8))
     assert exc.value.status == _lib.ERR_INVALID
+    dc = operators.boundary.helmholtz.single_layer(sp, sp, sp, 3.0 + 0.5j).descriptor
+    regular_into(out, dc, sp, sp, Parameters(), precision=_lib.MIXED, overwrite=True, rows=(0, 8))
     regular_into(out, dc, sp, sp, Parameters(), overwrite=True, rows=(0, 8))
     _usable()
 

@@ -23,11 +23,13 @@ KERNELS = [
     ("helmholtz_adjoint_double_layer", [4.0, 0.0]),
     ("helmholtz_combined_field", [7.0, 0.0, 0.0, -7.0]),
     ("helmholtz_combined_field", [40.0, 0.0, 1.5, -40.0]),  # |k| (R_i + R_j) > 1: reduced phase
-    # complex wavenumbers: the FP64 sweep as phase class 3 (the mixed path runs per pair)
+    # complex wavenumbers: the FP64 sweep as phase class 3, the mixed sweep with the amplitude e^{-beta r'}
+    # split about the centroids (the last case: |k| (R_i + R_j) > 1 and a strong damping)
     ("helmholtz_single_layer", [4.0, 0.7]),
     ("helmholtz_double_layer", [4.0, 0.7]),
     ("helmholtz_adjoint_double_layer", [4.0, 0.7]),
     ("helmholtz_combined_field", [7.0, 0.5, 0.0, -7.0]),
+    ("helmholtz_combined_field", [30.0, 9.0, 1.0, -30.0]),
     # modified Helmholtz (real kernel; FP64 sweep, the mixed path runs per pair)
     ("modified_helmholtz_single_layer", [2.0]),
     ("modified_helmholtz_double_layer", [2.0]),
