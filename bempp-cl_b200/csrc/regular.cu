@@ -295,7 +295,7 @@ constexpr bool stripe_kernel() {
            K == BEMPPCUDA_HELMHOLTZ_COMBINED || K == BEMPPCUDA_LAPLACE_SLP;
 }
 
-// The symmetric sweep of launch_dp0 in stripe mode (real wavenumber; mixed or FP64).
+// The symmetric sweep of launch_dp0 in stripe mode (real or complex wavenumber; mixed or FP64).
 template <int K>
 static cudaError_t launch_dp0_stripe(const RegParams &prm, const QuadRule &rule, int mixed, int phase_class,
                                      int64_t row0, int64_t row1, int tile_rows, dim3 sgrid, cudaStream_t st) {
