@@ -66,27 +66,40 @@ __device__ __forceinline__ void run_tile(const BatchDev &P, const QuadRule &rule
     }
 }
 
-// Symmetric sweep of one problem (real k; k > 0 on the mixed path): tile
-// (tx, ty) = columns [128 tx, 128 tx + 128) x rows [rows ty, rows ty + rows).
+// Symmetric sweep of one problem (Re k > 0 on the mixed path; a complex k is phase class 3 of the FP64
+// tile and the amplitude split of the mixed one): tile (tx, ty) = columns [128 tx, 128 tx + 128) x rows
+// [rows ty, rows ty + rows).
 template <int K>
 __device__ __forceinline__ void run_tile_sym(const BatchDev &P, const QuadRule &rule, int64_t tx, int64_t ty,
                                              TileShared &sh) {
     const int64_t t0 = ty * P.rows;
     const int rows = P.rows;
     if (P.precision == BEMPPCUDA_FP64) {
-        if (P.phase_class == 2)
+        if (KernelTraits<K>::helm && P.ck)
+            regular_dp0_fp64_sym_tile<K, 3>(P.prm, rule, tx, t0, rows, sh.b64s);
+        else if (P.phase_class == 2)
             regular_dp0_fp64_sym_tile<K, 2>(P.prm, rule, tx, t0, rows, sh.b64s);
         else if (P.phase_class == 1)
             regular_dp0_fp64_sym_tile<K, 1>(P.prm, rule, tx, t0, rows, sh.b64s);
         else
             regular_dp0_fp64_sym_tile<K, 0>(P.prm, rule, tx, t0, rows, sh.b64s);
-    } else {
-        if (P.phase_class == 2)
+    } else if constexpr (KernelTraits<K>::helm) {
+        if (P.ck) {
+            if (P.phase_class == 2)
+                regular_dp0_mixed_sym_tile<K, 2, false, true>(P.prm, rule, tx, t0, rows, sh.b32q);
+            else if (P.phase_class == 1)
+                regular_dp0_mixed_sym_tile<K, 1, false, true>(P.prm, rule, tx, t0, rows, sh.b32q);
+            else
+                regular_dp0_mixed_sym_tile<K, 0, false, true>(P.prm, rule, tx, t0, rows, sh.b32q);
+        } else if (P.phase_class == 2) {
             regular_dp0_mixed_sym_tile<K, 2>(P.prm, rule, tx, t0, rows, sh.b32q);
-        else if (P.phase_class == 1)
+        } else if (P.phase_class == 1) {
             regular_dp0_mixed_sym_tile<K, 1>(P.prm, rule, tx, t0, rows, sh.b32q);
-        else
+        } else {
             regular_dp0_mixed_sym_tile<K, 0>(P.prm, rule, tx, t0, rows, sh.b32q);
+        }
+    } else {
+        regular_dp0_mixed_sym_tile<K, 0>(P.prm, rule, tx, t0, rows, sh.b32q);
     }
 }
 
@@ -205,10 +218,10 @@ static int rows_of(const bemppcuda_batch_args *a) {
     return (a->rows_per_item >= 1 && a->rows_per_item <= DP0_TCHUNK) ? a->rows_per_item : DP0_TCHUNK;
 }
 
-// The symmetric sweep needs a real wavenumber (k > 0 for the scaled mixed
-// path) and a row height that divides the 128-column block.
+// The symmetric sweep needs Re k > 0 on the scaled mixed path (a complex k included) and a row height
+// that divides the 128-column block.
 static bool sym_of(const bemppcuda_batch_problem &p, int rows) {
-    if (DP0_THREADS % rows != 0 || p.params[1] != 0.0) return false;
+    if (DP0_THREADS % rows != 0) return false;
     return p.precision == BEMPPCUDA_FP64 || p.params[0] > 0.0;
 }
 
