@@ -30,7 +30,7 @@ struct SymTraits {
     static constexpr bool swap = (K == BEMPPCUDA_LAPLACE_ADLP || K == BEMPPCUDA_HELMHOLTZ_ADLP ||
                                   K == BEMPPCUDA_MODHELM_ADLP);
     static constexpr bool helm = KernelTraits<K>::helm;
-    static constexpr bool modhelm = KernelTraits<K>::modhelm;  // FP64 tile only
+    static constexpr bool modhelm = KernelTraits<K>::modhelm;
     static constexpr bool supported = slp_part || dlp_part;
 };
 
@@ -327,7 +327,8 @@ __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm,
     using ST = SymTraits<K>;
     static_assert(!CK || ST::helm, "complex wavenumber: the Helmholtz kernels");
     constexpr int NP = NQ6 / 2;
-    const double kap = ST::helm ? prm.p[0] : 1.0;  // callers guarantee Re k > 0 for the Helmholtz family
+    // units of 1/kappa: Re k (Helmholtz), omega (modified Helmholtz), 1 (Laplace); callers guarantee kappa > 0
+    const double kap = ST::helm || ST::modhelm ? prm.p[0] : 1.0;
     const double betd = CK ? prm.p[1] / prm.p[0] : 0.0;
     const float2 bet2 = b2((float)betd);
     const int tcount = (int)min((int64_t)rows, prm.ntest - t0);
@@ -406,7 +407,8 @@ __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm,
             const double rc = rc2 * rsqrt64(rc2);
             float ph_s = 0.f, ph_c = 1.f;
             if (ST::helm) phase_reduced32(rc, &ph_s, &ph_c);
-            const double amp = CK ? exp_neg_reduced(betd * rc) : 1.0;  // e^{-beta r_c'}
+            // e^{-beta r_c'} (complex k), e^{-r_c'} (modified Helmholtz)
+            const double amp = CK ? exp_neg_reduced(betd * rc) : (ST::modhelm ? exp_neg_reduced(rc) : 1.0);
             const float D0f = (float)D0, D1f = (float)D1, D2f = (float)D2;
             const float2 rcf2 = b2((float)rc), rc2f2 = b2((float)rc2);
             // k (y - x).n_j = cp_p (y lies in the plane of j, so (y - c_j).n_j = 0) and
@@ -452,9 +454,19 @@ __device__ __forceinline__ void regular_dp0_mixed_sym_tile(const RegParams &prm,
                     const float2 rinv = f2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
                     const float2 f = mul2(wq2[j], rinv);
                     if (!ST::helm) {
-                        if (ST::slp_part) s0r = add2(f, s0r);
+                        // modified Helmholtz: e^{-theta} per pair (e^{-r_c'} per element pair), the double
+                        // layers' (1 + r') e^{-theta}
+                        float2 am = b2(1.f), am1 = b2(1.f);
+                        if (ST::modhelm) {
+                            const float2 den = fma2(r2, rinv, rcf2);
+                            const float2 th = mul2(sdot, f2(rcp_approx(den.x), rcp_approx(den.y)));
+                            am = f2(__expf(-th.x), __expf(-th.y));
+                            am1 = mul2(am, fma2(r2, rinv, b2(1.f)));
+                        }
+                        if (ST::slp_part) s0r = ST::modhelm ? fma2(f, am, s0r) : add2(f, s0r);
                         if (ST::dlp_part) {
-                            const float2 fr = mul2(mul2(f, rinv), rinv);
+                            float2 fr = mul2(mul2(f, rinv), rinv);
+                            if (ST::modhelm) fr = mul2(fr, am1);
                             pur = add2(fr, pur);
                             vr = fma2(fr, ynt[j], vr);
                         }

@@ -324,12 +324,11 @@ static cudaError_t launch_dp0(const RegParams &prm, const QuadRule &rule, int mi
                               int64_t row0, int64_t row1, cudaStream_t st) {
     dim3 grid((unsigned)((prm.ntrial + DP0_THREADS - 1) / DP0_THREADS), (unsigned)((prm.ntest + DP0_TCHUNK - 1) / DP0_TCHUNK));
     if constexpr (SymTraits<K>::supported) {
-        // same DP0 space on both sides; the mixed tiles need Re k > 0 (scaled units; a complex k adds
-        // the amplitude split), the FP64 tiles take a complex k as phase class 3
-        // (modified Helmholtz: FP64 only)
+        // same DP0 space on both sides; the mixed tiles need Re k > 0 or omega > 0 (scaled units; a
+        // complex k adds the amplitude split), the FP64 tiles take a complex k as phase class 3
         const bool helm = KernelTraits<K>::helm;
         const bool ck_sym = helm && prm.p[1] != 0.0;
-        const bool sweep_ok = helm ? (!mixed || prm.p[0] > 0.0) : !(KernelTraits<K>::modhelm && mixed);
+        const bool sweep_ok = helm || KernelTraits<K>::modhelm ? (!mixed || prm.p[0] > 0.0) : true;
         if (sym && sweep_ok) {
             // rows per tile: 32, or 16 / 8 when 32-row tiles would leave the GPU under four waves of
             // working CTAs (about half the tiles lie below the diagonal and exit; 3 CTAs per SM)
@@ -339,11 +338,9 @@ static cudaError_t launch_dp0(const RegParams &prm, const QuadRule &rule, int mi
                 tile_rows /= 2;
             const dim3 sgrid(grid.x, (unsigned)((row1 - row0 + tile_rows - 1) / tile_rows));
             if (prm.tresult) return launch_dp0_stripe<K>(prm, rule, mixed, phase_class, row0, row1, tile_rows, sgrid, st);
-            if constexpr (!KernelTraits<K>::modhelm) {
-                if (mixed) {
-                    launch_mixed_sym<K, false>(prm, rule, phase_class, row0, row1, tile_rows, sgrid, st);
-                    return cudaGetLastError();
-                }
+            if (mixed) {
+                launch_mixed_sym<K, false>(prm, rule, phase_class, row0, row1, tile_rows, sgrid, st);
+                return cudaGetLastError();
             }
             if constexpr (!KernelTraits<K>::helm) {  // no phase: one instance
                 regular_dp0_fp64_sym<K, 0><<<sgrid, DP0_THREADS, 0, st>>>(prm, rule, row0, row1, tile_rows);
@@ -651,7 +648,7 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
                             a->kernel == BEMPPCUDA_HELMHOLTZ_DLP || a->kernel == BEMPPCUDA_HELMHOLTZ_ADLP ||
                             a->kernel == BEMPPCUDA_HELMHOLTZ_COMBINED;
     const bool sym_ok = sym && sym_kernel &&
-                        (laplace || a->precision != BEMPPCUDA_MIXED || (!modhelm && a->params[0] > 0.0));
+                        (laplace || a->precision != BEMPPCUDA_MIXED || a->params[0] > 0.0);
     if (ranged && (!sym_ok || a->row_begin < 0 || a->row_end > prm.ntest || a->row_begin >= a->row_end)) {
         bc_set_error("row range [%lld, %lld) needs the symmetric sweep and 0 <= begin < end <= %lld rows",
                      (long long)a->row_begin, (long long)a->row_end, (long long)prm.ntest);

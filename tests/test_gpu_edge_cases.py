@@ -73,13 +73,16 @@ def test_mismatched_sizes_and_row_ranges_are_rejected():
         with pytest.raises(_lib.BemppCudaError) as exc:
             regular_into(out, d, sp, sp, Parameters(), overwrite=True, rows=rows)
         assert exc.value.status == _lib.ERR_INVALID
-    # a row range needs the symmetric sweep: the mixed tiles have none for modified Helmholtz ->
-    # rejected, not ignored; complex wavenumbers sweep in both precisions -> accepted
+    # a row range needs the symmetric sweep: the mixed tiles measure lengths in units of 1 / Re k and have
+    # none for Re k <= 0 -> rejected, not ignored; complex wavenumbers with Re k > 0 and modified
+    # Helmholtz sweep in both precisions -> accepted
+    di = operators.boundary.helmholtz.single_layer(sp, sp, sp, -3.0).descriptor
+    with pytest.raises(_lib.BemppCudaError) as exc:
+        regular_into(out, di, sp, sp, Parameters(), precision=_lib.MIXED, overwrite=True, rows=(0, 8))
+    assert exc.value.status == _lib.ERR_INVALID
     dm = operators.boundary.modified_helmholtz.single_layer(sp, sp, sp, 2.0).descriptor
     real_out = torch.empty((n, n), dtype=torch.float64, device="cuda")
-    with pytest.raises(_lib.BemppCudaError) as exc:
-        regular_into(real_out, dm, sp, sp, Parameters(), precision=_lib.MIXED, overwrite=True, rows=(0, 8))
-    assert exc.value.status == _lib.ERR_INVALID
+    regular_into(real_out, dm, sp, sp, Parameters(), precision=_lib.MIXED, overwrite=True, rows=(0, 8))
     dc = operators.boundary.helmholtz.single_layer(sp, sp, sp, 3.0 + 0.5j).descriptor
     regular_into(out, dc, sp, sp, Parameters(), precision=_lib.MIXED, overwrite=True, rows=(0, 8))
     regular_into(out, dc, sp, sp, Parameters(), overwrite=True, rows=(0, 8))

@@ -30,10 +30,11 @@ KERNELS = [
     ("helmholtz_adjoint_double_layer", [4.0, 0.7]),
     ("helmholtz_combined_field", [7.0, 0.5, 0.0, -7.0]),
     ("helmholtz_combined_field", [30.0, 9.0, 1.0, -30.0]),
-    # modified Helmholtz (real kernel; FP64 sweep, the mixed path runs per pair)
+    # modified Helmholtz (real kernel; both sweeps, the mixed one with e^{-r'} split about the centroids)
     ("modified_helmholtz_single_layer", [2.0]),
     ("modified_helmholtz_double_layer", [2.0]),
     ("modified_helmholtz_adjoint_double_layer", [6.0]),
+    ("modified_helmholtz_double_layer", [25.0]),
 ]
 
 
