@@ -582,19 +582,30 @@ class PotentialOperator(object):
 
     def __init__(self, space, points, descriptor, device_interface="cuda", parameters=None):
         self.space = space
-        self.points = _np.asarray(points, dtype=_np.float64)
+        # the operator's own copy: the points are uploaded once per device and reused by every evaluation
+        self.points = _np.array(points, dtype=_np.float64, copy=True)
         self.descriptor = descriptor
         self.device_interface = device_interface or "cuda"
         self.parameters = _params(parameters)
+        self._points_dev = {}
+
+    def _device_points(self):
+        """The evaluation points as a (npoints, 3) device tensor on the current device."""
+        import torch
+
+        dev = torch.cuda.current_device()
+        pts = self._points_dev.get(dev)
+        if pts is None:
+            pts = torch.as_tensor(_np.ascontiguousarray(self.points.T), device="cuda")
+            self._points_dev[dev] = pts
+        return pts
 
     def evaluate_device(self, coefficients):
         """(kernel_dimension, npoints) complex device tensor for dof ``coefficients``."""
-        from .assembly import evaluate_potential_device
+        from .assembly import evaluate_potential_device, precision_of
 
         local = self.space.map_to_full_grid @ _np.asarray(coefficients)
-        from .assembly import precision_of
-
-        return evaluate_potential_device(self.space, self.descriptor, self.points, local, self.parameters,
+        return evaluate_potential_device(self.space, self.descriptor, self._device_points(), local, self.parameters,
                                          precision=precision_of(self.device_interface))
 
     def evaluate(self, grid_fun):
