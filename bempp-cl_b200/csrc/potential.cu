@@ -957,6 +957,201 @@ __global__ void __launch_bounds__(PS_THREADS) farfield_maxwell_mixed(PotParams p
     }
 }
 
+// Mixed-precision Maxwell magnetic potential (maxwell_mfield_potential, numba_kernels.py:2363-2433):
+// H(x) = sum_y G (i k d - 1) / d^2 (x - y) x v_y, d = |x - y|, v the weighted basis values.  In units of
+// 1/kappa (kappa = Re k) about the source's element centroid, as potential_scalar_mixed:
+//   H = -(kappa^2 / 4 pi) sum_e e^{i r_c'} sum_q h (d' x v),  h = (i r' - 1) e^{i theta} / r'^3,
+// d' = kappa (y - x) = D + yo; a complex k adds e^{-beta r'} (beta = Im k / Re k) split the same way and
+// (i k d - 1) = -(1 + beta r') + i r'.  Per pair in packed FP32 (the thread's two points): r', theta, h, the
+// cross product d' x v and h times it; per (point, element) in FP64: D, r_c', the phase and amplitude and
+// the sums over elements.  A point within 4 kappa R of an element takes that element's sources in FP64.
+// The electric potential is not done this way: its divergence term cancels between the two triangles of
+// each RWG function, which FP32 element sums do not survive (the same reason as the electric far field).
+template <int PHC, int NQ, bool CK>
+__global__ void __launch_bounds__(PS_THREADS) potential_mfield_mixed(PotParams prm, int64_t chunk_elems,
+                                                                     double near_r) {
+    static_assert(PS_PPT == 2, "two evaluation points per thread, packed");
+    __shared__ float4 syo[PS_SOURCES];       // yo, |yo|^2
+    __shared__ float4 sv01[PS_SOURCES];      // v_0, v_1 (re, im)
+    __shared__ float2 sv2[PS_SOURCES];       // v_2 (re, im)
+    __shared__ double scen[PS_SOURCES * 3];  // kappa c_e
+    const int nq = NQ > 0 ? NQ : prm.nq;
+    const int tile_elems = PS_SOURCES / nq;
+    const int64_t ebeg = (int64_t)blockIdx.y * chunk_elems;
+    const int64_t eend = min(ebeg + chunk_elems, prm.nsupport);
+    const int64_t pbase = (int64_t)blockIdx.x * (PS_THREADS * PS_PPT) + threadIdx.x;
+    const double kap = prm.p[0], ki = CK ? prm.p[1] : 0.0;
+    const double betd = CK ? ki / kap : 0.0;
+    const float bet = (float)betd;
+    double x[PS_PPT][3], hr[PS_PPT][3], hi[PS_PPT][3];  // hr, hi: the sums in units of -kappa^2 / 4 pi
+#pragma unroll
+    for (int j = 0; j < PS_PPT; ++j) {
+        const int64_t pj = min(pbase + j * PS_THREADS, prm.npoints - 1);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            x[j][d] = prm.points[3 * pj + d];
+            hr[j][d] = hi[j][d] = 0.0;
+        }
+    }
+    const double unit = -kap * kap * BC_INV_4PI;  // the sums' unit
+    const double inv_unit = 1.0 / unit;
+    const int64_t n = prm.nsrc;
+    const double *o = prm.src;
+    for (int64_t t0 = ebeg; t0 < eend; t0 += tile_elems) {
+        const int te = (int)min((int64_t)tile_elems, eend - t0);
+        const int ns = te * nq;
+        const int64_t s0 = t0 * nq;
+        __syncthreads();
+        for (int e = threadIdx.x; e < te; e += PS_THREADS) {
+            const int64_t el = prm.support[t0 + e];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) scen[3 * e + d] = kap * __ldg(prm.g + (22 + d) * prm.ne + el);
+        }
+        __syncthreads();
+        for (int s = threadIdx.x; s < ns; s += PS_THREADS) {
+            const int64_t gs = s0 + s;
+            const int e = s / nq;
+            const float y0 = (float)fma(kap, o[gs], -scen[3 * e]), y1 = (float)fma(kap, o[n + gs], -scen[3 * e + 1]),
+                        y2 = (float)fma(kap, o[2 * n + gs], -scen[3 * e + 2]);
+            syo[s] = make_float4(y0, y1, y2, fmaf(y2, y2, fmaf(y1, y1, y0 * y0)));
+            sv01[s] = make_float4((float)o[6 * n + gs], (float)o[7 * n + gs], (float)o[8 * n + gs],
+                                  (float)o[9 * n + gs]);
+            sv2[s] = make_float2((float)o[10 * n + gs], (float)o[11 * n + gs]);
+        }
+        __syncthreads();
+        for (int e = 0; e < te; ++e) {
+            double rc[PS_PPT];
+            float dd[3][PS_PPT], rc2h[PS_PPT];
+#pragma unroll
+            for (int j = 0; j < PS_PPT; ++j) {
+                const double D0 = fma(-kap, x[j][0], scen[3 * e]), D1 = fma(-kap, x[j][1], scen[3 * e + 1]),
+                             D2 = fma(-kap, x[j][2], scen[3 * e + 2]);
+                const double rc2 = fma(D2, D2, fma(D1, D1, D0 * D0));
+                rc2h[j] = (float)rc2;
+                const double y0 = (double)rsqrt_approx(fmaxf(rc2h[j], 1e-30f));
+                const double r0 = rc2 * y0;
+                rc[j] = fma(r0, 0.5 * fma(-r0, y0, 1.0), r0);
+                dd[0][j] = (float)D0;
+                dd[1][j] = (float)D1;
+                dd[2][j] = (float)D2;
+            }
+            const float2 Dh0 = f2(dd[0][0], dd[0][1]), Dh1 = f2(dd[1][0], dd[1][1]), Dh2 = f2(dd[2][0], dd[2][1]);
+            const float2 Dx = add2(Dh0, Dh0), Dy = add2(Dh1, Dh1), Dz = add2(Dh2, Dh2);  // 2 D
+            const float2 rcf = f2((float)rc[0], (float)rc[1]);
+            const float2 rc2f = f2(rc2h[0], rc2h[1]);
+            float2 sr[3] = {b2(0.f), b2(0.f), b2(0.f)}, si[3] = {b2(0.f), b2(0.f), b2(0.f)};
+#pragma unroll(NQ > 0 ? NQ : 1)
+            for (int q = 0; q < nq; ++q) {
+                const float4 yo = syo[e * nq + q];
+                const float4 va = sv01[e * nq + q];
+                const float2 vb = sv2[e * nq + q];
+                const float2 sdot = fma2(Dz, b2(yo.z), fma2(Dy, b2(yo.y), fma2(Dx, b2(yo.x), b2(yo.w))));
+                const float2 r2 = add2(rc2f, sdot);
+                const float2 rinv = f2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+                const float2 den = fma2(r2, rinv, rcf);  // r' + r_c'
+                const float2 th = mul2(sdot, f2(rcp_approx(den.x), rcp_approx(den.y)));
+                float2 sn, cs;
+                sincos2<PHC>(th, &sn, &cs);
+                if (CK) {
+                    const float2 am = f2(__expf(-bet * th.x), __expf(-bet * th.y));
+                    cs = mul2(cs, am);
+                    sn = mul2(sn, am);
+                }
+                // h = (i r' - 1) e^{i theta} / r'^3 with a = 1 (+ beta r'): (-(a cs + r' sn), r' cs - a sn) / r'^3
+                const float2 rp = mul2(r2, rinv), r3 = mul2(rinv, mul2(rinv, rinv));
+                const float2 a = CK ? fma2(b2(bet), rp, b2(1.f)) : b2(1.f);
+                const float2 hre = mul2(r3, mul2(fma2(rp, sn, CK ? mul2(a, cs) : cs), b2(-1.f)));
+                const float2 him = mul2(r3, fma2(rp, cs, mul2(CK ? mul2(a, sn) : sn, b2(-1.f))));
+                // d' = D + yo, then d' x v (real and imaginary parts of v)
+                const float2 p0 = add2(Dh0, b2(yo.x)), p1 = add2(Dh1, b2(yo.y)), p2 = add2(Dh2, b2(yo.z));
+                const float2 vr0 = b2(va.x), vi0 = b2(va.y), vr1 = b2(va.z), vi1 = b2(va.w), vr2 = b2(vb.x),
+                             vi2 = b2(vb.y);
+                const float2 cr[3] = {fma2(p1, vr2, mul2(mul2(p2, vr1), b2(-1.f))),
+                                      fma2(p2, vr0, mul2(mul2(p0, vr2), b2(-1.f))),
+                                      fma2(p0, vr1, mul2(mul2(p1, vr0), b2(-1.f)))};
+                const float2 ci[3] = {fma2(p1, vi2, mul2(mul2(p2, vi1), b2(-1.f))),
+                                      fma2(p2, vi0, mul2(mul2(p0, vi2), b2(-1.f))),
+                                      fma2(p0, vi1, mul2(mul2(p1, vi0), b2(-1.f)))};
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    sr[d] = fma2(hre, cr[d], fma2(him, mul2(ci[d], b2(-1.f)), sr[d]));
+                    si[d] = fma2(hre, ci[d], fma2(him, cr[d], si[d]));
+                }
+            }
+            // times e^{i r_c'} (and e^{-beta r_c'}), into the FP64 sums; near elements in FP64 instead
+            float s0f, c0f, s1f, c1f;
+            phase_reduced32(rc[0], &s0f, &c0f);
+            phase_reduced32(rc[1], &s1f, &c1f);
+            const float2 cs = f2(c0f, c1f), sn = f2(s0f, s1f), msn = mul2(sn, b2(-1.f));
+            const double amp[2] = {CK ? exp_neg_reduced(betd * rc[0]) : 1.0, CK ? exp_neg_reduced(betd * rc[1]) : 1.0};
+            float2 pr[3], pi[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                pr[d] = fma2(cs, sr[d], mul2(msn, si[d]));
+                pi[d] = fma2(cs, si[d], mul2(sn, sr[d]));
+            }
+#pragma unroll
+            for (int j = 0; j < PS_PPT; ++j) {
+                if (rc[j] < near_r) {
+                    // FP64: sum_q G (i k d - 1) / d^2 (x - y) x v over the element's sources
+                    double nr[3] = {0.0, 0.0, 0.0}, ni[3] = {0.0, 0.0, 0.0};
+                    const int64_t g0 = s0 + (int64_t)e * nq;
+                    for (int q = 0; q < nq; ++q) {
+                        const int64_t gq = g0 + q;
+                        const double df[3] = {x[j][0] - o[gq], x[j][1] - o[n + gq], x[j][2] - o[2 * n + gq]};
+                        const double d2 = fma(df[2], df[2], fma(df[1], df[1], df[0] * df[0]));
+                        const double dinv = rsqrt64(d2), dist = d2 * dinv;
+                        double snd, csd;
+                        sincos_cw64(kap * dist, &snd, &csd);
+                        const double am = CK ? exp(-ki * dist) : 1.0;
+                        // G (i k d - 1) / d^2 without 1 / (4 pi): e^{ikd} ((-1 - ki d) + i kr d) / d^3
+                        const double g3 = am * dinv * dinv * dinv, c0 = -fma(ki, dist, 1.0), c1 = kap * dist;
+                        const double fr = g3 * (csd * c0 - snd * c1), fi = g3 * fma(csd, c1, snd * c0);
+                        const double vrr[3] = {o[6 * n + gq], o[8 * n + gq], o[10 * n + gq]};
+                        const double vii[3] = {o[7 * n + gq], o[9 * n + gq], o[11 * n + gq]};
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) {
+                            const int d1 = (d + 1) % 3, d2i = (d + 2) % 3;
+                            const double xr = df[d1] * vrr[d2i] - df[d2i] * vrr[d1];
+                            const double xi = df[d1] * vii[d2i] - df[d2i] * vii[d1];
+                            nr[d] += fr * xr - fi * xi;
+                            ni[d] += fr * xi + fi * xr;
+                        }
+                    }
+                    // into the sums' unit: the FP64 terms lack 1 / (4 pi), the unit is -kappa^2 / (4 pi)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        hr[j][d] = fma(nr[d], BC_INV_4PI * inv_unit, hr[j][d]);
+                        hi[j][d] = fma(ni[d], BC_INV_4PI * inv_unit, hi[j][d]);
+                    }
+                } else {
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        hr[j][d] = fma(amp[j], (double)(j ? pr[d].y : pr[d].x), hr[j][d]);
+                        hi[j][d] = fma(amp[j], (double)(j ? pi[d].y : pi[d].x), hi[j][d]);
+                    }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < PS_PPT; ++j) {
+        const int64_t pj = pbase + j * PS_THREADS;
+        if (pj >= prm.npoints) break;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            double *out = prm.result + 2 * (d * prm.npoints + pj);
+            if (gridDim.y == 1) {
+                out[0] = unit * hr[j][d];
+                out[1] = unit * hi[j][d];
+            } else {
+                atomicAdd(out, unit * hr[j][d]);
+                atomicAdd(out + 1, unit * hi[j][d]);
+            }
+        }
+    }
+}
+
 // Grid of the per-point kernels: point blocks x source chunks; with more than one chunk the
 // chunks add their sums with atomics into the zeroed result.  The chunk count c minimises
 //   ceil(pblocks c / slots) (1/c + 1/64),
@@ -1037,6 +1232,32 @@ static cudaError_t launch_far_maxwell_nq(const PotParams &prm, cudaStream_t st) 
     if (err != cudaSuccess) return err;
     fn<<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems);
     return cudaGetLastError();
+}
+
+template <int PHC, bool CK>
+static cudaError_t launch_mfield_nq(const PotParams &prm, double near_r, cudaStream_t st) {
+    auto fn = prm.nq == 6 ? potential_mfield_mixed<PHC, 6, CK> : potential_mfield_mixed<PHC, 0, CK>;
+    dim3 grid;
+    int64_t chunk_elems = 0;
+    const cudaError_t err = scalar_grid(prm, (const void *)fn, &grid, &chunk_elems, st, 3);
+    if (err != cudaSuccess) return err;
+    fn<<<grid, PS_THREADS, 0, st>>>(prm, chunk_elems, near_r);
+    return cudaGetLastError();
+}
+
+// Mixed-precision Maxwell magnetic potential (real or complex k, Re k > 0).
+static cudaError_t launch_mfield_mixed(const PotParams &prm, double phase_radius, cudaStream_t st) {
+    const double kr = fabs(prm.p[0]) * phase_radius;
+    const int phc = (phase_radius > 0.0 && kr <= 0.5) ? 2 : (phase_radius > 0.0 && kr <= 1.0) ? 1 : 0;
+    const double near_r = 4.0 * prm.p[0] * phase_radius;  // units of 1 / Re k
+    if (prm.p[1] != 0.0) {
+        if (phc == 2) return launch_mfield_nq<2, true>(prm, near_r, st);
+        if (phc == 1) return launch_mfield_nq<1, true>(prm, near_r, st);
+        return launch_mfield_nq<0, true>(prm, near_r, st);
+    }
+    if (phc == 2) return launch_mfield_nq<2, false>(prm, near_r, st);
+    if (phc == 1) return launch_mfield_nq<1, false>(prm, near_r, st);
+    return launch_mfield_nq<0, false>(prm, near_r, st);
 }
 
 // Mixed-precision Maxwell magnetic far field (the electric one stays FP64: farfield_maxwell_mixed).
@@ -1150,13 +1371,15 @@ int bc_potential_launch(const bemppcuda_potential_args *a, double *workspace, cu
           a->kernel == BEMPPCUDA_MODHELM_SLP || a->kernel == BEMPPCUDA_MODHELM_DLP ||
           a->kernel == BEMPPCUDA_FARFIELD_SLP || a->kernel == BEMPPCUDA_FARFIELD_DLP) &&
          a->params[0] > 0.0);
-    // Maxwell: the magnetic far field (the electric one's divergence sum cancels between neighbouring
-    // elements, which FP32 element sums do not survive; farfield_maxwell_mixed)
-    const bool maxwell_far = maxwell && a->assembly == BEMPPCUDA_ASM_MFIE && a->kernel == BEMPPCUDA_FARFIELD_SLP &&
+    // Maxwell: the magnetic potential and far field (the electric ones' divergence sums cancel between
+    // neighbouring elements, which FP32 element sums do not survive; farfield_maxwell_mixed)
+    const bool maxwell_far = maxwell && a->assembly == BEMPPCUDA_ASM_MFIE &&
+                             (a->kernel == BEMPPCUDA_FARFIELD_SLP || a->kernel == BEMPPCUDA_HELMHOLTZ_SLP) &&
                              a->params[0] > 0.0;
     if (mixed && (maxwell ? !maxwell_far : !mixed_kernel)) {
         bc_set_error("mixed-precision potentials: Laplace, Helmholtz (Re k > 0) and modified Helmholtz (w > 0) "
-                     "single / double layer potentials, Helmholtz and Maxwell magnetic far fields (Re k > 0) only");
+                     "single / double layer potentials, Helmholtz far fields, the Maxwell magnetic potential and far "
+                     "field (Re k > 0) only");
         return BEMPPCUDA_ERR_UNSUPPORTED;
     }
     // the FP64 treatment of points next to the surface needs the bound R on source offsets
@@ -1179,7 +1402,8 @@ int bc_potential_launch(const bemppcuda_potential_args *a, double *workspace, cu
                                a->kernel == BEMPPCUDA_HELMHOLTZ_SLP || a->kernel == BEMPPCUDA_HELMHOLTZ_DLP ||
                                a->kernel == BEMPPCUDA_MODHELM_SLP || a->kernel == BEMPPCUDA_MODHELM_DLP;
         if (mixed && maxwell && prm.nsupport > 0) {
-            err = launch_far_maxwell(prm, a->phase_radius, st);
+            err = a->kernel == BEMPPCUDA_FARFIELD_SLP ? launch_far_maxwell(prm, a->phase_radius, st)
+                                                      : launch_mfield_mixed(prm, a->phase_radius, st);
         } else if (mixed && prm.nsupport > 0) {
             err = launch_scalar_mixed(prm, a->kernel, a->phase_radius, st);
         } else if (!maxwell && per_point && prm.nsupport > 0) {
