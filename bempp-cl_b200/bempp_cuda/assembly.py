@@ -11,7 +11,8 @@ Precision: ``device_interface`` "cuda" is FP64 end to end; "cuda_mixed"
 evaluates the regular pairs in FP32 where the library has a mixed kernel
 (DP0 scalar kernels; P1 single, double, adjoint double layer and
 hypersingular operators; the Maxwell electric and magnetic fields; scalar
-potentials, Helmholtz far fields and the Maxwell magnetic far field) and
+potentials, Helmholtz far fields and the Maxwell magnetic potential and far
+field) and
 keeps the singular pairs, per-entry sums and element-pair factors in FP64.
 Operators without a mixed kernel run in FP64 and say so once
 (``MixedPrecisionFallback``).
@@ -479,9 +480,9 @@ def evaluate_potential_device(space, descriptor, points, local_coefficients, par
     (dense_potential_assembler.py:30-34); ``points`` is a (3, npoints) array.
     ``precision=MIXED`` evaluates the point-source pairs of Laplace,
     Helmholtz (real or complex k) and modified Helmholtz single / double
-    layer potentials, Helmholtz far fields and the Maxwell magnetic far field
-    in FP32; the library refuses it for the Maxwell potentials and electric
-    far field, which the operator layer then runs in FP64.
+    layer potentials, Helmholtz far fields and the Maxwell magnetic potential
+    and far field in FP32; the library refuses it for the Maxwell electric
+    potential and far field, which the operator layer then runs in FP64.
     """
     require_cuda()
     kernel, assembly = kernel_ids(descriptor)

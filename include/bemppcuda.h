@@ -194,8 +194,8 @@ typedef struct {
     int32_t precision; /* BEMPPCUDA_FP64, or BEMPPCUDA_MIXED (FP32 point-source pairs, FP64 per-element
                           phase, amplitude and sums) for Laplace, Helmholtz (Re k > 0, real or complex k)
                           and modified Helmholtz (omega > 0) single / double layer potentials,
-                          Helmholtz far fields and the Maxwell magnetic far field (Re k > 0); other
-                          kernels return BEMPPCUDA_ERR_UNSUPPORTED under MIXED */
+                          Helmholtz far fields and the Maxwell magnetic potential and far field
+                          (Re k > 0); other kernels return BEMPPCUDA_ERR_UNSUPPORTED under MIXED */
     int32_t pad0;
     double params[4];
     bemppcuda_grid grid;
