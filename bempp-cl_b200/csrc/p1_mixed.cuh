@@ -146,7 +146,10 @@ __device__ __forceinline__ void mfie_block_moments(const double mre[3][3], const
     }
 }
 
-template <int ASM, int K, int PHC, bool SYM, bool CK = false>
+// NT, NS: test / trial functions per element, 3 (P1, DP1, RWG / SNC) or 1 (a P0 space beside a P1 one: its
+// constant function takes the rule's weights in place of the P1 shape weights; scalar operators, no
+// symmetric sweep).
+template <int ASM, int K, int PHC, bool SYM, bool CK = false, int NT = 3, int NS = 3>
 __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, QuadRule rule) {
     constexpr bool LAP = K == BEMPPCUDA_LAPLACE_SLP || K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_LAPLACE_ADLP;
     constexpr bool MH = K == BEMPPCUDA_MODHELM_SLP || K == BEMPPCUDA_MODHELM_DLP || K == BEMPPCUDA_MODHELM_ADLP;
@@ -159,6 +162,8 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
     constexpr bool DL = K == BEMPPCUDA_HELMHOLTZ_DLP || K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_MODHELM_DLP;
     constexpr bool AD = K == BEMPPCUDA_HELMHOLTZ_ADLP || K == BEMPPCUDA_LAPLACE_ADLP || K == BEMPPCUDA_MODHELM_ADLP;
     static_assert(!CK || (!REAL && !RWG), "complex wavenumber: the Helmholtz scalar operators");
+    static_assert((NT == 3 && NS == 3) || (ASM == BEMPPCUDA_ASM_SCALAR && !SYM && (NT == 1 || NS == 1)),
+                  "P0 beside P1: scalar operators, per-pair sweep");
     constexpr bool SKEW = SYM && (DL || AD);
     constexpr bool NS_SUM = DL || SKEW;  // sums multiplied by d'.n_s per test point
     constexpr bool NT_SUM = AD || SKEW;  // sums with -d'.n_t per pair
@@ -200,8 +205,8 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
         }
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
-            sb.mult[idx][i] = prm.tmult[t * 3 + i] * (RWG ? edge_length(prm.tg, prm.tne, t, i) : 1.0);
-            sb.row[idx][i] = prm.tl2g[t * 3 + i];
+            sb.mult[idx][i] = i < NT ? prm.tmult[t * NT + i] * (RWG ? edge_length(prm.tg, prm.tne, t, i) : 1.0) : 0.0;
+            sb.row[idx][i] = i < NT ? prm.tl2g[t * NT + i] : 0;
         }
         if (RWG) {
 #pragma unroll
@@ -257,8 +262,8 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
     double smul[3];
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-        scol[j] = prm.sl2g[s * 3 + j];
-        smul[j] = prm.smult[s * 3 + j] * (RWG ? edge_length(prm.sg, prm.sne, s, j) : 1.0);
+        scol[j] = j < NS ? prm.sl2g[s * NS + j] : -1;  // no slot past the element's functions
+        smul[j] = j < NS ? prm.smult[s * NS + j] * (RWG ? edge_length(prm.sg, prm.sne, s, j) : 1.0) : 0.0;
     }
     // the warp's columns (distinct trial dofs) and this lane's staging positions
     const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
@@ -280,7 +285,7 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
         if (done || (prm.grids_identical && shares_vertex(sb.v[tt], sv0, sv1, sv2))) {
             // no pair: zeros in this lane's staging positions
 #pragma unroll
-            for (int i = 0; i < 3; ++i)
+            for (int i = 0; i < NT; ++i)
 #pragma unroll
                 for (int j = 0; j < 3; ++j)
                     if (pos[j] >= 0) {
@@ -373,8 +378,9 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
                     }
                 }
 #pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    const float2 w = f2(rule.swf[2 * jj][j], rule.swf[2 * jj + 1][j]);
+                for (int j = 0; j < NS; ++j) {
+                    const float2 w = NS == 3 ? f2(rule.swf[2 * jj][j], rule.swf[2 * jj + 1][j])
+                                             : f2(rule.wf[2 * jj], rule.wf[2 * jj + 1]);
                     if (!AD || SKEW) {  // plain sums (single layer; double layer: times d'.n_s below)
                         tre[j] = fma2(kr, w, tre[j]);
                         if (!REAL) tim[j] = fma2(ki, w, tim[j]);
@@ -387,11 +393,11 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
                 }
             }
 #pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                const float ph = rule.swf[p][i];
+            for (int i = 0; i < NT; ++i) {
+                const float ph = NT == 3 ? rule.swf[p][i] : rule.wf[p];
                 const float phs = NS_SUM ? ph * dns : ph;
 #pragma unroll
-                for (int j = 0; j < 3; ++j) {
+                for (int j = 0; j < NS; ++j) {
                     if (!DL && !AD) {
                         lre[i][j] = fmaf(ph, tre[j].x + tre[j].y, lre[i][j]);
                         if (!REAL) lim[i][j] = fmaf(ph, tim[j].x + tim[j].y, lim[i][j]);
@@ -496,10 +502,10 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
             }
         }
 #pragma unroll
-        for (int i = 0; i < 3; ++i) {
+        for (int i = 0; i < NT; ++i) {
             const double mt = sb.mult[tt][i];
 #pragma unroll
-            for (int j = 0; j < 3; ++j) {
+            for (int j = 0; j < NS; ++j) {
                 const double ms = smul[j];
                 if (pos[j] < 0) continue;
                 if (mt == 0.0 || ms == 0.0) {
@@ -545,7 +551,7 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
             }
         };
 #pragma unroll
-        for (int i = 0; i < 3; ++i) {
+        for (int i = 0; i < NT; ++i) {
             const int64_t row = sb.row[tt][i];
             for (int c = (int)lane; c < ncols; c += 32) {
                 const int b = wc.start[c], e = wc.start[c + 1];

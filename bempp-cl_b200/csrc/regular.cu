@@ -494,11 +494,34 @@ static void p1_mixed_phase(const RegParams &prm, const QuadRule &rule, int phase
     }
 }
 
+// A P0 space beside a P1 one (scalar operators): per-pair sweep, the general phase class.
+template <int K, int NT, int NS>
+static void p1_mixed_pair(const RegParams &prm, const QuadRule &rule, dim3 grid, cudaStream_t st) {
+    constexpr bool helm = K == BEMPPCUDA_HELMHOLTZ_SLP || K == BEMPPCUDA_HELMHOLTZ_DLP || K == BEMPPCUDA_HELMHOLTZ_ADLP;
+    if constexpr (helm) {
+        if (prm.p[1] != 0.0) {
+            regular_p1_mixed<BEMPPCUDA_ASM_SCALAR, K, 0, false, true, NT, NS><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+            return;
+        }
+    }
+    regular_p1_mixed<BEMPPCUDA_ASM_SCALAR, K, 0, false, false, NT, NS><<<grid, DP0_THREADS, 0, st>>>(prm, rule);
+}
+
 template <int ASM, int K>
 static cudaError_t launch_p1_mixed(const RegParams &prm, const QuadRule &rule, int phase_class, bool sym,
                                    cudaStream_t st) {
     dim3 grid((unsigned)((prm.ntrial + DP0_THREADS - 1) / DP0_THREADS),
               (unsigned)((prm.ntest + P1_TCHUNK - 1) / P1_TCHUNK));
+    if constexpr (ASM == BEMPPCUDA_ASM_SCALAR) {
+        if (prm.tnshape == 3 && prm.snshape == 1) {
+            p1_mixed_pair<K, 3, 1>(prm, rule, grid, st);
+            return cudaGetLastError();
+        }
+        if (prm.tnshape == 1 && prm.snshape == 3) {
+            p1_mixed_pair<K, 1, 3>(prm, rule, grid, st);
+            return cudaGetLastError();
+        }
+    }
     constexpr bool helm = (K == BEMPPCUDA_HELMHOLTZ_SLP || K == BEMPPCUDA_HELMHOLTZ_DLP ||
                            K == BEMPPCUDA_HELMHOLTZ_ADLP) && ASM != BEMPPCUDA_ASM_EFIE && ASM != BEMPPCUDA_ASM_MFIE;
     const bool ck = helm && prm.p[1] != 0.0;
@@ -614,9 +637,15 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
         (a->assembly == BEMPPCUDA_ASM_MODHELM_HYP && a->kernel == BEMPPCUDA_MODHELM_SLP);
     const bool p1_params = (helm_k && a->params[0] > 0.0 && a->is_complex) ||
                            (lap_k && !a->is_complex) || (mh_k && a->params[0] > 0.0 && !a->is_complex);
-    const bool p1_mixed = a->nq == NQ6 && !a->overwrite && a->test.nshape == 3 && a->trial.nshape == 3 &&
-                          a->test.shapeset == BEMPPCUDA_SHAPE_P1 && a->trial.shapeset == BEMPPCUDA_SHAPE_P1 &&
-                          p1_family && p1_params;
+    // both sides P1 / DP1, or a P0 space beside a P1 one (scalar operators)
+    const bool p1_both = a->test.nshape == 3 && a->trial.nshape == 3 && a->test.shapeset == BEMPPCUDA_SHAPE_P1 &&
+                         a->trial.shapeset == BEMPPCUDA_SHAPE_P1;
+    const bool p1_p0 = a->assembly == BEMPPCUDA_ASM_SCALAR &&
+                       ((a->test.nshape == 3 && a->test.shapeset == BEMPPCUDA_SHAPE_P1 && a->trial.nshape == 1 &&
+                         a->trial.shapeset == BEMPPCUDA_SHAPE_P0) ||
+                        (a->test.nshape == 1 && a->test.shapeset == BEMPPCUDA_SHAPE_P0 && a->trial.nshape == 3 &&
+                         a->trial.shapeset == BEMPPCUDA_SHAPE_P1));
+    const bool p1_mixed = a->nq == NQ6 && !a->overwrite && (p1_both || p1_p0) && p1_family && p1_params;
     // ... and the Maxwell electric and magnetic fields on RWG / SNC (same FP32 core; 6-point rule,
     // real k > 0)
     const bool rwg_mixed = a->nq == NQ6 && !a->overwrite &&

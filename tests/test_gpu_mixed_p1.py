@@ -5,9 +5,10 @@ operators on P1 -- Helmholtz (real and complex k), Laplace and modified
 Helmholtz -- evaluate their regular pairs in FP32 (``regular_p1_mixed``) under
 ``device_interface="cuda_mixed"``; their operator error against the FP64 path
 and the oracle is held to the mixed-precision bound (1e-6 relative
-Frobenius); so do the Maxwell electric and magnetic fields on RWG / SNC.
-Operators without a mixed kernel (a P1 domain with a DP0 dual space) run in
-FP64 under the same interface.
+Frobenius); so do a P1 space beside a DP0 one and the Maxwell electric and
+magnetic fields on RWG / SNC (real k).  Operators without a mixed kernel (the
+Maxwell fields with a complex wavenumber) run in FP64 under the same
+interface.
 """
 
 import numpy as np
@@ -117,22 +118,33 @@ def test_mixed_p1_sweeps_agree(family, name, k):
         assert (torch.linalg.norm(a - ref) / torch.linalg.norm(ref)).item() < tol, key
 
 
-@pytest.mark.parametrize("path,k", [("laplace.double_layer", None), ("helmholtz.single_layer", 3.0 + 0.5j)])
-def test_mixed_interface_without_mixed_kernel_is_fp64(path, k):
-    """A P1 domain with a DP0 dual space has no mixed kernel: FP64 under cuda_mixed."""
-    from bempp_cuda import operators
-    from bempp_cuda.shapes import regular_sphere
+@pytest.mark.parametrize("path,k", [("laplace.double_layer", None), ("helmholtz.single_layer", 3.0 + 0.5j),
+                                    ("helmholtz.adjoint_double_layer", 4.0), ("modified_helmholtz.single_layer", 2.0)])
+@pytest.mark.parametrize("p1_side", ["domain", "dual"])
+def test_mixed_p1_p0_pairs(oracle, path, k, p1_side):
+    """A P1 space beside a DP0 one (either side): the mixed P1 kernel with the P0 side's constant function,
+    within 1e-6 of FP64 and of the oracle."""
+    from cases import oracle_dense
+
+    from bempp_cuda import assembly, operators
+    from bempp_cuda.shapes import ellipsoid
     from bempp_cuda.space import function_space
 
-    grid = regular_sphere(2)
+    grid = ellipsoid(3, 1.1, 0.9, 1.0)
     p1, dp0 = function_space(grid, "P", 1), function_space(grid, "DP", 0)
+    dom, dual = (p1, dp0) if p1_side == "domain" else (dp0, p1)
     f = operators.boundary
     for part in path.split("."):
         f = getattr(f, part)
-    args = (p1, p1, dp0) if k is None else (p1, p1, dp0, k)
-    a64 = f(*args, device_interface="cuda").weak_form().tensor
+    args = (dom, dom, dual) if k is None else (dom, dom, dual, k)
+    op64 = f(*args, device_interface="cuda")
+    a64 = op64.weak_form().tensor
+    assembly.FP64_FALLBACKS.clear()
     amx = f(*args, device_interface="cuda_mixed").weak_form().tensor
-    assert (torch.linalg.norm(amx - a64) / torch.linalg.norm(a64)).item() < 1e-13
+    assert not assembly.FP64_FALLBACKS  # a mixed kernel ran
+    err = (torch.linalg.norm(amx - a64) / torch.linalg.norm(a64)).item()
+    assert 0.0 < err < 1e-6, err
+    assert rel_fro(amx.cpu().numpy(), oracle_dense(oracle, op64, dom, dual)) < 1e-6
 
 
 @pytest.mark.parametrize("k", [1.0, 3.0, 20.0])
@@ -203,8 +215,8 @@ def test_mixed_maxwell_mfie_against_fp64_and_oracle(oracle, k):
 
 
 def test_operators_without_mixed_kernel_warn_and_run_fp64():
-    """cuda_mixed on an operator without a mixed-precision kernel (a P1 domain with a DP0 dual space) warns
-    once (MixedPrecisionFallback) and gives the FP64 weak form."""
+    """cuda_mixed on an operator without a mixed-precision kernel (the Maxwell electric field with a complex
+    wavenumber) warns once (MixedPrecisionFallback) and gives the FP64 weak form."""
     import warnings
 
     from bempp_cuda import assembly, operators
@@ -212,14 +224,14 @@ def test_operators_without_mixed_kernel_warn_and_run_fp64():
     from bempp_cuda.space import function_space
 
     grid = regular_sphere(2)
-    p1, dp0 = function_space(grid, "P", 1), function_space(grid, "DP", 0)
+    rwg, snc = function_space(grid, "RWG", 0), function_space(grid, "SNC", 0)
     assembly.FP64_FALLBACKS.clear()
     with warnings.catch_warnings(record=True) as caught:
         warnings.simplefilter("always")
-        mixed = operators.boundary.helmholtz.single_layer(p1, p1, dp0, 2.0,
+        mixed = operators.boundary.maxwell.electric_field(rwg, rwg, snc, 2.0 + 0.5j,
                                                           device_interface="cuda_mixed").weak_form().A
     assert any(issubclass(w.category, assembly.MixedPrecisionFallback) for w in caught)
-    fp64 = operators.boundary.helmholtz.single_layer(p1, p1, dp0, 2.0).weak_form().A
+    fp64 = operators.boundary.maxwell.electric_field(rwg, rwg, snc, 2.0 + 0.5j).weak_form().A
     assert np.array_equal(mixed, fp64) or np.linalg.norm(mixed - fp64) <= 1e-15 * np.linalg.norm(fp64)
 
 
