@@ -10,12 +10,11 @@ reference's own descriptor / space / parameter objects (duck-typed: a
 Precision: ``device_interface`` "cuda" is FP64 end to end; "cuda_mixed"
 evaluates the regular pairs in FP32 where the library has a mixed kernel
 (DP0 scalar kernels; P1 single, double, adjoint double layer and
-hypersingular operators, P1 beside P0; the Maxwell electric and magnetic fields; scalar
-potentials, Helmholtz far fields and the Maxwell magnetic potential and far
-field) and keeps the singular pairs, per-entry sums and element-pair factors
-in FP64.
-Operators without a mixed kernel run in FP64 and say so once
-(``MixedPrecisionFallback``).
+hypersingular operators, P1 beside P0; the Maxwell electric and magnetic
+fields; scalar potentials, Helmholtz far fields and the Maxwell magnetic
+potential and far field) and keeps the singular pairs, per-entry sums and
+element-pair factors in FP64.  Operators without a mixed kernel run in FP64
+and say so once (``MixedPrecisionFallback``).
 """
 
 import numpy as _np
