@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
     constexpr bool RWG = EFIE || MFIE;
     constexpr bool DL = K == BEMPPCUDA_HELMHOLTZ_DLP || K == BEMPPCUDA_LAPLACE_DLP || K == BEMPPCUDA_MODHELM_DLP;
     constexpr bool AD = K == BEMPPCUDA_HELMHOLTZ_ADLP || K == BEMPPCUDA_LAPLACE_ADLP || K == BEMPPCUDA_MODHELM_ADLP;
-    static_assert(!CK || (!REAL && !RWG), "complex wavenumber: the Helmholtz scalar operators");
+    static_assert(!CK || !REAL, "complex wavenumber: the Helmholtz kernels");
     static_assert((NT == 3 && NS == 3) || (ASM == BEMPPCUDA_ASM_SCALAR && !SYM && (NT == 1 || NS == 1)),
                   "P0 beside P1: scalar operators, per-pair sweep");
     constexpr bool SKEW = SYM && (DL || AD);
@@ -448,7 +448,7 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
                     mim[a][b] = kap * (double)lim[a][b];
                 }
             }
-            efie_block<false>(mre, mim, scurl[tt][0], scurl[tt][1], gs.j0, gs.j1, kap, 0.0, ere, eim);
+            efie_block<CK>(mre, mim, scurl[tt][0], scurl[tt][1], gs.j0, gs.j1, kap, CK ? prm.p[1] : 0.0, ere, eim);
         } else if (MFIE) {
             // the moments of H = k^3 h (units of 1/k), then the block from the FP64 geometry
             const double k3 = kap * kap * kap;

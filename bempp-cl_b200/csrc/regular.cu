@@ -522,8 +522,8 @@ static cudaError_t launch_p1_mixed(const RegParams &prm, const QuadRule &rule, i
             return cudaGetLastError();
         }
     }
-    constexpr bool helm = (K == BEMPPCUDA_HELMHOLTZ_SLP || K == BEMPPCUDA_HELMHOLTZ_DLP ||
-                           K == BEMPPCUDA_HELMHOLTZ_ADLP) && ASM != BEMPPCUDA_ASM_EFIE && ASM != BEMPPCUDA_ASM_MFIE;
+    constexpr bool helm = K == BEMPPCUDA_HELMHOLTZ_SLP || K == BEMPPCUDA_HELMHOLTZ_DLP ||
+                          K == BEMPPCUDA_HELMHOLTZ_ADLP;
     const bool ck = helm && prm.p[1] != 0.0;
     if (ck) {
         if constexpr (helm) {
@@ -647,16 +647,16 @@ int bc_regular_launch(const bemppcuda_regular_args *a, cudaStream_t st) {
                          a->trial.shapeset == BEMPPCUDA_SHAPE_P1));
     const bool p1_mixed = a->nq == NQ6 && !a->overwrite && (p1_both || p1_p0) && p1_family && p1_params;
     // ... and the Maxwell electric and magnetic fields on RWG / SNC (same FP32 core; 6-point rule,
-    // real k > 0)
+    // Re k > 0)
     const bool rwg_mixed = a->nq == NQ6 && !a->overwrite &&
                            (a->assembly == BEMPPCUDA_ASM_EFIE || a->assembly == BEMPPCUDA_ASM_MFIE) &&
-                           a->kernel == BEMPPCUDA_HELMHOLTZ_SLP && a->params[1] == 0.0 && a->params[0] > 0.0 &&
+                           a->kernel == BEMPPCUDA_HELMHOLTZ_SLP && a->params[0] > 0.0 &&
                            a->test.shapeset == BEMPPCUDA_SHAPE_RWG && a->trial.shapeset == BEMPPCUDA_SHAPE_RWG &&
                            a->test.nshape == 3 && a->trial.nshape == 3;
     if (a->precision == BEMPPCUDA_MIXED && !dp0 && !p1_mixed && !rwg_mixed) {
         bc_set_error("mixed precision is implemented for DP0 scalar kernels, the P1 single, double, adjoint "
                      "double layer and hypersingular operators (Helmholtz with Re k > 0, Laplace, modified "
-                     "Helmholtz) and the Maxwell electric and magnetic fields (real k), with the 6-point rule");
+                     "Helmholtz) and the Maxwell electric and magnetic fields (Re k > 0), with the 6-point rule");
         return BEMPPCUDA_ERR_UNSUPPORTED;
     }
     cudaError_t err = cudaSuccess;

@@ -6,9 +6,8 @@ Helmholtz -- evaluate their regular pairs in FP32 (``regular_p1_mixed``) under
 ``device_interface="cuda_mixed"``; their operator error against the FP64 path
 and the oracle is held to the mixed-precision bound (1e-6 relative
 Frobenius); so do a P1 space beside a DP0 one and the Maxwell electric and
-magnetic fields on RWG / SNC (real k).  Operators without a mixed kernel (the
-Maxwell fields with a complex wavenumber) run in FP64 under the same
-interface.
+magnetic fields on RWG / SNC (real and complex k).  Operators without a
+mixed kernel (Re k <= 0) run in FP64 under the same interface.
 """
 
 import numpy as np
@@ -147,7 +146,7 @@ def test_mixed_p1_p0_pairs(oracle, path, k, p1_side):
     assert rel_fro(amx.cpu().numpy(), oracle_dense(oracle, op64, dom, dual)) < 1e-6
 
 
-@pytest.mark.parametrize("k", [1.0, 3.0, 20.0])
+@pytest.mark.parametrize("k", [1.0, 3.0, 20.0, 3.0 + 0.6j])
 def test_mixed_maxwell_efie_against_fp64_and_oracle(oracle, k):
     """EFIE (RWG domain, SNC dual) under cuda_mixed: moments from the FP32 P1 single-layer core; k = 1, 3, 20
     on a 512-element ellipsoid reach the three phase classes.  Symmetric and per-pair sweeps agree."""
@@ -179,7 +178,7 @@ def test_mixed_maxwell_efie_against_fp64_and_oracle(oracle, k):
     assert (torch.linalg.norm(outs[0] - a64) / torch.linalg.norm(a64)).item() < 1e-6
 
 
-@pytest.mark.parametrize("k", [1.0, 3.0, 20.0])
+@pytest.mark.parametrize("k", [1.0, 3.0, 20.0, 3.0 + 0.6j])
 def test_mixed_maxwell_mfie_against_fp64_and_oracle(oracle, k):
     """MFIE (RWG domain, SNC dual) under cuda_mixed: the nine FP32 moments of e^{ikr}(ikr - 1)/r^3 and the
     FP64 determinants det(P_ti - P_sj, J_t^a, J_s^b); k = 1, 3, 20 on a 512-element ellipsoid reach the three
@@ -215,8 +214,9 @@ def test_mixed_maxwell_mfie_against_fp64_and_oracle(oracle, k):
 
 
 def test_operators_without_mixed_kernel_warn_and_run_fp64():
-    """cuda_mixed on an operator without a mixed-precision kernel (the Maxwell electric field with a complex
-    wavenumber) warns once (MixedPrecisionFallback) and gives the FP64 weak form."""
+    """cuda_mixed on an operator without a mixed-precision kernel (a negative real wavenumber on P1: the
+    mixed kernels measure lengths in units of 1 / Re k) warns once (MixedPrecisionFallback) and gives the
+    FP64 weak form."""
     import warnings
 
     from bempp_cuda import assembly, operators
@@ -224,14 +224,14 @@ def test_operators_without_mixed_kernel_warn_and_run_fp64():
     from bempp_cuda.space import function_space
 
     grid = regular_sphere(2)
-    rwg, snc = function_space(grid, "RWG", 0), function_space(grid, "SNC", 0)
+    p1 = function_space(grid, "P", 1)
     assembly.FP64_FALLBACKS.clear()
     with warnings.catch_warnings(record=True) as caught:
         warnings.simplefilter("always")
-        mixed = operators.boundary.maxwell.electric_field(rwg, rwg, snc, 2.0 + 0.5j,
+        mixed = operators.boundary.helmholtz.single_layer(p1, p1, p1, -2.0,
                                                           device_interface="cuda_mixed").weak_form().A
     assert any(issubclass(w.category, assembly.MixedPrecisionFallback) for w in caught)
-    fp64 = operators.boundary.maxwell.electric_field(rwg, rwg, snc, 2.0 + 0.5j).weak_form().A
+    fp64 = operators.boundary.helmholtz.single_layer(p1, p1, p1, -2.0).weak_form().A
     assert np.array_equal(mixed, fp64) or np.linalg.norm(mixed - fp64) <= 1e-15 * np.linalg.norm(fp64)
 
 
