@@ -107,7 +107,7 @@ typedef struct {
     int32_t assembly;   /* BEMPPCUDA_ASM_* */
     int32_t precision;  /* BEMPPCUDA_FP64 or BEMPPCUDA_MIXED: DP0 scalar kernels; P1 single, double,
                            adjoint double layer and hypersingular (Helmholtz with Re k > 0, Laplace,
-                           modified Helmholtz), P1 beside P0 for the scalar operators; Maxwell electric and magnetic fields (real k > 0);
+                           modified Helmholtz), P1 beside P0 for the scalar operators; Maxwell electric and magnetic fields (Re k > 0);
                            6-point rule.
                            Other operators return BEMPPCUDA_ERR_UNSUPPORTED under MIXED */
     int32_t is_complex; /* result is complex128 (1) or float64 (0) */
