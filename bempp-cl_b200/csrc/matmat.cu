@@ -276,8 +276,13 @@ __device__ __forceinline__ void tc_group(const MatmatDev &P, const double2 *cons
 // Compiled for 8 CTAs per SM (64 registers, a few bytes of spill): the product waits on its loads, and
 // 32 warps per SM keep more of them in flight than the 20 that 88 registers allowed (25 x 8192^2 x 8
 // right-hand sides: 5.32 against 4.77 TB/s; 6 CTAs per SM: no gain).
+#ifndef BC_MATMAT_TC_MIN_BLOCKS
+#define BC_MATMAT_TC_MIN_BLOCKS 8
+#endif
+
 template <int NR, int MT>
-__global__ void __launch_bounds__(TC_WARPS * 32, 8) matmat_c128_tc(const MatmatDev *__restrict__ probs, int nproblems) {
+__global__ void __launch_bounds__(TC_WARPS * 32, BC_MATMAT_TC_MIN_BLOCKS) matmat_c128_tc(const MatmatDev *__restrict__ probs,
+                                                                                       int nproblems) {
     using L = TcLayout<NR, MT>;
     constexpr int GW = 4;                 // columns per group
     constexpr int STEP = 16 * TC_WARPS;  // columns per step of the CTA
