@@ -38,6 +38,7 @@ struct MatmatDev {
     double2 *y;
     int64_t rows, cols, lda, ldx, ldy;
     int64_t block_begin;
+    int64_t wide;  // every row of A starts on a 32-byte boundary (A 32-byte aligned, lda even)
 };
 
 // one pipeline stage: a 16 x 64 tile of A and the matching 64 x NR rows of X, transposed
@@ -206,7 +207,21 @@ __global__ void __launch_bounds__(MM_THREADS, 2) matmat_c128(const MatmatDev *__
 // B fragments (B[k = t][n = g]) come from X[j0 + t][c] with c = g / 2 (output columns 0-7 =
 // complex columns 0-3) and 4 + g / 2 (columns 4-7, when NR > 4), cached in L1 since every warp of
 // the problem reads the same X.  The accumulator fragment of lane (g, t), C[g][2t], C[g][2t + 1],
-// is the complex entry Y[row g][4 n + t]: stored directly.  Columns beyond NR read zero.
+// is the complex entry Y[row g][4 n + t]: stored directly.  Columns beyond NR read zero.  Where
+// the rows of A are 32-byte aligned a lane loads two consecutive complex entries at once
+// (tc_group_wide) and runs the two k4 steps of both columns.
+//
+// From 5 right-hand sides on, the real form above takes 4 m8n8k4 products per 8 rows and 4 complex
+// columns (2 k steps x 2 n8 tiles), which at 8 right-hand sides keeps the DMMA pipe about 3/4 busy
+// at the bandwidth the kernel streams A.  Those sizes use Gauss's three-multiplication form instead
+// (Higham, "Stability of a method for multiplying complex matrices with three real
+// multiplications", SIAM J. Matrix Anal. Appl. 13, 1992):
+//   T1 = Re A Re X,  T2 = Im A Im X,  T3 = (Re A + Im A)(Re X + Im X),
+//   Re Y = T1 - T2,  Im Y = T3 - T1 - T2,
+// three n8 tiles with n = complex column g (B[k = t][n = g] = X[j0 + t][g]) and k the complex
+// column t of A: 3 products instead of 4, two FP64 additions per loaded A and X value.  The error
+// stays normwise of the order of the unit roundoff times |A| |X| (Higham's bound).  Lane (g, t)
+// ends with T1..T3 at row g, complex columns 2t and 2t + 1.
 constexpr int TC_WARPS = 4;
 
 __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
@@ -230,54 +245,90 @@ __device__ __forceinline__ float2 ld_stream(const float2 *p) {
 
 template <int NR, int MT>
 struct TcLayout {
-    static constexpr int NT = NR > 4 ? 2 : 1;  // n8 tiles of the real output (2 NR columns)
+    static constexpr bool GAUSS = NR > 4;      // three-multiplication form
+    static constexpr int NT = GAUSS ? 3 : 1;   // n8 accumulator tiles (T1..T3, or 2 NR real columns)
     static constexpr int ROWS = 8 * MT;        // rows per CTA: its warps split the columns
 };
 
+// A[row][j], A[row][j + 1] with one 32-byte load (p 32-byte aligned), with a hint to fetch the
+// 256-byte L2 stretch around it
+__device__ __forceinline__ void ld_wide(const double2 *p, double2 &lo, double2 &hi) {
+    unsigned long long a, b, c, d;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::256B.v4.b64 {%0,%1,%2,%3}, [%4];\n"
+                 : "=l"(a), "=l"(b), "=l"(c), "=l"(d)
+                 : "l"(p));
+    lo = make_double2(__longlong_as_double(a), __longlong_as_double(b));
+    hi = make_double2(__longlong_as_double(c), __longlong_as_double(d));
+}
+
+// The products of one k4 step: lane (g, t) holds av[m] = A[row g of tile m][j] (zero when !jok)
+// and fetches the B fragments of column j itself.
+template <int NR, int MT>
+__device__ __forceinline__ void tc_column(const MatmatDev &P, const double2 (&av)[MT], int64_t j, bool jok, int g,
+                                          double (&acc)[MT][TcLayout<NR, MT>::NT][2]) {
+    if constexpr (TcLayout<NR, MT>::GAUSS) {
+        const double2 xv = (jok && g < NR) ? __ldg(P.x + j * P.ldx + g) : make_double2(0.0, 0.0);
+        const double xs = xv.x + xv.y;
+#pragma unroll
+        for (int m = 0; m < MT; ++m) {
+            dmma(acc[m][0], av[m].x, xv.x);
+            dmma(acc[m][1], av[m].y, xv.y);
+            dmma(acc[m][2], av[m].x + av[m].y, xs);
+        }
+    } else {
+        const int c = g >> 1;
+        const double2 xv = (jok && c < NR) ? __ldg(P.x + j * P.ldx + c) : make_double2(0.0, 0.0);
+        const double bre = (g & 1) ? xv.y : xv.x;   // B[2j][g]
+        const double bim = (g & 1) ? xv.x : -xv.y;  // B[2j + 1][g]
+#pragma unroll
+        for (int m = 0; m < MT; ++m) {
+            dmma(acc[m][0], av[m].x, bre);
+            dmma(acc[m][0], av[m].y, bim);
+        }
+    }
+}
+
+// 4 columns per warp, lane (g, t) taking column j0 + t with one 16-byte load per row; MASK: columns
+// past the end read zero
 template <int NR, int MT, bool MASK>
 __device__ __forceinline__ void tc_group(const MatmatDev &P, const double2 *const (&arow)[MT], int64_t j0, int g,
                                          int t, double (&acc)[MT][TcLayout<NR, MT>::NT][2]) {
-    constexpr int NT = TcLayout<NR, MT>::NT;
-    constexpr int H = 1;
-    const int c0 = g >> 1;
-    const bool odd = g & 1;
-    double2 av[H][MT];
-    double bre[H][NT], bim[H][NT];
+    const int64_t j = j0 + t;
+    const bool jok = !MASK || j < P.cols;
+    double2 av[MT];
 #pragma unroll
-    for (int h = 0; h < H; ++h) {
-        const int64_t j = j0 + H * t + h;
-        const bool jok = !MASK || j < P.cols;
+    for (int m = 0; m < MT; ++m) av[m] = jok ? ld_stream(arow[m] + j) : make_double2(0.0, 0.0);
+    tc_column<NR, MT>(P, av, j, jok, g, acc);
+}
+
+// 8 columns per warp, lane (g, t) taking columns j0 + 2t and j0 + 2t + 1 with one 32-byte load per
+// row (rows 32-byte aligned, j0 even, both columns in range): half the load instructions, and twice
+// the bytes per request in flight
+template <int NR, int MT>
+__device__ __forceinline__ void tc_group_wide(const MatmatDev &P, const double2 *const (&arow)[MT], int64_t j0,
+                                              int g, int t, double (&acc)[MT][TcLayout<NR, MT>::NT][2]) {
+    const int64_t j = j0 + 2 * t;
+    double2 lo[MT], hi[MT];
 #pragma unroll
-        for (int n = 0; n < NT; ++n) {
-            const int c = 4 * n + c0;
-            const double2 xv = (jok && c < NR) ? __ldg(P.x + j * P.ldx + c) : make_double2(0.0, 0.0);
-            bre[h][n] = odd ? xv.y : xv.x;   // B[2j][g]
-            bim[h][n] = odd ? xv.x : -xv.y;  // B[2j + 1][g]
-        }
-#pragma unroll
-        for (int m = 0; m < MT; ++m) av[h][m] = jok ? ld_stream(arow[m] + j) : make_double2(0.0, 0.0);
-    }
-#pragma unroll
-    for (int h = 0; h < H; ++h)
-#pragma unroll
-        for (int m = 0; m < MT; ++m)
-#pragma unroll
-            for (int n = 0; n < NT; ++n) {
-                dmma(acc[m][n], av[h][m].x, bre[h][n]);
-                dmma(acc[m][n], av[h][m].y, bim[h][n]);
-            }
+    for (int m = 0; m < MT; ++m) ld_wide(arow[m] + j, lo[m], hi[m]);
+    tc_column<NR, MT>(P, lo, j, true, g, acc);
+    tc_column<NR, MT>(P, hi, j + 1, true, g, acc);
 }
 
 // A CTA owns 8 MT rows of one problem; its TC_WARPS warps split the columns in steps of
 // 16 TC_WARPS (warp w takes columns 16 w .. 16 w + 15 of each step, so a step reads one contiguous
 // 256-byte-per-warp stretch of every row), then add their accumulators in shared memory in a fixed
 // order.  Splitting the columns instead of the rows keeps four times as many CTAs for the same
-// matrix (problems of a few thousand rows still fill the GPU) without atomics.
-// Compiled for 8 CTAs per SM (64 registers, a few bytes of spill): the product waits on its loads, and
-// 32 warps per SM keep more of them in flight than the 20 that 88 registers allowed (25 x 8192^2 x 8
-// right-hand sides: 5.32 against 4.77 TB/s; 6 CTAs per SM: no gain).
+// matrix (problems of a few thousand rows still fill the GPU) without atomics.  Problems whose rows
+// start on 32-byte boundaries (MatmatDev::wide) stream A with 32-byte loads, the others with 16-byte
+// loads; the ragged last columns always take the masked 16-byte form.
+// Compiled for 7 CTAs per SM (72 registers, some spill to L1): the product waits on its loads, and
+// 28 warps per SM keep more of them in flight than the 20 that 88 registers allowed.  25 x 8192^2
+// x 8 right-hand sides, CUDA events: 4.77 TB/s (real form, 16-byte loads, 5 CTAs / SM), 5.3
+// (8 CTAs / SM), 5.7 (three-multiplication form), 6.5 (32-byte loads), 6.7 (7 CTAs / SM; 6 and 8:
+// 6.6 and 6.5).
 #ifndef BC_MATMAT_TC_MIN_BLOCKS
-#define BC_MATMAT_TC_MIN_BLOCKS 8
+#define BC_MATMAT_TC_MIN_BLOCKS 7
 #endif
 
 template <int NR, int MT>
@@ -308,9 +359,16 @@ __global__ void __launch_bounds__(TC_WARPS * 32, BC_MATMAT_TC_MIN_BLOCKS) matmat
 #pragma unroll
         for (int n = 0; n < L::NT; ++n) acc[m][n][0] = acc[m][n][1] = 0.0;
     const int64_t full = P.cols / STEP * STEP;
-    for (int64_t j0 = 16 * warp; j0 < full; j0 += STEP) {
+    if (P.wide) {
+        for (int64_t j0 = 16 * warp; j0 < full; j0 += STEP) {
 #pragma unroll
-        for (int u = 0; u < 4; ++u) tc_group<NR, MT, false>(P, arow, j0 + u * GW, g, t, acc);
+            for (int u = 0; u < 2; ++u) tc_group_wide<NR, MT>(P, arow, j0 + 8 * u, g, t, acc);
+        }
+    } else {
+        for (int64_t j0 = 16 * warp; j0 < full; j0 += STEP) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) tc_group<NR, MT, false>(P, arow, j0 + u * GW, g, t, acc);
+        }
     }
     for (int64_t j0 = full + 16 * warp; j0 < P.cols; j0 += STEP)
         for (int u = 0; u < 4 && j0 + u * GW < P.cols; ++u) tc_group<NR, MT, true>(P, arow, j0 + u * GW, g, t, acc);
@@ -337,10 +395,20 @@ __global__ void __launch_bounds__(TC_WARPS * 32, BC_MATMAT_TC_MIN_BLOCKS) matmat
 #pragma unroll
         for (int m = 0; m < MT; ++m) {
             const int64_t r = r0 + 8 * m + g;
+            if constexpr (L::GAUSS) {
 #pragma unroll
-            for (int n = 0; n < L::NT; ++n) {
-                const int c = 4 * n + t;
-                if (r < P.rows && c < NR) P.y[r * P.ldy + c] = make_double2(acc[m][n][0], acc[m][n][1]);
+                for (int q = 0; q < 2; ++q) {
+                    const int c = 2 * t + q;
+                    const double t12 = acc[m][0][q] + acc[m][1][q];
+                    if (r < P.rows && c < NR)
+                        P.y[r * P.ldy + c] = make_double2(acc[m][0][q] - acc[m][1][q], acc[m][2][q] - t12);
+                }
+            } else {
+#pragma unroll
+                for (int n = 0; n < L::NT; ++n) {
+                    const int c = 4 * n + t;
+                    if (r < P.rows && c < NR) P.y[r * P.ldy + c] = make_double2(acc[m][n][0], acc[m][n][1]);
+                }
             }
         }
     }
@@ -506,6 +574,7 @@ extern "C" int bemppcuda_matmat_prepare(bemppcuda_matmat_args *a, void *stream) 
         d.ldx = p.ldx;
         d.ldy = p.ldy;
         d.block_begin = blocks;
+        d.wide = (reinterpret_cast<uintptr_t>(p.a) % 32 == 0 && p.lda % 2 == 0) ? 1 : 0;
         const int64_t rpb = matmat_rows_per_block(a->nrhs);
         blocks += (p.rows + rpb - 1) / rpb;
     }

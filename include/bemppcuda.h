@@ -398,7 +398,12 @@ int bemppcuda_matmat_prepare(bemppcuda_matmat_args *args, void *stream);
    captured in a CUDA graph once bemppcuda_matmat_prepare has run).  FP64
    sums; the order differs from a BLAS product's, so results agree with it to
    rounding, not bit for bit.  2 to 8 right-hand sides run on the FP64 tensor
-   cores (mma.sync m8n8k4 .f64), 1 on the FP64 pipe. */
+   cores (mma.sync m8n8k4 .f64), 1 on the FP64 pipe; 5 to 8 use Gauss's
+   three-multiplication complex product, whose error is bounded normwise
+   (of the order of the unit roundoff times |A| |X|), so an imaginary part
+   much smaller than that product may carry a larger relative error.
+   Problems whose a is 32-byte aligned with an even lda are read with
+   32-byte loads (faster); any 16-byte aligned layout is accepted. */
 int bemppcuda_matmat_launch(const bemppcuda_matmat_args *args, void *stream);
 
 /* y = A x, one right-hand side: the matvec of the solve (DenseDiscreteBoundaryOperator._matvec,

@@ -26,7 +26,7 @@ def _rel(a, b):
     return (torch.linalg.norm(a - b) / torch.linalg.norm(b)).item()
 
 
-@pytest.mark.parametrize("nrhs", [1, 3, 8, 11, 16])
+@pytest.mark.parametrize("nrhs", [1, 3, 5, 8, 11, 14, 16])
 def test_ragged_problems_match_matmul(nrhs):
     """Rectangular and ragged sizes (1 row, 1 column, non-multiples of the 16-row / 64-column tiles);
     more than 8 right-hand sides run as several launches over column groups."""
@@ -59,6 +59,51 @@ def test_strided_views_and_overwrite():
     mask = torch.ones_like(big_y, dtype=torch.bool)
     mask[10:250, 3:7] = False
     assert bool((big_y[mask] == 7.0 + 7.0j).all())
+
+
+@pytest.mark.parametrize("nrhs", [2, 4, 6, 8])
+def test_aligned_and_unaligned_rows(nrhs):
+    """The same matrix at a 32-byte aligned address (rows read with 32-byte loads), 16 bytes past it
+    and with an odd row stride (16-byte loads): all three agree with the library product, and the
+    two 16-byte forms with each other bit for bit."""
+    from bempp_cuda.matmat import BatchedProduct
+
+    rng = np.random.default_rng(40 + nrhs)
+    rows, cols = 300, 1000
+    base = torch.zeros(rows * (cols + 2) + 4, dtype=torch.complex128, device="cuda")
+    assert base.data_ptr() % 32 == 0
+    src = _c128(rng, (rows, cols))
+    views = [
+        base[: rows * cols].view(rows, cols),  # aligned, lda even
+        base[1 : 1 + rows * (cols + 2)].view(rows, cols + 2)[:, :cols],  # 16 bytes off, lda even
+        base[2 : 2 + rows * (cols + 1)].view(rows, cols + 1)[:, :cols],  # aligned, lda odd
+    ]
+    x = _c128(rng, (cols, nrhs))
+    ref = src @ x
+    outs = []
+    for a in views:
+        a.copy_(src)
+        y = torch.empty((rows, nrhs), dtype=torch.complex128, device="cuda")
+        BatchedProduct([a], [x], [y]).launch()
+        torch.cuda.synchronize()
+        assert _rel(y, ref) < 1e-14
+        outs.append(y)
+    assert torch.equal(outs[1], outs[2])
+
+
+def test_nearly_real_products():
+    """Gauss's form (5 to 8 right-hand sides) keeps the normwise bound when the product is almost
+    real: the imaginary part's error stays at rounding level relative to |A| |X|."""
+    from bempp_cuda.matmat import matmat
+
+    rng = np.random.default_rng(9)
+    a = torch.as_tensor(rng.standard_normal((512, 512)) + 1e-9j * rng.standard_normal((512, 512)), device="cuda")
+    x = torch.as_tensor(rng.standard_normal((512, 8)) + 1e-9j * rng.standard_normal((512, 8)), device="cuda")
+    (y,) = matmat([a], [x])
+    torch.cuda.synchronize()
+    ref = a @ x
+    scale = (a.abs() @ x.abs()).max().item()
+    assert (y - ref).abs().max().item() < 1e-13 * scale
 
 
 def test_graph_capture_of_products():
