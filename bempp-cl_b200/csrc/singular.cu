@@ -354,6 +354,62 @@ static cudaError_t launch_sing_dp0(const SingParams &prm, int phase_class, cudaS
     return cudaGetLastError();
 }
 
+}  // namespace bc
+
+#include "singular_p1.cuh"  // singular_p1, on SingParams, pair_in_range and SING_WARPS above
+
+namespace bc {
+
+template <int ASM, int K>
+static cudaError_t launch_sing_p1(const SingParams &prm, int phase_class, cudaStream_t st) {
+    const unsigned blocks = (unsigned)((prm.npairs + SING_WARPS - 1) / SING_WARPS);
+    if constexpr (!SingDp0Traits<K>::helm) {
+        singular_p1<ASM, K, 0><<<blocks, 32 * SING_WARPS, 0, st>>>(prm);
+    } else {
+        if (phase_class == 3)
+            singular_p1<ASM, K, 3><<<blocks, 32 * SING_WARPS, 0, st>>>(prm);
+        else if (phase_class == 2)
+            singular_p1<ASM, K, 2><<<blocks, 32 * SING_WARPS, 0, st>>>(prm);
+        else if (phase_class == 1)
+            singular_p1<ASM, K, 1><<<blocks, 32 * SING_WARPS, 0, st>>>(prm);
+        else
+            singular_p1<ASM, K, 0><<<blocks, 32 * SING_WARPS, 0, st>>>(prm);
+    }
+    return cudaGetLastError();
+}
+
+// P1 x P1 (three shapes on both sides): the scalar kernels without the combined field, and the
+// three hypersingular operators; false when the pair list needs the generic kernel
+static bool launch_p1_pairs(const bemppcuda_singular_args *a, const SingParams &prm, int phase_class,
+                            cudaStream_t st, cudaError_t *err) {
+    if (prm.nt != 3 || prm.ns != 3) return false;
+    switch (a->assembly) {
+    case BEMPPCUDA_ASM_SCALAR:
+        switch (a->kernel) {
+        case BEMPPCUDA_LAPLACE_SLP: *err = launch_sing_p1<0, BEMPPCUDA_LAPLACE_SLP>(prm, 0, st); return true;
+        case BEMPPCUDA_LAPLACE_DLP: *err = launch_sing_p1<0, BEMPPCUDA_LAPLACE_DLP>(prm, 0, st); return true;
+        case BEMPPCUDA_LAPLACE_ADLP: *err = launch_sing_p1<0, BEMPPCUDA_LAPLACE_ADLP>(prm, 0, st); return true;
+        case BEMPPCUDA_HELMHOLTZ_SLP:
+            *err = launch_sing_p1<0, BEMPPCUDA_HELMHOLTZ_SLP>(prm, phase_class, st);
+            return true;
+        case BEMPPCUDA_HELMHOLTZ_DLP:
+            *err = launch_sing_p1<0, BEMPPCUDA_HELMHOLTZ_DLP>(prm, phase_class, st);
+            return true;
+        case BEMPPCUDA_HELMHOLTZ_ADLP:
+            *err = launch_sing_p1<0, BEMPPCUDA_HELMHOLTZ_ADLP>(prm, phase_class, st);
+            return true;
+        case BEMPPCUDA_MODHELM_SLP: *err = launch_sing_p1<0, BEMPPCUDA_MODHELM_SLP>(prm, 0, st); return true;
+        case BEMPPCUDA_MODHELM_DLP: *err = launch_sing_p1<0, BEMPPCUDA_MODHELM_DLP>(prm, 0, st); return true;
+        case BEMPPCUDA_MODHELM_ADLP: *err = launch_sing_p1<0, BEMPPCUDA_MODHELM_ADLP>(prm, 0, st); return true;
+        default: return false;
+        }
+    case BEMPPCUDA_ASM_LAPLACE_HYP: *err = launch_sing_p1<1, BEMPPCUDA_LAPLACE_SLP>(prm, 0, st); return true;
+    case BEMPPCUDA_ASM_HELM_HYP: *err = launch_sing_p1<2, BEMPPCUDA_HELMHOLTZ_SLP>(prm, phase_class, st); return true;
+    case BEMPPCUDA_ASM_MODHELM_HYP: *err = launch_sing_p1<3, BEMPPCUDA_MODHELM_SLP>(prm, 0, st); return true;
+    default: return false;
+    }
+}
+
 template <int ASM, int K>
 static cudaError_t launch_sing(const SingParams &prm, cudaStream_t st) {
     const unsigned blocks = (unsigned)((prm.npairs + SING_WARPS - 1) / SING_WARPS);
@@ -400,12 +456,18 @@ int bc_singular_launch(const bemppcuda_singular_args *a, cudaStream_t st) {
     if (prm.npairs == 0) return BEMPPCUDA_OK;
     cudaError_t err = cudaSuccess;
     const bool real_k = a->params[1] == 0.0;
+    // a complex wavenumber takes phase class 3 (no centroid factoring)
+    const double theta = fabs(a->params[0]) * a->phase_radius;
+    const int phase_class = !real_k ? 3 : a->phase_radius > 0.0 ? (theta <= 0.5 ? 2 : (theta <= 1.0 ? 1 : 0)) : 0;
+    if (launch_p1_pairs(a, prm, phase_class, st, &err)) {
+        if (err != cudaSuccess) {
+            bc_set_error("singular assembly launch failed: %s", cudaGetErrorString(err));
+            return BEMPPCUDA_ERR_CUDA;
+        }
+        return BEMPPCUDA_OK;
+    }
     if (a->assembly == BEMPPCUDA_ASM_SCALAR && prm.nt == 1 && prm.ns == 1 &&
         (a->kernel <= BEMPPCUDA_MODHELM_ADLP || a->kernel == BEMPPCUDA_HELMHOLTZ_COMBINED)) {
-        // a complex wavenumber takes phase class 3 (no centroid factoring)
-        const double theta = fabs(a->params[0]) * a->phase_radius;
-        const int phase_class = !real_k ? 3
-                                : a->phase_radius > 0.0 ? (theta <= 0.5 ? 2 : (theta <= 1.0 ? 1 : 0)) : 0;
         switch (a->kernel) {
         case BEMPPCUDA_LAPLACE_SLP: err = launch_sing_dp0<BEMPPCUDA_LAPLACE_SLP>(prm, 0, st); break;
         case BEMPPCUDA_LAPLACE_DLP: err = launch_sing_dp0<BEMPPCUDA_LAPLACE_DLP>(prm, 0, st); break;
