@@ -1405,6 +1405,31 @@ def _points_case(torch, path, k, directions):
                                               precision=_lib.MIXED)), 0
 
 
+def _singular_p1_case(torch, name):
+    """The singular pass of a Helmholtz operator on P1 of regular_sphere(5), k = 5 (Sauter-Schwab pairs of
+    one space), added into a 4098 x 4098 complex128 matrix."""
+    from bempp_cuda import operators
+    from bempp_cuda.assembly import singular_into_dense
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+
+    sp = function_space(regular_sphere(5), "P", 1)
+    op = getattr(operators.boundary.helmholtz, name)(sp, sp, sp, 5.0)
+    n = sp.global_dof_count
+    out = torch.zeros((n, n), dtype=torch.complex128, device="cuda")
+    return (lambda: singular_into_dense(out, op.descriptor, sp, sp, op.parameters)), 0
+
+
+def _case_singular_p1_dlp(torch, args=None):
+    """The FP64 singular pass of the Helmholtz double layer on P1 of regular_sphere(5), k = 5."""
+    return _singular_p1_case(torch, "double_layer")
+
+
+def _case_singular_p1_slp(torch, args=None):
+    """The FP64 singular pass of the Helmholtz single layer on P1 of regular_sphere(5), k = 5."""
+    return _singular_p1_case(torch, "single_layer")
+
+
 def _case_potential_mixed(torch, args=None):
     """The mixed Helmholtz single-layer potential, 10 000 points, P1 on regular_sphere(5), k = 5."""
     return _points_case(torch, "potential.helmholtz.single_layer", 5.0, False)
@@ -1417,7 +1442,8 @@ def _case_farfield_mixed(torch, args=None):
 
 PROFILE_CASES = {"matmat_3x8192": _case_matmat, "gemv_16384": _case_gemv, "mixed_sym_l5": _case_mixed_sym,
                  "apply_l5": _case_apply, "p1_mixed_dlp_l5": _case_p1_mixed_dlp, "p1_fp64_dlp_l5": _case_p1_fp64_dlp,
-                 "p1_fp64_slp_l5": _case_p1_fp64_slp,
+                 "p1_fp64_slp_l5": _case_p1_fp64_slp, "singular_p1_dlp_l5": _case_singular_p1_dlp,
+                 "singular_p1_slp_l5": _case_singular_p1_slp,
                  "potential_mixed_l5": _case_potential_mixed, "farfield_mixed_l5": _case_farfield_mixed}
 
 
