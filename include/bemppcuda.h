@@ -180,11 +180,12 @@ typedef struct {
     double phase_radius; /* 2 x largest centroid-to-vertex distance of the grid, or 0 (unknown):
                             when |k| * phase_radius <= 1 the DP0 path factors exp(ikr) about the
                             centroid distance (|r - r_c| <= R_i + R_j holds for adjacent pairs too) */
-    int64_t mirror_weights_offset; /* dense DP0 output with the same space on both sides and every pair
+    int64_t mirror_weights_offset; /* dense output with the same space on both sides and every pair
                                       listed in both orders: the pairs whose weights start at this offset
                                       use a rule that is symmetric under exchanging test and trial points
                                       (the vertex-adjacent rule), so the pair with test < trial adds both
-                                      entries and its reverse adds nothing; 0 = off */
+                                      entries (blocks) and its reverse adds nothing -- DP0 scalar kernels,
+                                      and on P1 x P1 the single layers and hypersingular operators; 0 = off */
 } bemppcuda_singular_args;
 
 /* Potential / far-field evaluation (numba_kernels.py:1788-1849, 2281-2570). */
