@@ -356,7 +356,8 @@ static cudaError_t launch_sing_dp0(const SingParams &prm, int phase_class, cudaS
 
 }  // namespace bc
 
-#include "singular_p1.cuh"  // singular_p1, on SingParams, pair_in_range and SING_WARPS above
+#include "singular_p1.cuh"   // singular_p1 and singular_rwg, on SingParams, pair_in_range and SING_WARPS above
+#include "singular_rwg.cuh"
 
 namespace bc {
 
@@ -378,8 +379,23 @@ static cudaError_t launch_sing_p1(const SingParams &prm, int phase_class, cudaSt
     return cudaGetLastError();
 }
 
-// P1 x P1 (three shapes on both sides): the scalar kernels without the combined field, and the
-// three hypersingular operators; false when the pair list needs the generic kernel
+template <int ASM>
+static cudaError_t launch_sing_rwg(const SingParams &prm, int phase_class, cudaStream_t st) {
+    const unsigned blocks = (unsigned)((prm.npairs + SING_WARPS - 1) / SING_WARPS);
+    if (phase_class == 3)
+        singular_rwg<ASM, 3><<<blocks, 32 * SING_WARPS, 0, st>>>(prm);
+    else if (phase_class == 2)
+        singular_rwg<ASM, 2><<<blocks, 32 * SING_WARPS, 0, st>>>(prm);
+    else if (phase_class == 1)
+        singular_rwg<ASM, 1><<<blocks, 32 * SING_WARPS, 0, st>>>(prm);
+    else
+        singular_rwg<ASM, 0><<<blocks, 32 * SING_WARPS, 0, st>>>(prm);
+    return cudaGetLastError();
+}
+
+// Three shapes on both sides: P1 x P1 for the scalar kernels without the combined field and the
+// three hypersingular operators, RWG / SNC for the Maxwell operators; false when the pair list needs
+// the generic kernel
 static bool launch_p1_pairs(const bemppcuda_singular_args *a, const SingParams &prm, int phase_class,
                             cudaStream_t st, cudaError_t *err) {
     if (prm.nt != 3 || prm.ns != 3) return false;
@@ -406,6 +422,8 @@ static bool launch_p1_pairs(const bemppcuda_singular_args *a, const SingParams &
     case BEMPPCUDA_ASM_LAPLACE_HYP: *err = launch_sing_p1<1, BEMPPCUDA_LAPLACE_SLP>(prm, 0, st); return true;
     case BEMPPCUDA_ASM_HELM_HYP: *err = launch_sing_p1<2, BEMPPCUDA_HELMHOLTZ_SLP>(prm, phase_class, st); return true;
     case BEMPPCUDA_ASM_MODHELM_HYP: *err = launch_sing_p1<3, BEMPPCUDA_MODHELM_SLP>(prm, 0, st); return true;
+    case BEMPPCUDA_ASM_EFIE: *err = launch_sing_rwg<BEMPPCUDA_ASM_EFIE>(prm, phase_class, st); return true;
+    case BEMPPCUDA_ASM_MFIE: *err = launch_sing_rwg<BEMPPCUDA_ASM_MFIE>(prm, phase_class, st); return true;
     default: return false;
     }
 }
