@@ -107,6 +107,45 @@ def test_dispatcher_regular_and_singular_parts(oracle, sphere2):
         assert rel_fro(vals, ref_vals) < 1e-12, key
 
 
+SINGULAR_VALUE_KEYS = sorted(k for k in cases.BOUNDARY if k.endswith("_p1_p1") or k.endswith("_rwg_snc"))
+
+
+@pytest.mark.parametrize("key", SINGULAR_VALUE_KEYS)
+def test_singular_values_p1_and_rwg(oracle, sphere2, key):
+    """Per-pair singular values (the reference interface's flat output, no mirroring) of every P1 x P1 and
+    RWG / SNC operator against the oracle: the P1 and Maxwell singular kernels in values mode."""
+    from bempp_cuda import cuda_assemblers
+    from bempp_cuda.quadrature import SingularPairs
+
+    op, domain, dual = cases.boundary_operator(key, sphere2)
+    d = op.descriptor
+    dtype = np.complex128 if d.is_complex else np.float64
+    arrays = SingularPairs(sphere2, 4, dual.localised_space.support, domain.localised_space.support).arrays()
+    nt, ns = dual.number_of_shape_functions, domain.number_of_shape_functions
+    vals = np.zeros(nt * ns * len(arrays[3]), dtype=dtype)
+    cuda_assemblers.singular_assembler("cuda", d, sphere2, domain.localised_space, dual.localised_space,
+                                       *arrays, d.options, vals)
+    _, _, ref_vals = oracle.singular_values(d.kernel_type, d.assembly_type, d.options, domain.localised_space,
+                                            dual.localised_space, arrays, d.is_complex)
+    assert rel_fro(vals, ref_vals) < 1e-12, key
+
+
+@pytest.mark.parametrize("key", ["helmholtz_slp_p1_p1", "helmholtz_dlp_p1_p1", "helmholtz_hyp_p1_p1",
+                                 "maxwell_efie_rwg_snc", "maxwell_mfie_rwg_snc"])
+@pytest.mark.parametrize("k", [0.7, 0.9, 12.0])
+def test_singular_phase_classes_dense(oracle, sphere2, key, k):
+    """Whole matrices (dense singular scatter, vertex pairs mirrored where the kernel allows) in each
+    phase class of regular_sphere(2) (2R = 2/3): |k| 2R <= 1/2 (k = 0.7), <= 1 (0.9) and the full
+    reduction (12), against the oracle."""
+    path, dsp, tsp, _ = cases.BOUNDARY[key]
+    from bempp_cuda.space import function_space
+
+    domain, dual = function_space(sphere2, *dsp), function_space(sphere2, *tsp)
+    op = cases.resolve("boundary." + path)(domain, domain, dual, k)
+    ref = cases.oracle_dense(oracle, op, domain, dual)
+    assert rel_fro(_gpu_dense(op), ref) < 1e-12, (key, k)
+
+
 LEG_POT = load_golden("legacy_potential.npz")
 NUM_POT = load_golden("numba_potential.npz")
 POT_KEYS = sorted({k.split("__")[0] for k in LEG_POT.files})
