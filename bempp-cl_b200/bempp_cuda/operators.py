@@ -588,6 +588,7 @@ class PotentialOperator(object):
         self.device_interface = device_interface or "cuda"
         self.parameters = _params(parameters)
         self._points_dev = {}
+        self._map_dev = {}
 
     def _device_points(self):
         """The evaluation points as a (npoints, 3) device tensor on the current device."""
@@ -600,11 +601,46 @@ class PotentialOperator(object):
             self._points_dev[dev] = pts
         return pts
 
+    def _device_map(self):
+        """``space.map_to_full_grid`` on the current device as a gather: for element-local slot
+        e * nshape + i the dof index and its multiplier (index 0 and multiplier 0 outside the support).
+        Each slot has one dof, so the gathered product equals the sparse product bit for bit."""
+        import torch
+
+        dev = torch.cuda.current_device()
+        m = self._map_dev.get(dev)
+        if m is None:
+            sp = self.space
+            nshape = int(sp.number_of_shape_functions)
+            ne = int(sp.grid.number_of_elements)
+            l2g = _np.asarray(sp.local2global).reshape(-1, nshape)
+            mult = _np.asarray(sp.local_multipliers, dtype=_np.float64).reshape(-1, nshape)
+            sup = _np.asarray(sp.support_elements, dtype=_np.int64)
+            idx = _np.zeros((ne, nshape), dtype=_np.int64)
+            mlt = _np.zeros((ne, nshape), dtype=_np.float64)
+            idx[sup] = l2g[sup]
+            mlt[sup] = mult[sup]
+            m = (torch.as_tensor(idx.ravel(), device="cuda"), torch.as_tensor(mlt.ravel(), device="cuda"))
+            self._map_dev[dev] = m
+        return m
+
     def evaluate_device(self, coefficients):
-        """(kernel_dimension, npoints) complex device tensor for dof ``coefficients``."""
+        """(kernel_dimension, npoints) complex device tensor for dof ``coefficients`` (host array or
+        device tensor of the space's global dof count)."""
+        import torch
+
         from .assembly import evaluate_potential_device, precision_of
 
-        local = self.space.map_to_full_grid @ _np.asarray(coefficients)
+        n = int(self.space.global_dof_count)
+        if isinstance(coefficients, torch.Tensor):
+            coeff = coefficients.to(device="cuda", dtype=torch.complex128).reshape(-1)
+        else:
+            coeff = torch.as_tensor(_np.ascontiguousarray(_np.asarray(coefficients, dtype=_np.complex128)).reshape(-1),
+                                    device="cuda")
+        if coeff.shape[0] != n:
+            raise ValueError("expected %d coefficients, got %d" % (n, coeff.shape[0]))
+        idx, mlt = self._device_map()
+        local = coeff.index_select(0, idx) * mlt
         return evaluate_potential_device(self.space, self.descriptor, self._device_points(), local, self.parameters,
                                          precision=precision_of(self.device_interface))
 

@@ -392,3 +392,27 @@ def test_mixed_far_field_non_unit_directions(oracle, scale):
     got = _check(oracle, f(space, dirs, k, device_interface="cuda_mixed"), space, tol=1e-6)
     ref = _check(oracle, f(space, dirs, k), space)
     assert rel_fro(got, ref) < 1e-6
+
+
+@pytest.mark.parametrize("kind", [("P", 1), ("DP", 0), ("DP", 1), ("RWG", 0)])
+def test_device_coefficient_map_equals_sparse_map(kind):
+    """The operator's device gather of element-local coefficients (dof index times multiplier per slot,
+    zero outside the support) equals ``space.map_to_full_grid @ x`` bit for bit, for full and
+    restricted supports, host and device coefficient inputs."""
+    from bempp_cuda import operators
+    from bempp_cuda.shapes import regular_sphere
+    from bempp_cuda.space import function_space
+
+    grid = regular_sphere(3)
+    # the full grid, and the elements of the upper half (centroid z > 0)
+    vertices, elements = np.asarray(grid.vertices), np.asarray(grid.elements)
+    upper = np.flatnonzero(vertices[2][elements].mean(axis=0) > 0.0)
+    spaces = [function_space(grid, *kind), function_space(grid, *kind, support_elements=upper)]
+    rng = np.random.default_rng(11)
+    for sp in spaces:
+        pot = operators.potential.helmholtz.single_layer(sp, rng.standard_normal((3, 5)) * 3.0, 2.0)
+        c = rng.standard_normal(sp.global_dof_count) + 1j * rng.standard_normal(sp.global_dof_count)
+        idx, mlt = pot._device_map()
+        for coeff in (torch.as_tensor(c, device="cuda"), torch.as_tensor(c)):
+            got = coeff.to("cuda").index_select(0, idx) * mlt
+            assert np.array_equal(got.cpu().numpy(), sp.map_to_full_grid @ c)
