@@ -1006,7 +1006,7 @@ def breadth_measure(args, torch, fp64_peak=None, fp32_peak=None):
               "gpu_ms": pms, "kernel_ms": kms, "gpu_qpe_per_s": qpe / (kms * 1e-3),
               "roofline": {"bound": "fp64", "flops_per_qpe": 28, "qpe": qpe, "achieved": pach, "unit": "TFLOP/s",
                            "peak": fp64_peak, "frac": pach / fp64_peak if fp64_peak else None},
-              "note": "gpu_ms: public API call with the host map_to_full_grid product and coefficient upload; "
+              "note": "gpu_ms: public API call with the coefficient upload and the device gather to element slots; "
                       "kernel_ms: device-resident points and element coefficients (source table + evaluation)"}
     if not args.skip_cpu:
         # oracle (port) at 500 seeded points of the 10 000: CPU rate (scaled to 10 000) and FP64 parity
