@@ -180,9 +180,12 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_p1_mixed(RegParams prm, Q
     const double betd = CK ? prm.p[1] / prm.p[0] : (MH ? 1.0 : 0.0);
     const float bet = (float)betd;
 
-    const int64_t t0 = (int64_t)blockIdx.y * P1_TCHUNK;
+    // test elements per CTA: P1_TCHUNK, and for the Maxwell operators ceil(ntest / gridDim.y) <= P1_TCHUNK
+    // (their launch picks 16 on small grids; a runtime height made the scalar kernels slower)
+    const int rows = RWG ? (int)((prm.ntest + gridDim.y - 1) / gridDim.y) : P1_TCHUNK;
+    const int64_t t0 = (int64_t)blockIdx.y * rows;
     if (SYM && t0 >= ((int64_t)blockIdx.x + 1) * DP0_THREADS) return;  // below the diagonal
-    const int tcount = (int)min((int64_t)P1_TCHUNK, prm.ntest - t0);
+    const int tcount = (int)min((int64_t)rows, prm.ntest - t0);
     for (int idx = threadIdx.x; idx < tcount; idx += blockDim.x) {
         const int64_t t = prm.tsup[t0 + idx];
         Geom g;

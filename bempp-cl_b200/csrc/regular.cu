@@ -394,6 +394,20 @@ static cudaError_t launch_dp0(const RegParams &prm, const QuadRule &rule, int mi
     return cudaGetLastError();
 }
 
+// Row blocks of the Maxwell sweeps (regular_rwg, regular_p1_mixed on RWG): 32 test elements per
+// CTA, or 16 when 32 would leave the GPU under four waves of working CTAs (a symmetric sweep's CTAs
+// below the diagonal exit at once; 3 CTAs per SM).  The kernels take their chunk height as
+// ceil(ntest / gridDim.y).  L4 (2048 elements), regular pass: electric field 0.52 -> 0.40 ms FP64,
+// 0.39 -> 0.31 ms mixed; magnetic field 0.38 -> 0.35 ms mixed.  The P1 scalar kernels keep 32 rows
+// as a compile-time height: a runtime one made the mixed hypersingular operator 4 % slower at L5.
+static unsigned lin_row_blocks(int64_t ntrial, int64_t ntest, bool sym) {
+    static_assert(P1_TCHUNK == 32 && RWG_TCHUNK == 32, "row blocks of 32 or 16 test elements");
+    const int64_t cols = (ntrial + DP0_THREADS - 1) / DP0_THREADS;
+    const int64_t wave = (int64_t)bc_sm_count() * 3;
+    const int rows = cols * ((ntest + 31) / 32) / (sym ? 2 : 1) < 4 * wave ? 16 : 32;
+    return (unsigned)((ntest + rows - 1) / rows);
+}
+
 template <int ASM, int K, int NT, int NS, bool SYM>
 static void launch_p1_phase(const RegParams &prm, const QuadRule &rule, int phase_class, dim3 grid, cudaStream_t st) {
     // the phase classes only concern exp(ikr): one instance for Laplace and modified Helmholtz
@@ -510,8 +524,10 @@ static void p1_mixed_pair(const RegParams &prm, const QuadRule &rule, dim3 grid,
 template <int ASM, int K>
 static cudaError_t launch_p1_mixed(const RegParams &prm, const QuadRule &rule, int phase_class, bool sym,
                                    cudaStream_t st) {
+    constexpr bool rwg = ASM == BEMPPCUDA_ASM_EFIE || ASM == BEMPPCUDA_ASM_MFIE;
     dim3 grid((unsigned)((prm.ntrial + DP0_THREADS - 1) / DP0_THREADS),
-              (unsigned)((prm.ntest + P1_TCHUNK - 1) / P1_TCHUNK));
+              rwg ? lin_row_blocks(prm.ntrial, prm.ntest, sym)
+                  : (unsigned)((prm.ntest + P1_TCHUNK - 1) / P1_TCHUNK));
     if constexpr (ASM == BEMPPCUDA_ASM_SCALAR) {
         if (prm.tnshape == 3 && prm.snshape == 1) {
             p1_mixed_pair<K, 3, 1>(prm, rule, grid, st);
@@ -544,8 +560,7 @@ static cudaError_t launch_p1_mixed(const RegParams &prm, const QuadRule &rule, i
 // nonzero wavenumber (rwg.cuh).
 template <int ASM>
 static cudaError_t launch_rwg(const RegParams &prm, const QuadRule &rule, int phase_class, bool sym, cudaStream_t st) {
-    dim3 grid((unsigned)((prm.ntrial + DP0_THREADS - 1) / DP0_THREADS),
-              (unsigned)((prm.ntest + RWG_TCHUNK - 1) / RWG_TCHUNK));
+    dim3 grid((unsigned)((prm.ntrial + DP0_THREADS - 1) / DP0_THREADS), lin_row_blocks(prm.ntrial, prm.ntest, sym));
     if (sym) {
         if (phase_class == 3)  // complex wavenumber
             regular_rwg<ASM, 3, true><<<grid, DP0_THREADS, 0, st>>>(prm, rule);

@@ -156,9 +156,11 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_rwg(RegParams prm, QuadRu
     constexpr bool CK = PHC == 3;
     __shared__ TestBlockRWG sb;
 
-    const int64_t t0 = (int64_t)blockIdx.y * RWG_TCHUNK;
+    // test elements per CTA: ceil(ntest / gridDim.y) <= RWG_TCHUNK (the launch picks the row blocks)
+    const int rows = (int)((prm.ntest + gridDim.y - 1) / gridDim.y);
+    const int64_t t0 = (int64_t)blockIdx.y * rows;
     if (SYM && t0 >= ((int64_t)blockIdx.x + 1) * DP0_THREADS) return;  // below the diagonal
-    const int tcount = (int)min((int64_t)RWG_TCHUNK, prm.ntest - t0);
+    const int tcount = (int)min((int64_t)rows, prm.ntest - t0);
     for (int idx = threadIdx.x; idx < tcount; idx += blockDim.x) {
         const int64_t t = prm.tsup[t0 + idx];
         Geom g;
