@@ -77,75 +77,6 @@ struct TestBlockP1m {
     int v[P1_TCHUNK][3];
 };
 
-// MFIE block of an element pair from the nine moments M[u][v] = sum_pq w_p w_q H u(p) v(q), u, v in
-// {1, xi, eta} (index 0, 1, 2; H = e^{ikr} (ikr - 1) / r^3 times 4 pi, any phase factor of the pair left
-// out) and the two elements' vertex 0 and Jacobian columns: the formula of the header comment.
-__device__ __forceinline__ void mfie_block_moments(const double mre[3][3], const double mim[3][3],
-                                                   const double tv0[3], const double tj0[3], const double tj1[3],
-                                                   const double sv0[3], const double sj0[3], const double sj1[3],
-                                                   double blk_re[3][3], double blk_im[3][3]) {
-    const double *tJ[2] = {tj0, tj1}, *sJ[2] = {sj0, sj1};
-    // C_ab = J_t^a x J_s^b, and the vertex offsets P - v0 = J (a_i, b_i): (j1, j0, 0) per function
-    double C[2][2][3];
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 2; ++b) {
-            C[a][b][0] = tJ[a][1] * sJ[b][2] - tJ[a][2] * sJ[b][1];
-            C[a][b][1] = tJ[a][2] * sJ[b][0] - tJ[a][0] * sJ[b][2];
-            C[a][b][2] = tJ[a][0] * sJ[b][1] - tJ[a][1] * sJ[b][0];
-        }
-    constexpr int oa[3] = {0, 1, 0}, ob[3] = {1, 0, 0};  // (a_i, b_i)
-    // det(P_ti - P_sj, C_ab) = (v0_t - v0_s + J_t o_i - J_s o_j) . C_ab
-    double e[2][2], ti[3][2][2], sj[3][2][2];
-    const double dv[3] = {tv0[0] - sv0[0], tv0[1] - sv0[1], tv0[2] - sv0[2]};
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 2; ++b) {
-            e[a][b] = dot3(dv, C[a][b]);
-            const double t0 = dot3(tj1, C[a][b]), t1 = dot3(tj0, C[a][b]);
-            const double s0 = dot3(sj1, C[a][b]), s1 = dot3(sj0, C[a][b]);
-            ti[0][a][b] = t0;
-            ti[1][a][b] = t1;
-            ti[2][a][b] = 0.0;
-            sj[0][a][b] = s0;
-            sj[1][a][b] = s1;
-            sj[2][a][b] = 0.0;
-        }
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        // test side shifted moments: Mt[a][v] = M[1 + a][v] - o_ia M[0][v]
-        double mtr[2][3], mti[2][3];
-#pragma unroll
-        for (int a = 0; a < 2; ++a) {
-            const int o = a == 0 ? oa[i] : ob[i];
-#pragma unroll
-            for (int v = 0; v < 3; ++v) {
-                mtr[a][v] = o ? mre[1 + a][v] - mre[0][v] : mre[1 + a][v];
-                mti[a][v] = o ? mim[1 + a][v] - mim[0][v] : mim[1 + a][v];
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            double vr = 0.0, vi = 0.0;
-#pragma unroll
-            for (int a = 0; a < 2; ++a)
-#pragma unroll
-                for (int b = 0; b < 2; ++b) {
-                    const int o = b == 0 ? oa[j] : ob[j];
-                    const double nr = o ? mtr[a][1 + b] - mtr[a][0] : mtr[a][1 + b];
-                    const double ni = o ? mti[a][1 + b] - mti[a][0] : mti[a][1 + b];
-                    const double det = e[a][b] + ti[i][a][b] - sj[j][a][b];
-                    vr = fma(det, nr, vr);
-                    vi = fma(det, ni, vi);
-                }
-            blk_re[i][j] = vr;
-            blk_im[i][j] = vi;
-        }
-    }
-}
-
 // NT, NS: test / trial functions per element, 3 (P1, DP1, RWG / SNC) or 1 (a P0 space beside a P1 one: its
 // constant function takes the rule's weights in place of the P1 shape weights; scalar operators, no
 // symmetric sweep).

@@ -18,7 +18,11 @@
 //          sum_pq w w G (J_t r_i) . (J_s r_j) = P - c_sj . V_t - c_ti . V_s + (c_ti . c_sj) M[1][1],
 //        P = sum_ab (J_ta . J_sb) M[e_a][e_b], V_t = sum_a J_ta M[e_a][1],
 //        V_s = sum_b J_sb M[1][e_b]  (e_0 = xi, e_1 = eta).
-//  MFIE: with H = w_p w_q G (ikr - 1) / r^2, d = x - y and d . (u x v) = u . (v x d),
+//  MFIE: with P_ti = v0_t + c_ti the vertex function i points away from, J_t r_i(p) = x_p - P_ti,
+//        so (x - y) . (J_t r_i x J_s r_j) = (P_ti - P_sj) . (J_t r_i x J_s r_j): the same nine
+//        moments, of H = G (ikr - 1) / r^2 in place of G, give the block (mfie_block_moments:
+//        MFIE_ij = sum_ab det(P_ti - P_sj, J_t^a, J_s^b) times the moments shifted by (a_i, b_i),
+//        (a_j, b_j)).  The singular kernel sums, with H = w_p w_q G (ikr - 1) / r^2, d = x - y,
 //          B(p) = sum_q H (w_s(q) x d),  C(p) = sum_q H d,
 //          MFIE_ij = PB - c_sj . PC - c_ti . QB + c_ti . (c_sj x QC),
 //        PB = sum_p w_t(p) . B(p), PC = sum_p C(p) x w_t(p), QB = sum_p B(p), QC = sum_p C(p).
@@ -43,6 +47,7 @@ struct TestBlockRWG {
     double j0[RWG_TCHUNK][3];
     double j1[RWG_TCHUNK][3];
     double c[RWG_TCHUNK][3];
+    double v0[RWG_TCHUNK][3];   // vertex 0 (MFIE moments)
     double fac[RWG_TCHUNK][3];  // edge length times multiplier of each test function
     int64_t row[RWG_TCHUNK][3];
     int v[RWG_TCHUNK][3];
@@ -149,6 +154,75 @@ __device__ __forceinline__ void mfie_block(double pbr, double pbi, const double 
         }
 }
 
+// MFIE block of an element pair from the nine moments M[u][v] = sum_pq w_p w_q H u(p) v(q), u, v in
+// {1, xi, eta} (index 0, 1, 2; H = e^{ikr} (ikr - 1) / r^3 times 4 pi, any phase factor of the pair left
+// out) and the two elements' vertex 0 and Jacobian columns: the formula of the header comment.
+__device__ __forceinline__ void mfie_block_moments(const double mre[3][3], const double mim[3][3],
+                                                   const double tv0[3], const double tj0[3], const double tj1[3],
+                                                   const double sv0[3], const double sj0[3], const double sj1[3],
+                                                   double blk_re[3][3], double blk_im[3][3]) {
+    const double *tJ[2] = {tj0, tj1}, *sJ[2] = {sj0, sj1};
+    // C_ab = J_t^a x J_s^b, and the vertex offsets P - v0 = J (a_i, b_i): (j1, j0, 0) per function
+    double C[2][2][3];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            C[a][b][0] = tJ[a][1] * sJ[b][2] - tJ[a][2] * sJ[b][1];
+            C[a][b][1] = tJ[a][2] * sJ[b][0] - tJ[a][0] * sJ[b][2];
+            C[a][b][2] = tJ[a][0] * sJ[b][1] - tJ[a][1] * sJ[b][0];
+        }
+    constexpr int oa[3] = {0, 1, 0}, ob[3] = {1, 0, 0};  // (a_i, b_i)
+    // det(P_ti - P_sj, C_ab) = (v0_t - v0_s + J_t o_i - J_s o_j) . C_ab
+    double e[2][2], ti[3][2][2], sj[3][2][2];
+    const double dv[3] = {tv0[0] - sv0[0], tv0[1] - sv0[1], tv0[2] - sv0[2]};
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            e[a][b] = dot3(dv, C[a][b]);
+            const double t0 = dot3(tj1, C[a][b]), t1 = dot3(tj0, C[a][b]);
+            const double s0 = dot3(sj1, C[a][b]), s1 = dot3(sj0, C[a][b]);
+            ti[0][a][b] = t0;
+            ti[1][a][b] = t1;
+            ti[2][a][b] = 0.0;
+            sj[0][a][b] = s0;
+            sj[1][a][b] = s1;
+            sj[2][a][b] = 0.0;
+        }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        // test side shifted moments: Mt[a][v] = M[1 + a][v] - o_ia M[0][v]
+        double mtr[2][3], mti[2][3];
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+            const int o = a == 0 ? oa[i] : ob[i];
+#pragma unroll
+            for (int v = 0; v < 3; ++v) {
+                mtr[a][v] = o ? mre[1 + a][v] - mre[0][v] : mre[1 + a][v];
+                mti[a][v] = o ? mim[1 + a][v] - mim[0][v] : mim[1 + a][v];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            double vr = 0.0, vi = 0.0;
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int b = 0; b < 2; ++b) {
+                    const int o = b == 0 ? oa[j] : ob[j];
+                    const double nr = o ? mtr[a][1 + b] - mtr[a][0] : mtr[a][1 + b];
+                    const double ni = o ? mti[a][1 + b] - mti[a][0] : mti[a][1 + b];
+                    const double det = e[a][b] + ti[i][a][b] - sj[j][a][b];
+                    vr = fma(det, nr, vr);
+                    vi = fma(det, ni, vi);
+                }
+            blk_re[i][j] = vr;
+            blk_im[i][j] = vi;
+        }
+    }
+}
+
 template <int ASM, int PHC, bool SYM>
 __global__ void __launch_bounds__(DP0_THREADS) regular_rwg(RegParams prm, QuadRule rule) {
     constexpr bool EFIE = ASM == BEMPPCUDA_ASM_EFIE;
@@ -171,6 +245,7 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_rwg(RegParams prm, QuadRu
             sb.j0[idx][d] = g.j0[d];
             sb.j1[idx][d] = g.j1[d];
             sb.c[idx][d] = __ldg(prm.tg + (22 + d) * prm.tne + t);
+            sb.v0[idx][d] = g.v0[d];
             sb.v[idx][d] = __ldg(prm.tel + 3 * t + d);
         }
 #pragma unroll
@@ -217,21 +292,17 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_rwg(RegParams prm, QuadRu
         }
         const double tj0[3] = {sb.j0[tt][0], sb.j0[tt][1], sb.j0[tt][2]};
         const double tj1[3] = {sb.j1[tt][0], sb.j1[tt][1], sb.j1[tt][2]};
-        // EFIE: moments M[u][v]; MFIE: PB, PC, QB, QC (complex)
+        // moments M[u][v] = sum_pq w_p w_q K u(p) v(q), u, v in {1, xi, eta}, of K = G (EFIE) or
+        // H = G (ikr - 1) / r^2 (MFIE), both times 4 pi and without the pair's phase factor
         double mre[3][3], mim[3][3];
-        double pbr = 0.0, pbi = 0.0, pcr[3], pci[3], qbr[3], qbi[3], qcr[3], qci[3];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
+        for (int a = 0; a < 3; ++a)
 #pragma unroll
             for (int b = 0; b < 3; ++b) mre[a][b] = mim[a][b] = 0.0;
-            pcr[a] = pci[a] = qbr[a] = qbi[a] = qcr[a] = qci[a] = 0.0;
-        }
         for (int p = 0; p < NQ6; ++p) {
             // x_p relative to the trial vertex 0: d = xs - w_s(q)
             const double xs[3] = {sb.x[tt][p][0] - gs.v0[0], sb.x[tt][p][1] - gs.v0[1], sb.x[tt][p][2] - gs.v0[2]};
-            double tre[3] = {0.0, 0.0, 0.0}, tim[3] = {0.0, 0.0, 0.0};  // EFIE: sum_q w_q G v(q)
-            double br[3] = {0.0, 0.0, 0.0}, bi[3] = {0.0, 0.0, 0.0};    // MFIE: B(p) / w_p
-            double cr[3] = {0.0, 0.0, 0.0}, ci[3] = {0.0, 0.0, 0.0};    // MFIE: C(p) / w_p
+            double tre[3] = {0.0, 0.0, 0.0}, tim[3] = {0.0, 0.0, 0.0};  // sum_q w_q K v(q)
 #pragma unroll
             for (int q = 0; q < NQ6; ++q) {
                 const double d[3] = {xs[0] - ws[q][0], xs[1] - ws[q][1], xs[2] - ws[q][2]};
@@ -250,82 +321,40 @@ __global__ void __launch_bounds__(DP0_THREADS) regular_rwg(RegParams prm, QuadRu
                     sn *= am;
                     cs *= am;
                 }
+                // EFIE: G 4 pi = (cs + i sn) / r; MFIE: H 4 pi = (cs + i sn)(-(1 + ki r) + i k r) / r^3
+                // (the phase exp(ik r_c) and 1 / (4 pi) are applied per pair)
+                double gr, gi;
                 if (EFIE) {
-                    // w_q G 4 pi (the phase exp(ik r_c) and 1 / (4 pi) are applied per pair)
-                    const double gr = cs * rinv, gi = sn * rinv;
-                    const double v[3] = {rule.w[q], rule.sw[q][1], rule.sw[q][2]};  // w_q (1, xi_q, eta_q)
-#pragma unroll
-                    for (int b = 0; b < 3; ++b) {
-                        tre[b] = fma(gr, v[b], tre[b]);
-                        tim[b] = fma(gi, v[b], tim[b]);
-                    }
+                    gr = cs * rinv;
+                    gi = sn * rinv;
                 } else {
-                    // w_q G (ikr - 1) / r^2 times 4 pi: (cs + i sn)(-1 + i k r) w_q / r^3
-                    const double f = rule.w[q] * (rinv * rinv * rinv);
-                    const double kq = kr * r;
-                    double hr, hi;
-                    if (CK) {
-                        const double a = fma(ki, r, 1.0);  // -(ikr - 1) real part: 1 + ki r
-                        hr = -fma(kq, sn, a * cs) * f;
-                        hi = fma(kq, cs, -a * sn) * f;
-                    } else {
-                        hr = -fma(kq, sn, cs) * f;
-                        hi = fma(kq, cs, -sn) * f;
-                    }
-                    double wxd[3];
-                    wxd[0] = fma(ws[q][1], d[2], -ws[q][2] * d[1]);
-                    wxd[1] = fma(ws[q][2], d[0], -ws[q][0] * d[2]);
-                    wxd[2] = fma(ws[q][0], d[1], -ws[q][1] * d[0]);
+                    const double f = rinv * rinv * rinv, kq = kr * r;
+                    const double a = CK ? fma(ki, r, 1.0) : 1.0;
+                    gr = -fma(kq, sn, a * cs) * f;
+                    gi = fma(kq, cs, -a * sn) * f;
+                }
+                const double v[3] = {rule.w[q], rule.sw[q][1], rule.sw[q][2]};  // w_q (1, xi_q, eta_q)
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        br[c] = fma(hr, wxd[c], br[c]);
-                        bi[c] = fma(hi, wxd[c], bi[c]);
-                        cr[c] = fma(hr, d[c], cr[c]);
-                        ci[c] = fma(hi, d[c], ci[c]);
-                    }
+                for (int b = 0; b < 3; ++b) {
+                    tre[b] = fma(gr, v[b], tre[b]);
+                    tim[b] = fma(gi, v[b], tim[b]);
                 }
             }
-            if (EFIE) {
-                const double u[3] = {rule.w[p], rule.sw[p][1], rule.sw[p][2]};  // w_p (1, xi_p, eta_p)
+            const double u[3] = {rule.w[p], rule.sw[p][1], rule.sw[p][2]};  // w_p (1, xi_p, eta_p)
 #pragma unroll
-                for (int a = 0; a < 3; ++a)
+            for (int a = 0; a < 3; ++a)
 #pragma unroll
-                    for (int b = 0; b < 3; ++b) {
-                        mre[a][b] = fma(u[a], tre[b], mre[a][b]);
-                        mim[a][b] = fma(u[a], tim[b], mim[a][b]);
-                    }
-            } else {
-                // w_p w_t(p) = J_t (w_p xi_p, w_p eta_p)
-                double wt[3];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) wt[c] = fma(tj1[c], rule.sw[p][2], tj0[c] * rule.sw[p][1]);
-                const double wp = rule.w[p];
-                pbr += dot3(wt, br);
-                pbi += dot3(wt, bi);
-                // C x w_t (w_p inside wt)
-                pcr[0] += fma(cr[1], wt[2], -cr[2] * wt[1]);
-                pcr[1] += fma(cr[2], wt[0], -cr[0] * wt[2]);
-                pcr[2] += fma(cr[0], wt[1], -cr[1] * wt[0]);
-                pci[0] += fma(ci[1], wt[2], -ci[2] * wt[1]);
-                pci[1] += fma(ci[2], wt[0], -ci[0] * wt[2]);
-                pci[2] += fma(ci[0], wt[1], -ci[1] * wt[0]);
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    qbr[c] = fma(wp, br[c], qbr[c]);
-                    qbi[c] = fma(wp, bi[c], qbi[c]);
-                    qcr[c] = fma(wp, cr[c], qcr[c]);
-                    qci[c] = fma(wp, ci[c], qci[c]);
+                for (int b = 0; b < 3; ++b) {
+                    mre[a][b] = fma(u[a], tre[b], mre[a][b]);
+                    mim[a][b] = fma(u[a], tim[b], mim[a][b]);
                 }
-            }
         }
-        // c_t = (J_t (0, 1), J_t (1, 0), 0) = (j1_t, j0_t, 0); likewise c_s
-        const double *ctv[2] = {tj1, tj0};
-        const double *csv[2] = {gs.j1, gs.j0};
         double blk_re[3][3], blk_im[3][3];
         if (EFIE) {
             efie_block<CK>(mre, mim, tj0, tj1, gs.j0, gs.j1, kr, ki, blk_re, blk_im);
         } else {
-            mfie_block(pbr, pbi, pcr, pci, qbr, qbi, qcr, qci, tj0, tj1, gs.j0, gs.j1, blk_re, blk_im);
+            const double tv0[3] = {sb.v0[tt][0], sb.v0[tt][1], sb.v0[tt][2]};
+            mfie_block_moments(mre, mim, tv0, tj0, tj1, gs.v0, gs.j0, gs.j1, blk_re, blk_im);
         }
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
